@@ -1,0 +1,492 @@
+// rs_capi.cu — the extern "C" boundary (include/rs_b200.h).
+//
+// Parameter defaults are the reference's constants.hpp set
+// (src/constants.hpp:185-350); derived quantities follow set_parameters
+// (fun.cu:1984-2058).  Contexts own only small workspaces (reduction partials,
+// per-row tip data) allocated at creation; no launcher allocates.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "rs_kernels.cuh"
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_check(const char *what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(RS_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return RS_OK;
+}
+
+}  // namespace
+
+struct rs_ctx {
+  rs_params p;
+  rs_derived d;
+  rs::StepCoef K;
+  rs::TfcCoef T;
+  int device;
+  rs::BlockPartial *partials;
+  int max_partials;
+  int *row_last;
+  double *row_f, *row_g;
+};
+
+extern "C" {
+
+int rs_abi_version(void) { return RS_ABI_VERSION; }
+const char *rs_last_error(void) { return g_err; }
+size_t rs_sizeof_params(void) { return sizeof(rs_params); }
+size_t rs_sizeof_step_args(void) { return sizeof(rs_step_args); }
+
+int rs_default_params(rs_params *p) {
+  if (!p) return fail(RS_E_INVALID, "rs_default_params: null");
+  memset(p, 0, sizeof(*p));
+  // Simulation namespace (constants.hpp:253-350)
+  p->nx_all = 768;
+  p->ny_all = 832;
+  p->i_tip_target = 768 - 268;
+  p->periodic_j = 1;        // boundaryCondition 0
+  p->tfc = 1;               // ifTFC 1 (main.cu:17)
+  p->one_eps = 1;           // if_1_eps
+  p->vp_ramp = 0;           // if_Vp_ramp
+  p->n_orientation = 1;
+  // Material namespace (constants.hpp:185-237)
+  p->cinf = 0.632514105;
+  p->W0 = 0.25;
+  p->S = 5.0;
+  p->Gamma = 199.0;
+  p->muk0 = 0.57;
+  p->Tmelt = 2161.59;
+  p->T_ref = 2118.35;
+  p->Dl = 2.05;
+  p->DT = 1.1e4;
+  p->latent_heat = 22003.0;
+  p->molar_weight = 64.418;
+  p->num_moles = 93353.43470588748;
+  p->cp = 40.0;
+  p->RR = 8.3145;
+  p->v0 = 1.17e-5;
+  p->AA = 12.0;             // SS == 5
+  p->ke = 0.8146631243899296;
+  p->dx = 0.6;              // SS == 5
+  p->dt = 0.0;
+  p->GG = 10 * 0.001;
+  p->Vp = 1.0;
+  p->eps1 = 0.06;
+  p->eps2 = 0.0;
+  p->epk1 = 0.15;
+  p->delta_initial = -1.0;
+  p->ratio_dxT_dx = 10;
+  p->orientation[0] = p->orientation[4] = p->orientation[8] = 1.0;  // Euler angles 0
+  p->Tcold = 2000.0;
+  p->length_sample_um = 50.0;
+  p->total_time_ns = 120.0 * 1000.0;
+  p->num_fields_output = p->num_tip_output = p->num_check_point_output = 120;
+  return RS_OK;
+}
+
+int rs_derive(const rs_params *p, rs_derived *d) {
+  if (!p || !d) return fail(RS_E_INVALID, "rs_derive: null");
+  memset(d, 0, sizeof(*d));
+  const double SS = p->S, W0 = p->W0, dx = p->dx;
+  d->W = SS * W0;
+  d->tau0 = (SS * W0) * (SS * W0) / (p->Gamma * p->muk0);
+  d->deltaT0 = p->Tmelt - p->T_ref;
+  d->a1 = 2.0 * std::sqrt(2.0) / 3.0;
+  const double latentHeat2 = p->latent_heat * p->num_moles;
+  const double surface_tension = p->Gamma * 1e-9 * latentHeat2 / p->Tmelt;
+  d->hh = surface_tension / (d->a1 * SS * W0 * 1.0e-9);
+  d->h0 = p->RR * p->Tmelt / p->v0;
+  const double DD = p->Dl * d->tau0 / ((SS * W0) * (SS * W0));
+  double dt = p->dt;
+  if (!(dt > 0)) {
+    dt = 0.6 * dx * dx / (4.0 * DD);
+    if (dt > 0.6 * dx * dx / 4.0) dt = 0.6 * dx * dx / 4.0;
+  }
+  d->dt = dt;
+  const double tau0 = d->tau0;
+  d->total_step = (int64_t)(p->total_time_ns / (tau0 * dt));
+  if (p->num_fields_output > 0) d->step_fields = (int32_t)(p->total_time_ns / p->num_fields_output / (tau0 * dt));
+  if (p->num_tip_output > 0) d->step_tip = (int32_t)(p->total_time_ns / p->num_tip_output / (tau0 * dt));
+  if (p->num_check_point_output > 0)
+    d->step_check_point = (int32_t)(p->total_time_ns / p->num_check_point_output / (tau0 * dt));
+  if (p->step_pull_back > 0)
+    d->step_pull_back = p->step_pull_back;
+  else if (p->vp_ramp)
+    d->step_pull_back = (int32_t)(SS * W0 * dx / (1.0 * dt * tau0));
+  else
+    d->step_pull_back = (int32_t)(SS * W0 * dx / (p->Vp * dt * tau0));
+  const int r = p->ratio_dxT_dx > 0 ? p->ratio_dxT_dx : 10;
+  const double DDT = p->DT * tau0 / ((SS * W0 * r) * (SS * W0 * r));
+  const double dtT = 0.9 * dx * dx / (4.0 * DDT);
+  int ratio = 1;
+  if (dtT < dt) ratio = (int)std::ceil(dt / dtT);
+  d->ratio_dt_dtT = ratio;
+  d->dtT = dt / ratio;
+  d->length_sample = std::ceil(p->length_sample_um * 1000 / (dx * SS * W0 * r)) * (dx * SS * W0 * r);
+  d->NxT = (int32_t)(d->length_sample / (dx * SS * W0 * r) + 2);
+  d->NxT_all = (int32_t)(std::ceil(1.0 * d->NxT / 64) * 64);
+  d->NyT = ((p->ny_all - 2) / r) + 2;
+  d->NyT_all = (int32_t)(std::ceil(1.0 * d->NyT / 4) * 4);
+  d->Thot = p->Tcold + p->GG * d->length_sample;
+  d->i_left_end_initial =
+      (int32_t)((p->Tmelt - d->deltaT0 - p->Tcold) / (p->GG * dx * SS * W0) - p->i_tip_target);
+  return RS_OK;
+}
+
+static int validate_params(const rs_params *p) {
+  if (p->n_orientation != 1) return fail(RS_E_UNSUPPORTED, "n_orientation=%d: only one orientation is supported", p->n_orientation);
+  if (p->nx_all < 8 || p->ny_all < 8) return fail(RS_E_INVALID, "grid %dx%d: need at least 8x8 cells", p->nx_all, p->ny_all);
+  if ((int64_t)p->nx_all * p->ny_all > (int64_t)1 << 31)
+    return fail(RS_E_INVALID, "grid %dx%d exceeds 2^31 cells", p->nx_all, p->ny_all);
+  if (!(p->dx > 0) || !(p->W0 > 0) || !(p->S > 0) || !(p->Gamma > 0) || !(p->muk0 > 0) || !(p->v0 > 0))
+    return fail(RS_E_INVALID, "non-positive material or grid constant");
+  if (!(p->cinf > 0 && p->cinf < 1)) return fail(RS_E_INVALID, "cinf=%g outside (0,1)", p->cinf);
+  if (p->tfc && p->ratio_dxT_dx < 1) return fail(RS_E_INVALID, "ratio_dxT_dx=%d", p->ratio_dxT_dx);
+  for (int k = 0; k < 9; ++k)
+    if (!std::isfinite(p->orientation[k])) return fail(RS_E_INVALID, "orientation[%d] not finite", k);
+  return RS_OK;
+}
+
+static void make_coef(const rs_params *p, const rs_derived *d, rs::StepCoef *K, rs::TfcCoef *T) {
+  memset(K, 0, sizeof(*K));
+  K->nx = p->nx_all;
+  K->ny = p->ny_all;
+  K->pitch = p->nx_all;
+  K->jmin = p->periodic_j ? p->ny_all - 2 : 1;
+  K->jmax = p->periodic_j ? 1 : p->ny_all - 2;
+  K->one_eps = p->one_eps;
+  K->tfc = p->tfc;
+  K->ratio = p->ratio_dxT_dx;
+  K->NxT_all = d->NxT_all;
+  K->NyT_all = d->NyT_all;
+  const double dx = p->dx;
+  K->dx = dx;
+  K->inv_2dx = 1.0 / (2.0 * dx);
+  K->inv_dx2 = 1.0 / (dx * dx);
+  K->inv_4dx2 = 1.0 / (4. * dx * dx);
+  K->inv_2dx2 = 1.0 / (2.0 * dx * dx);
+  K->dt = d->dt;
+  K->eps1 = p->eps1;
+  K->eps2 = p->eps2;
+  K->epk1 = p->epk1;
+  K->ox1 = p->orientation[0];
+  K->ox2 = p->orientation[1];
+  K->oy1 = p->orientation[3];
+  K->oy2 = p->orientation[4];
+  K->oz1 = p->orientation[6];
+  K->oz2 = p->orientation[7];
+  K->drive = 1.0 / (2.0 * d->hh * p->v0);
+  K->inv_h0v0 = 1.0 / (d->h0 * p->v0);
+  K->cfac = d->dt * p->Dl / (p->Gamma * p->muk0) / (dx * dx);
+  K->AA = p->AA;
+  K->RR = p->RR;
+  K->cinf = p->cinf;
+  K->Tmelt = p->Tmelt;
+  K->deltaT0 = d->deltaT0;
+  K->dxT = dx * p->ratio_dxT_dx;
+  K->noise_amp = p->noise_amplitude > 0 ? p->noise_amplitude * std::sqrt(d->dt) : 0.0;
+  K->seed_lo = (uint32_t)p->seed;
+  K->seed_hi = (uint32_t)(p->seed >> 32);
+  K->W0 = p->W0;
+  K->S = p->S;
+  K->Lref = std::log(p->cinf / (1.0 - p->cinf));
+
+  memset(T, 0, sizeof(*T));
+  T->nx = p->nx_all;
+  T->ny = p->ny_all;
+  T->pitch = p->nx_all;
+  T->ratio = p->ratio_dxT_dx;
+  T->NxT = d->NxT;
+  T->NyT = d->NyT;
+  T->NxT_all = d->NxT_all;
+  T->NyT_all = d->NyT_all;
+  T->jTmin = p->periodic_j ? d->NyT - 2 : 1;
+  T->jTmax = p->periodic_j ? 1 : d->NyT - 2;
+  T->ratio_dt_dtT = d->ratio_dt_dtT;
+  T->Sint = (int32_t)p->S;
+  T->Tcold = p->Tcold;
+  T->Thot = d->Thot;
+  T->dx = dx;
+  T->dxT = dx * p->ratio_dxT_dx;
+  T->dtT = d->dtT;
+  T->Lcp = p->latent_heat / p->cp;
+  T->W0 = p->W0;
+  T->GG = p->GG;
+  T->S = p->S;
+  T->DT = p->DT;
+  T->Gmuk = p->Gamma * p->muk0;
+}
+
+int rs_create(const rs_params *p, rs_ctx **out) {
+  if (!p || !out) return fail(RS_E_INVALID, "rs_create: null argument");
+  *out = nullptr;
+  int rc = validate_params(p);
+  if (rc) return rc;
+  rs_ctx *c = new (std::nothrow) rs_ctx;
+  if (!c) return fail(RS_E_INVALID, "rs_create: out of host memory");
+  memset(c, 0, sizeof(*c));
+  c->p = *p;
+  rs_derive(p, &c->d);
+  make_coef(&c->p, &c->d, &c->K, &c->T);
+  if (cudaGetDevice(&c->device) != cudaSuccess) {
+    delete c;
+    return fail(RS_E_CUDA, "rs_create: no CUDA device");
+  }
+  const int ni = p->nx_all - 2, nj = p->ny_all - 2;
+  c->max_partials = ((ni + 31) / 32) * ((nj + 7) / 8) + (p->ny_all + 7) / 8 + 64;
+  cudaError_t e = cudaMalloc(&c->partials, sizeof(rs::BlockPartial) * c->max_partials);
+  if (e == cudaSuccess) e = cudaMalloc(&c->row_last, sizeof(int) * p->ny_all);
+  if (e == cudaSuccess) e = cudaMalloc(&c->row_f, sizeof(double) * p->ny_all);
+  if (e == cudaSuccess) e = cudaMalloc(&c->row_g, sizeof(double) * p->ny_all);
+  if (e != cudaSuccess) {
+    rs_destroy(c);
+    return fail(RS_E_CUDA, "rs_create: cudaMalloc: %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return RS_OK;
+}
+
+int rs_destroy(rs_ctx *c) {
+  if (!c) return RS_OK;
+  cudaFree(c->partials);
+  cudaFree(c->row_last);
+  cudaFree(c->row_f);
+  cudaFree(c->row_g);
+  delete c;
+  return RS_OK;
+}
+
+int rs_get_derived(const rs_ctx *c, rs_derived *d) {
+  if (!c || !d) return fail(RS_E_INVALID, "rs_get_derived: null");
+  *d = c->d;
+  return RS_OK;
+}
+
+static int check_fields(const rs_ctx *c, const rs_fields *f, const char *what, bool need_c = true) {
+  if (!f) return fail(RS_E_INVALID, "%s: null field set", what);
+  if (f->precision != RS_F64 && f->precision != RS_F32)
+    return fail(RS_E_INVALID, "%s: precision tag %d", what, f->precision);
+  if (!f->psi || (need_c && !f->c)) return fail(RS_E_INVALID, "%s: psi and c are required", what);
+  const int pitch = f->pitch ? f->pitch : c->p.nx_all;
+  if (pitch != c->p.nx_all) return fail(RS_E_UNSUPPORTED, "%s: pitch %d != nx_all %d", what, pitch, c->p.nx_all);
+  const size_t al = f->precision == RS_F64 ? 8 : 4;
+  if (((uintptr_t)f->psi | (uintptr_t)f->c | (uintptr_t)f->phi) % al)
+    return fail(RS_E_INVALID, "%s: misaligned field pointer", what);
+  return RS_OK;
+}
+
+static rs::StepScalars step_scalars(const rs_ctx *c, const rs_step_args *a) {
+  const rs_params &p = c->p;
+  rs::StepScalars P;
+  memset(&P, 0, sizeof(P));
+  P.step = a->step;
+  // get_delta (fun.cu:1610-1619): delta(i) = d0 + d1 i
+  const double d1 = p.GG * p.dx * p.S * p.W0 / c->d.deltaT0;
+  P.d1 = d1;
+  P.d0 = p.delta_initial + d1 * (double)(-p.i_tip_target + a->i_offset_history - p.i_offset_history_initial) -
+         p.GG * (a->l_offset_Vp - p.l_offset_Vp_initial) * p.S * p.W0 / c->d.deltaT0;
+  P.pull_back = a->pull_back ? 1 : 0;
+  P.i_offset = a->i_offset;
+  P.i_left_end_T = a->i_left_end_T;
+  P.T_coarse = (const double *)a->T_coarse;
+  return P;
+}
+
+int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_step_args *a, rs_stream_t stream) {
+  if (!c || !a) return fail(RS_E_INVALID, "rs_step: null argument");
+  int rc = check_fields(c, cur, "rs_step cur");
+  if (!rc) rc = check_fields(c, next, "rs_step next");
+  if (rc) return rc;
+  if (cur->precision != next->precision) return fail(RS_E_INVALID, "rs_step: cur/next precision differ");
+  if (cur->psi == next->psi || cur->c == next->c || (next->phi && (next->phi == cur->psi || next->phi == cur->c)))
+    return fail(RS_E_INVALID, "rs_step: cur and next alias");
+  if (c->p.tfc && !a->T_coarse) return fail(RS_E_INVALID, "rs_step: TFC needs T_coarse");
+  if (c->p.tfc && cur->precision == RS_F32)
+    return fail(RS_E_UNSUPPORTED, "rs_step: the FP32 path supports the frozen temperature only");
+  const rs::StepScalars P = step_scalars(c, a);
+  cudaStream_t st = (cudaStream_t)stream;
+  const bool red = a->mass_out || a->itip_out;
+  int nb = 0;
+  int lr;
+  if (cur->precision == RS_F64)
+    lr = rs::launch_step_f64(c->K, P, (const double *)cur->psi, (const double *)cur->c, (double *)next->psi,
+                             (double *)next->c, (double *)next->phi, red ? c->partials : nullptr,
+                             c->max_partials, &nb, st);
+  else
+    lr = rs::launch_step_f32(c->K, P, (const float *)cur->psi, (const float *)cur->c, (float *)next->psi,
+                             (float *)next->c, (float *)next->phi, red ? c->partials : nullptr,
+                             c->max_partials, &nb, st);
+  if (lr) return fail(RS_E_INVALID, "rs_step: grid too large for the reduction workspace");
+  if ((rc = cuda_check("rs_step"))) return rc;
+  if (red) {
+    const double off = cur->precision == RS_F32 ? (double)(c->p.nx_all - 2) * (c->p.ny_all - 2) * c->p.cinf : 0.0;
+    rs::launch_reduce_partials(c->partials, nb, off, a->mass_out, a->itip_out, st);
+    if ((rc = cuda_check("rs_step reduce"))) return rc;
+  }
+  return RS_OK;
+}
+
+int rs_pull_back(rs_ctx *c, const rs_fields *cur, const rs_fields *next, int32_t i_offset, rs_stream_t stream) {
+  if (!c) return fail(RS_E_INVALID, "rs_pull_back: null ctx");
+  int rc = check_fields(c, cur, "rs_pull_back cur");
+  if (!rc) rc = check_fields(c, next, "rs_pull_back next");
+  if (rc) return rc;
+  if (cur->precision != next->precision) return fail(RS_E_INVALID, "rs_pull_back: precision differs");
+  if (cur->psi == next->psi || cur->c == next->c) return fail(RS_E_INVALID, "rs_pull_back: cur and next alias");
+  rs::launch_pull_back(cur->precision, c->K, cur->c, cur->psi, cur->phi, next->c, next->psi, next->phi, i_offset,
+                       (cudaStream_t)stream);
+  return cuda_check("rs_pull_back");
+}
+
+int rs_itip(rs_ctx *c, const rs_fields *f, int32_t *d_itip, rs_stream_t stream) {
+  if (!c || !d_itip) return fail(RS_E_INVALID, "rs_itip: null argument");
+  int rc = check_fields(c, f, "rs_itip");
+  if (rc) return rc;
+  int nb = 0;
+  if (rs::launch_grid_partials(f->precision, c->K, f->c, f->psi, c->p.cinf, c->partials, c->max_partials, &nb,
+                               (cudaStream_t)stream))
+    return fail(RS_E_INVALID, "rs_itip: workspace too small");
+  rs::launch_reduce_partials(c->partials, nb, 0.0, nullptr, d_itip, (cudaStream_t)stream);
+  return cuda_check("rs_itip");
+}
+
+int rs_mass(rs_ctx *c, const rs_fields *f, double *d_mass, rs_stream_t stream) {
+  if (!c || !d_mass) return fail(RS_E_INVALID, "rs_mass: null argument");
+  int rc = check_fields(c, f, "rs_mass");
+  if (rc) return rc;
+  int nb = 0;
+  if (rs::launch_grid_partials(f->precision, c->K, f->c, f->psi, c->p.cinf, c->partials, c->max_partials, &nb,
+                               (cudaStream_t)stream))
+    return fail(RS_E_INVALID, "rs_mass: workspace too small");
+  rs::launch_reduce_partials(c->partials, nb, 0.0, d_mass, nullptr, (cudaStream_t)stream);
+  return cuda_check("rs_mass");
+}
+
+int rs_precise_tip(rs_ctx *c, const rs_fields *f, rs_tip *d_tip, rs_stream_t stream) {
+  if (!c || !d_tip) return fail(RS_E_INVALID, "rs_precise_tip: null argument");
+  int rc = check_fields(c, f, "rs_precise_tip", false);
+  if (rc) return rc;
+  rs::launch_precise_tip(f->precision, c->K, f->psi, c->row_last, c->row_f, c->row_g, d_tip, (cudaStream_t)stream);
+  return cuda_check("rs_precise_tip");
+}
+
+int rs_initial(rs_ctx *c, const rs_fields *f, rs_stream_t stream) {
+  if (!c) return fail(RS_E_INVALID, "rs_initial: null ctx");
+  int rc = check_fields(c, f, "rs_initial");
+  if (rc) return rc;
+  rs::launch_initial_reference(f->precision, c->K, c->p.i_tip_target, f->c, f->psi, f->phi, (cudaStream_t)stream);
+  return cuda_check("rs_initial");
+}
+
+int rs_initial_planar(rs_ctx *c, const rs_fields *f, double c_liquid, double c_solid, uint64_t seed,
+                      rs_stream_t stream) {
+  if (!c) return fail(RS_E_INVALID, "rs_initial_planar: null ctx");
+  int rc = check_fields(c, f, "rs_initial_planar");
+  if (rc) return rc;
+  if (!(c_liquid > 0 && c_liquid < 1 && c_solid > 0 && c_solid < 1))
+    return fail(RS_E_INVALID, "rs_initial_planar: compositions must lie in (0,1)");
+  rs::launch_initial_planar(f->precision, c->K, c->p.i_tip_target, c_liquid, c_solid, seed, f->c, f->psi, f->phi,
+                            (cudaStream_t)stream);
+  return cuda_check("rs_initial_planar");
+}
+
+int rs_temperature_init(rs_ctx *c, double *d_T, rs_stream_t stream) {
+  if (!c || !d_T) return fail(RS_E_INVALID, "rs_temperature_init: null argument");
+  rs::launch_temperature_init(c->T, d_T, (cudaStream_t)stream);
+  return cuda_check("rs_temperature_init");
+}
+
+static double vp_ramp(const rs_params &p, double t) {
+  if (p.vp_ramp) return p.Vp + 0.0107587 * (t * 0.001);  // Vp_ramp, fun.cu:1974-1982
+  return p.Vp;
+}
+
+int rs_temperature_step(rs_ctx *c, double *d_T, double *d_T_next, const double *d_dphidt, int64_t step,
+                        rs_stream_t stream) {
+  if (!c || !d_T || !d_T_next || !d_dphidt) return fail(RS_E_INVALID, "rs_temperature_step: null argument");
+  if (d_T == d_T_next) return fail(RS_E_INVALID, "rs_temperature_step: T and T_next alias");
+  cudaStream_t st = (cudaStream_t)stream;
+  const double adv = vp_ramp(c->p, step * c->d.tau0 * c->d.dt) * c->d.tau0 / (c->p.S * c->p.W0);
+  double *a = d_T, *b = d_T_next;
+  for (int s = 0; s < c->d.ratio_dt_dtT; ++s) {
+    rs::launch_temperature_substep(c->T, a, b, d_dphidt, adv, st);
+    double *t = a;
+    a = b;
+    b = t;
+  }
+  if (a != d_T) {
+    const size_t bytes = sizeof(double) * (size_t)c->d.NxT_all * c->d.NyT_all;
+    if (cudaMemcpyAsync(d_T, a, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return cuda_check("rs_temperature_step copy");
+  }
+  return cuda_check("rs_temperature_step");
+}
+
+int rs_interpolate_temperature(rs_ctx *c, const double *d_T, double *d_T_fine, int32_t i_left_end,
+                               rs_stream_t stream) {
+  if (!c || !d_T || !d_T_fine) return fail(RS_E_INVALID, "rs_interpolate_temperature: null argument");
+  rs::launch_interpolate_temperature(c->T, c->K, d_T, d_T_fine, i_left_end, (cudaStream_t)stream);
+  return cuda_check("rs_interpolate_temperature");
+}
+
+int rs_integrate_phi(rs_ctx *c, const rs_fields *cur, const rs_fields *next, double *d_dphidt, int32_t i_left_end,
+                     rs_stream_t stream) {
+  if (!c || !d_dphidt) return fail(RS_E_INVALID, "rs_integrate_phi: null argument");
+  int rc = check_fields(c, cur, "rs_integrate_phi cur", false);
+  if (!rc) rc = check_fields(c, next, "rs_integrate_phi next", false);
+  if (rc) return rc;
+  rs::launch_integrate_phi(cur->precision, c->T, cur->psi, next->psi, d_dphidt, i_left_end, 1.0,
+                           (cudaStream_t)stream);
+  return cuda_check("rs_integrate_phi");
+}
+
+// Host build of the Ti-Nb evaluator (fun.cu:1671-1720) from the same
+// pure-element functions the kernels use.
+int rs_calphad_eval(int32_t which, const double *T, const double *cc, double *out, size_t n) {
+  if (!T || !cc || !out) return fail(RS_E_INVALID, "rs_calphad_eval: null argument");
+  const double RR = 8.3145;
+  for (size_t k = 0; k < n; ++k) {
+    const double t = T[k], c = cc[k], lT = std::log(t), onemc = 1.0 - c;
+    double v;
+    if (which == 0 || which == 1) {
+      double log_part;
+      if (c < 1.e-8)
+        log_part = RR * t * (onemc * std::log(onemc));
+      else if (onemc < 1.e-8)
+        log_part = RR * t * (c * std::log(c));
+      else
+        log_part = RR * t * (onemc * std::log(onemc) + c * std::log(c));
+      if (which == 0)
+        v = log_part + onemc * rs::g_nb_liq(t, lT) + c * rs::g_ti_liq(t, lT) + c * onemc * rs::kL0Liq;
+      else
+        v = log_part + onemc * rs::g_nb_bcc(t, lT) + c * rs::g_ti_bcc(t, lT) + c * onemc * rs::kL0Bcc;
+    } else if (which == 2 || which == 3) {
+      double log_part = 0.;
+      if (c > 1.e-8 && onemc > 1.e-8) log_part = RR * t * std::log(c / onemc);
+      if (which == 2)
+        v = rs::g_ti_liq(t, lT) - rs::g_nb_liq(t, lT) + rs::kL0Liq * (1.0 - 2.0 * c) + log_part;
+      else
+        v = rs::g_ti_bcc(t, lT) - rs::g_nb_bcc(t, lT) + rs::kL0Bcc * (1.0 - 2.0 * c) + log_part;
+    } else {
+      return fail(RS_E_INVALID, "rs_calphad_eval: which=%d", which);
+    }
+    out[k] = v;
+  }
+  return RS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,176 @@
+// rs_common.cuh — device/host helpers shared by the phase-field kernels.
+//
+// Physics follows the reference (fun.cu); every helper cites the lines it
+// restates.  Kernel-side coefficients are precomputed on the host into
+// StepCoef so that no kernel re-derives constants per cell.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/rs_b200.h"
+
+#define RS_HD __host__ __device__ __forceinline__
+
+namespace rs {
+
+// Redlich-Kister L0 terms (fun.cu:1668-1669, constant in T)
+constexpr double kL0Bcc = 12315.25;
+constexpr double kL0Liq = 5144.29;
+
+// ---------------------------------------------------------------- CALPHAD
+// SGTE-style pure-element Gibbs energies (fun.cu:1628-1666).  logT is passed
+// in so that one log serves all four functions at a temperature.
+RS_HD double g_ti_bcc(double T, double logT) {
+  if (T >= 1155.0 && T < 1941.0)
+    return 6667.385 + 105.366379 * T - 22.3771 * T * logT + 1.21707e-3 * (T * T) -
+           0.84534e-6 * ((T * T) * T) - 2002750.0 / T;
+  else if (T >= 1941.0)
+    return 26483.26 - 182.426471 * T + 19.0900905 * T * logT - 22.00832e-3 * (T * T) +
+           1.228863e-6 * ((T * T) * T) + 1400501.0 / T;
+  return NAN;
+}
+RS_HD double g_ti_liq(double T, double logT) {
+  if (T >= 1300.0 && T < 1941.0)
+    return 369519.198 - 2554.0225 * T + 342.059267 * T * logT - 163.409355e-3 * (T * T) +
+           12.457117e-6 * ((T * T) * T) - 67034516.0 / T;
+  else if (T >= 1941.0 && T < 4000.0)
+    return -19887.066 + 298.7367 * T - 46.29 * T * logT;
+  return NAN;
+}
+RS_HD double g_nb_bcc(double T, double logT) {
+  if (T >= 298.15 && T < 2750.0)
+    return -8519.353 + 142.045475 * T - 26.4711 * T * logT + 0.203475e-3 * (T * T) -
+           0.35012e-6 * ((T * T) * T) + 93399.0 / T;
+  else if (T >= 2750.0) {
+    const double t3 = (T * T) * T;
+    return -37669.3 + 271.720843 * T - 41.77 * T * logT + 1528.238e29 / ((t3 * t3) * t3);
+  }
+  return NAN;
+}
+RS_HD double g_nb_liq(double T, double logT) {
+  if (T >= 298.15 && T < 2750.0) {
+    const double t2 = T * T;
+    return 21262.202 + 131.229057 * T - 26.4711 * T * logT + 0.203475e-3 * t2 -
+           0.35012e-6 * (t2 * T) + 93399.0 / T - 306.098e-25 * (((t2 * t2) * t2) * T);
+  } else if (T >= 2750.0)
+    return -7499.398 + 260.756148 * T - 41.77 * T * logT;
+  return NAN;
+}
+
+// Temperature-only CALPHAD groups.  With these, per cell
+//   mu    = 0.5(1+g) Gsc + 0.5(1-g) Glc          (fun.cu:1443-1452)
+//   Gsc   = dGs + L0_BCC (1-2c) + RT log(c/(1-c)) (fun.cu:1711-1720)
+//   Glc   = dGl + L0_Liq (1-2c) + RT log(c/(1-c)) (fun.cu:1700-1709)
+//   Gl-Gs = (1-c) A_Nb + c A_Ti + c(1-c)(L0_Liq - L0_BCC)
+// (the ideal-mixing terms of Gl and Gs, fun.cu:1671-1698, cancel exactly).
+struct TTerms {
+  double dGs;   // G_Ti_BCC - G_Nb_BCC
+  double dGl;   // G_Ti_Liq - G_Nb_Liq
+  double A_nb;  // G_Nb_Liq - G_Nb_BCC
+  double A_ti;  // G_Ti_Liq - G_Ti_BCC
+  double RT;    // RR T
+};
+
+RS_HD TTerms t_terms(double T, double RR) {
+  const double lT = log(T);
+  const double tb = g_ti_bcc(T, lT), tl = g_ti_liq(T, lT);
+  const double nb = g_nb_bcc(T, lT), nl = g_nb_liq(T, lT);
+  TTerms r;
+  r.dGs = tb - nb;
+  r.dGl = tl - nl;
+  r.A_nb = nl - nb;
+  r.A_ti = tl - tb;
+  r.RT = RR * T;
+  return r;
+}
+
+// interpolation functions (fun.cu:189-196)
+RS_HD double gg(double p) {
+  const double p2 = p * p;
+  return 1.875 * p - 1.25 * (p2 * p) + 0.375 * ((p2 * p2) * p);
+}
+RS_HD double dgg_dp(double p) {
+  const double a = 1.0 - p * p;
+  return 1.875 * (a * a);
+}
+RS_HD double qq(double AA, double p) {
+  const double a = 1.0 - p;
+  return 0.5 * AA * a - 0.25 * (AA - 1) * (a * a);
+}
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter-based RNG,
+// so noise for (seed, step, cell) needs no stored state.
+RS_HD void philox4x32(uint32_t x[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint64_t p0 = (uint64_t)0xD2511F53u * x[0];
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * x[2];
+    const uint32_t y0 = (uint32_t)(p1 >> 32) ^ x[1] ^ k0;
+    const uint32_t y2 = (uint32_t)(p0 >> 32) ^ x[3] ^ k1;
+    x[0] = y0;
+    x[1] = (uint32_t)p1;
+    x[2] = y2;
+    x[3] = (uint32_t)p0;
+  }
+}
+RS_HD double u53(uint32_t a, uint32_t b) {
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6) + 0.5) * (1.0 / 9007199254740992.0);
+}
+// counter layout of the interface noise draw for (step, cell)
+RS_HD void noise_counter(uint32_t x[4], int64_t step, int64_t cell) {
+  x[0] = (uint32_t)cell;
+  x[1] = (uint32_t)((uint64_t)cell >> 32);
+  x[2] = (uint32_t)step;
+  x[3] = (uint32_t)((uint64_t)step >> 32) ^ 0x4E4F4953u;
+}
+
+// ---------------------------------------------------------------- coefficients
+// Everything the step kernel needs, derived once on the host.
+struct StepCoef {
+  int32_t nx, ny, pitch;
+  int32_t jmin, jmax;   // rows copied into ghost rows 0 and ny-1
+  int32_t one_eps;
+  int32_t tfc;
+  int32_t ratio;        // TFC coarse/fine ratio
+  int32_t NxT_all;
+  double dx;
+  double inv_2dx, inv_dx2, inv_4dx2, inv_2dx2;
+  double dt;
+  double eps1, eps2, epk1;
+  double ox1, ox2, oy1, oy2, oz1, oz2;   // orientation rows (fun.cu:1080-1085)
+  double drive;       // 1 / (2 hh v0)        (fun.cu:1195)
+  double inv_h0v0;    // 1 / (h0 v0)          (fun.cu:1454)
+  double cfac;        // dt Dl / (Gamma muk0) / dx^2 (fun.cu:1461)
+  double AA;
+  double RR;
+  double cinf;
+  double Tmelt, deltaT0;
+  double dxT;         // TFC: dx * ratio
+  double noise_amp;   // amplitude * sqrt(dt); 0 = off
+  uint32_t seed_lo, seed_hi;
+  double W0, S;       // tip radius scale dx W0 S (fun.cu:2941)
+  int32_t NyT_all;
+  int32_t reserved;
+  // FP32 path: chemical potential relative to the melt composition
+  double Lref;        // log(cinf / (1 - cinf))
+};
+
+// Per-step frozen-temperature line: T(i) = Tmelt + deltaT0 (d0 + d1 i)
+// (get_delta, fun.cu:1610-1619, regrouped per step on the host).
+struct StepScalars {
+  int64_t step;
+  double d0, d1;
+  int32_t pull_back, i_offset;
+  int32_t i_left_end_T;
+  int32_t reserved;
+  const double *T_coarse;
+};
+
+}  // namespace rs

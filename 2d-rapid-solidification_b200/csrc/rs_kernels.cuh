@@ -1,0 +1,88 @@
+// rs_kernels.cuh — launcher declarations and block-reduction helpers.
+#pragma once
+
+#include "rs_common.cuh"
+
+namespace rs {
+
+// Per-block partial results of a grid pass: sum of interior c (FP64) and the
+// largest column with psi > 0 (the coarse tip, get_itip_all_grain fun.cu:1745).
+struct BlockPartial {
+  double mass;
+  int32_t itip;
+  int32_t pad;
+};
+
+template <int NT>
+__device__ __forceinline__ void block_partial(double mass, int itip, BlockPartial *out) {
+  __shared__ double s_m[NT / 32];
+  __shared__ int s_i[NT / 32];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mass += __shfl_down_sync(0xffffffffu, mass, o);
+  itip = __reduce_max_sync(0xffffffffu, itip);
+  if ((tid & 31) == 0) {
+    s_m[tid >> 5] = mass;
+    s_i[tid >> 5] = itip;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double m = 0.0;
+    int it = 0;
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) {
+      m += s_m[w];
+      it = max(it, s_i[w]);
+    }
+    BlockPartial b;
+    b.mass = m;
+    b.itip = it;
+    b.pad = 0;
+    out[blockIdx.y * gridDim.x + blockIdx.x] = b;
+  }
+}
+
+// ---- launchers (return 0, or -1 when a size limit is exceeded)
+int launch_step_f64(const StepCoef &K, const StepScalars &P, const double *psi, const double *c,
+                    double *psi_n, double *c_n, double *phi_n, BlockPartial *partials,
+                    int max_partials, int *nblocks_out, cudaStream_t st);
+int launch_step_f32(const StepCoef &K, const StepScalars &P, const float *psi, const float *c,
+                    float *psi_n, float *c_n, float *phi_n, BlockPartial *partials, int max_partials,
+                    int *nblocks_out, cudaStream_t st);
+void launch_reduce_partials(const BlockPartial *partials, int n, double mass_offset,
+                            double *mass_out, int32_t *itip_out, cudaStream_t st);
+
+// frame / reductions / tip (rs_frame.cu); precision 0 = double, 1 = float
+void launch_pull_back(int precision, const StepCoef &K, const void *c, const void *psi,
+                      const void *phi, void *c_n, void *psi_n, void *phi_n, int i_offset,
+                      cudaStream_t st);
+int launch_grid_partials(int precision, const StepCoef &K, const void *c, const void *psi,
+                         double c_offset, BlockPartial *partials, int max_partials,
+                         int *nblocks_out, cudaStream_t st);
+void launch_precise_tip(int precision, const StepCoef &K, const void *psi, int *row_last,
+                        double *row_f, double *row_g, rs_tip *out, cudaStream_t st);
+
+// initial conditions and coarse temperature (rs_init.cu)
+void launch_initial_reference(int precision, const StepCoef &K, int i_tip_target, void *c,
+                              void *psi, void *phi, cudaStream_t st);
+void launch_initial_planar(int precision, const StepCoef &K, int i_tip_target, double c_liquid,
+                           double c_solid, uint64_t seed, void *c, void *psi, void *phi,
+                           cudaStream_t st);
+
+struct TfcCoef {
+  int32_t nx, ny, pitch, ratio;
+  int32_t NxT, NyT, NxT_all, NyT_all;
+  int32_t jTmin, jTmax;
+  int32_t ratio_dt_dtT, Sint;
+  double Tcold, Thot, dx, dxT, dtT, Lcp, W0, GG, S, DT, Gmuk;
+};
+void launch_temperature_init(const TfcCoef &T, double *d_T, cudaStream_t st);
+// adv = Vp_ramp(step tau0 dt) tau0 / (S W0), per step (fun.cu:1563)
+void launch_temperature_substep(const TfcCoef &T, const double *Tin, double *Tout,
+                                const double *dphidt, double adv, cudaStream_t st);
+void launch_interpolate_temperature(const TfcCoef &T, const StepCoef &K, const double *d_T,
+                                    double *d_T_fine, int i_left_end, cudaStream_t st);
+void launch_integrate_phi(int precision, const TfcCoef &T, const void *psi, const void *psi_n,
+                          double *dphidt, int i_left_end, double psi_scale, cudaStream_t st);
+
+}  // namespace rs

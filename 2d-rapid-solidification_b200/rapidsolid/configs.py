@@ -1,0 +1,86 @@
+"""Named workloads (synthetic inputs) of the coupled phase-field step.
+
+Axes follow the reference: i is the growth axis (contiguous), j is periodic.
+The benchmark configurations are written growth-along-y; their y is the
+reference's i and their x the reference's j.  Concentrations are the
+reference's variable c = Ti mole fraction, so "Ti-10at%Nb" is c = 0.90.
+
+Ti-10Nb phase boundaries come from the exact Ti-Nb evaluator (common tangent
+of the liquid and BCC Gibbs energies, fun.cu:1671-1720):
+  T_liquidus(c_l = 0.90) = 1974.99160 K, solid in equilibrium c_s = 0.879550
+  T_solidus (c_s = 0.90) = 1968.14983 K
+tests/test_configs.py re-derives them with the library's evaluator.
+"""
+from ._abi import Params
+
+C_LIQUID_TI10NB = 0.90
+T_LIQUIDUS_TI10NB = 1974.9916030759996
+C_SOLID_AT_TLIQ = 0.8795504308633851
+T_SOLIDUS_TI10NB = 1968.1498345850491
+
+
+def default_params(lib=None):
+    """constants.hpp parameter set (src/constants.hpp:185-350)."""
+    p = Params()
+    if lib is not None:
+        rc = lib.rs_default_params(p)
+        if rc != 0:
+            raise RuntimeError("rs_default_params failed")
+        return p
+    p.nx_all, p.ny_all, p.i_tip_target = 768, 832, 768 - 268
+    p.periodic_j, p.tfc, p.one_eps, p.vp_ramp, p.n_orientation = 1, 1, 1, 0, 1
+    p.cinf, p.W0, p.S, p.Gamma, p.muk0 = 0.632514105, 0.25, 5.0, 199.0, 0.57
+    p.Tmelt, p.T_ref, p.Dl, p.DT = 2161.59, 2118.35, 2.05, 1.1e4
+    p.latent_heat, p.molar_weight, p.num_moles, p.cp = 22003.0, 64.418, 93353.43470588748, 40.0
+    p.RR, p.v0, p.AA, p.ke = 8.3145, 1.17e-5, 12.0, 0.8146631243899296
+    p.dx, p.dt, p.GG, p.Vp = 0.6, 0.0, 10 * 0.001, 1.0
+    p.eps1, p.eps2, p.epk1 = 0.06, 0.0, 0.15
+    p.delta_initial, p.l_offset_Vp_initial, p.i_offset_history_initial = -1.0, 0.0, 0
+    p.ratio_dxT_dx = 10
+    for k in range(9):
+        p.orientation[k] = 1.0 if k in (0, 4, 8) else 0.0
+    p.noise_amplitude, p.seed = 0.0, 0
+    p.Tcold, p.length_sample_um = 2000.0, 50.0
+    p.total_time_ns = 120.0 * 1000.0
+    p.num_fields_output = p.num_tip_output = p.num_check_point_output = 120
+    p.step_pull_back = 0
+    return p
+
+
+def _ti10nb(p, n_i, n_j, G_K_per_m, V_m_per_s):
+    p.nx_all, p.ny_all = n_i, n_j
+    p.tfc, p.vp_ramp = 0, 0
+    p.dx = 0.8
+    p.dt = 0.9 * p.dx * p.dx / 4.0          # 0.9 of the explicit limit dx^2/4
+    p.GG = G_K_per_m * 1e-9                  # K/nm
+    p.Vp = V_m_per_s
+    p.i_tip_target = 16                      # front at y0 = 16 dx
+    p.cinf = C_LIQUID_TI10NB                 # melt entering through the pull-back
+    deltaT0 = p.Tmelt - p.T_ref
+    p.delta_initial = (T_LIQUIDUS_TI10NB - p.Tmelt) / deltaT0
+    return p
+
+
+def plain_small(lib=None):
+    """256x256 (Nx_all x Ny_all) FP64, frozen T, G = 1e6 K/m, V = 0.05 m/s, 500 steps."""
+    return _ti10nb(default_params(lib), 256, 256, 1.0e6, 0.05)
+
+
+def scale_fp32(lib=None):
+    """2048x2048 FP32 bulk, G = 5e6 K/m, V = 0.5 m/s, interface noise 0.01, 20000 steps."""
+    p = _ti10nb(default_params(lib), 2048, 2048, 5.0e6, 0.5)
+    p.noise_amplitude = 0.01
+    p.seed = 20240611
+    return p
+
+
+def small(n_i, n_j, lib=None, **kw):
+    """A small Ti-10Nb grid for parity tests."""
+    p = _ti10nb(default_params(lib), n_i, n_j, kw.pop("G", 1.0e6), kw.pop("V", 0.05))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+IC_SEED = 7
+STEPS = {"plain_small": 500, "scale_fp32": 20000}

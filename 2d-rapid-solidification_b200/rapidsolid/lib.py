@@ -1,0 +1,222 @@
+"""ctypes binding of lib/librsb200.so (the C-ABI of include/rs_b200.h).
+
+Device memory and streams come from PyTorch; every compute call goes through
+the CUDA library.  There is no CPU fallback: a missing or unloadable library
+raises at load time.
+"""
+import ctypes as C
+import os
+
+from . import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "lib", "librsb200.so")
+
+_lib = None
+
+
+class RsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rs error {code}: {msg}")
+        self.code = code
+
+
+def build():
+    """Compile the CUDA library in-tree (nvcc, sm_100a)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", PKG, "-j4"], check=True)
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {PKG}`")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, sz = C.c_void_p, C.c_int32, C.c_int64, C.c_size_t
+    sig = {
+        "rs_abi_version": ([], C.c_int),
+        "rs_last_error": ([], C.c_char_p),
+        "rs_sizeof_params": ([], sz),
+        "rs_sizeof_step_args": ([], sz),
+        "rs_default_params": ([vp], C.c_int),
+        "rs_derive": ([vp, vp], C.c_int),
+        "rs_create": ([vp, C.POINTER(vp)], C.c_int),
+        "rs_destroy": ([vp], C.c_int),
+        "rs_get_derived": ([vp, vp], C.c_int),
+        "rs_step": ([vp, vp, vp, vp, vp], C.c_int),
+        "rs_pull_back": ([vp, vp, vp, i32, vp], C.c_int),
+        "rs_itip": ([vp, vp, vp, vp], C.c_int),
+        "rs_precise_tip": ([vp, vp, vp, vp], C.c_int),
+        "rs_mass": ([vp, vp, vp, vp], C.c_int),
+        "rs_initial": ([vp, vp, vp], C.c_int),
+        "rs_initial_planar": ([vp, vp, C.c_double, C.c_double, C.c_uint64, vp], C.c_int),
+        "rs_temperature_init": ([vp, vp, vp], C.c_int),
+        "rs_temperature_step": ([vp, vp, vp, vp, i64, vp], C.c_int),
+        "rs_integrate_phi": ([vp, vp, vp, vp, i32, vp], C.c_int),
+        "rs_interpolate_temperature": ([vp, vp, vp, i32, vp], C.c_int),
+        "rs_calphad_eval": ([i32, vp, vp, vp, sz], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    if L.rs_abi_version() != _abi.RS_ABI_VERSION:
+        raise RuntimeError("librsb200.so ABI version mismatch: rebuild the library")
+    if L.rs_sizeof_params() != C.sizeof(_abi.Params) or L.rs_sizeof_step_args() != C.sizeof(_abi.StepArgs):
+        raise RuntimeError("rs_params/rs_step_args layout differs from rapidsolid._abi")
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != 0:
+        raise RsError(rc, load().rs_last_error().decode())
+
+
+def default_params():
+    p = _abi.Params()
+    check(load().rs_default_params(C.byref(p)))
+    return p
+
+
+def derive(p):
+    d = _abi.Derived()
+    check(load().rs_derive(C.byref(p), C.byref(d)))
+    return d
+
+
+def calphad_eval(which, T, c):
+    """Host Ti-Nb evaluator: which 0 Gl, 1 Gs, 2 Glc, 3 Gsc (numpy float64 arrays)."""
+    import numpy as np
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    c = np.ascontiguousarray(c, dtype=np.float64)
+    out = np.empty_like(T)
+    check(load().rs_calphad_eval(which, T.ctypes.data, c.ctypes.data, out.ctypes.data, T.size))
+    return out
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+class FieldSet:
+    """Device field set: psi and c (and optionally phi) as (ny_all, nx_all) tensors.
+
+    float64 sets hold c; float32 sets hold c - cinf (see include/rs_b200.h).
+    """
+
+    def __init__(self, p, dtype, device="cuda", with_phi=False):
+        import torch
+        shape = (p.ny_all, p.nx_all)
+        self.dtype = dtype
+        self.psi = torch.zeros(shape, dtype=dtype, device=device)
+        self.c = torch.zeros(shape, dtype=dtype, device=device)
+        self.phi = torch.zeros(shape, dtype=dtype, device=device) if with_phi else None
+        self.precision = _abi.RS_F64 if dtype == torch.float64 else _abi.RS_F32
+
+    def fields(self):
+        return _abi.Fields(c=self.c.data_ptr(), psi=self.psi.data_ptr(),
+                           phi=None if self.phi is None else self.phi.data_ptr(),
+                           precision=self.precision, pitch=0)
+
+
+class Context:
+    """One simulation context (rs_create); owns small device workspaces."""
+
+    def __init__(self, p):
+        self.lib = load()
+        self.p = p
+        self._h = C.c_void_p()
+        check(self.lib.rs_create(C.byref(p), C.byref(self._h)))
+        self.d = _abi.Derived()
+        check(self.lib.rs_get_derived(self._h, C.byref(self.d)))
+
+    def close(self):
+        if self._h:
+            self.lib.rs_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- hot path
+    def step(self, cur, nxt, step, i_offset_history=0, l_offset_Vp=0.0, pull_back=None,
+             T_coarse=None, i_left_end=0, i_left_end_T=0, mass_out=None, itip_out=None, stream=None):
+        a = _abi.StepArgs()
+        a.step = step
+        a.i_offset_history = i_offset_history
+        a.pull_back = 0 if pull_back is None else 1
+        a.i_offset = 0 if pull_back is None else int(pull_back)
+        a.i_left_end = i_left_end
+        a.i_left_end_T = i_left_end_T
+        a.l_offset_Vp = l_offset_Vp
+        a.T_coarse = None if T_coarse is None else T_coarse.data_ptr()
+        a.mass_out = None if mass_out is None else mass_out.data_ptr()
+        a.itip_out = None if itip_out is None else itip_out.data_ptr()
+        fc, fn = cur.fields(), nxt.fields()
+        check(self.lib.rs_step(self._h, C.byref(fc), C.byref(fn), C.byref(a), _stream(stream)))
+
+    def step_args_ptrs(self, cur, nxt):
+        """Prebuilt (cur, next) rs_fields for callers that loop in Python."""
+        return cur.fields(), nxt.fields()
+
+    def pull_back(self, cur, nxt, i_offset, stream=None):
+        fc, fn = cur.fields(), nxt.fields()
+        check(self.lib.rs_pull_back(self._h, C.byref(fc), C.byref(fn), int(i_offset), _stream(stream)))
+
+    def itip(self, fs, out, stream=None):
+        f = fs.fields()
+        check(self.lib.rs_itip(self._h, C.byref(f), _ptr(out), _stream(stream)))
+
+    def mass(self, fs, out, stream=None):
+        f = fs.fields()
+        check(self.lib.rs_mass(self._h, C.byref(f), _ptr(out), _stream(stream)))
+
+    def precise_tip(self, fs, out, stream=None):
+        """out: a uint8 CUDA tensor of sizeof(rs_tip) bytes."""
+        f = fs.fields()
+        check(self.lib.rs_precise_tip(self._h, C.byref(f), _ptr(out), _stream(stream)))
+
+    # ---- initial conditions
+    def initial(self, fs, stream=None):
+        f = fs.fields()
+        check(self.lib.rs_initial(self._h, C.byref(f), _stream(stream)))
+
+    def initial_planar(self, fs, c_liquid, c_solid, seed, stream=None):
+        f = fs.fields()
+        check(self.lib.rs_initial_planar(self._h, C.byref(f), c_liquid, c_solid, seed, _stream(stream)))
+
+    # ---- coarse temperature
+    def temperature_init(self, T, stream=None):
+        check(self.lib.rs_temperature_init(self._h, _ptr(T), _stream(stream)))
+
+    def temperature_step(self, T, T_next, dphidt, step, stream=None):
+        check(self.lib.rs_temperature_step(self._h, _ptr(T), _ptr(T_next), _ptr(dphidt), step, _stream(stream)))
+
+    def integrate_phi(self, cur, nxt, dphidt, i_left_end, stream=None):
+        fc, fn = cur.fields(), nxt.fields()
+        check(self.lib.rs_integrate_phi(self._h, C.byref(fc), C.byref(fn), _ptr(dphidt), int(i_left_end),
+                                        _stream(stream)))
+
+    def interpolate_temperature(self, T, T_fine, i_left_end, stream=None):
+        check(self.lib.rs_interpolate_temperature(self._h, _ptr(T), _ptr(T_fine), int(i_left_end), _stream(stream)))
+
+
+def tip_from_bytes(buf):
+    """rs_tip from a CPU uint8 tensor / bytes."""
+    t = _abi.Tip()
+    C.memmove(C.byref(t), bytes(buf), C.sizeof(_abi.Tip))
+    return t

@@ -1,0 +1,334 @@
+"""Throughput of the coupled phase-field step on B200.
+
+Workload (one step = one time step of the whole grid):
+  Ti-10at%Nb directional solidification, 2048 x 2048 cells (Nx_all x Ny_all,
+  2046^2 interior), FP32 fields (psi, c - cinf) double-buffered, exact CALPHAD
+  chemistry, frozen temperature G = 5e6 K/m, V = 0.5 m/s, moving frame on
+  (pull-back every step_pull_back = 1008 steps), seeded Philox interface
+  noise of amplitude 0.01.  Synthetic input: seeded planar front.
+
+Metric: Gcell-steps/s = interior cells x steps / s (whole job over N GPUs).
+
+Device timing: CUDA events on the launching stream around each step; the
+64 MiB working set fits in L2, so a 256 MiB buffer is written between timed
+steps (outside the events) and every step reads its fields from HBM.
+e2e: the same steps through the C-ABI from pinned host buffers: H2D of the
+initial fields, every step's fused FP64 solute-mass reduction read back to
+the host, D2H of the final fields, all inside one event-timed region.
+
+python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+Under torchrun each rank runs an independent replica (the path has no
+exchange step); time is the max over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "2d-rapid-solidification_b200"))
+
+METRIC = "Gcell-steps/s, %HBM peak; surrogate vs exact CALPHAD at ≤0.5% tip-speed error"
+UNIT = "Gcell-steps/s"
+BYTES_PER_CELL = {"f32": 16, "f64": 32}  # psi, c read once + written once
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel_tag):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel_tag)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def run_ours(args):
+    import torch
+    from rapidsolid import configs, lib
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    p = configs.scale_fp32()
+    ctx = lib.Context(p)
+    d = ctx.d
+    dtype = torch.float32
+    a, b = lib.FieldSet(p, dtype), lib.FieldSet(p, dtype)
+    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    st = torch.cuda.current_stream()
+    cells = (p.nx_all - 2) * (p.ny_all - 2)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    itip = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    state = {"step": 0, "hist": 0, "l": 0.0, "a": a, "b": b}
+    launches = [0]
+
+    def vp_dl(n):
+        return p.Vp * d.dt * d.tau0 / (p.S * p.W0)
+
+    def one_step(mass_out=None):
+        """main.cu loop body: pull-back every step_pull_back steps (coarse tip
+        reduced on the device, 4-byte read), fused step."""
+        n = state["step"]
+        pb = None
+        if n % d.step_pull_back == 0:
+            ctx.itip(state["a"], itip)
+            launches[0] += 2
+            pb = int(itip.item()) - p.i_tip_target
+            state["hist"] += pb
+        ctx.step(state["a"], state["b"], n, i_offset_history=state["hist"], l_offset_Vp=state["l"],
+                 pull_back=pb, mass_out=mass_out)
+        launches[0] += 1 + (1 if mass_out is not None else 0)
+        state["l"] += vp_dl(n)
+        state["a"], state["b"] = state["b"], state["a"]
+        state["step"] = n + 1
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches[0] = 0
+    t_wall = time.time()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(st)
+        one_step()
+        ev[k][1].record(st)
+    torch.cuda.synchronize()
+    t_wall = time.time() - t_wall
+    clk = clocks.stop()
+    gpu_launches = launches[0]
+    ms_steps = [s.elapsed_time(e) for s, e in ev]
+    total_ms = sum(ms_steps)
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * cells * args.steps / (total_ms * 1e-3) / 1e9
+
+    # roofline of the step kernel: median launch duration
+    srt = sorted(ms_steps)
+    kern_ms = srt[len(srt) // 2]
+    alg_bytes = BYTES_PER_CELL["f32"] * cells
+    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+
+    # ---- e2e through the C-ABI with host buffers
+    e2e_steps = args.steps
+    h_psi = torch.empty((p.ny_all, p.nx_all), dtype=dtype, pin_memory=True)
+    h_c = torch.empty_like(h_psi).pin_memory()
+    h_psi.copy_(state["a"].psi)
+    h_c.copy_(state["a"].c)
+    h_mass = torch.zeros(e2e_steps, dtype=torch.float64, pin_memory=True)
+    d_mass = torch.zeros(e2e_steps, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    state["a"].psi.copy_(h_psi, non_blocking=True)
+    state["a"].c.copy_(h_c, non_blocking=True)
+    for k in range(e2e_steps):
+        one_step(mass_out=d_mass[k:k + 1])
+        h_mass[k:k + 1].copy_(d_mass[k:k + 1], non_blocking=True)
+    h_psi.copy_(state["a"].psi, non_blocking=True)
+    h_c.copy_(state["a"].c, non_blocking=True)
+    e1.record(st)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    field_bytes = 2 * h_psi.numel() * h_psi.element_size()
+    e2e = {"value": world * cells * e2e_steps / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": field_bytes / e2e_steps, "d2h_bytes_per_step": 8 + field_bytes / e2e_steps,
+           "ms_per_step": e2e_ms / e2e_steps,
+           "note": "C-ABI rs_step from pinned host fields; per-step FP64 mass read back; no L2 flush"}
+
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (FP64 column CALPHAD groups, FP64 mass sum)",
+        "data": "synthetic (seeded planar Ti-10Nb front, Philox noise)",
+        "config": {"workload": "Ti-10Nb directional solidification 2048x2048 FP32 exact CALPHAD, frozen T "
+                               "G=5e6 K/m V=0.5 m/s, moving frame, interface noise 0.01",
+                   "grid": [p.nx_all, p.ny_all], "interior_cells": cells, "dx_W": p.dx, "dt_tau0": d.dt,
+                   "step_pull_back": d.step_pull_back, "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": alg_bytes, "kernel": "step_f32_kernel",
+                     "kernel_ms_median": round(kern_ms, 5), "traffic": profiled_traffic("step_f32_2048")},
+        "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk, "wall_s_timed": round(t_wall, 3),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(p, seconds=args.cpu_seconds)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def cpu_baseline(p, seconds=12.0, steps=None):
+    """The CPU FP64 restatement (oracle, OpenMP on all host threads) timed on a
+    bounded sample of the same workload: the full grid for a few steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from rapidsolid import configs
+    d = pyoracle.derive(p)
+    s = pyoracle.initial_planar(p, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    t0 = time.time()
+    pyoracle.run(p, d, s, 1)
+    t1 = time.time() - t0
+    n = steps or max(1, min(50, int(seconds / max(t1, 1e-3))))
+    t0 = time.time()
+    pyoracle.run(p, d, s, n)
+    dt = time.time() - t0
+    cells = (p.nx_all - 2) * (p.ny_all - 2)
+    return {"value": round(cells * n / dt / 1e9, 5), "unit": UNIT, "cores": pyoracle.lib().ro_num_threads(),
+            "kind": "port", "sample": f"{n} FP64 steps of the {p.nx_all}x{p.ny_all} grid ({dt:.1f} s)",
+            "cpu": _cpu_model()}
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
+def run_reference(args):
+    """The reference path has no CPU implementation of its own (its step is
+    CUDA); its CPU form is the FP64 restatement in oracle/ (OpenMP, all host
+    threads), timed on a bounded sample: each step is one full-grid step."""
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from rapidsolid import configs
+    p = configs.scale_fp32()
+    d = pyoracle.derive(p)
+    s = pyoracle.initial_planar(p, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    steps = max(1, min(args.steps, 20))
+    warm = max(0, min(args.warmup, 1))
+    if warm:
+        s = pyoracle.run(p, d, s, warm)
+    t0 = time.time()
+    pyoracle.run(p, d, s, steps, step0=warm)
+    dt = time.time() - t0
+    cells = (p.nx_all - 2) * (p.ny_all - 2)
+    value = cells * steps / dt / 1e9
+    cores = pyoracle.lib().ro_num_threads()
+    sample = f"{steps} FP64 steps of the {p.nx_all}x{p.ny_all} grid after {warm} warm-up"
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": round(dt * 1e3 / steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+            "config": {"workload": "Ti-10Nb directional solidification 2048x2048, exact CALPHAD, frozen T",
+                       "grid": [p.nx_all, p.ny_all]},
+            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample, "cpu": _cpu_model()},
+            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

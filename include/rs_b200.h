@@ -1,0 +1,236 @@
+/*
+ * rs_b200.h — C-ABI of the B200 coupled phase-field time step
+ * (Ti–Nb directional solidification, quantitative phase field + CALPHAD).
+ *
+ * The reference program has no library API: its hot path sits behind the kernel
+ * launch sites of the host step loop (src/main.cu:191-233, identical to
+ * fun.cu:466-506) with kernel signatures in src/main.hpp:54-83.  Every entry
+ * point below replaces one of those launch sites (or one host routine that
+ * copies a full field to the host), cited per function.
+ *
+ * Conventions
+ *  - Grid: nx_all x ny_all cells including a one-cell ghost ring; cell (i, j)
+ *    lives at  j * pitch + i  (reference pos(i,j) = j*Nx_all + i, fun.cu:176).
+ *    i is the growth axis (contiguous), j is periodic (or no-flux).
+ *  - The caller owns every field buffer (device memory) and passes a CUDA
+ *    stream (a cudaStream_t cast to void*; NULL = legacy default stream).
+ *    Launchers never allocate: per-context workspaces come from rs_create.
+ *  - Every function returns 0 on success or a negative RS_E* code; the
+ *    message of the last failure on the calling thread is rs_last_error().
+ *  - One orientation (N_or = 1): the order parameter phi equals
+ *    clamp(psi, -1, 1) after every reference step (compute_psi,
+ *    fun.cu:1232-1273), so a field set stores psi and c; phi is optional and,
+ *    when given, is written as the clamped copy for drop-in callers.
+ */
+#ifndef RS_B200_H_
+#define RS_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RS_ABI_VERSION 3
+
+/* status codes */
+#define RS_OK 0
+#define RS_E_INVALID (-1)   /* bad argument (sizes, pointers, alignment) */
+#define RS_E_CUDA (-2)      /* a CUDA runtime call failed */
+#define RS_E_UNSUPPORTED (-3)
+#define RS_E_STATE (-4)     /* e.g. a device-side bounded wait gave up */
+#define RS_E_IO (-5)        /* file missing, truncated or malformed */
+
+/* field precision tags */
+#define RS_F64 0
+#define RS_F32 1
+
+typedef void *rs_stream_t; /* cudaStream_t */
+
+/*
+ * Run parameters.  Defaults (rs_default_params) are the reference's
+ * constants.hpp parameter set (src/constants.hpp:185-350); the macro names of
+ * the reference are given beside each field.
+ */
+typedef struct rs_params {
+  /* grid and switches */
+  int32_t nx_all;          /* Nx_all (run.sh -DNx_all) */
+  int32_t ny_all;          /* Ny_all */
+  int32_t i_tip_target;    /* i_tip_target (Nx-268 in the reference) */
+  int32_t periodic_j;      /* Periodic: 1 periodic j, 0 no-flux */
+  int32_t tfc;             /* ifTFC: 1 coarse-grid temperature, 0 frozen */
+  int32_t one_eps;         /* if_1_eps: 1 -> (eps1), 0 -> (eps1, eps2) */
+  int32_t vp_ramp;         /* if_Vp_ramp */
+  int32_t n_orientation;   /* num_orientation; only 1 is supported */
+  /* material (constants.hpp Material namespace) */
+  double cinf;             /* nominal Ti mole fraction of the melt */
+  double W0;               /* nm */
+  double S;                /* SS = W/W0 */
+  double Gamma;            /* K nm */
+  double muk0;             /* nm/ns/K */
+  double Tmelt;            /* K */
+  double T_ref;            /* K; deltaT0 = Tmelt - T_ref */
+  double Dl;               /* nm^2/ns */
+  double DT;               /* nm^2/ns, thermal diffusivity (TFC) */
+  double latent_heat;      /* J/mol */
+  double molar_weight;     /* g/mol */
+  double num_moles;        /* mol/m^3 */
+  double cp;               /* J/mol/K */
+  double RR;               /* J/mol/K */
+  double v0;               /* m^3/mol */
+  double AA;               /* interface mobility enhancement (12 for SS=5) */
+  double ke;               /* dilute-model partition coefficient (reported only) */
+  /* run */
+  double dx;               /* grid spacing in units of W */
+  double dt;               /* time step in units of tau0; <= 0: set_parameters rule */
+  double GG;               /* K/nm, temperature gradient */
+  double Vp;               /* m/s, pulling velocity */
+  double eps1, eps2, epk1; /* anisotropy strengths */
+  double delta_initial;    /* initial dimensionless undercooling at i_tip_target */
+  double l_offset_Vp_initial;
+  int32_t i_offset_history_initial;
+  int32_t ratio_dxT_dx;    /* coarse/fine spacing ratio (TFC), 10 */
+  double orientation[9];   /* crystal axes projected on the lab frame */
+  /* interface noise (off in the reference; Philox keyed by seed, step, cell) */
+  double noise_amplitude;
+  uint64_t seed;
+  /* TFC */
+  double Tcold;            /* K */
+  double length_sample_um; /* um, coarse-domain length (50 in fun.cu) */
+  /* host-loop cadence (reference set_parameters) */
+  double total_time_ns;
+  int32_t num_fields_output;
+  int32_t num_tip_output;
+  int32_t num_check_point_output;
+  int32_t step_pull_back;  /* <= 0: derived as in set_parameters */
+} rs_params;
+
+/* Quantities derived from rs_params exactly as set_parameters does
+ * (fun.cu:1984-2058) plus the dimensional groups of the macro set. */
+typedef struct rs_derived {
+  double tau0, deltaT0, a1, W, hh, h0, dt, dtT, length_sample, Thot;
+  int64_t total_step;
+  int32_t step_fields, step_tip, step_check_point, step_pull_back;
+  int32_t ratio_dt_dtT, NxT, NyT, NxT_all, NyT_all, i_left_end_initial;
+} rs_derived;
+
+/* A field set on the device.  psi and c are required; phi is optional.
+ * RS_F64 sets hold c itself (the reference's layout).  RS_F32 sets hold
+ * c - cinf: the offset keeps FP32 updates far below ulp(c) (solute
+ * conservation); rs_mass adds cinf back. */
+typedef struct rs_fields {
+  void *c;
+  void *psi;
+  void *phi;          /* may be NULL; written as clamp(psi,-1,1) when set */
+  int32_t precision;  /* RS_F64 or RS_F32 */
+  int32_t pitch;      /* elements per row; 0 means nx_all */
+} rs_fields;
+
+/* Per-step arguments: the scalars the reference passes to its kernels by
+ * value (fun.cu:466-478) plus the fused moving-frame shift. */
+typedef struct rs_step_args {
+  int64_t step;
+  int32_t i_offset_history; /* accumulated shift, enters the frozen T */
+  int32_t pull_back;        /* 1: apply pull_back(i_offset) to cur first */
+  int32_t i_offset;         /* shift of this pull-back */
+  int32_t i_left_end;       /* TFC: left border of the phase-field window */
+  int32_t i_left_end_T;     /* TFC: i_left_end the fine T was interpolated with */
+  int32_t reserved;
+  double l_offset_Vp;       /* pulled distance in W */
+  const void *T_coarse;     /* TFC: coarse T (double, NxT_all x NyT_all) */
+  double *mass_out;         /* device: if set, receives sum of interior c_next */
+  int32_t *itip_out;        /* device: if set, receives max i with psi_next>0 */
+} rs_step_args;
+
+/* Precise tip (fun.cu:2612-2622 TIP). */
+typedef struct rs_tip {
+  int32_t i, j;
+  int32_t status;   /* fit_parabola status: 0 ok, -2 singular, -3 flat */
+  int32_t reserved;
+  double x, y, R;
+} rs_tip;
+
+typedef struct rs_ctx rs_ctx;
+
+/* ---- library ---- */
+int rs_abi_version(void);
+const char *rs_last_error(void);
+size_t rs_sizeof_params(void);
+size_t rs_sizeof_step_args(void);
+
+/* Fill the constants.hpp parameter set (src/constants.hpp:185-350). */
+int rs_default_params(rs_params *p);
+/* Derived quantities, as set_parameters (fun.cu:1984-2058). */
+int rs_derive(const rs_params *p, rs_derived *d);
+
+/* Context: validates parameters, uploads orientation and per-context
+ * workspaces (reduction partials, tip rows).  Replaces the cudaMalloc block of
+ * main() for everything that is not a caller-owned field (fun.cu:374-409). */
+int rs_create(const rs_params *p, rs_ctx **out);
+int rs_destroy(rs_ctx *ctx);
+int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
+
+/* ---- hot path ---- */
+/* One fused time step: pull_back (optional, fun.cu:1469-1492) +
+ * compute_phi (fun.cu:1143-1218) + compute_psi (fun.cu:1232-1273) +
+ * compute_c_CALPHAD (fun.cu:1365-1467), frozen temperature (get_delta,
+ * fun.cu:1610-1619) or on-the-fly interpolated coarse T (TFC,
+ * interpolate_temperature fun.cu:1580-1608), ghost cells included.
+ * cur and next must not alias.  Replaces the launches at main.cu:191-213. */
+int rs_step(rs_ctx *ctx, const rs_fields *cur, const rs_fields *next,
+            const rs_step_args *args, rs_stream_t stream);
+
+/* Column shift of the moving frame, standalone form of the pull_back kernel
+ * (fun.cu:1469-1492, launched at main.cu:179-181). */
+int rs_pull_back(rs_ctx *ctx, const rs_fields *cur, const rs_fields *next,
+                 int32_t i_offset, rs_stream_t stream);
+
+/* Coarse tip column: max i (>= 1) with psi > 0 over every row
+ * (get_itip_all_grain, fun.cu:1745-1754), reduced on the device into
+ * *d_itip instead of copying psi to the host (set_pull_back, fun.cu:697). */
+int rs_itip(rs_ctx *ctx, const rs_fields *f, int32_t *d_itip, rs_stream_t stream);
+
+/* Precise tip on the device (get_precise_tip, fun.cu:2895-2954: row scan
+ * get_tip_int 2880, quartic fits get_precise_x 2694, parabola fit_parabola
+ * 2809).  *d_tip is device memory. */
+int rs_precise_tip(rs_ctx *ctx, const rs_fields *f, rs_tip *d_tip, rs_stream_t stream);
+
+/* Sum of c over the interior cells in double precision into *d_mass. */
+int rs_mass(rs_ctx *ctx, const rs_fields *f, double *d_mass, rs_stream_t stream);
+
+/* ---- initial conditions ---- */
+/* Reference initial condition (kernel initial, fun.cu:983-1021): tanh front
+ * at i_tip_target + 0.5 sin(2 pi j / Ny), c = cinf (0.3184 tanh + 0.6816). */
+int rs_initial(rs_ctx *ctx, const rs_fields *f, rs_stream_t stream);
+/* Planar front at i_tip_target + U(-1/2, 1/2) per row j (Philox keyed by
+ * seed and j), phi = -tanh((i - i0(j)) dx / sqrt 2), c blended from
+ * c_solid (phi = 1) to c_liquid (phi = -1). */
+int rs_initial_planar(rs_ctx *ctx, const rs_fields *f, double c_liquid,
+                      double c_solid, uint64_t seed, rs_stream_t stream);
+
+/* ---- coarse temperature (TFC) ---- */
+/* initial_temperature (fun.cu:1023-1028). T is double, NxT_all x NyT_all. */
+int rs_temperature_init(rs_ctx *ctx, double *d_T, rs_stream_t stream);
+/* ratio_dt_dtT sub-steps of compute_temperature (fun.cu:1537-1578) on the
+ * coarse grid with the latent-heat source dphidt.  T and T_next are swapped
+ * internally; the final T is left in d_T. */
+int rs_temperature_step(rs_ctx *ctx, double *d_T, double *d_T_next,
+                        const double *d_dphidt, int64_t step, rs_stream_t stream);
+/* integrate_phi (fun.cu:1494-1535): latent-heat source per coarse cell,
+ * 0.5 * sum of (psi_next - psi) over its ratio x ratio fine cells. */
+int rs_integrate_phi(rs_ctx *ctx, const rs_fields *cur, const rs_fields *next,
+                     double *d_dphidt, int32_t i_left_end, rs_stream_t stream);
+/* interpolate_temperature (fun.cu:1580-1608): bilinear coarse -> fine. */
+int rs_interpolate_temperature(rs_ctx *ctx, const double *d_T, double *d_T_fine,
+                               int32_t i_left_end, rs_stream_t stream);
+
+/* ---- host-side helpers (no device work) ---- */
+/* CALPHAD Ti-Nb evaluator (fun.cu:1628-1720), host build of the same code
+ * the kernels use.  which: 0 Gl, 1 Gs, 2 Glc, 3 Gsc. */
+int rs_calphad_eval(int32_t which, const double *T, const double *c, double *out, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RS_B200_H_ */

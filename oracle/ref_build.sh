@@ -1,0 +1,55 @@
+#!/usr/bin/env bash
+# Builds the reference's own kernels and host routines into oracle/_ref/
+# (test infrastructure; outputs never leave oracle/_ref/, which is git-ignored).
+#
+# Source: old-fun.cu of the reference (same kernels as fun.cu, src/constants.hpp
+# material set).  The single-file program is compiled as it lies; a patched copy
+# is written under oracle/_ref/src/ with four macro edits the reference's own
+# run scripts make by hand (run.sh:75-90, src.sed):
+#   ifTFC 1 -> 0            frozen temperature (the synthetic workloads' T model)
+#   dx 0.6  -> REF_DX       grid spacing of the workload (0.8 W)
+#   i_tip_target (Nx-268) -> REF_ITIP   (Nx-268 is negative on small grids)
+#   main -> ref_main        so that oracle/ref_harness.cu supplies main()
+# and two edits to host-only code off the step path that does not compile as
+# shipped (old-fun.cu:2002 uses `step`/`h_para` out of scope in save_parameters;
+# old-fun.cu:2205 assigns to a constexpr in AutoBlockSize):
+#   drop the "current pulling velocity" fprintf; constexpr int best_metric -> int
+# Everything else comes in through -D exactly as run.sh passes it.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${REF_ROOT:-/root/reference}"
+OUT="$HERE/_ref"
+if [ ! -f "$REF/old-fun.cu" ]; then
+  echo "ref_build: $REF/old-fun.cu not present; keeping prebuilt $OUT" >&2
+  exit 0
+fi
+mkdir -p "$OUT/src"
+PATCHED="$OUT/src/old-fun.fta.cu"
+sed -e 's/^#define[[:space:]]*ifTFC[[:space:]]*1/#define ifTFC 0/' \
+    -e 's/^\([[:space:]]*\)#define dx 0\.[0-9]*/\1#define dx REF_DX/' \
+    -e 's/^#define[[:space:]]*i_tip_target[[:space:]]*(Nx-268)/#define i_tip_target REF_ITIP/' \
+    -e '/current pulling velocity.*Vp_ramp(step/d' \
+    -e 's/constexpr int best_metric/int best_metric/' \
+    "$REF/old-fun.cu" > "$PATCHED"
+grep -q '^#define ifTFC 0' "$PATCHED"
+grep -q '#define dx REF_DX' "$PATCHED"
+grep -q '^#define i_tip_target REF_ITIP' "$PATCHED"
+
+NVCC="${NVCC:-nvcc}"
+COMMON=(-std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -ccbin g++
+        -Xcompiler -ffp-contract=off -w
+        -DREF_PATCHED="\"$PATCHED\"" -DREF_DX=0.8
+        -Dtotal_time=1000 -Dif_load=0 '-Dpath_input="./"' -Drun_time=1 -Drandom_seed=0
+        -DVp=0.05 -DGG=0.001 -Deps1=0.06 -Deps2=0 -Depk1=0.15 -Dmain=ref_main)
+
+build() { # name nx ny itip extra...
+  local name=$1 nx=$2 ny=$3 itip=$4; shift 4
+  "$NVCC" "${COMMON[@]}" -DNx_all="$nx" -DNy_all="$ny" -DREF_ITIP="$itip" "$@" \
+      "$HERE/ref_harness.cu" -o "$OUT/$name"
+}
+build ref_harness_64 64 64 24
+build ref_harness_64_nofma 64 64 24 -fmad=false
+build ref_harness_256 256 256 16
+build ref_harness_256_nofma 256 256 16 -fmad=false
+build ref_harness_2048 2048 2048 16 -UGG -DGG=0.005 -UVp -DVp=0.5
+echo "ref_build: built $(ls "$OUT" | grep -c ref_harness) harness binaries in $OUT"

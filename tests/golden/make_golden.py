@@ -1,0 +1,158 @@
+"""Generates the golden fixtures of tests/golden/ from the reference's own code.
+
+The reference ships no tests or golden vectors, so its own routines, compiled
+by oracle/ref_build.sh from the reference sources (old-fun.cu, constants.hpp
+parameter set), are run on seeded inputs and their raw FP64 outputs kept:
+
+  python tests/golden/make_golden.py cpu        # host routines, runs anywhere
+      calphad_ref.npz   Gl, Gs, Glc, Gsc on a (T, c) grid (fun.cu:1628-1720)
+      tip_ref.npz       get_itip_all_grain + get_precise_tip on psi fields
+  python tests/golden/make_golden.py gpu OUT    # reference kernels, needs a GPU
+      OUT/step64.npz    64x64: pull_back(3) then 1 and 40 steps, plus the
+                        nofma build (fun.cu kernels with -fmad=false)
+      OUT/c1_500.npz    256x256 Ti-10Nb: pull_back(auto) then 500 steps
+
+The inputs are built with the oracle's initial-condition routines (seeded), so
+the fixtures record inputs by seed, not by value.
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "2d-rapid-solidification_b200"))
+import pyoracle  # noqa: E402
+from rapidsolid import configs  # noqa: E402
+
+
+def calphad_grid():
+    T = np.concatenate([np.linspace(1150.0, 3100.0, 40), [1155.0, 1300.0, 1940.999, 1941.0, 2749.999,
+                                                          2750.0, 3999.0, 4000.0, 1100.0, 298.0]])
+    c = np.array([0.0, 1e-9, 1e-8, 2e-8, 1e-6, 0.01, 0.1, 0.3, 0.5, 0.632514105, 0.7, 0.8795504308633851,
+                  0.9, 0.95, 0.99, 1 - 2e-8, 1 - 1e-8, 1 - 1e-9, 1.0])
+    TT, CC = np.meshgrid(T, c, indexing="ij")
+    return TT.ravel().copy(), CC.ravel().copy()
+
+
+def run_calphad(binary):
+    T, c = calphad_grid()
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        fout = os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            np.array([float(T.size)]).tofile(f)
+            T.tofile(f)
+            c.tofile(f)
+        subprocess.run([binary, "calphad", fin, fout], check=True)
+        out = np.fromfile(fout, dtype=np.float64).reshape(-1, 4)
+    return T, c, out
+
+
+def tip_fields():
+    """psi fields on which the reference's tip routines are evaluated."""
+    fields = {}
+    p64 = configs.small(64, 64, i_tip_target=24)
+    d64 = pyoracle.derive(p64)
+    s = pyoracle.initial_reference(p64)
+    fields["ref_ic_64"] = s.psi.copy()
+    s2 = pyoracle.initial_planar(p64, 0.90, configs.C_SOLID_AT_TLIQ, 11)
+    fields["planar_64"] = s2.psi.copy()
+    # a bump: tanh front with a Gaussian protrusion, not centred on the tip row
+    i = np.arange(64)[None, :]
+    j = np.arange(64)[:, None]
+    i0 = 24 + 6.0 * np.exp(-((j - 37.3) / 5.0) ** 2)
+    fields["bump_64"] = -np.tanh((i - i0) * 0.8 / np.sqrt(2.0))
+    # the bump after 30 oracle steps
+    sb = pyoracle.State(p64)
+    sb.psi[:] = fields["bump_64"]
+    sb.phi[:] = np.clip(sb.psi, -1, 1)
+    sb.c[:] = 0.90 - (0.90 - configs.C_SOLID_AT_TLIQ) * 0.5 * (1 + sb.phi)
+    fields["bump_64_30"] = pyoracle.run(p64, d64, sb, 30).psi.copy()
+    # periodic wrap: protrusion across the j boundary
+    i0w = 24 + 5.0 * np.exp(-((np.minimum(np.abs(j - 1.5), 62 - np.abs(j - 1.5))) / 4.0) ** 2)
+    fields["wrap_64"] = -np.tanh((i - i0w) * 0.8 / np.sqrt(2.0))
+    return fields
+
+
+def run_tip(binary, psi):
+    with tempfile.TemporaryDirectory() as td:
+        f = os.path.join(td, "psi.bin")
+        np.ascontiguousarray(psi, dtype=np.float64).tofile(f)
+        r = subprocess.run([binary, "tip", f], check=True, capture_output=True, text=True)
+    vals = r.stdout.strip().splitlines()[-1].split()
+    return [float(v) for v in vals]
+
+
+def make_cpu():
+    b = pyoracle.ref_binary("ref_harness_64")
+    T, c, out = run_calphad(b)
+    np.savez_compressed(os.path.join(HERE, "calphad_ref.npz"), T=T, c=c, G=out)
+    fields = tip_fields()
+    names = sorted(fields)
+    tips = np.array([run_tip(b, fields[n]) for n in names])
+    np.savez_compressed(os.path.join(HERE, "tip_ref.npz"), names=np.array(names), tips=tips,
+                        **{"psi_" + n: fields[n] for n in names})
+    print("wrote calphad_ref.npz, tip_ref.npz")
+
+
+def write_state(d, s):
+    os.makedirs(d, exist_ok=True)
+    for k in ("c", "phi", "psi"):
+        getattr(s, k).astype(np.float64).tofile(os.path.join(d, k + ".bin"))
+
+
+def read_state(d, shape):
+    return {k: np.fromfile(os.path.join(d, k + ".bin"), dtype=np.float64).reshape(shape)
+            for k in ("c", "phi", "psi")}
+
+
+def run_steps(binary, s, nsteps, dt, delta_initial, pull, offset, td, tag):
+    din = os.path.join(td, tag + "_in")
+    dout = os.path.join(td, tag + "_out")
+    write_state(din, s)
+    os.makedirs(dout, exist_ok=True)
+    subprocess.run([binary, "step", din, dout, str(nsteps), repr(dt), repr(delta_initial), str(pull),
+                    str(offset)], check=True)
+    return read_state(dout, s.c.shape)
+
+
+def make_gpu(out_dir):
+    os.makedirs(out_dir, exist_ok=True)
+    p64 = configs.small(64, 64, i_tip_target=24)
+    d64 = pyoracle.derive(p64)
+    s64 = pyoracle.initial_planar(p64, 0.90, configs.C_SOLID_AT_TLIQ, 3)
+    res = {"in_c": s64.c, "in_psi": s64.psi, "dt": d64.dt, "delta_initial": p64.delta_initial}
+    with tempfile.TemporaryDirectory() as td:
+        for binname, tag in (("ref_harness_64", "fma"), ("ref_harness_64_nofma", "nofma")):
+            b = pyoracle.ref_binary(binname)
+            for n in (1, 40):
+                r = run_steps(b, s64, n, d64.dt, p64.delta_initial, 1, 3, td, f"{tag}{n}")
+                for k in ("c", "psi"):
+                    res[f"{tag}_{n}_{k}"] = r[k]
+    np.savez_compressed(os.path.join(out_dir, "step64.npz"), **res)
+
+    p = configs.plain_small()
+    d = pyoracle.derive(p)
+    s = pyoracle.initial_planar(p, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    res = {"dt": d.dt, "delta_initial": p.delta_initial, "seed": configs.IC_SEED}
+    with tempfile.TemporaryDirectory() as td:
+        for binname, tag in (("ref_harness_256", "fma"), ("ref_harness_256_nofma", "nofma")):
+            r = run_steps(pyoracle.ref_binary(binname), s, 500, d.dt, p.delta_initial, 1, "auto", td, tag)
+            for k in ("c", "psi"):
+                res[f"{tag}_{k}"] = r[k]
+    np.savez_compressed(os.path.join(out_dir, "c1_500.npz"), **res)
+    print("wrote", out_dir)
+
+
+if __name__ == "__main__":
+    if sys.argv[1] == "cpu":
+        make_cpu()
+    elif sys.argv[1] == "gpu":
+        make_gpu(sys.argv[2])
+    else:
+        raise SystemExit("usage: make_golden.py cpu | gpu OUT_DIR")

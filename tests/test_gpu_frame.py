@@ -1,0 +1,171 @@
+"""Moving frame, reductions, tip tracker, initial conditions and the coarse
+temperature on the GPU against the oracle."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import pyoracle
+from helpers import golden, maxabs, perturbed_state
+from rapidsolid import _abi, configs, lib
+from test_gpu_step import download, upload
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("off", [-5, 0, 2, 40])
+def test_pull_back_standalone(dtype, off):
+    dt = torch.float64 if dtype == "f64" else torch.float32
+    p = configs.small(64, 40, i_tip_target=20)
+    s = perturbed_state(p, 11, amp=0.2)
+    if dt == torch.float32:  # compare on FP32-representable inputs
+        s.psi[:] = s.psi.astype(np.float32)
+        s.c[:] = (s.c - p.cinf).astype(np.float32).astype(np.float64) + p.cinf
+    ctx = lib.Context(p)
+    cur, nxt = upload(p, s, dt), lib.FieldSet(p, dt)
+    ctx.pull_back(cur, nxt, off)
+    g = download(p, nxt)
+    o = pyoracle.pull_back(p, s, off)
+    assert maxabs(g.psi, o.psi) == 0.0
+    assert maxabs(g.c, o.c) <= (0.0 if dt == torch.float64 else 1e-15)
+
+
+def test_itip_and_mass():
+    p = configs.small(96, 72, i_tip_target=30)
+    s = perturbed_state(p, 13, amp=0.4)
+    ctx = lib.Context(p)
+    fs = upload(p, s)
+    out_i = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out_m = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ctx.itip(fs, out_i)
+    ctx.mass(fs, out_m)
+    assert out_i.item() == pyoracle.itip(p, s.psi)
+    assert abs(out_m.item() - pyoracle.mass(p, s.c)) <= 1e-13 * pyoracle.mass(p, s.c)
+    # all-liquid field: get_itip_all_grain returns 1
+    fs.psi.fill_(-1.0)
+    ctx.itip(fs, out_i)
+    assert out_i.item() == 1
+
+
+@pytest.mark.parametrize("idx", range(5))
+def test_precise_tip_matches_reference_fixture(idx):
+    z = golden("tip_ref.npz")
+    name = str(z["names"][idx])
+    ref = z["tips"][idx]
+    p = configs.small(64, 64, i_tip_target=24)
+    psi = z["psi_" + name]
+    ctx = lib.Context(p)
+    fs = lib.FieldSet(p, torch.float64)
+    fs.psi.copy_(torch.from_numpy(psi))
+    out = torch.zeros(C.sizeof(_abi.Tip), dtype=torch.uint8, device="cuda")
+    ctx.precise_tip(fs, out)
+    t = lib.tip_from_bytes(out.cpu().numpy().tobytes())
+    assert (t.i, t.j) == (int(ref[1]), int(ref[2]))
+    assert t.status == 0
+    assert abs(t.x - ref[3]) <= 1e-12 * max(1, abs(ref[3]))
+    assert abs(t.y - ref[4]) <= 1e-12 * max(1, abs(ref[4]))
+    assert abs(t.R - ref[5]) <= 1e-9 * max(1, abs(ref[5]))
+
+
+def test_precise_tip_on_evolved_fields_f32():
+    p = configs.small(128, 96, i_tip_target=40, G=5e6, V=0.5)
+    d = pyoracle.derive(p)
+    s = perturbed_state(p, 21, amp=0.6)
+    s = pyoracle.run(p, d, s, 50)
+    psi32 = s.psi.astype(np.float32)
+    ctx = lib.Context(p)
+    fs = lib.FieldSet(p, torch.float32)
+    fs.psi.copy_(torch.from_numpy(psi32))
+    out = torch.zeros(C.sizeof(_abi.Tip), dtype=torch.uint8, device="cuda")
+    ctx.precise_tip(fs, out)
+    t = lib.tip_from_bytes(out.cpu().numpy().tobytes())
+    o = pyoracle.precise_tip(p, d, psi32.astype(np.float64))
+    assert (t.i, t.j, t.status) == (o.i, o.j, o.status)
+    assert abs(t.x - o.x) <= 1e-11 and abs(t.y - o.y) <= 1e-11
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_initial_conditions(dtype):
+    dt = torch.float64 if dtype == "f64" else torch.float32
+    tol = 1e-14 if dt == torch.float64 else 1e-7
+    p = configs.small(64, 48, i_tip_target=20)
+    ctx = lib.Context(p)
+    fs = lib.FieldSet(p, dt)
+    ctx.initial(fs)
+    g = download(p, fs)
+    o = pyoracle.initial_reference(p)
+    assert maxabs(g.psi, o.psi) <= tol and maxabs(g.c, o.c) <= tol
+    ctx.initial_planar(fs, 0.9, 0.88, 99)
+    g = download(p, fs)
+    o = pyoracle.initial_planar(p, 0.9, 0.88, 99)
+    assert maxabs(g.psi, o.psi) <= tol and maxabs(g.c, o.c) <= tol
+
+
+def tfc_params():
+    p = configs.small(64, 42, i_tip_target=20, tfc=1, G=1e7, V=0.5)
+    p.length_sample_um = 1.0
+    # coarse domain starts 30 cells left of the window (i_left_end ~ 30)
+    p.Tcold = p.T_ref - p.GG * p.dx * p.S * p.W0 * (p.i_tip_target + 30)
+    return p
+
+
+def test_temperature_kernels():
+    p = tfc_params()
+    d = pyoracle.derive(p)
+    ctx = lib.Context(p)
+    nT = d.NxT_all * d.NyT_all
+    T = torch.zeros(nT, dtype=torch.float64, device="cuda")
+    ctx.temperature_init(T)
+    To = np.zeros(nT)
+    pyoracle.lib().ro_initial_temperature(C.byref(p), C.byref(d), pyoracle._p(To))
+    assert maxabs(T.cpu().numpy(), To) == 0.0
+    # source from a psi change, then one temperature step
+    s = perturbed_state(p, 3, amp=0.3)
+    s2 = pyoracle.step(p, d, s, 0, T_fine=np.full(s.c.shape, configs.T_LIQUIDUS_TI10NB))
+    cur, nxt = upload(p, s), upload(p, s2)
+    ile = 3
+    dphidt = torch.zeros(nT, dtype=torch.float64, device="cuda")
+    ctx.integrate_phi(cur, nxt, dphidt, ile)
+    Do = np.zeros(nT)
+    pyoracle.lib().ro_integrate_phi(C.byref(p), C.byref(d), pyoracle._p(Do), pyoracle._p(s.psi),
+                                    pyoracle._p(s2.psi), ile)
+    assert maxabs(dphidt.cpu().numpy(), Do) == 0.0
+    Tn = torch.empty_like(T)
+    ctx.temperature_step(T, Tn, dphidt, 7)
+    a, b = To.copy(), To.copy()
+    for _ in range(d.ratio_dt_dtT):
+        pyoracle.lib().ro_compute_temperature(C.byref(p), C.byref(d), pyoracle._p(a), pyoracle._p(b),
+                                              pyoracle._p(Do), 7)
+        a, b = b, a
+    g = T.cpu().numpy().reshape(d.NyT_all, d.NxT_all)
+    o = a.reshape(d.NyT_all, d.NxT_all)
+    assert maxabs(g[:d.NyT, :d.NxT], o[:d.NyT, :d.NxT]) <= 1e-12
+    Tf = torch.zeros((p.ny_all, p.nx_all), dtype=torch.float64, device="cuda")
+    ctx.interpolate_temperature(T, Tf, ile)
+    Tfo = np.zeros((p.ny_all, p.nx_all))
+    pyoracle.lib().ro_interpolate_temperature(C.byref(p), C.byref(d), pyoracle._p(np.ascontiguousarray(o.ravel())),
+                                              pyoracle._p(Tfo), ile)
+    assert maxabs(Tf.cpu().numpy(), Tfo) <= 1e-11
+
+
+def test_tfc_step_f64():
+    """The fused step evaluates the fine T by bilinear interpolation of the
+    coarse T on the fly; same result as interpolate_temperature + step."""
+    p = tfc_params()
+    d = pyoracle.derive(p)
+    ctx = lib.Context(p)
+    nT = d.NxT_all * d.NyT_all
+    T = torch.zeros(nT, dtype=torch.float64, device="cuda")
+    ctx.temperature_init(T)
+    ile = d.i_left_end_initial
+    Tf = np.zeros((p.ny_all, p.nx_all))
+    pyoracle.lib().ro_interpolate_temperature(C.byref(p), C.byref(d), pyoracle._p(T.cpu().numpy()),
+                                              pyoracle._p(Tf), ile)
+    s = perturbed_state(p, 19, amp=0.3)
+    cur, nxt = upload(p, s), lib.FieldSet(p, torch.float64)
+    ctx.step(cur, nxt, 0, T_coarse=T, i_left_end=ile, i_left_end_T=ile)
+    o = pyoracle.step(p, d, s, 0, T_fine=Tf)
+    g = download(p, nxt)
+    assert maxabs(g.psi, o.psi) <= 1e-13 and maxabs(g.c, o.c) <= 1e-13
