@@ -4,10 +4,13 @@
 // (src/constants.hpp:185-350); derived quantities follow set_parameters
 // (fun.cu:1984-2058).  Contexts own only small workspaces (reduction partials,
 // per-row tip data) allocated at creation; no launcher allocates.
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "rs_kernels.cuh"
@@ -32,6 +35,12 @@ int cuda_check(const char *what) {
 
 }  // namespace
 
+struct TmaEntry {
+  const void *ptr;
+  int precision;
+  CUtensorMap map;
+};
+
 struct rs_ctx {
   rs_params p;
   rs_derived d;
@@ -42,7 +51,61 @@ struct rs_ctx {
   int max_partials;
   int *row_last;
   double *row_f, *row_g;
+  int *d_err;          // set by a device-side bounded wait that gave up
+  int use_tma;         // RS_OPT_TMA
+  TmaEntry tma[8];     // tensor-map cache keyed by field pointer
+  int tma_n, tma_next;
 };
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
+
+// 2D tiled descriptor of one field (row pitch = nx_all elements), box of
+// kTmaBoxW32/64 x kTmaBoxH elements, zero fill outside the array.  Returns false
+// when TMA cannot be used (alignment, driver entry point).
+bool field_map(rs_ctx *c, const void *ptr, int precision, CUtensorMap *out) {
+  for (int k = 0; k < c->tma_n; ++k)
+    if (c->tma[k].ptr == ptr && c->tma[k].precision == precision) {
+      *out = c->tma[k].map;
+      return true;
+    }
+  auto enc = encode_fn();
+  const size_t es = precision == RS_F64 ? 8 : 4;
+  const uint64_t row_bytes = (uint64_t)c->p.nx_all * es;
+  if (!enc || ((uintptr_t)ptr % 16) || (row_bytes % 16)) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)c->p.nx_all, (cuuint64_t)c->p.ny_all};
+  cuuint64_t strides[1] = {row_bytes};
+  cuuint32_t box[2] = {(cuuint32_t)(precision == RS_F64 ? rs::kTmaBoxW64 : rs::kTmaBoxW32), (cuuint32_t)rs::kTmaBoxH};
+  cuuint32_t estr[2] = {1, 1};
+  CUtensorMap m;
+  const CUresult r = enc(&m, precision == RS_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                         const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return false;
+  TmaEntry &e = c->tma[c->tma_next];
+  e.ptr = ptr;
+  e.precision = precision;
+  e.map = m;
+  c->tma_next = (c->tma_next + 1) % 8;
+  if (c->tma_n < 8) ++c->tma_n;
+  *out = m;
+  return true;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -252,6 +315,9 @@ int rs_create(const rs_params *p, rs_ctx **out) {
   if (e == cudaSuccess) e = cudaMalloc(&c->row_last, sizeof(int) * p->ny_all);
   if (e == cudaSuccess) e = cudaMalloc(&c->row_f, sizeof(double) * p->ny_all);
   if (e == cudaSuccess) e = cudaMalloc(&c->row_g, sizeof(double) * p->ny_all);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
+  c->use_tma = 1;
   if (e != cudaSuccess) {
     rs_destroy(c);
     return fail(RS_E_CUDA, "rs_create: cudaMalloc: %s", cudaGetErrorString(e));
@@ -266,6 +332,7 @@ int rs_destroy(rs_ctx *c) {
   cudaFree(c->row_last);
   cudaFree(c->row_f);
   cudaFree(c->row_g);
+  cudaFree(c->d_err);
   delete c;
   return RS_OK;
 }
@@ -322,20 +389,55 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
   const bool red = a->mass_out || a->itip_out;
   int nb = 0;
   int lr;
+  rs::TmaMaps tm;
+  const rs::TmaMaps *tmp = nullptr;
+  // the TMA kernel stores column pairs as 8/16-byte vectors
+  const uintptr_t vec = cur->precision == RS_F64 ? 16 : 8;
+  const bool out_aligned =
+      ((uintptr_t)next->psi % vec) == 0 && ((uintptr_t)next->c % vec) == 0 && ((uintptr_t)next->phi % vec) == 0;
+  if (c->use_tma && out_aligned && !c->p.tfc && !a->pull_back && field_map(c, cur->psi, cur->precision, &tm.psi) &&
+      field_map(c, cur->c, cur->precision, &tm.c))
+    tmp = &tm;
   if (cur->precision == RS_F64)
     lr = rs::launch_step_f64(c->K, P, (const double *)cur->psi, (const double *)cur->c, (double *)next->psi,
                              (double *)next->c, (double *)next->phi, red ? c->partials : nullptr,
-                             c->max_partials, &nb, st);
+                             c->max_partials, &nb, tmp, c->d_err, st);
   else
     lr = rs::launch_step_f32(c->K, P, (const float *)cur->psi, (const float *)cur->c, (float *)next->psi,
                              (float *)next->c, (float *)next->phi, red ? c->partials : nullptr,
-                             c->max_partials, &nb, st);
+                             c->max_partials, &nb, tmp, c->d_err, st);
+  if (lr == -3) return fail(RS_E_CUDA, "rs_step: cannot configure shared memory of the TMA kernel");
   if (lr) return fail(RS_E_INVALID, "rs_step: grid too large for the reduction workspace");
   if ((rc = cuda_check("rs_step"))) return rc;
   if (red) {
     const double off = cur->precision == RS_F32 ? (double)(c->p.nx_all - 2) * (c->p.ny_all - 2) * c->p.cinf : 0.0;
     rs::launch_reduce_partials(c->partials, nb, off, a->mass_out, a->itip_out, st);
     if ((rc = cuda_check("rs_step reduce"))) return rc;
+  }
+  return RS_OK;
+}
+
+int rs_set_option(rs_ctx *c, int32_t option, int64_t value) {
+  if (!c) return fail(RS_E_INVALID, "rs_set_option: null ctx");
+  switch (option) {
+    case RS_OPT_TMA:
+      c->use_tma = value ? 1 : 0;
+      return RS_OK;
+    default:
+      return fail(RS_E_INVALID, "rs_set_option: unknown option %d", option);
+  }
+}
+
+int rs_device_status(rs_ctx *c, rs_stream_t stream) {
+  if (!c) return fail(RS_E_INVALID, "rs_device_status: null ctx");
+  int h = 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return cuda_check("rs_device_status");
+  if (h) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), st);
+    return fail(RS_E_STATE, "a device-side wait gave up (pipeline stalled); results of the affected steps are invalid");
   }
   return RS_OK;
 }

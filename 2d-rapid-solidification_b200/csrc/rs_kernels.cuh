@@ -1,6 +1,8 @@
 // rs_kernels.cuh — launcher declarations and block-reduction helpers.
 #pragma once
 
+#include <cuda.h>
+
 #include "rs_common.cuh"
 
 namespace rs {
@@ -42,13 +44,22 @@ __device__ __forceinline__ void block_partial(double mass, int itip, BlockPartia
   }
 }
 
+// TMA descriptors of the current psi and c fields (built on the host)
+struct TmaMaps {
+  CUtensorMap psi;
+  CUtensorMap c;
+};
+constexpr int kTmaBoxW32 = 252;  // input columns per CTA window, FP32 (multiple of 4)
+constexpr int kTmaBoxW64 = 250;  // input columns per CTA window, FP64 (multiple of 2)
+constexpr int kTmaBoxH = 6;      // rows per TMA tile
+
 // ---- launchers (return 0, or -1 when a size limit is exceeded)
 int launch_step_f64(const StepCoef &K, const StepScalars &P, const double *psi, const double *c,
                     double *psi_n, double *c_n, double *phi_n, BlockPartial *partials,
-                    int max_partials, int *nblocks_out, cudaStream_t st);
+                    int max_partials, int *nblocks_out, const TmaMaps *tm, int *err, cudaStream_t st);
 int launch_step_f32(const StepCoef &K, const StepScalars &P, const float *psi, const float *c,
                     float *psi_n, float *c_n, float *phi_n, BlockPartial *partials, int max_partials,
-                    int *nblocks_out, cudaStream_t st);
+                    int *nblocks_out, const TmaMaps *tm, int *err, cudaStream_t st);
 void launch_reduce_partials(const BlockPartial *partials, int n, double mass_offset,
                             double *mass_out, int32_t *itip_out, cudaStream_t st);
 

@@ -5,7 +5,8 @@ rs_sizeof_params()/rs_sizeof_step_args() and the tests compare them.
 """
 import ctypes as C
 
-RS_ABI_VERSION = 3
+RS_ABI_VERSION = 4
+RS_OPT_TMA = 1
 RS_OK = 0
 RS_E_INVALID = -1
 RS_E_CUDA = -2

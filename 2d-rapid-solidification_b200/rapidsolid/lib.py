@@ -58,6 +58,8 @@ def load():
         "rs_integrate_phi": ([vp, vp, vp, vp, i32, vp], C.c_int),
         "rs_interpolate_temperature": ([vp, vp, vp, i32, vp], C.c_int),
         "rs_calphad_eval": ([i32, vp, vp, vp, sz], C.c_int),
+        "rs_set_option": ([vp, i32, i64], C.c_int),
+        "rs_device_status": ([vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -151,6 +153,13 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def set_option(self, option, value):
+        check(self.lib.rs_set_option(self._h, option, value))
+
+    def device_status(self, stream=None):
+        """Raises RsError(RS_E_STATE) if a device-side wait gave up."""
+        check(self.lib.rs_device_status(self._h, _stream(stream)))
 
     # ---- hot path
     def step(self, cur, nxt, step, i_offset_history=0, l_offset_Vp=0.0, pull_back=None,

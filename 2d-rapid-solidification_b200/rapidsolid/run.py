@@ -1,0 +1,57 @@
+"""Run a named workload through the C-ABI for a number of steps.
+
+    python -m rapidsolid.run --config scale_fp32 --precision f32 --steps 8
+    (from 2d-rapid-solidification_b200/, or with it on PYTHONPATH)
+
+Used for profiling: every step is one rs_step launch on the whole grid,
+starting from the seeded planar Ti-10Nb front of the configuration.  The
+moving frame (pull-back every step_pull_back steps) and the per-step frozen
+temperature follow the reference loop (main.cu:156-240).
+"""
+import argparse
+import sys
+
+from . import _abi, configs, lib
+
+
+def main(argv=None):
+    import torch
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--config", default="scale_fp32", choices=["plain_small", "scale_fp32"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--grid", type=int, default=0, help="override Nx_all = Ny_all")
+    ap.add_argument("--no-tma", action="store_true", help="use the register-prefetch kernel")
+    a = ap.parse_args(argv)
+    p = getattr(configs, a.config)()
+    if a.grid:
+        p.nx_all = p.ny_all = a.grid
+    ctx = lib.Context(p)
+    if a.no_tma:
+        ctx.set_option(_abi.RS_OPT_TMA, 0)
+    d = ctx.d
+    dt = torch.float64 if a.precision == "f64" else torch.float32
+    cur, nxt = lib.FieldSet(p, dt), lib.FieldSet(p, dt)
+    ctx.initial_planar(cur, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    itip = torch.zeros(1, dtype=torch.int32, device="cuda")
+    mass = torch.zeros(1, dtype=torch.float64, device="cuda")
+    hist, l = 0, 0.0
+    for n in range(a.steps):
+        pb = None
+        if n % d.step_pull_back == 0:
+            ctx.itip(cur, itip)
+            pb = int(itip.item()) - p.i_tip_target
+            hist += pb
+        ctx.step(cur, nxt, n, i_offset_history=hist, l_offset_Vp=l, pull_back=pb)
+        l += p.Vp * d.dt * d.tau0 / (p.S * p.W0)
+        cur, nxt = nxt, cur
+    ctx.mass(cur, mass)
+    torch.cuda.synchronize()
+    ctx.device_status()
+    print(f"{a.config} {a.precision} grid {p.nx_all}x{p.ny_all}: {a.steps} steps, "
+          f"solute mass {mass.item():.12g}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -159,8 +159,15 @@ def run_ours(args):
     torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # clocks are sampled from before to after the timed region (200 ms period):
+    # untimed steps keep the GPU under load while the sampler starts
     clocks = ClockSampler(local)
     clocks.start()
+    t_pre = time.time()
+    while time.time() - t_pre < args.clock_preroll:
+        for _ in range(20):
+            one_step()
+        torch.cuda.synchronize()
     launches[0] = 0
     t_wall = time.time()
     for k in range(args.steps):
@@ -170,8 +177,13 @@ def run_ours(args):
         ev[k][1].record(st)
     torch.cuda.synchronize()
     t_wall = time.time() - t_wall
-    clk = clocks.stop()
     gpu_launches = launches[0]
+    t_post = time.time()
+    while time.time() - t_post < 0.3:
+        for _ in range(20):
+            one_step()
+        torch.cuda.synchronize()
+    clk = clocks.stop()
     ms_steps = [s.elapsed_time(e) for s, e in ev]
     total_ms = sum(ms_steps)
     if dist:
@@ -233,7 +245,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": alg_bytes, "kernel": "step_f32_kernel",
+                     "algorithmic_bytes_per_launch": alg_bytes, "kernel": "rs::step_tma_kernel<float, 16>",
                      "kernel_ms_median": round(kern_ms, 5), "traffic": profiled_traffic("step_f32_2048")},
         "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk, "wall_s_timed": round(t_wall, 3),
     }
@@ -320,6 +332,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--clock-preroll", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

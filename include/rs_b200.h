@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define RS_ABI_VERSION 3
+#define RS_ABI_VERSION 4
 
 /* status codes */
 #define RS_OK 0
@@ -170,6 +170,16 @@ int rs_derive(const rs_params *p, rs_derived *d);
 int rs_create(const rs_params *p, rs_ctx **out);
 int rs_destroy(rs_ctx *ctx);
 int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
+
+/* Options: RS_OPT_TMA (default 1) stages the step's field tiles into shared
+ * memory with TMA copies; 0 selects the register-prefetch kernel (always used
+ * for pull-back steps, the coarse temperature and unaligned fields). */
+#define RS_OPT_TMA 1
+int rs_set_option(rs_ctx *ctx, int32_t option, int64_t value);
+
+/* Device-side waits are bounded: if one gave up since the last call, returns
+ * RS_E_STATE (and clears the flag).  Synchronizes the stream. */
+int rs_device_status(rs_ctx *ctx, rs_stream_t stream);
 
 /* ---- hot path ---- */
 /* One fused time step: pull_back (optional, fun.cu:1469-1492) +

@@ -48,12 +48,14 @@ def make(name, nx=64, ny=48):
     return p
 
 
+@pytest.mark.parametrize("tma", [1, 0])
 @pytest.mark.parametrize("name", sorted(VARIANTS))
-def test_single_step_f64(name):
+def test_single_step_f64(name, tma):
     p = make(name)
     d = pyoracle.derive(p)
     s = perturbed_state(p, 17, amp=0.25)
     ctx = lib.Context(p)
+    ctx.set_option(_abi.RS_OPT_TMA, tma)
     cur = upload(p, s, with_phi=True)
     nxt = lib.FieldSet(p, torch.float64, with_phi=True)
     ctx.step(cur, nxt, 3, i_offset_history=2, l_offset_Vp=0.37)
@@ -62,6 +64,7 @@ def test_single_step_f64(name):
     g = download(p, nxt)
     for k in ("psi", "phi", "c"):
         assert maxabs(getattr(g, k), getattr(o, k)) <= 1e-13, k
+    ctx.device_status()
 
 
 def test_rotated_orientation_f64():
@@ -108,12 +111,15 @@ def run_gpu(ctx, p, d, s, nsteps, dtype=torch.float64):
     return download(p, a)
 
 
-def test_many_steps_f64():
-    p = make("steep", 96, 80)
+@pytest.mark.parametrize("tma", [1, 0])
+def test_many_steps_f64(tma):
+    p = make("steep", 256, 200)
     d = pyoracle.derive(p)
     s = perturbed_state(p, 31, amp=0.3)
     ctx = lib.Context(p)
+    ctx.set_option(_abi.RS_OPT_TMA, tma)
     g = run_gpu(ctx, p, d, s, 200)
+    ctx.device_status()
     o = s
     l = 0.0
     for n in range(200):
@@ -155,11 +161,13 @@ def test_plain_small_500_steps_parity():
         assert maxabs(g.c[1:-1, 1:-1], z[f"{tag}_c"][1:-1, 1:-1]) <= 1e-10
 
 
-def test_single_step_f32_close_to_oracle():
+@pytest.mark.parametrize("tma", [1, 0])
+def test_single_step_f32_close_to_oracle(tma):
     p = make("steep", 64, 48)
     d = pyoracle.derive(p)
     s = perturbed_state(p, 8, amp=0.25)
     ctx = lib.Context(p)
+    ctx.set_option(_abi.RS_OPT_TMA, tma)
     cur, nxt = upload(p, s, torch.float32), lib.FieldSet(p, torch.float32)
     ctx.step(cur, nxt, 0)
     o = pyoracle.step(p, d, s, 0)
@@ -167,6 +175,22 @@ def test_single_step_f32_close_to_oracle():
     # inputs are rounded to FP32 first; compare increments
     assert maxabs(g.psi - s.psi, o.psi - s.psi) <= 5e-6
     assert maxabs(g.c - s.c, o.c - s.c) <= 5e-8
+
+
+def test_tma_and_register_paths_agree():
+    """Both kernels run the same per-cell arithmetic; they differ only where
+    the compiler contracts a multiply-add differently."""
+    for dtype, tol_psi, tol_c in ((torch.float64, 1e-13, 1e-13), (torch.float32, 1e-5, 1e-7)):
+        p = make("noise", 300, 130)
+        d = pyoracle.derive(p)
+        s = perturbed_state(p, 77, amp=0.3)
+        out = []
+        for tma in (1, 0):
+            ctx = lib.Context(p)
+            ctx.set_option(_abi.RS_OPT_TMA, tma)
+            out.append(run_gpu(ctx, p, d, s, 30, dtype))
+            ctx.device_status()
+        assert maxabs(out[0].psi, out[1].psi) <= tol_psi and maxabs(out[0].c, out[1].c) <= tol_c
 
 
 def test_f32_tracks_f64_over_steps():
