@@ -40,6 +40,21 @@ def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(x, dist, device):
+    """Largest value of x over all ranks (time of the slowest replica)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, cells, steps, max_ms):
+    """Whole-job Gcell-steps/s: every rank advances its own replica."""
+    return world * cells * steps / (max_ms * 1e-3) / 1e9
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -185,13 +200,9 @@ def run_ours(args):
         torch.cuda.synchronize()
     clk = clocks.stop()
     ms_steps = [s.elapsed_time(e) for s, e in ev]
-    total_ms = sum(ms_steps)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(ms_steps), dist, "cuda")
     ms_per_step = total_ms / args.steps
-    value = world * cells * args.steps / (total_ms * 1e-3) / 1e9
+    value = job_throughput(world, cells, args.steps, total_ms)
 
     # roofline of the step kernel: median launch duration
     srt = sorted(ms_steps)
@@ -222,13 +233,9 @@ def run_ours(args):
     h_c.copy_(state["a"].c, non_blocking=True)
     e1.record(st)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     field_bytes = 2 * h_psi.numel() * h_psi.element_size()
-    e2e = {"value": world * cells * e2e_steps / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+    e2e = {"value": job_throughput(world, cells, e2e_steps, e2e_ms), "unit": UNIT,
            "h2d_bytes_per_step": field_bytes / e2e_steps, "d2h_bytes_per_step": 8 + field_bytes / e2e_steps,
            "ms_per_step": e2e_ms / e2e_steps,
            "note": "C-ABI rs_step from pinned host fields; per-step FP64 mass read back; no L2 flush"}

@@ -9,6 +9,8 @@
 #   ifTFC 1 -> 0            frozen temperature (the synthetic workloads' T model)
 #   dx 0.6  -> REF_DX       grid spacing of the workload (0.8 W)
 #   i_tip_target (Nx-268) -> REF_ITIP   (Nx-268 is negative on small grids)
+#   cinf 0.632514105 -> REF_CINF  nominal melt composition of the workload
+#                           (the pull_back fill value, fun.cu:1484)
 #   main -> ref_main        so that oracle/ref_harness.cu supplies main()
 # and two edits to host-only code off the step path that does not compile as
 # shipped (old-fun.cu:2002 uses `step`/`h_para` out of scope in save_parameters;
@@ -28,17 +30,19 @@ PATCHED="$OUT/src/old-fun.fta.cu"
 sed -e 's/^#define[[:space:]]*ifTFC[[:space:]]*1/#define ifTFC 0/' \
     -e 's/^\([[:space:]]*\)#define dx 0\.[0-9]*/\1#define dx REF_DX/' \
     -e 's/^#define[[:space:]]*i_tip_target[[:space:]]*(Nx-268)/#define i_tip_target REF_ITIP/' \
+    -e 's/^#define[[:space:]]*cinf[[:space:]]*(0\.632514105)/#define cinf REF_CINF/' \
     -e '/current pulling velocity.*Vp_ramp(step/d' \
     -e 's/constexpr int best_metric/int best_metric/' \
     "$REF/old-fun.cu" > "$PATCHED"
 grep -q '^#define ifTFC 0' "$PATCHED"
 grep -q '#define dx REF_DX' "$PATCHED"
 grep -q '^#define i_tip_target REF_ITIP' "$PATCHED"
+grep -q '^#define cinf REF_CINF' "$PATCHED"
 
 NVCC="${NVCC:-nvcc}"
 COMMON=(-std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -ccbin g++
         -Xcompiler -ffp-contract=off -w
-        -DREF_PATCHED="\"$PATCHED\"" -DREF_DX=0.8
+        -DREF_PATCHED="\"$PATCHED\"" -DREF_DX=0.8 -DREF_CINF=0.90
         -Dtotal_time=1000 -Dif_load=0 '-Dpath_input="./"' -Drun_time=1 -Drandom_seed=0
         -DVp=0.05 -DGG=0.001 -Deps1=0.06 -Deps2=0 -Depk1=0.15 -Dmain=ref_main)
 
