@@ -35,6 +35,11 @@ int cuda_check(const char *what) {
 
 }  // namespace
 
+namespace rs {
+// lets other translation units of the library report through rs_last_error()
+int set_error(int code, const char *msg) { return fail(code, "%s", msg); }
+}  // namespace rs
+
 struct TmaEntry {
   const void *ptr;
   int precision;

@@ -10,6 +10,10 @@
 //    per-row results and performs the quartic and parabola least-squares fits
 //    (fun.cu:2648-2865) in FP64.  This file is compiled with -fmad=false so that
 //    the fits round like the reference's host code.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
 #include "rs_kernels.cuh"
 
 namespace rs {
@@ -324,3 +328,104 @@ void launch_precise_tip(int precision, const StepCoef &K, const void *psi, int *
 }
 
 }  // namespace rs
+
+// ---------------------------------------------------------------- no-allocation tip
+// rs_precise_tip_noalloc: the precise tip for callers that cannot allocate
+// device memory.  rs_precise_tip takes its per-row scratch (last psi > 0
+// column and the two candidate tip values of every row) from a context that
+// rs_create fills with cudaMalloc.  Some hosts cannot do that: a host that
+// hands all device memory to its own pool allocator and forbids cudaMalloc
+// once it runs, or a time-stepping loop that must not take the implicit
+// device-wide synchronisation of cudaMalloc/cudaFree.  This entry point needs
+// no context: its scratch is the file-scope array below, which every GPU that
+// loads the library holds (RS_NOALLOC_TIP_MAX_ROWS rows, 20 bytes per row,
+// 320 KiB) until the process exits.
+//
+// Host code cannot use the array's name as a device address (it names a host
+// stand-in); the device address is looked up once per device with
+// cudaGetSymbolAddress, with that device current, on the first call made on
+// that device.  Make that first call before any stream capture.
+//
+// Every call shares the same scratch and it keeps the last call's contents.
+// Nothing in it needs to start at zero: each call writes every row entry it
+// later reads.  Calls whose kernels overlap on the GPU (different streams,
+// different host threads) race on the scratch and must be ordered by the
+// caller.
+namespace rs {
+namespace {
+
+struct alignas(256) TipScratch {
+  int last[RS_NOALLOC_TIP_MAX_ROWS];
+  double f[RS_NOALLOC_TIP_MAX_ROWS];
+  double g[RS_NOALLOC_TIP_MAX_ROWS];
+};
+static __device__ __align__(256) TipScratch g_tip_scratch;
+
+constexpr int kMaxDevices = 64;
+struct DeviceScratch {
+  TipScratch *ptr;
+  bool ready;
+};
+DeviceScratch g_dev_scratch[kMaxDevices];
+std::mutex g_dev_scratch_mu;
+
+int tip_scratch_for_current_device(TipScratch **out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return rs::set_error(RS_E_CUDA, "rs_precise_tip_noalloc: no CUDA device");
+  if (dev < 0 || dev >= kMaxDevices) return rs::set_error(RS_E_UNSUPPORTED, "rs_precise_tip_noalloc: device index too large");
+  std::lock_guard<std::mutex> lock(g_dev_scratch_mu);
+  DeviceScratch &d = g_dev_scratch[dev];
+  if (!d.ready) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_tip_scratch);
+    if (e != cudaSuccess) {
+      char msg[256];
+      snprintf(msg, sizeof(msg), "rs_precise_tip_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      return rs::set_error(RS_E_CUDA, msg);
+    }
+    d.ptr = static_cast<TipScratch *>(p);
+    d.ready = true;
+  }
+  *out = d.ptr;
+  return RS_OK;
+}
+
+}  // namespace
+}  // namespace rs
+
+extern "C" int rs_precise_tip_noalloc(const rs_params *p, const rs_fields *f, rs_tip *d_tip, rs_stream_t stream) {
+  if (!p || !f || !d_tip || !f->psi) return rs::set_error(RS_E_INVALID, "rs_precise_tip_noalloc: null argument");
+  if (f->precision != RS_F64 && f->precision != RS_F32)
+    return rs::set_error(RS_E_INVALID, "rs_precise_tip_noalloc: precision tag");
+  if (p->nx_all < 8 || p->ny_all < 8) return rs::set_error(RS_E_INVALID, "rs_precise_tip_noalloc: grid below 8x8");
+  if (p->ny_all > RS_NOALLOC_TIP_MAX_ROWS)
+    return rs::set_error(RS_E_INVALID, "rs_precise_tip_noalloc: ny_all exceeds RS_NOALLOC_TIP_MAX_ROWS");
+  const int pitch = f->pitch ? f->pitch : p->nx_all;
+  if (pitch != p->nx_all) return rs::set_error(RS_E_UNSUPPORTED, "rs_precise_tip_noalloc: pitch must equal nx_all");
+  if ((uintptr_t)f->psi % (f->precision == RS_F64 ? 8 : 4))
+    return rs::set_error(RS_E_INVALID, "rs_precise_tip_noalloc: misaligned psi");
+  rs::TipScratch *sc = nullptr;
+  int rc = rs::tip_scratch_for_current_device(&sc);
+  if (rc) return rc;
+  // the tip kernels read only these geometry fields of the step coefficients
+  rs::StepCoef K;
+  memset(&K, 0, sizeof(K));
+  K.nx = p->nx_all;
+  K.ny = p->ny_all;
+  K.pitch = pitch;
+  K.jmin = p->periodic_j ? p->ny_all - 2 : 1;
+  K.jmax = p->periodic_j ? 1 : p->ny_all - 2;
+  K.dx = p->dx;
+  K.W0 = p->W0;
+  K.S = p->S;
+  rs::launch_precise_tip(f->precision, K, f->psi, sc->last, sc->f, sc->g, d_tip, (cudaStream_t)stream);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    char msg[256];
+    snprintf(msg, sizeof(msg), "rs_precise_tip_noalloc: %s", cudaGetErrorString(e));
+    return rs::set_error(RS_E_CUDA, msg);
+  }
+  return RS_OK;
+}
+
+

@@ -96,4 +96,7 @@ void launch_interpolate_temperature(const TfcCoef &T, const StepCoef &K, const d
 void launch_integrate_phi(int precision, const TfcCoef &T, const void *psi, const void *psi_n,
                           double *dphidt, int i_left_end, double psi_scale, cudaStream_t st);
 
+// records a message for rs_last_error() and returns code (rs_capi.cu)
+int set_error(int code, const char *msg);
+
 }  // namespace rs

@@ -60,6 +60,7 @@ def load():
         "rs_calphad_eval": ([i32, vp, vp, vp, sz], C.c_int),
         "rs_set_option": ([vp, i32, i64], C.c_int),
         "rs_device_status": ([vp, vp], C.c_int),
+        "rs_precise_tip_noalloc": ([vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

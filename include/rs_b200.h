@@ -206,6 +206,19 @@ int rs_itip(rs_ctx *ctx, const rs_fields *f, int32_t *d_itip, rs_stream_t stream
  * 2809).  *d_tip is device memory. */
 int rs_precise_tip(rs_ctx *ctx, const rs_fields *f, rs_tip *d_tip, rs_stream_t stream);
 
+/* Precise tip without any device allocation (no counterpart in the
+ * reference): same result as rs_precise_tip, for callers that cannot
+ * allocate device memory (their device memory belongs to a pool allocator
+ * that forbids cudaMalloc once the run starts, or their loop must not take
+ * the device-wide synchronisation of cudaMalloc/cudaFree).  Needs no rs_ctx;
+ * per-row scratch is a static device array of RS_NOALLOC_TIP_MAX_ROWS rows
+ * (320 KiB, held by every GPU that loads the library); larger ny_all is
+ * rejected with RS_E_INVALID.  The first call on a device looks up the
+ * array's device address and should come before any stream capture.  All
+ * calls share the scratch: calls whose kernels overlap on the GPU race. */
+#define RS_NOALLOC_TIP_MAX_ROWS 16384
+int rs_precise_tip_noalloc(const rs_params *p, const rs_fields *f, rs_tip *d_tip, rs_stream_t stream);
+
 /* Sum of c over the interior cells in double precision into *d_mass. */
 int rs_mass(rs_ctx *ctx, const rs_fields *f, double *d_mass, rs_stream_t stream);
 
