@@ -47,7 +47,7 @@ def default_params(lib=None):
     return p
 
 
-def _ti10nb(p, n_i, n_j, G_K_per_m, V_m_per_s):
+def _ti10nb(p, n_i, n_j, G_K_per_m, V_m_per_s, T0=T_LIQUIDUS_TI10NB):
     p.nx_all, p.ny_all = n_i, n_j
     p.tfc, p.vp_ramp = 0, 0
     p.dx = 0.8
@@ -57,7 +57,7 @@ def _ti10nb(p, n_i, n_j, G_K_per_m, V_m_per_s):
     p.i_tip_target = 16                      # front at y0 = 16 dx
     p.cinf = C_LIQUID_TI10NB                 # melt entering through the pull-back
     deltaT0 = p.Tmelt - p.T_ref
-    p.delta_initial = (T_LIQUIDUS_TI10NB - p.Tmelt) / deltaT0
+    p.delta_initial = (T0 - p.Tmelt) / deltaT0  # T(i_tip_target) = T0 at t = 0
     return p
 
 
@@ -67,8 +67,14 @@ def plain_small(lib=None):
 
 
 def scale_fp32(lib=None):
-    """2048x2048 FP32 bulk, G = 5e6 K/m, V = 0.5 m/s, interface noise 0.01, 20000 steps."""
-    p = _ti10nb(default_params(lib), 2048, 2048, 5.0e6, 0.5)
+    """2048x2048 FP32 bulk, G = 5e6 K/m, V = 0.5 m/s, interface noise 0.01, 20000 steps.
+
+    The front starts at the solidus isotherm: the c = 0.90 melt ahead of it is
+    undercooled by T_liquidus - T_solidus = 6.84 K, so the front grows from
+    the first step (about 1.3 m/s, relaxing to about 0.4 m/s after 10^4
+    steps) and the moving frame shifts about every thousand steps.
+    """
+    p = _ti10nb(default_params(lib), 2048, 2048, 5.0e6, 0.5, T0=T_SOLIDUS_TI10NB)
     p.noise_amplitude = 0.01
     p.seed = 20240611
     return p
