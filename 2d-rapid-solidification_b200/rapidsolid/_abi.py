@@ -5,7 +5,7 @@ rs_sizeof_params()/rs_sizeof_step_args() and the tests compare them.
 """
 import ctypes as C
 
-RS_ABI_VERSION = 4
+RS_ABI_VERSION = 5
 RS_OPT_TMA = 1
 RS_OK = 0
 RS_E_INVALID = -1
@@ -76,3 +76,14 @@ class Tip(C.Structure):
     _fields_ = [("i", C.c_int32), ("j", C.c_int32), ("status", C.c_int32),
                 ("reserved", C.c_int32), ("x", C.c_double), ("y", C.c_double),
                 ("R", C.c_double)]
+
+
+class RunState(C.Structure):
+    """rs_run_state — dynamic state recorded in parameters.txt."""
+    _fields_ = [
+        ("step", C.c_int64), ("i_offset_history", C.c_int32), ("i_left_end_initial", C.c_int32),
+        ("i_left_end", C.c_int32), ("ratio_dt_dtT", C.c_int32), ("NxT", C.c_int32), ("NyT", C.c_int32),
+        ("NxT_all", C.c_int32), ("NyT_all", C.c_int32), ("l_offset_Vp", C.c_double), ("delta", C.c_double),
+        ("dt", C.c_double), ("dtT", C.c_double), ("length_sample", C.c_double), ("Tcold", C.c_double),
+        ("Thot", C.c_double), ("gamma0", C.c_double), ("gamma1", C.c_double), ("path_input", C.c_char_p),
+    ]

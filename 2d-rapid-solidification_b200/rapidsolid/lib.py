@@ -61,6 +61,13 @@ def load():
         "rs_set_option": ([vp, i32, i64], C.c_int),
         "rs_device_status": ([vp, vp], C.c_int),
         "rs_precise_tip_noalloc": ([vp, vp, vp, vp], C.c_int),
+        "rs_write_parameters": ([C.c_char_p, vp, vp], C.c_int),
+        "rs_read_parameters": ([C.c_char_p, i32, vp], C.c_int),
+        "rs_write_check_point": ([C.c_char_p, vp, i32, i32], C.c_int),
+        "rs_read_check_point": ([C.c_char_p, vp, i32, i32], C.c_int),
+        "rs_write_check_point_temperature": ([C.c_char_p, vp, i32, i32, i32], C.c_int),
+        "rs_read_check_point_temperature": ([C.c_char_p, vp, i32, i32, i32], C.c_int),
+        "rs_write_field_text": ([C.c_char_p, vp, i32, i32, i32, i32], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -99,6 +106,30 @@ def calphad_eval(which, T, c):
     out = np.empty_like(T)
     check(load().rs_calphad_eval(which, T.ctypes.data, c.ctypes.data, out.ctypes.data, T.size))
     return out
+
+
+def write_parameters(path, p, state):
+    check(load().rs_write_parameters(str(path).encode(), C.byref(p), C.byref(state)))
+
+
+def read_parameters(path, tfc):
+    s = _abi.RunState()
+    check(load().rs_read_parameters(str(path).encode(), int(tfc), C.byref(s)))
+    return s
+
+
+def write_check_point(path, field):
+    """field: C-contiguous float64 numpy array (Ny_all, Nx_all)."""
+    import numpy as np
+    a = np.ascontiguousarray(field, dtype=np.float64)
+    check(load().rs_write_check_point(str(path).encode(), a.ctypes.data, a.shape[1], a.shape[0]))
+
+
+def read_check_point(path, nx_all, ny_all):
+    import numpy as np
+    a = np.empty((ny_all, nx_all))
+    check(load().rs_read_check_point(str(path).encode(), a.ctypes.data, nx_all, ny_all))
+    return a
 
 
 def _ptr(t):

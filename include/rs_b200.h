@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define RS_ABI_VERSION 4
+#define RS_ABI_VERSION 5
 
 /* status codes */
 #define RS_OK 0
@@ -247,6 +247,37 @@ int rs_integrate_phi(rs_ctx *ctx, const rs_fields *cur, const rs_fields *next,
 /* interpolate_temperature (fun.cu:1580-1608): bilinear coarse -> fine. */
 int rs_interpolate_temperature(rs_ctx *ctx, const double *d_T, double *d_T_fine,
                                int32_t i_left_end, rs_stream_t stream);
+
+/* ---- restart and snapshot files (host only) ---- */
+/* Dynamic state recorded in parameters.txt (fields of the reference's
+ * constants struct, src/main.hpp:10-53). */
+typedef struct rs_run_state {
+  int64_t step;
+  int32_t i_offset_history;
+  int32_t i_left_end_initial;
+  int32_t i_left_end;
+  int32_t ratio_dt_dtT, NxT, NyT, NxT_all, NyT_all;
+  double l_offset_Vp;
+  double delta;            /* printed as "delta_initial" (save_parameters prints para->delta) */
+  double dt;               /* written: <= 0 means the derived dt; read: the file's %g value */
+  double dtT, length_sample, Tcold, Thot;
+  double gamma0, gamma1;   /* orientation angles reported in the file (degrees) */
+  const char *path_input;  /* reported input path; NULL writes "./" */
+} rs_run_state;
+/* save_parameters layout (fun.cu:2060-2202). */
+int rs_write_parameters(const char *path, const rs_params *p, const rs_run_state *s);
+/* load_parameters positional read (fun.cu:2204-2388); tfc: read the TFC block. */
+int rs_read_parameters(const char *path, int32_t tfc, rs_run_state *s);
+/* check_point_<field>.bin: raw FP64, i fastest (fun.cu:1848-1872, 1894-1918). */
+int rs_write_check_point(const char *path, const double *h_field, int32_t nx_all, int32_t ny_all);
+int rs_read_check_point(const char *path, double *h_field, int32_t nx_all, int32_t ny_all);
+/* check_point_temperature.bin: NyT x NxT of the NxT_all-pitched coarse T
+ * (fun.cu:1874-1892, 1946-1971). */
+int rs_write_check_point_temperature(const char *path, const double *h_T, int32_t NxT, int32_t NyT, int32_t NxT_all);
+int rs_read_check_point_temperature(const char *path, double *h_T, int32_t NxT, int32_t NyT, int32_t NxT_all);
+/* <field>_<k>.txt snapshot, "%g\t" per cell (save_field, fun.cu:1768-1790). */
+int rs_write_field_text(const char *path, const double *h_field, int32_t nx_all, int32_t ny_all, int32_t di,
+                        int32_t dj);
 
 /* ---- host-side helpers (no device work) ---- */
 /* CALPHAD Ti-Nb evaluator (fun.cu:1628-1720), host build of the same code

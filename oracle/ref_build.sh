@@ -56,4 +56,11 @@ build ref_harness_64_nofma 64 64 24 -fmad=false
 build ref_harness_256 256 256 16
 build ref_harness_256_nofma 256 256 16 -fmad=false
 build ref_harness_2048 2048 2048 16 -UGG -DGG=0.005 -UVp -DVp=0.5
-echo "ref_build: built $(ls "$OUT" | grep -c ref_harness) harness binaries in $OUT"
+# fun.cu as shipped (its own -D list, run.sh:75-90) for the parameter-file
+# layout: save_parameters / load_parameters only, host code.
+"$NVCC" -std=c++17 -O2 -gencode arch=compute_100a,code=sm_100a -ccbin g++ -w \
+    -DREF_SOURCE="\"$REF/fun.cu\"" -Dmain=ref_main \
+    -Dtotal_time=120000 -Dif_load=0 '-Dpath_input="./"' -Drun_time=4 -Drandom_seed=3 \
+    -DVp=0.6 -DGG=0.002 -Deps1=0.02 -Deps2=0.001 -Depk1=0.1 -DNx_all=768 -DNy_all=832 -DMAX_GPU=1 \
+    "$HERE/ref_params_harness.cu" -o "$OUT/ref_params_harness"
+echo "ref_build: built $(ls "$OUT" | grep -c harness) harness binaries in $OUT"

@@ -7,6 +7,10 @@ parameter set), are run on seeded inputs and their raw FP64 outputs kept:
   python tests/golden/make_golden.py cpu        # host routines, runs anywhere
       calphad_ref.npz   Gl, Gs, Glc, Gsc on a (T, c) grid (fun.cu:1628-1720)
       tip_ref.npz       get_itip_all_grain + get_precise_tip on psi fields
+      parameters_ref.txt  save_parameters of fun.cu (its own -D list) after
+                        set_parameters, step 123, i_offset_history 7,
+                        l_offset_Vp 0.5, delta -1.25 (fun.cu:1984-2202)
+      parameters_ref_loaded.txt  the fields load_parameters sets from it
   python tests/golden/make_golden.py gpu OUT    # reference kernels, needs a GPU
       OUT/step64.npz    64x64: pull_back(3) then 1 and 40 steps, plus the
                         nofma build (fun.cu kernels with -fmad=false)
@@ -97,7 +101,21 @@ def make_cpu():
     tips = np.array([run_tip(b, fields[n]) for n in names])
     np.savez_compressed(os.path.join(HERE, "tip_ref.npz"), names=np.array(names), tips=tips,
                         **{"psi_" + n: fields[n] for n in names})
-    print("wrote calphad_ref.npz, tip_ref.npz")
+    with tempfile.TemporaryDirectory() as td:
+        subprocess.run([pyoracle.ref_binary("ref_params_harness"), "save", "123", "7", "0.5", "-1.25"], check=True,
+                       cwd=td, capture_output=True)
+        with open(os.path.join(td, "parameters.txt"), "rb") as f:
+            data = f.read()
+        loaded = subprocess.run([pyoracle.ref_binary("ref_params_harness"), "load"], check=True, cwd=td,
+                                capture_output=True, text=True).stdout.strip().splitlines()[-1]
+    with open(os.path.join(HERE, "parameters_ref.txt"), "wb") as f:
+        f.write(data)
+    # what load_parameters sets from that file: step, i_offset_history_initial,
+    # l_offset_Vp_initial, delta_initial, dt, i_left_end_initial, i_left_end,
+    # NxT, NyT, NxT_all, NyT_all, length_sample, dtT, ratio_dt_dtT, Tcold, Thot
+    with open(os.path.join(HERE, "parameters_ref_loaded.txt"), "w") as f:
+        f.write(loaded + "\n")
+    print("wrote calphad_ref.npz, tip_ref.npz, parameters_ref.txt")
 
 
 def write_state(d, s):
