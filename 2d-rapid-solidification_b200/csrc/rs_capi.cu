@@ -57,6 +57,8 @@ struct rs_ctx {
   int *row_last;
   double *row_f, *row_g;
   int *d_err;          // set by a device-side bounded wait that gave up
+  float *col_tab;      // per-column CALPHAD table of the FP32 TMA kernel
+  int col_tab_len;
   int use_tma;         // RS_OPT_TMA
   TmaEntry tma[8];     // tensor-map cache keyed by field pointer
   int tma_n, tma_next;
@@ -322,6 +324,8 @@ int rs_create(const rs_params *p, rs_ctx **out) {
   if (e == cudaSuccess) e = cudaMalloc(&c->row_g, sizeof(double) * p->ny_all);
   if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
+  c->col_tab_len = rs::col_tab_len(p->nx_all);
+  if (e == cudaSuccess) e = cudaMalloc(&c->col_tab, sizeof(float) * rs::kColTabFields * c->col_tab_len);
   c->use_tma = 1;
   if (e != cudaSuccess) {
     rs_destroy(c);
@@ -338,6 +342,7 @@ int rs_destroy(rs_ctx *c) {
   cudaFree(c->row_f);
   cudaFree(c->row_g);
   cudaFree(c->d_err);
+  cudaFree(c->col_tab);
   delete c;
   return RS_OK;
 }
@@ -396,13 +401,16 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
   int lr;
   rs::TmaMaps tm;
   const rs::TmaMaps *tmp = nullptr;
-  // the TMA kernel stores column pairs as 8/16-byte vectors
-  const uintptr_t vec = cur->precision == RS_F64 ? 16 : 8;
+  // the TMA kernel stores groups of four FP32 columns as 16-byte vectors
+  const uintptr_t vec = 16;
   const bool out_aligned =
       ((uintptr_t)next->psi % vec) == 0 && ((uintptr_t)next->c % vec) == 0 && ((uintptr_t)next->phi % vec) == 0;
   if (c->use_tma && out_aligned && !c->p.tfc && !a->pull_back && field_map(c, cur->psi, cur->precision, &tm.psi) &&
-      field_map(c, cur->c, cur->precision, &tm.c))
+      field_map(c, cur->c, cur->precision, &tm.c)) {
+    tm.col_tab = c->col_tab;
+    tm.col_tab_len = c->col_tab_len;
     tmp = &tm;
+  }
   if (cur->precision == RS_F64)
     lr = rs::launch_step_f64(c->K, P, (const double *)cur->psi, (const double *)cur->c, (double *)next->psi,
                              (double *)next->c, (double *)next->phi, red ? c->partials : nullptr,

@@ -44,14 +44,25 @@ __device__ __forceinline__ void block_partial(double mass, int itip, BlockPartia
   }
 }
 
-// TMA descriptors of the current psi and c fields (built on the host)
+// Inputs of the TMA-staged FP32 kernel: descriptors of the current psi and c
+// fields (built on the host) and the context's per-column table workspace.
 struct TmaMaps {
   CUtensorMap psi;
   CUtensorMap c;
+  float *col_tab;   // kColTabFields arrays of col_tab_len floats
+  int col_tab_len;
 };
-constexpr int kTmaBoxW32 = 252;  // input columns per CTA window, FP32 (multiple of 4)
+constexpr int kTmaBoxW32 = 128;  // input columns of an FP32 tile (multiple of 4)
 constexpr int kTmaBoxW64 = 250;  // input columns per CTA window, FP64 (multiple of 2)
-constexpr int kTmaBoxH = 6;      // rows per TMA tile
+constexpr int kTileRows = 16;    // output rows of an FP32 tile
+constexpr int kTmaBoxH = kTileRows + 2;  // input rows of an FP32 tile
+constexpr int kColTabFields = 5;
+// length of the per-column table for nx_all columns: tiles start every
+// kTmaBoxW32 - 4 columns and read kTmaBoxW32
+inline int col_tab_len(int nx_all) {
+  const int ni = nx_all - 2, step = kTmaBoxW32 - 4;
+  return ((ni + step - 1) / step) * step + kTmaBoxW32;
+}
 
 // ---- launchers (return 0, or -1 when a size limit is exceeded)
 int launch_step_f64(const StepCoef &K, const StepScalars &P, const double *psi, const double *c,
@@ -60,6 +71,14 @@ int launch_step_f64(const StepCoef &K, const StepScalars &P, const double *psi, 
 int launch_step_f32(const StepCoef &K, const StepScalars &P, const float *psi, const float *c,
                     float *psi_n, float *c_n, float *phi_n, BlockPartial *partials, int max_partials,
                     int *nblocks_out, const TmaMaps *tm, int *err, cudaStream_t st);
+template <typename R>
+struct Coef;
+// FP32 TMA-staged kernel (rs_step_f32.cu): frozen temperature, no pull-back.
+// Launches the per-column table kernel and the tile kernel; nparts_out gets
+// the number of partials written.
+int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScalars &P, const TmaMaps &tm,
+                        float *psi_n, float *c_n, float *phi_n, BlockPartial *partials, int max_partials,
+                        int *nparts_out, int *err, cudaStream_t st);
 void launch_reduce_partials(const BlockPartial *partials, int n, double mass_offset,
                             double *mass_out, int32_t *itip_out, cudaStream_t st);
 

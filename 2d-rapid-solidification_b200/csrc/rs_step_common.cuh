@@ -1,0 +1,278 @@
+// rs_step_common.cuh — per-cell arithmetic shared by the step kernels:
+// working-precision traits, kernel constants, the anisotropic operator, the
+// CALPHAD column groups, the interface phi update and the TMA/mbarrier
+// primitives.  The mathematics is stated in rs_step.cu.
+#pragma once
+
+#include <cuda.h>
+
+#include <type_traits>
+
+#include "rs_kernels.cuh"
+
+namespace rs {
+
+// FP32 chemical-potential remainder log(c/(1-c)) - log(cinf/(1-cinf)) =
+// log((1+s)/(1-s)) = 2 atanh(s), s = delta / (2 cinf (1-c) + delta):
+// odd series to s^9 for |s| < 1/9 (truncation < 1e-10 relative), hardware
+// log beyond.
+__device__ __forceinline__ float lam_fast(float d, float omc, float two_cinf) {
+  const float s = __fdividef(d, fmaf(two_cinf, omc, d));
+  const float s2 = s * s;
+  float p = fmaf(s2, 1.0f / 9.0f, 1.0f / 7.0f);
+  p = fmaf(s2, p, 1.0f / 5.0f);
+  p = fmaf(s2, p, 1.0f / 3.0f);
+  p = fmaf(s2, p, 1.0f);
+  float r = (s + s) * p;
+  if (fabsf(s) >= 1.0f / 9.0f) r = __logf(__fdividef(1.0f + s, 1.0f - s));
+  return r;
+}
+
+template <typename R>
+struct Tr;
+
+template <>
+struct Tr<double> {
+  using S = double;  // storage
+  static constexpr bool kDelta = false;
+  __device__ static double rcp(double x) { return 1.0 / x; }
+  __device__ static double div(double a, double b) { return a / b; }
+  // RT (log(c/(1-c)) - Lref), with the L(c) = 0 guard of fun.cu:1704-1706
+  __device__ static double lam(double c, double omc, double d, double cinf, double Lref) {
+    if (c > 1.e-8 && omc > 1.e-8) return log(c / omc) - Lref;
+    return -Lref;
+  }
+  __device__ static double normal(uint32_t x[4]) {
+    const double u1 = u53(x[0], x[1]), u2 = u53(x[2], x[3]);
+    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+  }
+};
+
+template <>
+struct Tr<float> {
+  using S = float;
+  static constexpr bool kDelta = true;
+  __device__ static float rcp(float x) { return __fdividef(1.0f, x); }
+  __device__ static float div(float a, float b) { return __fdividef(a, b); }
+  __device__ static float lam(float c, float omc, float d, float cinf, float Lref) {
+    if (c > 1.e-8f && omc > 1.e-8f) return lam_fast(d, omc, cinf + cinf);
+    return -Lref;
+  }
+  __device__ static float normal(uint32_t x[4]) {
+    const float u1 = ((x[0] >> 8) + 0.5f) * (1.0f / 16777216.0f);
+    const float u2 = ((x[2] >> 8) + 0.5f) * (1.0f / 16777216.0f);
+    return sqrtf(-2.0f * __logf(u1)) * __cosf(6.2831853f * u2);
+  }
+};
+
+// Kernel constants in the working precision.
+template <typename R>
+struct Coef {
+  R inv_2dx, inv_dx2, inv_4dx2, inv_2dx2, dt;
+  R eps1, eps2, epk1;
+  R k0, k1, k2, k3, k4;                  // |n|^4 harmonics
+  R ox1, ox2, oy1, oy2, oz1, oz2;        // two-eps fallback
+  R as0, ak0;                            // a_s, a_k at |grad phi| = 0
+  R drive, cflux, AA, cinf, Lref, noise_amp, c_floor;
+  int one_eps;
+};
+
+template <typename R>
+Coef<R> make_coef(const StepCoef &K) {
+  Coef<R> F;
+  F.inv_2dx = (R)K.inv_2dx;
+  F.inv_dx2 = (R)K.inv_dx2;
+  F.inv_4dx2 = (R)K.inv_4dx2;
+  F.inv_2dx2 = (R)K.inv_2dx2;
+  F.dt = (R)K.dt;
+  F.eps1 = (R)K.eps1;
+  F.eps2 = (R)K.eps2;
+  F.epk1 = (R)K.epk1;
+  // n_k = a_k cos + b_k sin for the three crystal axes (rows of the
+  // orientation matrix, fun.cu:1080-1085); sum of n_k^4 in harmonics
+  const double ab[3][2] = {{K.ox1, K.ox2}, {K.oy1, K.oy2}, {K.oz1, K.oz2}};
+  double k0 = 0, k1 = 0, k2 = 0, k3 = 0, k4 = 0;
+  for (int k = 0; k < 3; ++k) {
+    const double a = ab[k][0], b = ab[k][1];
+    const double a2 = a * a, b2 = b * b;
+    k0 += (3 * a2 * a2 + 6 * a2 * b2 + 3 * b2 * b2) / 8;
+    k1 += (a2 * a2 - b2 * b2) / 2;
+    k2 += a2 * a * b + a * b2 * b;
+    k3 += (a2 * a2 - 6 * a2 * b2 + b2 * b2) / 8;
+    k4 += (a2 * a * b - a * b2 * b) / 2;
+  }
+  F.k0 = (R)k0;
+  F.k1 = (R)k1;
+  F.k2 = (R)k2;
+  F.k3 = (R)k3;
+  F.k4 = (R)k4;
+  F.ox1 = (R)K.ox1;
+  F.ox2 = (R)K.ox2;
+  F.oy1 = (R)K.oy1;
+  F.oy2 = (R)K.oy2;
+  F.oz1 = (R)K.oz1;
+  F.oz2 = (R)K.oz2;
+  if (K.one_eps) {
+    F.as0 = (R)(1.0 - 3.0 * K.eps1);
+    F.ak0 = (R)(1.0 - 3.0 * K.epk1);
+  } else {
+    F.as0 = (R)(1.0 + K.eps1 * (0.0 - 0.6) + K.eps2 * (0.0 - 17.0 / 7.0));
+    F.ak0 = (R)(1.0 + K.epk1 * (0.0 - 0.6));
+  }
+  F.drive = (R)K.drive;
+  F.cflux = (R)(0.25 * K.cfac * K.inv_h0v0);  // face-mobility 1/4 folded in
+  F.AA = (R)K.AA;
+  F.cinf = (R)K.cinf;
+  F.Lref = (R)K.Lref;
+  F.noise_amp = (R)K.noise_amp;
+  F.c_floor = (R)1.0e-6;
+  F.one_eps = K.one_eps;
+  return F;
+}
+
+// anisotropic operator of get_anisotropy (fun.cu:1030-1139)
+template <typename R>
+__device__ __forceinline__ R anisotropy(const Coef<R> &F, R phi00, R phi10, R phim0,
+                                        R phi01, R phi0m, R phi11, R phim1, R phi1m, R phimm, R &as,
+                                        R &ak) {
+  const R px = (phi10 - phim0) * F.inv_2dx;
+  const R py = (phi01 - phi0m) * F.inv_2dx;
+  const R g2 = px * px + py * py;
+  const R dxx = (phi10 - R(2) * phi00 + phim0) * F.inv_dx2;
+  const R dyy = (phi01 - R(2) * phi00 + phi0m) * F.inv_dx2;
+  const R dxy = (phi11 - phim1 - phi1m + phimm) * F.inv_4dx2;
+  const R lap = (R(2) / R(3)) * (dxx + dyy) +
+                (R(1) / R(3)) * (phi11 + phim1 + phi1m + phimm - R(4) * phi00) * F.inv_2dx2;
+  // |grad phi| > 1e-15 (fun.cu:1056)
+  if (!(g2 > R(1.0e-30))) {
+    as = F.as0;
+    ak = F.ak0;
+    return (as * as) * lap;
+  }
+  const R ig2 = Tr<R>::rcp(g2);
+  const R dtx = (px * dxy - py * dxx) * ig2;
+  const R dty = (px * dyy - py * dxy) * ig2;
+  R da1, da2;
+  if (F.one_eps) {
+    const R C2 = (px * px - py * py) * ig2;
+    const R S2 = R(2) * px * py * ig2;
+    const R C4 = C2 * C2 - S2 * S2;
+    const R S4 = R(2) * S2 * C2;
+    const R np4 = F.k0 + F.k1 * C2 + F.k2 * S2 + F.k3 * C4 + F.k4 * S4;
+    const R d1 = R(2) * (F.k2 * C2 - F.k1 * S2) + R(4) * (F.k4 * C4 - F.k3 * S4);
+    const R d2 = R(-4) * (F.k1 * C2 + F.k2 * S2) - R(16) * (F.k3 * C4 + F.k4 * S4);
+    ak = R(1) - R(3) * F.epk1 + R(4) * F.epk1 * np4;
+    as = R(1) - R(3) * F.eps1 + R(4) * F.eps1 * np4;
+    da1 = R(4) * F.eps1 * d1;
+    da2 = R(4) * F.eps1 * d2;
+  } else {
+    // (eps1, eps2) form needs the sextic (n_x n_y n_z)^2: explicit directions
+    const R ia = sqrt(ig2);
+    const R cs = px * ia, sn = py * ia;
+    const R nx = F.ox1 * cs + F.ox2 * sn, ny = F.oy1 * cs + F.oy2 * sn, nz = F.oz1 * cs + F.oz2 * sn;
+    const R nx1 = F.ox2 * cs - F.ox1 * sn, ny1 = F.oy2 * cs - F.oy1 * sn, nz1 = F.oz2 * cs - F.oz1 * sn;
+    const R nx3 = nx * nx * nx, ny3 = ny * ny * ny, nz3 = nz * nz * nz;
+    const R np4 = nx3 * nx + ny3 * ny + nz3 * nz;
+    const R dnp4_1 = R(4) * (nx3 * nx1 + ny3 * ny1 + nz3 * nz1);
+    const R ax = nx * nx1, ay = ny * ny1, az = nz * nz1;
+    const R dnp4_2 = R(4) * (R(3) * (ax * ax + ay * ay + az * az) - np4);
+    const R xyz = nx * ny * nz;
+    ak = R(1) + F.epk1 * (np4 - R(0.6));
+    as = R(1) + F.eps1 * (np4 - R(0.6)) + F.eps2 * (R(3) * np4 + R(66) * (xyz * xyz) - R(17) / R(7));
+    const R t1 = nx1 * ny * nz + nx * ny1 * nz + nx * ny * nz1;
+    const R dnp2_1 = R(2) * xyz * t1;
+    R dnp2_2 = (nx1 * ny * nz) * (nx1 * ny * nz) + (nx * ny1 * nz) * (nx * ny1 * nz) +
+               (nx * ny * nz1) * (nx * ny * nz1);
+    dnp2_2 += -nx * nx * (ny * nz) * (ny * nz) - ny * ny * (nx * nz) * (nx * nz) - nz * nz * (nx * ny) * (nx * ny);
+    dnp2_2 += R(4) * xyz * (nx1 * ny1 * nz + nx * ny1 * nz1 + nx1 * ny * nz1);
+    dnp2_2 *= R(2);
+    da1 = (F.eps1 + R(3) * F.eps2) * dnp4_1 + R(66) * F.eps2 * dnp2_1;
+    da2 = (F.eps1 + R(3) * F.eps2) * dnp4_2 + R(66) * F.eps2 * dnp2_2;
+  }
+  return (as * as) * lap + R(2) * as * da1 * (dtx * px + dty * py) + (da2 * as + da1 * da1) * (dty * px - dtx * py);
+}
+
+__device__ __forceinline__ double t_fine_at(const StepCoef &K, const double *__restrict__ T, int ile, int i, int j) {
+  // interpolate_temperature (fun.cu:1580-1608); indices clamped where the
+  // reference would read outside the coarse array
+  int iT = (i - 1 + ile) / K.ratio;
+  int jT = (int)((j - 1 + K.dxT) / K.ratio);
+  const double x = (i - 1.0 + ile) / K.ratio - iT;
+  const double y = (j - 1.0 + K.dxT) / K.ratio - jT;
+  iT = min(max(iT, 0), K.NxT_all - 2);
+  jT = min(max(jT, 0), K.NyT_all - 2);
+  const double f00 = T[(int64_t)jT * K.NxT_all + iT];
+  const double f10 = T[(int64_t)jT * K.NxT_all + iT + 1];
+  const double f01 = T[(int64_t)(jT + 1) * K.NxT_all + iT];
+  const double f11 = T[(int64_t)(jT + 1) * K.NxT_all + iT + 1];
+  const double a10 = f10 - f00, a01 = f01 - f00, a11 = f11 - f10 - f01 + f00;
+  return f00 + a10 * x + a01 * y + a11 * x * y;
+}
+
+// column (or, with TFC, cell) CALPHAD groups in the working precision
+template <typename R>
+struct ColT {
+  R A_nb, A_ti, D, RT;
+  double Kc;  // K(T), FP64
+};
+
+template <typename R>
+__device__ __forceinline__ ColT<R> col_terms(const StepCoef &K, double T) {
+  const TTerms t = t_terms(T, K.RR);
+  ColT<R> c;
+  c.A_nb = (R)t.A_nb;
+  c.A_ti = (R)t.A_ti;
+  c.D = (R)(0.5 * (t.dGs - t.dGl));
+  c.RT = (R)t.RT;
+  c.Kc = 0.5 * (t.dGs + t.dGl) + 0.5 * (kL0Bcc + kL0Liq) * (1.0 - 2.0 * K.cinf) + t.RT * K.Lref;
+  return c;
+}
+
+// phi update of one interface cell (compute_phi, fun.cu:1143-1218, with the
+// renormalisation of compute_psi); only warps that see an interface row run it.
+template <typename R>
+__device__ __forceinline__ R phi_cell(const Coef<R> *__restrict__ Fp, R p00, R p10, R pm0, R p01, R p0m, R p11,
+                                   R pm1, R p1m, R pmm, R c00, R Anb, R Ati, int64_t step, int64_t cell,
+                                   uint32_t seed_lo, uint32_t seed_hi) {
+  const Coef<R> &F = *Fp;
+  R as, ak;
+  const R an = anisotropy<R>(F, p00, p10, pm0, p01, p0m, p11, pm1, p1m, pmm, as, ak);
+  const R dG = (R(1) - c00) * Anb + c00 * Ati + c00 * (R(1) - c00) * R(kL0Liq - kL0Bcc);
+  const R q = R(1) - p00 * p00;
+  const R term = p00 - p00 * p00 * p00 + an + dG * (R(1.875) * (q * q)) * F.drive;
+  R pn = p00 + Tr<R>::div(F.dt * ak, as * as) * term;
+  if (F.noise_amp > R(0) && q > R(1.0e-3)) {
+    uint32_t x[4];
+    noise_counter(x, step, cell);
+    philox4x32(x, seed_lo, seed_hi);
+    pn += F.noise_amp * q * Tr<R>::normal(x);
+  }
+  return pn > R(1) ? R(1) : pn;  // renormalisation (fun.cu:1252-1261)
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace rs
