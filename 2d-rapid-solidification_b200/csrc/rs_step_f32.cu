@@ -66,6 +66,7 @@ struct alignas(128) TileSmem {
   float S[kTRin][kIn];
   float mu[kTRin][kIn];
   uint16_t list[kTR * kOut];  // interface cells: row << 8 | column
+  uint8_t pmask[kTRin][32];   // per lane: bits 0-3 psi <= -1, bits 4-7 psi >= 1 of its four cells
   uint32_t liq, sol;          // bit r: every cell of input row r has psi == -1 / +1
   int nlist;
   double part_mass[kWarps];
@@ -133,18 +134,25 @@ __global__ void __launch_bounds__(kThreads, 5)
 
   const int col = 4 * lane;  // tile column of this lane's first cell
   const int gi = x0 + col;   // its global column
-  uint32_t inm = 0, outm = 0;  // per cell: inside the array / an output cell
+  uint32_t outm = 0;  // per cell: an output cell
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    if (gi + q <= K.nx - 1) inm |= 1u << q;
+  for (int q = 0; q < 4; ++q)
     if (col + q >= 1 && col + q <= kOut && gi + q <= K.nx - 2) outm |= 1u << q;
-  }
+  // interior tiles: no ghost column, every lane's cells are outputs except
+  // cell 0 of lane 0 and cells 1..3 of lane 31
+  const bool interior = x0 >= 4 && x0 + kOut <= K.nx - 3;
   const float two_cinf = F.cinf + F.cinf;
   const float cflux4 = 0.25f * F.cflux;
   const float floor_d = F.c_floor - F.cinf;
   constexpr float KL = (float)(-2.0 * kL0Liq);
   constexpr float L0sum = (float)(kL0Bcc + kL0Liq);
   constexpr float L0half = (float)(0.5 * (kL0Bcc - kL0Liq));
+  // delta range of the series form: s = delta / (A + B delta) with
+  // A = 2 cinf (1 - cinf), B = 1 - 2 cinf, so |s| < 1/9 for
+  // -A/(9+B) < delta < A/(9-B) (taken 0.1 % inside)
+  const float sA = 2.f * F.cinf * (1.f - F.cinf), sB = 1.f - 2.f * F.cinf;
+  const float d_hi = 0.999f * sA / (9.f - sB), d_lo = -0.999f * sA / (9.f + sB);
+  constexpr uint32_t kMinus1 = 0xBF800000u, kPlus1 = 0x3F800000u;
 
   // the column table of this step (programmatic dependency on its kernel)
   asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -161,6 +169,19 @@ __global__ void __launch_bounds__(kThreads, 5)
     }
   }
 
+  // columns beyond the array (right-most tiles; zero-filled by TMA) become
+  // bulk melt, so they never force the general path; no output reads them
+  if (x0 + kIn > K.nx) {
+    for (int k = threadIdx.x; k < kTRin * kIn; k += kThreads) {
+      const int rr = k / kIn, x = k % kIn;
+      if (x0 + x >= K.nx) {
+        sm.psi[rr][x] = -1.f;
+        sm.d[rr][x] = 0.f;
+      }
+    }
+    __syncthreads();
+  }
+
   // ---- phase 1: per-cell terms; warp w takes input rows w, w+4, ...
 #pragma unroll 1
   for (int rr = warp; rr < kTRin; rr += kWarps) {
@@ -168,6 +189,7 @@ __global__ void __launch_bounds__(kThreads, 5)
     if (y > K.ny - 1) {  // beyond the array (last tile): never read by an output
       st4(&sm.S[rr][col], 0.f, 0.f, 0.f, 0.f);
       st4(&sm.mu[rr][col], 0.f, 0.f, 0.f, 0.f);
+      sm.pmask[rr][lane] = 0xFFu;
       if (lane == 0) {
         atomicOr(&sm.liq, 1u << rr);
         atomicOr(&sm.sol, 1u << rr);
@@ -176,31 +198,46 @@ __global__ void __launch_bounds__(kThreads, 5)
     }
     const float4 pv4 = ld4(&sm.psi[rr][col]), dv4 = ld4(&sm.d[rr][col]);
     const float pv[4] = {pv4.x, pv4.y, pv4.z, pv4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
-    float cc[4], om[4], sv[4], Sv[4], mv[4];
-    uint32_t code = 7u;
+    float cc[4], om[4], Sv[4], mv[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       cc[q] = F.cinf + dv[q];
       om[q] = 1.f - cc[q];
-      sv[q] = __fdividef(dv[q], fmaf(two_cinf, om[q], dv[q]));
-      const bool liq = pv[q] == -1.f, sol = pv[q] == 1.f;
-      const bool fast = liq && fabsf(sv[q]) < (1.f / 9.f);
-      code &= ((inm >> q) & 1u) ? ((liq ? 1u : 0u) | (sol ? 2u : 0u) | (fast ? 4u : 0u)) : 7u;
     }
-    code = __reduce_and_sync(FULL, code);
-    if (code & 4u) {
-      // bulk liquid: lam = 2 atanh(s) by its odd series (|s| < 1/9)
+    // the row is bulk melt when every psi is exactly -1 and every delta is in
+    // the series range (bit tests on psi, min/max on delta)
+    const uint32_t b0 = __float_as_uint(pv[0]), b1 = __float_as_uint(pv[1]), b2 = __float_as_uint(pv[2]),
+                   b3 = __float_as_uint(pv[3]);
+    const uint32_t band = b0 & b1 & b2 & b3, bor = b0 | b1 | b2 | b3;
+    const float dmx = fmaxf(fmaxf(dv[0], dv[1]), fmaxf(dv[2], dv[3]));
+    const float dmn = fminf(fminf(dv[0], dv[1]), fminf(dv[2], dv[3]));
+    const bool liq4 = band == kMinus1 && bor == kMinus1;
+    uint32_t code;
+    if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
+      code = 5u;
+      sm.pmask[rr][lane] = 0x0Fu;
+      // lam = 2 atanh(s) by its odd series
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const float s2 = sv[q] * sv[q];
+        const float sv = __fdividef(dv[q], fmaf(two_cinf, om[q], dv[q]));
+        const float s2 = sv * sv;
         float p = fmaf(s2, 1.f / 9.f, 1.f / 7.f);
         p = fmaf(s2, p, 1.f / 5.f);
         p = fmaf(s2, p, 1.f / 3.f);
-        p = fmaf(s2, p, 1.f);
+        const float lh = fmaf(sv * s2, p, sv);  // atanh(s)
         Sv[q] = cc[q] * om[q];
-        mv[q] = fmaf(RTa[q], (sv[q] + sv[q]) * p, dv[q] * KL);
+        mv[q] = fmaf(RTa[q] + RTa[q], lh, dv[q] * KL);
       }
     } else {
+      const bool sol4 = band == kPlus1 && bor == kPlus1;
+      code = (__all_sync(FULL, liq4) ? 1u : 0u) | (__all_sync(FULL, sol4) ? 2u : 0u);
+      uint32_t L = 0u, Sm = 0u;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (pv[q] <= -1.f) L |= 1u << q;
+        if (pv[q] >= 1.f) Sm |= 1u << q;
+      }
+      sm.pmask[rr][lane] = (uint8_t)(L | (Sm << 4));
       // general form (fun.cu:1424-1452)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -286,18 +323,17 @@ __global__ void __launch_bounds__(kThreads, 5)
       const uint32_t w3 = 7u << (rr - 1);
       const bool uni_liq = (liq & w3) == w3;
       if (!uni_liq && (sol & w3) != w3) {
+        // phi masks of rows rr-1 .. rr+1, this lane's cells with one cell of
+        // each neighbouring lane
+        const uint32_t pk = (uint32_t)sm.pmask[rr - 1][lane] | ((uint32_t)sm.pmask[rr][lane] << 8) |
+                            ((uint32_t)sm.pmask[rr + 1][lane] << 16);
+        const uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
         uint32_t Lv = 0x3Fu, Sv = 0x3Fu;
 #pragma unroll
-        for (int dr = -1; dr <= 1; ++dr) {
-          const float4 a = ld4(&sm.psi[rr + dr][col]);
-          const uint32_t L = (a.x <= -1.f ? 1u : 0u) | (a.y <= -1.f ? 2u : 0u) | (a.z <= -1.f ? 4u : 0u) |
-                             (a.w <= -1.f ? 8u : 0u);
-          const uint32_t S = (a.x >= 1.f ? 1u : 0u) | (a.y >= 1.f ? 2u : 0u) | (a.z >= 1.f ? 4u : 0u) |
-                             (a.w >= 1.f ? 8u : 0u);
-          const uint32_t pk = L | (S << 4);
-          const uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
-          Lv &= (L << 1) | ((lf >> 3) & 1u) | ((rt & 1u) << 5);
-          Sv &= (S << 1) | ((lf >> 7) & 1u) | (((rt >> 4) & 1u) << 5);
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t L = (pk >> (8 * k)) & 0xFu, S = (pk >> (8 * k + 4)) & 0xFu;
+          Lv &= (L << 1) | ((lf >> (8 * k + 3)) & 1u) | (((rt >> (8 * k)) & 1u) << 5);
+          Sv &= (S << 1) | ((lf >> (8 * k + 7)) & 1u) | (((rt >> (8 * k + 4)) & 1u) << 5);
         }
         needs = ~((Lv & (Lv >> 1) & (Lv >> 2)) | (Sv & (Sv >> 1) & (Sv >> 2))) & outm;
         const uint32_t cnt = __popc(needs);
@@ -321,7 +357,25 @@ __global__ void __launch_bounds__(kThreads, 5)
       // stores, ghost copies (compute_boundary_individual, fun.cu:1220-1230)
       auto store_row = [&](int rowi) {
         const int64_t o = (int64_t)rowi * K.pitch + gi;
-        if ((outm & 0xEu) == 0xEu && ((outm & 1u) || gi == 0)) {
+        if (interior) {
+          if (lane != 0 && lane != 31) {
+            put(psi_n, o, po[0], po[1], po[2], po[3]);
+            put(c_n, o, dn[0], dn[1], dn[2], dn[3]);
+            if (phi_n) put(phi_n, o, clamp1(po[0]), clamp1(po[1]), clamp1(po[2]), clamp1(po[3]));
+          } else {
+            // lane 0: cell 1 alone, cells 2-3 as a pair; lane 31: cell 0
+            const int64_t o1 = lane == 0 ? o + 1 : o;
+            const float p1 = lane == 0 ? po[1] : po[0], c1 = lane == 0 ? dn[1] : dn[0];
+            psi_n[o1] = p1;
+            c_n[o1] = c1;
+            if (phi_n) phi_n[o1] = clamp1(p1);
+            if (lane == 0) {
+              *reinterpret_cast<float2 *>(psi_n + o + 2) = make_float2(po[2], po[3]);
+              *reinterpret_cast<float2 *>(c_n + o + 2) = make_float2(dn[2], dn[3]);
+              if (phi_n) *reinterpret_cast<float2 *>(phi_n + o + 2) = make_float2(clamp1(po[2]), clamp1(po[3]));
+            }
+          }
+        } else if ((outm & 0xEu) == 0xEu && ((outm & 1u) || gi == 0)) {
           // cells 1..3 are outputs; cell 0 is an output or the ghost column 0
           const float p0 = (outm & 1u) ? po[0] : po[1], c0 = (outm & 1u) ? dn[0] : dn[1];
           put(psi_n, o, p0, po[1], po[2], po[3]);
