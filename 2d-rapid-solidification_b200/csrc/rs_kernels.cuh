@@ -52,17 +52,14 @@ struct TmaMaps {
   float *col_tab;   // kColTabFields arrays of col_tab_len floats
   int col_tab_len;
 };
-constexpr int kTmaBoxW32 = 128;  // input columns of an FP32 tile (multiple of 4)
+constexpr int kTileOutW = 128;                  // output columns of an FP32 tile
+constexpr int kTmaBoxW32 = kTileOutW + 8;        // input columns (4 each side keep x 16-byte aligned)
 constexpr int kTmaBoxW64 = 250;  // input columns per CTA window, FP64 (multiple of 2)
 constexpr int kTileRows = 16;    // output rows of an FP32 tile
 constexpr int kTmaBoxH = kTileRows + 2;  // input rows of an FP32 tile
 constexpr int kColTabFields = 5;
-// length of the per-column table for nx_all columns: tiles start every
-// kTmaBoxW32 - 4 columns and read kTmaBoxW32
-inline int col_tab_len(int nx_all) {
-  const int ni = nx_all - 2, step = kTmaBoxW32 - 4;
-  return ((ni + step - 1) / step) * step + kTmaBoxW32;
-}
+// length of the per-column table (entry k is column k - 4) for nx_all columns
+inline int col_tab_len(int nx_all) { return ((nx_all + kTileOutW - 1) / kTileOutW) * kTileOutW + kTmaBoxW32; }
 
 // ---- launchers (return 0, or -1 when a size limit is exceeded)
 int launch_step_f64(const StepCoef &K, const StepScalars &P, const double *psi, const double *c,

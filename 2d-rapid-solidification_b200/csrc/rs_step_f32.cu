@@ -11,19 +11,22 @@
 //     its CTAs start, issue their TMA loads, and wait for the table only
 //     where they first read it.
 //
-// A CTA of 128 threads owns a tile of kTileRows output rows x 124 output
-// columns (input 18 x 128, one TMA box per field; tiles start every 124
-// columns, so every TMA x coordinate is 16-byte aligned).  Four adjacent
-// columns per lane.
-//   phase 1  per-cell S = q(psi) c (1-c) and mu'' (below) of all 18 input
-//            rows into shared memory, plus per-row flags "every cell has
-//            psi == -1" / "== +1";
-//   phase 2  each warp writes 4 output rows: fluxes through the faces from
-//            the shared S and mu'', the c update, stores; psi is copied
-//            where the 3x3 phi neighbourhood is uniformly +-1 (then
-//            phi_next = phi exactly) and the other cells are listed;
+// A CTA of 128 threads owns a tile of 16 output rows x 128 output columns
+// (x0 .. x0+127, x0 a multiple of 128).  Its input, 18 rows x 136 columns
+// (x0-4 .. x0+131, so the TMA x coordinate stays 16-byte aligned), arrives in
+// shared memory by one TMA box per field.  Four adjacent columns per lane.
+//   phase 1  per-cell S = q(psi) c (1-c) and mu'' (below) of the 18 input
+//            rows into shared memory, with per-row flags "every psi == -1" /
+//            "== +1" and per-lane phi masks; the halo columns x0-1 and
+//            x0+128 are computed by 36 threads on the side;
+//   phase 2  each warp computes 4 output rows: fluxes through the faces from
+//            the shared S and mu'', the c update (kept in registers); cells
+//            whose 3x3 phi neighbourhood is not uniformly +-1 are listed;
 //   phase 3  the listed interface cells are updated one per thread
-//            (phi_cell), so a tile's interface work is spread over the CTA.
+//            (phi_cell), so a tile's interface work is spread over the CTA;
+//   phase 4  new psi and c are written into the shared tile, ghost columns
+//            copied there, and each output row leaves by one bulk async copy
+//            per field (ghost rows by one more).
 // Arithmetic:
 //   * mu = K(T) + C0(T) + mu'' with C0 = -D - (L0_BCC - L0_Liq)(1 - 2 cinf)/2
 //     (D, K(T) as in rs_step.cu), so
@@ -44,35 +47,44 @@
 namespace rs {
 namespace {
 
-constexpr int kIn = kTmaBoxW32;     // input columns of a tile
-constexpr int kOut = kIn - 4;       // output columns of a tile
-constexpr int kTR = kTileRows;      // output rows of a tile
-constexpr int kTRin = kTmaBoxH;     // input rows of a tile
+constexpr int kW = kTileOutW;     // output columns of a tile
+constexpr int kWin = kTmaBoxW32;  // input columns of a tile (kW + 8)
+constexpr int kTR = kTileRows;    // output rows of a tile
+constexpr int kTRin = kTmaBoxH;   // input rows of a tile
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRowsPerWarp = kTR / kWarps;
+constexpr int kHaloL = 3, kHaloR = kW + 4;  // box columns of x0-1 and x0+kW
 constexpr uint32_t kWaitLimit = 1u << 20;
 constexpr unsigned FULL = 0xffffffffu;
-static_assert(kIn == 32 * 4, "four columns per lane");
-static_assert(kTR % kWarps == 0, "output rows are split evenly over the warps");
+static_assert(kW == 32 * 4, "four columns per lane");
+static_assert(kTR % kWarps == 0 && kRowsPerWarp == 4, "four output rows per warp");
 static_assert(kTRin <= 32, "row flags are 32-bit masks");
+static_assert(2 * kTRin <= kThreads && 4 * kTR <= kThreads, "one thread per halo cell and per row copy");
 
-// column table arrays (kColTabFields of them, col_tab_len floats each)
+// column table arrays (kColTabFields of them, col_tab_len floats each);
+// entry k describes column k - 4
 enum { kTabRT = 0, kTabC0 = 1, kTabDK = 2, kTabAnb = 3, kTabAti = 4 };
 
 struct alignas(128) TileSmem {
-  float psi[kTRin][kIn];  // TMA destinations
-  float d[kTRin][kIn];
-  float S[kTRin][kIn];
-  float mu[kTRin][kIn];
-  uint16_t list[kTR * kOut];  // interface cells: row << 8 | column
-  uint8_t pmask[kTRin][32];   // per lane: bits 0-3 psi <= -1, bits 4-7 psi >= 1 of its four cells
-  uint32_t liq, sol;          // bit r: every cell of input row r has psi == -1 / +1
+  // TMA destinations (128-byte aligned); rows 1..16 receive the new psi / c - cinf
+  alignas(128) float psi[kTRin][kWin];
+  alignas(128) float d[kTRin][kWin];
+  alignas(16) float S[kTRin][kWin];  // after phase 2: new psi of the listed cells
+  alignas(16) float mu[kTRin][kWin];
+  uint16_t list[kTR * kW];   // interface cells: row << 8 | output column
+  uint8_t pmask[kTRin][32];  // per lane: bits 0-3 psi <= -1, bits 4-7 psi >= 1 of its four cells
+  uint8_t hmask[kTRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
+  uint32_t liq, sol;         // bit r: every cell of input row r has psi == -1 / +1
   int nlist;
   double part_mass[kWarps];
   int part_itip[kWarps];
   uint64_t full;
 };
+
+static_assert(offsetof(TileSmem, psi) % 128 == 0 && offsetof(TileSmem, d) % 128 == 0,
+              "TMA destinations start on 128-byte boundaries");
+static_assert((kWin * sizeof(float)) % 16 == 0, "rows stay 16-byte aligned for float4 and bulk copies");
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void st4(float *p, float a, float b, float c, float e) {
@@ -80,14 +92,35 @@ __device__ __forceinline__ void st4(float *p, float a, float b, float c, float e
 }
 __device__ __forceinline__ float clamp1(float v) { return fminf(fmaxf(v, -1.f), 1.f); }
 
+// general per-cell terms (fun.cu:1424-1452)
+__device__ __forceinline__ void cell_terms(const Coef<float> &F, float pv, float dv, float RT, float C0, float &S,
+                                           float &mu) {
+  constexpr float L0sum = (float)(kL0Bcc + kL0Liq);
+  constexpr float L0half = (float)(0.5 * (kL0Bcc - kL0Liq));
+  const float c = F.cinf + dv, om = 1.f - c;
+  const float a = 1.f - pv;
+  S = (0.5f * F.AA * a - 0.25f * (F.AA - 1.f) * (a * a)) * c * om;
+  const float p2 = pv * pv;
+  const float g = pv * (1.875f + p2 * (-1.25f + 0.375f * p2));
+  const float lam = Tr<float>::lam(c, om, dv, F.cinf, F.Lref);
+  mu = -(g + 1.f) * C0 - dv * fmaf(2.f * L0half, g, L0sum) + RT * lam;
+}
+
+// shared -> global bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_store(void *gdst, const void *ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(ssrc)),
+               "r"(bytes)
+               : "memory");
+}
+
 __global__ void __launch_bounds__(128) column_table_kernel(const StepCoef K, const double d0, const double d1,
                                                            const int len, float *__restrict__ tab) {
   // the tile kernel may start now; it waits for this grid before reading tab
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= len) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= len) return;
   auto kc = [&](int col, TTerms &tt, double &C0) {
-    const int gi = min(col, K.nx - 1);
+    const int gi = min(max(col, 0), K.nx - 1);
     const double T = (d0 + d1 * gi) * K.deltaT0 + K.Tmelt;  // get_delta, fun.cu:1610-1619
     tt = t_terms(T, K.RR);
     const double D = 0.5 * (tt.dGs - tt.dGl);
@@ -96,12 +129,12 @@ __global__ void __launch_bounds__(128) column_table_kernel(const StepCoef K, con
   };
   TTerms t0, t1;
   double c0, c1;
-  const double k0 = kc(i, t0, c0), k1 = kc(i + 1, t1, c1);
-  tab[kTabRT * len + i] = (float)t0.RT;
-  tab[kTabC0 * len + i] = (float)c0;
-  tab[kTabDK * len + i] = (float)(k1 - k0);  // (K + C0)(i+1) - (K + C0)(i)
-  tab[kTabAnb * len + i] = (float)t0.A_nb;
-  tab[kTabAti * len + i] = (float)t0.A_ti;
+  const double k0 = kc(k - 4, t0, c0), k1 = kc(k - 3, t1, c1);
+  tab[kTabRT * len + k] = (float)t0.RT;
+  tab[kTabC0 * len + k] = (float)c0;
+  tab[kTabDK * len + k] = (float)(k1 - k0);  // (K + C0)(i+1) - (K + C0)(i)
+  tab[kTabAnb * len + k] = (float)t0.A_nb;
+  tab[kTabAti * len + k] = (float)t0.A_ti;
 }
 
 __global__ void __launch_bounds__(kThreads, 5)
@@ -113,9 +146,9 @@ __global__ void __launch_bounds__(kThreads, 5)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int x0 = kOut * blockIdx.y;  // first input column of the tile
+  const int x0 = kW * blockIdx.y;       // first output column of the tile
   const int y0 = 1 + kTR * blockIdx.x;  // first output row; input rows y0-1 .. y0+kTR
-  constexpr uint32_t kTileBytes = 2u * kTRin * kIn * sizeof(float);
+  constexpr uint32_t kTileBytes = 2u * kTRin * kWin * sizeof(float);
 
   if (smem_u32(smem_raw) & 127u) {  // TMA destinations must be 128-byte aligned
     if (threadIdx.x == 0) atomicExch(err, 2);
@@ -125,8 +158,8 @@ __global__ void __launch_bounds__(kThreads, 5)
     mbar_init(&sm.full, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     mbar_expect_tx(&sm.full, kTileBytes);
-    tma_load_2d(&sm.psi[0][0], &tm_psi, &sm.full, x0, y0 - 1);
-    tma_load_2d(&sm.d[0][0], &tm_c, &sm.full, x0, y0 - 1);
+    tma_load_2d(&sm.psi[0][0], &tm_psi, &sm.full, x0 - 4, y0 - 1);
+    tma_load_2d(&sm.d[0][0], &tm_c, &sm.full, x0 - 4, y0 - 1);
     sm.liq = 0u;
     sm.sol = 0u;
     sm.nlist = 0;
@@ -134,19 +167,15 @@ __global__ void __launch_bounds__(kThreads, 5)
 
   const int col = 4 * lane;  // tile column of this lane's first cell
   const int gi = x0 + col;   // its global column
-  uint32_t outm = 0;  // per cell: an output cell
+  const int bc = col + 4;    // its box column
+  uint32_t outm = 0;         // per cell: an interior (output) cell
 #pragma unroll
   for (int q = 0; q < 4; ++q)
-    if (col + q >= 1 && col + q <= kOut && gi + q <= K.nx - 2) outm |= 1u << q;
-  // interior tiles: no ghost column, every lane's cells are outputs except
-  // cell 0 of lane 0 and cells 1..3 of lane 31
-  const bool interior = x0 >= 4 && x0 + kOut <= K.nx - 3;
+    if (gi + q >= 1 && gi + q <= K.nx - 2) outm |= 1u << q;
   const float two_cinf = F.cinf + F.cinf;
   const float cflux4 = 0.25f * F.cflux;
   const float floor_d = F.c_floor - F.cinf;
   constexpr float KL = (float)(-2.0 * kL0Liq);
-  constexpr float L0sum = (float)(kL0Bcc + kL0Liq);
-  constexpr float L0half = (float)(0.5 * (kL0Bcc - kL0Liq));
   // delta range of the series form: s = delta / (A + B delta) with
   // A = 2 cinf (1 - cinf), B = 1 - 2 cinf, so |s| < 1/9 for
   // -A/(9+B) < delta < A/(9-B) (taken 0.1 % inside)
@@ -156,7 +185,9 @@ __global__ void __launch_bounds__(kThreads, 5)
 
   // the column table of this step (programmatic dependency on its kernel)
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  const float4 RTv = ld4(tab + kTabRT * tab_len + gi), C0v = ld4(tab + kTabC0 * tab_len + gi);
+  const float *tRT = tab + kTabRT * tab_len + 4, *tC0 = tab + kTabC0 * tab_len + 4;
+  const float *tDK = tab + kTabDK * tab_len + 4;
+  const float4 RTv = ld4(tRT + gi), C0v = ld4(tC0 + gi);
   const float RTa[4] = {RTv.x, RTv.y, RTv.z, RTv.w}, C0a[4] = {C0v.x, C0v.y, C0v.z, C0v.w};
   __syncthreads();  // barrier initialised, flags cleared
   {
@@ -168,13 +199,12 @@ __global__ void __launch_bounds__(kThreads, 5)
       }
     }
   }
-
   // columns beyond the array (right-most tiles; zero-filled by TMA) become
   // bulk melt, so they never force the general path; no output reads them
-  if (x0 + kIn > K.nx) {
-    for (int k = threadIdx.x; k < kTRin * kIn; k += kThreads) {
-      const int rr = k / kIn, x = k % kIn;
-      if (x0 + x >= K.nx) {
+  if (x0 + kW + 4 > K.nx) {
+    for (int k = threadIdx.x; k < kTRin * kWin; k += kThreads) {
+      const int rr = k / kWin, x = k % kWin;
+      if (x0 - 4 + x >= K.nx) {
         sm.psi[rr][x] = -1.f;
         sm.d[rr][x] = 0.f;
       }
@@ -185,10 +215,9 @@ __global__ void __launch_bounds__(kThreads, 5)
   // ---- phase 1: per-cell terms; warp w takes input rows w, w+4, ...
 #pragma unroll 1
   for (int rr = warp; rr < kTRin; rr += kWarps) {
-    const int y = y0 - 1 + rr;
-    if (y > K.ny - 1) {  // beyond the array (last tile): never read by an output
-      st4(&sm.S[rr][col], 0.f, 0.f, 0.f, 0.f);
-      st4(&sm.mu[rr][col], 0.f, 0.f, 0.f, 0.f);
+    if (y0 - 1 + rr > K.ny - 1) {  // beyond the array (last tile): never read by an output
+      st4(&sm.S[rr][bc], 0.f, 0.f, 0.f, 0.f);
+      st4(&sm.mu[rr][bc], 0.f, 0.f, 0.f, 0.f);
       sm.pmask[rr][lane] = 0xFFu;
       if (lane == 0) {
         atomicOr(&sm.liq, 1u << rr);
@@ -196,16 +225,11 @@ __global__ void __launch_bounds__(kThreads, 5)
       }
       continue;
     }
-    const float4 pv4 = ld4(&sm.psi[rr][col]), dv4 = ld4(&sm.d[rr][col]);
+    const float4 pv4 = ld4(&sm.psi[rr][bc]), dv4 = ld4(&sm.d[rr][bc]);
     const float pv[4] = {pv4.x, pv4.y, pv4.z, pv4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
-    float cc[4], om[4], Sv[4], mv[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      cc[q] = F.cinf + dv[q];
-      om[q] = 1.f - cc[q];
-    }
-    // the row is bulk melt when every psi is exactly -1 and every delta is in
-    // the series range (bit tests on psi, min/max on delta)
+    float Sv[4], mv[4];
+    // bulk melt: every psi exactly -1 (bit tests) and every delta in the
+    // series range
     const uint32_t b0 = __float_as_uint(pv[0]), b1 = __float_as_uint(pv[1]), b2 = __float_as_uint(pv[2]),
                    b3 = __float_as_uint(pv[3]);
     const uint32_t band = b0 & b1 & b2 & b3, bor = b0 | b1 | b2 | b3;
@@ -214,19 +238,19 @@ __global__ void __launch_bounds__(kThreads, 5)
     const bool liq4 = band == kMinus1 && bor == kMinus1;
     uint32_t code;
     if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
-      code = 5u;
+      code = 1u;
       sm.pmask[rr][lane] = 0x0Fu;
-      // lam = 2 atanh(s) by its odd series
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const float sv = __fdividef(dv[q], fmaf(two_cinf, om[q], dv[q]));
+        const float c = F.cinf + dv[q], om = 1.f - c;
+        const float sv = __fdividef(dv[q], fmaf(two_cinf, om, dv[q]));
         const float s2 = sv * sv;
         float p = fmaf(s2, 1.f / 9.f, 1.f / 7.f);
         p = fmaf(s2, p, 1.f / 5.f);
         p = fmaf(s2, p, 1.f / 3.f);
-        const float lh = fmaf(sv * s2, p, sv);  // atanh(s)
-        Sv[q] = cc[q] * om[q];
-        mv[q] = fmaf(RTa[q] + RTa[q], lh, dv[q] * KL);
+        const float ath = fmaf(sv * s2, p, sv);  // atanh(s); lam = 2 atanh(s)
+        Sv[q] = c * om;
+        mv[q] = fmaf(RTa[q] + RTa[q], ath, dv[q] * KL);
       }
     } else {
       const bool sol4 = band == kPlus1 && bor == kPlus1;
@@ -236,66 +260,83 @@ __global__ void __launch_bounds__(kThreads, 5)
       for (int q = 0; q < 4; ++q) {
         if (pv[q] <= -1.f) L |= 1u << q;
         if (pv[q] >= 1.f) Sm |= 1u << q;
+        cell_terms(F, pv[q], dv[q], RTa[q], C0a[q], Sv[q], mv[q]);
       }
       sm.pmask[rr][lane] = (uint8_t)(L | (Sm << 4));
-      // general form (fun.cu:1424-1452)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const float a = 1.f - pv[q];
-        Sv[q] = (0.5f * F.AA * a - 0.25f * (F.AA - 1.f) * (a * a)) * cc[q] * om[q];
-        const float p2 = pv[q] * pv[q];
-        const float g = pv[q] * (1.875f + p2 * (-1.25f + 0.375f * p2));
-        const float lam = Tr<float>::lam(cc[q], om[q], dv[q], F.cinf, F.Lref);
-        mv[q] = -(g + 1.f) * C0a[q] - dv[q] * fmaf(2.f * L0half, g, L0sum) + RTa[q] * lam;
-      }
     }
-    st4(&sm.S[rr][col], Sv[0], Sv[1], Sv[2], Sv[3]);
-    st4(&sm.mu[rr][col], mv[0], mv[1], mv[2], mv[3]);
+    st4(&sm.S[rr][bc], Sv[0], Sv[1], Sv[2], Sv[3]);
+    st4(&sm.mu[rr][bc], mv[0], mv[1], mv[2], mv[3]);
     if (lane == 0) {
       if (code & 1u) atomicOr(&sm.liq, 1u << rr);
       if (code & 2u) atomicOr(&sm.sol, 1u << rr);
     }
   }
-  const float4 dKv = ld4(tab + kTabDK * tab_len + gi);
-  const float dKa[4] = {dKv.x, dKv.y, dKv.z, dKv.w};
+  // halo columns x0-1 and x0+kW, one thread per cell
+  if (threadIdx.x < 2 * kTRin) {
+    const int rr = threadIdx.x >> 1, side = threadIdx.x & 1;
+    const int x = side ? kHaloR : kHaloL, g = x0 - 4 + x;
+    float Sh = 0.f, mh = 0.f;
+    uint8_t hm = 3u;
+    if (y0 - 1 + rr <= K.ny - 1) {
+      const float pv = sm.psi[rr][x];
+      cell_terms(F, pv, sm.d[rr][x], tRT[g], tC0[g], Sh, mh);
+      hm = (pv <= -1.f ? 1u : 0u) | (pv >= 1.f ? 2u : 0u);
+    }
+    sm.S[rr][x] = Sh;
+    sm.mu[rr][x] = mh;
+    sm.hmask[rr][side] = hm;
+  }
+  const float4 dKv = ld4(tDK + gi);
+  const float dKl = tDK[gi - 1];
+  const float dKa[5] = {dKl, dKv.x, dKv.y, dKv.z, dKv.w};  // faces x-1|x for x = col .. col+4
   __syncthreads();
 
-  // ---- phase 2: warp w writes output rows 1 + 4w .. 4 + 4w of the tile
+  // ---- phase 2: warp w computes output rows 1 + 4w .. 4 + 4w of the tile
   const uint32_t liq = sm.liq, sol = sm.sol;
   const bool red = partials != nullptr;
   double mass = 0.0;
   int itip = 0;
   struct Row {
-    float s[4], m[4], s4, m4, q[4];
+    float s[4], m[4], sl, sr, ml, mr, q[5];  // q[f]: S pair sum of the face left of cell f (f = 0..4)
   };
   auto load_row = [&](int rr, Row &R) {
-    const float4 s = ld4(&sm.S[rr][col]), m = ld4(&sm.mu[rr][col]);
+    const float4 s = ld4(&sm.S[rr][bc]), m = ld4(&sm.mu[rr][bc]);
     R.s[0] = s.x; R.s[1] = s.y; R.s[2] = s.z; R.s[3] = s.w;
     R.m[0] = m.x; R.m[1] = m.y; R.m[2] = m.z; R.m[3] = m.w;
-    R.s4 = __shfl_down_sync(FULL, s.x, 1);  // column 4 (next lane's first cell)
-    R.m4 = __shfl_down_sync(FULL, m.x, 1);
-    R.q[0] = R.s[0] + R.s[1];
-    R.q[1] = R.s[1] + R.s[2];
-    R.q[2] = R.s[2] + R.s[3];
-    R.q[3] = R.s[3] + R.s4;
+    R.sl = __shfl_up_sync(FULL, s.w, 1);
+    R.ml = __shfl_up_sync(FULL, m.w, 1);
+    R.sr = __shfl_down_sync(FULL, s.x, 1);
+    R.mr = __shfl_down_sync(FULL, m.x, 1);
+    if (lane == 0) {
+      R.sl = sm.S[rr][kHaloL];
+      R.ml = sm.mu[rr][kHaloL];
+    }
+    if (lane == 31) {
+      R.sr = sm.S[rr][kHaloR];
+      R.mr = sm.mu[rr][kHaloR];
+    }
+    R.q[0] = R.sl + R.s[0];
+    R.q[1] = R.s[0] + R.s[1];
+    R.q[2] = R.s[1] + R.s[2];
+    R.q[3] = R.s[2] + R.s[3];
+    R.q[4] = R.s[3] + R.sr;
   };
   // fluxes through the faces between rows A and B = A+1 (compute_c_CALPHAD F01/F0m)
   auto vface = [&](const Row &A, const Row &B, float jv[4]) {
-    float pp[4];
+    float pp[6];
+    pp[0] = A.sl + B.sl;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) pp[q] = A.s[q] + B.s[q];
-    const float pl = __shfl_up_sync(FULL, pp[3], 1), pr = __shfl_down_sync(FULL, pp[0], 1);
+    for (int q = 0; q < 4; ++q) pp[q + 1] = A.s[q] + B.s[q];
+    pp[5] = A.sr + B.sr;
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
-      jv[q] = fmaf(6.f, pp[q], (q ? pp[q - 1] : pl) + (q < 3 ? pp[q + 1] : pr)) * (B.m[q] - A.m[q]);
-  };
-  auto put = [&](float *f, int64_t o, float a, float b, float c, float e) {
-    *reinterpret_cast<float4 *>(f + o) = make_float4(a, b, c, e);
+    for (int q = 0; q < 4; ++q) jv[q] = fmaf(6.f, pp[q + 1], pp[q] + pp[q + 2]) * (B.m[q] - A.m[q]);
   };
 
   const int rbase = 1 + kRowsPerWarp * warp;
   Row ra, rb, rc;
   float jv_lo[4], jv_hi[4];
+  float dn[kRowsPerWarp][4];
+  uint32_t needs_all = 0u;  // 4 bits per output row
   load_row(rbase - 1, ra);
   load_row(rbase, rb);
   vface(ra, rb, jv_lo);
@@ -304,116 +345,68 @@ __global__ void __launch_bounds__(kThreads, 5)
     const int rr = rbase + j;  // tile input row of the output row
     load_row(rr + 1, rc);
     vface(rb, rc, jv_hi);
-    const int r = y0 - 1 + rr;  // global row
-    if (r <= K.ny - 2) {
-      // fluxes through the faces (i+1/2, r)
-      const float mnext[4] = {rb.m[1], rb.m[2], rb.m[3], rb.m4};
-      float jh[4];
+    // fluxes through the faces (x-1/2, r) for x = col .. col+4
+    const float mm[6] = {rb.ml, rb.m[0], rb.m[1], rb.m[2], rb.m[3], rb.mr};
+    float jh[5];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) jh[q] = fmaf(6.f, rb.q[q], ra.q[q] + rc.q[q]) * (mnext[q] - rb.m[q] + dKa[q]);
-      const float jl = __shfl_up_sync(FULL, jh[3], 1);
-      const float4 dv4 = ld4(&sm.d[rr][col]), pv4 = ld4(&sm.psi[rr][col]);
-      const float dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
-      float dn[4], po[4] = {pv4.x, pv4.y, pv4.z, pv4.w};
+    for (int f = 0; f < 5; ++f) jh[f] = fmaf(6.f, rb.q[f], ra.q[f] + rc.q[f]) * (mm[f + 1] - mm[f] + dKa[f]);
+    const float4 dv4 = ld4(&sm.d[rr][bc]);
+    const float dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      dn[j][q] = fmaxf(fmaf(cflux4, (jh[q + 1] - jh[q]) + (jv_hi[q] - jv_lo[q]), dv[q]), floor_d);
+    const bool live = y0 - 1 + rr <= K.ny - 2;
+    if (red && live) {
 #pragma unroll
       for (int q = 0; q < 4; ++q)
-        dn[q] = fmaxf(fmaf(cflux4, (jh[q] - (q ? jh[q - 1] : jl)) + (jv_hi[q] - jv_lo[q]), dv[q]), floor_d);
-      // phi: copied where the 3x3 neighbourhood is uniformly +-1, listed otherwise
-      uint32_t needs = 0u;
-      const uint32_t w3 = 7u << (rr - 1);
-      const bool uni_liq = (liq & w3) == w3;
-      if (!uni_liq && (sol & w3) != w3) {
-        // phi masks of rows rr-1 .. rr+1, this lane's cells with one cell of
-        // each neighbouring lane
-        const uint32_t pk = (uint32_t)sm.pmask[rr - 1][lane] | ((uint32_t)sm.pmask[rr][lane] << 8) |
-                            ((uint32_t)sm.pmask[rr + 1][lane] << 16);
-        const uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
-        uint32_t Lv = 0x3Fu, Sv = 0x3Fu;
+        if ((outm >> q) & 1u) mass += (double)dn[j][q];
+    }
+    // phi: cells whose 3x3 neighbourhood is not uniformly +-1 are listed
+    const uint32_t w3 = 7u << (rr - 1);
+    if (live && (liq & w3) != w3 && (sol & w3) != w3) {
+      const uint32_t pk = (uint32_t)sm.pmask[rr - 1][lane] | ((uint32_t)sm.pmask[rr][lane] << 8) |
+                          ((uint32_t)sm.pmask[rr + 1][lane] << 16);
+      uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
+      if (lane == 0) {
+        lf = 0u;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          const uint32_t L = (pk >> (8 * k)) & 0xFu, S = (pk >> (8 * k + 4)) & 0xFu;
-          Lv &= (L << 1) | ((lf >> (8 * k + 3)) & 1u) | (((rt >> (8 * k)) & 1u) << 5);
-          Sv &= (S << 1) | ((lf >> (8 * k + 7)) & 1u) | (((rt >> (8 * k + 4)) & 1u) << 5);
-        }
-        needs = ~((Lv & (Lv >> 1) & (Lv >> 2)) | (Sv & (Sv >> 1) & (Sv >> 2))) & outm;
-        const uint32_t cnt = __popc(needs);
-        uint32_t incl = cnt;  // inclusive warp scan of the counts
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t v = __shfl_up_sync(FULL, incl, o);
-          if (lane >= o) incl += v;
-        }
-        const uint32_t total = __shfl_sync(FULL, incl, 31);
-        int base = 0;
-        if (lane == 31 && total) base = atomicAdd(&sm.nlist, (int)total);
-        base = __shfl_sync(FULL, base, 31);
-        uint32_t off = (uint32_t)base + incl - cnt;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          if ((needs >> q) & 1u) sm.list[off++] = (uint16_t)((rr << 8) | (col + q));
-          po[q] = clamp1(po[q]);  // placeholder; the listed cells are rewritten in phase 3
+          const uint32_t h = sm.hmask[rr - 1 + k][0];
+          lf |= ((h & 1u) << (8 * k + 3)) | (((h >> 1) & 1u) << (8 * k + 7));
         }
       }
-      // stores, ghost copies (compute_boundary_individual, fun.cu:1220-1230)
-      auto store_row = [&](int rowi) {
-        const int64_t o = (int64_t)rowi * K.pitch + gi;
-        if (interior) {
-          if (lane != 0 && lane != 31) {
-            put(psi_n, o, po[0], po[1], po[2], po[3]);
-            put(c_n, o, dn[0], dn[1], dn[2], dn[3]);
-            if (phi_n) put(phi_n, o, clamp1(po[0]), clamp1(po[1]), clamp1(po[2]), clamp1(po[3]));
-          } else {
-            // lane 0: cell 1 alone, cells 2-3 as a pair; lane 31: cell 0
-            const int64_t o1 = lane == 0 ? o + 1 : o;
-            const float p1 = lane == 0 ? po[1] : po[0], c1 = lane == 0 ? dn[1] : dn[0];
-            psi_n[o1] = p1;
-            c_n[o1] = c1;
-            if (phi_n) phi_n[o1] = clamp1(p1);
-            if (lane == 0) {
-              *reinterpret_cast<float2 *>(psi_n + o + 2) = make_float2(po[2], po[3]);
-              *reinterpret_cast<float2 *>(c_n + o + 2) = make_float2(dn[2], dn[3]);
-              if (phi_n) *reinterpret_cast<float2 *>(phi_n + o + 2) = make_float2(clamp1(po[2]), clamp1(po[3]));
-            }
-          }
-        } else if ((outm & 0xEu) == 0xEu && ((outm & 1u) || gi == 0)) {
-          // cells 1..3 are outputs; cell 0 is an output or the ghost column 0
-          const float p0 = (outm & 1u) ? po[0] : po[1], c0 = (outm & 1u) ? dn[0] : dn[1];
-          put(psi_n, o, p0, po[1], po[2], po[3]);
-          put(c_n, o, c0, dn[1], dn[2], dn[3]);
-          if (phi_n) put(phi_n, o, clamp1(p0), clamp1(po[1]), clamp1(po[2]), clamp1(po[3]));
-          if (gi + 3 == K.nx - 2) {
-            psi_n[o + 4] = po[3];
-            c_n[o + 4] = dn[3];
-            if (phi_n) phi_n[o + 4] = clamp1(po[3]);
-          }
-        } else {
+      if (lane == 31) {
+        rt = 0u;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            if (!((outm >> q) & 1u)) continue;
-            psi_n[o + q] = po[q];
-            c_n[o + q] = dn[q];
-            if (phi_n) phi_n[o + q] = clamp1(po[q]);
-            if (gi + q == K.nx - 2) {
-              psi_n[o + q + 1] = po[q];
-              c_n[o + q + 1] = dn[q];
-              if (phi_n) phi_n[o + q + 1] = clamp1(po[q]);
-            }
-          }
-        }
-      };
-      store_row(r);
-      if (r == K.jmin) store_row(0);
-      if (r == K.jmax) store_row(K.ny - 1);
-      if (red) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if ((outm >> q) & 1u) mass += (double)dn[q];
-        if (!uni_liq) {
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (((outm & ~needs) >> q) & 1u && po[q] > 0.f) itip = max(itip, gi + q == K.nx - 2 ? K.nx - 1 : gi + q);
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t h = sm.hmask[rr - 1 + k][1];
+          rt |= ((h & 1u) << (8 * k)) | (((h >> 1) & 1u) << (8 * k + 4));
         }
       }
+      uint32_t Lv = 0x3Fu, Sv = 0x3Fu;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t L = (pk >> (8 * k)) & 0xFu, S = (pk >> (8 * k + 4)) & 0xFu;
+        Lv &= (L << 1) | ((lf >> (8 * k + 3)) & 1u) | (((rt >> (8 * k)) & 1u) << 5);
+        Sv &= (S << 1) | ((lf >> (8 * k + 7)) & 1u) | (((rt >> (8 * k + 4)) & 1u) << 5);
+      }
+      const uint32_t needs = ~((Lv & (Lv >> 1) & (Lv >> 2)) | (Sv & (Sv >> 1) & (Sv >> 2))) & outm;
+      const uint32_t cnt = __popc(needs);
+      uint32_t incl = cnt;  // inclusive warp scan of the counts
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t total = __shfl_sync(FULL, incl, 31);
+      int base = 0;
+      if (lane == 31 && total) base = atomicAdd(&sm.nlist, (int)total);
+      base = __shfl_sync(FULL, base, 31);
+      uint32_t off = (uint32_t)base + incl - cnt;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if ((needs >> q) & 1u) sm.list[off++] = (uint16_t)((rr << 8) | (col + q));
+      needs_all |= needs << (4 * j);
     }
     ra = rb;
     rb = rc;
@@ -426,29 +419,92 @@ __global__ void __launch_bounds__(kThreads, 5)
   const int nlist = sm.nlist;
   for (int idx = threadIdx.x; idx < nlist; idx += kThreads) {
     const uint32_t e = sm.list[idx];
-    const int rr = (int)(e >> 8), x = (int)(e & 0xFFu);
-    const int r = y0 - 1 + rr, g = x0 + x;
+    const int rr = (int)(e >> 8), x = (int)(e & 0xFFu) + 4;  // box column
+    const int r = y0 - 1 + rr, g = x0 + x - 4;
     const float res = phi_cell<float>(
         &F, clamp1(sm.psi[rr][x]), clamp1(sm.psi[rr][x + 1]), clamp1(sm.psi[rr][x - 1]), clamp1(sm.psi[rr + 1][x]),
         clamp1(sm.psi[rr - 1][x]), clamp1(sm.psi[rr + 1][x + 1]), clamp1(sm.psi[rr + 1][x - 1]),
         clamp1(sm.psi[rr - 1][x + 1]), clamp1(sm.psi[rr - 1][x - 1]), F.cinf + sm.d[rr][x],
-        tab[kTabAnb * tab_len + g], tab[kTabAti * tab_len + g], PS.step, (int64_t)r * K.nx + g, K.seed_lo,
+        tab[kTabAnb * tab_len + 4 + g], tab[kTabAti * tab_len + 4 + g], PS.step, (int64_t)r * K.nx + g, K.seed_lo,
         K.seed_hi);
-    const float ph = clamp1(res);
-    const int gx = g == 1 ? 0 : (g == K.nx - 2 ? K.nx - 1 : -1);
-    auto put1 = [&](int row) {
-      const int64_t o = (int64_t)row * K.pitch;
-      psi_n[o + g] = res;
-      if (phi_n) phi_n[o + g] = ph;
-      if (gx >= 0) {
-        psi_n[o + gx] = res;
-        if (phi_n) phi_n[o + gx] = ph;
-      }
-    };
-    put1(r);
-    if (r == K.jmin) put1(0);
-    if (r == K.jmax) put1(K.ny - 1);
+    sm.S[rr][x] = res;
     if (red && res > 0.f) itip = max(itip, g == K.nx - 2 ? K.nx - 1 : g);
+  }
+  __syncthreads();
+
+  // ---- phase 4: new psi and c into the tile rows
+#pragma unroll
+  for (int j = 0; j < kRowsPerWarp; ++j) {
+    const int rr = rbase + j;
+    const float4 pv4 = ld4(&sm.psi[rr][bc]);
+    const float pv[4] = {pv4.x, pv4.y, pv4.z, pv4.w};
+    const bool live = y0 - 1 + rr <= K.ny - 2;
+    float po[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const bool listed = (needs_all >> (4 * j + q)) & 1u;
+      po[q] = listed ? sm.S[rr][bc + q] : clamp1(pv[q]);  // phi_next = phi where uniformly +-1
+      if (red && live && !listed && ((outm >> q) & 1u) && po[q] > 0.f)
+        itip = max(itip, gi + q == K.nx - 2 ? K.nx - 1 : gi + q);
+    }
+    st4(&sm.psi[rr][bc], po[0], po[1], po[2], po[3]);
+    st4(&sm.d[rr][bc], dn[j][0], dn[j][1], dn[j][2], dn[j][3]);
+  }
+  const int nrow = min(kTR, K.ny - 1 - y0);  // output rows of this tile inside the interior
+  const int ncol = min(kW, K.nx - x0);       // columns of this tile inside the array (a multiple of 4)
+  if (x0 == 0 || x0 + kW >= K.nx) {
+    // ghost columns 0 and nx-1 (compute_boundary_individual, fun.cu:1220-1230)
+    __syncthreads();
+    if (threadIdx.x < nrow) {
+      const int rr = 1 + threadIdx.x;
+      if (x0 == 0) {
+        sm.psi[rr][4] = sm.psi[rr][5];
+        sm.d[rr][4] = sm.d[rr][5];
+      }
+      if (x0 + kW >= K.nx) {
+        const int x = K.nx - 1 - x0 + 4;
+        sm.psi[rr][x] = sm.psi[rr][x - 1];
+        sm.d[rr][x] = sm.d[rr][x - 1];
+      }
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // tile writes -> bulk copies
+  __syncthreads();
+
+  // ---- bulk copies: thread (row j, field, kind): kind 0 the row itself,
+  // kind 1 its ghost copies (row jmin -> 0, row jmax -> ny-1)
+  if (threadIdx.x < 4 * kTR) {
+    const int j = threadIdx.x >> 2, field = threadIdx.x & 1, kind = (threadIdx.x >> 1) & 1;
+    const int r = y0 + j;
+    if (j < nrow) {
+      float *f = field ? c_n : psi_n;
+      const float *src = field ? &sm.d[1 + j][4] : &sm.psi[1 + j][4];
+      const uint32_t bytes = (uint32_t)ncol * 4u;
+      bool any = false;
+      if (kind == 0) {
+        bulk_store(f + (int64_t)r * K.pitch + x0, src, bytes);
+        any = true;
+      } else {
+        if (r == K.jmin) {
+          bulk_store(f + x0, src, bytes);
+          any = true;
+        }
+        if (r == K.jmax) {
+          bulk_store(f + (int64_t)(K.ny - 1) * K.pitch + x0, src, bytes);
+          any = true;
+        }
+      }
+      if (any) asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+  }
+  if (phi_n) {  // phi = clamp(psi) of the same rows, plain stores
+    for (int k = threadIdx.x; k < nrow * ncol; k += kThreads) {
+      const int j = k / ncol, x = k % ncol, r = y0 + j;
+      const float v = clamp1(sm.psi[1 + j][4 + x]);
+      phi_n[(int64_t)r * K.pitch + x0 + x] = v;
+      if (r == K.jmin) phi_n[x0 + x] = v;
+      if (r == K.jmax) phi_n[(int64_t)(K.ny - 1) * K.pitch + x0 + x] = v;
+    }
   }
 
   if (partials) {
@@ -473,6 +529,8 @@ __global__ void __launch_bounds__(kThreads, 5)
       partials[(int64_t)blockIdx.y * gridDim.x + blockIdx.x] = b;
     }
   }
+  // shared memory stays allocated until the copies have read it
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
 }  // namespace
@@ -480,12 +538,13 @@ __global__ void __launch_bounds__(kThreads, 5)
 int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScalars &P, const TmaMaps &tm,
                         float *psi_n, float *c_n, float *phi_n, BlockPartial *partials, int max_partials,
                         int *nparts_out, int *err, cudaStream_t st) {
-  const int ni = K.nx - 2, nj = K.ny - 2;
+  const int nj = K.ny - 2;
+  if (K.nx % 4 || K.pitch != K.nx) return -1;  // rows are copied in 16-byte units
   // column-major: consecutive CTAs share a column strip and its halo rows in L2
-  const dim3 grid((nj + kTR - 1) / kTR, (ni + kOut - 1) / kOut), block(kThreads);
+  const dim3 grid((nj + kTR - 1) / kTR, (K.nx + kW - 1) / kW), block(kThreads);
   const int nparts = grid.x * grid.y;
   if (partials && nparts > max_partials) return -1;
-  if (tm.col_tab_len < (int)grid.y * kOut + kIn) return -1;
+  if (tm.col_tab_len < (int)grid.y * kW + kWin) return -1;
   const size_t smem = sizeof(TileSmem);
   static bool attr_done = false;
   if (!attr_done) {
