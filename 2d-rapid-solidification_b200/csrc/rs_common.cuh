@@ -21,39 +21,48 @@ constexpr double kL0Liq = 5144.29;
 
 // ---------------------------------------------------------------- CALPHAD
 // SGTE-style pure-element Gibbs energies (fun.cu:1628-1666).  logT is passed
-// in so that one log serves all four functions at a temperature.
-RS_HD double g_ti_bcc(double T, double logT) {
+// in so that one log serves all four functions at a temperature.  With
+// iT = 1/T > 0 the c/T terms are evaluated as c * iT (one division for all
+// four functions, used where the result is rounded to FP32); with iT = 0 they
+// divide as the reference does.
+RS_HD double over_T(double c, double T, double iT) { return iT > 0.0 ? c * iT : c / T; }
+
+RS_HD double g_ti_bcc(double T, double logT, double iT = 0.0) {
   if (T >= 1155.0 && T < 1941.0)
     return 6667.385 + 105.366379 * T - 22.3771 * T * logT + 1.21707e-3 * (T * T) -
-           0.84534e-6 * ((T * T) * T) - 2002750.0 / T;
+           0.84534e-6 * ((T * T) * T) - over_T(2002750.0, T, iT);
   else if (T >= 1941.0)
     return 26483.26 - 182.426471 * T + 19.0900905 * T * logT - 22.00832e-3 * (T * T) +
-           1.228863e-6 * ((T * T) * T) + 1400501.0 / T;
+           1.228863e-6 * ((T * T) * T) + over_T(1400501.0, T, iT);
   return NAN;
 }
-RS_HD double g_ti_liq(double T, double logT) {
+RS_HD double g_ti_liq(double T, double logT, double iT = 0.0) {
   if (T >= 1300.0 && T < 1941.0)
     return 369519.198 - 2554.0225 * T + 342.059267 * T * logT - 163.409355e-3 * (T * T) +
-           12.457117e-6 * ((T * T) * T) - 67034516.0 / T;
+           12.457117e-6 * ((T * T) * T) - over_T(67034516.0, T, iT);
   else if (T >= 1941.0 && T < 4000.0)
     return -19887.066 + 298.7367 * T - 46.29 * T * logT;
   return NAN;
 }
-RS_HD double g_nb_bcc(double T, double logT) {
+RS_HD double g_nb_bcc(double T, double logT, double iT = 0.0) {
   if (T >= 298.15 && T < 2750.0)
     return -8519.353 + 142.045475 * T - 26.4711 * T * logT + 0.203475e-3 * (T * T) -
-           0.35012e-6 * ((T * T) * T) + 93399.0 / T;
+           0.35012e-6 * ((T * T) * T) + over_T(93399.0, T, iT);
   else if (T >= 2750.0) {
     const double t3 = (T * T) * T;
+    if (iT > 0.0) {
+      const double i3 = (iT * iT) * iT;
+      return -37669.3 + 271.720843 * T - 41.77 * T * logT + 1528.238e29 * ((i3 * i3) * i3);
+    }
     return -37669.3 + 271.720843 * T - 41.77 * T * logT + 1528.238e29 / ((t3 * t3) * t3);
   }
   return NAN;
 }
-RS_HD double g_nb_liq(double T, double logT) {
+RS_HD double g_nb_liq(double T, double logT, double iT = 0.0) {
   if (T >= 298.15 && T < 2750.0) {
     const double t2 = T * T;
     return 21262.202 + 131.229057 * T - 26.4711 * T * logT + 0.203475e-3 * t2 -
-           0.35012e-6 * (t2 * T) + 93399.0 / T - 306.098e-25 * (((t2 * t2) * t2) * T);
+           0.35012e-6 * (t2 * T) + over_T(93399.0, T, iT) - 306.098e-25 * (((t2 * t2) * t2) * T);
   } else if (T >= 2750.0)
     return -7499.398 + 260.756148 * T - 41.77 * T * logT;
   return NAN;
@@ -73,10 +82,12 @@ struct TTerms {
   double RT;    // RR T
 };
 
-RS_HD TTerms t_terms(double T, double RR) {
+// recip: evaluate the c/T terms with one reciprocal (FP32 tables)
+RS_HD TTerms t_terms(double T, double RR, bool recip = false) {
   const double lT = log(T);
-  const double tb = g_ti_bcc(T, lT), tl = g_ti_liq(T, lT);
-  const double nb = g_nb_bcc(T, lT), nl = g_nb_liq(T, lT);
+  const double iT = recip ? 1.0 / T : 0.0;
+  const double tb = g_ti_bcc(T, lT, iT), tl = g_ti_liq(T, lT, iT);
+  const double nb = g_nb_bcc(T, lT, iT), nl = g_nb_liq(T, lT, iT);
   TTerms r;
   r.dGs = tb - nb;
   r.dGl = tl - nl;

@@ -113,28 +113,29 @@ __device__ __forceinline__ void bulk_store(void *gdst, const void *ssrc, uint32_
                : "memory");
 }
 
-__global__ void __launch_bounds__(128) column_table_kernel(const StepCoef K, const double d0, const double d1,
-                                                           const int len, float *__restrict__ tab) {
+// One thread per column, one t_terms each (c/T terms by one reciprocal: the
+// groups are rounded to FP32); K + C0 of the next column comes from the
+// neighbouring thread, so blocks overlap by one column and write 127 entries.
+constexpr int kTabBlock = 128;
+__global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef K, const double d0, const double d1,
+                                                                 const int len, float *__restrict__ tab) {
   // the tile kernel may start now; it waits for this grid before reading tab
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= len) return;
-  auto kc = [&](int col, TTerms &tt, double &C0) {
-    const int gi = min(max(col, 0), K.nx - 1);
-    const double T = (d0 + d1 * gi) * K.deltaT0 + K.Tmelt;  // get_delta, fun.cu:1610-1619
-    tt = t_terms(T, K.RR);
-    const double D = 0.5 * (tt.dGs - tt.dGl);
-    C0 = -D - 0.5 * (kL0Bcc - kL0Liq) * (1.0 - 2.0 * K.cinf);
-    return 0.5 * (tt.dGs + tt.dGl) + 0.5 * (kL0Bcc + kL0Liq) * (1.0 - 2.0 * K.cinf) + tt.RT * K.Lref + C0;
-  };
-  TTerms t0, t1;
-  double c0, c1;
-  const double k0 = kc(k - 4, t0, c0), k1 = kc(k - 3, t1, c1);
-  tab[kTabRT * len + k] = (float)t0.RT;
-  tab[kTabC0 * len + k] = (float)c0;
-  tab[kTabDK * len + k] = (float)(k1 - k0);  // (K + C0)(i+1) - (K + C0)(i)
-  tab[kTabAnb * len + k] = (float)t0.A_nb;
-  tab[kTabAti * len + k] = (float)t0.A_ti;
+  __shared__ double kc[kTabBlock];
+  const int k = blockIdx.x * (kTabBlock - 1) + threadIdx.x;  // table entry; column k - 4
+  const int gi = min(max(k - 4, 0), K.nx - 1);
+  const double T = (d0 + d1 * gi) * K.deltaT0 + K.Tmelt;  // get_delta, fun.cu:1610-1619
+  const TTerms tt = t_terms(T, K.RR, true);
+  const double D = 0.5 * (tt.dGs - tt.dGl);
+  const double C0 = -D - 0.5 * (kL0Bcc - kL0Liq) * (1.0 - 2.0 * K.cinf);
+  kc[threadIdx.x] = 0.5 * (tt.dGs + tt.dGl) + 0.5 * (kL0Bcc + kL0Liq) * (1.0 - 2.0 * K.cinf) + tt.RT * K.Lref + C0;
+  __syncthreads();
+  if (threadIdx.x == kTabBlock - 1 || k >= len) return;
+  tab[kTabRT * len + k] = (float)tt.RT;
+  tab[kTabC0 * len + k] = (float)C0;
+  tab[kTabDK * len + k] = (float)(kc[threadIdx.x + 1] - kc[threadIdx.x]);  // (K + C0)(i+1) - (K + C0)(i)
+  tab[kTabAnb * len + k] = (float)tt.A_nb;
+  tab[kTabAti * len + k] = (float)tt.A_ti;
 }
 
 __global__ void __launch_bounds__(kThreads, 5)
@@ -552,7 +553,7 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
       return -3;
     attr_done = true;
   }
-  column_table_kernel<<<(tm.col_tab_len + 127) / 128, 128, 0, st>>>(K, P.d0, P.d1, tm.col_tab_len, tm.col_tab);
+  column_table_kernel<<<(tm.col_tab_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(K, P.d0, P.d1, tm.col_tab_len, tm.col_tab);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
