@@ -105,3 +105,11 @@ def test_phase_boundaries_of_ti10nb():
     assert abs(cs - configs.C_SOLID_AT_TLIQ) < 1e-6
     cl, cs = tangent(configs.T_SOLIDUS_TI10NB)
     assert abs(cs - 0.90) < 1e-6
+
+
+def test_driver_binary_prints_usage():
+    """The host driver is built beside the library and starts without a GPU."""
+    import subprocess
+    drv = os.path.join(os.path.dirname(lib.LIB_PATH), "rs_run")
+    r = subprocess.run([drv, "--help"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "usage: rs_run" in r.stdout
