@@ -57,6 +57,8 @@ struct rs_ctx {
   int *row_last;
   double *row_f, *row_g;
   int *d_err;          // set by a device-side bounded wait that gave up
+  const void *pb_cur;  // psi of the cur set of the last rs_step that fused a pull-back
+  int32_t pb_offset;   // and its shift (read by rs_integrate_phi)
   float *col_tab;      // per-column CALPHAD table of the FP32 TMA kernel
   int col_tab_len;
   int use_tma;         // RS_OPT_TMA
@@ -396,6 +398,8 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
     return fail(RS_E_UNSUPPORTED, "rs_step: the FP32 path supports the frozen temperature only");
   const rs::StepScalars P = step_scalars(c, a);
   cudaStream_t st = (cudaStream_t)stream;
+  c->pb_cur = a->pull_back ? cur->psi : nullptr;
+  c->pb_offset = a->pull_back ? a->i_offset : 0;
   const bool red = a->mass_out || a->itip_out;
   int nb = 0;
   int lr;
@@ -564,7 +568,9 @@ int rs_integrate_phi(rs_ctx *c, const rs_fields *cur, const rs_fields *next, dou
   int rc = check_fields(c, cur, "rs_integrate_phi cur", false);
   if (!rc) rc = check_fields(c, next, "rs_integrate_phi next", false);
   if (rc) return rc;
-  rs::launch_integrate_phi(cur->precision, c->T, cur->psi, next->psi, d_dphidt, i_left_end, 1.0,
+  // a pull-back fused into the last rs_step on this cur shifted its read side only
+  const int off = (c->pb_cur && cur->psi == c->pb_cur) ? c->pb_offset : 0;
+  rs::launch_integrate_phi(cur->precision, c->T, cur->psi, next->psi, d_dphidt, i_left_end, off,
                            (cudaStream_t)stream);
   return cuda_check("rs_integrate_phi");
 }

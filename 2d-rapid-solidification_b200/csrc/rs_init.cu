@@ -159,8 +159,11 @@ void launch_interpolate_temperature(const TfcCoef &T, const StepCoef &, const do
 // integrate_phi (fun.cu:1494-1535): latent-heat source per coarse cell, summed
 // in the reference's order (rows outer, columns inner)
 template <typename R>
+// psi is read through the pull_back column remap of i_offset (0: none), so
+// the source of a step whose shift was fused into rs_step sees the shifted
+// field, as after the reference's pull_back swap (fun.cu:451-463).
 __global__ void integrate_phi_kernel(const TfcCoef T, const R *__restrict__ psi, const R *__restrict__ psi_n,
-                                     double *__restrict__ dphidt, int ile) {
+                                     double *__restrict__ dphidt, int ile, int i_offset) {
   const int iT = blockIdx.x * blockDim.x + threadIdx.x;
   const int jT = blockIdx.y * blockDim.y + threadIdx.y;
   if (iT >= T.NxT_all || jT >= T.NyT_all) return;
@@ -175,7 +178,8 @@ __global__ void integrate_phi_kernel(const TfcCoef T, const R *__restrict__ psi,
     for (int j = 1 + r * (jT - 1); j <= r * jT; j++)
       for (int i = i0; i <= in; i++) {
         const int64_t o = (int64_t)j * T.pitch + i;
-        integral += (double)psi_n[o] - (double)psi[o];
+        const int is = i_offset ? min(max(i + i_offset, 1), T.nx - 2) : i;  // pull_back, fun.cu:1476-1487
+        integral += (double)psi_n[o] - (double)psi[(int64_t)j * T.pitch + is];
       }
     dphidt[(int64_t)jT * T.NxT_all + iT] = integral * 0.5;
   } else {
@@ -184,12 +188,12 @@ __global__ void integrate_phi_kernel(const TfcCoef T, const R *__restrict__ psi,
 }
 
 void launch_integrate_phi(int precision, const TfcCoef &T, const void *psi, const void *psi_n,
-                          double *dphidt, int ile, double, cudaStream_t st) {
+                          double *dphidt, int ile, int i_offset, cudaStream_t st) {
   dim3 b(64, 4), g((T.NxT_all + 63) / 64, (T.NyT_all + 3) / 4);
   if (precision == RS_F64)
-    integrate_phi_kernel<double><<<g, b, 0, st>>>(T, (const double *)psi, (const double *)psi_n, dphidt, ile);
+    integrate_phi_kernel<double><<<g, b, 0, st>>>(T, (const double *)psi, (const double *)psi_n, dphidt, ile, i_offset);
   else
-    integrate_phi_kernel<float><<<g, b, 0, st>>>(T, (const float *)psi, (const float *)psi_n, dphidt, ile);
+    integrate_phi_kernel<float><<<g, b, 0, st>>>(T, (const float *)psi, (const float *)psi_n, dphidt, ile, i_offset);
 }
 
 }  // namespace rs

@@ -110,7 +110,7 @@ void launch_temperature_substep(const TfcCoef &T, const double *Tin, double *Tou
 void launch_interpolate_temperature(const TfcCoef &T, const StepCoef &K, const double *d_T,
                                     double *d_T_fine, int i_left_end, cudaStream_t st);
 void launch_integrate_phi(int precision, const TfcCoef &T, const void *psi, const void *psi_n,
-                          double *dphidt, int i_left_end, double psi_scale, cudaStream_t st);
+                          double *dphidt, int i_left_end, int i_offset, cudaStream_t st);
 
 // records a message for rs_last_error() and returns code (rs_capi.cu)
 int set_error(int code, const char *msg);

@@ -241,7 +241,10 @@ int rs_temperature_init(rs_ctx *ctx, double *d_T, rs_stream_t stream);
 int rs_temperature_step(rs_ctx *ctx, double *d_T, double *d_T_next,
                         const double *d_dphidt, int64_t step, rs_stream_t stream);
 /* integrate_phi (fun.cu:1494-1535): latent-heat source per coarse cell,
- * 0.5 * sum of (psi_next - psi) over its ratio x ratio fine cells. */
+ * 0.5 * sum of (psi_next - psi) over its ratio x ratio fine cells.  When the
+ * last rs_step on this context fused a pull-back into its read of cur, psi of
+ * cur is read through the same shift, as the reference integrates after its
+ * pull_back swap (fun.cu:451-486). */
 int rs_integrate_phi(rs_ctx *ctx, const rs_fields *cur, const rs_fields *next,
                      double *d_dphidt, int32_t i_left_end, rs_stream_t stream);
 /* interpolate_temperature (fun.cu:1580-1608): bilinear coarse -> fine. */

@@ -169,3 +169,76 @@ def test_tfc_step_f64():
     o = pyoracle.step(p, d, s, 0, T_fine=Tf)
     g = download(p, nxt)
     assert maxabs(g.psi, o.psi) <= 1e-13 and maxabs(g.c, o.c) <= 1e-13
+
+
+def test_tfc_loop_with_pull_back_f64():
+    """The coarse-temperature loop of fun.cu:431-514 over 120 steps, pull-back
+    every 30 steps with non-zero shifts, on the GPU (pull-back fused into
+    rs_step, rs_integrate_phi reading cur through the same shift) against the
+    oracle doing the reference's order: pull_back, step, integrate_phi on the
+    shifted field, ratio_dt_dtT temperature sub-steps, interpolate_temperature."""
+    p = tfc_params()
+    p.step_pull_back = 30
+    d = pyoracle.derive(p)
+    nsteps, nT = 120, d.NxT_all * d.NyT_all
+    # the front starts 5 cells ahead of i_tip_target, so the frame shifts
+    p0 = tfc_params()
+    p0.i_tip_target += 5
+    s0 = perturbed_state(p0, 23, amp=0.2)
+    L = pyoracle.lib()
+    pr = lambda a: pyoracle._p(np.ascontiguousarray(a))
+    # oracle
+    s = s0.copy()
+    T = np.zeros(nT)
+    L.ro_initial_temperature(C.byref(p), C.byref(d), pr(T))
+    ile = d.i_left_end_initial
+    Tf = np.zeros((p.ny_all, p.nx_all))
+    L.ro_interpolate_temperature(C.byref(p), C.byref(d), pr(T), pr(Tf), ile)
+    hist, l, shifts = 0, 0.0, []
+    for n in range(nsteps):
+        if n % d.step_pull_back == 0:
+            off = pyoracle.itip(p, s.psi) - p.i_tip_target
+            shifts.append(off)
+            hist += off
+            ile = d.i_left_end_initial + hist - int(l / p.dx)
+            s = pyoracle.pull_back(p, s, off)
+        s2 = pyoracle.step(p, d, s, n, i_offset_history=hist, l_offset_Vp=l, T_fine=Tf)
+        D = np.zeros(nT)
+        L.ro_integrate_phi(C.byref(p), C.byref(d), pr(D), pr(s.psi), pr(s2.psi), ile)
+        a, b = T.copy(), T.copy()
+        for _ in range(d.ratio_dt_dtT):
+            L.ro_compute_temperature(C.byref(p), C.byref(d), pr(a), pr(b), pr(D), n)
+            a, b = b, a
+        T = a
+        L.ro_interpolate_temperature(C.byref(p), C.byref(d), pr(T), pr(Tf), ile)
+        s = s2
+        l += pyoracle.l_offset_increment(p, d, n)
+    assert any(shifts), shifts
+    # GPU
+    ctx = lib.Context(p)
+    ga, gb = upload(p, s0), lib.FieldSet(p, torch.float64)
+    Tg = torch.zeros(nT, dtype=torch.float64, device="cuda")
+    Tn, dphidt = torch.zeros_like(Tg), torch.zeros_like(Tg)
+    ctx.temperature_init(Tg)
+    itip = torch.zeros(1, dtype=torch.int32, device="cuda")
+    hist, l = 0, 0.0
+    ile = ile_T = d.i_left_end_initial
+    for n in range(nsteps):
+        pb = None
+        if n % d.step_pull_back == 0:
+            ctx.itip(ga, itip)
+            pb = int(itip.item()) - p.i_tip_target
+            hist += pb
+            ile = d.i_left_end_initial + hist - int(l / p.dx)
+        ctx.step(ga, gb, n, i_offset_history=hist, l_offset_Vp=l, pull_back=pb, T_coarse=Tg, i_left_end=ile,
+                 i_left_end_T=ile_T)
+        ctx.integrate_phi(ga, gb, dphidt, ile)
+        ctx.temperature_step(Tg, Tn, dphidt, n)
+        ile_T = ile
+        l += pyoracle.l_offset_increment(p, d, n)
+        ga, gb = gb, ga
+    g = download(p, ga)
+    assert maxabs(g.psi, s.psi) <= 1e-10 and maxabs(g.c, s.c) <= 1e-10
+    Tgh = Tg.cpu().numpy().reshape(d.NyT_all, d.NxT_all)
+    To = T.reshape(d.NyT_all, d.NxT_all)
+    assert maxabs(Tgh[:d.NyT, :d.NxT], To[:d.NyT, :d.NxT]) <= 1e-9
