@@ -13,7 +13,8 @@
 #include <mutex>
 #include <new>
 
-#include "rs_kernels.cuh"
+#include "rs_mlp.cuh"
+#include "rs_surrogate.cuh"
 
 namespace {
 
@@ -61,6 +62,10 @@ struct rs_ctx {
   int32_t pb_offset;   // and its shift (read by rs_integrate_phi)
   float *col_tab;      // per-column CALPHAD table of the FP32 TMA kernel
   int col_tab_len;
+  rs::SurrArgs surr;   // learned CALPHAD surrogate of the FP32 step (surr.w == nullptr: exact)
+  float *mlp_w;        // its FP32 parameters (device)
+  uint16_t *mlp_b16;   // BF16 W2 (32 x 32) and W3 padded to 8 rows (device)
+  unsigned long long *mlp_audit;  // max error bits of mu'' and dG, fallback and audit counts
   int use_tma;         // RS_OPT_TMA
   TmaEntry tma[8];     // tensor-map cache keyed by field pointer
   int tma_n, tma_next;
@@ -345,6 +350,9 @@ int rs_destroy(rs_ctx *c) {
   cudaFree(c->row_g);
   cudaFree(c->d_err);
   cudaFree(c->col_tab);
+  cudaFree(c->mlp_w);
+  cudaFree(c->mlp_b16);
+  cudaFree(c->mlp_audit);
   delete c;
   return RS_OK;
 }
@@ -413,6 +421,7 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
       field_map(c, cur->c, cur->precision, &tm.c)) {
     tm.col_tab = c->col_tab;
     tm.col_tab_len = c->col_tab_len;
+    tm.surr = c->surr.w ? &c->surr : nullptr;
     tmp = &tm;
   }
   if (cur->precision == RS_F64)
@@ -573,6 +582,131 @@ int rs_integrate_phi(rs_ctx *c, const rs_fields *cur, const rs_fields *next, dou
   rs::launch_integrate_phi(cur->precision, c->T, cur->psi, next->psi, d_dphidt, i_left_end, off,
                            (cudaStream_t)stream);
   return cuda_check("rs_integrate_phi");
+}
+
+// ---------------------------------------------------------------- surrogate
+static rs::MlpBox to_box(const rs_mlp_box *b) {
+  rs::MlpBox m;
+  m.T_lo = b->T_lo;
+  m.T_hi = b->T_hi;
+  m.c_lo = b->c_lo;
+  m.c_hi = b->c_hi;
+  for (int q = 0; q < 2; ++q) {
+    m.y_mean[q] = b->y_mean[q];
+    m.y_scale[q] = b->y_scale[q];
+  }
+  return m;
+}
+
+static bool box_ok(const rs_mlp_box *b) {
+  return b && b->T_hi > b->T_lo && b->c_hi > b->c_lo && b->c_lo > 0.0 && b->c_hi < 1.0 && b->y_scale[0] > 0.0 &&
+         b->y_scale[1] > 0.0;
+}
+
+int rs_mlp_sample(const rs_params *p, const rs_mlp_box *box, int64_t n, uint64_t seed, float *d_x, float *d_y,
+                  rs_stream_t stream) {
+  if (!p || !d_x || !d_y || n < 0) return fail(RS_E_INVALID, "rs_mlp_sample: bad argument");
+  if (!box || !(box->T_hi > box->T_lo) || !(box->c_hi > box->c_lo) || box->c_lo <= 0.0 || box->c_hi >= 1.0)
+    return fail(RS_E_INVALID, "rs_mlp_sample: box must have T_lo < T_hi and 0 < c_lo < c_hi < 1");
+  rs::launch_mlp_sample(p->cinf, p->RR, to_box(box), n, seed, d_x, d_y, (cudaStream_t)stream);
+  return cuda_check("rs_mlp_sample");
+}
+
+int rs_mlp_grad(const rs_mlp_box *box, const float *d_w, int64_t n, const float *d_x, const float *d_y,
+                float *d_grad, double *d_loss, rs_stream_t stream) {
+  if (!box_ok(box) || !d_w || !d_x || !d_y || !d_grad || !d_loss || n < 0)
+    return fail(RS_E_INVALID, "rs_mlp_grad: bad argument");
+  if (rs::launch_mlp_grad(to_box(box), d_w, n, d_x, d_y, d_grad, d_loss, (cudaStream_t)stream))
+    return fail(RS_E_CUDA, "rs_mlp_grad: cannot configure shared memory");
+  return cuda_check("rs_mlp_grad");
+}
+
+int rs_mlp_adam(float *d_w, const float *d_grad, float *d_m, float *d_v, int64_t t, float lr, float scale,
+                rs_stream_t stream) {
+  if (!d_w || !d_grad || !d_m || !d_v || t < 1) return fail(RS_E_INVALID, "rs_mlp_adam: bad argument");
+  rs::launch_mlp_adam(d_w, d_grad, d_m, d_v, t, lr, scale, (cudaStream_t)stream);
+  return cuda_check("rs_mlp_adam");
+}
+
+int rs_mlp_forward(const rs_mlp_box *box, const float *d_w, int64_t n, const float *d_x, float *d_out,
+                   rs_stream_t stream) {
+  if (!box_ok(box) || !d_w || !d_x || !d_out || n < 0) return fail(RS_E_INVALID, "rs_mlp_forward: bad argument");
+  rs::launch_mlp_forward(to_box(box), d_w, n, d_x, d_out, (cudaStream_t)stream);
+  return cuda_check("rs_mlp_forward");
+}
+
+static uint16_t to_bf16(float f) {  // round to nearest even
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
+int rs_set_surrogate(rs_ctx *c, const float *d_w, const rs_mlp_box *box) {
+  if (!c) return fail(RS_E_INVALID, "rs_set_surrogate: null context");
+  if (!d_w) {
+    c->surr.w = nullptr;
+    return RS_OK;
+  }
+  if (!box_ok(box)) return fail(RS_E_INVALID, "rs_set_surrogate: bad box");
+  cudaError_t e = cudaSuccess;
+  if (!c->mlp_w) e = cudaMalloc(&c->mlp_w, sizeof(float) * rs::kMlpNParams);
+  if (e == cudaSuccess && !c->mlp_b16) e = cudaMalloc(&c->mlp_b16, sizeof(uint16_t) * rs::kSurrB16);
+  if (e == cudaSuccess && !c->mlp_audit) {
+    e = cudaMalloc(&c->mlp_audit, sizeof(unsigned long long) * 4);
+    if (e == cudaSuccess) e = cudaMemset(c->mlp_audit, 0, sizeof(unsigned long long) * 4);
+  }
+  float hw[rs::kMlpNParams];
+  if (e == cudaSuccess) e = cudaMemcpy(hw, d_w, sizeof(hw), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(RS_E_CUDA, "rs_set_surrogate: %s", cudaGetErrorString(e));
+  // BF16 copies of the tensor-core layers: W2[i][j] and W3 padded to 8 rows
+  uint16_t hb[rs::kSurrB16];
+  memset(hb, 0, sizeof(hb));
+  for (int k = 0; k < rs::kMlpH * rs::kMlpH; ++k) hb[k] = to_bf16(hw[rs::kOffW2 + k]);
+  for (int k = 0; k < 2 * rs::kMlpH; ++k) hb[rs::kMlpH * rs::kMlpH + k] = to_bf16(hw[rs::kOffW3 + k]);
+  e = cudaMemcpy(c->mlp_w, hw, sizeof(hw), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(c->mlp_b16, hb, sizeof(hb), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail(RS_E_CUDA, "rs_set_surrogate: %s", cudaGetErrorString(e));
+  rs::SurrArgs &s = c->surr;
+  s.w = c->mlp_w;
+  s.b16 = c->mlp_b16;
+  s.audit = c->mlp_audit;
+  s.T_mid = (float)(0.5 * (box->T_lo + box->T_hi));
+  s.T_ihalf = (float)(2.0 / (box->T_hi - box->T_lo));
+  s.c_mid = (float)(0.5 * (box->c_lo + box->c_hi));
+  s.c_ihalf = (float)(2.0 / (box->c_hi - box->c_lo));
+  s.T_lo = (float)box->T_lo;
+  s.T_hi = (float)box->T_hi;
+  s.c_lo = (float)box->c_lo;
+  s.c_hi = (float)box->c_hi;
+  for (int q = 0; q < 2; ++q) {
+    s.y_mean[q] = (float)box->y_mean[q];
+    s.y_scale[q] = (float)box->y_scale[q];
+  }
+  return RS_OK;
+}
+
+int rs_surrogate_audit(rs_ctx *c, double *max_err_mu, double *max_err_dG, int64_t *n_fallback, int64_t *n_audit,
+                       rs_stream_t stream) {
+  if (!c) return fail(RS_E_INVALID, "rs_surrogate_audit: null context");
+  unsigned long long h[4] = {0, 0, 0, 0};
+  cudaStream_t st = (cudaStream_t)stream;
+  if (c->mlp_audit) {
+    if (cudaMemcpyAsync(h, c->mlp_audit, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemsetAsync(c->mlp_audit, 0, sizeof(h), st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+      return fail(RS_E_CUDA, "rs_surrogate_audit: copy failed");
+  }
+  float f[2];
+  for (int q = 0; q < 2; ++q) {
+    const uint32_t u = (uint32_t)h[q];
+    memcpy(&f[q], &u, 4);
+  }
+  if (max_err_mu) *max_err_mu = f[0];
+  if (max_err_dG) *max_err_dG = f[1];
+  if (n_fallback) *n_fallback = (int64_t)h[2];
+  if (n_audit) *n_audit = (int64_t)h[3];
+  return RS_OK;
 }
 
 // Host build of the Ti-Nb evaluator (fun.cu:1671-1720) from the same

@@ -46,11 +46,13 @@ __device__ __forceinline__ void block_partial(double mass, int itip, BlockPartia
 
 // Inputs of the TMA-staged FP32 kernel: descriptors of the current psi and c
 // fields (built on the host) and the context's per-column table workspace.
+struct SurrArgs;
 struct TmaMaps {
   CUtensorMap psi;
   CUtensorMap c;
   float *col_tab;   // kColTabFields arrays of col_tab_len floats
   int col_tab_len;
+  const SurrArgs *surr;  // learned CALPHAD surrogate, or nullptr (exact)
 };
 constexpr int kTileOutW = 128;                  // output columns of an FP32 tile
 constexpr int kTmaBoxW32 = kTileOutW + 8;        // input columns (4 each side keep x 16-byte aligned)

@@ -230,14 +230,14 @@ __device__ __forceinline__ ColT<R> col_terms(const StepCoef &K, double T) {
 
 // phi update of one interface cell (compute_phi, fun.cu:1143-1218, with the
 // renormalisation of compute_psi); only warps that see an interface row run it.
+// with the driving force dG = Gl - Gs of the cell given
 template <typename R>
-__device__ __forceinline__ R phi_cell(const Coef<R> *__restrict__ Fp, R p00, R p10, R pm0, R p01, R p0m, R p11,
-                                   R pm1, R p1m, R pmm, R c00, R Anb, R Ati, int64_t step, int64_t cell,
-                                   uint32_t seed_lo, uint32_t seed_hi) {
+__device__ __forceinline__ R phi_cell_dG(const Coef<R> *__restrict__ Fp, R p00, R p10, R pm0, R p01, R p0m, R p11,
+                                      R pm1, R p1m, R pmm, R dG, int64_t step, int64_t cell, uint32_t seed_lo,
+                                      uint32_t seed_hi) {
   const Coef<R> &F = *Fp;
   R as, ak;
   const R an = anisotropy<R>(F, p00, p10, pm0, p01, p0m, p11, pm1, p1m, pmm, as, ak);
-  const R dG = (R(1) - c00) * Anb + c00 * Ati + c00 * (R(1) - c00) * R(kL0Liq - kL0Bcc);
   const R q = R(1) - p00 * p00;
   const R term = p00 - p00 * p00 * p00 + an + dG * (R(1.875) * (q * q)) * F.drive;
   R pn = p00 + Tr<R>::div(F.dt * ak, as * as) * term;
@@ -248,6 +248,14 @@ __device__ __forceinline__ R phi_cell(const Coef<R> *__restrict__ Fp, R p00, R p
     pn += F.noise_amp * q * Tr<R>::normal(x);
   }
   return pn > R(1) ? R(1) : pn;  // renormalisation (fun.cu:1252-1261)
+}
+
+template <typename R>
+__device__ __forceinline__ R phi_cell(const Coef<R> *__restrict__ Fp, R p00, R p10, R pm0, R p01, R p0m, R p11,
+                                   R pm1, R p1m, R pmm, R c00, R Anb, R Ati, int64_t step, int64_t cell,
+                                   uint32_t seed_lo, uint32_t seed_hi) {
+  const R dG = (R(1) - c00) * Anb + c00 * Ati + c00 * (R(1) - c00) * R(kL0Liq - kL0Bcc);
+  return phi_cell_dG<R>(Fp, p00, p10, pm0, p01, p0m, p11, pm1, p1m, pmm, dG, step, cell, seed_lo, seed_hi);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }

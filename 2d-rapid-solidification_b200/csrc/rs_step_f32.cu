@@ -43,6 +43,7 @@
 //     flux constant.
 // Fields store psi and delta = c - cinf (include/rs_b200.h).
 #include "rs_step_common.cuh"
+#include "rs_surrogate.cuh"
 
 namespace rs {
 namespace {
@@ -138,12 +139,15 @@ __global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef 
   tab[kTabAti * len + k] = (float)tt.A_ti;
 }
 
-__global__ void __launch_bounds__(kThreads, 5)
+// SURR: mu'' and the driving force of in-box cells come from the learned
+// surrogate (rs_surrogate.cuh) instead of the exact evaluation.
+template <bool SURR>
+__global__ void __launch_bounds__(kThreads, SURR ? 3 : 5)
     tile_kernel(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<float> F,
                 const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
                 const __grid_constant__ CUtensorMap tm_c, const float *__restrict__ tab, const int tab_len,
                 float *__restrict__ psi_n, float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *partials,
-                int *err) {
+                int *err, const __grid_constant__ SurrArgs SA) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -190,6 +194,45 @@ __global__ void __launch_bounds__(kThreads, 5)
   const float *tDK = tab + kTabDK * tab_len + 4;
   const float4 RTv = ld4(tRT + gi), C0v = ld4(tC0 + gi);
   const float RTa[4] = {RTv.x, RTv.y, RTv.z, RTv.w}, C0a[4] = {C0v.x, C0v.y, C0v.z, C0v.w};
+  // surrogate: per-lane fragments, and the scaled inputs as T(x) = TnA + TnB x
+  // (tile column x; frozen T is linear in the column) and c = cnA + delta c_ihalf
+  SurrConst SC;
+  float TnA = 0.f, TnB = 0.f, cnA = 0.f;
+  const float *tAnb = tab + kTabAnb * tab_len + 4, *tAti = tab + kTabAti * tab_len + 4;
+  if constexpr (SURR) {
+    SC = surr_load(SA, lane);
+    const double T0 = (PS.d0 + PS.d1 * x0) * K.deltaT0 + K.Tmelt;
+    TnA = (float)((T0 - SA.T_mid) * SA.T_ihalf);
+    TnB = (float)(PS.d1 * K.deltaT0 * SA.T_ihalf);
+    cnA = (F.cinf - SA.c_mid) * SA.c_ihalf;
+  }
+  auto net_inputs = [&](int rr, int b, float in[3]) {  // b: box column
+    in[0] = fmaf(TnB, (float)(b - 4), TnA);
+    in[1] = fmaf(sm.d[rr][b], SA.c_ihalf, cnA);
+    in[2] = clamp1(sm.psi[rr][b]);
+  };
+  // store the surrogate mu'' of one cell, or keep the exact value already in
+  // place (out-of-box and audited cells); audited cells record the errors
+  auto net_store = [&](int rr, int b, const float in[3], const float o[2]) {
+    const int gx = x0 + b - 4;
+    const float T = SA.T_mid + in[0] / SA.T_ihalf, c = F.cinf + sm.d[rr][b];
+    const bool inbox = T >= SA.T_lo && T <= SA.T_hi && c >= SA.c_lo && c <= SA.c_hi;
+    const bool real = gx >= 0 && gx <= K.nx - 1;
+    const bool audit = real && surr_audit_cell(PS.step, (int64_t)(y0 - 1 + rr) * K.nx + gx);
+    const float mu_net = fmaf(o[0], SA.y_scale[0], SA.y_mean[0]);
+    if (inbox && !audit) {
+      sm.mu[rr][b] = mu_net;
+    } else if (real) {
+      if (!inbox) atomicAdd(&SA.audit[2], 1ull);
+      if (audit) {
+        const float dG_ex = (1.f - c) * tAnb[gx] + c * tAti[gx] + c * (1.f - c) * (float)(kL0Liq - kL0Bcc);
+        const float dG_net = fmaf(o[1], SA.y_scale[1], SA.y_mean[1]);
+        atomicMax(&SA.audit[0], (unsigned long long)__float_as_uint(fabsf(mu_net - sm.mu[rr][b])));
+        atomicMax(&SA.audit[1], (unsigned long long)__float_as_uint(fabsf(dG_net - dG_ex)));
+        atomicAdd(&SA.audit[3], 1ull);
+      }
+    }
+  };
   __syncthreads();  // barrier initialised, flags cleared
   {
     uint32_t tries = 0;
@@ -271,10 +314,28 @@ __global__ void __launch_bounds__(kThreads, 5)
       if (code & 1u) atomicOr(&sm.liq, 1u << rr);
       if (code & 2u) atomicOr(&sm.sol, 1u << rr);
     }
+    if constexpr (SURR) {  // the row's 128 cells through the network, 16 at a time
+      __syncwarp();
+      const int g = lane >> 2;
+#pragma unroll 1
+      for (int mt = 0; mt < kW / 16; ++mt) {
+        const int ba = 4 + 16 * mt + g, bb = ba + 8;
+        float in0[3], in1[3], o0[2], o1[2];
+        net_inputs(rr, ba, in0);
+        net_inputs(rr, bb, in1);
+        surr_tile16(SC, in0, in1, o0, o1);
+        if ((lane & 3) == 0) {
+          net_store(rr, ba, in0, o0);
+          net_store(rr, bb, in1, o1);
+        }
+      }
+    }
   }
-  // halo columns x0-1 and x0+kW, one thread per cell
-  if (threadIdx.x < 2 * kTRin) {
-    const int rr = threadIdx.x >> 1, side = threadIdx.x & 1;
+  // halo columns x0-1 and x0+kW, one thread per cell (surrogate: warp 0
+  // alone, then the same network pass as the rows)
+  if (SURR ? warp == 0 : threadIdx.x < 2 * kTRin) {
+   for (int i = SURR ? lane : (int)threadIdx.x; i < 2 * kTRin; i += 32) {
+    const int rr = i >> 1, side = i & 1;
     const int x = side ? kHaloR : kHaloL, g = x0 - 4 + x;
     float Sh = 0.f, mh = 0.f;
     uint8_t hm = 3u;
@@ -286,6 +347,26 @@ __global__ void __launch_bounds__(kThreads, 5)
     sm.S[rr][x] = Sh;
     sm.mu[rr][x] = mh;
     sm.hmask[rr][side] = hm;
+    if (!SURR) break;
+   }
+   if constexpr (SURR) {
+    __syncwarp();
+    const int g = lane >> 2;
+#pragma unroll 1
+    for (int mt = 0; mt < (2 * kTRin + 15) / 16; ++mt) {
+      const int ia = 16 * mt + g, ib = ia + 8;
+      const int ra = ia < 2 * kTRin ? ia >> 1 : 0, rb = ib < 2 * kTRin ? ib >> 1 : 0;
+      const int xa = (ia & 1) ? kHaloR : kHaloL, xb = (ib & 1) ? kHaloR : kHaloL;
+      float in0[3], in1[3], o0[2], o1[2];
+      net_inputs(ra, xa, in0);
+      net_inputs(rb, xb, in1);
+      surr_tile16(SC, in0, in1, o0, o1);
+      if ((lane & 3) == 0) {
+        if (ia < 2 * kTRin && y0 - 1 + ra <= K.ny - 1) net_store(ra, xa, in0, o0);
+        if (ib < 2 * kTRin && y0 - 1 + rb <= K.ny - 1) net_store(rb, xb, in1, o1);
+      }
+    }
+   }
   }
   const float4 dKv = ld4(tDK + gi);
   const float dKl = tDK[gi - 1];
@@ -422,11 +503,22 @@ __global__ void __launch_bounds__(kThreads, 5)
     const uint32_t e = sm.list[idx];
     const int rr = (int)(e >> 8), x = (int)(e & 0xFFu) + 4;  // box column
     const int r = y0 - 1 + rr, g = x0 + x - 4;
-    const float res = phi_cell<float>(
+    const float c00 = F.cinf + sm.d[rr][x];
+    float dG = (1.f - c00) * tAnb[g] + c00 * tAti[g] + c00 * (1.f - c00) * (float)(kL0Liq - kL0Bcc);
+    if constexpr (SURR) {  // driving force from the surrogate for in-box, unaudited cells
+      float in[3], o[2];
+      net_inputs(rr, x, in);
+      const float T = SA.T_mid + in[0] / SA.T_ihalf;
+      if (T >= SA.T_lo && T <= SA.T_hi && c00 >= SA.c_lo && c00 <= SA.c_hi &&
+          !surr_audit_cell(PS.step, (int64_t)r * K.nx + g)) {
+        surr_scalar(SA, in, o);
+        dG = fmaf(o[1], SA.y_scale[1], SA.y_mean[1]);
+      }
+    }
+    const float res = phi_cell_dG<float>(
         &F, clamp1(sm.psi[rr][x]), clamp1(sm.psi[rr][x + 1]), clamp1(sm.psi[rr][x - 1]), clamp1(sm.psi[rr + 1][x]),
         clamp1(sm.psi[rr - 1][x]), clamp1(sm.psi[rr + 1][x + 1]), clamp1(sm.psi[rr + 1][x - 1]),
-        clamp1(sm.psi[rr - 1][x + 1]), clamp1(sm.psi[rr - 1][x - 1]), F.cinf + sm.d[rr][x],
-        tab[kTabAnb * tab_len + 4 + g], tab[kTabAti * tab_len + 4 + g], PS.step, (int64_t)r * K.nx + g, K.seed_lo,
+        clamp1(sm.psi[rr - 1][x + 1]), clamp1(sm.psi[rr - 1][x - 1]), dG, PS.step, (int64_t)r * K.nx + g, K.seed_lo,
         K.seed_hi);
     sm.S[rr][x] = res;
     if (red && res > 0.f) itip = max(itip, g == K.nx - 2 ? K.nx - 1 : g);
@@ -547,12 +639,15 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   if (partials && nparts > max_partials) return -1;
   if (tm.col_tab_len < (int)grid.y * kW + kWin) return -1;
   const size_t smem = sizeof(TileSmem);
-  static bool attr_done = false;
-  if (!attr_done) {
-    if (cudaFuncSetAttribute(tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return -3;
-    attr_done = true;
+  const bool surr = tm.surr != nullptr;
+  auto kfn = surr ? tile_kernel<true> : tile_kernel<false>;
+  static bool attr_done[2] = {false, false};
+  if (!attr_done[surr]) {
+    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -3;
+    attr_done[surr] = true;
   }
+  SurrArgs sa = {};
+  if (surr) sa = *tm.surr;
   column_table_kernel<<<(tm.col_tab_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(K, P.d0, P.d1, tm.col_tab_len, tm.col_tab);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
@@ -565,8 +660,8 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   cfg.attrs = at;
   cfg.numAttrs = 1;
   const float *tab = tm.col_tab;
-  if (cudaLaunchKernelEx(&cfg, tile_kernel, K, F, P, tm.psi, tm.c, tab, tm.col_tab_len, psi_n, c_n, phi_n, partials,
-                         err) != cudaSuccess)
+  if (cudaLaunchKernelEx(&cfg, kfn, K, F, P, tm.psi, tm.c, tab, tm.col_tab_len, psi_n, c_n, phi_n, partials, err,
+                         sa) != cudaSuccess)
     return -3;
   if (nparts_out) *nparts_out = nparts;
   return 0;

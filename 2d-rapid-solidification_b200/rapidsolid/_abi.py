@@ -5,7 +5,8 @@ rs_sizeof_params()/rs_sizeof_step_args() and the tests compare them.
 """
 import ctypes as C
 
-RS_ABI_VERSION = 5
+RS_ABI_VERSION = 6
+RS_MLP_NPARAMS = 1250
 RS_OPT_TMA = 1
 RS_OK = 0
 RS_E_INVALID = -1
@@ -87,3 +88,9 @@ class RunState(C.Structure):
         ("dt", C.c_double), ("dtT", C.c_double), ("length_sample", C.c_double), ("Tcold", C.c_double),
         ("Thot", C.c_double), ("gamma0", C.c_double), ("gamma1", C.c_double), ("path_input", C.c_char_p),
     ]
+
+
+class MlpBox(C.Structure):
+    """rs_mlp_box — training box and output scaling of the CALPHAD surrogate."""
+    _fields_ = [("T_lo", C.c_double), ("T_hi", C.c_double), ("c_lo", C.c_double), ("c_hi", C.c_double),
+                ("y_mean", C.c_double * 2), ("y_scale", C.c_double * 2)]

@@ -68,6 +68,12 @@ def load():
         "rs_write_check_point_temperature": ([C.c_char_p, vp, i32, i32, i32], C.c_int),
         "rs_read_check_point_temperature": ([C.c_char_p, vp, i32, i32, i32], C.c_int),
         "rs_write_field_text": ([C.c_char_p, vp, i32, i32, i32, i32], C.c_int),
+        "rs_mlp_sample": ([vp, vp, i64, C.c_uint64, vp, vp, vp], C.c_int),
+        "rs_mlp_grad": ([vp, vp, i64, vp, vp, vp, vp, vp], C.c_int),
+        "rs_mlp_adam": ([vp, vp, vp, vp, i64, C.c_float, C.c_float, vp], C.c_int),
+        "rs_mlp_forward": ([vp, vp, i64, vp, vp, vp], C.c_int),
+        "rs_set_surrogate": ([vp, vp, vp], C.c_int),
+        "rs_surrogate_audit": ([vp, vp, vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -251,6 +257,20 @@ class Context:
         fc, fn = cur.fields(), nxt.fields()
         check(self.lib.rs_integrate_phi(self._h, C.byref(fc), C.byref(fn), _ptr(dphidt), int(i_left_end),
                                         _stream(stream)))
+
+    def set_surrogate(self, w=None, box=None):
+        """Use the learned CALPHAD surrogate in the FP32 step (w: RS_MLP_NPARAMS
+        float32 device tensor, box: _abi.MlpBox); w None: exact evaluation."""
+        check(self.lib.rs_set_surrogate(self._h, None if w is None else _ptr(w),
+                                        None if box is None else C.byref(box)))
+
+    def surrogate_audit(self, stream=None):
+        """(max |mu'' error|, max |dG error|, fallback cells, audited cells) since the last call."""
+        em, eg = C.c_double(), C.c_double()
+        nf, na = C.c_int64(), C.c_int64()
+        check(self.lib.rs_surrogate_audit(self._h, C.byref(em), C.byref(eg), C.byref(nf), C.byref(na),
+                                          _stream(stream)))
+        return em.value, eg.value, nf.value, na.value
 
     def interpolate_temperature(self, T, T_fine, i_left_end, stream=None):
         check(self.lib.rs_interpolate_temperature(self._h, _ptr(T), _ptr(T_fine), int(i_left_end), _stream(stream)))

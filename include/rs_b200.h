@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define RS_ABI_VERSION 5
+#define RS_ABI_VERSION 6
 
 /* status codes */
 #define RS_OK 0
@@ -281,6 +281,45 @@ int rs_read_check_point_temperature(const char *path, double *h_T, int32_t NxT, 
 /* <field>_<k>.txt snapshot, "%g\t" per cell (save_field, fun.cu:1768-1790). */
 int rs_write_field_text(const char *path, const double *h_field, int32_t nx_all, int32_t ny_all, int32_t di,
                         int32_t dj);
+
+/* ---- learned CALPHAD surrogate (no counterpart in the reference) ----
+ * A 3 -> 32 -> 32 -> 2 SiLU network mapping (T, c, phi), scaled to [-1, 1]
+ * over a training box, to the two per-cell CALPHAD terms of the FP32 step:
+ * the chemical potential relative to the melt's column value (mu'') and the
+ * driving force Gl - Gs (fun.cu:1671-1720).  Parameters are one FP32 vector
+ * of RS_MLP_NPARAMS: W1[32][3], b1[32], W2[32][32], b2[32], W3[2][32], b3[2].
+ * Outputs are scaled: raw = y_mean + y_scale * network output. */
+#define RS_MLP_NPARAMS 1250
+typedef struct rs_mlp_box {
+  double T_lo, T_hi;       /* K */
+  double c_lo, c_hi;       /* Ti mole fraction */
+  double y_mean[2], y_scale[2];
+} rs_mlp_box;
+/* n training samples, uniform over the box (Philox keyed by seed and index):
+ * d_x[n][3] scaled inputs, d_y[n][2] exact targets (FP64 evaluator, rounded). */
+int rs_mlp_sample(const rs_params *p, const rs_mlp_box *box, int64_t n, uint64_t seed, float *d_x, float *d_y,
+                  rs_stream_t stream);
+/* Adds the gradient of sum over samples of |out - (y - y_mean)/y_scale|^2 to
+ * d_grad (not cleared) and the loss to *d_loss (double, not cleared). */
+int rs_mlp_grad(const rs_mlp_box *box, const float *d_w, int64_t n, const float *d_x, const float *d_y,
+                float *d_grad, double *d_loss, rs_stream_t stream);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) on scale * d_grad; t counts from 1. */
+int rs_mlp_adam(float *d_w, const float *d_grad, float *d_m, float *d_v, int64_t t, float lr, float scale,
+                rs_stream_t stream);
+/* FP32 forward pass: d_out[n][2] raw (unscaled) outputs. */
+int rs_mlp_forward(const rs_mlp_box *box, const float *d_w, int64_t n, const float *d_x, float *d_out,
+                   rs_stream_t stream);
+/* Selects the surrogate for the FP32 step of this context (d_w = NULL: the
+ * exact evaluation).  The context keeps a copy of the weights (BF16 for the
+ * tensor-core layer, FP32 for the others) and of the box.  Cells whose T or c
+ * lie outside the box, and one cell in 1024 per step (audit), are evaluated
+ * exactly. */
+int rs_set_surrogate(rs_ctx *ctx, const float *d_w, const rs_mlp_box *box);
+/* Largest |surrogate - exact| of mu'' and dG over the audited cells and the
+ * counts of fallback and audited cells since the last call; clears them.
+ * Synchronizes the stream. */
+int rs_surrogate_audit(rs_ctx *ctx, double *max_err_mu, double *max_err_dG, int64_t *n_fallback,
+                       int64_t *n_audit, rs_stream_t stream);
 
 /* ---- host-side helpers (no device work) ---- */
 /* CALPHAD Ti-Nb evaluator (fun.cu:1628-1720), host build of the same code

@@ -1,0 +1,100 @@
+"""The learned CALPHAD surrogate: training data, forward and backward kernels
+against the CPU restatement (oracle/pymlp.py) and the exact evaluator."""
+import numpy as np
+import pytest
+
+import pymlp
+from rapidsolid import _abi, configs, lib, surrogate
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def exact_targets(p, box, x):
+    """mu'' = mu(T, c, phi) - Glc(T, cinf) and dG = Gl - Gs from the host build
+    of the reference evaluator (fun.cu:1671-1720)."""
+    x = x.astype(np.float64)
+    T = box.T_lo + (box.T_hi - box.T_lo) * (x[:, 0] + 1.0) / 2.0
+    c = box.c_lo + (box.c_hi - box.c_lo) * (x[:, 1] + 1.0) / 2.0
+    phi = x[:, 2]
+    g = phi * (1.875 + phi * phi * (-1.25 + 0.375 * phi * phi))
+    Glc, Gsc = lib.calphad_eval(2, T, c), lib.calphad_eval(3, T, c)
+    mu = 0.5 * (1 + g) * Gsc + 0.5 * (1 - g) * Glc
+    ref = lib.calphad_eval(2, T, np.full_like(T, p.cinf))
+    return np.stack([mu - ref, lib.calphad_eval(0, T, c) - lib.calphad_eval(1, T, c)], axis=1)
+
+
+def test_samples_are_exact_targets():
+    p = configs.scale_fp32()
+    box = surrogate.default_box()
+    x, y = surrogate.sample(p, box, 4096, seed=5)
+    xh, yh = x.cpu().numpy(), y.cpu().numpy().astype(np.float64)
+    assert np.abs(xh).max() <= 1.0
+    ye = exact_targets(p, box, xh)
+    # the GPU evaluates in FP64 from the unrounded draw and stores FP32
+    assert np.abs(yh - ye).max() <= 2e-6 * np.abs(ye).max() + 1e-2
+
+
+def test_forward_and_gradient_match_numpy():
+    p = configs.scale_fp32()
+    box = surrogate.default_box()
+    x, y = surrogate.sample(p, box, 512, seed=9)
+    box.y_mean[0], box.y_mean[1], box.y_scale[0], box.y_scale[1] = 100.0, -50.0, 3000.0, 800.0
+    w = surrogate.init_weights(3)
+    w += np.random.default_rng(4).normal(0, 0.05, w.shape).astype(np.float32)  # non-zero biases
+    wt = torch.from_numpy(w).cuda()
+    out = surrogate.forward(box, wt, x).cpu().numpy()
+    o_ref, _ = pymlp.forward(w, x.cpu().numpy())
+    out_ref = o_ref * np.array(box.y_scale[:]) + np.array(box.y_mean[:])
+    assert np.abs(out - out_ref).max() <= 1e-5 * np.abs(out_ref).max()
+    g, loss = surrogate.grad(box, wt, x, y)
+    l_ref, g_ref = pymlp.loss_and_grad(w, x.cpu().numpy(), y.cpu().numpy(), box.y_mean[:], box.y_scale[:])
+    assert abs(loss.item() - l_ref) <= 1e-5 * l_ref
+    g = g.cpu().numpy().astype(np.float64)
+    assert np.linalg.norm(g - g_ref) <= 1e-5 * np.linalg.norm(g_ref)
+    # every parameter block is exercised
+    for a, b in ((0, 96), (96, 128), (128, 1152), (1152, 1184), (1184, 1248), (1248, 1250)):
+        assert np.abs(g_ref[a:b]).max() > 0
+
+
+def test_training_reduces_the_error():
+    p = configs.scale_fp32()
+    w, box, hist = surrogate.train(p, n_samples=1 << 16, epochs=6, batch=2048, lr=3e-3, seed=2)
+    assert hist[-1] < 0.2 * hist[0]
+    x, y = surrogate.sample(p, box, 8192, seed=77)
+    emax, erms = surrogate.errors(box, w, x, y)
+    # six short epochs: well below the spread of the targets, not converged
+    assert erms[0] < 0.5 * box.y_scale[0] and erms[1] < 0.5 * box.y_scale[1]
+
+
+def test_surrogate_step_runs_with_audit():
+    """The FP32 step with the surrogate in place of the exact per-cell
+    evaluation: finite fields, the audit visits one cell in 1024 per step and
+    finds no out-of-box cell on this workload, and a learned form that still
+    moves the front (its accuracy is measured, not asserted to a tolerance:
+    see the surrogate notes of the design document)."""
+    p = configs.scale_fp32()
+    p.nx_all = p.ny_all = 512
+    w, box, _ = surrogate.train(p, n_samples=1 << 18, epochs=8, batch=4096, lr=3e-3, seed=4)
+    out = {}
+    for use in (False, True):
+        ctx = lib.Context(p)
+        if use:
+            ctx.set_surrogate(w, box)
+        a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
+        ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+        for n in range(1, 301):
+            ctx.step(a, b, n)
+            a, b = b, a
+        torch.cuda.synchronize()
+        ctx.device_status()
+        out[use] = (a.psi.cpu().numpy(), a.c.cpu().numpy(), ctx.surrogate_audit() if use else None)
+    psi, c, (emu, edg, nfb, naud) = out[True]
+    assert np.isfinite(psi).all() and np.isfinite(c).all()
+    cells = (p.nx_all - 2) * (p.ny_all - 2) + 2 * 18 * 0  # audited cells are interior or halo columns
+    assert nfb == 0
+    assert 0.5 * 300 * cells / 1024 < naud < 2.0 * 300 * (p.nx_all * p.ny_all) / 1024
+    assert 0.0 < emu and 0.0 < edg
+    # the front stays where the exact run has it to within a few cells
+    ifront = lambda ps: (ps.reshape(p.ny_all, p.nx_all)[1:-1, 1:-1] > 0).sum(1).mean()
+    assert abs(ifront(psi) - ifront(out[False][0])) < 3.0
