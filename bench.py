@@ -260,12 +260,123 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, seconds=args.cpu_seconds)
+    if rank == 0 and world == 1 and not args.no_side_legs:
+        fp64 = fp64_leg(p, flush)
+        line["fp64_exact"] = fp64
+        line["fp32_exact_vs_fp64_exact"] = round(value / fp64["value"], 3)
+        line["surrogate"] = surrogate_leg(p, flush, value, fp64["value"])
     ctx.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def _timed_steps(ctx, p, d, a, b, flush, n0, nsteps):
+    """Median CUDA-event time (ms) of nsteps steps, L2 flushed between them."""
+    import torch
+    ts = []
+    for k in range(nsteps):
+        flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.step(a, b, n0 + k)
+        e1.record()
+        a, b = b, a
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ts.sort()
+    return ts[len(ts) // 2]
+
+
+def fp64_leg(p, flush, nsteps=30):
+    """The exact FP64 step (the drop-in's precision) on the same workload."""
+    import torch
+    from rapidsolid import configs, lib
+    ctx = lib.Context(p)
+    a, b = lib.FieldSet(p, torch.float64), lib.FieldSet(p, torch.float64)
+    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    for k in range(1, 6):
+        ctx.step(a, b, k)
+        a, b = b, a
+    ms = _timed_steps(ctx, p, ctx.d, a, b, flush, 6, nsteps)
+    cells = (p.nx_all - 2) * (p.ny_all - 2)
+    ctx.close()
+    return {"value": round(cells / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms, 5), "steps": nsteps,
+            "kernel": "rs::step_kernel<double, H, 3, false> (register prefetch)",
+            "note": "median of CUDA-event step times, L2 flushed"}
+
+
+def _tip_run(p, use_w, box, nsteps=20000, every=1000):
+    """The C2 loop (moving frame, tip every `every` steps): tip positions."""
+    import ctypes as C
+    import torch
+    from rapidsolid import _abi, configs, lib
+    ctx = lib.Context(p)
+    d = ctx.d
+    if use_w is not None:
+        ctx.set_surrogate(use_w, box)
+    a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
+    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    itip = torch.zeros(1, dtype=torch.int32, device="cuda")
+    tipbuf = torch.zeros(C.sizeof(_abi.Tip), dtype=torch.uint8, device="cuda")
+    hist, l, xs = 0, 0.0, []
+    for n in range(nsteps + 1):
+        if n % every == 0:
+            ctx.precise_tip(a, tipbuf)
+            t = lib.tip_from_bytes(tipbuf.cpu().numpy().tobytes())
+            xs.append((hist + t.x) * p.dx)
+            if n == nsteps:
+                break
+        pb = None
+        if n % d.step_pull_back == 0:
+            ctx.itip(a, itip)
+            pb = int(itip.item()) - p.i_tip_target
+            hist += pb
+        ctx.step(a, b, n, i_offset_history=hist, l_offset_Vp=l, pull_back=pb)
+        l += p.Vp * d.dt * d.tau0 / (p.S * p.W0)
+        a, b = b, a
+    torch.cuda.synchronize()
+    audit = ctx.surrogate_audit() if use_w is not None else None
+    ctx.close()
+    half = len(xs) // 2
+    v = (xs[-1] - xs[half]) * p.S * p.W0 / ((nsteps - half * every) * d.tau0 * d.dt)
+    return xs, v, audit
+
+
+def surrogate_leg(p, flush, fp32_value, fp64_value, nsteps=30):
+    """The FP32 step with the learned CALPHAD surrogate (trained here on the
+    GPU by the library's kernels, box fitted to the run): speed, and tip speed
+    against the exact FP32 step over the full 20000-step run."""
+    import torch
+    from rapidsolid import configs, lib, surrogate
+    t0 = time.time()
+    w, box, hist = surrogate.train(p, box=surrogate.fitted_box(), epochs=40)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    ctx = lib.Context(p)
+    ctx.set_surrogate(w, box)
+    a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
+    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    for k in range(1, 6):
+        ctx.step(a, b, k)
+        a, b = b, a
+    ms = _timed_steps(ctx, p, ctx.d, a, b, flush, 6, nsteps)
+    ctx.close()
+    cells = (p.nx_all - 2) * (p.ny_all - 2)
+    value = cells / (ms * 1e-3) / 1e9
+    x0, v0, _ = _tip_run(p, None, None)
+    x1, v1, audit = _tip_run(p, w, box)
+    return {"value": round(value, 3), "ms_per_step": round(ms, 5), "vs_fp32_exact": round(value / fp32_value, 3),
+            "vs_fp64_exact": round(value / fp64_value, 3),
+            "tip_speed_error": round(abs(v1 - v0) / v0, 5), "tip_speed_m_s": [round(v0, 6), round(v1, 6)],
+            "tip_position_max_dx": round(max(abs(u - q) for u, q in zip(x0, x1)) / p.dx, 4),
+            "box": {"T": [box.T_lo, box.T_hi], "c": [box.c_lo, box.c_hi]}, "train_s": round(t_train, 2),
+            "train_scaled_mse": hist[-1],
+            "audit": {"max_err_mu_J_mol": audit[0], "max_err_dG_J_mol": audit[1], "fallback_cells": audit[2],
+                      "audited_cells": audit[3]},
+            "note": "3->32->32->2 SiLU, BF16 mma.sync hidden layers, exact fallback out of box and 1/1024 audit"}
 
 
 def cpu_baseline(p, seconds=12.0, steps=None):
@@ -343,6 +454,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--clock-preroll", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-side-legs", action="store_true", help="skip the FP64 and surrogate legs")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
