@@ -12,7 +12,11 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <string>
+#include <vector>
+#include <algorithm>
 
+#include "rs_ensemble.cuh"
 #include "rs_mlp.cuh"
 #include "rs_surrogate.cuh"
 
@@ -707,6 +711,313 @@ int rs_surrogate_audit(rs_ctx *c, double *max_err_mu, double *max_err_dG, int64_
   if (n_fallback) *n_fallback = (int64_t)h[2];
   if (n_audit) *n_audit = (int64_t)h[3];
   return RS_OK;
+}
+
+// ---------------------------------------------------------------- ensemble
+struct rs_ens {
+  int n = 0;
+  std::vector<rs_ctx *> ctx;
+  std::vector<rs_fields> A, B;
+  std::vector<int> bound;
+  rs::EnsRun *h_runs = nullptr;  // pinned host mirror of the descriptors
+  rs::EnsRun *d_runs = nullptr;
+  int32_t *d_tblk = nullptr, *d_order[3] = {nullptr, nullptr, nullptr};
+  int ntblk = 0, ntiles = 0, choice = 0;
+  bool ready = false;
+  cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+  cudaStream_t cap = nullptr;
+  int32_t *d_itip = nullptr, *h_itip = nullptr;
+};
+
+namespace {
+
+int ens_prepare(rs_ens *e) {
+  if (e->ready) return RS_OK;
+  for (int r = 0; r < e->n; ++r)
+    if (!e->bound[r]) return fail(RS_E_STATE, "rs_ensemble: run %d has no field sets bound", r);
+  std::vector<int32_t> tblk, ord[3];
+  for (int r = 0; r < e->n; ++r) {
+    const rs::EnsRun &R = e->h_runs[r];
+    const int nb = (R.tab_len + 126) / 127;
+    for (int b = 0; b < nb; ++b) tblk.push_back((r << 16) | b);
+    for (int t = 0; t < R.ntiles; ++t) ord[0].push_back((r << 16) | t);
+  }
+  std::vector<int> by(e->n);
+  for (int r = 0; r < e->n; ++r) by[r] = r;
+  std::stable_sort(by.begin(), by.end(), [&](int a, int b) { return e->h_runs[a].ntiles > e->h_runs[b].ntiles; });
+  for (int r : by)
+    for (int t = 0; t < e->h_runs[r].ntiles; ++t) ord[1].push_back((r << 16) | t);
+  int tmax = 0;
+  for (int r = 0; r < e->n; ++r) tmax = std::max(tmax, e->h_runs[r].ntiles);
+  for (int t = 0; t < tmax; ++t)
+    for (int r = 0; r < e->n; ++r)
+      if (t < e->h_runs[r].ntiles) ord[2].push_back((r << 16) | t);
+  e->ntblk = (int)tblk.size();
+  e->ntiles = (int)ord[0].size();
+  cudaError_t c = cudaMalloc(&e->d_runs, sizeof(rs::EnsRun) * e->n);
+  if (c == cudaSuccess) c = cudaMalloc(&e->d_tblk, sizeof(int32_t) * tblk.size());
+  for (int k = 0; k < 3 && c == cudaSuccess; ++k) c = cudaMalloc(&e->d_order[k], sizeof(int32_t) * e->ntiles);
+  if (c == cudaSuccess) c = cudaMemcpy(e->d_tblk, tblk.data(), sizeof(int32_t) * tblk.size(), cudaMemcpyHostToDevice);
+  for (int k = 0; k < 3 && c == cudaSuccess; ++k)
+    c = cudaMemcpy(e->d_order[k], ord[k].data(), sizeof(int32_t) * e->ntiles, cudaMemcpyHostToDevice);
+  if (c == cudaSuccess) c = cudaMemcpy(e->d_runs, e->h_runs, sizeof(rs::EnsRun) * e->n, cudaMemcpyHostToDevice);
+  if (c == cudaSuccess) c = cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking);
+  if (c != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble: %s", cudaGetErrorString(c));
+  e->ready = true;
+  return RS_OK;
+}
+
+int ens_graph(rs_ens *e, cudaGraphExec_t *out) {
+  if (e->exec[e->choice]) {
+    *out = e->exec[e->choice];
+    return RS_OK;
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t c = cudaStreamBeginCapture(e->cap, cudaStreamCaptureModeThreadLocal);
+  if (c == cudaSuccess) {
+    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles, true, e->ctx[0]->d_err,
+                        e->cap);
+    c = cudaStreamEndCapture(e->cap, &g);
+  }
+  if (c == cudaSuccess) c = cudaGraphInstantiate(&e->exec[e->choice], g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (c != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble: graph capture: %s", cudaGetErrorString(c));
+  *out = e->exec[e->choice];
+  return RS_OK;
+}
+
+}  // namespace
+
+int rs_ensemble_create(const rs_params *params, int32_t nruns, rs_ens **out) {
+  if (!params || !out || nruns < 1 || nruns > 32767) return fail(RS_E_INVALID, "rs_ensemble_create: bad argument");
+  *out = nullptr;
+  for (int r = 0; r < nruns; ++r)
+    if (params[r].tfc || params[r].vp_ramp)
+      return fail(RS_E_UNSUPPORTED, "rs_ensemble_create: run %d: the ensemble steps frozen-temperature runs "
+                                    "without the Vp ramp", r);
+  rs_ens *e = new (std::nothrow) rs_ens;
+  if (!e) return fail(RS_E_INVALID, "rs_ensemble_create: out of host memory");
+  e->n = nruns;
+  e->ctx.assign(nruns, nullptr);
+  e->A.resize(nruns);
+  e->B.resize(nruns);
+  e->bound.assign(nruns, 0);
+  int rc = RS_OK;
+  for (int r = 0; r < nruns && rc == RS_OK; ++r) rc = rs_create(&params[r], &e->ctx[r]);
+  cudaError_t c = cudaSuccess;
+  if (rc == RS_OK) c = cudaMallocHost(&e->h_runs, sizeof(rs::EnsRun) * nruns);
+  if (rc == RS_OK && c == cudaSuccess) c = cudaMalloc(&e->d_itip, sizeof(int32_t));
+  if (rc == RS_OK && c == cudaSuccess) c = cudaMallocHost(&e->h_itip, sizeof(int32_t));
+  if (rc == RS_OK && c != cudaSuccess) rc = fail(RS_E_CUDA, "rs_ensemble_create: %s", cudaGetErrorString(c));
+  if (rc != RS_OK) {
+    const std::string msg = rs_last_error();
+    rs_ensemble_destroy(e);
+    return fail(rc, "%s", msg.c_str());
+  }
+  memset(e->h_runs, 0, sizeof(rs::EnsRun) * nruns);
+  *out = e;
+  return RS_OK;
+}
+
+int rs_ensemble_destroy(rs_ens *e) {
+  if (!e) return RS_OK;
+  for (int k = 0; k < 3; ++k)
+    if (e->exec[k]) cudaGraphExecDestroy(e->exec[k]);
+  if (e->cap) cudaStreamDestroy(e->cap);
+  cudaFree(e->d_runs);
+  cudaFree(e->d_tblk);
+  for (int k = 0; k < 3; ++k) cudaFree(e->d_order[k]);
+  cudaFree(e->d_itip);
+  cudaFreeHost(e->h_itip);
+  cudaFreeHost(e->h_runs);
+  for (rs_ctx *c : e->ctx) rs_destroy(c);
+  delete e;
+  return RS_OK;
+}
+
+int rs_ensemble_context(rs_ens *e, int32_t run, rs_ctx **ctx) {
+  if (!e || !ctx || run < 0 || run >= e->n) return fail(RS_E_INVALID, "rs_ensemble_context: bad argument");
+  *ctx = e->ctx[run];
+  return RS_OK;
+}
+
+int rs_ensemble_bind(rs_ens *e, int32_t run, const rs_fields *a, const rs_fields *b) {
+  if (!e || !a || !b || run < 0 || run >= e->n) return fail(RS_E_INVALID, "rs_ensemble_bind: bad argument");
+  if (e->ready) return fail(RS_E_STATE, "rs_ensemble_bind: the ensemble has started");
+  rs_ctx *c = e->ctx[run];
+  const rs_fields *fs[2] = {a, b};
+  rs::EnsRun &R = e->h_runs[run];
+  for (int k = 0; k < 2; ++k) {
+    const rs_fields *f = fs[k];
+    if (f->precision != RS_F32 || !f->c || !f->psi || (f->pitch && f->pitch != c->p.nx_all) ||
+        ((uintptr_t)f->c % 16) || ((uintptr_t)f->psi % 16) || (c->p.nx_all % 4))
+      return fail(RS_E_INVALID, "rs_ensemble_bind: run %d: FP32 field sets, 16-byte aligned, pitch nx_all, "
+                                "nx_all a multiple of 4", run);
+    if (!field_map(c, f->psi, RS_F32, &R.map_psi[k]) || !field_map(c, f->c, RS_F32, &R.map_c[k]))
+      return fail(RS_E_CUDA, "rs_ensemble_bind: run %d: no tensor map", run);
+    R.psi[k] = (float *)f->psi;
+    R.c[k] = (float *)f->c;
+  }
+  const rs_params &p = c->p;
+  R.K = c->K;
+  R.F = rs::make_coef<float>(c->K);
+  R.tab = c->col_tab;
+  R.tab_len = c->col_tab_len;
+  R.nrt = (p.ny_all - 2 + rs::kTileRows - 1) / rs::kTileRows;
+  R.ntiles = R.nrt * ((p.nx_all + rs::kTileOutW - 1) / rs::kTileOutW);
+  if (R.ntiles > 65535 || (R.tab_len + 126) / 127 > 65535)
+    return fail(RS_E_INVALID, "rs_ensemble_bind: run %d is too large for the ensemble", run);
+  R.active = 1;
+  R.hist = R.hist_init = p.i_offset_history_initial;
+  R.i_tip_target = p.i_tip_target;
+  R.step = 0;
+  R.l = R.l_init = p.l_offset_Vp_initial;
+  R.inc_l = p.Vp * c->d.dt * c->d.tau0 / (p.S * p.W0);
+  R.delta_initial = p.delta_initial;
+  R.d1 = p.GG * p.dx * p.S * p.W0 / c->d.deltaT0;
+  R.GG = p.GG;
+  R.S = p.S;
+  R.W0 = p.W0;
+  R.deltaT0 = c->d.deltaT0;
+  e->A[run] = *a;
+  e->B[run] = *b;
+  e->bound[run] = 1;
+  return RS_OK;
+}
+
+int rs_ensemble_steps(rs_ens *e, int64_t nsteps, rs_stream_t stream) {
+  if (!e || nsteps < 0) return fail(RS_E_INVALID, "rs_ensemble_steps: bad argument");
+  int rc = ens_prepare(e);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  bool dirty = false;  // the host mirror differs from the device copy
+  while (nsteps > 0) {
+    int64_t m = INT64_MAX;  // steps until the next pull-back of any run
+    for (int r = 0; r < e->n; ++r) {
+      const int64_t spb = e->ctx[r]->d.step_pull_back;
+      m = std::min(m, (spb - e->h_runs[r].step % spb) % spb);
+    }
+    if (m > 0) {  // no pull-back: replay the graph
+      if (dirty) {
+        if (cudaMemcpyAsync(e->d_runs, e->h_runs, sizeof(rs::EnsRun) * e->n, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess)
+          return fail(RS_E_CUDA, "rs_ensemble_steps: state upload failed");
+        dirty = false;
+      }
+      cudaGraphExec_t ex;
+      if ((rc = ens_graph(e, &ex))) return rc;
+      const int64_t k = std::min(m, nsteps);
+      for (int64_t q = 0; q < k; ++q)
+        if (cudaGraphLaunch(ex, st) != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble_steps: graph launch");
+      for (int r = 0; r < e->n; ++r)
+        for (int64_t q = 0; q < k; ++q) {
+          e->h_runs[r].step += 1;
+          e->h_runs[r].l += e->h_runs[r].inc_l;
+        }
+      nsteps -= k;
+      continue;
+    }
+    // a pull-back step (set_pull_back, fun.cu:693-742) for the runs due, the
+    // batched launch for the others
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble_steps: sync failed");
+    for (int r = 0; r < e->n; ++r) {
+      rs::EnsRun &R = e->h_runs[r];
+      R.active = 1;
+      if (R.step % e->ctx[r]->d.step_pull_back) continue;
+      const int par = (int)(R.step & 1);
+      const rs_fields &cur = par ? e->B[r] : e->A[r], &nxt = par ? e->A[r] : e->B[r];
+      if ((rc = rs_itip(e->ctx[r], &cur, e->d_itip, stream))) return rc;
+      if (cudaMemcpyAsync(e->h_itip, e->d_itip, sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess)
+        return fail(RS_E_CUDA, "rs_ensemble_steps: tip readback failed");
+      rs_step_args a;
+      memset(&a, 0, sizeof(a));
+      a.step = R.step;
+      a.pull_back = 1;
+      a.i_offset = *e->h_itip - e->ctx[r]->p.i_tip_target;
+      R.hist += a.i_offset;
+      a.i_offset_history = R.hist;
+      a.l_offset_Vp = R.l;
+      if ((rc = rs_step(e->ctx[r], &cur, &nxt, &a, stream))) return rc;
+      R.active = 0;
+      R.step += 1;
+      R.l += R.inc_l;
+    }
+    if (cudaMemcpyAsync(e->d_runs, e->h_runs, sizeof(rs::EnsRun) * e->n, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return fail(RS_E_CUDA, "rs_ensemble_steps: state upload failed");
+    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles, true,
+                        e->ctx[0]->d_err, st);
+    if ((rc = cuda_check("rs_ensemble_steps"))) return rc;
+    // the upload above reads h_runs: finish it before the mirror changes
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble_steps: sync failed");
+    for (int r = 0; r < e->n; ++r) {
+      rs::EnsRun &R = e->h_runs[r];
+      if (R.active) {
+        R.step += 1;
+        R.l += R.inc_l;
+      }
+      R.active = 1;
+    }
+    dirty = true;
+    nsteps -= 1;
+  }
+  if (dirty) {
+    if (cudaMemcpyAsync(e->d_runs, e->h_runs, sizeof(rs::EnsRun) * e->n, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return fail(RS_E_CUDA, "rs_ensemble_steps: state upload failed");
+  }
+  return RS_OK;
+}
+
+int rs_ensemble_state(rs_ens *e, int32_t run, int64_t *step, int32_t *i_offset_history, double *l_offset_Vp,
+                      int32_t *current) {
+  if (!e || run < 0 || run >= e->n) return fail(RS_E_INVALID, "rs_ensemble_state: bad argument");
+  const rs::EnsRun &R = e->h_runs[run];
+  if (step) *step = R.step;
+  if (i_offset_history) *i_offset_history = R.hist;
+  if (l_offset_Vp) *l_offset_Vp = R.l;
+  if (current) *current = (int32_t)(R.step & 1);
+  return RS_OK;
+}
+
+int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choice, rs_stream_t stream) {
+  if (!e || reps < 1) return fail(RS_E_INVALID, "rs_ensemble_autotune: bad argument");
+  int rc = ens_prepare(e);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(e->d_runs, e->h_runs, sizeof(rs::EnsRun) * e->n, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return fail(RS_E_CUDA, "rs_ensemble_autotune: state upload failed");
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  double best = 1e300;
+  int pick = 0;
+  for (int k = 0; k < 3; ++k) {
+    // without the advance kernel a launch recomputes the same step: the runs do not move
+    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->ctx[0]->d_err, st);
+    cudaEventRecord(t0, st);
+    for (int q = 0; q < reps; ++q)
+      rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->ctx[0]->d_err,
+                          st);
+    cudaEventRecord(t1, st);
+    float ms = 0.f;
+    if (cudaEventSynchronize(t1) != cudaSuccess || cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) {
+      cudaEventDestroy(t0);
+      cudaEventDestroy(t1);
+      return fail(RS_E_CUDA, "rs_ensemble_autotune: timing failed");
+    }
+    const double mean = ms / reps;
+    if (ms_out) ms_out[k] = mean;
+    if (mean < best) {
+      best = mean;
+      pick = k;
+    }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  e->choice = pick;
+  if (choice) *choice = pick;
+  return cuda_check("rs_ensemble_autotune");
 }
 
 // Host build of the Ti-Nb evaluator (fun.cu:1671-1720) from the same

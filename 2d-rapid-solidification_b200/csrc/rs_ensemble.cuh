@@ -1,0 +1,34 @@
+// rs_ensemble.cuh — per-run descriptor of the batched ensemble: everything the
+// FP32 tile kernel takes as launch arguments for one field set, plus the
+// run's step state, kept in device memory so that one launch serves every
+// run and a CUDA graph of it can be replayed step after step.
+#pragma once
+
+#include "rs_step_common.cuh"
+
+namespace rs {
+
+struct alignas(64) EnsRun {
+  CUtensorMap map_psi[2], map_c[2];  // field sets A (0) and B (1); current = step & 1
+  StepCoef K;
+  Coef<float> F;
+  float *psi[2], *c[2];
+  float *tab;  // the run's column table (rs_step_f32.cu layout)
+  int32_t tab_len;
+  int32_t nrt, ntiles;  // row tiles, tiles
+  int32_t active;       // 0: the run is stepped outside the batched launch this step
+  int32_t hist;         // i_offset_history
+  int32_t hist_init, i_tip_target;
+  int32_t pad;
+  int64_t step;
+  double l, inc_l;      // l_offset_Vp and its per-step increment
+  // frozen temperature line (get_delta, fun.cu:1610-1619), evaluated as rs_step does
+  double delta_initial, d1, GG, S, W0, deltaT0, l_init;
+};
+
+// launches of rs_step_f32.cu for the ensemble: table blocks listed by
+// (run, block of that run), tiles in `order` as run << 16 | tile of that run
+int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
+                    bool advance, int *err, cudaStream_t st);
+
+}  // namespace rs

@@ -44,6 +44,7 @@
 // Fields store psi and delta = c - cinf (include/rs_b200.h).
 #include "rs_step_common.cuh"
 #include "rs_surrogate.cuh"
+#include "rs_ensemble.cuh"
 
 namespace rs {
 namespace {
@@ -118,12 +119,10 @@ __device__ __forceinline__ void bulk_store(void *gdst, const void *ssrc, uint32_
 // groups are rounded to FP32); K + C0 of the next column comes from the
 // neighbouring thread, so blocks overlap by one column and write 127 entries.
 constexpr int kTabBlock = 128;
-__global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef K, const double d0, const double d1,
-                                                                 const int len, float *__restrict__ tab) {
-  // the tile kernel may start now; it waits for this grid before reading tab
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+__device__ __forceinline__ void table_block(const StepCoef &K, const double d0, const double d1, const int len,
+                                            float *__restrict__ tab, const int blk) {
   __shared__ double kc[kTabBlock];
-  const int k = blockIdx.x * (kTabBlock - 1) + threadIdx.x;  // table entry; column k - 4
+  const int k = blk * (kTabBlock - 1) + threadIdx.x;  // table entry; column k - 4
   const int gi = min(max(k - 4, 0), K.nx - 1);
   const double T = (d0 + d1 * gi) * K.deltaT0 + K.Tmelt;  // get_delta, fun.cu:1610-1619
   const TTerms tt = t_terms(T, K.RR, true);
@@ -139,20 +138,28 @@ __global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef 
   tab[kTabAti * len + k] = (float)tt.A_ti;
 }
 
+__global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef K, const double d0, const double d1,
+                                                                 const int len, float *__restrict__ tab) {
+  // the tile kernel may start now; it waits for this grid before reading tab
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  table_block(K, d0, d1, len, tab, blockIdx.x);
+}
+
 // SURR: mu'' and the driving force of in-box cells come from the learned
 // surrogate (rs_surrogate.cuh) instead of the exact evaluation.
+// The work of one CTA on tile (row tile tr, column tile tc) of a field set;
+// part: this tile's partial (mass, coarse tip), or nullptr.
 template <bool SURR>
-__global__ void __launch_bounds__(kThreads, SURR ? 3 : 5)
-    tile_kernel(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<float> F,
-                const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
-                const __grid_constant__ CUtensorMap tm_c, const float *__restrict__ tab, const int tab_len,
-                float *__restrict__ psi_n, float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *partials,
-                int *err, const __grid_constant__ SurrArgs SA) {
+__device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &F, const StepScalars &PS,
+                                          const CUtensorMap *tm_psi, const CUtensorMap *tm_c,
+                                          const float *__restrict__ tab, const int tab_len, float *__restrict__ psi_n,
+                                          float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *part,
+                                          int *err, const SurrArgs &SA, const int tr, const int tc) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int x0 = kW * blockIdx.y;       // first output column of the tile
-  const int y0 = 1 + kTR * blockIdx.x;  // first output row; input rows y0-1 .. y0+kTR
+  const int x0 = kW * tc;       // first output column of the tile
+  const int y0 = 1 + kTR * tr;  // first output row; input rows y0-1 .. y0+kTR
   constexpr uint32_t kTileBytes = 2u * kTRin * kWin * sizeof(float);
 
   if (smem_u32(smem_raw) & 127u) {  // TMA destinations must be 128-byte aligned
@@ -163,8 +170,8 @@ __global__ void __launch_bounds__(kThreads, SURR ? 3 : 5)
     mbar_init(&sm.full, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     mbar_expect_tx(&sm.full, kTileBytes);
-    tma_load_2d(&sm.psi[0][0], &tm_psi, &sm.full, x0 - 4, y0 - 1);
-    tma_load_2d(&sm.d[0][0], &tm_c, &sm.full, x0 - 4, y0 - 1);
+    tma_load_2d(&sm.psi[0][0], tm_psi, &sm.full, x0 - 4, y0 - 1);
+    tma_load_2d(&sm.d[0][0], tm_c, &sm.full, x0 - 4, y0 - 1);
     sm.liq = 0u;
     sm.sol = 0u;
     sm.nlist = 0;
@@ -375,7 +382,7 @@ __global__ void __launch_bounds__(kThreads, SURR ? 3 : 5)
 
   // ---- phase 2: warp w computes output rows 1 + 4w .. 4 + 4w of the tile
   const uint32_t liq = sm.liq, sol = sm.sol;
-  const bool red = partials != nullptr;
+  const bool red = part != nullptr;
   double mass = 0.0;
   int itip = 0;
   struct Row {
@@ -600,7 +607,7 @@ __global__ void __launch_bounds__(kThreads, SURR ? 3 : 5)
     }
   }
 
-  if (partials) {
+  if (part) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mass += __shfl_down_sync(FULL, mass, o);
     itip = __reduce_max_sync(FULL, itip);
@@ -619,14 +626,85 @@ __global__ void __launch_bounds__(kThreads, SURR ? 3 : 5)
         b.itip = max(b.itip, sm.part_itip[w]);
       }
       b.pad = 0;
-      partials[(int64_t)blockIdx.y * gridDim.x + blockIdx.x] = b;
+      *part = b;
     }
   }
   // shared memory stays allocated until the copies have read it
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+template <bool SURR>
+__global__ void __launch_bounds__(kThreads, SURR ? 3 : 5)
+    tile_kernel(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<float> F,
+                const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
+                const __grid_constant__ CUtensorMap tm_c, const float *__restrict__ tab, const int tab_len,
+                float *__restrict__ psi_n, float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *partials,
+                int *err, const __grid_constant__ SurrArgs SA) {
+  tile_body<SURR>(K, F, PS, &tm_psi, &tm_c, tab, tab_len, psi_n, c_n, phi_n,
+                  partials ? partials + ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) : nullptr, err, SA, blockIdx.x,
+                  blockIdx.y);
+}
+
+// ---------------------------------------------------------------- ensemble
+// d0 of the frozen temperature line, evaluated in the order rs_step uses on
+// the host (no contraction), so an ensemble run matches the same run stepped
+// alone bit for bit
+__device__ __forceinline__ double ens_d0(const EnsRun &R) {
+  double t = __dmul_rn(R.GG, __dsub_rn(R.l, R.l_init));
+  t = __dmul_rn(t, R.S);
+  t = __dmul_rn(t, R.W0);
+  t = __ddiv_rn(t, R.deltaT0);
+  const double k = (double)(-R.i_tip_target + R.hist - R.hist_init);
+  return __dsub_rn(__dadd_rn(R.delta_initial, __dmul_rn(R.d1, k)), t);
+}
+
+__global__ void __launch_bounds__(kTabBlock) ens_table_kernel(const EnsRun *__restrict__ runs,
+                                                              const int32_t *__restrict__ tblk) {
+  const int32_t e = tblk[blockIdx.x];
+  const EnsRun &R = runs[e >> 16];
+  if (!R.active) return;
+  table_block(R.K, ens_d0(R), R.d1, R.tab_len, R.tab, e & 0xFFFF);
+}
+
+__global__ void __launch_bounds__(kThreads, 5) ens_tile_kernel(const EnsRun *__restrict__ runs,
+                                                              const int32_t *__restrict__ order, int *err) {
+  const int32_t e = order[blockIdx.x];
+  const EnsRun &R = runs[e >> 16];
+  if (!R.active) return;
+  const int t = e & 0xFFFF, par = (int)(R.step & 1);
+  StepScalars PS;
+  memset(&PS, 0, sizeof(PS));
+  PS.step = R.step;
+  PS.d0 = ens_d0(R);
+  PS.d1 = R.d1;
+  const SurrArgs none = {};
+  tile_body<false>(R.K, R.F, PS, &R.map_psi[par], &R.map_c[par], R.tab, R.tab_len, R.psi[par ^ 1], R.c[par ^ 1],
+                   nullptr, nullptr, err, none, t % R.nrt, t / R.nrt);
+}
+
+__global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nruns || !runs[r].active) return;
+  runs[r].step += 1;
+  runs[r].l += runs[r].inc_l;
+}
+
 }  // namespace
+
+int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
+                    bool advance, int *err, cudaStream_t st) {
+  const size_t smem = sizeof(TileSmem);
+  static bool attr_done = false;
+  if (!attr_done) {
+    if (cudaFuncSetAttribute(ens_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return -3;
+    attr_done = true;
+  }
+  ens_table_kernel<<<ntblk, kTabBlock, 0, st>>>(runs, tblk);
+  ens_tile_kernel<<<ntiles, kThreads, smem, st>>>(runs, order, err);
+  if (advance) ens_advance_kernel<<<(nruns + 63) / 64, 64, 0, st>>>(const_cast<EnsRun *>(runs), nruns);
+  return 0;
+}
 
 int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScalars &P, const TmaMaps &tm,
                         float *psi_n, float *c_n, float *phi_n, BlockPartial *partials, int max_partials,

@@ -5,7 +5,7 @@ rs_sizeof_params()/rs_sizeof_step_args() and the tests compare them.
 """
 import ctypes as C
 
-RS_ABI_VERSION = 6
+RS_ABI_VERSION = 7
 RS_MLP_NPARAMS = 1250
 RS_OPT_TMA = 1
 RS_OK = 0

@@ -90,3 +90,89 @@ def small(n_i, n_j, lib=None, **kw):
 
 IC_SEED = 7
 STEPS = {"plain_small": 500, "scale_fp32": 20000}
+
+
+def _tangent(T, cl, cs, iters=12):
+    """Common tangent of the liquid and solid Gibbs energies at T (host build of
+    the reference evaluator, fun.cu:1671-1720): equal chemical potential
+    (Glc = Gsc) and equal intercepts (G - c dG/dc).  Returns (c_liquid, c_solid)."""
+    import numpy as np
+    from . import lib
+
+    def f(a, b):
+        ga = lib.calphad_eval(0, [T], [a])[0] - a * lib.calphad_eval(2, [T], [a])[0]
+        gb = lib.calphad_eval(1, [T], [b])[0] - b * lib.calphad_eval(3, [T], [b])[0]
+        return np.array([lib.calphad_eval(2, [T], [a])[0] - lib.calphad_eval(3, [T], [b])[0], ga - gb])
+    for _ in range(iters):
+        r = f(cl, cs)
+        h = 1e-7
+        J = np.column_stack([(f(cl + h, cs) - r) / h, (f(cl, cs + h) - r) / h])
+        dl, ds = np.linalg.solve(J, r)
+        cl, cs = cl - dl, cs - ds
+    return cl, cs
+
+
+def phase_boundaries(c0):
+    """(T_liquidus, c_solid at T_liquidus, T_solidus) of the melt c_Ti = c0: the
+    tangent compositions are followed up in T from the Ti melting point in
+    2 K steps (warm-started Newton) to bracket the crossings, then bisected."""
+    import math
+
+    # start from the known Ti-10Nb tangent and walk in T both ways (higher T:
+    # both tangent compositions drop; the lens closes at the Ti melting point)
+    pts = [(T_LIQUIDUS_TI10NB, C_LIQUID_TI10NB, C_SOLID_AT_TLIQ)]
+    for step in (1.0, -1.0):
+        T, cl, cs = pts[0]
+        for _ in range(800):
+            T += step
+            if T <= 1941.5:
+                break
+            cl, cs = _tangent(T, cl, cs, iters=6)
+            if not (math.isfinite(cl) and math.isfinite(cs)) or not (0.0 < cs < cl < 1.0):
+                break
+            pts.append((T, cl, cs))
+            if (step > 0 and cl < c0 and cs < c0) or (step < 0 and cl > c0 and cs > c0):
+                break
+    pts.sort()
+
+    def bisect(which):
+        for (Ta, la, sa), (Tb, lb, sb) in zip(pts, pts[1:]):
+            fa, fb = (la if which == 0 else sa) - c0, (lb if which == 0 else sb) - c0
+            if fa >= 0 > fb:
+                cl, cs = la, sa
+                for _ in range(50):
+                    Tm = 0.5 * (Ta + Tb)
+                    cl, cs = _tangent(Tm, cl, cs, iters=8)
+                    fm = (cl if which == 0 else cs) - c0
+                    if fm >= 0:
+                        Ta = Tm
+                    else:
+                        Tb = Tm
+                return 0.5 * (Ta + Tb), cl, cs
+        raise ValueError(f"no phase boundary found for c0 = {c0}")
+    T_liq, _, cs_liq = bisect(0)
+    T_sol, _, _ = bisect(1)
+    return T_liq, cs_liq, T_sol
+
+
+def ensemble(n=64, seed=2024, lib=None):
+    """The batched-ensemble workload: n Ti-Nb runs, sizes drawn between 256x256
+    and 1024x2048 (multiples of 4), V log-uniform in [0.01, 2] m/s, G
+    log-uniform in [1e5, 1e7] K/m, x_Nb of the melt uniform in [0.05, 0.20];
+    each front starts at its solidus (as the scale workload).  Returns a list
+    of (params, c_liquid, c_solid) for rs_initial_planar."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    runs = []
+    for k in range(n):
+        nx = int(rng.integers(64, 257)) * 4
+        ny = int(rng.integers(64, 513)) * 4
+        V = float(np.exp(rng.uniform(np.log(0.01), np.log(2.0))))
+        G = float(np.exp(rng.uniform(np.log(1e5), np.log(1e7))))
+        c0 = 1.0 - float(rng.uniform(0.05, 0.20))
+        T_liq, cs, T_sol = phase_boundaries(c0)
+        p = _ti10nb(default_params(lib), nx, ny, G, V, T0=T_sol)
+        p.cinf = c0
+        p.seed = seed + k
+        runs.append((p, c0, cs))
+    return runs

@@ -73,6 +73,13 @@ def load():
         "rs_mlp_adam": ([vp, vp, vp, vp, i64, C.c_float, C.c_float, vp], C.c_int),
         "rs_mlp_forward": ([vp, vp, i64, vp, vp, vp], C.c_int),
         "rs_set_surrogate": ([vp, vp, vp], C.c_int),
+        "rs_ensemble_create": ([vp, i32, C.POINTER(vp)], C.c_int),
+        "rs_ensemble_destroy": ([vp], C.c_int),
+        "rs_ensemble_context": ([vp, i32, C.POINTER(vp)], C.c_int),
+        "rs_ensemble_bind": ([vp, i32, vp, vp], C.c_int),
+        "rs_ensemble_steps": ([vp, i64, vp], C.c_int),
+        "rs_ensemble_state": ([vp, i32, vp, vp, vp, vp], C.c_int),
+        "rs_ensemble_autotune": ([vp, i32, vp, vp, vp], C.c_int),
         "rs_surrogate_audit": ([vp, vp, vp, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -171,20 +178,25 @@ class FieldSet:
 
 
 class Context:
-    """One simulation context (rs_create); owns small device workspaces."""
+    """One simulation context (rs_create); owns small device workspaces.
+    With handle, wraps a context owned elsewhere (an ensemble run)."""
 
-    def __init__(self, p):
+    def __init__(self, p, handle=None):
         self.lib = load()
         self.p = p
+        self._owned = handle is None
         self._h = C.c_void_p()
-        check(self.lib.rs_create(C.byref(p), C.byref(self._h)))
+        if handle is None:
+            check(self.lib.rs_create(C.byref(p), C.byref(self._h)))
+        else:
+            self._h = handle
         self.d = _abi.Derived()
         check(self.lib.rs_get_derived(self._h, C.byref(self.d)))
 
     def close(self):
-        if self._h:
+        if self._h and self._owned:
             self.lib.rs_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -281,3 +293,56 @@ def tip_from_bytes(buf):
     t = _abi.Tip()
     C.memmove(C.byref(t), bytes(buf), C.sizeof(_abi.Tip))
     return t
+
+
+class Ensemble:
+    """Batched ensemble of FP32 runs (rs_ensemble_*): one launch steps all runs,
+    pull-back-free stretches replay a CUDA graph.  runs: list of _abi.Params."""
+
+    def __init__(self, runs):
+        self.lib = load()
+        self.params = list(runs)
+        arr = (_abi.Params * len(runs))(*runs)
+        self._h = C.c_void_p()
+        check(self.lib.rs_ensemble_create(arr, len(runs), C.byref(self._h)))
+        self.ctx = []
+        for r, p in enumerate(self.params):
+            h = C.c_void_p()
+            check(self.lib.rs_ensemble_context(self._h, r, C.byref(h)))
+            self.ctx.append(Context(p, handle=h))
+        self.sets = [None] * len(runs)
+
+    def bind(self, run, a, b):
+        fa, fb = a.fields(), b.fields()
+        check(self.lib.rs_ensemble_bind(self._h, run, C.byref(fa), C.byref(fb)))
+        self.sets[run] = (a, b)
+
+    def steps(self, n, stream=None):
+        check(self.lib.rs_ensemble_steps(self._h, n, _stream(stream)))
+
+    def state(self, run):
+        """(step, i_offset_history, l_offset_Vp, current field set)."""
+        st, h, l, cur = C.c_int64(), C.c_int32(), C.c_double(), C.c_int32()
+        check(self.lib.rs_ensemble_state(self._h, run, C.byref(st), C.byref(h), C.byref(l), C.byref(cur)))
+        return st.value, h.value, l.value, self.sets[run][cur.value]
+
+    def autotune(self, reps=5, stream=None):
+        """(choice, [mean ms of the three tile orders])."""
+        ms = (C.c_double * 3)()
+        ch = C.c_int32()
+        check(self.lib.rs_ensemble_autotune(self._h, reps, ms, C.byref(ch), _stream(stream)))
+        return ch.value, list(ms)
+
+    def close(self):
+        for c in self.ctx:
+            c.close()
+        self.ctx = []
+        if self._h:
+            self.lib.rs_ensemble_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define RS_ABI_VERSION 6
+#define RS_ABI_VERSION 7
 
 /* status codes */
 #define RS_OK 0
@@ -320,6 +320,34 @@ int rs_set_surrogate(rs_ctx *ctx, const float *d_w, const rs_mlp_box *box);
  * Synchronizes the stream. */
 int rs_surrogate_audit(rs_ctx *ctx, double *max_err_mu, double *max_err_dG, int64_t *n_fallback,
                        int64_t *n_audit, rs_stream_t stream);
+
+/* ---- batched ensemble (no counterpart in the reference) ----
+ * Many independent FP32 runs of uneven size stepped by one launch of the tile
+ * kernel over all their tiles (plus one launch for their column tables).
+ * Each run has its own context (parameters, frozen temperature, moving frame)
+ * and two caller-owned FP32 field sets A and B; A holds the fields at even
+ * steps.  Step state lives on the device, so stretches of steps in which no
+ * run pulls back are replayed from a CUDA graph; a run's pull-back step
+ * (every step_pull_back of its own) is taken by rs_itip + rs_step on its
+ * context, as main.cu does.  Runs must use the frozen temperature without
+ * the Vp ramp. */
+typedef struct rs_ens rs_ens;
+int rs_ensemble_create(const rs_params *params, int32_t nruns, rs_ens **out);
+int rs_ensemble_destroy(rs_ens *e);
+/* the context of a run (initial conditions, mass, tip, ... of its fields) */
+int rs_ensemble_context(rs_ens *e, int32_t run, rs_ctx **ctx);
+/* the run's two field sets (FP32, 16-byte aligned, pitch nx_all) */
+int rs_ensemble_bind(rs_ens *e, int32_t run, const rs_fields *a, const rs_fields *b);
+/* nsteps steps of every run; returns after queueing them on the stream
+ * (pull-back steps read one int back) */
+int rs_ensemble_steps(rs_ens *e, int64_t nsteps, rs_stream_t stream);
+/* a run's step, i_offset_history, l_offset_Vp and current set (0 = A, 1 = B) */
+int rs_ensemble_state(rs_ens *e, int32_t run, int64_t *step, int32_t *i_offset_history, double *l_offset_Vp,
+                      int32_t *current);
+/* Times the tile orders (0 run by run, 1 largest runs first, 2 runs
+ * interleaved) over reps launches without advancing the runs, keeps the
+ * fastest; ms_out[3] receives the mean launch times. */
+int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choice, rs_stream_t stream);
 
 /* ---- host-side helpers (no device work) ---- */
 /* CALPHAD Ti-Nb evaluator (fun.cu:1628-1720), host build of the same code

@@ -1,0 +1,66 @@
+"""Batched ensemble (rs_ensemble_*): runs of uneven size stepped by one
+launch, pull-back-free stretches replayed from a CUDA graph, must equal the
+same runs stepped one by one through rs_step, bit for bit."""
+import numpy as np
+import pytest
+
+from rapidsolid import configs, lib
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+# (nx_all, ny_all, V m/s, G K/m): different pull-back cadences and sizes
+RUNS = [(256, 200, 2.0, 5e6), (384, 136, 1.5, 2e6), (200, 300, 0.9, 8e6), (132, 132, 0.5, 1e6), (516, 72, 0.3, 3e6)]
+STEPS = 600
+
+
+def params():
+    out = []
+    for k, (nx, ny, V, G) in enumerate(RUNS):
+        p = configs._ti10nb(configs.default_params(), nx, ny, G, V, T0=configs.T_SOLIDUS_TI10NB)
+        p.noise_amplitude, p.seed = 0.01, 100 + k
+        out.append(p)
+    return out
+
+
+def single(p):
+    ctx = lib.Context(p)
+    d = ctx.d
+    a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
+    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, 7)
+    itip = torch.zeros(1, dtype=torch.int32, device="cuda")
+    hist, l = 0, 0.0
+    for n in range(STEPS):
+        pb = None
+        if n % d.step_pull_back == 0:
+            ctx.itip(a, itip)
+            pb = int(itip.item()) - p.i_tip_target
+            hist += pb
+        ctx.step(a, b, n, i_offset_history=hist, l_offset_Vp=l, pull_back=pb)
+        l += p.Vp * d.dt * d.tau0 / (p.S * p.W0)
+        a, b = b, a
+    torch.cuda.synchronize()
+    return a.psi.cpu().numpy(), a.c.cpu().numpy(), hist, l
+
+
+def test_ensemble_equals_single_runs():
+    ps = params()
+    ens = lib.Ensemble(ps)
+    for r, p in enumerate(ps):
+        a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
+        ens.ctx[r].initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, 7)
+        ens.bind(r, a, b)
+    choice, ms = ens.autotune(reps=3)
+    assert choice in (0, 1, 2) and all(m > 0 for m in ms)
+    ens.steps(250)
+    ens.steps(STEPS - 250)
+    torch.cuda.synchronize()
+    assert any(ps[r].Vp >= 1.0 for r in range(len(ps)))  # some run pulls back inside the stretch
+    for r, p in enumerate(ps):
+        step, hist, l, cur = ens.state(r)
+        assert step == STEPS
+        psi, c, hist1, l1 = single(p)
+        assert hist == hist1 and l == l1
+        assert np.array_equal(cur.psi.cpu().numpy(), psi), r
+        assert np.array_equal(cur.c.cpu().numpy(), c), r
+    ens.close()
