@@ -265,6 +265,7 @@ def run_ours(args):
         line["fp64_exact"] = fp64
         line["fp32_exact_vs_fp64_exact"] = round(value / fp64["value"], 3)
         line["surrogate"] = surrogate_leg(p, flush, value, fp64["value"])
+        line["ensemble"] = ensemble_leg(flush)
     ctx.close()
     if dist:
         dist.barrier()
@@ -377,6 +378,54 @@ def surrogate_leg(p, flush, fp32_value, fp64_value, nsteps=30):
             "audit": {"max_err_mu_J_mol": audit[0], "max_err_dG_J_mol": audit[1], "fallback_cells": audit[2],
                       "audited_cells": audit[3]},
             "note": "3->32->32->2 SiLU, BF16 mma.sync hidden layers, exact fallback out of box and 1/1024 audit"}
+
+
+def ensemble_leg(flush, nruns=64, nsteps=100):
+    """The batched ensemble of uneven runs (64 Ti-Nb runs, sizes 256^2 ..
+    1024x2048, V 0.01-2 m/s, G 1e5-1e7 K/m, x_Nb 0.05-0.20, seeded): aggregate
+    Gcell-steps/s of the one-launch, graph-replayed step, against the same runs
+    stepped one rs_step at a time."""
+    import torch
+    from rapidsolid import configs, lib
+    runs = configs.ensemble(nruns)
+    ps = [p for p, _, _ in runs]
+    cells = sum((p.nx_all - 2) * (p.ny_all - 2) for p in ps)
+    ens = lib.Ensemble(ps)
+    for r, (p, cl, cs) in enumerate(runs):
+        a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
+        ens.ctx[r].initial_planar(a, cl, cs, 7 + r)
+        ens.bind(r, a, b)
+    choice, tune_ms = ens.autotune(reps=5)
+    ens.steps(3)  # step 0 pulls every run back (eager), then graph replays
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.fill_(1.0)
+    e0.record()
+    ens.steps(nsteps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    # the same runs one by one (two launches per run and step)
+    ctxs = [ens.ctx[r] for r in range(nruns)]
+    cur = [ens.state(r)[3] for r in range(nruns)]
+    nxt = [ens.sets[r][0] if cur[r] is ens.sets[r][1] else ens.sets[r][1] for r in range(nruns)]
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for k in range(10):
+        for r in range(nruns):
+            ctxs[r].step(cur[r], nxt[r], 1)
+    s1.record()
+    torch.cuda.synchronize()
+    ms_single = s0.elapsed_time(s1) / 10
+    ens.close()
+    return {"value": round(cells * nsteps / (ms * 1e-3) / 1e9, 3), "runs": nruns, "cells": cells,
+            "ms_per_step": round(ms / nsteps, 5), "steps": nsteps,
+            "one_by_one": {"value": round(cells / (ms_single * 1e-3) / 1e9, 3), "ms_per_step": round(ms_single, 5)},
+            "autotune": {"choice": ["run by run", "largest first", "interleaved"][choice],
+                         "ms_per_launch": [round(x, 5) for x in tune_ms]},
+            "note": "FP32 exact path (the surrogate is slower and less accurate, see its leg); CUDA graph "
+                    "replays between pull-backs; every run equals its single run bit for bit (tests)"}
 
 
 def cpu_baseline(p, seconds=12.0, steps=None):
