@@ -68,7 +68,7 @@ struct rs_ctx {
   int col_tab_len;
   rs::SurrArgs surr;   // learned CALPHAD surrogate of the FP32 step (surr.w == nullptr: exact)
   float *mlp_w;        // its FP32 parameters (device)
-  uint16_t *mlp_b16;   // BF16 W2 (32 x 32) and W3 padded to 8 rows (device)
+  uint16_t *mlp_b16;   // FP16 W2 (32 x 32) and W3 padded to 8 rows (device)
   unsigned long long *mlp_audit;  // max error bits of mu'' and dG, fallback and audit counts
   int use_tma;         // RS_OPT_TMA
   TmaEntry tma[8];     // tensor-map cache keyed by field pointer
@@ -639,12 +639,8 @@ int rs_mlp_forward(const rs_mlp_box *box, const float *d_w, int64_t n, const flo
   return cuda_check("rs_mlp_forward");
 }
 
-static uint16_t to_bf16(float f) {  // round to nearest even
-  uint32_t u;
-  memcpy(&u, &f, 4);
-  if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
-  u += 0x7fffu + ((u >> 16) & 1u);
-  return (uint16_t)(u >> 16);
+static uint16_t to_f16(float f) {  // round to nearest even
+  return __half_as_ushort(__float2half_rn(f));
 }
 
 int rs_set_surrogate(rs_ctx *c, const float *d_w, const rs_mlp_box *box) {
@@ -664,11 +660,11 @@ int rs_set_surrogate(rs_ctx *c, const float *d_w, const rs_mlp_box *box) {
   float hw[rs::kMlpNParams];
   if (e == cudaSuccess) e = cudaMemcpy(hw, d_w, sizeof(hw), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail(RS_E_CUDA, "rs_set_surrogate: %s", cudaGetErrorString(e));
-  // BF16 copies of the tensor-core layers: W2[i][j] and W3 padded to 8 rows
+  // FP16 copies of the tensor-core layers: W2[i][j] and W3 padded to 8 rows
   uint16_t hb[rs::kSurrB16];
   memset(hb, 0, sizeof(hb));
-  for (int k = 0; k < rs::kMlpH * rs::kMlpH; ++k) hb[k] = to_bf16(hw[rs::kOffW2 + k]);
-  for (int k = 0; k < 2 * rs::kMlpH; ++k) hb[rs::kMlpH * rs::kMlpH + k] = to_bf16(hw[rs::kOffW3 + k]);
+  for (int k = 0; k < rs::kMlpH * rs::kMlpH; ++k) hb[k] = to_f16(hw[rs::kOffW2 + k]);
+  for (int k = 0; k < 2 * rs::kMlpH; ++k) hb[rs::kMlpH * rs::kMlpH + k] = to_f16(hw[rs::kOffW3 + k]);
   e = cudaMemcpy(c->mlp_w, hw, sizeof(hw), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(c->mlp_b16, hb, sizeof(hb), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail(RS_E_CUDA, "rs_set_surrogate: %s", cudaGetErrorString(e));

@@ -145,8 +145,10 @@ __global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef 
   table_block(K, d0, d1, len, tab, blockIdx.x);
 }
 
-// SURR: mu'' and the driving force of in-box cells come from the learned
-// surrogate (rs_surrogate.cuh) instead of the exact evaluation.
+// SURR: mu'' and the driving force of in-box cells that are not bulk melt
+// come from the learned surrogate (rs_surrogate.cuh) instead of the exact
+// evaluation.  Bulk-melt cells (psi == -1 exactly, delta in the series range)
+// keep the exact series form: it is exact and cheaper than the network.
 // The work of one CTA on tile (row tile tr, column tile tc) of a field set;
 // part: this tile's partial (mass, coarse tip), or nullptr.
 template <bool SURR>
@@ -203,16 +205,19 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   const float RTa[4] = {RTv.x, RTv.y, RTv.z, RTv.w}, C0a[4] = {C0v.x, C0v.y, C0v.z, C0v.w};
   // surrogate: per-lane fragments, and the scaled inputs as T(x) = TnA + TnB x
   // (tile column x; frozen T is linear in the column) and c = cnA + delta c_ihalf
-  SurrConst SC;
   float TnA = 0.f, TnB = 0.f, cnA = 0.f;
   const float *tAnb = tab + kTabAnb * tab_len + 4, *tAti = tab + kTabAti * tab_len + 4;
   if constexpr (SURR) {
-    SC = surr_load(SA, lane);
     const double T0 = (PS.d0 + PS.d1 * x0) * K.deltaT0 + K.Tmelt;
     TnA = (float)((T0 - SA.T_mid) * SA.T_ihalf);
     TnB = (float)(PS.d1 * K.deltaT0 * SA.T_ihalf);
     cnA = (F.cinf - SA.c_mid) * SA.c_ihalf;
   }
+  // a cell the series form covers (the network is not used there)
+  auto melt_cell = [&](int rr, int b) {
+    const float dv = sm.d[rr][b];
+    return __float_as_uint(sm.psi[rr][b]) == kMinus1 && dv < d_hi && dv > d_lo;
+  };
   auto net_inputs = [&](int rr, int b, float in[3]) {  // b: box column
     in[0] = fmaf(TnB, (float)(b - 4), TnA);
     in[1] = fmaf(sm.d[rr][b], SA.c_ihalf, cnA);
@@ -289,7 +294,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const bool liq4 = band == kMinus1 && bor == kMinus1;
     uint32_t code;
     if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
-      code = 1u;
+      code = 1u | 4u;  // 4: every cell in the series form
       sm.pmask[rr][lane] = 0x0Fu;
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -321,19 +326,24 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       if (code & 1u) atomicOr(&sm.liq, 1u << rr);
       if (code & 2u) atomicOr(&sm.sol, 1u << rr);
     }
-    if constexpr (SURR) {  // the row's 128 cells through the network, 16 at a time
-      __syncwarp();
-      const int g = lane >> 2;
+    if constexpr (SURR) {  // the row's non-melt cells through the network, 16 at a time
+      if (!(code & 4u)) {
+        __syncwarp();
+        const SurrConst SC = surr_load(SA, lane);
+        const int g = lane >> 2;
 #pragma unroll 1
-      for (int mt = 0; mt < kW / 16; ++mt) {
-        const int ba = 4 + 16 * mt + g, bb = ba + 8;
-        float in0[3], in1[3], o0[2], o1[2];
-        net_inputs(rr, ba, in0);
-        net_inputs(rr, bb, in1);
-        surr_tile16(SC, in0, in1, o0, o1);
-        if ((lane & 3) == 0) {
-          net_store(rr, ba, in0, o0);
-          net_store(rr, bb, in1, o1);
+        for (int mt = 0; mt < kW / 16; ++mt) {
+          const int ba = 4 + 16 * mt + g, bb = ba + 8;
+          const bool na = !melt_cell(rr, ba), nb = !melt_cell(rr, bb);
+          if (!__any_sync(FULL, na || nb)) continue;
+          float in0[3], in1[3], o0[2], o1[2];
+          net_inputs(rr, ba, in0);
+          net_inputs(rr, bb, in1);
+          surr_tile16(SC, in0, in1, o0, o1);
+          if ((lane & 3) == 0) {
+            if (na) net_store(rr, ba, in0, o0);
+            if (nb) net_store(rr, bb, in1, o1);
+          }
         }
       }
     }
@@ -365,13 +375,17 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       const int ia = 16 * mt + g, ib = ia + 8;
       const int ra = ia < 2 * kTRin ? ia >> 1 : 0, rb = ib < 2 * kTRin ? ib >> 1 : 0;
       const int xa = (ia & 1) ? kHaloR : kHaloL, xb = (ib & 1) ? kHaloR : kHaloL;
+      const bool na = ia < 2 * kTRin && y0 - 1 + ra <= K.ny - 1 && !melt_cell(ra, xa);
+      const bool nb = ib < 2 * kTRin && y0 - 1 + rb <= K.ny - 1 && !melt_cell(rb, xb);
+      if (!__any_sync(FULL, na || nb)) continue;
+      const SurrConst SC = surr_load(SA, lane);
       float in0[3], in1[3], o0[2], o1[2];
       net_inputs(ra, xa, in0);
       net_inputs(rb, xb, in1);
       surr_tile16(SC, in0, in1, o0, o1);
       if ((lane & 3) == 0) {
-        if (ia < 2 * kTRin && y0 - 1 + ra <= K.ny - 1) net_store(ra, xa, in0, o0);
-        if (ib < 2 * kTRin && y0 - 1 + rb <= K.ny - 1) net_store(rb, xb, in1, o1);
+        if (na) net_store(ra, xa, in0, o0);
+        if (nb) net_store(rb, xb, in1, o1);
       }
     }
    }
@@ -507,6 +521,30 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
 
   // ---- phase 3: interface cells, one per thread (compute_phi, fun.cu:1143-1218)
   const int nlist = sm.nlist;
+  if constexpr (SURR) {
+    // network driving force of the listed cells, 16 per warp pass, into the
+    // mu'' slots of those cells (mu'' is not read after phase 2)
+    if (nlist > 16 * warp) {
+      const SurrConst SC = surr_load(SA, lane);
+      const int g = lane >> 2;
+#pragma unroll 1
+      for (int base = 16 * warp; base < nlist; base += 16 * kWarps) {
+        const int ia = base + g, ib = ia + 8;
+        const uint32_t ea = sm.list[min(ia, nlist - 1)], eb = sm.list[min(ib, nlist - 1)];
+        const int ra = (int)(ea >> 8), xa = (int)(ea & 0xFFu) + 4, rb = (int)(eb >> 8), xb = (int)(eb & 0xFFu) + 4;
+        float in0[3], in1[3], o0[2], o1[2];
+        net_inputs(ra, xa, in0);
+        net_inputs(rb, xb, in1);
+        surr_tile16(SC, in0, in1, o0, o1);
+        __syncwarp();  // every lane has read its inputs before any slot is overwritten
+        if ((lane & 3) == 0) {
+          if (ia < nlist) sm.mu[ra][xa] = fmaf(o0[1], SA.y_scale[1], SA.y_mean[1]);
+          if (ib < nlist) sm.mu[rb][xb] = fmaf(o1[1], SA.y_scale[1], SA.y_mean[1]);
+        }
+      }
+    }
+    __syncthreads();
+  }
   for (int idx = threadIdx.x; idx < nlist; idx += kThreads) {
     const uint32_t e = sm.list[idx];
     const int rr = (int)(e >> 8), x = (int)(e & 0xFFu) + 4;  // box column
@@ -514,14 +552,12 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const float c00 = F.cinf + sm.d[rr][x];
     float dG = (1.f - c00) * tAnb[g] + c00 * tAti[g] + c00 * (1.f - c00) * (float)(kL0Liq - kL0Bcc);
     if constexpr (SURR) {  // driving force from the surrogate for in-box, unaudited cells
-      float in[3], o[2];
+      float in[3];
       net_inputs(rr, x, in);
       const float T = SA.T_mid + in[0] / SA.T_ihalf;
       if (T >= SA.T_lo && T <= SA.T_hi && c00 >= SA.c_lo && c00 <= SA.c_hi &&
-          !surr_audit_cell(PS.step, (int64_t)r * K.nx + g)) {
-        surr_scalar(SA, in, o);
-        dG = fmaf(o[1], SA.y_scale[1], SA.y_mean[1]);
-      }
+          !surr_audit_cell(PS.step, (int64_t)r * K.nx + g))
+        dG = sm.mu[rr][x];
     }
     const float res = phi_cell_dG<float>(
         &F, clamp1(sm.psi[rr][x]), clamp1(sm.psi[rr][x + 1]), clamp1(sm.psi[rr][x - 1]), clamp1(sm.psi[rr + 1][x]),
@@ -635,7 +671,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
 }
 
 template <bool SURR>
-__global__ void __launch_bounds__(kThreads, SURR ? 3 : 5)
+__global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
     tile_kernel(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<float> F,
                 const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
                 const __grid_constant__ CUtensorMap tm_c, const float *__restrict__ tab, const int tab_len,

@@ -69,10 +69,11 @@ def test_training_reduces_the_error():
 
 def test_surrogate_step_runs_with_audit():
     """The FP32 step with the surrogate in place of the exact per-cell
-    evaluation: finite fields, the audit visits one cell in 1024 per step and
-    finds no out-of-box cell on this workload, and a learned form that still
-    moves the front (its accuracy is measured, not asserted to a tolerance:
-    see the surrogate notes of the design document)."""
+    evaluation of every cell that is not bulk melt: finite fields, the audit
+    visits about one such cell in 1024 per step and finds no out-of-box cell
+    on this workload, and a learned form that still moves the front (its
+    accuracy is measured, not asserted to a tolerance: see the surrogate
+    notes of the design document)."""
     p = configs.scale_fp32()
     p.nx_all = p.ny_all = 512
     w, box, _ = surrogate.train(p, n_samples=1 << 18, epochs=8, batch=4096, lr=3e-3, seed=4)
@@ -91,9 +92,11 @@ def test_surrogate_step_runs_with_audit():
         out[use] = (a.psi.cpu().numpy(), a.c.cpu().numpy(), ctx.surrogate_audit() if use else None)
     psi, c, (emu, edg, nfb, naud) = out[True]
     assert np.isfinite(psi).all() and np.isfinite(c).all()
-    cells = (p.nx_all - 2) * (p.ny_all - 2) + 2 * 18 * 0  # audited cells are interior or halo columns
+    # cells the network evaluates: psi not exactly -1 (the melt keeps its
+    # exact series form), plus tile halo columns next to them
+    non_melt = int((out[False][0] != -1.0).sum())
     assert nfb == 0
-    assert 0.5 * 300 * cells / 1024 < naud < 2.0 * 300 * (p.nx_all * p.ny_all) / 1024
+    assert 0.3 * 300 * non_melt / 1024 < naud < 3.0 * 300 * non_melt / 1024
     assert 0.0 < emu and 0.0 < edg
     # the front stays where the exact run has it to within a few cells
     ifront = lambda ps: (ps.reshape(p.ny_all, p.nx_all)[1:-1, 1:-1] > 0).sum(1).mean()
