@@ -1,0 +1,38 @@
+// rs_peri3d.cuh — launchers of the 3D three-phase step (rs_peri3d.cu).
+#pragma once
+
+#include <cuda.h>
+
+#include "rs_common.cuh"
+
+namespace rs {
+
+constexpr int kP3MaxCaps = 16;
+
+// tensor maps of one field set (3D, dims nx, ny, nz; box of
+// peri3d_box_width x peri3d_box_height x 1 elements)
+struct P3Maps {
+  CUtensorMap phi1, phi2, c;
+};
+
+// initial state: front, cap centres (host-drawn), compositions
+struct P3Init {
+  uint64_t seed;
+  double z_front, amp, radius, roff;
+  double ca, cb, clb;
+  int n_alpha;
+  double cx[kP3MaxCaps], cy[kP3MaxCaps];
+};
+
+int peri3d_box_width(int precision);
+int peri3d_box_height();
+int launch_peri3d_step(const rs3_params &p, const P3Maps &m, int precision, void *o1, void *o2, void *oc,
+                       int64_t step, int *err, cudaStream_t st);
+int launch_peri3d_mu(const rs3_params &p, int precision, const void *f1, const void *f2, const void *fc, void *mu,
+                     cudaStream_t st);
+int launch_peri3d_mass(const rs3_params &p, int precision, const void *fc, double *partial, int nparts, double *out,
+                       cudaStream_t st);
+int launch_peri3d_init(const rs3_params &p, int precision, const P3Init &ini, void *f1, void *f2, void *fc,
+                       cudaStream_t st);
+
+}  // namespace rs

@@ -5,7 +5,7 @@ rs_sizeof_params()/rs_sizeof_step_args() and the tests compare them.
 """
 import ctypes as C
 
-RS_ABI_VERSION = 7
+RS_ABI_VERSION = 8
 RS_MLP_NPARAMS = 1250
 RS_OPT_TMA = 1
 RS_OK = 0
@@ -94,3 +94,23 @@ class MlpBox(C.Structure):
     """rs_mlp_box — training box and output scaling of the CALPHAD surrogate."""
     _fields_ = [("T_lo", C.c_double), ("T_hi", C.c_double), ("c_lo", C.c_double), ("c_hi", C.c_double),
                 ("y_mean", C.c_double * 2), ("y_scale", C.c_double * 2)]
+
+
+class Params3(C.Structure):
+    """rs3_params — the 3D three-phase model (TiAg.cu macro names in comments)."""
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("z_chunk", C.c_int32),
+        ("dt", C.c_double),                                   # DT
+        ("dx_inv", C.c_double), ("dy_inv", C.c_double), ("dz_inv", C.c_double),  # DXin ..
+        ("a1", C.c_double), ("a2", C.c_double), ("a3", C.c_double), ("b", C.c_double),
+        ("lam", C.c_double), ("alpha", C.c_double), ("Da", C.c_double), ("Db", C.c_double),
+        ("A1", C.c_double), ("A2", C.c_double), ("B11", C.c_double), ("B12", C.c_double),
+        ("B21", C.c_double), ("B22", C.c_double),
+        ("T_ref", C.c_double), ("G_T", C.c_double), ("V_T", C.c_double), ("z_T", C.c_double),
+    ]
+
+
+class Fields3(C.Structure):
+    """rs3_fields — one 3D device field set (phi1, phi2, c)."""
+    _fields_ = [("phi1", C.c_void_p), ("phi2", C.c_void_p), ("c", C.c_void_p),
+                ("precision", C.c_int32), ("reserved", C.c_int32)]

@@ -176,3 +176,34 @@ def ensemble(n=64, seed=2024, lib=None):
         p.seed = seed + k
         runs.append((p, c0, cs))
     return runs
+
+
+# ---------------------------------------------------------------- 3D variant
+# Units of the 3D three-phase model (the reference's TiAg.cu is dimensionless):
+# T is an undercooling in units of 1/0.000321787 K (TiAg.cu:52 sets
+# 60 * 0.000321787 for 60 K); one model length unit is 50 nm (dx = 1/DXin =
+# 0.5 units = 25 nm); one model time unit is 1 ns.  These scales map the
+# workload's G and V onto the model; they are this build's choice, not the
+# reference's.
+T_PER_K = 0.000321787
+LENGTH_UNIT_M = 50e-9
+TIME_UNIT_S = 1e-9
+IC3 = dict(z_front=24.0, amp=0.5, n_alpha=4, cap_radius=30.0, seed=11)
+STEPS["peritectic_3d"] = 5000
+
+
+def peritectic_3d(G_K_per_m=2.0e6, V_m_per_s=0.2, nx=512, ny=512, nz=1024, lib=None):
+    """3D three-phase directional solidification on one GPU: 512 x 512 x 1024
+    (ghost layers included), the reference model's constants, a frozen
+    gradient G moving at V.  The undercooling falls with z (melt above the
+    beta front), and T = T_ref at the front plane at step 0."""
+    if lib is None:
+        from . import lib as _lib
+        lib = _lib
+    p = lib.default_params3()
+    p.nx, p.ny, p.nz = nx, ny, nz
+    dx_m = LENGTH_UNIT_M / p.dx_inv
+    p.G_T = -G_K_per_m * dx_m * T_PER_K
+    p.V_T = V_m_per_s * p.dt * TIME_UNIT_S / dx_m
+    p.z_T = IC3["z_front"]
+    return p

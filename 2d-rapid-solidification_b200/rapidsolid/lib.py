@@ -81,6 +81,15 @@ def load():
         "rs_ensemble_state": ([vp, i32, vp, vp, vp, vp], C.c_int),
         "rs_ensemble_autotune": ([vp, i32, vp, vp, vp], C.c_int),
         "rs_surrogate_audit": ([vp, vp, vp, vp, vp, vp], C.c_int),
+        "rs3_default_params": ([vp], C.c_int),
+        "rs3_sizeof_params": ([], sz),
+        "rs3_create": ([vp, C.POINTER(vp)], C.c_int),
+        "rs3_destroy": ([vp], C.c_int),
+        "rs3_step": ([vp, vp, vp, i64, vp], C.c_int),
+        "rs3_mu": ([vp, vp, vp, vp], C.c_int),
+        "rs3_mass": ([vp, vp, vp, vp], C.c_int),
+        "rs3_initial": ([vp, vp, C.c_double, C.c_double, i32, C.c_double, C.c_uint64, vp], C.c_int),
+        "rs3_device_status": ([vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -90,6 +99,8 @@ def load():
         raise RuntimeError("librsb200.so ABI version mismatch: rebuild the library")
     if L.rs_sizeof_params() != C.sizeof(_abi.Params) or L.rs_sizeof_step_args() != C.sizeof(_abi.StepArgs):
         raise RuntimeError("rs_params/rs_step_args layout differs from rapidsolid._abi")
+    if L.rs3_sizeof_params() != C.sizeof(_abi.Params3):
+        raise RuntimeError("rs3_params layout differs from rapidsolid._abi")
     _lib = L
     return L
 
@@ -346,3 +357,70 @@ class Ensemble:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- 3D variant
+
+def default_params3():
+    """rs3_params with the constants of the reference's TiAg.cu (512 x 512 x 128, isothermal)."""
+    p = _abi.Params3()
+    check(load().rs3_default_params(C.byref(p)))
+    return p
+
+
+class FieldSet3:
+    """3D device field set: phi1, phi2, c as (nz, ny, nx) tensors."""
+
+    def __init__(self, p, dtype, device="cuda"):
+        import torch
+        shape = (p.nz, p.ny, p.nx)
+        self.dtype = dtype
+        self.phi1 = torch.zeros(shape, dtype=dtype, device=device)
+        self.phi2 = torch.zeros(shape, dtype=dtype, device=device)
+        self.c = torch.zeros(shape, dtype=dtype, device=device)
+        self.precision = _abi.RS_F64 if dtype == torch.float64 else _abi.RS_F32
+
+    def fields(self):
+        return _abi.Fields3(phi1=self.phi1.data_ptr(), phi2=self.phi2.data_ptr(), c=self.c.data_ptr(),
+                            precision=self.precision, reserved=0)
+
+
+class Context3:
+    """A 3D three-phase context (rs3_create)."""
+
+    def __init__(self, p):
+        self.lib = load()
+        self.p = p
+        self._h = C.c_void_p()
+        check(self.lib.rs3_create(C.byref(p), C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            self.lib.rs3_destroy(self._h)
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, cur, nxt, step, stream=None):
+        a, b = cur.fields(), nxt.fields()
+        check(self.lib.rs3_step(self._h, C.byref(a), C.byref(b), step, _stream(stream)))
+
+    def mu(self, fs, out, stream=None):
+        f = fs.fields()
+        check(self.lib.rs3_mu(self._h, C.byref(f), _ptr(out), _stream(stream)))
+
+    def mass(self, fs, out, stream=None):
+        f = fs.fields()
+        check(self.lib.rs3_mass(self._h, C.byref(f), _ptr(out), _stream(stream)))
+
+    def initial(self, fs, z_front, amp, n_alpha, cap_radius, seed, stream=None):
+        f = fs.fields()
+        check(self.lib.rs3_initial(self._h, C.byref(f), z_front, amp, n_alpha, cap_radius, seed,
+                                   _stream(stream)))
+
+    def device_status(self, stream=None):
+        check(self.lib.rs3_device_status(self._h, _stream(stream)))

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define RS_ABI_VERSION 7
+#define RS_ABI_VERSION 8
 
 /* status codes */
 #define RS_OK 0
@@ -348,6 +348,69 @@ int rs_ensemble_state(rs_ens *e, int32_t run, int64_t *step, int32_t *i_offset_h
  * interleaved) over reps launches without advancing the runs, keeps the
  * fastest; ms_out[3] receives the mean launch times. */
 int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choice, rs_stream_t stream);
+
+/* ---- 3D three-phase variant (one GPU) ----
+ * The reference's 3D peritectic model, multi/peritectic_multiGPU/TiAg.cu:
+ * two stored order parameters phi1 (liquid) and phi2 (solid alpha), the
+ * third phase phi3 = 1 - phi1 - phi2 (solid beta), the diffusion potential
+ * mu = c - sum_i r_i g_i(phi) (computeMu, TiAg.cu:461-470) and the explicit
+ * update of phi1, phi2 and c (diffuse, TiAg.cu:503-561), with periodic x, y
+ * and no-flux z ghost layers (the boundaryMu and boundary kernels,
+ * TiAg.cu:472-500, 565-605).  Cell (x, y, z) lives at (z * ny + y) * nx + x (TiAg.cu pos).
+ * One domain on one GPU: the reference's z-slab exchange between GPUs
+ * (TiAg.cu:279-331) has no counterpart.
+ * Extension beyond the reference: a frozen temperature
+ *   T(z, step) = T_ref + G_T (z - z_T - V_T step)
+ * enters through B1(T) = B11 + B12 T, B2(T) = B21 + B22 T (TiAg.cu:61-62);
+ * G_T = 0 is the reference's isothermal model. */
+typedef struct rs3_params {
+  int32_t nx, ny, nz;               /* extents incl. ghost layers (TiAg Nx, Ny, devNz) */
+  int32_t z_chunk;                  /* planes per CTA of the z march (0: 64) */
+  double dt;                        /* DT */
+  double dx_inv, dy_inv, dz_inv;    /* DXin, DYin, DZin */
+  double a1, a2, a3, b;             /* three-phase well terms */
+  double lambda, alpha, Da, Db;     /* coupling, diffusivity, solid diffusivities */
+  double A1, A2, B11, B12, B21, B22;
+  double T_ref;                     /* T of TiAg.cu (60 * 0.000321787) */
+  double G_T;                       /* dT per cell along z */
+  double V_T;                       /* isotherm speed, cells per step */
+  double z_T;                       /* plane where T = T_ref at step 0 */
+} rs3_params;
+
+/* A 3D field set on the device (nx * ny * nz elements each, 16-byte aligned). */
+typedef struct rs3_fields {
+  void *phi1;
+  void *phi2;
+  void *c;
+  int32_t precision; /* RS_F64 or RS_F32 */
+  int32_t reserved;
+} rs3_fields;
+
+typedef struct rs3_ctx rs3_ctx;
+
+/* TiAg.cu's constants (TiAg.cu:19-62) on a 512 x 512 x 128 domain, isothermal */
+int rs3_default_params(rs3_params *p);
+size_t rs3_sizeof_params(void);
+int rs3_create(const rs3_params *p, rs3_ctx **out);
+int rs3_destroy(rs3_ctx *ctx);
+/* One step (TiAg.cu:269-340): computeMu, boundaryMu, diffuse, boundary,
+ * fused into one launch: next = step(cur), ghost layers included. */
+int rs3_step(rs3_ctx *ctx, const rs3_fields *cur, const rs3_fields *next, int64_t step, rs_stream_t stream);
+/* mu of every cell, ghost layers as images (computeMu + boundaryMu);
+ * d_mu has the set's precision */
+int rs3_mu(rs3_ctx *ctx, const rs3_fields *f, void *d_mu, rs_stream_t stream);
+/* FP64 sum of c over the interior (the avg_c numerator, TiAg.cu:237-249) */
+int rs3_mass(rs3_ctx *ctx, const rs3_fields *f, double *d_mass, rs_stream_t stream);
+/* Initial state: solid beta below the plane z_front + U(-amp, amp) (one
+ * seeded draw per (x, y) column), liquid above, and n_alpha spherical alpha
+ * caps of base radius cap_radius and contact angle 1.33 rad on the front at
+ * seeded (x, y) positions (the cap shape of TiAg.cu initial, 400-444).
+ * Compositions are the model's own equilibrium values at T_ref (TiAg.cu ca,
+ * cb, clb): beta cb, alpha ca, liquid clb.  Ghost layers are images. */
+int rs3_initial(rs3_ctx *ctx, const rs3_fields *f, double z_front, double amp, int32_t n_alpha,
+                double cap_radius, uint64_t seed, rs_stream_t stream);
+/* RS_E_STATE if a step kernel's bounded wait for a plane load gave up */
+int rs3_device_status(rs3_ctx *ctx, rs_stream_t stream);
 
 /* ---- host-side helpers (no device work) ---- */
 /* CALPHAD Ti-Nb evaluator (fun.cu:1628-1720), host build of the same code

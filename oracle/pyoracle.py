@@ -61,6 +61,15 @@ def lib():
         L.ro_run_steps.argtypes = [vp] * 8 + [C.c_int64, C.c_int64, C.c_int, C.c_double]
         L.ro_run_steps.restype = C.c_int
         L.ro_num_threads.restype = C.c_int
+        L.ro3_default_params.argtypes = [vp]
+        L.ro3_equilibrium.argtypes = [vp, vp]
+        L.ro3_boundary.argtypes = [vp, vp]
+        L.ro3_mu.argtypes = [vp] * 5
+        L.ro3_step.argtypes = [vp, C.c_int64] + [vp] * 7
+        L.ro3_mass.restype = C.c_double
+        L.ro3_mass.argtypes = [vp, vp]
+        L.ro3_cap_centres.argtypes = [vp, C.c_int, C.c_uint64, vp, vp]
+        L.ro3_initial.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_uint64, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -169,3 +178,54 @@ def philox(ctr, key):
 def ref_binary(name):
     """Path of a reference harness binary built by oracle/ref_build.sh."""
     return os.path.join(REF_DIR, name)
+
+
+# ---------------------------------------------------------------- 3D (TiAg.cu)
+
+def default_params3():
+    p = _abi.Params3()
+    lib().ro3_default_params(C.byref(p))
+    return p
+
+
+def equilibrium3(p):
+    """ca, cb, cla, clb at T_ref (TiAg.cu:64-67)."""
+    out = np.zeros(4)
+    lib().ro3_equilibrium(C.byref(p), _p(out))
+    return out
+
+
+def zeros3(p):
+    return np.zeros((p.nz, p.ny, p.nx))
+
+
+def initial3(p, z_front, amp, n_alpha, cap_radius, seed):
+    f = [zeros3(p) for _ in range(3)]
+    lib().ro3_initial(C.byref(p), z_front, amp, n_alpha, cap_radius, seed, *[_p(a) for a in f])
+    return f
+
+
+def boundary3(p, a):
+    lib().ro3_boundary(C.byref(p), _p(a))
+
+
+def mu3(p, phi1, phi2, c):
+    mu = zeros3(p)
+    lib().ro3_mu(C.byref(p), _p(phi1), _p(phi2), _p(c), _p(mu))
+    return mu
+
+
+def step3(p, step_index, phi1, phi2, c):
+    out = [zeros3(p) for _ in range(3)]
+    lib().ro3_step(C.byref(p), step_index, _p(phi1), _p(phi2), _p(c), *[_p(a) for a in out], None)
+    return out
+
+
+def run3(p, f, nsteps, step0=0):
+    for k in range(nsteps):
+        f = step3(p, step0 + k, *f)
+    return f
+
+
+def mass3(p, c):
+    return lib().ro3_mass(C.byref(p), _p(c))

@@ -63,4 +63,24 @@ build ref_harness_2048 2048 2048 16 -UGG -DGG=0.005 -UVp -DVp=0.5
     -Dtotal_time=120000 -Dif_load=0 '-Dpath_input="./"' -Drun_time=4 -Drandom_seed=3 \
     -DVp=0.6 -DGG=0.002 -Deps1=0.02 -Deps2=0.001 -Depk1=0.1 -DNx_all=768 -DNy_all=832 -DMAX_GPU=1 \
     "$HERE/ref_params_harness.cu" -o "$OUT/ref_params_harness"
+# The 3D three-phase model, multi/peritectic_multiGPU/TiAg.cu: a copy with its
+# grid macros set to the harness size (the reference edits Nx, Ny, Nz, devNz
+# by hand per run), main renamed; oracle/ref3_harness.cu drives the kernels.
+TIAG="$REF/multi/peritectic_multiGPU/TiAg.cu"
+if [ -f "$TIAG" ]; then
+  build3() { # name nx ny devnz
+    local name=$1 nx=$2 ny=$3 dnz=$4
+    local src="$OUT/src/TiAg.$nx.$ny.$dnz.cu"
+    sed -e "s/^#define[[:space:]]*Nx[[:space:]]*512/#define Nx $nx/" \
+        -e "s/^#define[[:space:]]*Ny[[:space:]]*512/#define Ny $ny/" \
+        -e "s/^#define[[:space:]]*Nz[[:space:]]*506.*/#define Nz (($dnz - 2) * Ngpu + 2)/" \
+        -e "s/^#define[[:space:]]*devNz[[:space:]]*128.*/#define devNz $dnz/" "$TIAG" > "$src"
+    grep -q "^#define Nx $nx" "$src"
+    grep -q "^#define devNz $dnz" "$src"
+    "$NVCC" -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -ccbin g++ -w \
+        -DREF3_SOURCE="\"$src\"" -Dmain=ref3_main "$HERE/ref3_harness.cu" -o "$OUT/$name"
+  }
+  build3 ref3_harness_32 32 32 20
+  build3 ref3_harness_512 512 512 128
+fi
 echo "ref_build: built $(ls "$OUT" | grep -c harness) harness binaries in $OUT"

@@ -89,6 +89,18 @@ int ro_run_steps(const rs_params *p, const rs_derived *d, double *c, double *phi
                  double l_offset_Vp0);
 int ro_num_threads(void);
 
+/* ---- 3D three-phase step (multi/peritectic_multiGPU/TiAg.cu), rs3_oracle.c ---- */
+void ro3_default_params(rs3_params *p);
+void ro3_equilibrium(const rs3_params *p, double out[4]); /* ca, cb, cla, clb */
+void ro3_boundary(const rs3_params *p, double *f);
+void ro3_mu(const rs3_params *p, const double *phi1, const double *phi2, const double *c, double *mu);
+void ro3_step(const rs3_params *p, int64_t step, const double *phi1, const double *phi2, const double *c,
+              double *phi1_n, double *phi2_n, double *c_n, double *mu_out);
+double ro3_mass(const rs3_params *p, const double *c);
+void ro3_cap_centres(const rs3_params *p, int n_alpha, uint64_t seed, double *cx, double *cy);
+void ro3_initial(const rs3_params *p, double z_front, double amp, int n_alpha, double cap_radius, uint64_t seed,
+                 double *phi1, double *phi2, double *c);
+
 #ifdef __cplusplus
 }
 #endif

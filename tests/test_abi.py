@@ -14,7 +14,7 @@ from rapidsolid import _abi, configs, lib
 
 def header_symbols():
     txt = open(os.path.join(ROOT, "include", "rs_b200.h")).read()
-    return sorted(set(re.findall(r"^(?:int|const char \*|size_t)\s+\*?(rs_\w+)\(", txt, flags=re.M)))
+    return sorted(set(re.findall(r"^(?:int|const char \*|size_t)\s+\*?(rs3?_\w+)\(", txt, flags=re.M)))
 
 
 def test_library_exports_every_declared_symbol():
