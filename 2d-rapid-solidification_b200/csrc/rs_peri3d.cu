@@ -69,7 +69,7 @@ template <typename R>
 struct K3 {  // kernel constants in the working precision
   int nx, ny, nz, z_chunk;
   R dt, dxi, dyi, dzi, dxi2, dyi2, dzi2;
-  R a1, a2, a3, b, lam, dt_alpha, Da_h, Db_h;
+  R a1, a2, a3, b, lam, Da2, Db2, cfx, cfy, cfz;
   R r1, r2, r3;
   double B11, B12, B21, B22, T_ref, G_T, V_T, z_T;
 };
@@ -93,9 +93,13 @@ K3<R> make_k3(const rs3_params &p) {
   k.a3 = (R)p.a3;
   k.b = (R)p.b;
   k.lam = (R)p.lambda;
-  k.dt_alpha = (R)(p.dt * p.alpha);
-  k.Da_h = (R)(p.Da * 0.5);
-  k.Db_h = (R)(p.Db * 0.5);
+  // c' = c + dt alpha sum_d din^2 (H+ - H-) / 2 with H = M dmu, M = phi1 + phi1'
+  // (+ Da (phi2 + phi2') + Db (phi3 + phi3')), TiAg.cu:543-552
+  k.Da2 = (R)p.Da;
+  k.Db2 = (R)p.Db;
+  k.cfx = (R)(0.5 * p.dt * p.alpha * p.dx_inv * p.dx_inv);
+  k.cfy = (R)(0.5 * p.dt * p.alpha * p.dy_inv * p.dy_inv);
+  k.cfz = (R)(0.5 * p.dt * p.alpha * p.dz_inv * p.dz_inv);
   k.r1 = (R)p.A1;
   k.r2 = (R)(-p.A1 - p.A2);
   k.r3 = (R)(-p.A1 + p.A2);
@@ -135,7 +139,8 @@ __device__ __forceinline__ bool p3_wait(uint64_t *bar, uint32_t parity, int *err
   return true;
 }
 
-template <typename R>
+// SD: solid diffusivities Da or Db non-zero (the reference sets both to 0)
+template <typename R, bool SD>
 __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
     peri3d_kernel(const __grid_constant__ K3<R> k, const __grid_constant__ CUtensorMap m1,
                   const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap mc,
@@ -198,13 +203,15 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
     return;
   }
 
-  // this thread's cells: x = tid % BX (+1 box column), rows tid / BX + r * (256 / BX)
-  const int ix = tid % C::BX, iy0 = tid / C::BX;
-  constexpr int kRowStep = kP3Threads / C::BX;
+  // this thread's cells: column ix, a strip of K consecutive rows (the y
+  // neighbours of the strip come from a register window)
+  constexpr int K = C::kCellsPerThread;
+  const int ix = tid % C::BX, iy0 = (tid / C::BX) * K;
   const int gx = xb + 1 + ix;  // array x of the output
   const bool xin = gx <= k.nx - 2;
   const int xg = gx == k.nx - 2 ? 0 : (gx == 1 ? k.nx - 1 : -1);  // ghost column it images
   const int64_t plane = (int64_t)k.nx * k.ny;
+  const R third = R(1) / R(3);
 
   for (int z = zo0; z < zo1; ++z) {
     if (!__syncthreads_and(mu_plane(z + 1))) {
@@ -221,67 +228,89 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
     const double B1 = k.B11 + k.B12 * Tz, B2 = k.B21 + k.B22 * Tz;
     const R s1 = (R)B1, s2 = (R)(-B1 - B2), s3 = (R)(-B1 + B2);
     const int zg = z == 1 ? 0 : (z == k.nz - 2 ? k.nz - 1 : -1);
-#pragma unroll
-    for (int r = 0; r < C::kCellsPerThread; ++r) {
-      const int iy = iy0 + r * kRowStep;
-      const int gy = yb + 1 + iy;
-      if (!xin || gy > k.ny - 2) continue;
-      const int e = (iy + 1) * C::BXin + ix + 1;  // box element of the cell
-      const R p1 = c1[e], p2 = c2[e], p3 = R(1) - p1 - p2, m0 = mu[e];
-      // chemical driving forces (fcphi, TiAg.cu:514-516)
-      const R w1 = s1 - k.r1 * m0, w2 = s2 - k.r2 * m0, w3 = s3 - k.r3 * m0;
-      const R fc1 = k.lam * (gp1(p1, p2, p3) * w1 + gp2(p2, p1, p3) * w2 + gp2(p3, p1, p2) * w3);
-      const R fc2 = k.lam * (gp2(p1, p2, p3) * w1 + gp1(p2, p3, p1) * w2 + gp2(p3, p2, p1) * w3);
-      const R fc3 = k.lam * (gp2(p1, p3, p2) * w1 + gp2(p2, p3, p1) * w2 + gp1(p3, p1, p2) * w3);
-      // neighbours
-      const R x1p = c1[e + 1], x1m = c1[e - 1], y1p = c1[e + C::BXin], y1m = c1[e - C::BXin], z1p = u1[e],
-              z1m = d1[e];
-      const R x2p = c2[e + 1], x2m = c2[e - 1], y2p = c2[e + C::BXin], y2m = c2[e - C::BXin], z2p = u2[e],
-              z2m = d2[e];
-      const R lap1 = (x1p + x1m - R(2) * p1) * k.dxi2 + (y1p + y1m - R(2) * p1) * k.dyi2 +
-                     (z1p + z1m - R(2) * p1) * k.dzi2;
-      const R lap2 = (x2p + x2m - R(2) * p2) * k.dxi2 + (y2p + y2m - R(2) * p2) * k.dyi2 +
-                     (z2p + z2m - R(2) * p2) * k.dzi2;
-      const R lap3 = -lap1 - lap2;
-      // multi-well terms (fphi, TiAg.cu:522-527)
-      const R f1 = R(2) * p1 * (R(1) - p1) * (R(1) - R(2) * p1) + k.a1 * ((p2 * p3) * (p2 * p3)) * (R(3) + R(2) * k.b * p1) +
-                   R(2) * k.a2 * p1 * (p3 * p3) * (R(3) * p1 * p3 + R(3) * p2 + k.b * (p2 * p2)) +
-                   R(2) * k.a3 * p1 * (p2 * p2) * (R(3) * p1 * p2 + R(3) * p3 + k.b * (p3 * p3)) + fc1;
-      const R f2 = R(2) * p2 * (R(1) - p2) * (R(1) - R(2) * p2) +
-                   R(2) * k.a1 * p2 * (p3 * p3) * (R(3) * p2 * p3 + R(3) * p1 + k.b * (p1 * p1)) +
-                   k.a2 * ((p1 * p3) * (p1 * p3)) * (R(3) + R(2) * k.b * p2) +
-                   R(2) * k.a3 * p2 * (p1 * p1) * (R(3) * p1 * p2 + R(3) * p3 + k.b * (p3 * p3)) + fc2;
-      const R f3 = R(2) * p3 * (R(1) - p3) * (R(1) - R(2) * p3) +
-                   R(2) * k.a1 * p3 * (p2 * p2) * (R(3) * p2 * p3 + R(3) * p1 + k.b * (p1 * p1)) +
-                   R(2) * k.a2 * p3 * (p1 * p1) * (R(3) * p1 * p3 + R(3) * p2 + k.b * (p2 * p2)) +
-                   k.a3 * ((p1 * p2) * (p1 * p2)) * (R(3) + R(2) * k.b * p3) + fc3;
-      const R mp1 = f1 - lap1, mp2 = f2 - lap2, mp3 = f3 - lap3;
-      const R third = R(0.333333333333333333333333333);
-      const R n1 = p1 + k.dt * (-(R(2) * mp1 - mp2 - mp3) * third);
-      const R n2 = p2 + k.dt * (-(R(2) * mp2 - mp1 - mp3) * third);
-      // solute fluxes through the six faces (TiAg.cu:543-550)
-      auto hface = [&](R q1, R q2, R dmu, R din) {
-        return (R(0.5) * (p1 + q1) + k.Da_h * (p2 + q2) + k.Db_h * (p3 + R(1) - q1 - q2)) * dmu * din;
-      };
-      const R Hxp = hface(x1p, x2p, mu[e + 1] - m0, k.dxi), Hxn = hface(x1m, x2m, m0 - mu[e - 1], k.dxi);
-      const R Hyp = hface(y1p, y2p, mu[e + C::BXin] - m0, k.dyi), Hyn = hface(y1m, y2m, m0 - mu[e - C::BXin], k.dyi);
-      const R Hzp = hface(z1p, z2p, muu[e] - m0, k.dzi), Hzn = hface(z1m, z2m, m0 - mud[e], k.dzi);
-      const R nc = cc[e] + k.dt_alpha * ((Hxp - Hxn) * k.dxi + (Hyp - Hyn) * k.dyi + (Hzp - Hzn) * k.dzi);
-      // the cell and every ghost cell that images it
-      const int yg = gy == k.ny - 2 ? 0 : (gy == 1 ? k.ny - 1 : -1);
-      const int xs[2] = {gx, xg}, ys[2] = {gy, yg}, zs[2] = {z, zg};
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int bq = 0; bq < 2; ++bq)
-#pragma unroll
-          for (int cq = 0; cq < 2; ++cq) {
-            if (xs[a] < 0 || ys[bq] < 0 || zs[cq] < 0) continue;
-            const int64_t o = (int64_t)zs[cq] * plane + (int64_t)ys[bq] * k.nx + xs[a];
-            o1[o] = n1;
-            o2[o] = n2;
-            oc[o] = nc;
-          }
+    if (xin) {
+      const int e0 = (iy0 + 1) * C::BXin + ix + 1;  // box element of the strip's first cell
+      R w1[K + 2], w2[K + 2], wm[K + 2];            // the strip's column, rows iy0-1 .. iy0+K
+  #pragma unroll
+      for (int r = 0; r < K + 2; ++r) {
+        const int e = e0 + (r - 1) * C::BXin;
+        w1[r] = c1[e];
+        w2[r] = c2[e];
+        wm[r] = mu[e];
+      }
+  #pragma unroll
+      for (int r = 0; r < K; ++r) {
+        const int gy = yb + 1 + iy0 + r;
+        if (gy > k.ny - 2) break;
+        const int e = e0 + r * C::BXin;
+        const R p1 = w1[r + 1], p2 = w2[r + 1], m0 = wm[r + 1], p3 = R(1) - p1 - p2;
+        const R d12 = p1 - p2, d23 = p2 - p3, d31 = p3 - p1;
+        // chemical driving forces (fcphi, TiAg.cu:514-516), with
+        // gp1(pi, pj, pk) = G_i and gp2(pi, pj, pk) = Q_i (pj - pk)
+        const R Q1 = R(7.5) * (p1 - R(1)) * (p1 * p1), Q2 = R(7.5) * (p2 - R(1)) * (p2 * p2),
+                Q3 = R(7.5) * (p3 - R(1)) * (p3 * p3);
+        const R G1 = R(3.75) * p1 * ((((R(3) * p1 - R(4)) * p1 - R(1)) * p1 + R(2)) + (R(3) * p1 - R(2)) * (d23 * d23));
+        const R G2 = R(3.75) * p2 * ((((R(3) * p2 - R(4)) * p2 - R(1)) * p2 + R(2)) + (R(3) * p2 - R(2)) * (d31 * d31));
+        const R G3 = R(3.75) * p3 * ((((R(3) * p3 - R(4)) * p3 - R(1)) * p3 + R(2)) + (R(3) * p3 - R(2)) * (d12 * d12));
+        const R o1w = s1 - k.r1 * m0, o2w = s2 - k.r2 * m0, o3w = s3 - k.r3 * m0;
+        const R A = Q1 * d23 * o1w, Bq = Q2 * d31 * o2w, Cq = Q3 * d12 * o3w;
+        // multi-well terms (fphi, TiAg.cu:522-527) with their shared factors
+        const R s12 = p1 * p2, s13 = p1 * p3, s23 = p2 * p3;
+        const R U1 = R(3) * s23 + R(3) * p1 + k.b * (p1 * p1), U2 = R(3) * s13 + R(3) * p2 + k.b * (p2 * p2),
+                U3 = R(3) * s12 + R(3) * p3 + k.b * (p3 * p3);
+        const R F1 = R(2) * p1 * (R(1) - p1) * (R(1) - R(2) * p1) + k.a1 * (s23 * s23) * (R(3) + R(2) * k.b * p1) +
+                     R(2) * k.a2 * p1 * (p3 * p3) * U2 + R(2) * k.a3 * p1 * (p2 * p2) * U3 +
+                     k.lam * (G1 * o1w - Bq + Cq);
+        const R F2 = R(2) * p2 * (R(1) - p2) * (R(1) - R(2) * p2) + R(2) * k.a1 * p2 * (p3 * p3) * U1 +
+                     k.a2 * (s13 * s13) * (R(3) + R(2) * k.b * p2) + R(2) * k.a3 * p2 * (p1 * p1) * U3 +
+                     k.lam * (A + G2 * o2w - Cq);
+        const R F3 = R(2) * p3 * (R(1) - p3) * (R(1) - R(2) * p3) + R(2) * k.a1 * p3 * (p2 * p2) * U1 +
+                     R(2) * k.a2 * p3 * (p1 * p1) * U2 + k.a3 * (s12 * s12) * (R(3) + R(2) * k.b * p3) +
+                     k.lam * (-A + Bq + G3 * o3w);
+        // neighbours
+        const R x1p = c1[e + 1], x1m = c1[e - 1], x2p = c2[e + 1], x2m = c2[e - 1];
+        const R z1p = u1[e], z1m = d1[e], z2p = u2[e], z2m = d2[e];
+        const R lap1 = (x1p + x1m - R(2) * p1) * k.dxi2 + (w1[r + 2] + w1[r] - R(2) * p1) * k.dyi2 +
+                       (z1p + z1m - R(2) * p1) * k.dzi2;
+        const R lap2 = (x2p + x2m - R(2) * p2) * k.dxi2 + (w2[r + 2] + w2[r] - R(2) * p2) * k.dyi2 +
+                       (z2p + z2m - R(2) * p2) * k.dzi2;
+        // phi_i' = phi_i - dt (2 mu_i - mu_j - mu_k) / 3 with mu_i = F_i - lap_i and
+        // lap_3 = -lap_1 - lap_2 (TiAg.cu:529-537)
+        const R n1 = p1 + k.dt * (lap1 - (R(2) * F1 - F2 - F3) * third);
+        const R n2 = p2 + k.dt * (lap2 - (R(2) * F2 - F1 - F3) * third);
+        // solute: face mobility (phi1 + phi1') / 2 (+ solid terms), TiAg.cu:543-552
+        auto mob = [&](R q1, R q2) {
+          R m = p1 + q1;
+          if constexpr (SD) m += k.Da2 * (p2 + q2) + k.Db2 * (p3 + R(1) - q1 - q2);
+          return m;
+        };
+        const R jx = mob(x1p, x2p) * (mu[e + 1] - m0) - mob(x1m, x2m) * (m0 - mu[e - 1]);
+        const R jy = mob(w1[r + 2], w2[r + 2]) * (wm[r + 2] - m0) - mob(w1[r], w2[r]) * (m0 - wm[r]);
+        const R jz = mob(z1p, z2p) * (muu[e] - m0) - mob(z1m, z2m) * (m0 - mud[e]);
+        const R nc = cc[e] + (k.cfx * jx + k.cfy * jy + k.cfz * jz);
+        // the cell and every ghost cell that images it
+        const int yg = gy == k.ny - 2 ? 0 : (gy == 1 ? k.ny - 1 : -1);
+        if ((xg & yg & zg) < 0) {  // no ghost cell images this one
+          const int64_t o = (int64_t)z * plane + (int64_t)gy * k.nx + gx;
+          o1[o] = n1;
+          o2[o] = n2;
+          oc[o] = nc;
+        } else {
+          const int xs[2] = {gx, xg}, ys[2] = {gy, yg}, zs[2] = {z, zg};
+  #pragma unroll
+          for (int a = 0; a < 2; ++a)
+  #pragma unroll
+            for (int bq = 0; bq < 2; ++bq)
+  #pragma unroll
+              for (int cq = 0; cq < 2; ++cq) {
+                if (xs[a] < 0 || ys[bq] < 0 || zs[cq] < 0) continue;
+                const int64_t o = (int64_t)zs[cq] * plane + (int64_t)ys[bq] * k.nx + xs[a];
+                o1[o] = n1;
+                o2[o] = n2;
+                oc[o] = nc;
+              }
+        }
+      }
     }
     __syncthreads();  // plane z-1's input and mu slots are free
     if (z + 3 <= zin1) {
@@ -413,15 +442,16 @@ int launch_step(const rs3_params &p, const P3Maps &m, R *o1, R *o2, R *oc, int64
   using C = P3Cfg<R>;
   const K3<R> k = make_k3<R>(p);
   const size_t smem = sizeof(P3Smem<R>) + 128;
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(peri3d_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return -3;
-    attr = true;
+  const bool sd = p.Da != 0.0 || p.Db != 0.0;
+  auto kfn = sd ? peri3d_kernel<R, true> : peri3d_kernel<R, false>;
+  static bool attr[2] = {false, false};
+  if (!attr[sd]) {
+    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -3;
+    attr[sd] = true;
   }
   const dim3 grid((p.nx - 2 + C::BX - 1) / C::BX, (p.ny - 2 + kP3BY - 1) / kP3BY,
                   (p.nz - 2 + k.z_chunk - 1) / k.z_chunk);
-  peri3d_kernel<R><<<grid, kP3Threads, smem, st>>>(k, m.phi1, m.phi2, m.c, o1, o2, oc, step, err);
+  kfn<<<grid, kP3Threads, smem, st>>>(k, m.phi1, m.phi2, m.c, o1, o2, oc, step, err);
   return 0;
 }
 
