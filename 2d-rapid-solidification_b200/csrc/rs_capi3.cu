@@ -61,7 +61,7 @@ bool encode_field(const rs3_params &p, const void *ptr, int precision, CUtensorM
   const size_t es = precision == RS_F64 ? 8 : 4;
   cuuint64_t dims[3] = {(cuuint64_t)p.nx, (cuuint64_t)p.ny, (cuuint64_t)p.nz};
   cuuint64_t strides[2] = {(cuuint64_t)p.nx * es, (cuuint64_t)p.nx * p.ny * es};
-  cuuint32_t box[3] = {(cuuint32_t)rs::peri3d_box_width(precision), (cuuint32_t)rs::peri3d_box_height(), 1};
+  cuuint32_t box[3] = {(cuuint32_t)rs::peri3d_box_width(precision), (cuuint32_t)rs::peri3d_box_height(precision), 1};
   cuuint32_t estr[3] = {1, 1, 1};
   return enc(out, precision == RS_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
              const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,

@@ -8,6 +8,8 @@
 // boundaryMu, diffuse) plus three boundary kernels and keeps mu as a field;
 // here one kernel does the step and mu never leaves shared memory.
 //
+// The FP32 step runs on packed FP32 pairs (rs_peri3d_x2.cu); this file's
+// step kernel is the FP64 one.
 // Kernel: a CTA owns a column of BX x BY output cells (x, y) and marches
 // through a chunk of z planes.  Every input plane (BX+4 (FP32) or BX+2 (FP64)
 // columns x BY+2 rows of phi1, phi2 and c) arrives by one 3D TMA box per
@@ -118,14 +120,6 @@ template <typename R>
 __device__ __forceinline__ R mu_of(const K3<R> &k, R p1, R p2, R c) {
   const R p3 = R(1) - p1 - p2;
   return c - k.r1 * g3(p1, p2, p3) - k.r2 * g3(p2, p3, p1) - k.r3 * g3(p3, p1, p2);
-}
-
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
-          "r"(smem_u32(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
 }
 
 template <typename R>
@@ -457,14 +451,14 @@ int launch_step(const rs3_params &p, const P3Maps &m, R *o1, R *o2, R *oc, int64
 
 }  // namespace
 
-int peri3d_box_width(int precision) { return precision == RS_F64 ? P3Cfg<double>::BXin : P3Cfg<float>::BXin; }
-int peri3d_box_height() { return kP3BY + 2; }
+int peri3d_box_width(int precision) { return precision == RS_F64 ? P3Cfg<double>::BXin : peri3d_x2_box_width(); }
+int peri3d_box_height(int precision) { return precision == RS_F64 ? kP3BY + 2 : peri3d_x2_box_height(); }
 
 int launch_peri3d_step(const rs3_params &p, const P3Maps &m, int precision, void *o1, void *o2, void *oc,
                        int64_t step, int *err, cudaStream_t st) {
   if (precision == RS_F64)
     return launch_step<double>(p, m, (double *)o1, (double *)o2, (double *)oc, step, err, st);
-  return launch_step<float>(p, m, (float *)o1, (float *)o2, (float *)oc, step, err, st);
+  return launch_peri3d_step_x2(p, m, (float *)o1, (float *)o2, (float *)oc, step, err, st);
 }
 
 int launch_peri3d_mu(const rs3_params &p, int precision, const void *f1, const void *f2, const void *fc, void *mu,

@@ -25,7 +25,11 @@ struct P3Init {
 };
 
 int peri3d_box_width(int precision);
-int peri3d_box_height();
+int peri3d_box_height(int precision);
+int peri3d_x2_box_width();
+int peri3d_x2_box_height();
+int launch_peri3d_step_x2(const rs3_params &p, const P3Maps &m, float *o1, float *o2, float *oc, int64_t step,
+                          int *err, cudaStream_t st);
 int launch_peri3d_step(const rs3_params &p, const P3Maps &m, int precision, void *o1, void *o2, void *oc,
                        int64_t step, int *err, cudaStream_t st);
 int launch_peri3d_mu(const rs3_params &p, int precision, const void *f1, const void *f2, const void *fc, void *mu,

@@ -124,6 +124,28 @@ def test_fp32_within_tolerance_of_fp64_oracle():
     assert abs(pyoracle.mass3(p, np.ascontiguousarray(out[2])) - m0) <= 1e-6 * abs(m0)
 
 
+@pytest.mark.parametrize("shape", [(36, 27, 13), (64, 48, 9), (132, 40, 70)])
+def test_fp32_ragged_sizes_within_tolerance(shape):
+    """The packed-pair FP32 kernel on partial tiles (x pairs beside the ghost
+    columns, rows past the last full tile) against the FP64 oracle."""
+    p = params(*shape)
+    f = pyoracle.initial3(p, 5.0, 0.5, 2, 4.0, 9)
+    out = run_gpu(p, f, 30, dtype=torch.float32)
+    ref = pyoracle.run3(p, f, 30)
+    assert maxdiff(out, ref) <= 2e-5
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-11), (torch.float32, 5e-5)])
+def test_nonzero_a1_and_solid_diffusion(dtype, tol):
+    """a1 and the solid diffusivities Da, Db (zero in the reference's set)
+    switch on the kernels' optional terms."""
+    p = params(64, 32, 24, a1=1.5, Da=0.3, Db=0.2)
+    f = pyoracle.initial3(p, 8.0, 0.5, 2, 5.0, 6)
+    out = run_gpu(p, f, 40, dtype=dtype)
+    ref = pyoracle.run3(p, f, 40)
+    assert maxdiff(out, ref) <= tol
+
+
 def test_mass_reduction():
     p = params(64, 48, 30)
     f = pyoracle.initial3(p, 10.0, 0.5, 3, 6.0, 2)
