@@ -15,7 +15,7 @@
 // columns x BY+2 rows of phi1, phi2 and c) arrives by one 3D TMA box per
 // field into a four-slot ring; the load of plane z+2 is in flight while plane
 // z is computed.  mu of each plane (tile plus x/y halo) is computed once into
-// a three-slot ring.  Outputs go straight to global memory (32 consecutive x
+// a four-slot ring.  Outputs go straight to global memory (32 consecutive x
 // per warp), and each output that a ghost cell images (x = 1, nx-2; y = 1,
 // ny-2; z = 1, nz-2) is written to its ghost cells too, which is what the
 // reference's boundary kernels leave there.
@@ -31,7 +31,7 @@ namespace {
 constexpr int kP3Threads = 256;
 constexpr int kP3BY = 16;            // output rows of a CTA
 constexpr int kP3Slots = 4;          // input plane ring
-constexpr int kP3MuSlots = 3;        // mu plane ring
+constexpr int kP3MuSlots = 4;        // mu plane ring
 constexpr uint32_t kP3WaitLimit = 1u << 22;
 
 template <typename R>
@@ -82,7 +82,7 @@ K3<R> make_k3(const rs3_params &p) {
   k.nx = p.nx;
   k.ny = p.ny;
   k.nz = p.nz;
-  k.z_chunk = p.z_chunk > 0 ? p.z_chunk : 64;
+  k.z_chunk = p.z_chunk > 0 ? p.z_chunk : 32;
   k.dt = (R)p.dt;
   k.dxi = (R)p.dx_inv;
   k.dyi = (R)p.dy_inv;
@@ -208,9 +208,16 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
   const R third = R(1) / R(3);
 
   for (int z = zo0; z < zo1; ++z) {
+    // one barrier per plane: after it every thread has finished plane z-1,
+    // so the input slot of plane z-2 takes the load of plane z+2 (mu has
+    // four slots: mu(z+1) overwrites mu(z-3))
     if (!__syncthreads_and(mu_plane(z + 1))) {
       drain(z + 1);
       return;
+    }
+    if (z + 2 <= zin1 && z + 2 > issued) {
+      if (tid == 0) issue(z + 2);
+      issued = z + 2;
     }
     const int q = z - zin0;
     const R *c1 = sm.in[q % kP3Slots][0], *c2 = sm.in[q % kP3Slots][1], *cc = sm.in[q % kP3Slots][2];
@@ -305,11 +312,6 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
               }
         }
       }
-    }
-    __syncthreads();  // plane z-1's input and mu slots are free
-    if (z + 3 <= zin1) {
-      if (tid == 0) issue(z + 3);
-      issued = z + 3;
     }
   }
 }

@@ -23,7 +23,7 @@ namespace {
 constexpr int kX2Threads = 224;
 constexpr int kX2BX = 64, kX2BXin = 72, kX2BY = 14, kX2BYin = 16;
 constexpr int kX2Plane = kX2BXin * kX2BYin;  // 1152 floats = 4608 bytes (36 x 128)
-constexpr int kX2Slots = 4, kX2MuSlots = 3;
+constexpr int kX2Slots = 4, kX2MuSlots = 4;
 constexpr uint32_t kX2WaitLimit = 1u << 22;
 static_assert((kX2Plane * 4) % 128 == 0, "TMA destinations stay 128-byte aligned");
 static_assert(kX2Threads == 32 * (kX2BY / 2) && kX2BX == 64, "a warp per row pair, a lane per column pair");
@@ -179,9 +179,16 @@ __global__ void __launch_bounds__(kX2Threads, 3)
   const bool xedge = !(v0 && v1) || gx == 1 || gx + 1 == k.nx - 2;  // a ghost column is involved
 
   for (int z = zo0; z < zo1; ++z) {
+    // one barrier per plane: after it every thread has finished plane z-1,
+    // so the input slot of plane z-2 takes the load of plane z+2 (mu has
+    // four slots: mu(z+1) overwrites mu(z-3))
     if (!__syncthreads_and(mu_plane(z + 1))) {
       drain(z + 1);
       return;
+    }
+    if (z + 2 <= zin1 && z + 2 > issued) {
+      if (tid == 0) issue(z + 2);
+      issued = z + 2;
     }
     const int q = z - zin0;
     const float *c1 = sm.in[q % kX2Slots][0], *c2 = sm.in[q % kX2Slots][1], *cc = sm.in[q % kX2Slots][2];
@@ -317,11 +324,6 @@ __global__ void __launch_bounds__(kX2Threads, 3)
         }
       }
     }
-    __syncthreads();  // plane z-1's input and mu slots are free
-    if (z + 3 <= zin1) {
-      if (tid == 0) issue(z + 3);
-      issued = z + 3;
-    }
   }
 }
 
@@ -336,7 +338,7 @@ int launch_peri3d_step_x2(const rs3_params &p, const P3Maps &m, float *o1, float
   k.nx = p.nx;
   k.ny = p.ny;
   k.nz = p.nz;
-  k.z_chunk = p.z_chunk > 0 ? p.z_chunk : 64;
+  k.z_chunk = p.z_chunk > 0 ? p.z_chunk : 32;
   k.a1 = (float)p.a1;
   k.a2 = (float)p.a2;
   k.a3 = (float)p.a3;

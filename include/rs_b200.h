@@ -365,7 +365,7 @@ int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choic
  * G_T = 0 is the reference's isothermal model. */
 typedef struct rs3_params {
   int32_t nx, ny, nz;               /* extents incl. ghost layers (TiAg Nx, Ny, devNz) */
-  int32_t z_chunk;                  /* planes per CTA of the z march (0: 64) */
+  int32_t z_chunk;                  /* planes per CTA of the z march (0: 32) */
   double dt;                        /* DT */
   double dx_inv, dy_inv, dz_inv;    /* DXin, DYin, DZin */
   double a1, a2, a3, b;             /* three-phase well terms */
