@@ -214,6 +214,12 @@ int rs3_initial(rs3_ctx *c, const rs3_fields *f, double z_front, double amp, int
   return launched("rs3_initial");
 }
 
+int rs3_c_offset(const rs3_params *p, double *out) {
+  if (!p || !out) return bad(RS_E_INVALID, "rs3_c_offset: null");
+  *out = rs::peri3d_c_offset(*p);
+  return RS_OK;
+}
+
 int rs3_device_status(rs3_ctx *c, rs_stream_t stream) {
   if (!c) return bad(RS_E_INVALID, "rs3_device_status: null");
   int h = 0;

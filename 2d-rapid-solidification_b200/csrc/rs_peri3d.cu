@@ -317,10 +317,11 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
 }
 
 // mu of every cell with image ghost layers (rs3_mu)
+// (FP32 sets hold c - c_off: c_off is added back here and in the mass)
 template <typename R>
 __global__ void __launch_bounds__(256) peri3d_mu_kernel(const K3<R> k, const R *__restrict__ f1,
                                                         const R *__restrict__ f2, const R *__restrict__ fc,
-                                                        R *__restrict__ mu) {
+                                                        R *__restrict__ mu, const double c_off) {
   const int64_t n = (int64_t)k.nx * k.ny * k.nz;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     int x = (int)(i % k.nx), y = (int)((i / k.nx) % k.ny), z = (int)(i / ((int64_t)k.nx * k.ny));
@@ -329,18 +330,18 @@ __global__ void __launch_bounds__(256) peri3d_mu_kernel(const K3<R> k, const R *
     y = y == 0 ? k.ny - 2 : (y == k.ny - 1 ? 1 : y);
     z = z == 0 ? 1 : (z == k.nz - 1 ? k.nz - 2 : z);
     const int64_t j = ((int64_t)z * k.ny + y) * k.nx + x;
-    mu[i] = mu_of(k, f1[j], f2[j], fc[j]);
+    mu[i] = (R)((double)mu_of(k, f1[j], f2[j], fc[j]) + c_off);
   }
 }
 
 template <typename R>
 __global__ void __launch_bounds__(256) peri3d_mass_kernel(const K3<R> k, const R *__restrict__ fc,
-                                                          double *__restrict__ partial) {
+                                                          double *__restrict__ partial, const double c_off) {
   double s = 0.0;
   const int64_t nxi = k.nx - 2, nyi = k.ny - 2, n = nxi * nyi * (k.nz - 2);
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t x = 1 + i % nxi, y = 1 + (i / nxi) % nyi, z = 1 + i / (nxi * nyi);
-    s += (double)fc[(z * k.ny + y) * k.nx + x];
+    s += (double)fc[(z * k.ny + y) * k.nx + x] + c_off;
   }
   __shared__ double sh[8];
 #pragma unroll
@@ -365,7 +366,7 @@ __global__ void peri3d_sum_kernel(const double *__restrict__ partial, int n, dou
 // initial state (rs3_initial); one thread per (x, y) column of the interior
 template <typename R>
 __global__ void peri3d_init_kernel(const K3<R> k, const P3Init ini, R *__restrict__ f1, R *__restrict__ f2,
-                                   R *__restrict__ fc) {
+                                   R *__restrict__ fc, const double c_off) {
   const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x, y = 1 + blockIdx.y;
   if (x > k.nx - 2 || y > k.ny - 2) return;
   uint32_t r[4] = {(uint32_t)x, (uint32_t)y, 0u, 0x5A465254u};
@@ -383,15 +384,15 @@ __global__ void peri3d_init_kernel(const K3<R> k, const P3Init ini, R *__restric
     if (cap) {
       f1[o] = R(0);
       f2[o] = R(1);
-      fc[o] = (R)ini.ca;
+      fc[o] = (R)(ini.ca - c_off);
     } else if (z < zc) {
       f1[o] = R(0);
       f2[o] = R(0);
-      fc[o] = (R)ini.cb;
+      fc[o] = (R)(ini.cb - c_off);
     } else {
       f1[o] = R(1);
       f2[o] = R(0);
-      fc[o] = (R)ini.clb;
+      fc[o] = (R)(ini.clb - c_off);
     }
   }
 }
@@ -453,6 +454,11 @@ int launch_step(const rs3_params &p, const P3Maps &m, R *o1, R *o2, R *oc, int64
 
 }  // namespace
 
+double peri3d_c_offset(const rs3_params &p) {  // clb at T_ref (TiAg.cu:67)
+  const double B1 = p.B11 + p.B12 * p.T_ref, B2 = p.B21 + p.B22 * p.T_ref;
+  return (B1 - 0.5 * B2) / (p.A1 - 0.5 * p.A2) + p.A1;
+}
+
 int peri3d_box_width(int precision) { return precision == RS_F64 ? P3Cfg<double>::BXin : peri3d_x2_box_width(); }
 int peri3d_box_height(int precision) { return precision == RS_F64 ? kP3BY + 2 : peri3d_x2_box_height(); }
 
@@ -469,19 +475,20 @@ int launch_peri3d_mu(const rs3_params &p, int precision, const void *f1, const v
   const unsigned blocks = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
   if (precision == RS_F64)
     peri3d_mu_kernel<double><<<blocks, 256, 0, st>>>(make_k3<double>(p), (const double *)f1, (const double *)f2,
-                                                     (const double *)fc, (double *)mu);
+                                                     (const double *)fc, (double *)mu, 0.0);
   else
     peri3d_mu_kernel<float><<<blocks, 256, 0, st>>>(make_k3<float>(p), (const float *)f1, (const float *)f2,
-                                                    (const float *)fc, (float *)mu);
+                                                    (const float *)fc, (float *)mu, peri3d_c_offset(p));
   return 0;
 }
 
 int launch_peri3d_mass(const rs3_params &p, int precision, const void *fc, double *partial, int nparts, double *out,
                        cudaStream_t st) {
   if (precision == RS_F64)
-    peri3d_mass_kernel<double><<<nparts, 256, 0, st>>>(make_k3<double>(p), (const double *)fc, partial);
+    peri3d_mass_kernel<double><<<nparts, 256, 0, st>>>(make_k3<double>(p), (const double *)fc, partial, 0.0);
   else
-    peri3d_mass_kernel<float><<<nparts, 256, 0, st>>>(make_k3<float>(p), (const float *)fc, partial);
+    peri3d_mass_kernel<float><<<nparts, 256, 0, st>>>(make_k3<float>(p), (const float *)fc, partial,
+                                                      peri3d_c_offset(p));
   peri3d_sum_kernel<<<1, 32, 0, st>>>(partial, nparts, out);
   return 0;
 }
@@ -490,9 +497,11 @@ int launch_peri3d_init(const rs3_params &p, int precision, const P3Init &ini, vo
                        cudaStream_t st) {
   const dim3 g((p.nx - 2 + 127) / 128, p.ny - 2);
   if (precision == RS_F64)
-    peri3d_init_kernel<double><<<g, 128, 0, st>>>(make_k3<double>(p), ini, (double *)f1, (double *)f2, (double *)fc);
+    peri3d_init_kernel<double><<<g, 128, 0, st>>>(make_k3<double>(p), ini, (double *)f1, (double *)f2, (double *)fc,
+                                                  0.0);
   else
-    peri3d_init_kernel<float><<<g, 128, 0, st>>>(make_k3<float>(p), ini, (float *)f1, (float *)f2, (float *)fc);
+    peri3d_init_kernel<float><<<g, 128, 0, st>>>(make_k3<float>(p), ini, (float *)f1, (float *)f2, (float *)fc,
+                                                 peri3d_c_offset(p));
   const int ext[3][2] = {{p.ny, p.nz}, {p.nx, p.nz}, {p.nx, p.ny}};
   for (int axis = 0; axis < 3; ++axis) {
     const dim3 gg((ext[axis][0] + 127) / 128, ext[axis][1]);

@@ -24,6 +24,7 @@ struct P3Init {
   double cx[kP3MaxCaps], cy[kP3MaxCaps];
 };
 
+double peri3d_c_offset(const rs3_params &p);  // FP32 sets hold c - this
 int peri3d_box_width(int precision);
 int peri3d_box_height(int precision);
 int peri3d_x2_box_width();

@@ -7,6 +7,11 @@
 // memory instructions of the scalar form, each lane rounded exactly as the
 // scalar FP32 operation.
 //
+// Field storage: an FP32 set holds c - c_off (c_off = clb, the melt's
+// composition at T_ref, rs3_c_offset), so that the small solute updates of
+// the melt are not lost below ulp(c); mu is carried as mu - c_off (only its
+// differences and s_i - r_i mu enter), with c_off folded into the s_i.
+//
 // Tile: output cells x0 .. x0+63 (x0 a multiple of 64, pairs start on even
 // x), rows y0+1 .. y0+14.  Input box per field and plane: x0-4 .. x0+67
 // (72 columns, TMA x 16-byte aligned) x y0 .. y0+15 (16 rows).  224 threads:
@@ -82,6 +87,7 @@ struct X2K {
   float r1, r2, r3;
   float dt, dt3, dxi2, dyi2, dzi2, cfx, cfy, cfz;
   double B11, B12, B21, B22, T_ref, G_T, V_T, z_T;
+  double r1d, r2d, r3d, c_off;  // r_i in FP64 and the storage offset of c
 };
 
 // mu = c - sum r_i g_i (TiAg.cu:461-470), with
@@ -197,7 +203,9 @@ __global__ void __launch_bounds__(kX2Threads, 3)
     const float *mu = sm.mu[q % kX2MuSlots], *mud = sm.mu[(q - 1) % kX2MuSlots], *muu = sm.mu[(q + 1) % kX2MuSlots];
     const double Tz = k.G_T == 0.0 ? k.T_ref : k.T_ref + k.G_T * ((double)z - k.z_T - k.V_T * (double)step);
     const double B1 = k.B11 + k.B12 * Tz, B2 = k.B21 + k.B22 * Tz;
-    const f2 s1 = bc((float)B1), s2 = bc((float)(-B1 - B2)), s3 = bc((float)(-B1 + B2));
+    // s_i - r_i c_off: the fields hold c - c_off, so mu - c_off is what mu2 returns
+    const f2 s1 = bc((float)(B1 - k.r1d * k.c_off)), s2 = bc((float)(-B1 - B2 - k.r2d * k.c_off)),
+             s3 = bc((float)(-B1 + B2 - k.r3d * k.c_off));
     const int zg = z == 1 ? 0 : (z == k.nz - 2 ? k.nz - 1 : -1);
     if (any) {
       // column window rows ry-1 .. ry+2 of phi1, phi2, mu (pairs)
@@ -365,6 +373,10 @@ int launch_peri3d_step_x2(const rs3_params &p, const P3Maps &m, float *o1, float
   k.G_T = p.G_T;
   k.V_T = p.V_T;
   k.z_T = p.z_T;
+  k.r1d = p.A1;
+  k.r2d = -p.A1 - p.A2;
+  k.r3d = -p.A1 + p.A2;
+  k.c_off = peri3d_c_offset(p);
   const bool a1 = p.a1 != 0.0, sd = p.Da != 0.0 || p.Db != 0.0;
   auto kfn = a1 ? (sd ? peri3d_x2_kernel<true, true> : peri3d_x2_kernel<true, false>)
                 : (sd ? peri3d_x2_kernel<false, true> : peri3d_x2_kernel<false, false>);

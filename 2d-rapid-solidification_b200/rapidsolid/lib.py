@@ -90,6 +90,7 @@ def load():
         "rs3_mass": ([vp, vp, vp, vp], C.c_int),
         "rs3_initial": ([vp, vp, C.c_double, C.c_double, i32, C.c_double, C.c_uint64, vp], C.c_int),
         "rs3_device_status": ([vp, vp], C.c_int),
+        "rs3_c_offset": ([vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -368,8 +369,16 @@ def default_params3():
     return p
 
 
+def c_offset3(p):
+    """The offset of c in FP32 3D sets (rs3_c_offset): they hold c - this."""
+    v = C.c_double()
+    check(load().rs3_c_offset(C.byref(p), C.byref(v)))
+    return v.value
+
+
 class FieldSet3:
-    """3D device field set: phi1, phi2, c as (nz, ny, nx) tensors."""
+    """3D device field set: phi1, phi2, c as (nz, ny, nx) tensors; float32
+    sets hold c - c_offset3(p) in c (see include/rs_b200.h)."""
 
     def __init__(self, p, dtype, device="cuda"):
         import torch

@@ -284,6 +284,9 @@ def run_ours(args):
         line["fp32_exact_vs_fp64_exact"] = round(value / fp64["value"], 3)
         line["surrogate"] = surrogate_leg(p, flush, value, fp64["value"])
         line["ensemble"] = ensemble_leg(flush)
+        del flush
+        torch.cuda.empty_cache()
+        line["peritectic_3d"] = peritectic_3d_leg(peak)
     ctx.close()
     if dist:
         dist.barrier()
@@ -406,6 +409,93 @@ def surrogate_leg(p, flush, fp32_value, fp64_value, nsteps=30):
             "note": "3->32->32->2 SiLU, FP16 mma.sync hidden layers; the network evaluates every cell that is "
                     "not bulk melt (the melt keeps its exact series form); exact fallback out of box and "
                     "1/1024 audit"}
+
+
+def peritectic_3d_leg(peak, nsteps_run=5000, ntimed=10):
+    """The 3D three-phase variant (the reference's TiAg.cu model) on one GPU:
+    512 x 512 x 1024 FP32 with a frozen gradient (G = 2e6 K/m, V = 0.2 m/s),
+    beta front at z = 24 +- 0.5 dx with four alpha caps.  Step time by CUDA
+    events (three fields of 1 GiB each per set: far beyond L2, no flush),
+    roofline against 24 algorithmic bytes per cell-step, the whole run's time
+    and solute drift; the FP64 kernel at the reference's own 512 x 512 x 128."""
+    import torch
+    from rapidsolid import configs, lib
+    out = {}
+    p = configs.peritectic_3d()
+    cells = (p.nx - 2) * (p.ny - 2) * (p.nz - 2)
+    ctx = lib.Context3(p)
+    a, b = lib.FieldSet3(p, torch.float32), lib.FieldSet3(p, torch.float32)
+    ctx.initial(a, **configs.IC3)
+    m = torch.zeros(2, dtype=torch.float64, device="cuda")
+    ctx.mass(a, m[0:1])
+    for k in range(3):
+        ctx.step(a, b, k)
+        a, b = b, a
+    ts = []
+    for k in range(3, 3 + ntimed):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.step(a, b, k)
+        e1.record()
+        a, b = b, a
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = sorted(ts)[len(ts) // 2]
+    # the whole run: nsteps_run steps from the initial state
+    ctx.initial(a, **configs.IC3)
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record()
+    for k in range(nsteps_run):
+        ctx.step(a, b, k)
+        a, b = b, a
+    r1.record()
+    ctx.mass(a, m[1:2])
+    torch.cuda.synchronize()
+    ctx.device_status()
+    run_ms = r0.elapsed_time(r1)
+    m0, m1 = m.tolist()
+    alg = 24 * cells
+    achieved = alg / (ms * 1e-3) / 1e9
+    out["fp32"] = {"value": round(cells / (ms * 1e-3) / 1e9, 3), "unit": "Gcell-steps/s", "ms_per_step": round(ms, 4),
+                   "grid": [p.nx, p.ny, p.nz], "interior_cells": cells,
+                   "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                                "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": alg,
+                                "kernel": "rs::peri3d_x2_kernel"},
+                   "run": {"steps": nsteps_run, "ms": round(run_ms, 1),
+                           "gcell_steps_s": round(cells * nsteps_run / (run_ms * 1e-3) / 1e9, 3),
+                           "solute_drift_rel": (m1 - m0) / m0},
+                   "G_T_per_cell": p.G_T, "V_T_cells_per_step": p.V_T}
+    ctx.close()
+    del a, b
+    torch.cuda.empty_cache()
+    q = configs.peritectic_3d(nz=128)
+    q.G_T = q.V_T = 0.0
+    cells = (q.nx - 2) * (q.ny - 2) * (q.nz - 2)
+    ctx = lib.Context3(q)
+    a, b = lib.FieldSet3(q, torch.float64), lib.FieldSet3(q, torch.float64)
+    ctx.initial(a, 100.0, 0.5, 4, 30.0, 5)
+    for k in range(3):
+        ctx.step(a, b, k)
+        a, b = b, a
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(3, 3 + ntimed):
+        ctx.step(a, b, k)
+        a, b = b, a
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / ntimed
+    achieved = 48 * cells / (ms * 1e-3) / 1e9
+    out["fp64_reference_size"] = {"value": round(cells / (ms * 1e-3) / 1e9, 3), "unit": "Gcell-steps/s",
+                                  "ms_per_step": round(ms, 4), "grid": [q.nx, q.ny, q.nz],
+                                  "roofline_frac": round(achieved / peak, 4), "kernel": "rs::peri3d_kernel<double>",
+                                  "note": "isothermal, the reference's Nx x Ny x devNz; its own kernels are timed "
+                                          "by the reference arm (bench.py --impl reference)"}
+    ctx.close()
+    out["note"] = ("one fused launch per step (computeMu + boundaryMu + diffuse + boundary of TiAg.cu); "
+                   "no CALPHAD in this model, so no surrogate path")
+    return out
 
 
 def ensemble_leg(flush, nruns=64, nsteps=100):

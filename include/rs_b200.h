@@ -377,7 +377,10 @@ typedef struct rs3_params {
   double z_T;                       /* plane where T = T_ref at step 0 */
 } rs3_params;
 
-/* A 3D field set on the device (nx * ny * nz elements each, 16-byte aligned). */
+/* A 3D field set on the device (nx * ny * nz elements each, 16-byte aligned).
+ * RS_F64 sets hold c itself; RS_F32 sets hold c - rs3_c_offset() (the melt's
+ * composition clb at T_ref), which keeps the melt's small solute updates
+ * above FP32 rounding.  rs3_mu and rs3_mass return true mu and sum c. */
 typedef struct rs3_fields {
   void *phi1;
   void *phi2;
@@ -409,6 +412,8 @@ int rs3_mass(rs3_ctx *ctx, const rs3_fields *f, double *d_mass, rs_stream_t stre
  * cb, clb): beta cb, alpha ca, liquid clb.  Ghost layers are images. */
 int rs3_initial(rs3_ctx *ctx, const rs3_fields *f, double z_front, double amp, int32_t n_alpha,
                 double cap_radius, uint64_t seed, rs_stream_t stream);
+/* the offset of c in RS_F32 sets: clb at T_ref (TiAg.cu:67) */
+int rs3_c_offset(const rs3_params *p, double *out);
 /* RS_E_STATE if a step kernel's bounded wait for a plane load gave up */
 int rs3_device_status(rs3_ctx *ctx, rs_stream_t stream);
 
