@@ -1,6 +1,7 @@
 """Run a named workload through the C-ABI for a number of steps.
 
     python -m rapidsolid.run --config scale_fp32 --precision f32 --steps 8
+    python -m rapidsolid.run --config peritectic_3d --nz 256 --steps 3
     (from 2d-rapid-solidification_b200/, or with it on PYTHONPATH)
 
 Used for profiling: every step is one rs_step launch on the whole grid,
@@ -17,12 +18,15 @@ from . import _abi, configs, lib
 def main(argv=None):
     import torch
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--config", default="scale_fp32", choices=["plain_small", "scale_fp32"])
+    ap.add_argument("--config", default="scale_fp32", choices=["plain_small", "scale_fp32", "peritectic_3d"])
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--grid", type=int, default=0, help="override Nx_all = Ny_all")
     ap.add_argument("--no-tma", action="store_true", help="use the register-prefetch kernel")
+    ap.add_argument("--nz", type=int, default=0, help="3D: override the number of z planes")
     a = ap.parse_args(argv)
+    if a.config == "peritectic_3d":
+        return run3(a)
     p = getattr(configs, a.config)()
     if a.grid:
         p.nx_all = p.ny_all = a.grid
@@ -50,6 +54,25 @@ def main(argv=None):
     ctx.device_status()
     print(f"{a.config} {a.precision} grid {p.nx_all}x{p.ny_all}: {a.steps} steps, "
           f"solute mass {mass.item():.12g}")
+    return 0
+
+
+def run3(a):
+    """The 3D three-phase workload: rs3_initial, then a.steps rs3_step launches."""
+    import torch
+    p = configs.peritectic_3d(nz=a.nz) if a.nz else configs.peritectic_3d()
+    ctx = lib.Context3(p)
+    dt = torch.float64 if a.precision == "f64" else torch.float32
+    cur, nxt = lib.FieldSet3(p, dt), lib.FieldSet3(p, dt)
+    ctx.initial(cur, **configs.IC3)
+    for n in range(a.steps):
+        ctx.step(cur, nxt, n)
+        cur, nxt = nxt, cur
+    mass = torch.zeros(1, dtype=torch.float64, device="cuda")
+    ctx.mass(cur, mass)
+    torch.cuda.synchronize()
+    ctx.device_status()
+    print(f"peritectic_3d {a.precision} grid {p.nx}x{p.ny}x{p.nz}: {a.steps} steps, solute mass {mass.item():.12g}")
     return 0
 
 

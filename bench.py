@@ -490,8 +490,8 @@ def peritectic_3d_leg(peak, nsteps_run=5000, ntimed=10):
     out["fp64_reference_size"] = {"value": round(cells / (ms * 1e-3) / 1e9, 3), "unit": "Gcell-steps/s",
                                   "ms_per_step": round(ms, 4), "grid": [q.nx, q.ny, q.nz],
                                   "roofline_frac": round(achieved / peak, 4), "kernel": "rs::peri3d_kernel<double>",
-                                  "note": "isothermal, the reference's Nx x Ny x devNz; its own kernels are timed "
-                                          "by the reference arm (bench.py --impl reference)"}
+                                  "note": "isothermal, the reference's Nx x Ny x devNz; the reference arm "
+                                          "(bench.py --impl reference) times its own kernels at this size"}
     ctx.close()
     out["note"] = ("one fused launch per step (computeMu + boundaryMu + diffuse + boundary of TiAg.cu); "
                    "no CALPHAD in this model, so no surrogate path")
@@ -542,7 +542,7 @@ def ensemble_leg(flush, nruns=64, nsteps=100):
             "one_by_one": {"value": round(cells / (ms_single * 1e-3) / 1e9, 3), "ms_per_step": round(ms_single, 5)},
             "autotune": {"choice": ["run by run", "largest first", "interleaved"][choice],
                          "ms_per_launch": [round(x, 5) for x in tune_ms]},
-            "note": "FP32 exact path (the surrogate is slower and less accurate, see its leg); CUDA graph "
+            "note": "FP32 exact path (the surrogate is slower, see its leg); CUDA graph "
                     "replays between pull-backs; every run equals its single run bit for bit (tests)"}
 
 
@@ -609,7 +609,37 @@ def run_reference(args):
             "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample, "cpu": _cpu_model()},
             "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    gpu = _reference_kernels_gpu(pyoracle)
+    if gpu:
+        line["reference_kernels_b200"] = gpu
     print(json.dumps(line))
+
+
+def _reference_kernels_gpu(pyoracle):
+    """The reference's own CUDA kernels, built from its sources into
+    oracle/_ref/ (FP64): the 2D step (compute_phi, compute_psi,
+    compute_c_CALPHAD at 2048 x 2048) and the 3D step (TiAg.cu computeMu,
+    boundaryMu, diffuse, boundary at its own 512 x 512 x 128).  Reported
+    beside the CPU arm; skipped without a GPU or without the binaries."""
+    import subprocess
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except ImportError:
+        return None
+    out = {}
+    for key, args in (("fp64_2d_2048", ["ref_harness_2048", "bench", "100", "0.144"]),
+                      ("fp64_3d_512x512x128", ["ref3_harness_512", "bench", "10"])):
+        binary = pyoracle.ref_binary(args[0])
+        if not os.path.exists(binary):
+            continue
+        try:
+            r = subprocess.run([binary] + args[1:], capture_output=True, text=True, timeout=300, check=True)
+            out[key] = json.loads(r.stdout.strip().splitlines()[-1])
+        except (subprocess.SubprocessError, ValueError, IndexError) as e:
+            out[key] = {"error": str(e)[:200]}
+    return out or None
 
 
 def main():
