@@ -348,10 +348,10 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       }
     }
   }
-  // halo columns x0-1 and x0+kW, one thread per cell (surrogate: warp 0
-  // alone, then the same network pass as the rows)
-  // (exact path: warps 2 and 3, which have one input row fewer than warps 0 and 1)
-  if (SURR ? warp == 0 : (threadIdx.x >= 64 && threadIdx.x < 64 + 2 * kTRin)) {
+  // halo columns x0-1 and x0+kW, one thread per cell, on warps 2 and 3, which
+  // have one input row fewer than warps 0 and 1 (surrogate: warp 3 alone,
+  // then the same network pass as the rows)
+  if (SURR ? warp == 3 : (threadIdx.x >= 64 && threadIdx.x < 64 + 2 * kTRin)) {
    for (int i = SURR ? lane : (int)threadIdx.x - 64; i < 2 * kTRin; i += 32) {
     const int rr = i >> 1, side = i & 1;
     const int x = side ? kHaloR : kHaloL, g = x0 - 4 + x;
