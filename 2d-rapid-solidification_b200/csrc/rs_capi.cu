@@ -70,6 +70,7 @@ struct rs_ctx {
   float *mlp_w;        // its FP32 parameters (device)
   uint16_t *mlp_b16;   // FP16 W2 (32 x 32) and W3 padded to 8 rows (device)
   unsigned long long *mlp_audit;  // max error bits of mu'' and dG, fallback and audit counts
+  unsigned int *red_counter;  // fused final reduction of the FP32 tile kernel (device, 0 between launches)
   int use_tma;         // RS_OPT_TMA
   TmaEntry tma[8];     // tensor-map cache keyed by field pointer
   int tma_n, tma_next;
@@ -335,6 +336,8 @@ int rs_create(const rs_params *p, rs_ctx **out) {
   if (e == cudaSuccess) e = cudaMalloc(&c->row_g, sizeof(double) * p->ny_all);
   if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&c->red_counter, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(c->red_counter, 0, sizeof(unsigned int));
   c->col_tab_len = rs::col_tab_len(p->nx_all);
   if (e == cudaSuccess) e = cudaMalloc(&c->col_tab, sizeof(float) * rs::kColTabFields * c->col_tab_len);
   c->use_tma = 1;
@@ -353,6 +356,7 @@ int rs_destroy(rs_ctx *c) {
   cudaFree(c->row_f);
   cudaFree(c->row_g);
   cudaFree(c->d_err);
+  cudaFree(c->red_counter);
   cudaFree(c->col_tab);
   cudaFree(c->mlp_w);
   cudaFree(c->mlp_b16);
@@ -426,6 +430,13 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
     tm.col_tab = c->col_tab;
     tm.col_tab_len = c->col_tab_len;
     tm.surr = c->surr.w ? &c->surr : nullptr;
+    tm.red = {};
+    if (red && cur->precision == RS_F32) {
+      tm.red.counter = c->red_counter;
+      tm.red.mass_offset = (double)(c->p.nx_all - 2) * (c->p.ny_all - 2) * c->p.cinf;
+      tm.red.mass_out = a->mass_out;
+      tm.red.itip_out = a->itip_out;
+    }
     tmp = &tm;
   }
   if (cur->precision == RS_F64)
@@ -439,7 +450,8 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
   if (lr == -3) return fail(RS_E_CUDA, "rs_step: cannot configure shared memory of the TMA kernel");
   if (lr) return fail(RS_E_INVALID, "rs_step: grid too large for the reduction workspace");
   if ((rc = cuda_check("rs_step"))) return rc;
-  if (red) {
+  // (the FP32 tile kernel reduces its partials itself)
+  if (red && !(tmp && cur->precision == RS_F32)) {
     const double off = cur->precision == RS_F32 ? (double)(c->p.nx_all - 2) * (c->p.ny_all - 2) * c->p.cinf : 0.0;
     rs::launch_reduce_partials(c->partials, nb, off, a->mass_out, a->itip_out, st);
     if ((rc = cuda_check("rs_step reduce"))) return rc;
@@ -467,6 +479,7 @@ int rs_device_status(rs_ctx *c, rs_stream_t stream) {
     return cuda_check("rs_device_status");
   if (h) {
     cudaMemsetAsync(c->d_err, 0, sizeof(int), st);
+    cudaMemsetAsync(c->red_counter, 0, sizeof(unsigned int), st);  // an aborted launch may have left it counting
     return fail(RS_E_STATE, "a device-side wait gave up (pipeline stalled); results of the affected steps are invalid");
   }
   return RS_OK;

@@ -47,12 +47,24 @@ __device__ __forceinline__ void block_partial(double mass, int itip, BlockPartia
 // Inputs of the TMA-staged FP32 kernel: descriptors of the current psi and c
 // fields (built on the host) and the context's per-column table workspace.
 struct SurrArgs;
+// Final reduction of the per-tile partials fused into the tile kernel: the
+// last CTA to finish (a counter in device memory, reset by that CTA) sums
+// them in the order of reduce_partials_kernel.  counter == nullptr: none.
+struct FinalRed {
+  unsigned int *counter;
+  const BlockPartial *partials;
+  int nparts;
+  double mass_offset;
+  double *mass_out;
+  int32_t *itip_out;
+};
 struct TmaMaps {
   CUtensorMap psi;
   CUtensorMap c;
   float *col_tab;   // kColTabFields arrays of col_tab_len floats
   int col_tab_len;
   const SurrArgs *surr;  // learned CALPHAD surrogate, or nullptr (exact)
+  FinalRed red;          // counter, offset and outputs (partials, nparts set by the launcher)
 };
 constexpr int kTileOutW = 128;                  // output columns of an FP32 tile
 constexpr int kTmaBoxW32 = kTileOutW + 8;        // input columns (4 each side keep x 16-byte aligned)

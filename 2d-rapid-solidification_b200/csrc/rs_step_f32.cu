@@ -82,6 +82,7 @@ struct alignas(128) TileSmem {
   double part_mass[kWarps];
   int part_itip[kWarps];
   uint64_t full;
+  int last;  // this CTA finished last (fused final reduction)
 };
 
 static_assert(offsetof(TileSmem, psi) % 128 == 0 && offsetof(TileSmem, d) % 128 == 0,
@@ -156,7 +157,8 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
                                           const CUtensorMap *tm_psi, const CUtensorMap *tm_c,
                                           const float *__restrict__ tab, const int tab_len, float *__restrict__ psi_n,
                                           float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *part,
-                                          int *err, const SurrArgs &SA, const int tr, const int tc) {
+                                          int *err, const SurrArgs &SA, const int tr, const int tc,
+                                          const FinalRed *FR) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -665,6 +667,41 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       b.pad = 0;
       *part = b;
     }
+    if (FR) {  // the last CTA to finish sums every partial (reduce_partials_kernel order)
+      if (threadIdx.x == 0) {
+        __threadfence();
+        sm.last = atomicAdd(FR->counter, 1u) == (unsigned)(FR->nparts - 1);
+      }
+      __syncthreads();
+      if (sm.last) {
+        __threadfence();
+        double *sm_m = reinterpret_cast<double *>(&sm.S[0][0]);  // S and mu are free now
+        int *sm_i = reinterpret_cast<int *>(&sm.mu[0][0]);
+        for (int v = threadIdx.x; v < 256; v += kThreads) {
+          double m = 0.0;
+          int it = 0;
+          for (int k = v; k < FR->nparts; k += 256) {
+            m += __ldcg(&FR->partials[k].mass);
+            it = max(it, __ldcg(&FR->partials[k].itip));
+          }
+          sm_m[v] = m;
+          sm_i[v] = it;
+        }
+        __syncthreads();
+        for (int sz = 128; sz > 0; sz >>= 1) {
+          for (int v = threadIdx.x; v < sz; v += kThreads) {
+            sm_m[v] += sm_m[v + sz];
+            sm_i[v] = max(sm_i[v], sm_i[v + sz]);
+          }
+          __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+          if (FR->mass_out) *FR->mass_out = sm_m[0] + FR->mass_offset;
+          if (FR->itip_out) *FR->itip_out = max(1, sm_i[0]);  // get_itip_all_grain starts at 1
+          *FR->counter = 0u;
+        }
+      }
+    }
   }
   // shared memory stays allocated until the copies have read it
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
@@ -676,10 +713,10 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
                 const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
                 const __grid_constant__ CUtensorMap tm_c, const float *__restrict__ tab, const int tab_len,
                 float *__restrict__ psi_n, float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *partials,
-                int *err, const __grid_constant__ SurrArgs SA) {
+                int *err, const __grid_constant__ SurrArgs SA, const __grid_constant__ FinalRed FR) {
   tile_body<SURR>(K, F, PS, &tm_psi, &tm_c, tab, tab_len, psi_n, c_n, phi_n,
                   partials ? partials + ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) : nullptr, err, SA, blockIdx.x,
-                  blockIdx.y);
+                  blockIdx.y, partials && FR.counter ? &FR : nullptr);
 }
 
 // ---------------------------------------------------------------- ensemble
@@ -716,7 +753,7 @@ __global__ void __launch_bounds__(kThreads, 5) ens_tile_kernel(const EnsRun *__r
   PS.d1 = R.d1;
   const SurrArgs none = {};
   tile_body<false>(R.K, R.F, PS, &R.map_psi[par], &R.map_c[par], R.tab, R.tab_len, R.psi[par ^ 1], R.c[par ^ 1],
-                   nullptr, nullptr, err, none, t % R.nrt, t / R.nrt);
+                   nullptr, nullptr, err, none, t % R.nrt, t / R.nrt, nullptr);
 }
 
 __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
@@ -775,8 +812,12 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   cfg.attrs = at;
   cfg.numAttrs = 1;
   const float *tab = tm.col_tab;
+  FinalRed fr = tm.red;
+  fr.partials = partials;
+  fr.nparts = nparts;
+  if (!partials || !(fr.mass_out || fr.itip_out)) fr.counter = nullptr;
   if (cudaLaunchKernelEx(&cfg, kfn, K, F, P, tm.psi, tm.c, tab, tm.col_tab_len, psi_n, c_n, phi_n, partials, err,
-                         sa) != cudaSuccess)
+                         sa, fr) != cudaSuccess)
     return -3;
   if (nparts_out) *nparts_out = nparts;
   return 0;
