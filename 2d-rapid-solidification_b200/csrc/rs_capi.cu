@@ -238,6 +238,8 @@ static int validate_params(const rs_params *p) {
     return fail(RS_E_INVALID, "non-positive material or grid constant");
   if (!(p->cinf > 0 && p->cinf < 1)) return fail(RS_E_INVALID, "cinf=%g outside (0,1)", p->cinf);
   if (p->tfc && p->ratio_dxT_dx < 1) return fail(RS_E_INVALID, "ratio_dxT_dx=%d", p->ratio_dxT_dx);
+  if (p->band && p->tfc) return fail(RS_E_UNSUPPORTED, "band mode: frozen temperature only");
+  if (p->band < 0 || p->band > 1 || p->j_offset < 0) return fail(RS_E_INVALID, "band=%d j_offset=%d", p->band, p->j_offset);
   for (int k = 0; k < 9; ++k)
     if (!std::isfinite(p->orientation[k])) return fail(RS_E_INVALID, "orientation[%d] not finite", k);
   return RS_OK;
@@ -248,8 +250,9 @@ static void make_coef(const rs_params *p, const rs_derived *d, rs::StepCoef *K, 
   K->nx = p->nx_all;
   K->ny = p->ny_all;
   K->pitch = p->nx_all;
-  K->jmin = p->periodic_j ? p->ny_all - 2 : 1;
-  K->jmax = p->periodic_j ? 1 : p->ny_all - 2;
+  K->jmin = p->band ? -1 : (p->periodic_j ? p->ny_all - 2 : 1);  // band: ghost rows come from the caller
+  K->jmax = p->band ? -1 : (p->periodic_j ? 1 : p->ny_all - 2);
+  K->j_offset = p->band ? p->j_offset : 0;
   K->one_eps = p->one_eps;
   K->tfc = p->tfc;
   K->ratio = p->ratio_dxT_dx;
@@ -523,6 +526,7 @@ int rs_mass(rs_ctx *c, const rs_fields *f, double *d_mass, rs_stream_t stream) {
 
 int rs_precise_tip(rs_ctx *c, const rs_fields *f, rs_tip *d_tip, rs_stream_t stream) {
   if (!c || !d_tip) return fail(RS_E_INVALID, "rs_precise_tip: null argument");
+  if (c->p.band) return fail(RS_E_UNSUPPORTED, "rs_precise_tip: needs the whole domain, not a band");
   int rc = check_fields(c, f, "rs_precise_tip", false);
   if (rc) return rc;
   rs::launch_precise_tip(f->precision, c->K, f->psi, c->row_last, c->row_f, c->row_g, d_tip, (cudaStream_t)stream);
@@ -801,7 +805,7 @@ int rs_ensemble_create(const rs_params *params, int32_t nruns, rs_ens **out) {
   if (!params || !out || nruns < 1 || nruns > 32767) return fail(RS_E_INVALID, "rs_ensemble_create: bad argument");
   *out = nullptr;
   for (int r = 0; r < nruns; ++r)
-    if (params[r].tfc || params[r].vp_ramp)
+    if (params[r].tfc || params[r].vp_ramp || params[r].band)
       return fail(RS_E_UNSUPPORTED, "rs_ensemble_create: run %d: the ensemble steps frozen-temperature runs "
                                     "without the Vp ramp", r);
   rs_ens *e = new (std::nothrow) rs_ens;

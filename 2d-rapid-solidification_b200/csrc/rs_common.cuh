@@ -168,7 +168,7 @@ struct StepCoef {
   uint32_t seed_lo, seed_hi;
   double W0, S;       // tip radius scale dx W0 S (fun.cu:2941)
   int32_t NyT_all;
-  int32_t reserved;
+  int32_t j_offset;   // band mode: global row of local row 0 (noise key); else 0
   // FP32 path: chemical potential relative to the melt composition
   double Lref;        // log(cinf / (1 - cinf))
 };

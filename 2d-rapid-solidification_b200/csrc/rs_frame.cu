@@ -398,6 +398,7 @@ extern "C" int rs_precise_tip_noalloc(const rs_params *p, const rs_fields *f, rs
   if (f->precision != RS_F64 && f->precision != RS_F32)
     return rs::set_error(RS_E_INVALID, "rs_precise_tip_noalloc: precision tag");
   if (p->nx_all < 8 || p->ny_all < 8) return rs::set_error(RS_E_INVALID, "rs_precise_tip_noalloc: grid below 8x8");
+  if (p->band) return rs::set_error(RS_E_UNSUPPORTED, "rs_precise_tip_noalloc: needs the whole domain, not a band");
   if (p->ny_all > RS_NOALLOC_TIP_MAX_ROWS)
     return rs::set_error(RS_E_INVALID, "rs_precise_tip_noalloc: ny_all exceeds RS_NOALLOC_TIP_MAX_ROWS");
   const int pitch = f->pitch ? f->pitch : p->nx_all;

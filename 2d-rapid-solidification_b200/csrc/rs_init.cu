@@ -49,7 +49,9 @@ __global__ void initial_planar_kernel(const StepCoef K, int itt, double c_l, dou
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= K.nx || j >= K.ny) return;
-  const int js = j == 0 ? K.jmin : (j == K.ny - 1 ? K.jmax : j);
+  // the row's draw: ghost rows take their image row's; in band mode every
+  // row, ghost rows included, takes its global row's
+  const int js = K.jmin < 0 ? j + K.j_offset : (j == 0 ? K.jmin : (j == K.ny - 1 ? K.jmax : j));
   uint32_t x[4] = {(uint32_t)js, 0u, 0u, 0x49434F46u};
   philox4x32(x, k0, k1);
   const double i0 = itt + (u53(x[0], x[1]) - 0.5);

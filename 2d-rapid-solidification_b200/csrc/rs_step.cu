@@ -48,6 +48,9 @@
 
 namespace rs {
 
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 // Per-lane state of a warp marching down a strip of 30 output columns, and
 // the work for one incoming row.
 template <typename R, bool TFC>
@@ -141,7 +144,9 @@ struct Strip {
     // flux through the face between rows row-1 and row (compute_c_CALPHAD
     // F01/F0m, fun.cu:1455-1459): weight (S00 + S01 + Shh + Snh)/4
     jv_lo = jv_hi;
-    jv_hi = (R(1.5) * (s1 + s2) + R(0.25) * ((sr1 + sr2) + (sl1 + sl2))) * (m2 - m1 + ku);
+    // face fluxes are rounded products: a contracted product would round a
+    // face differently at the end of a strip, and so depend on the tiling
+    jv_hi = mul_rn((R(1.5) * (s1 + s2) + R(0.25) * ((sr1 + sr2) + (sl1 + sl2))), (m2 - m1 + ku));
     if (k < 2) return;
 
     // ---- output row r = row - 1
@@ -159,7 +164,7 @@ struct Strip {
       R pn = p1 + Tr<R>::div(F.dt * ak, as * as) * term;
       if (F.noise_amp > R(0) && q > R(1.0e-3)) {
         uint32_t x[4];
-        noise_counter(x, PS.step, (int64_t)r * K.nx + gi);
+        noise_counter(x, PS.step, (int64_t)(r + K.j_offset) * K.nx + gi);
         philox4x32(x, K.seed_lo, K.seed_hi);
         pn += F.noise_amp * q * Tr<R>::normal(x);
       }
@@ -167,7 +172,7 @@ struct Strip {
     }
     // c: flux through the face (i+1/2, r) (F10/Fm0), weight (S00+S10+Shh+Shn)/4
     const R mr = __shfl_down_sync(FULL, m1, 1);
-    const R jh = (R(1.5) * (s1 + sr1) + R(0.25) * ((s2 + sr2) + (s0 + sr0))) * (mr - m1 + (TFC ? kr1 : dKr));
+    const R jh = mul_rn((R(1.5) * (s1 + sr1) + R(0.25) * ((s2 + sr2) + (s0 + sr0))), (mr - m1 + (TFC ? kr1 : dKr)));
     const R jh_left = __shfl_up_sync(FULL, jh, 1);
     const R dc = F.cflux * ((jh - jh_left) + (jv_hi - jv_lo));
     const R dn = fmax(d1 + dc, Tr<R>::kDelta ? F.c_floor - cinf : F.c_floor);  // floor, fun.cu:1464

@@ -232,7 +232,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const float T = SA.T_mid + in[0] / SA.T_ihalf, c = F.cinf + sm.d[rr][b];
     const bool inbox = T >= SA.T_lo && T <= SA.T_hi && c >= SA.c_lo && c <= SA.c_hi;
     const bool real = gx >= 0 && gx <= K.nx - 1;
-    const bool audit = real && surr_audit_cell(PS.step, (int64_t)(y0 - 1 + rr) * K.nx + gx);
+    const bool audit = real && surr_audit_cell(PS.step, (int64_t)(y0 - 1 + rr + K.j_offset) * K.nx + gx);
     const float mu_net = fmaf(o[0], SA.y_scale[0], SA.y_mean[0]);
     if (inbox && !audit) {
       sm.mu[rr][b] = mu_net;
@@ -427,7 +427,11 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     R.q[3] = R.s[2] + R.s[3];
     R.q[4] = R.s[3] + R.sr;
   };
-  // fluxes through the faces between rows A and B = A+1 (compute_c_CALPHAD F01/F0m)
+  // fluxes through the faces between rows A and B = A+1 (compute_c_CALPHAD
+  // F01/F0m).  Face fluxes are rounded products (__fmul_rn): a contracted
+  // product would round a face differently depending on where the face falls
+  // in a warp's rows, and so on the tiling (row bands must equal the whole
+  // domain bit for bit).
   auto vface = [&](const Row &A, const Row &B, float jv[4]) {
     float pp[6];
     pp[0] = A.sl + B.sl;
@@ -435,7 +439,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     for (int q = 0; q < 4; ++q) pp[q + 1] = A.s[q] + B.s[q];
     pp[5] = A.sr + B.sr;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) jv[q] = fmaf(6.f, pp[q + 1], pp[q] + pp[q + 2]) * (B.m[q] - A.m[q]);
+    for (int q = 0; q < 4; ++q) jv[q] = __fmul_rn(fmaf(6.f, pp[q + 1], pp[q] + pp[q + 2]), B.m[q] - A.m[q]);
   };
 
   const int rbase = 1 + kRowsPerWarp * warp;
@@ -455,7 +459,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const float mm[6] = {rb.ml, rb.m[0], rb.m[1], rb.m[2], rb.m[3], rb.mr};
     float jh[5];
 #pragma unroll
-    for (int f = 0; f < 5; ++f) jh[f] = fmaf(6.f, rb.q[f], ra.q[f] + rc.q[f]) * (mm[f + 1] - mm[f] + dKa[f]);
+    for (int f = 0; f < 5; ++f) jh[f] = __fmul_rn(fmaf(6.f, rb.q[f], ra.q[f] + rc.q[f]), mm[f + 1] - mm[f] + dKa[f]);
     const float4 dv4 = ld4(&sm.d[rr][bc]);
     const float dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
 #pragma unroll
@@ -558,13 +562,13 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       net_inputs(rr, x, in);
       const float T = SA.T_mid + in[0] / SA.T_ihalf;
       if (T >= SA.T_lo && T <= SA.T_hi && c00 >= SA.c_lo && c00 <= SA.c_hi &&
-          !surr_audit_cell(PS.step, (int64_t)r * K.nx + g))
+          !surr_audit_cell(PS.step, (int64_t)(r + K.j_offset) * K.nx + g))
         dG = sm.mu[rr][x];
     }
     const float res = phi_cell_dG<float>(
         &F, clamp1(sm.psi[rr][x]), clamp1(sm.psi[rr][x + 1]), clamp1(sm.psi[rr][x - 1]), clamp1(sm.psi[rr + 1][x]),
         clamp1(sm.psi[rr - 1][x]), clamp1(sm.psi[rr + 1][x + 1]), clamp1(sm.psi[rr + 1][x - 1]),
-        clamp1(sm.psi[rr - 1][x + 1]), clamp1(sm.psi[rr - 1][x - 1]), dG, PS.step, (int64_t)r * K.nx + g, K.seed_lo,
+        clamp1(sm.psi[rr - 1][x + 1]), clamp1(sm.psi[rr - 1][x - 1]), dG, PS.step, (int64_t)(r + K.j_offset) * K.nx + g, K.seed_lo,
         K.seed_hi);
     sm.S[rr][x] = res;
     if (red && res > 0.f) itip = max(itip, g == K.nx - 2 ? K.nx - 1 : g);

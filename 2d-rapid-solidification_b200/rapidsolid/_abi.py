@@ -5,7 +5,7 @@ rs_sizeof_params()/rs_sizeof_step_args() and the tests compare them.
 """
 import ctypes as C
 
-RS_ABI_VERSION = 8
+RS_ABI_VERSION = 9
 RS_MLP_NPARAMS = 1250
 RS_OPT_TMA = 1
 RS_OK = 0
@@ -38,7 +38,7 @@ class Params(C.Structure):
         ("Tcold", C.c_double), ("length_sample_um", C.c_double),
         ("total_time_ns", C.c_double), ("num_fields_output", C.c_int32),
         ("num_tip_output", C.c_int32), ("num_check_point_output", C.c_int32),
-        ("step_pull_back", C.c_int32),
+        ("step_pull_back", C.c_int32), ("j_offset", C.c_int32), ("band", C.c_int32),
     ]
 
 

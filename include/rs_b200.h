@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define RS_ABI_VERSION 8
+#define RS_ABI_VERSION 9
 
 /* status codes */
 #define RS_OK 0
@@ -104,6 +104,14 @@ typedef struct rs_params {
   int32_t num_tip_output;
   int32_t num_check_point_output;
   int32_t step_pull_back;  /* <= 0: derived as in set_parameters */
+  /* Row bands of one domain over several devices (the reference's
+   * fun_multi.cu splits j the same way).  band = 1: this context holds global
+   * rows j_offset .. j_offset + ny_all - 1, its ghost rows 0 and ny_all - 1
+   * are supplied by the caller (the neighbouring bands' edge rows), the step
+   * does not write them, and the interface noise is keyed by the global row.
+   * Frozen temperature only; rs_precise_tip needs the whole domain. */
+  int32_t j_offset;
+  int32_t band;
 } rs_params;
 
 /* Quantities derived from rs_params exactly as set_parameters does

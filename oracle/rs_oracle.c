@@ -401,6 +401,7 @@ static void apply_ghosts(const rs_params *p, double *f) {
     f[pos(p, 0, j)] = f[pos(p, 1, j)];
     f[pos(p, Nx - 1, j)] = f[pos(p, Nx - 2, j)];
   }
+  if (p->band) return; /* row bands: the ghost rows are the neighbouring bands' rows */
   for (int i = 0; i < Nx; ++i) {
     f[pos(p, i, 0)] = f[pos(p, i, jmin)];
     f[pos(p, i, Ny - 1)] = f[pos(p, i, jmax)];
@@ -442,7 +443,8 @@ void ro_step(const rs_params *p, const rs_derived *d, const double *c,
       if (p->noise_amplitude > 0.0) {
         double w = 1.0 - phi00 * phi00;
         if (w > 1.0e-3)
-          pn += p->noise_amplitude * sqrt(dt) * w * noise_normal(p->seed, step, ps);
+          pn += p->noise_amplitude * sqrt(dt) * w *
+                noise_normal(p->seed, step, ps + (p->band ? (int64_t)p->j_offset * p->nx_all : 0));
       }
       phi_next[ps] = pn;
     }
@@ -795,7 +797,7 @@ void ro_initial_planar(const rs_params *p, double *c, double *phi, double *psi,
   const int jmin = p->periodic_j ? Ny - 2 : 1;
   const int jmax = p->periodic_j ? 1 : Ny - 2;
   for (int j = 0; j < Ny; ++j) {
-    int js = j == 0 ? jmin : (j == Ny - 1 ? jmax : j);
+    int js = p->band ? j + p->j_offset : (j == 0 ? jmin : (j == Ny - 1 ? jmax : j));
     const uint32_t ctr[4] = {(uint32_t)js, 0u, 0u, 0x49434F46u};
     const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
     uint32_t o[4];
