@@ -413,8 +413,6 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
   if (cur->psi == next->psi || cur->c == next->c || (next->phi && (next->phi == cur->psi || next->phi == cur->c)))
     return fail(RS_E_INVALID, "rs_step: cur and next alias");
   if (c->p.tfc && !a->T_coarse) return fail(RS_E_INVALID, "rs_step: TFC needs T_coarse");
-  if (c->p.tfc && cur->precision == RS_F32)
-    return fail(RS_E_UNSUPPORTED, "rs_step: the FP32 path supports the frozen temperature only");
   const rs::StepScalars P = step_scalars(c, a);
   cudaStream_t st = (cudaStream_t)stream;
   c->pb_cur = a->pull_back ? cur->psi : nullptr;

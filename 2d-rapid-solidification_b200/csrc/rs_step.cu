@@ -323,7 +323,6 @@ int launch_step_f64(const StepCoef &K, const StepScalars &P, const double *psi, 
 int launch_step_f32(const StepCoef &K, const StepScalars &P, const float *psi, const float *c, float *psi_n,
                     float *c_n, float *phi_n, BlockPartial *partials, int max_partials, int *nb, const TmaMaps *tm,
                     int *err, cudaStream_t st) {
-  if (K.tfc) return -2;
   return launch<float>(K, P, psi, c, psi_n, c_n, phi_n, partials, max_partials, nb, tm, err, st);
 }
 
