@@ -83,6 +83,16 @@ def test_errors_are_reported_not_raised():
     bad.nx_all = 4
     assert L.rs_create(C.byref(bad), C.byref(h)) == _abi.RS_E_INVALID
     assert L.rs_calphad_eval(7, None, None, None, 0) == _abi.RS_E_INVALID
+    # row bands: frozen temperature only, a non-negative global row offset
+    bad = configs.plain_small()
+    bad.band, bad.j_offset, bad.tfc = 1, 10, 1
+    assert L.rs_create(C.byref(bad), C.byref(h)) == _abi.RS_E_UNSUPPORTED
+    bad.tfc, bad.j_offset = 0, -1
+    assert L.rs_create(C.byref(bad), C.byref(h)) == _abi.RS_E_INVALID
+    # 3D: extents and the x alignment of the tensor maps
+    p3 = lib.default_params3()
+    p3.nx = 30
+    assert L.rs3_create(C.byref(p3), C.byref(h)) == _abi.RS_E_INVALID
 
 
 def test_phase_boundaries_of_ti10nb():
