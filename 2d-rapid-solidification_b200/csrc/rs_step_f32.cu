@@ -18,7 +18,8 @@
 //   phase 1  per-cell S = q(psi) c (1-c) and mu'' (below) of the 18 input
 //            rows into shared memory, with per-row flags "every psi == -1" /
 //            "== +1" and per-lane phi masks; the halo columns x0-1 and
-//            x0+128 are computed by 36 threads on the side;
+//            x0+128 are computed by 36 threads of warps 2 and 3 (one input
+//            row fewer than warps 0 and 1);
 //   phase 2  each warp computes 4 output rows: fluxes through the faces from
 //            the shared S and mu'', the c update (kept in registers); cells
 //            whose 3x3 phi neighbourhood is not uniformly +-1 are listed;
@@ -26,7 +27,10 @@
 //            (phi_cell), so a tile's interface work is spread over the CTA;
 //   phase 4  new psi and c are written into the shared tile, ghost columns
 //            copied there, and each output row leaves by one bulk async copy
-//            per field (ghost rows by one more).
+//            per field (ghost rows by one more, except in row-band mode);
+//   partials when the caller wants the solute mass or the coarse tip, each
+//            CTA writes its partial sums and the last CTA to finish reduces
+//            them all (same order as the separate reduction kernel).
 // Arithmetic:
 //   * mu = K(T) + C0(T) + mu'' with C0 = -D - (L0_BCC - L0_Liq)(1 - 2 cinf)/2
 //     (D, K(T) as in rs_step.cu), so
@@ -40,7 +44,10 @@
 //     6 P_i + P_{i-1} + P_{i+1} with P_i = S(i,r) + S(i,r+1), and the face
 //     (i+1/2, r) has 6 Q_r + Q_{r-1} + Q_{r+1} with Q_r = S(i,r) + S(i+1,r):
 //     four times the 1.5 / 0.25 weights of rs_step.cu, the 4 folded into the
-//     flux constant.
+//     flux constant; face fluxes are rounded products, so a cell's result
+//     does not depend on where the tiling puts it;
+//   * interface noise is keyed by the global cell (row + j_offset in
+//     row-band mode).
 // Fields store psi and delta = c - cinf (include/rs_b200.h).
 #include "rs_step_common.cuh"
 #include "rs_surrogate.cuh"
