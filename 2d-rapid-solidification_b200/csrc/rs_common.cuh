@@ -5,11 +5,28 @@
 // StepCoef so that no kernel re-derives constants per cell.
 #pragma once
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 #include "../../include/rs_b200.h"
+
+namespace rs {
+// Raises a kernel's dynamic shared-memory limit on the current device, once
+// per device: the attribute belongs to each device's context, so a process
+// that drives several GPUs must set it on every one.  `done` is the call
+// site's bit set of devices already set (devices 0..63; others every call).
+inline bool smem_limit_once(const void *kernel, int bytes, std::atomic<unsigned long long> &done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  const unsigned long long bit = dev >= 0 && dev < 64 ? 1ull << dev : 0ull;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return true;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) return false;
+  done.fetch_or(bit, std::memory_order_acq_rel);
+  return true;
+}
+}  // namespace rs
 
 #define RS_HD __host__ __device__ __forceinline__
 

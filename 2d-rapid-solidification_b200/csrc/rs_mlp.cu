@@ -186,12 +186,8 @@ int launch_mlp_grad(const MlpBox &box, const float *w, int64_t n, const float *x
                     double *loss, cudaStream_t st) {
   if (n <= 0) return 0;
   const size_t smem = sizeof(float) * kGradThreads * (3 + 4 * kMlpH + 2);
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return -3;
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  if (!smem_limit_once((const void *)grad_kernel, (int)smem, attr)) return -3;
   grad_kernel<<<(unsigned)((n + kGradThreads - 1) / kGradThreads), kGradThreads, smem, st>>>(box, w, n, x, y, grad,
                                                                                              loss);
   return 0;

@@ -441,11 +441,8 @@ int launch_step(const rs3_params &p, const P3Maps &m, R *o1, R *o2, R *oc, int64
   const size_t smem = sizeof(P3Smem<R>) + 128;
   const bool sd = p.Da != 0.0 || p.Db != 0.0;
   auto kfn = sd ? peri3d_kernel<R, true> : peri3d_kernel<R, false>;
-  static bool attr[2] = {false, false};
-  if (!attr[sd]) {
-    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -3;
-    attr[sd] = true;
-  }
+  static std::atomic<unsigned long long> attr[2];
+  if (!smem_limit_once((const void *)kfn, (int)smem, attr[sd])) return -3;
   const dim3 grid((p.nx - 2 + C::BX - 1) / C::BX, (p.ny - 2 + kP3BY - 1) / kP3BY,
                   (p.nz - 2 + k.z_chunk - 1) / k.z_chunk);
   kfn<<<grid, kP3Threads, smem, st>>>(k, m.phi1, m.phi2, m.c, o1, o2, oc, step, err);

@@ -381,12 +381,9 @@ int launch_peri3d_step_x2(const rs3_params &p, const P3Maps &m, float *o1, float
   auto kfn = a1 ? (sd ? peri3d_x2_kernel<true, true> : peri3d_x2_kernel<true, false>)
                 : (sd ? peri3d_x2_kernel<false, true> : peri3d_x2_kernel<false, false>);
   const size_t smem = sizeof(X2Smem) + 128;
-  static bool attr[4] = {false, false, false, false};
+  static std::atomic<unsigned long long> attr[4];
   const int which = (a1 ? 2 : 0) + (sd ? 1 : 0);
-  if (!attr[which]) {
-    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -3;
-    attr[which] = true;
-  }
+  if (!smem_limit_once((const void *)kfn, (int)smem, attr[which])) return -3;
   const dim3 grid((p.nx + kX2BX - 1) / kX2BX, (p.ny - 2 + kX2BY - 1) / kX2BY, (p.nz - 2 + k.z_chunk - 1) / k.z_chunk);
   kfn<<<grid, kX2Threads, smem, st>>>(k, m.phi1, m.phi2, m.c, o1, o2, oc, step, err);
   return 0;

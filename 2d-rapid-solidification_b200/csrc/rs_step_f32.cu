@@ -779,12 +779,8 @@ __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
 int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
                     bool advance, int *err, cudaStream_t st) {
   const size_t smem = sizeof(TileSmem);
-  static bool attr_done = false;
-  if (!attr_done) {
-    if (cudaFuncSetAttribute(ens_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return -3;
-    attr_done = true;
-  }
+  static std::atomic<unsigned long long> attr_done{0};
+  if (!smem_limit_once((const void *)ens_tile_kernel, (int)smem, attr_done)) return -3;
   ens_table_kernel<<<ntblk, kTabBlock, 0, st>>>(runs, tblk);
   ens_tile_kernel<<<ntiles, kThreads, smem, st>>>(runs, order, err);
   if (advance) ens_advance_kernel<<<(nruns + 63) / 64, 64, 0, st>>>(const_cast<EnsRun *>(runs), nruns);
@@ -804,11 +800,8 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   const size_t smem = sizeof(TileSmem);
   const bool surr = tm.surr != nullptr;
   auto kfn = surr ? tile_kernel<true> : tile_kernel<false>;
-  static bool attr_done[2] = {false, false};
-  if (!attr_done[surr]) {
-    if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -3;
-    attr_done[surr] = true;
-  }
+  static std::atomic<unsigned long long> attr_done[2];
+  if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr])) return -3;
   SurrArgs sa = {};
   if (surr) sa = *tm.surr;
   column_table_kernel<<<(tm.col_tab_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(K, P.d0, P.d1, tm.col_tab_len, tm.col_tab);
