@@ -1,6 +1,7 @@
 """The C++ host driver (lib/rs_run): the reference's main() loop on the C-ABI.
 
-The driver's FP64 run must equal, bit for bit, the same loop written in
+The driver's run (FP64, and FP32 with --precision f32) must equal, bit for
+bit, the same loop written in
 Python over the same entry points (pull-back cadence, frozen temperature with
 the Vp ramp, fun.cu:431-514), and a restart that loads its own check point and
 runs no step must write the same files back (save/load_check_point,
@@ -30,13 +31,13 @@ def run_driver(out, *extra):
     return r.stdout
 
 
-def python_loop(steps, tfc):
+def python_loop(steps, tfc, dtype=torch.float64):
     """The loop body of fun.cu:431-514 over the Python binding (no files)."""
     p = lib.default_params()
     p.nx_all, p.ny_all, p.i_tip_target, p.tfc = NX, NY, ITIP, tfc
     ctx = lib.Context(p)
     d = ctx.d
-    a, b = lib.FieldSet(p, torch.float64), lib.FieldSet(p, torch.float64)
+    a, b = lib.FieldSet(p, dtype), lib.FieldSet(p, dtype)
     ctx.initial(a)
     itip = torch.zeros(1, dtype=torch.int32, device="cuda")
     T = Tn = dphidt = None
@@ -66,18 +67,21 @@ def python_loop(steps, tfc):
         a, b = b, a
     torch.cuda.synchronize()
     c = a.c.double().cpu().numpy().reshape(NY, NX)
+    if dtype == torch.float32:  # FP32 sets hold c - cinf
+        c = p.cinf + c
     phi = np.clip(a.psi.double().cpu().numpy().reshape(NY, NX), -1.0, 1.0)
     Th = None if T is None else T.cpu().numpy()
     return c, phi, hist, l, Th, d
 
 
+@pytest.mark.parametrize("precision", ["f64", "f32"])
 @pytest.mark.parametrize("tfc", [1, 0])
-def test_driver_equals_python_loop(tmp_path, tfc):
+def test_driver_equals_python_loop(tmp_path, tfc, precision):
     out = run_driver(tmp_path, "--steps", str(STEPS), "--tfc", str(tfc), "--tip-every", "100",
-                     "--check-every", "1000000")
+                     "--check-every", "1000000", "--precision", precision)
     c = np.fromfile(tmp_path / "data" / "check_point_c.bin", dtype=np.float64).reshape(NY, NX)
     phi = np.fromfile(tmp_path / "data" / "check_point_phi.bin", dtype=np.float64).reshape(NY, NX)
-    c_ref, phi_ref, hist, l, T, d = python_loop(STEPS, tfc)
+    c_ref, phi_ref, hist, l, T, d = python_loop(STEPS, tfc, torch.float32 if precision == "f32" else torch.float64)
     assert np.array_equal(c, c_ref)
     assert np.array_equal(phi, phi_ref)
     s = lib.read_parameters(tmp_path / "parameters.txt", tfc=tfc)
