@@ -400,6 +400,7 @@ static rs::StepScalars step_scalars(const rs_ctx *c, const rs_step_args *a) {
   P.pull_back = a->pull_back ? 1 : 0;
   P.i_offset = a->i_offset;
   P.i_left_end_T = a->i_left_end_T;
+  P.i_front = p.i_tip_target;
   P.T_coarse = (const double *)a->T_coarse;
   return P;
 }

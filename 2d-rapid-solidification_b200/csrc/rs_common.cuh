@@ -159,6 +159,15 @@ RS_HD void noise_counter(uint32_t x[4], int64_t step, int64_t cell) {
   x[3] = (uint32_t)((uint64_t)step >> 32) ^ 0x4E4F4953u;
 }
 
+// Launch order of the column blocks of a 2D step: k-th block launched -> block
+// index, for n blocks with the front in block f: f, then f-1 down to 0 (the
+// solid and mushy zone behind it), then n-1 down to f+1 (melt).  The slow
+// blocks at the front start first instead of being left for the last wave.
+__host__ __device__ __forceinline__ int front_first_block(int k, int f, int n) {
+  f = f < 0 ? 0 : (f > n - 1 ? n - 1 : f);
+  return (f - k + n) % n;
+}
+
 // ---------------------------------------------------------------- coefficients
 // Everything the step kernel needs, derived once on the host.
 struct StepCoef {
@@ -197,7 +206,10 @@ struct StepScalars {
   double d0, d1;
   int32_t pull_back, i_offset;
   int32_t i_left_end_T;
-  int32_t reserved;
+  // column the moving frame keeps the front at (i_tip_target): the order the
+  // 2D step kernels launch their column blocks in (front_first_block);
+  // results do not depend on it
+  int32_t i_front;
   const double *T_coarse;
 };
 

@@ -22,7 +22,8 @@
 // (fun.cu:1424-1432) and the chemical potential mu (fun.cu:1443-1452) are
 // computed once per cell, vertical neighbours come from a three-row register
 // window and horizontal neighbours from warp shuffles.  No shared memory, no
-// block barriers.
+// block barriers.  Column blocks launch from the one holding the front
+// (front_first_block): its interface rows are the slowest.
 //
 // Arithmetic (identical mathematics to the reference, regrouped):
 //   * anisotropy (get_anisotropy, fun.cu:1030-1139): with n = R (cos, sin, 0),
@@ -235,10 +236,15 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3)
                 typename Tr<R>::S *__restrict__ c_n, typename Tr<R>::S *__restrict__ phi_n, BlockPartial *partials) {
   using S = typename Tr<R>::S;
   const int nx = K.nx, ny = K.ny, pitch = K.pitch;
-  const int wc = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);  // warp column
-  const int X = 1 + 30 * wc;                                            // first output column
-  const int gi = X - 1 + (int)(threadIdx.x & 31);                       // this lane's column
-  const int y0 = 1 + blockIdx.y * H;
+  const int wpb = blockDim.x >> 5;
+  // blockIdx.x walks the row blocks of one column block, blockIdx.y the column
+  // blocks, from the one holding column PS.i_front
+  const int ncb = gridDim.y, rb = blockIdx.x;
+  const int cb = front_first_block((int)blockIdx.y, max(PS.i_front - 1, 0) / (30 * wpb), ncb);
+  const int wc = cb * wpb + (int)(threadIdx.x >> 5);     // warp column
+  const int X = 1 + 30 * wc;                             // first output column
+  const int gi = X - 1 + (int)(threadIdx.x & 31);        // this lane's column
+  const int y0 = 1 + rb * H;
   const int y_last = min(y0 + H - 1, ny - 2);
   const bool active_warp = X <= nx - 2;
 
@@ -275,8 +281,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3)
       }
     }
   }
-  if (partials)
-    st.write_partial(partials, ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5));
+  if (partials) st.write_partial(partials, ((int64_t)rb * ncb + cb) * wpb + (int)(threadIdx.x >> 5));
 }
 
 template <typename R>
@@ -294,7 +299,8 @@ static int launch(const StepCoef &K, const StepScalars &P, const typename Tr<R>:
   constexpr int PF = 3;   // rows in flight per lane (multiple of the 3-row window)
   int H = 64;
   while (H > 16 && (int64_t)wcols * ((nj + H - 1) / H) < 148 * 16) H /= 2;
-  dim3 block(32 * WPB), grid((wcols + WPB - 1) / WPB, (nj + H - 1) / H);
+  dim3 block(32 * WPB), grid((nj + H - 1) / H, (wcols + WPB - 1) / WPB);
+  if (grid.y > 65535) return -1;
   const int nw = grid.x * grid.y * WPB;
   if (partials && nw > max_partials) return -1;
 #define RS_LAUNCH(HH)                                                                                   \

@@ -40,6 +40,9 @@
 //   * rows whose cells are all bulk liquid (psi = -1 exactly, |s| < 1/9) take
 //     the short form: g(-1) = -1 and q(-1) = 1, so
 //     mu'' = -2 L0_Liq delta + RT lam(delta) and S = c (1 - c);
+//   * rows whose cells have psi = +1 exactly over their 3x3 neighbourhoods
+//     (deep solid) store S = mu'' = 0: q(1) = 0, so every face weight touching
+//     the row is 0 and its mu'' enters no flux (no network pass either);
 //   * face weights use pair sums: the face (i, r+1/2) has
 //     6 P_i + P_{i-1} + P_{i+1} with P_i = S(i,r) + S(i,r+1), and the face
 //     (i+1/2, r) has 6 Q_r + Q_{r-1} + Q_{r+1} with Q_r = S(i,r) + S(i+1,r):
@@ -48,6 +51,8 @@
 //     does not depend on where the tiling puts it;
 //   * interface noise is keyed by the global cell (row + j_offset in
 //     row-band mode).
+// Launch order: the tile columns from the one holding the front
+// (front_first_block), whose interface and network work is the slowest.
 // Fields store psi and delta = c - cinf (include/rs_b200.h).
 #include "rs_step_common.cuh"
 #include "rs_surrogate.cuh"
@@ -227,6 +232,38 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const float dv = sm.d[rr][b];
     return __float_as_uint(sm.psi[rr][b]) == kMinus1 && dv < d_hi && dv > d_lo;
   };
+  // a halo cell's mu'' enters only the face to the tile's edge column, whose
+  // weight is 0 when psi is exactly +1 on both columns over rows rr-1..rr+1;
+  // column -1 (left-most tile) enters no face at all (column 0 is a ghost)
+  auto halo_mu_used = [&](int rr, int b) {
+    if (b == kHaloL && x0 == 0) return false;
+    const int b2 = b == kHaloL ? b + 1 : b - 1;
+    bool solid = true;
+    for (int r2 = max(rr - 1, 0); r2 <= min(rr + 1, kTRin - 1); ++r2)
+      solid = solid && __float_as_uint(sm.psi[r2][b]) == kPlus1 && __float_as_uint(sm.psi[r2][b2]) == kPlus1;
+    return !solid;
+  };
+  // per lane, bit q: psi is exactly +1 over the 3x3 neighbourhood of cell
+  // bc+q (rows of the box only: faces to rows outside it are not computed;
+  // column -1 of the left-most tile enters no face, column 0 being a ghost).
+  // S = q(1) c (1 - c) = 0 there, so every face weight touching the cell is 0
+  // and its mu'' enters no flux (0 times a finite difference)
+  auto solid3 = [&](int rr) -> uint32_t {
+    const int xh = lane == 0 ? kHaloL : kHaloR;
+    uint32_t v = 0xFu;
+    bool hs = true;  // the halo column beside lanes 0 and 31
+    for (int r2 = max(rr - 1, 0); r2 <= min(rr + 1, kTRin - 1); ++r2) {
+      const float4 q4 = ld4(&sm.psi[r2][bc]);
+      v &= (__float_as_uint(q4.x) == kPlus1 ? 1u : 0u) | (__float_as_uint(q4.y) == kPlus1 ? 2u : 0u) |
+           (__float_as_uint(q4.z) == kPlus1 ? 4u : 0u) | (__float_as_uint(q4.w) == kPlus1 ? 8u : 0u);
+      hs = hs && __float_as_uint(sm.psi[r2][xh]) == kPlus1;
+    }
+    uint32_t lf = __shfl_up_sync(FULL, v >> 3, 1) & 1u, rt = __shfl_down_sync(FULL, v, 1) & 1u;
+    if (lane == 0) lf = (hs || x0 == 0) ? 1u : 0u;
+    if (lane == 31) rt = hs ? 1u : 0u;
+    const uint32_t e = lf | (v << 1) | (rt << 5);  // bit k: box column bc-1+k
+    return e & (e >> 1) & (e >> 2) & 0xFu;
+  };
   auto net_inputs = [&](int rr, int b, float in[3]) {  // b: box column
     in[0] = fmaf(TnB, (float)(b - 4), TnA);
     in[1] = fmaf(sm.d[rr][b], SA.c_ihalf, cnA);
@@ -301,7 +338,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const float dmx = fmaxf(fmaxf(dv[0], dv[1]), fmaxf(dv[2], dv[3]));
     const float dmn = fminf(fminf(dv[0], dv[1]), fminf(dv[2], dv[3]));
     const bool liq4 = band == kMinus1 && bor == kMinus1;
-    uint32_t code;
+    uint32_t code, s3 = 0u;
     if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
       code = 1u | 4u;  // 4: every cell in the series form
       sm.pmask[rr][lane] = 0x0Fu;
@@ -320,14 +357,32 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     } else {
       const bool sol4 = band == kPlus1 && bor == kPlus1;
       code = (__all_sync(FULL, liq4) ? 1u : 0u) | (__all_sync(FULL, sol4) ? 2u : 0u);
-      uint32_t L = 0u, Sm = 0u;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (pv[q] <= -1.f) L |= 1u << q;
-        if (pv[q] >= 1.f) Sm |= 1u << q;
-        cell_terms(F, pv[q], dv[q], RTa[q], C0a[q], Sv[q], mv[q]);
+      // deep solid row: no cell's mu'' enters a flux (solid3), so S = mu'' = 0
+      // gives the same fluxes.  The surrogate also skips solid3 cells, which
+      // pays only where a whole 16-cell network pass (lanes 4m .. 4m+3) is
+      // solid
+      bool want = (code & 2u) != 0u;
+      if constexpr (SURR) {
+        const uint32_t fs = __ballot_sync(FULL, sol4);
+        want = want || (fs & (fs >> 1) & (fs >> 2) & (fs >> 3) & 0x11111111u) != 0u;
       }
-      sm.pmask[rr][lane] = (uint8_t)(L | (Sm << 4));
+      if (want) s3 = solid3(rr);
+      const bool deep = (code & 2u) && __all_sync(FULL, s3 == 0xFu);
+      if (deep) {
+        code |= 8u;  // 8: mu'' not needed (no network pass either)
+        sm.pmask[rr][lane] = 0xF0u;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) Sv[q] = mv[q] = 0.f;
+      } else {
+        uint32_t L = 0u, Sm = 0u;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (pv[q] <= -1.f) L |= 1u << q;
+          if (pv[q] >= 1.f) Sm |= 1u << q;
+          cell_terms(F, pv[q], dv[q], RTa[q], C0a[q], Sv[q], mv[q]);
+        }
+        sm.pmask[rr][lane] = (uint8_t)(L | (Sm << 4));
+      }
     }
     st4(&sm.S[rr][bc], Sv[0], Sv[1], Sv[2], Sv[3]);
     st4(&sm.mu[rr][bc], mv[0], mv[1], mv[2], mv[3]);
@@ -336,14 +391,20 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       if (code & 2u) atomicOr(&sm.sol, 1u << rr);
     }
     if constexpr (SURR) {  // the row's non-melt cells through the network, 16 at a time
-      if (!(code & 4u)) {
+      if (!(code & (4u | 8u))) {
         __syncwarp();
         const SurrConst SC = surr_load(SA, lane);
         const int g = lane >> 2;
+        const bool any3 = __any_sync(FULL, s3 != 0u);
 #pragma unroll 1
         for (int mt = 0; mt < kW / 16; ++mt) {
           const int ba = 4 + 16 * mt + g, bb = ba + 8;
-          const bool na = !melt_cell(rr, ba), nb = !melt_cell(rr, bb);
+          bool na = !melt_cell(rr, ba), nb = !melt_cell(rr, bb);
+          if (any3) {  // warp-uniform
+            const uint32_t sa = __shfl_sync(FULL, s3, (ba - 4) >> 2), sb = __shfl_sync(FULL, s3, (bb - 4) >> 2);
+            na = na && !((sa >> ((ba - 4) & 3)) & 1u);
+            nb = nb && !((sb >> ((bb - 4) & 3)) & 1u);
+          }
           if (!__any_sync(FULL, na || nb)) continue;
           float in0[3], in1[3], o0[2], o1[2];
           net_inputs(rr, ba, in0);
@@ -384,8 +445,8 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       const int ia = 16 * mt + g, ib = ia + 8;
       const int ra = ia < 2 * kTRin ? ia >> 1 : 0, rb = ib < 2 * kTRin ? ib >> 1 : 0;
       const int xa = (ia & 1) ? kHaloR : kHaloL, xb = (ib & 1) ? kHaloR : kHaloL;
-      const bool na = ia < 2 * kTRin && y0 - 1 + ra <= K.ny - 1 && !melt_cell(ra, xa);
-      const bool nb = ib < 2 * kTRin && y0 - 1 + rb <= K.ny - 1 && !melt_cell(rb, xb);
+      const bool na = ia < 2 * kTRin && y0 - 1 + ra <= K.ny - 1 && !melt_cell(ra, xa) && halo_mu_used(ra, xa);
+      const bool nb = ib < 2 * kTRin && y0 - 1 + rb <= K.ny - 1 && !melt_cell(rb, xb) && halo_mu_used(rb, xb);
       if (!__any_sync(FULL, na || nb)) continue;
       const SurrConst SC = surr_load(SA, lane);
       float in0[3], in1[3], o0[2], o1[2];
@@ -725,9 +786,13 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
                 const __grid_constant__ CUtensorMap tm_c, const float *__restrict__ tab, const int tab_len,
                 float *__restrict__ psi_n, float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *partials,
                 int *err, const __grid_constant__ SurrArgs SA, const __grid_constant__ FinalRed FR) {
+  // blockIdx.x walks the tile rows of one tile column (they share halo rows
+  // in L2), blockIdx.y the tile columns, from the one holding column PS.i_front
+  const int tr = blockIdx.x;
+  const int tc = front_first_block((int)blockIdx.y, max(PS.i_front, 0) / kW, (int)gridDim.y);
   tile_body<SURR>(K, F, PS, &tm_psi, &tm_c, tab, tab_len, psi_n, c_n, phi_n,
-                  partials ? partials + ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) : nullptr, err, SA, blockIdx.x,
-                  blockIdx.y, partials && FR.counter ? &FR : nullptr);
+                  partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr, err, SA, tr, tc,
+                  partials && FR.counter ? &FR : nullptr);
 }
 
 // ---------------------------------------------------------------- ensemble
@@ -794,6 +859,7 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   if (K.nx % 4 || K.pitch != K.nx) return -1;  // rows are copied in 16-byte units
   // column-major: consecutive CTAs share a column strip and its halo rows in L2
   const dim3 grid((nj + kTR - 1) / kTR, (K.nx + kW - 1) / kW), block(kThreads);
+  if (grid.y > 65535) return -1;
   const int nparts = grid.x * grid.y;
   if (partials && nparts > max_partials) return -1;
   if (tm.col_tab_len < (int)grid.y * kW + kWin) return -1;

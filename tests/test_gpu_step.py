@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import pyoracle
-from helpers import golden, maxabs, perturbed_state
+from helpers import fix_ghosts, golden, maxabs, perturbed_state
 from rapidsolid import _abi, configs, lib
 
 torch = pytest.importorskip("torch")
@@ -175,6 +175,52 @@ def test_single_step_f32_close_to_oracle(tma):
     # inputs are rounded to FP32 first; compare increments
     assert maxabs(g.psi - s.psi, o.psi - s.psi) <= 5e-6
     assert maxabs(g.c - s.c, o.c - s.c) <= 5e-8
+
+
+def solid_with_pocket(p, seed):
+    """Planar front at i_tip_target with a wide solid behind it (psi exactly
+    +1 in FP32 from about 16 cells behind the front) holding a liquid pocket
+    of radius 5 at (i, j) = (190, 33), and seeded c noise in the solid: tile
+    rows of the solid are deep solid except those next to the pocket."""
+    s = pyoracle.initial_planar(p, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, seed)
+    ny, nx = s.psi.shape
+    j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    pocket = np.tanh((np.hypot(i - 190.0, j - 33.0) - 5.0) * p.dx / np.sqrt(2.0))
+    psi = np.minimum(s.psi, pocket)
+    c = s.c + 0.5 * (1.0 - pocket) * (configs.C_LIQUID_TI10NB - configs.C_SOLID_AT_TLIQ)
+    c = c + 2e-3 * np.random.default_rng(seed).standard_normal(c.shape) * (psi > 0.9)
+    s.psi[:] = psi
+    s.phi[:] = psi
+    s.c[:] = c
+    fix_ghosts(p, s)
+    return s
+
+
+@pytest.mark.parametrize("tma", [1, 0])
+def test_f32_step_with_deep_solid_close_to_oracle(tma):
+    """Rows whose 3x3 neighbourhoods are all psi = +1 skip the per-cell mu''
+    (every face weight there is 0); rows beside the pocket's interface must
+    not.  One step against the FP64 oracle, increments compared as in the
+    single-step test, and the deep solid left exactly unchanged."""
+    p = configs.small(640, 70, i_tip_target=400, G=5e6, V=0.5)
+    d = pyoracle.derive(p)
+    s = solid_with_pocket(p, 5)
+    ctx = lib.Context(p)
+    ctx.set_option(_abi.RS_OPT_TMA, tma)
+    cur, nxt = upload(p, s, torch.float32), lib.FieldSet(p, torch.float32)
+    s32 = download(p, cur)  # the FP32-rounded input
+    ctx.step(cur, nxt, 0)
+    o = pyoracle.step(p, d, s32, 0)
+    g = download(p, nxt)
+    assert maxabs(g.psi - s32.psi, o.psi - s32.psi) <= 5e-6
+    assert maxabs(g.c - s32.c, o.c - s32.c) <= 5e-8
+    deep = np.ones_like(s32.psi, dtype=bool)
+    for dj in (-1, 0, 1):
+        for di in (-1, 0, 1):
+            deep &= np.roll(np.roll(s32.psi == 1.0, dj, 0), di, 1)
+    deep[[0, -1], :] = deep[:, [0, -1]] = False
+    assert deep[1:-1, 130:380].mean() > 0.5
+    assert np.array_equal(g.c[deep], s32.c[deep]) and np.array_equal(g.psi[deep], s32.psi[deep])
 
 
 def test_tma_and_register_paths_agree():

@@ -101,3 +101,44 @@ def test_surrogate_step_runs_with_audit():
     # the front stays where the exact run has it to within a few cells
     ifront = lambda ps: (ps.reshape(p.ny_all, p.nx_all)[1:-1, 1:-1] > 0).sum(1).mean()
     assert abs(ifront(psi) - ifront(out[False][0])) < 3.0
+
+
+def test_surrogate_skips_deep_solid_rows():
+    """A wide solid (psi exactly +1) with a liquid pocket: tile rows whose 3x3
+    neighbourhoods are all solid take no network pass (their mu'' enters no
+    flux).  One step with the surrogate against the exact FP32 step: the deep
+    solid is left exactly unchanged, and the c increments near the pocket
+    agree to within the network's error (a row wrongly taken as deep would
+    lose its whole flux there).  The network is trained on the box fitted to
+    the workload (the pocket's T and c lie inside it), whose mu'' error is a
+    few per cent of the mu'' differences that drive the pocket's fluxes."""
+    from test_gpu_step import download, solid_with_pocket, upload
+    p = configs.small(640, 70, i_tip_target=400, G=5e6, V=0.5)
+    s = solid_with_pocket(p, 5)
+    w, box, _ = surrogate.train(p, box=surrogate.fitted_box(), epochs=40, seed=4)
+    out = {}
+    for use in (False, True):
+        ctx = lib.Context(p)
+        if use:
+            ctx.set_surrogate(w, box)
+        cur, nxt = upload(p, s, torch.float32), lib.FieldSet(p, torch.float32)
+        s32 = download(p, cur)
+        ctx.step(cur, nxt, 0)
+        torch.cuda.synchronize()
+        ctx.device_status()
+        out[use] = download(p, nxt)
+    g, e = out[True], out[False]
+    assert np.isfinite(g.psi).all() and np.isfinite(g.c).all()
+    solid = s32.psi == 1.0
+    deep = solid.copy()
+    for dj in (-1, 0, 1):
+        for di in (-1, 0, 1):
+            deep &= np.roll(np.roll(solid, dj, 0), di, 1)
+    deep[[0, -1], :] = deep[:, [0, -1]] = False
+    assert np.array_equal(g.c[deep], s32.c[deep]) and np.array_equal(g.psi[deep], s32.psi[deep])
+    near = np.zeros_like(deep)
+    near[20:47, 175:206] = True  # the pocket and its interface
+    de = e.c - s32.c
+    assert np.abs(de[near]).max() > 1e-6
+    err, ref = np.abs((g.c - s32.c) - de)[near].max(), np.abs(de[near]).max()
+    assert err <= 0.5 * ref, (err, ref, ctx.surrogate_audit())
