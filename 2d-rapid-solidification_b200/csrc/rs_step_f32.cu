@@ -170,7 +170,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
                                           const float *__restrict__ tab, const int tab_len, float *__restrict__ psi_n,
                                           float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *part,
                                           int *err, const SurrArgs &SA, const int tr, const int tc,
-                                          const FinalRed *FR) {
+                                          const FinalRed *FR, const int pf_tr = -1, const int pf_tc = -1) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -300,6 +300,12 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
         break;
       }
     }
+  }
+  // this tile is in: pull the tile of the CTA that will start about one
+  // resident wave later into L2, so its loads overlap this wave's arithmetic
+  if (pf_tc >= 0 && threadIdx.x == 0) {
+    tma_prefetch_2d(tm_psi, kW * pf_tc - 4, kTR * pf_tr);
+    tma_prefetch_2d(tm_c, kW * pf_tc - 4, kTR * pf_tr);
   }
   // columns beyond the array (right-most tiles; zero-filled by TMA) become
   // bulk melt, so they never force the general path; no output reads them
@@ -785,14 +791,23 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
                 const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
                 const __grid_constant__ CUtensorMap tm_c, const float *__restrict__ tab, const int tab_len,
                 float *__restrict__ psi_n, float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *partials,
-                int *err, const __grid_constant__ SurrArgs SA, const __grid_constant__ FinalRed FR) {
+                int *err, const __grid_constant__ SurrArgs SA, const __grid_constant__ FinalRed FR,
+                const int wave) {
   // blockIdx.x walks the tile rows of one tile column (they share halo rows
   // in L2), blockIdx.y the tile columns, from the one holding column PS.i_front
+  const int f = max(PS.i_front, 0) / kW;
   const int tr = blockIdx.x;
-  const int tc = front_first_block((int)blockIdx.y, max(PS.i_front, 0) / kW, (int)gridDim.y);
+  const int tc = front_first_block((int)blockIdx.y, f, (int)gridDim.y);
+  // the block launched `wave` (CTAs resident at once) positions later
+  const int64_t nxt = (int64_t)blockIdx.y * gridDim.x + blockIdx.x + wave;
+  int pf_tr = -1, pf_tc = -1;
+  if (wave > 0 && nxt < (int64_t)gridDim.x * gridDim.y) {
+    pf_tr = (int)(nxt % gridDim.x);
+    pf_tc = front_first_block((int)(nxt / gridDim.x), f, (int)gridDim.y);
+  }
   tile_body<SURR>(K, F, PS, &tm_psi, &tm_c, tab, tab_len, psi_n, c_n, phi_n,
                   partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr, err, SA, tr, tc,
-                  partials && FR.counter ? &FR : nullptr);
+                  partials && FR.counter ? &FR : nullptr, pf_tr, pf_tc);
 }
 
 // ---------------------------------------------------------------- ensemble
@@ -868,6 +883,19 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   auto kfn = surr ? tile_kernel<true> : tile_kernel<false>;
   static std::atomic<unsigned long long> attr_done[2];
   if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr])) return -3;
+  // CTAs resident at once on this device (the prefetch distance), once per device
+  static std::atomic<int> wave_of[2][64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -3;
+  int wave = dev >= 0 && dev < 64 ? wave_of[surr][dev].load(std::memory_order_relaxed) : 0;
+  if (wave == 0) {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return -3;
+    wave = per_sm * sms;
+    if (dev >= 0 && dev < 64) wave_of[surr][dev].store(wave, std::memory_order_relaxed);
+  }
   SurrArgs sa = {};
   if (surr) sa = *tm.surr;
   column_table_kernel<<<(tm.col_tab_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(K, P.d0, P.d1, tm.col_tab_len, tm.col_tab);
@@ -887,7 +915,7 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   fr.nparts = nparts;
   if (!partials || !(fr.mass_out || fr.itip_out)) fr.counter = nullptr;
   if (cudaLaunchKernelEx(&cfg, kfn, K, F, P, tm.psi, tm.c, tab, tm.col_tab_len, psi_n, c_n, phi_n, partials, err,
-                         sa, fr) != cudaSuccess)
+                         sa, fr, wave) != cudaSuccess)
     return -3;
   if (nparts_out) *nparts_out = nparts;
   return 0;
