@@ -53,6 +53,10 @@
 //     row-band mode).
 // Launch order: the tile columns from the one holding the front
 // (front_first_block), whose interface and network work is the slowest.
+// After phase 1 each CTA prefetches into L2 the input tile of the block
+// launched one resident wave later, so the tiles of the next wave arrive
+// while this wave computes (the CTAs of a wave otherwise load, compute and
+// store in step).
 // Fields store psi and delta = c - cinf (include/rs_b200.h).
 #include "rs_step_common.cuh"
 #include "rs_surrogate.cuh"
@@ -301,12 +305,6 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       }
     }
   }
-  // this tile is in: pull the tile of the CTA that will start about one
-  // resident wave later into L2, so its loads overlap this wave's arithmetic
-  if (pf_tc >= 0 && threadIdx.x == 0) {
-    tma_prefetch_2d(tm_psi, kW * pf_tc - 4, kTR * pf_tr);
-    tma_prefetch_2d(tm_c, kW * pf_tc - 4, kTR * pf_tr);
-  }
   // columns beyond the array (right-most tiles; zero-filled by TMA) become
   // bulk melt, so they never force the general path; no output reads them
   if (x0 + kW + 4 > K.nx) {
@@ -470,6 +468,13 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   const float dKl = tDK[gi - 1];
   const float dKa[5] = {dKl, dKv.x, dKv.y, dKv.z, dKv.w};  // faces x-1|x for x = col .. col+4
   __syncthreads();
+  // phase 1 done: pull the tile of the CTA that will start about one resident
+  // wave later into L2, so its loads overlap the rest of this wave's
+  // arithmetic (issued after the own load and phase 1, it measured fastest)
+  if (pf_tc >= 0 && threadIdx.x == 0) {
+    tma_prefetch_2d(tm_psi, kW * pf_tc - 4, kTR * pf_tr);
+    tma_prefetch_2d(tm_c, kW * pf_tc - 4, kTR * pf_tr);
+  }
 
   // ---- phase 2: warp w computes output rows 1 + 4w .. 4 + 4w of the tile
   const uint32_t liq = sm.liq, sol = sm.sol;
