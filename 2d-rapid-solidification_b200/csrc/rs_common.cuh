@@ -165,7 +165,8 @@ RS_HD void noise_counter(uint32_t x[4], int64_t step, int64_t cell) {
 // blocks at the front start first instead of being left for the last wave.
 __host__ __device__ __forceinline__ int front_first_block(int k, int f, int n) {
   f = f < 0 ? 0 : (f > n - 1 ? n - 1 : f);
-  return (f - k + n) % n;
+  const int b = f - k;  // 0 <= k < n
+  return b < 0 ? b + n : b;
 }
 
 // ---------------------------------------------------------------- coefficients

@@ -804,9 +804,9 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
   const int tr = blockIdx.x;
   const int tc = front_first_block((int)blockIdx.y, f, (int)gridDim.y);
   // the block launched `wave` (CTAs resident at once) positions later
-  const int64_t nxt = (int64_t)blockIdx.y * gridDim.x + blockIdx.x + wave;
+  const unsigned nxt = blockIdx.y * gridDim.x + blockIdx.x + (unsigned)wave;
   int pf_tr = -1, pf_tc = -1;
-  if (wave > 0 && nxt < (int64_t)gridDim.x * gridDim.y) {
+  if (wave > 0 && nxt < gridDim.x * gridDim.y) {
     pf_tr = (int)(nxt % gridDim.x);
     pf_tc = front_first_block((int)(nxt / gridDim.x), f, (int)gridDim.y);
   }
@@ -879,7 +879,7 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   if (K.nx % 4 || K.pitch != K.nx) return -1;  // rows are copied in 16-byte units
   // column-major: consecutive CTAs share a column strip and its halo rows in L2
   const dim3 grid((nj + kTR - 1) / kTR, (K.nx + kW - 1) / kW), block(kThreads);
-  if (grid.y > 65535) return -1;
+  if (grid.y > 65535 || (int64_t)grid.x * grid.y > (1 << 30)) return -1;
   const int nparts = grid.x * grid.y;
   if (partials && nparts > max_partials) return -1;
   if (tm.col_tab_len < (int)grid.y * kW + kWin) return -1;
