@@ -168,13 +168,13 @@ __global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef 
 // keep the exact series form: it is exact and cheaper than the network.
 // The work of one CTA on tile (row tile tr, column tile tc) of a field set;
 // part: this tile's partial (mass, coarse tip), or nullptr.
-template <bool SURR>
+template <bool SURR, typename Prefetch>
 __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &F, const StepScalars &PS,
                                           const CUtensorMap *tm_psi, const CUtensorMap *tm_c,
                                           const float *__restrict__ tab, const int tab_len, float *__restrict__ psi_n,
                                           float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *part,
                                           int *err, const SurrArgs &SA, const int tr, const int tc,
-                                          const FinalRed *FR, const int pf_tr = -1, const int pf_tc = -1) {
+                                          const FinalRed *FR, const Prefetch &prefetch) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -471,10 +471,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   // phase 1 done: pull the tile of the CTA that will start about one resident
   // wave later into L2, so its loads overlap the rest of this wave's
   // arithmetic (issued after the own load and phase 1, it measured fastest)
-  if (pf_tc >= 0 && threadIdx.x == 0) {
-    tma_prefetch_2d(tm_psi, kW * pf_tc - 4, kTR * pf_tr);
-    tma_prefetch_2d(tm_c, kW * pf_tc - 4, kTR * pf_tr);
-  }
+  if (threadIdx.x == 0) prefetch();
 
   // ---- phase 2: warp w computes output rows 1 + 4w .. 4 + 4w of the tile
   const uint32_t liq = sm.liq, sol = sm.sol;
@@ -810,9 +807,15 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
     pf_tr = (int)(nxt % gridDim.x);
     pf_tc = front_first_block((int)(nxt / gridDim.x), f, (int)gridDim.y);
   }
+  auto prefetch = [&]() {
+    if (pf_tc >= 0) {
+      tma_prefetch_2d(&tm_psi, kW * pf_tc - 4, kTR * pf_tr);
+      tma_prefetch_2d(&tm_c, kW * pf_tc - 4, kTR * pf_tr);
+    }
+  };
   tile_body<SURR>(K, F, PS, &tm_psi, &tm_c, tab, tab_len, psi_n, c_n, phi_n,
                   partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr, err, SA, tr, tc,
-                  partials && FR.counter ? &FR : nullptr, pf_tr, pf_tc);
+                  partials && FR.counter ? &FR : nullptr, prefetch);
 }
 
 // ---------------------------------------------------------------- ensemble
@@ -837,7 +840,8 @@ __global__ void __launch_bounds__(kTabBlock) ens_table_kernel(const EnsRun *__re
 }
 
 __global__ void __launch_bounds__(kThreads, 5) ens_tile_kernel(const EnsRun *__restrict__ runs,
-                                                              const int32_t *__restrict__ order, int *err) {
+                                                              const int32_t *__restrict__ order, int *err,
+                                                              const int wave) {
   const int32_t e = order[blockIdx.x];
   const EnsRun &R = runs[e >> 16];
   if (!R.active) return;
@@ -848,8 +852,20 @@ __global__ void __launch_bounds__(kThreads, 5) ens_tile_kernel(const EnsRun *__r
   PS.d0 = ens_d0(R);
   PS.d1 = R.d1;
   const SurrArgs none = {};
+  // the tile of the block launched `wave` (CTAs resident at once) positions
+  // later, looked up by the issuing thread only: it may belong to another run
+  auto prefetch = [&]() {
+    const int nb = (int)blockIdx.x + wave;
+    if (wave <= 0 || nb >= (int)gridDim.x) return;
+    const int32_t e2 = order[nb];
+    const EnsRun &R2 = runs[e2 >> 16];
+    if (!R2.active) return;
+    const int t2 = e2 & 0xFFFF, p2 = (int)(R2.step & 1);
+    tma_prefetch_2d(&R2.map_psi[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
+    tma_prefetch_2d(&R2.map_c[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
+  };
   tile_body<false>(R.K, R.F, PS, &R.map_psi[par], &R.map_c[par], R.tab, R.tab_len, R.psi[par ^ 1], R.c[par ^ 1],
-                   nullptr, nullptr, err, none, t % R.nrt, t / R.nrt, nullptr);
+                   nullptr, nullptr, err, none, t % R.nrt, t / R.nrt, nullptr, prefetch);
 }
 
 __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
@@ -861,13 +877,33 @@ __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
 
 }  // namespace
 
+// CTAs of a kernel resident at once on the current device (the prefetch
+// distance of the tile kernels), once per device; -1 on a CUDA error
+static int resident_ctas(const void *kfn, int threads, size_t smem, std::atomic<int> (&cache)[64]) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  int wave = dev >= 0 && dev < 64 ? cache[dev].load(std::memory_order_relaxed) : 0;
+  if (wave == 0) {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return -1;
+    wave = per_sm * sms;
+    if (dev >= 0 && dev < 64) cache[dev].store(wave, std::memory_order_relaxed);
+  }
+  return wave;
+}
+
 int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
                     bool advance, int *err, cudaStream_t st) {
   const size_t smem = sizeof(TileSmem);
   static std::atomic<unsigned long long> attr_done{0};
   if (!smem_limit_once((const void *)ens_tile_kernel, (int)smem, attr_done)) return -3;
+  static std::atomic<int> wave_of[64];
+  const int wave = resident_ctas((const void *)ens_tile_kernel, kThreads, smem, wave_of);
+  if (wave < 0) return -3;
   ens_table_kernel<<<ntblk, kTabBlock, 0, st>>>(runs, tblk);
-  ens_tile_kernel<<<ntiles, kThreads, smem, st>>>(runs, order, err);
+  ens_tile_kernel<<<ntiles, kThreads, smem, st>>>(runs, order, err, wave);
   if (advance) ens_advance_kernel<<<(nruns + 63) / 64, 64, 0, st>>>(const_cast<EnsRun *>(runs), nruns);
   return 0;
 }
@@ -888,19 +924,9 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   auto kfn = surr ? tile_kernel<true> : tile_kernel<false>;
   static std::atomic<unsigned long long> attr_done[2];
   if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr])) return -3;
-  // CTAs resident at once on this device (the prefetch distance), once per device
   static std::atomic<int> wave_of[2][64];
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return -3;
-  int wave = dev >= 0 && dev < 64 ? wave_of[surr][dev].load(std::memory_order_relaxed) : 0;
-  if (wave == 0) {
-    int per_sm = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-      return -3;
-    wave = per_sm * sms;
-    if (dev >= 0 && dev < 64) wave_of[surr][dev].store(wave, std::memory_order_relaxed);
-  }
+  const int wave = resident_ctas((const void *)kfn, kThreads, smem, wave_of[surr]);
+  if (wave < 0) return -3;
   SurrArgs sa = {};
   if (surr) sa = *tm.surr;
   column_table_kernel<<<(tm.col_tab_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(K, P.d0, P.d1, tm.col_tab_len, tm.col_tab);
