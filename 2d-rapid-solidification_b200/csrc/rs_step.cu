@@ -40,9 +40,9 @@
 //     fluxes see neighbour differences of 1e-1..1e2 J/mol).
 //   * Gl - Gs = (1-c) A_Nb + c A_Ti + c(1-c)(L0_Liq - L0_BCC): the ideal-mixing
 //     terms of Gl and Gs (fun.cu:1671-1698) cancel exactly.
-//   * FP64 bulk-melt rows (every psi exactly -1, |s| < 1/9) take
+//   * FP64 rows whose cells all have |s| < 1/9 take
 //     log(c/(1-c)) - log(cinf/(1-cinf)) = 2 atanh(s), s = delta/(2 cinf (1-c)
-//     + delta), as a series to s^15 in place of the division and logarithm;
+//     + delta), as a series to s^15 in place of the logarithm;
 //   * exact shortcuts, warp-uniform: if all nine phi of every cell of the row
 //     are the same +-1, phi_next = phi (phi - phi^3 = 0, g'(+-1) = 0, grad = 0);
 //     if all nine S are 0 (solid, q(1) = 0) the solute update is dc = 0.
@@ -123,14 +123,14 @@ struct Strip {
     constexpr R L0half = R(0.5 * (kL0Bcc - kL0Liq));
     R lam;
     if constexpr (sizeof(R) == 8) {
-      // bulk melt row (every psi exactly -1, |s| < 1/9): log(c/(1-c)) - Lref =
-      // 2 atanh(s), s = delta / (2 cinf (1 - c) + delta), by its series to
-      // s^15 (truncation below 3.3e-17 relative) instead of a division and
-      // a logarithm; the difference is rounding-level, and free of the
+      // rows whose cells all have |s| < 1/9 (the melt, and a solid near the
+      // melt's composition): log(c/(1-c)) - Lref = 2 atanh(s),
+      // s = delta / (2 cinf (1 - c) + delta), by its series to s^15
+      // (truncation below 3.3e-17 relative) instead of a logarithm and a
+      // second division; the difference is rounding-level, and free of the
       // cancellation of log(c/(1-c)) - Lref
-      const bool liq_row = __all_sync(FULL, pv == R(-1));
-      const R sv = liq_row ? d / (R(2) * cinf * omc + d) : R(0);
-      if (liq_row && __all_sync(FULL, fabs(sv) < R(1.0 / 9.0))) {
+      const R sv = d / (R(2) * cinf * omc + d);
+      if (__all_sync(FULL, fabs(sv) < R(1.0 / 9.0))) {
         const R s2 = sv * sv;
         R p = R(1.0 / 15.0);
         p = fma(p, s2, R(1.0 / 13.0));
