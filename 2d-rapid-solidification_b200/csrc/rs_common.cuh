@@ -28,6 +28,25 @@ inline bool smem_limit_once(const void *kernel, int bytes, std::atomic<unsigned 
 }
 }  // namespace rs
 
+namespace rs {
+// CTAs of a kernel resident at once on the current device (occupancy x SMs),
+// computed once per device; -1 on a CUDA error
+inline int resident_ctas(const void *kfn, int threads, size_t smem, std::atomic<int> (&cache)[64]) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  int n = dev >= 0 && dev < 64 ? cache[dev].load(std::memory_order_relaxed) : 0;
+  if (n == 0) {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return -1;
+    n = per_sm * sms;
+    if (dev >= 0 && dev < 64) cache[dev].store(n, std::memory_order_relaxed);
+  }
+  return n;
+}
+}  // namespace rs
+
 #define RS_HD __host__ __device__ __forceinline__
 
 namespace rs {

@@ -16,8 +16,9 @@
 // rs_step_f32.cu.
 //
 // Layout of the work here: a warp owns a strip of 30 output columns (32 input
-// columns with a one-column halo on each side) and marches down H rows.  Each
-// row of psi and c is loaded once per warp with a coalesced 32-lane load
+// columns with a one-column halo on each side) and marches down H rows (H
+// chosen per launch, below).
+// Each row of psi and c is loaded once per warp with a coalesced 32-lane load
 // (issued P rows ahead), the per-cell quantities phi, S = q(psi)c(1-c)
 // (fun.cu:1424-1432) and the chemical potential mu (fun.cu:1443-1452) are
 // computed once per cell, vertical neighbours come from a three-row register
@@ -257,11 +258,12 @@ struct Strip {
 
 // Register-prefetch kernel: every lane loads its own column P rows ahead.
 // Handles the pull-back remap, the coarse-grid temperature and any pitch.
-template <typename R, int H, int P, bool TFC>
+template <typename R, int P, bool TFC>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3)
     step_kernel(const StepCoef K, const Coef<R> F, const StepScalars PS, const typename Tr<R>::S *__restrict__ psi,
                 const typename Tr<R>::S *__restrict__ cst, typename Tr<R>::S *__restrict__ psi_n,
-                typename Tr<R>::S *__restrict__ c_n, typename Tr<R>::S *__restrict__ phi_n, BlockPartial *partials) {
+                typename Tr<R>::S *__restrict__ c_n, typename Tr<R>::S *__restrict__ phi_n, BlockPartial *partials,
+                const int H) {
   using S = typename Tr<R>::S;
   const int nx = K.nx, ny = K.ny, pitch = K.pitch;
   const int wpb = blockDim.x >> 5;
@@ -325,25 +327,42 @@ static int launch(const StepCoef &K, const StepScalars &P, const typename Tr<R>:
   const int wcols = (ni + 29) / 30;
   constexpr int WPB = 4;  // warps per block (adjacent column strips)
   constexpr int PF = 3;   // rows in flight per lane (multiple of the 3-row window)
+  auto kfn = tfc ? step_kernel<R, PF, true> : step_kernel<R, PF, false>;
+  static std::atomic<int> resident_of[2][64];
+  const int resident = resident_ctas((const void *)kfn, 32 * WPB, 0, resident_of[tfc]);
+  if (resident <= 0) return -3;
+  // rows per block.  Frozen temperature, and FP32: 64, halved while the grid
+  // has fewer than 16 warp strips per SM; the blocks at the front take far
+  // longer than the others, and a part-filled last wave absorbs them (a grid
+  // of exactly full waves measured slower with a front, faster without one).
+  // FP64 with the coarse-grid temperature, where every cell evaluates its
+  // CALPHAD groups in FP64 and the blocks cost about the same: the height in
+  // [16, 64] whose grid fills its last wave of resident blocks best, by
+  // (waves) x (H + 4) (H rows, 2 halo rows and about 2 rows' worth of
+  // per-strip setup), among heights giving at least three waves where there
+  // are such (FP32 measured no gain from it)
+  const bool fill = tfc && sizeof(R) == 8;
+  const int ncb = (wcols + WPB - 1) / WPB;
   int H = 64;
-  while (H > 16 && (int64_t)wcols * ((nj + H - 1) / H) < 148 * 16) H /= 2;
-  dim3 block(32 * WPB), grid((nj + H - 1) / H, (wcols + WPB - 1) / WPB);
+  while (!fill && H > 16 && (int64_t)wcols * ((nj + H - 1) / H) < 148 * 16) H /= 2;
+  int64_t best = fill ? INT64_MAX : 0;
+  for (int pass = 0; pass < 2 && best == INT64_MAX; ++pass) {
+    for (int h = 16; h <= 64; ++h) {
+      const int64_t blocks = (int64_t)ncb * ((nj + h - 1) / h);
+      const int64_t waves = (blocks + resident - 1) / resident;
+      if (pass == 0 && waves < 3) continue;
+      const int64_t cost = waves * (h + 4);
+      if (cost < best) {
+        best = cost;
+        H = h;
+      }
+    }
+  }
+  dim3 block(32 * WPB), grid((nj + H - 1) / H, ncb);
   if (grid.y > 65535) return -1;
   const int nw = grid.x * grid.y * WPB;
   if (partials && nw > max_partials) return -1;
-#define RS_LAUNCH(HH)                                                                                   \
-  if (tfc)                                                                                              \
-    step_kernel<R, HH, PF, true><<<grid, block, 0, st>>>(K, F, P, psi, c, psi_n, c_n, phi_n, partials); \
-  else                                                                                                  \
-    step_kernel<R, HH, PF, false><<<grid, block, 0, st>>>(K, F, P, psi, c, psi_n, c_n, phi_n, partials);
-  if (H == 64) {
-    RS_LAUNCH(64)
-  } else if (H == 32) {
-    RS_LAUNCH(32)
-  } else {
-    RS_LAUNCH(16)
-  }
-#undef RS_LAUNCH
+  kfn<<<grid, block, 0, st>>>(K, F, P, psi, c, psi_n, c_n, phi_n, partials, H);
   if (nwarps_out) *nwarps_out = nw;
   return 0;
 }

@@ -877,23 +877,6 @@ __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
 
 }  // namespace
 
-// CTAs of a kernel resident at once on the current device (the prefetch
-// distance of the tile kernels), once per device; -1 on a CUDA error
-static int resident_ctas(const void *kfn, int threads, size_t smem, std::atomic<int> (&cache)[64]) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
-  int wave = dev >= 0 && dev < 64 ? cache[dev].load(std::memory_order_relaxed) : 0;
-  if (wave == 0) {
-    int per_sm = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, smem) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-      return -1;
-    wave = per_sm * sms;
-    if (dev >= 0 && dev < 64) cache[dev].store(wave, std::memory_order_relaxed);
-  }
-  return wave;
-}
-
 int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
                     bool advance, int *err, cudaStream_t st) {
   const size_t smem = sizeof(TileSmem);
