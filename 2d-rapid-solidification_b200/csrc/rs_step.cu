@@ -258,12 +258,14 @@ struct Strip {
 
 // Register-prefetch kernel: every lane loads its own column P rows ahead.
 // Handles the pull-back remap, the coarse-grid temperature and any pitch.
-template <typename R, int P, bool TFC>
+// HC: rows per block fixed at compile time, or 0 for the launch argument H_rt
+template <typename R, int HC, int P, bool TFC>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 3)
     step_kernel(const StepCoef K, const Coef<R> F, const StepScalars PS, const typename Tr<R>::S *__restrict__ psi,
                 const typename Tr<R>::S *__restrict__ cst, typename Tr<R>::S *__restrict__ psi_n,
                 typename Tr<R>::S *__restrict__ c_n, typename Tr<R>::S *__restrict__ phi_n, BlockPartial *partials,
-                const int H) {
+                const int H_rt) {
+  const int H = HC > 0 ? HC : H_rt;
   using S = typename Tr<R>::S;
   const int nx = K.nx, ny = K.ny, pitch = K.pitch;
   const int wpb = blockDim.x >> 5;
@@ -327,10 +329,6 @@ static int launch(const StepCoef &K, const StepScalars &P, const typename Tr<R>:
   const int wcols = (ni + 29) / 30;
   constexpr int WPB = 4;  // warps per block (adjacent column strips)
   constexpr int PF = 3;   // rows in flight per lane (multiple of the 3-row window)
-  auto kfn = tfc ? step_kernel<R, PF, true> : step_kernel<R, PF, false>;
-  static std::atomic<int> resident_of[2][64];
-  const int resident = resident_ctas((const void *)kfn, 32 * WPB, 0, resident_of[tfc]);
-  if (resident <= 0) return -3;
   // rows per block.  Frozen temperature, and FP32: 64, halved while the grid
   // has fewer than 16 warp strips per SM; the blocks at the front take far
   // longer than the others, and a part-filled last wave absorbs them (a grid
@@ -341,11 +339,20 @@ static int launch(const StepCoef &K, const StepScalars &P, const typename Tr<R>:
   // (waves) x (H + 4) (H rows, 2 halo rows and about 2 rows' worth of
   // per-strip setup), among heights giving at least three waves where there
   // are such (FP32 measured no gain from it)
-  const bool fill = tfc && sizeof(R) == 8;
+  constexpr bool kFillable = sizeof(R) == 8;
+  const bool fill = kFillable && tfc;
   const int ncb = (wcols + WPB - 1) / WPB;
   int H = 64;
   while (!fill && H > 16 && (int64_t)wcols * ((nj + H - 1) / H) < 148 * 16) H /= 2;
   int64_t best = fill ? INT64_MAX : 0;
+  int resident = 1;
+  if constexpr (kFillable) {
+    if (fill) {
+      static std::atomic<int> resident_of[64];
+      resident = resident_ctas((const void *)step_kernel<R, 0, PF, true>, 32 * WPB, 0, resident_of);
+      if (resident <= 0) return -3;
+    }
+  }
   for (int pass = 0; pass < 2 && best == INT64_MAX; ++pass) {
     for (int h = 16; h <= 64; ++h) {
       const int64_t blocks = (int64_t)ncb * ((nj + h - 1) / h);
@@ -362,7 +369,20 @@ static int launch(const StepCoef &K, const StepScalars &P, const typename Tr<R>:
   if (grid.y > 65535) return -1;
   const int nw = grid.x * grid.y * WPB;
   if (partials && nw > max_partials) return -1;
-  kfn<<<grid, block, 0, st>>>(K, F, P, psi, c, psi_n, c_n, phi_n, partials, H);
+#define RS_LAUNCH(HC, TF) step_kernel<R, HC, PF, TF><<<grid, block, 0, st>>>(K, F, P, psi, c, psi_n, c_n, phi_n, partials, H)
+  if constexpr (kFillable) {
+    if (fill) RS_LAUNCH(0, true);
+  }
+  if (!fill) {
+    if (H == 64) {
+      if (tfc) RS_LAUNCH(64, true); else RS_LAUNCH(64, false);
+    } else if (H == 32) {
+      if (tfc) RS_LAUNCH(32, true); else RS_LAUNCH(32, false);
+    } else {
+      if (tfc) RS_LAUNCH(16, true); else RS_LAUNCH(16, false);
+    }
+  }
+#undef RS_LAUNCH
   if (nwarps_out) *nwarps_out = nw;
   return 0;
 }
