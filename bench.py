@@ -336,7 +336,7 @@ def fp64_leg(p, flush, nsteps=30):
     cells = (p.nx_all - 2) * (p.ny_all - 2)
     ctx.close()
     return {"value": round(cells / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms, 5), "steps": nsteps,
-            "kernel": "rs::step_kernel<double, 3, false> (register prefetch)",
+            "kernel": "rs::step_kernel<double, H, 3, false> (register prefetch)",
             "note": "median of CUDA-event step times, L2 flushed"}
 
 
