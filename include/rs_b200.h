@@ -318,10 +318,11 @@ int rs_mlp_adam(float *d_w, const float *d_grad, float *d_m, float *d_v, int64_t
 int rs_mlp_forward(const rs_mlp_box *box, const float *d_w, int64_t n, const float *d_x, float *d_out,
                    rs_stream_t stream);
 /* Selects the surrogate for the FP32 step of this context (d_w = NULL: the
- * exact evaluation).  The context keeps a copy of the weights (BF16 for the
- * tensor-core layer, FP32 for the others) and of the box.  Cells whose T or c
- * lie outside the box, and one cell in 1024 per step (audit), are evaluated
- * exactly. */
+ * exact evaluation).  The context keeps a copy of the weights (FP16 for the
+ * two tensor-core layers, FP32 for the first) and of the box.  The network
+ * stands in for the cells outside the exact bulk-melt form; cells whose T or
+ * c lie outside the box, and one cell in 1024 per step of those (audit), are
+ * evaluated exactly. */
 int rs_set_surrogate(rs_ctx *ctx, const float *d_w, const rs_mlp_box *box);
 /* Largest |surrogate - exact| of mu'' and dG over the audited cells and the
  * counts of fallback and audited cells since the last call; clears them.
