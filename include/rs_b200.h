@@ -228,7 +228,7 @@ int rs_precise_tip(rs_ctx *ctx, const rs_fields *f, rs_tip *d_tip, rs_stream_t s
 int rs_precise_tip_noalloc(const rs_params *p, const rs_fields *f, rs_tip *d_tip, rs_stream_t stream);
 
 /* Sum of c over the interior cells in double precision into *d_mass: the
- * numerator of get_average (src/main.cu:1483-1493), reduced on the device. */
+ * numerator of get_average (fun.cu:1756-1766), reduced on the device. */
 int rs_mass(rs_ctx *ctx, const rs_fields *f, double *d_mass, rs_stream_t stream);
 
 /* ---- initial conditions ---- */
