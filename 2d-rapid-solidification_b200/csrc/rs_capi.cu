@@ -66,12 +66,15 @@ struct rs_ctx {
   int32_t pb_offset;   // and its shift (read by rs_integrate_phi)
   float *col_tab;      // per-column CALPHAD table of the FP32 TMA kernel
   int col_tab_len;
+  double *col_tab64;   // and of the FP64 TMA kernel
+  int col_tab64_len;
   rs::SurrArgs surr;   // learned CALPHAD surrogate of the FP32 step (surr.w == nullptr: exact)
   float *mlp_w;        // its FP32 parameters (device)
   uint16_t *mlp_b16;   // FP16 W2 (32 x 32) and W3 padded to 8 rows (device)
   unsigned long long *mlp_audit;  // max error bits of mu'' and dG, fallback and audit counts
   unsigned int *red_counter;  // fused final reduction of the FP32 tile kernel (device, 0 between launches)
   int use_tma;         // RS_OPT_TMA
+  uint32_t wait_limit; // RS_OPT_WAIT_LIMIT (0: the kernels' default)
   TmaEntry tma[8];     // tensor-map cache keyed by field pointer
   int tma_n, tma_next;
 };
@@ -343,6 +346,8 @@ int rs_create(const rs_params *p, rs_ctx **out) {
   if (e == cudaSuccess) e = cudaMemset(c->red_counter, 0, sizeof(unsigned int));
   c->col_tab_len = rs::col_tab_len(p->nx_all);
   if (e == cudaSuccess) e = cudaMalloc(&c->col_tab, sizeof(float) * rs::kColTabFields * c->col_tab_len);
+  c->col_tab64_len = rs::col_tab64_len(p->nx_all);
+  if (e == cudaSuccess) e = cudaMalloc(&c->col_tab64, sizeof(double) * rs::kColTabFields * c->col_tab64_len);
   c->use_tma = 1;
   if (e != cudaSuccess) {
     rs_destroy(c);
@@ -361,6 +366,7 @@ int rs_destroy(rs_ctx *c) {
   cudaFree(c->d_err);
   cudaFree(c->red_counter);
   cudaFree(c->col_tab);
+  cudaFree(c->col_tab64);
   cudaFree(c->mlp_w);
   cudaFree(c->mlp_b16);
   cudaFree(c->mlp_audit);
@@ -401,6 +407,7 @@ static rs::StepScalars step_scalars(const rs_ctx *c, const rs_step_args *a) {
   P.i_offset = a->i_offset;
   P.i_left_end_T = a->i_left_end_T;
   P.i_front = p.i_tip_target;
+  P.wait_limit = c->wait_limit;
   P.T_coarse = (const double *)a->T_coarse;
   return P;
 }
@@ -423,7 +430,7 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
   int lr;
   rs::TmaMaps tm;
   const rs::TmaMaps *tmp = nullptr;
-  // the TMA kernel stores groups of four FP32 columns as 16-byte vectors
+  // the TMA kernels store whole rows by 16-byte bulk copies
   const uintptr_t vec = 16;
   const bool out_aligned =
       ((uintptr_t)next->psi % vec) == 0 && ((uintptr_t)next->c % vec) == 0 && ((uintptr_t)next->phi % vec) == 0;
@@ -431,11 +438,14 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
       field_map(c, cur->c, cur->precision, &tm.c)) {
     tm.col_tab = c->col_tab;
     tm.col_tab_len = c->col_tab_len;
-    tm.surr = c->surr.w ? &c->surr : nullptr;
+    tm.col_tab64 = c->col_tab64;
+    tm.col_tab64_len = c->col_tab64_len;
+    tm.surr = c->surr.w && cur->precision == RS_F32 ? &c->surr : nullptr;
     tm.red = {};
-    if (red && cur->precision == RS_F32) {
+    if (red) {  // both tile kernels reduce their partials themselves
       tm.red.counter = c->red_counter;
-      tm.red.mass_offset = (double)(c->p.nx_all - 2) * (c->p.ny_all - 2) * c->p.cinf;
+      tm.red.mass_offset =
+          cur->precision == RS_F32 ? (double)(c->p.nx_all - 2) * (c->p.ny_all - 2) * c->p.cinf : 0.0;
       tm.red.mass_out = a->mass_out;
       tm.red.itip_out = a->itip_out;
     }
@@ -452,8 +462,8 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
   if (lr == -3) return fail(RS_E_CUDA, "rs_step: cannot configure shared memory of the TMA kernel");
   if (lr) return fail(RS_E_INVALID, "rs_step: grid too large for the reduction workspace");
   if ((rc = cuda_check("rs_step"))) return rc;
-  // (the FP32 tile kernel reduces its partials itself)
-  if (red && !(tmp && cur->precision == RS_F32)) {
+  // (the tile kernels reduce their partials themselves)
+  if (red && !tmp) {
     const double off = cur->precision == RS_F32 ? (double)(c->p.nx_all - 2) * (c->p.ny_all - 2) * c->p.cinf : 0.0;
     rs::launch_reduce_partials(c->partials, nb, off, a->mass_out, a->itip_out, st);
     if ((rc = cuda_check("rs_step reduce"))) return rc;
@@ -466,6 +476,10 @@ int rs_set_option(rs_ctx *c, int32_t option, int64_t value) {
   switch (option) {
     case RS_OPT_TMA:
       c->use_tma = value ? 1 : 0;
+      return RS_OK;
+    case RS_OPT_WAIT_LIMIT:
+      if (value < 0 || value > (int64_t)1 << 30) return fail(RS_E_INVALID, "rs_set_option: wait limit %lld", (long long)value);
+      c->wait_limit = (uint32_t)value;
       return RS_OK;
     default:
       return fail(RS_E_INVALID, "rs_set_option: unknown option %d", option);

@@ -230,6 +230,9 @@ struct StepScalars {
   // 2D step kernels launch their column blocks in (front_first_block);
   // results do not depend on it
   int32_t i_front;
+  // tries of a bounded device-side wait before it gives up (0: the kernel's
+  // default); a test option makes it tiny so that the give-up path runs
+  uint32_t wait_limit;
   const double *T_coarse;
 };
 

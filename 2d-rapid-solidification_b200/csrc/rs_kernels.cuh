@@ -61,19 +61,25 @@ struct FinalRed {
 struct TmaMaps {
   CUtensorMap psi;
   CUtensorMap c;
-  float *col_tab;   // kColTabFields arrays of col_tab_len floats
+  float *col_tab;   // kColTabFields arrays of col_tab_len floats (FP32 step)
   int col_tab_len;
+  double *col_tab64;  // kColTabFields arrays of col_tab64_len doubles (FP64 step)
+  int col_tab64_len;
   const SurrArgs *surr;  // learned CALPHAD surrogate, or nullptr (exact)
   FinalRed red;          // counter, offset and outputs (partials, nparts set by the launcher)
 };
 constexpr int kTileOutW = 128;                  // output columns of an FP32 tile
 constexpr int kTmaBoxW32 = kTileOutW + 8;        // input columns (4 each side keep x 16-byte aligned)
-constexpr int kTmaBoxW64 = 250;  // input columns per CTA window, FP64 (multiple of 2)
-constexpr int kTileRows = 16;    // output rows of an FP32 tile
-constexpr int kTmaBoxH = kTileRows + 2;  // input rows of an FP32 tile
+constexpr int kTileOutW64 = 64;                  // output columns of an FP64 tile
+constexpr int kTmaBoxW64 = kTileOutW64 + 8;      // its input columns
+constexpr int kTileRows = 16;    // output rows of a tile
+constexpr int kTmaBoxH = kTileRows + 2;  // input rows of a tile
 constexpr int kColTabFields = 5;
 // length of the per-column table (entry k is column k - 4) for nx_all columns
 inline int col_tab_len(int nx_all) { return ((nx_all + kTileOutW - 1) / kTileOutW) * kTileOutW + kTmaBoxW32; }
+inline int col_tab64_len(int nx_all) {
+  return ((nx_all + kTileOutW64 - 1) / kTileOutW64) * kTileOutW64 + kTmaBoxW64;
+}
 
 // ---- launchers (return 0, or -1 when a size limit is exceeded)
 int launch_step_f64(const StepCoef &K, const StepScalars &P, const double *psi, const double *c,
@@ -89,6 +95,11 @@ struct Coef;
 // the number of partials written.
 int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScalars &P, const TmaMaps &tm,
                         float *psi_n, float *c_n, float *phi_n, BlockPartial *partials, int max_partials,
+                        int *nparts_out, int *err, cudaStream_t st);
+// FP64 TMA-staged kernel (rs_step_f64t.cu): frozen temperature, no pull-back,
+// even nx_all; column table + tile kernel, final reduction fused.
+int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScalars &P, const TmaMaps &tm,
+                        double *psi_n, double *c_n, double *phi_n, BlockPartial *partials, int max_partials,
                         int *nparts_out, int *err, cudaStream_t st);
 void launch_reduce_partials(const BlockPartial *partials, int n, double mass_offset,
                             double *mass_out, int32_t *itip_out, cudaStream_t st);

@@ -12,12 +12,17 @@
 //
 // Parameters are one flat FP32 vector (RS_MLP_NPARAMS):
 //   W1[32][3], b1[32], W2[32][32], b2[32], W3[2][32], b3[2]   (row = output unit)
+#include <cooperative_groups.h>
+
 #include "rs_mlp.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace rs {
 namespace {
 
 constexpr int kGradThreads = 128;
+constexpr int kGradCtas = 8;  // CTAs of the one gradient cluster (portable size)
 
 __device__ __forceinline__ double mu2_exact(double T, double c, double phi, double cinf, double RR) {
   const TTerms tt = t_terms(T, RR);
@@ -54,13 +59,20 @@ __global__ void sample_kernel(const double cinf, const double RR, const MlpBox b
   y[2 * k + 1] = (float)dG_exact(T, c, RR);
 }
 
-// One thread per sample: forward, loss on the scaled outputs, backward; the
-// per-sample activations and deltas go to shared memory and each thread then
-// sums a share of the weight gradients over the block's samples.
-__global__ void __launch_bounds__(kGradThreads) grad_kernel(const MlpBox box, const float *__restrict__ w,
-                                                            const int64_t n, const float *__restrict__ x,
-                                                            const float *__restrict__ y, float *__restrict__ grad,
-                                                            double *__restrict__ loss) {
+// The gradient of one call is computed by ONE cluster of kGradCtas CTAs, so
+// that its sums have a fixed order and two trainings with the same seed give
+// the same weights: CTA r takes the sample chunks r, r + kGradCtas, ... of
+// kGradThreads samples; per chunk, one thread per sample runs forward, loss
+// and backward into shared memory, and each thread then adds the chunk's
+// contribution to the weight gradients it owns (parameters t, t + 128, ...)
+// in sample order.  At the end CTA 0 adds the CTAs' partial gradients and
+// losses, read from their shared memory (distributed shared memory), in rank
+// order, to grad and loss.
+constexpr int kParamsPerThread = (kMlpNParams + kGradThreads - 1) / kGradThreads;
+
+__global__ void __cluster_dims__(kGradCtas, 1, 1) __launch_bounds__(kGradThreads)
+    grad_kernel(const MlpBox box, const float *__restrict__ w, const int64_t n, const float *__restrict__ x,
+                const float *__restrict__ y, float *__restrict__ grad, double *__restrict__ loss) {
   extern __shared__ float sh[];
   float *sx = sh;                                   // [kGradThreads][3]
   float *h1 = sx + kGradThreads * 3;                // [kGradThreads][H]
@@ -68,81 +80,111 @@ __global__ void __launch_bounds__(kGradThreads) grad_kernel(const MlpBox box, co
   float *d1 = h2 + kGradThreads * kMlpH;            // [kGradThreads][H]
   float *d2 = d1 + kGradThreads * kMlpH;            // [kGradThreads][H]
   float *d3 = d2 + kGradThreads * kMlpH;            // [kGradThreads][2]
+  float *part = d3 + kGradThreads * 2;              // [kMlpNParams] this CTA's gradient
   __shared__ double sloss[kGradThreads / 32];
+  __shared__ double cta_loss;
+  cg::cluster_group cluster = cg::this_cluster();
+  const unsigned rank = cluster.block_rank();
   const MlpView W(w);
   const int t = threadIdx.x;
-  const int64_t k = (int64_t)blockIdx.x * kGradThreads + t;
-  const bool live = k < n;
-  float xi[3] = {0.f, 0.f, 0.f};
-  if (live)
-    for (int q = 0; q < 3; ++q) xi[q] = x[3 * k + q];
-  float z1[kMlpH], a1[kMlpH], z2[kMlpH], a2[kMlpH], o[2];
-  mlp_forward_full(W, xi, z1, a1, z2, a2, o);
-  float e[2] = {0.f, 0.f};
-  double l = 0.0;
-  if (live) {
-    for (int q = 0; q < 2; ++q) {
-      e[q] = o[q] - (float)((y[2 * k + q] - box.y_mean[q]) / box.y_scale[q]);
-      l += (double)e[q] * e[q];
+  float acc[kParamsPerThread];
+#pragma unroll
+  for (int i = 0; i < kParamsPerThread; ++i) acc[i] = 0.f;
+  double lsum = 0.0;  // thread 0: this CTA's loss
+  for (int64_t base = (int64_t)rank * kGradThreads; base < n; base += (int64_t)kGradCtas * kGradThreads) {
+    const int64_t k = base + t;
+    const bool live = k < n;
+    float xi[3] = {0.f, 0.f, 0.f};
+    if (live)
+      for (int q = 0; q < 3; ++q) xi[q] = x[3 * k + q];
+    float z1[kMlpH], a1[kMlpH], z2[kMlpH], a2[kMlpH], o[2];
+    mlp_forward_full(W, xi, z1, a1, z2, a2, o);
+    float e[2] = {0.f, 0.f};
+    double l = 0.0;
+    if (live) {
+      for (int q = 0; q < 2; ++q) {
+        e[q] = o[q] - (float)((y[2 * k + q] - box.y_mean[q]) / box.y_scale[q]);
+        l += (double)e[q] * e[q];
+      }
+    }
+    // backward: dL/do = 2 e (dead samples carry 0 deltas)
+    float g3[2] = {2.f * e[0], 2.f * e[1]};
+    float g2[kMlpH], g1[kMlpH];
+#pragma unroll
+    for (int i = 0; i < kMlpH; ++i) {
+      const float s = g3[0] * W.w3(0, i) + g3[1] * W.w3(1, i);
+      g2[i] = s * silu_grad(z2[i]);
+    }
+#pragma unroll
+    for (int j = 0; j < kMlpH; ++j) {
+      float s = 0.f;
+#pragma unroll
+      for (int i = 0; i < kMlpH; ++i) s += g2[i] * W.w2(i, j);
+      g1[j] = s * silu_grad(z1[j]);
+    }
+    for (int q = 0; q < 3; ++q) sx[t * 3 + q] = xi[q];
+    for (int i = 0; i < kMlpH; ++i) {
+      h1[t * kMlpH + i] = a1[i];
+      h2[t * kMlpH + i] = a2[i];
+      d1[t * kMlpH + i] = g1[i];
+      d2[t * kMlpH + i] = g2[i];
+    }
+    d3[t * 2 + 0] = g3[0];
+    d3[t * 2 + 1] = g3[1];
+    for (int off = 16; off > 0; off >>= 1) l += __shfl_down_sync(0xffffffffu, l, off);
+    if ((t & 31) == 0) sloss[t >> 5] = l;
+    __syncthreads();
+    if (t == 0)
+      for (int q = 0; q < kGradThreads / 32; ++q) lsum += sloss[q];
+    // this chunk's weight gradients, summed over its samples in order
+#pragma unroll
+    for (int i = 0; i < kParamsPerThread; ++i) {
+      const int p = t + i * kGradThreads;
+      if (p >= kMlpNParams) break;
+      float s = 0.f;
+      if (p < kOffB1) {  // W1[h][q]
+        const int h = p / 3, q = p % 3;
+        for (int m = 0; m < kGradThreads; ++m) s += d1[m * kMlpH + h] * sx[m * 3 + q];
+      } else if (p < kOffW2) {
+        const int h = p - kOffB1;
+        for (int m = 0; m < kGradThreads; ++m) s += d1[m * kMlpH + h];
+      } else if (p < kOffB2) {  // W2[i][j]
+        const int i2 = (p - kOffW2) / kMlpH, j = (p - kOffW2) % kMlpH;
+        for (int m = 0; m < kGradThreads; ++m) s += d2[m * kMlpH + i2] * h1[m * kMlpH + j];
+      } else if (p < kOffW3) {
+        const int i2 = p - kOffB2;
+        for (int m = 0; m < kGradThreads; ++m) s += d2[m * kMlpH + i2];
+      } else if (p < kOffB3) {  // W3[q][i]
+        const int q = (p - kOffW3) / kMlpH, i2 = (p - kOffW3) % kMlpH;
+        for (int m = 0; m < kGradThreads; ++m) s += d3[m * 2 + q] * h2[m * kMlpH + i2];
+      } else {
+        const int q = p - kOffB3;
+        for (int m = 0; m < kGradThreads; ++m) s += d3[m * 2 + q];
+      }
+      acc[i] += s;
+    }
+    __syncthreads();  // the chunk's arrays are read before the next chunk writes them
+  }
+#pragma unroll
+  for (int i = 0; i < kParamsPerThread; ++i) {
+    const int p = t + i * kGradThreads;
+    if (p < kMlpNParams) part[p] = acc[i];
+  }
+  if (t == 0) cta_loss = lsum;
+  cluster.sync();  // every CTA's partial is in its shared memory
+  if (rank == 0) {
+    for (int p = t; p < kMlpNParams; p += kGradThreads) {
+      float s = 0.f;
+      for (unsigned r = 0; r < kGradCtas; ++r) s += cluster.map_shared_rank(part, r)[p];
+      grad[p] += s;
+    }
+    if (t == 0) {
+      double l = 0.0;
+      for (unsigned r = 0; r < kGradCtas; ++r) l += *cluster.map_shared_rank(&cta_loss, r);
+      *loss += l;
     }
   }
-  // backward: dL/do = 2 e
-  float g3[2] = {2.f * e[0], 2.f * e[1]};
-  float g2[kMlpH], g1[kMlpH];
-#pragma unroll
-  for (int i = 0; i < kMlpH; ++i) {
-    const float s = g3[0] * W.w3(0, i) + g3[1] * W.w3(1, i);
-    g2[i] = s * silu_grad(z2[i]);
-  }
-#pragma unroll
-  for (int j = 0; j < kMlpH; ++j) {
-    float s = 0.f;
-#pragma unroll
-    for (int i = 0; i < kMlpH; ++i) s += g2[i] * W.w2(i, j);
-    g1[j] = s * silu_grad(z1[j]);
-  }
-  for (int q = 0; q < 3; ++q) sx[t * 3 + q] = xi[q];
-  for (int i = 0; i < kMlpH; ++i) {
-    h1[t * kMlpH + i] = a1[i];
-    h2[t * kMlpH + i] = a2[i];
-    d1[t * kMlpH + i] = g1[i];
-    d2[t * kMlpH + i] = g2[i];
-  }
-  d3[t * 2 + 0] = g3[0];
-  d3[t * 2 + 1] = g3[1];
-  // block loss
-  for (int off = 16; off > 0; off >>= 1) l += __shfl_down_sync(0xffffffffu, l, off);
-  if ((t & 31) == 0) sloss[t >> 5] = l;
-  __syncthreads();
-  if (t == 0) {
-    double s = 0.0;
-    for (int q = 0; q < kGradThreads / 32; ++q) s += sloss[q];
-    atomicAdd(loss, s);
-  }
-  // weight gradients summed over the block's samples (dead samples carry 0 deltas)
-  for (int p = t; p < kMlpNParams; p += kGradThreads) {
-    float s = 0.f;
-    if (p < kOffB1) {  // W1[h][q]
-      const int h = p / 3, q = p % 3;
-      for (int m = 0; m < kGradThreads; ++m) s += d1[m * kMlpH + h] * sx[m * 3 + q];
-    } else if (p < kOffW2) {
-      const int h = p - kOffB1;
-      for (int m = 0; m < kGradThreads; ++m) s += d1[m * kMlpH + h];
-    } else if (p < kOffB2) {  // W2[i][j]
-      const int i = (p - kOffW2) / kMlpH, j = (p - kOffW2) % kMlpH;
-      for (int m = 0; m < kGradThreads; ++m) s += d2[m * kMlpH + i] * h1[m * kMlpH + j];
-    } else if (p < kOffW3) {
-      const int i = p - kOffB2;
-      for (int m = 0; m < kGradThreads; ++m) s += d2[m * kMlpH + i];
-    } else if (p < kOffB3) {  // W3[q][i]
-      const int q = (p - kOffW3) / kMlpH, i = (p - kOffW3) % kMlpH;
-      for (int m = 0; m < kGradThreads; ++m) s += d3[m * 2 + q] * h2[m * kMlpH + i];
-    } else {
-      const int q = p - kOffB3;
-      for (int m = 0; m < kGradThreads; ++m) s += d3[m * 2 + q];
-    }
-    atomicAdd(&grad[p], s);
-  }
+  cluster.sync();  // CTA 0 has read the others' shared memory before they exit
 }
 
 // Adam (Kingma & Ba 2015) on the gradient scaled by `scale` (1 / batch size)
@@ -185,11 +227,10 @@ int launch_mlp_sample(double cinf, double RR, const MlpBox &box, int64_t n, uint
 int launch_mlp_grad(const MlpBox &box, const float *w, int64_t n, const float *x, const float *y, float *grad,
                     double *loss, cudaStream_t st) {
   if (n <= 0) return 0;
-  const size_t smem = sizeof(float) * kGradThreads * (3 + 4 * kMlpH + 2);
+  const size_t smem = sizeof(float) * (kGradThreads * (3 + 4 * kMlpH + 2) + kMlpNParams);
   static std::atomic<unsigned long long> attr{0};
   if (!smem_limit_once((const void *)grad_kernel, (int)smem, attr)) return -3;
-  grad_kernel<<<(unsigned)((n + kGradThreads - 1) / kGradThreads), kGradThreads, smem, st>>>(box, w, n, x, y, grad,
-                                                                                             loss);
+  grad_kernel<<<kGradCtas, kGradThreads, smem, st>>>(box, w, n, x, y, grad, loss);  // one cluster
   return 0;
 }
 

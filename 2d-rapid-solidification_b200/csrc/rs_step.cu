@@ -11,9 +11,9 @@
 //   * ghost cells (compute_boundary_individual, fun.cu:1220-1230) are written
 //     by the cell they copy, corners included.
 //
-// Two kernels: this file's register-prefetch kernel (FP64, pull-back steps,
-// coarse-grid temperature) and the TMA-staged FP32 tile kernel of
-// rs_step_f32.cu.
+// Three kernels: this file's register-prefetch kernel (pull-back steps, the
+// coarse-grid temperature, unaligned fields) and the TMA-staged tile kernels
+// of rs_step_f32.cu (FP32) and rs_step_f64t.cu (FP64).
 //
 // Layout of the work here: a warp owns a strip of 30 output columns (32 input
 // columns with a one-column halo on each side) and marches down H rows (H
@@ -323,9 +323,14 @@ static int launch(const StepCoef &K, const StepScalars &P, const typename Tr<R>:
   const Coef<R> F = make_coef<R>(K);
   const int ni = K.nx - 2, nj = K.ny - 2;
   const bool tfc = K.tfc != 0;
-  if (tm && !tfc && !P.pull_back && sizeof(R) == 4)
-    return launch_step_f32_tma(K, make_coef<float>(K), P, *tm, (float *)psi_n, (float *)c_n, (float *)phi_n,
-                               partials, max_partials, nwarps_out, err, st);
+  if (tm && !tfc && !P.pull_back) {
+    if constexpr (sizeof(R) == 4)
+      return launch_step_f32_tma(K, make_coef<float>(K), P, *tm, (float *)psi_n, (float *)c_n, (float *)phi_n,
+                                 partials, max_partials, nwarps_out, err, st);
+    else
+      return launch_step_f64_tma(K, F, P, *tm, (double *)psi_n, (double *)c_n, (double *)phi_n, partials,
+                                 max_partials, nwarps_out, err, st);
+  }
   const int wcols = (ni + 29) / 30;
   constexpr int WPB = 4;  // warps per block (adjacent column strips)
   constexpr int PF = 3;   // rows in flight per lane (multiple of the 3-row window)

@@ -295,14 +295,89 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       }
     }
   };
+  // the partial sums of this tile and the fused final reduction (the last
+  // CTA to finish sums every partial, in reduce_partials_kernel's order)
+  auto finish = [&](double mass, int itip) {
+    if (!part) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mass += __shfl_down_sync(FULL, mass, o);
+    itip = __reduce_max_sync(FULL, itip);
+    if (lane == 0) {
+      sm.part_mass[warp] = mass;
+      sm.part_itip[warp] = itip;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      BlockPartial b;
+      b.mass = 0.0;
+      b.itip = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) {
+        b.mass += sm.part_mass[w];
+        b.itip = max(b.itip, sm.part_itip[w]);
+      }
+      b.pad = 0;
+      *part = b;
+    }
+    if (!FR) return;
+    if (threadIdx.x == 0) {
+      __threadfence();
+      sm.last = atomicAdd(FR->counter, 1u) == (unsigned)(FR->nparts - 1);
+    }
+    __syncthreads();
+    if (!sm.last) return;
+    __threadfence();
+    double *sm_m = reinterpret_cast<double *>(&sm.S[0][0]);  // S and mu are free now
+    int *sm_i = reinterpret_cast<int *>(&sm.mu[0][0]);
+    for (int v = threadIdx.x; v < 256; v += kThreads) {
+      double m = 0.0;
+      int it = 0;
+      for (int k = v; k < FR->nparts; k += 256) {
+        m += __ldcg(&FR->partials[k].mass);
+        it = max(it, __ldcg(&FR->partials[k].itip));
+      }
+      sm_m[v] = m;
+      sm_i[v] = it;
+    }
+    __syncthreads();
+    for (int sz = 128; sz > 0; sz >>= 1) {
+      for (int v = threadIdx.x; v < sz; v += kThreads) {
+        sm_m[v] += sm_m[v + sz];
+        sm_i[v] = max(sm_i[v], sm_i[v + sz]);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      if (FR->mass_out) *FR->mass_out = sm_m[0] + FR->mass_offset;
+      if (FR->itip_out) *FR->itip_out = max(1, sm_i[0]);  // get_itip_all_grain starts at 1
+      *FR->counter = 0u;
+    }
+  };
   __syncthreads();  // barrier initialised, flags cleared
   {
+    // bounded wait for the tile; if any thread gives up, the whole CTA skips
+    // the tile: no phase runs on a partly filled tile and nothing is stored.
+    // Thread 0 first waits (bounded again) for the load still in flight into
+    // this CTA's shared memory, and the CTA still reports a (zero) partial,
+    // so the fused final reduction keeps its count
+    const uint32_t limit = PS.wait_limit ? PS.wait_limit : kWaitLimit;
     uint32_t tries = 0;
+    bool gave_up = false;
     while (!mbar_try_wait(&sm.full, 0)) {
-      if (++tries >= kWaitLimit) {
-        atomicExch(err, 1);
+      if (++tries >= limit) {
+        gave_up = true;
         break;
       }
+    }
+    if (__syncthreads_or(gave_up)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        for (uint32_t t = 0; t < kWaitLimit && !mbar_try_wait(&sm.full, 0); ++t) {
+        }
+      }
+      __syncthreads();
+      finish(0.0, 0);
+      return;
     }
   }
   // columns beyond the array (right-most tiles; zero-filled by TMA) become
@@ -726,63 +801,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     }
   }
 
-  if (part) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mass += __shfl_down_sync(FULL, mass, o);
-    itip = __reduce_max_sync(FULL, itip);
-    if (lane == 0) {
-      sm.part_mass[warp] = mass;
-      sm.part_itip[warp] = itip;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      BlockPartial b;
-      b.mass = 0.0;
-      b.itip = 0;
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) {
-        b.mass += sm.part_mass[w];
-        b.itip = max(b.itip, sm.part_itip[w]);
-      }
-      b.pad = 0;
-      *part = b;
-    }
-    if (FR) {  // the last CTA to finish sums every partial (reduce_partials_kernel order)
-      if (threadIdx.x == 0) {
-        __threadfence();
-        sm.last = atomicAdd(FR->counter, 1u) == (unsigned)(FR->nparts - 1);
-      }
-      __syncthreads();
-      if (sm.last) {
-        __threadfence();
-        double *sm_m = reinterpret_cast<double *>(&sm.S[0][0]);  // S and mu are free now
-        int *sm_i = reinterpret_cast<int *>(&sm.mu[0][0]);
-        for (int v = threadIdx.x; v < 256; v += kThreads) {
-          double m = 0.0;
-          int it = 0;
-          for (int k = v; k < FR->nparts; k += 256) {
-            m += __ldcg(&FR->partials[k].mass);
-            it = max(it, __ldcg(&FR->partials[k].itip));
-          }
-          sm_m[v] = m;
-          sm_i[v] = it;
-        }
-        __syncthreads();
-        for (int sz = 128; sz > 0; sz >>= 1) {
-          for (int v = threadIdx.x; v < sz; v += kThreads) {
-            sm_m[v] += sm_m[v + sz];
-            sm_i[v] = max(sm_i[v], sm_i[v + sz]);
-          }
-          __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-          if (FR->mass_out) *FR->mass_out = sm_m[0] + FR->mass_offset;
-          if (FR->itip_out) *FR->itip_out = max(1, sm_i[0]);  // get_itip_all_grain starts at 1
-          *FR->counter = 0u;
-        }
-      }
-    }
-  }
+  finish(mass, itip);
   // shared memory stays allocated until the copies have read it
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }

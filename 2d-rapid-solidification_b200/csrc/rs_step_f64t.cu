@@ -1,0 +1,727 @@
+// rs_step_f64t.cu — the FP64 (exact, drop-in) fused phase-field step on
+// TMA-staged tiles.
+//
+// Same equations as the register-prefetch kernel of rs_step.cu
+// (compute_phi / compute_psi / compute_c_CALPHAD, fun.cu:1143-1467) and the
+// same tile organisation as the FP32 kernel of rs_step_f32.cu, in FP64 on the
+// reference's own field layout (psi and c as doubles).  One step is two
+// launches:
+//   * column_table_kernel_f64: the per-column CALPHAD groups of this step's
+//     frozen temperature (col_terms, get_delta fun.cu:1610-1619) in FP64;
+//   * tile_kernel_f64, launched as a programmatic dependent of the table
+//     kernel: its CTAs start, issue their TMA loads, and wait for the table
+//     only where they first read it.
+//
+// A CTA of 128 threads owns a tile of 16 output rows x 64 output columns
+// (x0 .. x0+63, x0 a multiple of 64).  Its input, 18 rows x 72 columns
+// (x0-4 .. x0+67, so the TMA x coordinate stays 16-byte aligned), arrives in
+// shared memory by one TMA box per field.  Two adjacent columns per lane
+// (16-byte double2 shared-memory accesses).
+//   phase 1  per-cell S = q(psi) c (1-c) and mu'' of the 18 input rows into
+//            shared memory, with per-row flags "every psi == -1" / "== +1"
+//            and per-lane phi masks; the halo columns x0-1 and x0+64 are
+//            computed by 36 threads of warps 2 and 3 (one input row fewer);
+//   phase 2  each warp computes 4 output rows: face fluxes from the shared S
+//            and mu'' (neighbours straight from shared memory), the c update
+//            (kept in registers); cells whose 3x3 phi neighbourhood is not
+//            uniformly +-1 are listed;
+//   phase 3  the listed interface cells are updated one per thread;
+//   phase 4  new psi and c are written into the shared tile, ghost columns
+//            copied there, and each output row leaves by one bulk async copy
+//            per field (ghost rows by one more, except in row-band mode);
+//   partials the solute mass (FP64) and coarse tip of the tile; the last CTA
+//            to finish reduces them all.
+// Arithmetic (identical mathematics to the reference, regrouped as in the
+// FP32 tile kernel):
+//   * mu = K(T) + C0(T) + mu'', C0 = -D - (L0_BCC - L0_Liq)(1 - 2 cinf)/2, so
+//       mu'' = -(g+1) C0 - delta (L0_BCC + L0_Liq + g (L0_BCC - L0_Liq)) + RT lam
+//     and K + C0 enters only through its column differences dK;
+//   * lam = log(c/(1-c)) - log(cinf/(1-cinf)) = 2 atanh(s),
+//     s = delta / (2 cinf (1-c) + delta), by its series to s^15 where every
+//     cell of the warp's row has |s| < 1/9 (truncation below 3.3e-17
+//     relative), else by the logarithm;
+//   * bulk melt rows (psi = -1 exactly, delta in the series range): g = -1,
+//     q = 1, so mu'' = -2 L0_Liq delta + RT lam and S = c (1 - c);
+//   * deep solid rows (psi = +1 over the 3x3 neighbourhoods) store
+//     S = mu'' = 0: every face weight touching them is 0;
+//   * face weights by pair sums (6 P_i + P_{i-1} + P_{i+1}, four times the
+//     1.5 / 0.25 weights, the 4 folded into the flux constant); face fluxes
+//     are rounded products, so a cell's result does not depend on the tiling.
+// Launch order: the tile columns from the one holding the front
+// (front_first_block).  After phase 1 each CTA prefetches into L2 the input
+// tile of the block launched one resident wave later.
+#include "rs_step_common.cuh"
+
+namespace rs {
+namespace {
+
+constexpr int kW = kTileOutW64;   // output columns of a tile
+constexpr int kWin = kTmaBoxW64;  // input columns of a tile (kW + 8)
+constexpr int kTR = kTileRows;    // output rows of a tile
+constexpr int kTRin = kTmaBoxH;   // input rows of a tile
+constexpr int kThreads = 128;
+constexpr int kWarps = kThreads / 32;
+constexpr int kRowsPerWarp = kTR / kWarps;
+constexpr int kHaloL = 3, kHaloR = kW + 4;  // box columns of x0-1 and x0+kW
+constexpr uint32_t kWaitLimit = 1u << 20;
+constexpr unsigned FULL = 0xffffffffu;
+constexpr unsigned long long kMinus1 = 0xBFF0000000000000ull, kPlus1 = 0x3FF0000000000000ull;
+static_assert(kW == 32 * 2, "two columns per lane");
+static_assert(kTR % kWarps == 0 && kRowsPerWarp == 4, "four output rows per warp");
+static_assert(kTRin <= 32, "row flags are 32-bit masks");
+static_assert(64 + 2 * kTRin <= kThreads && 4 * kTR <= kThreads, "one thread per halo cell and per row copy");
+
+// column table arrays (kColTabFields of them, len doubles each); entry k
+// describes column k - 4
+enum { kTabRT = 0, kTabC0 = 1, kTabDK = 2, kTabAnb = 3, kTabAti = 4 };
+
+struct alignas(128) TileSmem64 {
+  // TMA destinations (128-byte aligned); rows 1..16 receive the new psi / c
+  alignas(128) double psi[kTRin][kWin];
+  alignas(128) double c[kTRin][kWin];
+  alignas(16) double S[kTRin][kWin];  // after phase 2: new psi of the listed cells
+  alignas(16) double mu[kTRin][kWin];
+  uint16_t list[kTR * kW];   // interface cells: row << 8 | output column
+  uint8_t pmask[kTRin][32];  // per lane: bits 0-1 psi <= -1, bits 4-5 psi >= 1 of its two cells
+  uint8_t hmask[kTRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
+  uint32_t liq, sol;         // bit r: every cell of input row r has psi == -1 / +1
+  int nlist;
+  double part_mass[kWarps];
+  int part_itip[kWarps];
+  uint64_t full;
+  int last;  // this CTA finished last (fused final reduction)
+};
+
+static_assert(offsetof(TileSmem64, psi) % 128 == 0 && offsetof(TileSmem64, c) % 128 == 0,
+              "TMA destinations start on 128-byte boundaries");
+static_assert((kWin * sizeof(double)) % 16 == 0, "rows stay 16-byte aligned for double2 and bulk copies");
+
+__device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
+__device__ __forceinline__ void st2(double *p, double a, double b) {
+  *reinterpret_cast<double2 *>(p) = make_double2(a, b);
+}
+__device__ __forceinline__ double clamp1(double v) { return fmin(fmax(v, -1.0), 1.0); }
+__device__ __forceinline__ unsigned long long bits(double v) { return (unsigned long long)__double_as_longlong(v); }
+
+// 2 atanh(s) by its odd series to s^15 (|s| < 1/9: truncation below
+// 3.3e-17 relative)
+__device__ __forceinline__ double lam_series(double s) {
+  const double s2 = s * s;
+  double p = 1.0 / 15.0;
+  p = fma(p, s2, 1.0 / 13.0);
+  p = fma(p, s2, 1.0 / 11.0);
+  p = fma(p, s2, 1.0 / 9.0);
+  p = fma(p, s2, 1.0 / 7.0);
+  p = fma(p, s2, 1.0 / 5.0);
+  p = fma(p, s2, 1.0 / 3.0);
+  return 2.0 * fma(s * s2, p, s);
+}
+
+// general per-cell terms (fun.cu:1424-1452); series: use 2 atanh(s)
+__device__ __forceinline__ void cell_terms(const Coef<double> &F, double pv, double c, double s, bool series,
+                                           double RT, double C0, double &S, double &mu) {
+  constexpr double L0sum = kL0Bcc + kL0Liq;
+  constexpr double L0half = 0.5 * (kL0Bcc - kL0Liq);
+  const double om = 1.0 - c, dv = c - F.cinf;
+  const double a = 1.0 - pv;
+  S = (0.5 * F.AA * a - 0.25 * (F.AA - 1.0) * (a * a)) * c * om;
+  const double p2 = pv * pv;
+  const double g = pv * (1.875 + p2 * (-1.25 + 0.375 * p2));
+  const double lam = series ? lam_series(s) : Tr<double>::lam(c, om, dv, F.cinf, F.Lref);
+  mu = -(g + 1.0) * C0 - dv * fma(2.0 * L0half, g, L0sum) + RT * lam;
+}
+
+// shared -> global bulk copy (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_store(void *gdst, const void *ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(ssrc)),
+               "r"(bytes)
+               : "memory");
+}
+
+// One thread per column, one exact FP64 col_terms each; K + C0 of the next
+// column comes from the neighbouring thread, so blocks overlap by one column
+// and write 127 entries.
+constexpr int kTabBlock = 128;
+__global__ void __launch_bounds__(kTabBlock) column_table_kernel_f64(const StepCoef K, const double d0,
+                                                                     const double d1, const int len,
+                                                                     double *__restrict__ tab) {
+  // the tile kernel may start now; it waits for this grid before reading tab
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  __shared__ double kc[kTabBlock];
+  const int k = blockIdx.x * (kTabBlock - 1) + threadIdx.x;  // table entry; column k - 4
+  const int gi = min(max(k - 4, 0), K.nx - 1);
+  const double T = (d0 + d1 * gi) * K.deltaT0 + K.Tmelt;  // get_delta, fun.cu:1610-1619
+  const ColT<double> ct = col_terms<double>(K, T);
+  const double C0 = -ct.D - 0.5 * (kL0Bcc - kL0Liq) * (1.0 - 2.0 * K.cinf);
+  kc[threadIdx.x] = ct.Kc + C0;
+  __syncthreads();
+  if (threadIdx.x == kTabBlock - 1 || k >= len) return;
+  tab[kTabRT * len + k] = ct.RT;
+  tab[kTabC0 * len + k] = C0;
+  tab[kTabDK * len + k] = kc[threadIdx.x + 1] - kc[threadIdx.x];  // (K + C0)(i+1) - (K + C0)(i)
+  tab[kTabAnb * len + k] = ct.A_nb;
+  tab[kTabAti * len + k] = ct.A_ti;
+}
+
+__global__ void __launch_bounds__(kThreads, 5)
+    tile_kernel_f64(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<double> F,
+                    const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
+                    const __grid_constant__ CUtensorMap tm_c, const double *__restrict__ tab, const int tab_len,
+                    double *__restrict__ psi_n, double *__restrict__ c_n, double *__restrict__ phi_n,
+                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int wave) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  TileSmem64 &sm = *reinterpret_cast<TileSmem64 *>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // blockIdx.x walks the tile rows of one tile column (they share halo rows
+  // in L2), blockIdx.y the tile columns, from the one holding column PS.i_front
+  const int f = max(PS.i_front, 0) / kW;
+  const int tr = blockIdx.x;
+  const int tc = front_first_block((int)blockIdx.y, f, (int)gridDim.y);
+  const int x0 = kW * tc;       // first output column of the tile
+  const int y0 = 1 + kTR * tr;  // first output row; input rows y0-1 .. y0+kTR
+  BlockPartial *part = partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr;
+  const FinalRed *FRp = partials && FR.counter ? &FR : nullptr;
+  constexpr uint32_t kTileBytes = 2u * kTRin * kWin * sizeof(double);
+
+  if (smem_u32(smem_raw) & 127u) {  // TMA destinations must be 128-byte aligned
+    if (threadIdx.x == 0) atomicExch(err, 2);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.full, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_expect_tx(&sm.full, kTileBytes);
+    tma_load_2d(&sm.psi[0][0], &tm_psi, &sm.full, x0 - 4, y0 - 1);
+    tma_load_2d(&sm.c[0][0], &tm_c, &sm.full, x0 - 4, y0 - 1);
+    sm.liq = 0u;
+    sm.sol = 0u;
+    sm.nlist = 0;
+  }
+
+  const int col = 2 * lane;  // tile column of this lane's first cell
+  const int gi = x0 + col;   // its global column
+  const int bc = col + 4;    // its box column
+  uint32_t outm = 0;         // per cell: an interior (output) cell
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+    if (gi + q >= 1 && gi + q <= K.nx - 2) outm |= 1u << q;
+  const double cinf = F.cinf;
+  const double cflux4 = 0.25 * F.cflux;
+  constexpr double KL = -2.0 * kL0Liq;
+  // delta range of the bulk-melt form: s = delta / (A + B delta) with
+  // A = 2 cinf (1 - cinf), B = 1 - 2 cinf, so |s| < 1/9 for
+  // -A/(9+B) < delta < A/(9-B) (taken 0.1 % inside)
+  const double sA = 2.0 * cinf * (1.0 - cinf), sB = 1.0 - 2.0 * cinf;
+  const double d_hi = 0.999 * sA / (9.0 - sB), d_lo = -0.999 * sA / (9.0 + sB);
+
+  // the partial sums of this tile and the fused final reduction (the last
+  // CTA to finish sums every partial, in reduce_partials_kernel's order)
+  auto finish = [&](double mass, int itip) {
+    if (!part) return;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mass += __shfl_down_sync(FULL, mass, o);
+    itip = __reduce_max_sync(FULL, itip);
+    if (lane == 0) {
+      sm.part_mass[warp] = mass;
+      sm.part_itip[warp] = itip;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      BlockPartial b;
+      b.mass = 0.0;
+      b.itip = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) {
+        b.mass += sm.part_mass[w];
+        b.itip = max(b.itip, sm.part_itip[w]);
+      }
+      b.pad = 0;
+      *part = b;
+    }
+    if (!FRp) return;
+    if (threadIdx.x == 0) {
+      __threadfence();
+      sm.last = atomicAdd(FRp->counter, 1u) == (unsigned)(FRp->nparts - 1);
+    }
+    __syncthreads();
+    if (!sm.last) return;
+    __threadfence();
+    double *sm_m = &sm.S[0][0];  // S and mu are free now
+    int *sm_i = reinterpret_cast<int *>(&sm.mu[0][0]);
+    for (int v = threadIdx.x; v < 256; v += kThreads) {
+      double m = 0.0;
+      int it = 0;
+      for (int k = v; k < FRp->nparts; k += 256) {
+        m += __ldcg(&FRp->partials[k].mass);
+        it = max(it, __ldcg(&FRp->partials[k].itip));
+      }
+      sm_m[v] = m;
+      sm_i[v] = it;
+    }
+    __syncthreads();
+    for (int sz = 128; sz > 0; sz >>= 1) {
+      for (int v = threadIdx.x; v < sz; v += kThreads) {
+        sm_m[v] += sm_m[v + sz];
+        sm_i[v] = max(sm_i[v], sm_i[v + sz]);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      if (FRp->mass_out) *FRp->mass_out = sm_m[0] + FRp->mass_offset;
+      if (FRp->itip_out) *FRp->itip_out = max(1, sm_i[0]);  // get_itip_all_grain starts at 1
+      *FRp->counter = 0u;
+    }
+  };
+
+  // the column table of this step (programmatic dependency on its kernel)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const double *tRT = tab + kTabRT * tab_len + 4, *tC0 = tab + kTabC0 * tab_len + 4;
+  const double *tDK = tab + kTabDK * tab_len + 4;
+  const double *tAnb = tab + kTabAnb * tab_len + 4, *tAti = tab + kTabAti * tab_len + 4;
+  const double2 RTv = ld2(tRT + gi), C0v = ld2(tC0 + gi);
+  const double RTa[2] = {RTv.x, RTv.y}, C0a[2] = {C0v.x, C0v.y};
+
+  // per lane, bit q: psi is exactly +1 over the 3x3 neighbourhood of cell
+  // bc+q (rows of the box only; column -1 of the left-most tile enters no
+  // face, column 0 being a ghost).  S = q(1) c (1 - c) = 0 there, so every
+  // face weight touching the cell is 0 and its mu'' enters no flux
+  auto solid3 = [&](int rr) -> uint32_t {
+    const int xh = lane == 0 ? kHaloL : kHaloR;
+    uint32_t v = 0x3u;
+    bool hs = true;  // the halo column beside lanes 0 and 31
+    for (int r2 = max(rr - 1, 0); r2 <= min(rr + 1, kTRin - 1); ++r2) {
+      const double2 q2 = ld2(&sm.psi[r2][bc]);
+      v &= (bits(q2.x) == kPlus1 ? 1u : 0u) | (bits(q2.y) == kPlus1 ? 2u : 0u);
+      hs = hs && bits(sm.psi[r2][xh]) == kPlus1;
+    }
+    uint32_t lf = __shfl_up_sync(FULL, v >> 1, 1) & 1u, rt = __shfl_down_sync(FULL, v, 1) & 1u;
+    if (lane == 0) lf = (hs || x0 == 0) ? 1u : 0u;
+    if (lane == 31) rt = hs ? 1u : 0u;
+    const uint32_t e = lf | (v << 1) | (rt << 3);  // bit k: box column bc-1+k
+    return e & (e >> 1) & (e >> 2) & 0x3u;
+  };
+
+  __syncthreads();  // barrier initialised, flags cleared
+  {
+    // bounded wait for the tile; if any thread gives up, the whole CTA skips
+    // the tile: no phase runs on a partly filled tile and nothing is stored.
+    // Thread 0 first waits (bounded again) for the load still in flight into
+    // this CTA's shared memory, and the CTA still reports a (zero) partial,
+    // so the fused final reduction keeps its count
+    const uint32_t limit = PS.wait_limit ? PS.wait_limit : kWaitLimit;
+    uint32_t tries = 0;
+    bool gave_up = false;
+    while (!mbar_try_wait(&sm.full, 0)) {
+      if (++tries >= limit) {
+        gave_up = true;
+        break;
+      }
+    }
+    if (__syncthreads_or(gave_up)) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        for (uint32_t t = 0; t < kWaitLimit && !mbar_try_wait(&sm.full, 0); ++t) {
+        }
+      }
+      __syncthreads();
+      finish(0.0, 0);
+      return;
+    }
+  }
+  // columns beyond the array (right-most tiles; zero-filled by TMA) become
+  // bulk melt, so they never force the general path; no output reads them
+  if (x0 + kW + 4 > K.nx) {
+    for (int k = threadIdx.x; k < kTRin * kWin; k += kThreads) {
+      const int rr = k / kWin, x = k % kWin;
+      if (x0 - 4 + x >= K.nx) {
+        sm.psi[rr][x] = -1.0;
+        sm.c[rr][x] = cinf;
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- phase 1: per-cell terms; warp w takes input rows w, w+4, ...
+#pragma unroll 1
+  for (int rr = warp; rr < kTRin; rr += kWarps) {
+    if (y0 - 1 + rr > K.ny - 1) {  // beyond the array (last tile): never read by an output
+      st2(&sm.S[rr][bc], 0.0, 0.0);
+      st2(&sm.mu[rr][bc], 0.0, 0.0);
+      sm.pmask[rr][lane] = 0x33u;
+      if (lane == 0) {
+        atomicOr(&sm.liq, 1u << rr);
+        atomicOr(&sm.sol, 1u << rr);
+      }
+      continue;
+    }
+    const double2 pv2 = ld2(&sm.psi[rr][bc]), cv2 = ld2(&sm.c[rr][bc]);
+    const double pv[2] = {pv2.x, pv2.y}, cv[2] = {cv2.x, cv2.y};
+    const double dv[2] = {cv[0] - cinf, cv[1] - cinf};
+    double Sv[2], mv[2];
+    const unsigned long long b0 = bits(pv[0]), b1 = bits(pv[1]);
+    const bool liq2 = b0 == kMinus1 && b1 == kMinus1;
+    const bool sol2 = b0 == kPlus1 && b1 == kPlus1;
+    uint32_t code;
+    if (__all_sync(FULL, liq2 && fmax(dv[0], dv[1]) < d_hi && fmin(dv[0], dv[1]) > d_lo)) {
+      // bulk melt: g = -1, q = 1
+      code = 1u;
+      sm.pmask[rr][lane] = 0x03u;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const double c = cv[q], om = 1.0 - c;
+        const double s = dv[q] / fma(2.0 * cinf, om, dv[q]);
+        Sv[q] = c * om;
+        mv[q] = fma(RTa[q], lam_series(s), dv[q] * KL);
+      }
+    } else {
+      code = (__all_sync(FULL, liq2) ? 1u : 0u) | (__all_sync(FULL, sol2) ? 2u : 0u);
+      // deep solid row: no cell's mu'' enters a flux, so S = mu'' = 0 gives
+      // the same fluxes
+      const uint32_t s3 = (code & 2u) ? solid3(rr) : 0u;
+      if ((code & 2u) && __all_sync(FULL, s3 == 0x3u)) {
+        sm.pmask[rr][lane] = 0x30u;
+        Sv[0] = Sv[1] = mv[0] = mv[1] = 0.0;
+      } else {
+        double s[2];
+        bool small = true;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          s[q] = dv[q] / fma(2.0 * cinf, 1.0 - cv[q], dv[q]);
+          small = small && fabs(s[q]) < 1.0 / 9.0;
+        }
+        const bool series = __all_sync(FULL, small);
+        uint32_t L = 0u, Sm = 0u;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          if (pv[q] <= -1.0) L |= 1u << q;
+          if (pv[q] >= 1.0) Sm |= 1u << q;
+          cell_terms(F, pv[q], cv[q], s[q], series, RTa[q], C0a[q], Sv[q], mv[q]);
+        }
+        sm.pmask[rr][lane] = (uint8_t)(L | (Sm << 4));
+      }
+    }
+    st2(&sm.S[rr][bc], Sv[0], Sv[1]);
+    st2(&sm.mu[rr][bc], mv[0], mv[1]);
+    if (lane == 0) {
+      if (code & 1u) atomicOr(&sm.liq, 1u << rr);
+      if (code & 2u) atomicOr(&sm.sol, 1u << rr);
+    }
+  }
+  // halo columns x0-1 and x0+kW, one thread per cell, on warps 2 and 3, which
+  // have one input row fewer than warps 0 and 1
+  if (threadIdx.x >= 64 && threadIdx.x < 64 + 2 * kTRin) {
+    const int i = (int)threadIdx.x - 64;
+    const int rr = i >> 1, side = i & 1;
+    const int x = side ? kHaloR : kHaloL, g = x0 - 4 + x;
+    double Sh = 0.0, mh = 0.0;
+    uint8_t hm = 3u;
+    if (y0 - 1 + rr <= K.ny - 1) {
+      const double pv = sm.psi[rr][x], cv = sm.c[rr][x];
+      const double dv = cv - cinf;
+      const double s = dv / fma(2.0 * cinf, 1.0 - cv, dv);
+      cell_terms(F, pv, cv, s, fabs(s) < 1.0 / 9.0, tRT[g], tC0[g], Sh, mh);
+      hm = (pv <= -1.0 ? 1u : 0u) | (pv >= 1.0 ? 2u : 0u);
+    }
+    sm.S[rr][x] = Sh;
+    sm.mu[rr][x] = mh;
+    sm.hmask[rr][side] = hm;
+  }
+  const double dKa[3] = {tDK[gi - 1], tDK[gi], tDK[gi + 1]};  // faces x-1|x for x = col .. col+2
+  __syncthreads();
+  // phase 1 done: pull the tile of the CTA that will start about one resident
+  // wave later into L2, so its loads overlap the rest of this wave's arithmetic
+  if (threadIdx.x == 0 && wave > 0) {
+    const unsigned nxt = blockIdx.y * gridDim.x + blockIdx.x + (unsigned)wave;
+    if (nxt < gridDim.x * gridDim.y) {
+      const int pf_tr = (int)(nxt % gridDim.x);
+      const int pf_tc = front_first_block((int)(nxt / gridDim.x), f, (int)gridDim.y);
+      tma_prefetch_2d(&tm_psi, kW * pf_tc - 4, kTR * pf_tr);
+      tma_prefetch_2d(&tm_c, kW * pf_tc - 4, kTR * pf_tr);
+    }
+  }
+
+  // ---- phase 2: warp w computes output rows 1 + 4w .. 4 + 4w of the tile
+  const uint32_t liq = sm.liq, sol = sm.sol;
+  const bool red = part != nullptr;
+  double mass = 0.0;
+  int itip = 0;
+  struct Row {
+    double s[2], m[2], sl, sr, ml, mr;
+  };
+  // S pair sums of the faces left of cell f (f = 0..2) of a row
+  struct Pairs {
+    double q[3];
+  };
+  auto load_row = [&](int rr, Row &R) {
+    const double2 s = ld2(&sm.S[rr][bc]), m = ld2(&sm.mu[rr][bc]);
+    R.s[0] = s.x;
+    R.s[1] = s.y;
+    R.m[0] = m.x;
+    R.m[1] = m.y;
+    R.sl = sm.S[rr][bc - 1];  // lane 0: the halo column x0-1
+    R.ml = sm.mu[rr][bc - 1];
+    R.sr = sm.S[rr][bc + 2];  // lane 31: the halo column x0+kW
+    R.mr = sm.mu[rr][bc + 2];
+  };
+  auto pairs = [](const Row &R) {
+    Pairs P;
+    P.q[0] = R.sl + R.s[0];
+    P.q[1] = R.s[0] + R.s[1];
+    P.q[2] = R.s[1] + R.sr;
+    return P;
+  };
+  // fluxes through the faces between rows A and B = A+1 (compute_c_CALPHAD
+  // F01/F0m), rounded products so that a face rounds the same wherever the
+  // tiling puts it
+  auto vface = [&](const Row &A, const Row &B, double jv[2]) {
+    const double pp[4] = {A.sl + B.sl, A.s[0] + B.s[0], A.s[1] + B.s[1], A.sr + B.sr};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) jv[q] = __dmul_rn(fma(6.0, pp[q + 1], pp[q] + pp[q + 2]), B.m[q] - A.m[q]);
+  };
+
+  const int rbase = 1 + kRowsPerWarp * warp;
+  Row rb, rc;
+  Pairs pa, pb, pc;
+  double jv_lo[2], jv_hi[2];
+  double dn[kRowsPerWarp][2];
+  uint32_t needs_all = 0u;  // 2 bits per output row
+  {
+    Row ra;
+    load_row(rbase - 1, ra);
+    load_row(rbase, rb);
+    vface(ra, rb, jv_lo);
+    pa = pairs(ra);
+    pb = pairs(rb);
+  }
+#pragma unroll
+  for (int j = 0; j < kRowsPerWarp; ++j) {
+    const int rr = rbase + j;  // tile input row of the output row
+    load_row(rr + 1, rc);
+    pc = pairs(rc);
+    vface(rb, rc, jv_hi);
+    // fluxes through the faces (x-1/2, r) for x = col .. col+2
+    const double mm[4] = {rb.ml, rb.m[0], rb.m[1], rb.mr};
+    double jh[3];
+#pragma unroll
+    for (int fc = 0; fc < 3; ++fc)
+      jh[fc] = __dmul_rn(fma(6.0, pb.q[fc], pa.q[fc] + pc.q[fc]), mm[fc + 1] - mm[fc] + dKa[fc]);
+    const double2 cv2 = ld2(&sm.c[rr][bc]);
+    const double cv[2] = {cv2.x, cv2.y};
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+      dn[j][q] = fmax(fma(cflux4, (jh[q + 1] - jh[q]) + (jv_hi[q] - jv_lo[q]), cv[q]), F.c_floor);
+    const bool live = y0 - 1 + rr <= K.ny - 2;
+    if (red && live) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        if ((outm >> q) & 1u) mass += dn[j][q];
+    }
+    // phi: cells whose 3x3 neighbourhood is not uniformly +-1 are listed
+    const uint32_t w3 = 7u << (rr - 1);
+    if (live && (liq & w3) != w3 && (sol & w3) != w3) {
+      // per input row k: bits 0-1 psi <= -1, bits 4-5 psi >= 1 of the lane's cells
+      const uint32_t pk = (uint32_t)sm.pmask[rr - 1][lane] | ((uint32_t)sm.pmask[rr][lane] << 8) |
+                          ((uint32_t)sm.pmask[rr + 1][lane] << 16);
+      uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
+      // left neighbour's second cell: its bits 1 and 5; right neighbour's first: bits 0 and 4
+      uint32_t lL = 0u, lS = 0u, rL = 0u, rS = 0u;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lL |= ((lf >> (8 * k + 1)) & 1u) << k;
+        lS |= ((lf >> (8 * k + 5)) & 1u) << k;
+        rL |= ((rt >> (8 * k)) & 1u) << k;
+        rS |= ((rt >> (8 * k + 4)) & 1u) << k;
+      }
+      if (lane == 0) {
+        lL = lS = 0u;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t h = sm.hmask[rr - 1 + k][0];
+          lL |= (h & 1u) << k;
+          lS |= ((h >> 1) & 1u) << k;
+        }
+      }
+      if (lane == 31) {
+        rL = rS = 0u;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t h = sm.hmask[rr - 1 + k][1];
+          rL |= (h & 1u) << k;
+          rS |= ((h >> 1) & 1u) << k;
+        }
+      }
+      // over the three rows, bit b: box column bc-1+b is liquid / solid
+      uint32_t Lv = 0xFu, Sv = 0xFu;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t L = (pk >> (8 * k)) & 0x3u, S = (pk >> (8 * k + 4)) & 0x3u;
+        Lv &= ((lL >> k) & 1u) | (L << 1) | (((rL >> k) & 1u) << 3);
+        Sv &= ((lS >> k) & 1u) | (S << 1) | (((rS >> k) & 1u) << 3);
+      }
+      const uint32_t needs = ~((Lv & (Lv >> 1) & (Lv >> 2)) | (Sv & (Sv >> 1) & (Sv >> 2))) & outm;
+      const uint32_t cnt = __popc(needs);
+      uint32_t incl = cnt;  // inclusive warp scan of the counts
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t total = __shfl_sync(FULL, incl, 31);
+      int base = 0;
+      if (lane == 31 && total) base = atomicAdd(&sm.nlist, (int)total);
+      base = __shfl_sync(FULL, base, 31);
+      uint32_t off = (uint32_t)base + incl - cnt;
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        if ((needs >> q) & 1u) sm.list[off++] = (uint16_t)((rr << 8) | (col + q));
+      needs_all |= needs << (2 * j);
+    }
+    rb = rc;
+    pa = pb;
+    pb = pc;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) jv_lo[q] = jv_hi[q];
+  }
+  __syncthreads();
+
+  // ---- phase 3: interface cells, one per thread (compute_phi, fun.cu:1143-1218)
+  const int nlist = sm.nlist;
+  for (int idx = threadIdx.x; idx < nlist; idx += kThreads) {
+    const uint32_t e = sm.list[idx];
+    const int rr = (int)(e >> 8), x = (int)(e & 0xFFu) + 4;  // box column
+    const int r = y0 - 1 + rr, g = x0 + x - 4;
+    const double c00 = sm.c[rr][x];
+    const double dG = (1.0 - c00) * tAnb[g] + c00 * tAti[g] + c00 * (1.0 - c00) * (kL0Liq - kL0Bcc);
+    const double res = phi_cell_dG<double>(
+        &F, clamp1(sm.psi[rr][x]), clamp1(sm.psi[rr][x + 1]), clamp1(sm.psi[rr][x - 1]), clamp1(sm.psi[rr + 1][x]),
+        clamp1(sm.psi[rr - 1][x]), clamp1(sm.psi[rr + 1][x + 1]), clamp1(sm.psi[rr + 1][x - 1]),
+        clamp1(sm.psi[rr - 1][x + 1]), clamp1(sm.psi[rr - 1][x - 1]), dG, PS.step,
+        (int64_t)(r + K.j_offset) * K.nx + g, K.seed_lo, K.seed_hi);
+    sm.S[rr][x] = res;
+    if (red && res > 0.0) itip = max(itip, g == K.nx - 2 ? K.nx - 1 : g);
+  }
+  __syncthreads();
+
+  // ---- phase 4: new psi and c into the tile rows
+#pragma unroll
+  for (int j = 0; j < kRowsPerWarp; ++j) {
+    const int rr = rbase + j;
+    const double2 pv2 = ld2(&sm.psi[rr][bc]);
+    const double pv[2] = {pv2.x, pv2.y};
+    const bool live = y0 - 1 + rr <= K.ny - 2;
+    double po[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const bool listed = (needs_all >> (2 * j + q)) & 1u;
+      po[q] = listed ? sm.S[rr][bc + q] : clamp1(pv[q]);  // phi_next = phi where uniformly +-1
+      if (red && live && !listed && ((outm >> q) & 1u) && po[q] > 0.0)
+        itip = max(itip, gi + q == K.nx - 2 ? K.nx - 1 : gi + q);
+    }
+    st2(&sm.psi[rr][bc], po[0], po[1]);
+    st2(&sm.c[rr][bc], dn[j][0], dn[j][1]);
+  }
+  const int nrow = min(kTR, K.ny - 1 - y0);  // output rows of this tile inside the interior
+  const int ncol = min(kW, K.nx - x0);       // columns of this tile inside the array (even)
+  if (x0 == 0 || x0 + kW >= K.nx) {
+    // ghost columns 0 and nx-1 (compute_boundary_individual, fun.cu:1220-1230)
+    __syncthreads();
+    if (threadIdx.x < nrow) {
+      const int rr = 1 + threadIdx.x;
+      if (x0 == 0) {
+        sm.psi[rr][4] = sm.psi[rr][5];
+        sm.c[rr][4] = sm.c[rr][5];
+      }
+      if (x0 + kW >= K.nx) {
+        const int x = K.nx - 1 - x0 + 4;
+        sm.psi[rr][x] = sm.psi[rr][x - 1];
+        sm.c[rr][x] = sm.c[rr][x - 1];
+      }
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // tile writes -> bulk copies
+  __syncthreads();
+
+  // ---- bulk copies: thread (row j, field, kind): kind 0 the row itself,
+  // kind 1 its ghost copies (row jmin -> 0, row jmax -> ny-1)
+  if (threadIdx.x < 4 * kTR) {
+    const int j = threadIdx.x >> 2, field = threadIdx.x & 1, kind = (threadIdx.x >> 1) & 1;
+    const int r = y0 + j;
+    if (j < nrow) {
+      double *fo = field ? c_n : psi_n;
+      const double *src = field ? &sm.c[1 + j][4] : &sm.psi[1 + j][4];
+      const uint32_t bytes = (uint32_t)ncol * 8u;
+      bool any = false;
+      if (kind == 0) {
+        bulk_store(fo + (int64_t)r * K.pitch + x0, src, bytes);
+        any = true;
+      } else {
+        if (r == K.jmin) {
+          bulk_store(fo + x0, src, bytes);
+          any = true;
+        }
+        if (r == K.jmax) {
+          bulk_store(fo + (int64_t)(K.ny - 1) * K.pitch + x0, src, bytes);
+          any = true;
+        }
+      }
+      if (any) asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+  }
+  if (phi_n) {  // phi = clamp(psi) of the same rows, plain stores
+    for (int k = threadIdx.x; k < nrow * ncol; k += kThreads) {
+      const int j = k / ncol, x = k % ncol, r = y0 + j;
+      const double v = clamp1(sm.psi[1 + j][4 + x]);
+      phi_n[(int64_t)r * K.pitch + x0 + x] = v;
+      if (r == K.jmin) phi_n[x0 + x] = v;
+      if (r == K.jmax) phi_n[(int64_t)(K.ny - 1) * K.pitch + x0 + x] = v;
+    }
+  }
+  finish(mass, itip);
+  // shared memory stays allocated until the copies have read it
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+}  // namespace
+
+int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScalars &P, const TmaMaps &tm,
+                        double *psi_n, double *c_n, double *phi_n, BlockPartial *partials, int max_partials,
+                        int *nparts_out, int *err, cudaStream_t st) {
+  const int nj = K.ny - 2;
+  if (K.nx % 2 || K.pitch != K.nx) return -1;  // rows are copied in 16-byte units
+  // column-major: consecutive CTAs share a column strip and its halo rows in L2
+  const dim3 grid((nj + kTR - 1) / kTR, (K.nx + kW - 1) / kW), block(kThreads);
+  if (grid.y > 65535 || (int64_t)grid.x * grid.y > (1 << 30)) return -1;
+  const int nparts = grid.x * grid.y;
+  if (partials && nparts > max_partials) return -1;
+  if (!tm.col_tab64 || tm.col_tab64_len < (int)grid.y * kW + kWin) return -1;
+  const size_t smem = sizeof(TileSmem64);
+  static std::atomic<unsigned long long> attr_done{0};
+  if (!smem_limit_once((const void *)tile_kernel_f64, (int)smem, attr_done)) return -3;
+  static std::atomic<int> wave_of[64];
+  const int wave = resident_ctas((const void *)tile_kernel_f64, kThreads, smem, wave_of);
+  if (wave < 0) return -3;
+  column_table_kernel_f64<<<(tm.col_tab64_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(
+      K, P.d0, P.d1, tm.col_tab64_len, tm.col_tab64);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const double *tab = tm.col_tab64;
+  FinalRed fr = tm.red;
+  fr.partials = partials;
+  fr.nparts = nparts;
+  if (!partials || !(fr.mass_out || fr.itip_out)) fr.counter = nullptr;
+  if (cudaLaunchKernelEx(&cfg, tile_kernel_f64, K, F, P, tm.psi, tm.c, tab, tm.col_tab64_len, psi_n, c_n, phi_n,
+                         partials, err, fr, wave) != cudaSuccess)
+    return -3;
+  if (nparts_out) *nparts_out = nparts;
+  return 0;
+}
+
+}  // namespace rs

@@ -66,18 +66,29 @@ def plain_small(lib=None):
     return _ti10nb(default_params(lib), 256, 256, 1.0e6, 0.05)
 
 
-def scale_fp32(lib=None):
-    """2048x2048 FP32 bulk, G = 5e6 K/m, V = 0.5 m/s, interface noise 0.01, 20000 steps.
+def scale(lib=None):
+    """2048x2048, G = 5e6 K/m, V = 0.5 m/s, interface noise 0.01, 20000 steps;
+    the field precision is the caller's (FP32 bulk or the FP64 exact path).
 
     The front starts at the solidus isotherm: the c = 0.90 melt ahead of it is
     undercooled by T_liquidus - T_solidus = 6.84 K, so the front grows from
     the first step (about 1.3 m/s, relaxing to about 0.4 m/s after 10^4
     steps) and the moving frame shifts about every thousand steps.
+
+    Output cadence of the reference loop over this run: its 20000 steps are
+    total_time, with the reference's num_fields_output = 100 field snapshots
+    (old-fun.cu:41-43), so step_fields = 200.
     """
     p = _ti10nb(default_params(lib), 2048, 2048, 5.0e6, 0.5, T0=T_SOLIDUS_TI10NB)
     p.noise_amplitude = 0.01
     p.seed = 20240611
+    tau0 = (p.S * p.W0) ** 2 / (p.Gamma * p.muk0)
+    p.total_time_ns = (STEPS["scale_fp32"] + 0.5) * tau0 * p.dt
+    p.num_fields_output = p.num_tip_output = p.num_check_point_output = 100
     return p
+
+
+scale_fp32 = scale  # the FP32 bulk configuration of the same workload
 
 
 def small(n_i, n_j, lib=None, **kw):

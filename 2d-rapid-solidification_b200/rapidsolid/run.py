@@ -57,6 +57,55 @@ def main(argv=None):
     return 0
 
 
+def tip_run(p, dtype, nsteps, every=1000, surrogate=None, ic_seed=None):
+    """The reference loop (main.cu:156-240) on the workload p from its seeded
+    planar front: pull-back every step_pull_back steps, the precise tip every
+    `every` steps as set_tip_output does (fun.cu:3024-3050).  surrogate:
+    (weights, box) of a trained network, or None for the exact evaluation.
+    Returns (tip positions x = (i_offset_history + tip.x) dx in units of W,
+    tip velocity in m/s over the second half of the run, the surrogate's
+    audit (or None), solute mass at the start and at the end)."""
+    import ctypes as C
+
+    import torch
+    ctx = lib.Context(p)
+    d = ctx.d
+    if surrogate is not None:
+        ctx.set_surrogate(*surrogate)
+    a, b = lib.FieldSet(p, dtype), lib.FieldSet(p, dtype)
+    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ,
+                       configs.IC_SEED if ic_seed is None else ic_seed)
+    itip = torch.zeros(1, dtype=torch.int32, device="cuda")
+    tipbuf = torch.zeros(C.sizeof(_abi.Tip), dtype=torch.uint8, device="cuda")
+    mass = torch.zeros(2, dtype=torch.float64, device="cuda")
+    ctx.mass(a, mass[0:1])
+    hist, l, xs = 0, 0.0, []
+    for n in range(nsteps + 1):
+        if n % every == 0:
+            ctx.precise_tip(a, tipbuf)
+            t = lib.tip_from_bytes(tipbuf.cpu().numpy().tobytes())
+            xs.append((hist + t.x) * p.dx)
+            if n == nsteps:
+                break
+        pb = None
+        if n % d.step_pull_back == 0:
+            ctx.itip(a, itip)
+            pb = int(itip.item()) - p.i_tip_target
+            hist += pb
+        ctx.step(a, b, n, i_offset_history=hist, l_offset_Vp=l, pull_back=pb)
+        l += p.Vp * d.dt * d.tau0 / (p.S * p.W0)
+        a, b = b, a
+    ctx.mass(a, mass[1:2])
+    torch.cuda.synchronize()
+    ctx.device_status()
+    audit = ctx.surrogate_audit() if surrogate is not None else None
+    ctx.close()
+    half = len(xs) // 2
+    v = (xs[-1] - xs[half]) * p.S * p.W0 / ((nsteps - half * every) * d.tau0 * d.dt)
+    m0, m1 = mass.tolist()
+    return xs, v, audit, m0, m1
+
+
 def run3(a):
     """The 3D three-phase workload: rs3_initial, then a.steps rs3_step launches."""
     import torch

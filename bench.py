@@ -1,20 +1,26 @@
 """Throughput of the coupled phase-field step on B200.
 
-Workload (one step = one time step of the whole grid):
-  Ti-10at%Nb directional solidification, 2048 x 2048 cells (Nx_all x Ny_all,
-  2046^2 interior), FP32 fields (psi, c - cinf) double-buffered, exact CALPHAD
-  chemistry, frozen temperature G = 5e6 K/m, V = 0.5 m/s, moving frame on
-  (pull-back every step_pull_back = 1008 steps), seeded Philox interface
-  noise of amplitude 0.01.  Synthetic input: seeded planar front.
+Workload (one step = one time step of the whole grid): Ti-10at%Nb
+directional solidification, 2048 x 2048 cells (Nx_all x Ny_all, 2046^2
+interior), exact CALPHAD chemistry, frozen temperature G = 5e6 K/m,
+V = 0.5 m/s, moving frame on (pull-back every step_pull_back = 1008 steps),
+seeded Philox interface noise of amplitude 0.01.  Synthetic input: seeded
+planar front.  The headline line computes in FP64, the reference's
+arithmetic (its CPU arm, `--impl reference`, runs the same configuration);
+the FP32 bulk path, the surrogate, the ensemble, the 3D variant, the
+reference's own 256^2 workload and grids far beyond L2 are side legs.
 
 Metric: Gcell-steps/s = interior cells x steps / s (whole job over N GPUs).
 
-Device timing: CUDA events on the launching stream around each step; the
-64 MiB working set fits in L2, so a 256 MiB buffer is written between timed
-steps (outside the events) and every step reads its fields from HBM.
-e2e: the same steps through the C-ABI from pinned host buffers: H2D of the
-initial fields, every step's fused FP64 solute-mass reduction read back to
-the host, D2H of the final fields, all inside one event-timed region.
+Device timing: CUDA events on the launching stream around each step.  The
+step's input fields fit in the 126 MB L2, so L2 is flushed between timed
+steps (outside the events): a 256 MiB buffer is written, then another
+256 MiB buffer is read, so that the step reads its fields from HBM and does
+not pay the write-back of the flush's dirty lines.
+e2e: one output interval of the reference loop (step_fields = 200 steps,
+fun.cu:437-446) through the C-ABI from pinned host buffers: H2D of the
+fields (a restart), every step's fused FP64 solute-mass reduction read back
+to the host, D2H of the fields (the snapshot), all in one event-timed region.
 
 python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 Under torchrun each rank runs an independent replica (the path has no
@@ -34,6 +40,15 @@ sys.path.insert(0, os.path.join(ROOT, "2d-rapid-solidification_b200"))
 METRIC = "Gcell-steps/s, %HBM peak; surrogate vs exact CALPHAD at ≤0.5% tip-speed error"
 UNIT = "Gcell-steps/s"
 BYTES_PER_CELL = {"f32": 16, "f64": 32}  # psi, c read once + written once
+WORKLOAD = ("Ti-10Nb directional solidification 2048x2048, exact CALPHAD, frozen T G=5e6 K/m V=0.5 m/s, "
+            "moving frame, interface noise 0.01")
+# kernels a step launches: the FP32 tile path (column table + tile, mass
+# reduction fused), the FP64 tile path (the same), and the register-prefetch
+# kernel that pull-back steps take (plus one reduction launch for the mass)
+# (kernel of the roofline, launches of a step without pull-back, whether the
+# mass reduction is fused into that kernel)
+STEP_PATH = {"f32": ("rs::tile_kernel<false>", 2, True),
+             "f64": ("rs::tile_kernel_f64", 2, True)}
 
 
 def rank_info():
@@ -72,6 +87,12 @@ def profiled_traffic(kernel_tag):
             return json.load(f).get(kernel_tag)
     except Exception:
         return None
+
+
+def workload_config(p, d):
+    """The workload both arms run (identical keys and values)."""
+    return {"workload": WORKLOAD, "grid": [p.nx_all, p.ny_all], "interior_cells": (p.nx_all - 2) * (p.ny_all - 2),
+            "dx_W": p.dx, "dt_tau0": d.dt, "step_pull_back": d.step_pull_back}
 
 
 class ClockSampler:
@@ -120,9 +141,182 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class Flush:
+    """L2 flush between timed steps: write a 256 MiB buffer (larger than the
+    126 MB L2), then read another 256 MiB buffer, so L2 holds clean lines of
+    unrelated data when the next step starts."""
+
+    def __init__(self):
+        import torch
+        n = 256 * 1024 * 1024 // 4
+        self.w = torch.empty(n, dtype=torch.float32, device="cuda")
+        self.r = torch.ones(n, dtype=torch.float32, device="cuda")
+        self.acc = None
+
+    def __call__(self, k):
+        self.w.fill_(float(k))
+        self.acc = self.r.sum()
+
+
+class Loop:
+    """The reference main() loop body on one field set pair through the
+    library (main.cu:156-240): pull-back every step_pull_back steps (coarse
+    tip reduced on the device, 4-byte read), then the fused step; counts the
+    library's kernel launches."""
+
+    def __init__(self, p, dtype, ic_seed=None):
+        import torch
+        from rapidsolid import configs, lib
+        self.torch = torch
+        self.p, self.dtype = p, dtype
+        self.prec = "f64" if dtype == torch.float64 else "f32"
+        self.ctx = lib.Context(p)
+        self.d = self.ctx.d
+        self.a, self.b = lib.FieldSet(p, dtype), lib.FieldSet(p, dtype)
+        self.ctx.initial_planar(self.a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ,
+                                configs.IC_SEED if ic_seed is None else ic_seed)
+        self.itip = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.n, self.hist, self.l = 0, 0, 0.0
+        self.launches = 0
+
+    def step(self, mass_out=None):
+        p, d, n = self.p, self.d, self.n
+        pb = None
+        if n % d.step_pull_back == 0:
+            self.ctx.itip(self.a, self.itip)
+            self.launches += 2  # block partials + final reduction
+            pb = int(self.itip.item()) - p.i_tip_target
+            self.hist += pb
+        self.ctx.step(self.a, self.b, n, i_offset_history=self.hist, l_offset_Vp=self.l, pull_back=pb,
+                      mass_out=mass_out)
+        # a pull-back step is one register-kernel launch (+1 reduction for the
+        # mass); the others launch the column table and the tile kernel, which
+        # reduces the mass itself
+        red = 1 if mass_out is not None else 0
+        _, nl, fused = STEP_PATH[self.prec]
+        self.launches += (1 + red) if pb is not None else nl + (0 if fused else red)
+        self.l += p.Vp * d.dt * d.tau0 / (p.S * p.W0)
+        self.a, self.b = self.b, self.a
+        self.n = n + 1
+
+    def close(self):
+        self.ctx.close()
+
+
+def timed_steps(loop, steps, flush, st):
+    """CUDA-event time (ms) of each of `steps` steps, L2 flushed before each."""
+    torch = loop.torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    loop.launches = 0
+    for k in range(steps):
+        flush(k)
+        ev[k][0].record(st)
+        loop.step()
+        ev[k][1].record(st)
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in ev], loop.launches
+
+
+def e2e_interval(loop, nsteps, dist, world, st):
+    """One output interval of the reference loop through the C-ABI, from
+    pinned host fields: H2D of psi and c (a restart), nsteps steps each with
+    its FP64 solute mass read back on a copy stream, D2H of psi and c (the
+    field snapshot of set_fields_output, fun.cu:621-666)."""
+    torch = loop.torch
+    p = loop.p
+    h_psi = torch.empty((p.ny_all, p.nx_all), dtype=loop.dtype, pin_memory=True)
+    h_c = torch.empty_like(h_psi).pin_memory()
+    h_psi.copy_(loop.a.psi)
+    h_c.copy_(loop.a.c)
+    h_mass = torch.zeros(nsteps, dtype=torch.float64, pin_memory=True)
+    d_mass = torch.zeros(nsteps, dtype=torch.float64, device="cuda")
+    cs = torch.cuda.Stream()
+    done = [torch.cuda.Event() for _ in range(nsteps)]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    loop.a.psi.copy_(h_psi, non_blocking=True)
+    loop.a.c.copy_(h_c, non_blocking=True)
+    for k in range(nsteps):
+        loop.step(mass_out=d_mass[k:k + 1])
+        done[k].record(st)
+        cs.wait_event(done[k])
+        with torch.cuda.stream(cs):
+            h_mass[k:k + 1].copy_(d_mass[k:k + 1], non_blocking=True)
+    h_psi.copy_(loop.a.psi, non_blocking=True)
+    h_c.copy_(loop.a.c, non_blocking=True)
+    st.wait_stream(cs)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    cells = (p.nx_all - 2) * (p.ny_all - 2)
+    field_bytes = 2 * h_psi.numel() * h_psi.element_size()
+    return {"value": round(job_throughput(world, cells, nsteps, ms), 4), "unit": UNIT,
+            "h2d_bytes_per_step": round(field_bytes / nsteps, 1),
+            "d2h_bytes_per_step": round(8 + field_bytes / nsteps, 1), "ms_per_step": round(ms / nsteps, 5),
+            "interval_steps": nsteps,
+            "note": "C-ABI rs_step over one output interval of the reference loop (step_fields steps): H2D of "
+                    "psi and c from pinned memory, every step's FP64 mass read back on a copy stream, D2H of "
+                    "psi and c; no L2 flush"}
+
+
+def roofline(prec, cells, kern_ms, peak, peak_kind, kernel):
+    alg = BYTES_PER_CELL[prec] * cells
+    achieved = alg / (kern_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg,
+            "kernel": kernel, "kernel_ms_median": round(kern_ms, 5),
+            "traffic": profiled_traffic(f"step_{prec}_2048")}
+
+
+def run_arm(p, dtype, args, flush, st, dist, world, clocks=None):
+    """Warm-up, timed steps (L2 flushed), roofline and e2e of one precision."""
+    loop = Loop(p, dtype)
+    for _ in range(args.warmup):
+        loop.step()
+    loop.torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    loop.torch.cuda.synchronize()
+    if clocks is not None:
+        # clocks are sampled from before to after the timed region (200 ms
+        # period): untimed steps keep the GPU under load while it starts
+        clocks.start()
+        t_pre = time.time()
+        while time.time() - t_pre < args.clock_preroll:
+            for _ in range(20):
+                loop.step()
+            loop.torch.cuda.synchronize()
+    t_wall = time.time()
+    ms_steps, launches = timed_steps(loop, args.steps, flush, st)
+    t_wall = time.time() - t_wall
+    clk = None
+    if clocks is not None:
+        t_post = time.time()
+        while time.time() - t_post < 0.3:
+            for _ in range(20):
+                loop.step()
+            loop.torch.cuda.synchronize()
+        clk = clocks.stop()
+    total_ms = max_over_ranks(sum(ms_steps), dist, "cuda")
+    cells = (p.nx_all - 2) * (p.ny_all - 2)
+    srt = sorted(ms_steps)
+    kern_ms = srt[len(srt) // 2]
+    peak, peak_kind = measured_peak()
+    out = {"value": round(job_throughput(world, cells, args.steps, total_ms), 4),
+           "ms_per_step": round(total_ms / args.steps, 5),
+           "roofline": roofline(loop.prec, cells, kern_ms, peak, peak_kind, STEP_PATH[loop.prec][0]),
+           "gpu_launches": launches, "wall_s_timed": round(t_wall, 3), "clocks": clk}
+    out["e2e"] = e2e_interval(loop, loop.d.step_fields, dist, world, st)
+    loop.close()
+    return out
+
+
 def run_ours(args):
     import torch
-    from rapidsolid import configs, lib
+    from rapidsolid import configs
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
@@ -132,172 +326,38 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    p = configs.scale_fp32()
-    ctx = lib.Context(p)
-    d = ctx.d
-    dtype = torch.float32
-    a, b = lib.FieldSet(p, dtype), lib.FieldSet(p, dtype)
-    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    p = configs.scale()
+    from rapidsolid import lib
+    d = lib.derive(p)
     st = torch.cuda.current_stream()
-    cells = (p.nx_all - 2) * (p.ny_all - 2)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    itip = torch.zeros(1, dtype=torch.int32, device="cuda")
-
-    state = {"step": 0, "hist": 0, "l": 0.0, "a": a, "b": b}
-    launches = [0]
-
-    def vp_dl(n):
-        return p.Vp * d.dt * d.tau0 / (p.S * p.W0)
-
-    def one_step(mass_out=None):
-        """main.cu loop body: pull-back every step_pull_back steps (coarse tip
-        reduced on the device, 4-byte read), fused step."""
-        n = state["step"]
-        pb = None
-        if n % d.step_pull_back == 0:
-            ctx.itip(state["a"], itip)
-            launches[0] += 2
-            pb = int(itip.item()) - p.i_tip_target
-            state["hist"] += pb
-        ctx.step(state["a"], state["b"], n, i_offset_history=state["hist"], l_offset_Vp=state["l"],
-                 pull_back=pb, mass_out=mass_out)
-        # a pull-back step is one register-kernel launch (+1 for its mass
-        # reduction); the others launch the column-table kernel and the tile
-        # kernel, which reduces the mass itself
-        launches[0] += (1 if pb is not None else 2) + (1 if mass_out is not None and pb is not None else 0)
-        state["l"] += vp_dl(n)
-        state["a"], state["b"] = state["b"], state["a"]
-        state["step"] = n + 1
-
-    for _ in range(args.warmup):
-        one_step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    # clocks are sampled from before to after the timed region (200 ms period):
-    # untimed steps keep the GPU under load while the sampler starts
-    clocks = ClockSampler(local)
-    clocks.start()
-    t_pre = time.time()
-    while time.time() - t_pre < args.clock_preroll:
-        for _ in range(20):
-            one_step()
-        torch.cuda.synchronize()
-    launches[0] = 0
-    t_wall = time.time()
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        ev[k][0].record(st)
-        one_step()
-        ev[k][1].record(st)
-    torch.cuda.synchronize()
-    t_wall = time.time() - t_wall
-    gpu_launches = launches[0]
-    t_post = time.time()
-    while time.time() - t_post < 0.3:
-        for _ in range(20):
-            one_step()
-        torch.cuda.synchronize()
-    clk = clocks.stop()
-    ms_steps = [s.elapsed_time(e) for s, e in ev]
-    total_ms = max_over_ranks(sum(ms_steps), dist, "cuda")
-    ms_per_step = total_ms / args.steps
-    value = job_throughput(world, cells, args.steps, total_ms)
-
-    # roofline of the step kernel: median launch duration
-    srt = sorted(ms_steps)
-    kern_ms = srt[len(srt) // 2]
-    alg_bytes = BYTES_PER_CELL["f32"] * cells
-    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
-    peak, peak_kind = measured_peak()
-    # the same bytes moved by a plain device copy (half read, half written)
-    # under the same flush: the floor of one step of this size
-    src = torch.ones(alg_bytes // 8, dtype=torch.float32, device="cuda")
-    dst = torch.empty_like(src)
-    cts = []
-    for k in range(max(args.steps, 10)):
-        flush.fill_(float(k))
-        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        c0.record(st)
-        dst.copy_(src)
-        c1.record(st)
-        torch.cuda.synchronize()
-        cts.append(c0.elapsed_time(c1))
-    copy_ms = sorted(cts)[len(cts) // 2]
-    del src, dst
-
-    # ---- e2e through the C-ABI with host buffers
-    e2e_steps = args.steps
-    h_psi = torch.empty((p.ny_all, p.nx_all), dtype=dtype, pin_memory=True)
-    h_c = torch.empty_like(h_psi).pin_memory()
-    h_psi.copy_(state["a"].psi)
-    h_c.copy_(state["a"].c)
-    h_mass = torch.zeros(e2e_steps, dtype=torch.float64, pin_memory=True)
-    d_mass = torch.zeros(e2e_steps, dtype=torch.float64, device="cuda")
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # each step's solute mass is read back on a copy stream, so the read
-    # overlaps the next step instead of holding the compute stream
-    cs = torch.cuda.Stream()
-    done = [torch.cuda.Event() for _ in range(e2e_steps)]
-    e0.record(st)
-    state["a"].psi.copy_(h_psi, non_blocking=True)
-    state["a"].c.copy_(h_c, non_blocking=True)
-    for k in range(e2e_steps):
-        one_step(mass_out=d_mass[k:k + 1])
-        done[k].record(st)
-        cs.wait_event(done[k])
-        with torch.cuda.stream(cs):
-            h_mass[k:k + 1].copy_(d_mass[k:k + 1], non_blocking=True)
-    h_psi.copy_(state["a"].psi, non_blocking=True)
-    h_c.copy_(state["a"].c, non_blocking=True)
-    st.wait_stream(cs)
-    e1.record(st)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
-    field_bytes = 2 * h_psi.numel() * h_psi.element_size()
-    e2e = {"value": job_throughput(world, cells, e2e_steps, e2e_ms), "unit": UNIT,
-           "h2d_bytes_per_step": field_bytes / e2e_steps, "d2h_bytes_per_step": 8 + field_bytes / e2e_steps,
-           "ms_per_step": e2e_ms / e2e_steps,
-           "note": "C-ABI rs_step from pinned host fields; per-step FP64 mass read back on a copy stream; "
-                   "no L2 flush"}
+    flush = Flush()
+    head = run_arm(p, torch.float64, args, flush, st, dist, world, clocks=ClockSampler(local))
 
     line = {
-        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (FP64 column CALPHAD groups, FP64 mass sum)",
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
         "data": "synthetic (seeded planar Ti-10Nb front, Philox noise)",
-        "config": {"workload": "Ti-10Nb directional solidification 2048x2048 FP32 exact CALPHAD, frozen T "
-                               "G=5e6 K/m V=0.5 m/s, moving frame, interface noise 0.01",
-                   "grid": [p.nx_all, p.ny_all], "interior_cells": cells, "dx_W": p.dx, "dt_tau0": d.dt,
-                   "step_pull_back": d.step_pull_back, "l2": "flushed between timed steps (256 MiB write)",
-                   "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": alg_bytes, "kernel": "rs::tile_kernel",
-                     "kernel_ms_median": round(kern_ms, 5), "traffic": profiled_traffic("step_f32_2048"),
-                     "copy_floor": {"ms": round(copy_ms, 5),
-                                    "frac": round(alg_bytes / (copy_ms * 1e-3) / 1e9 / peak, 4),
-                                    "note": "device copy of the same bytes under the same L2 flush"}},
-        "e2e": e2e, "gpu_launches": gpu_launches, "clocks": clk, "wall_s_timed": round(t_wall, 3),
+        "config": workload_config(p, d), "parallelism": f"replicas x{world}",
+        "l2": "flushed between timed steps (256 MiB written, then 256 MiB read)",
+        "roofline": head["roofline"], "e2e": head["e2e"], "gpu_launches": head["gpu_launches"],
+        "clocks": head["clocks"], "wall_s_timed": head["wall_s_timed"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, seconds=args.cpu_seconds)
     if rank == 0 and world == 1 and not args.no_side_legs:
-        fp64 = fp64_leg(p, flush)
-        line["fp64_exact"] = fp64
-        line["fp32_exact_vs_fp64_exact"] = round(value / fp64["value"], 3)
-        line["surrogate"] = surrogate_leg(p, flush, value, fp64["value"])
+        fp32 = run_arm(p, torch.float32, args, flush, st, None, 1)
+        fp32.pop("clocks")
+        line["fp32_exact"] = fp32
+        line["fp32_exact_vs_fp64_exact"] = round(fp32["value"] / head["value"], 3)
+        line["c1_plain_small"] = c1_leg()
+        line["surrogate"] = surrogate_leg(p, flush, fp32["value"], head["value"])
         line["ensemble"] = ensemble_leg(flush)
         del flush
         torch.cuda.empty_cache()
-        line["peritectic_3d"] = peritectic_3d_leg(peak)
-    ctx.close()
+        line["beyond_l2"] = beyond_l2_leg()
+        torch.cuda.empty_cache()
+        line["peritectic_3d"] = peritectic_3d_leg(measured_peak()[0])
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -305,12 +365,102 @@ def run_ours(args):
         print(json.dumps(line))
 
 
+def c1_leg(nsteps=500):
+    """The reference's own workload: 256^2 FP64, frozen T
+    G = 1e6 K/m, V = 0.05 m/s, 500 steps with the pull-back of step 0
+    (main.cu's cadence), timed as one run launch by launch, and with steps
+    1..499 replayed from a CUDA graph captured once (the step arguments of a
+    frozen-temperature run are known in advance; step_pull_back = 10082)."""
+    import torch
+    from rapidsolid import configs
+    p = configs.plain_small()
+    cells = (p.nx_all - 2) * (p.ny_all - 2)
+    warm = Loop(p, torch.float64)
+    for _ in range(3):  # first launches of each kernel, not timed
+        warm.step()
+    torch.cuda.synchronize()
+    warm.close()
+    out = {}
+    # launch by launch: the whole run
+    loop = Loop(p, torch.float64)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(nsteps):
+        loop.step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["eager"] = {"value": round(cells * nsteps / (ms * 1e-3) / 1e9, 3), "ms_run": round(ms, 4),
+                    "us_per_step": round(ms * 1e3 / nsteps, 3)}
+    loop.close()
+    # step 0 (pull-back, coarse tip read back) eagerly, then steps 1..499 as
+    # one graph; the capture does not execute, so the replay starts from the
+    # state after step 0
+    loop = Loop(p, torch.float64)
+    loop.step()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    cs = torch.cuda.Stream()
+    cs.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(cs):
+        with torch.cuda.graph(g, stream=cs):
+            for _ in range(nsteps - 1):
+                loop.step()
+    torch.cuda.synchronize()
+    e0.record()
+    g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["graph"] = {"value": round(cells * (nsteps - 1) / (ms * 1e-3) / 1e9, 3), "ms_steps_1_499": round(ms, 4),
+                    "us_per_step": round(ms * 1e3 / (nsteps - 1), 3)}
+    del g
+    loop.close()
+    out["note"] = ("256x256 FP64, 500 steps; the reference arm (bench.py --impl reference) times the reference's "
+                   "own kernels on this run (reference_kernels_b200.fp64_2d_256_c1)")
+    return out
+
+
+def beyond_l2_leg(n=8192, steps=10):
+    """The C2 step on an 8192 x 8192 grid (FP32: 512 MiB per field set,
+    FP64: 1 GiB), far beyond the 126 MB L2: no flush is needed and the
+    sustained HBM fraction is read directly from back-to-back steps."""
+    import torch
+    from rapidsolid import configs
+    p = configs.scale()
+    p.nx_all = p.ny_all = n
+    cells = (n - 2) * (n - 2)
+    peak, peak_kind = measured_peak()
+    out = {}
+    for prec, dtype in (("f32", torch.float32), ("f64", torch.float64)):
+        loop = Loop(p, dtype)
+        for _ in range(3):
+            loop.step()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for k in range(steps):
+            ev[k][0].record()
+            loop.step()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        ts = sorted(s.elapsed_time(e) for s, e in ev)
+        ms = ts[len(ts) // 2]
+        rl = roofline(prec, cells, ms, peak, peak_kind, STEP_PATH[prec][0])
+        rl.pop("traffic")
+        out[prec] = {"value": round(cells / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms, 5), "roofline": rl}
+        loop.close()
+        torch.cuda.empty_cache()
+    out["grid"] = [n, n]
+    return out
+
+
 def _timed_steps(ctx, p, d, a, b, flush, n0, nsteps):
     """Median CUDA-event time (ms) of nsteps steps, L2 flushed between them."""
     import torch
     ts = []
     for k in range(nsteps):
-        flush.fill_(float(k))
+        flush(k)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         ctx.step(a, b, n0 + k)
@@ -322,76 +472,22 @@ def _timed_steps(ctx, p, d, a, b, flush, n0, nsteps):
     return ts[len(ts) // 2]
 
 
-def fp64_leg(p, flush, nsteps=30):
-    """The exact FP64 step (the drop-in's precision) on the same workload."""
-    import torch
-    from rapidsolid import configs, lib
-    ctx = lib.Context(p)
-    a, b = lib.FieldSet(p, torch.float64), lib.FieldSet(p, torch.float64)
-    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
-    for k in range(1, 6):
-        ctx.step(a, b, k)
-        a, b = b, a
-    ms = _timed_steps(ctx, p, ctx.d, a, b, flush, 6, nsteps)
-    cells = (p.nx_all - 2) * (p.ny_all - 2)
-    ctx.close()
-    return {"value": round(cells / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms, 5), "steps": nsteps,
-            "kernel": "rs::step_kernel<double, H, 3, false> (register prefetch)",
-            "note": "median of CUDA-event step times, L2 flushed"}
-
-
-def _tip_run(p, use_w, box, nsteps=20000, every=1000):
-    """The C2 loop (moving frame, tip every `every` steps): tip positions."""
-    import ctypes as C
-    import torch
-    from rapidsolid import _abi, configs, lib
-    ctx = lib.Context(p)
-    d = ctx.d
-    if use_w is not None:
-        ctx.set_surrogate(use_w, box)
-    a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
-    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
-    itip = torch.zeros(1, dtype=torch.int32, device="cuda")
-    tipbuf = torch.zeros(C.sizeof(_abi.Tip), dtype=torch.uint8, device="cuda")
-    hist, l, xs = 0, 0.0, []
-    for n in range(nsteps + 1):
-        if n % every == 0:
-            ctx.precise_tip(a, tipbuf)
-            t = lib.tip_from_bytes(tipbuf.cpu().numpy().tobytes())
-            xs.append((hist + t.x) * p.dx)
-            if n == nsteps:
-                break
-        pb = None
-        if n % d.step_pull_back == 0:
-            ctx.itip(a, itip)
-            pb = int(itip.item()) - p.i_tip_target
-            hist += pb
-        ctx.step(a, b, n, i_offset_history=hist, l_offset_Vp=l, pull_back=pb)
-        l += p.Vp * d.dt * d.tau0 / (p.S * p.W0)
-        a, b = b, a
-    torch.cuda.synchronize()
-    audit = ctx.surrogate_audit() if use_w is not None else None
-    ctx.close()
-    half = len(xs) // 2
-    v = (xs[-1] - xs[half]) * p.S * p.W0 / ((nsteps - half * every) * d.tau0 * d.dt)
-    return xs, v, audit
-
-
-def surrogate_leg(p, flush, fp32_value, fp64_value, nsteps=30):
+def surrogate_leg(p, flush, fp32_value, fp64_value, nsteps=30, seeds=(1, 2, 3)):
     """The FP32 step with the learned CALPHAD surrogate (trained here on the
-    GPU by the library's kernels): speed, and tip speed against the exact FP32
-    step over the full 20000-step run, for the box fitted to the run and for
-    the wide training box of the workload definition."""
+    GPU by the library's kernels, deterministically for a seed): speed with
+    the network of the workload definition's wide box, and tip speed and
+    position against the exact FP32 step over the full 20000-step run, for
+    three training seeds of the wide box and for the box fitted to the run."""
     import torch
-    from rapidsolid import configs, lib, surrogate
-    boxes = {"fitted": surrogate.fitted_box(), "wide": surrogate.default_box()}
+    from rapidsolid import configs, lib, run, surrogate
     trained = {}
-    for name, bx in boxes.items():
+    for name, bx, seed in [("wide", surrogate.default_box, sd) for sd in seeds] + \
+                          [("fitted", surrogate.fitted_box, seeds[0])]:
         t0 = time.time()
-        w, box, hist = surrogate.train(p, box=bx, epochs=40)
+        w, box, hist = surrogate.train(p, box=bx(), epochs=40, seed=seed)
         torch.cuda.synchronize()
-        trained[name] = (w, box, hist, time.time() - t0)
-    w, box = trained["fitted"][:2]
+        trained[(name, seed)] = (w, box, hist, time.time() - t0)
+    w, box = trained[("wide", seeds[0])][:2]
     ctx = lib.Context(p)
     ctx.set_surrogate(w, box)
     a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
@@ -403,22 +499,25 @@ def surrogate_leg(p, flush, fp32_value, fp64_value, nsteps=30):
     ctx.close()
     cells = (p.nx_all - 2) * (p.ny_all - 2)
     value = cells / (ms * 1e-3) / 1e9
-    x0, v0, _ = _tip_run(p, None, None)
+    x0, v0, _, _, _ = run.tip_run(p, torch.float32, configs.STEPS["scale_fp32"])
     accuracy = {}
-    for name, (w, box, hist, t_train) in trained.items():
-        x1, v1, audit = _tip_run(p, w, box)
-        accuracy[name] = {
-            "tip_speed_error": round(abs(v1 - v0) / v0, 5), "tip_speed_m_s": [round(v0, 6), round(v1, 6)],
+    for (name, seed), (w, box, hist, t_train) in trained.items():
+        x1, v1, audit, m0, m1 = run.tip_run(p, torch.float32, configs.STEPS["scale_fp32"], surrogate=(w, box))
+        accuracy[f"{name}_seed{seed}"] = {
+            "tip_speed_error": round(abs(v1 - v0) / v0, 6), "tip_speed_m_s": [round(v0, 6), round(v1, 6)],
             "tip_position_max_dx": round(max(abs(u - q) for u, q in zip(x0, x1)) / p.dx, 4),
+            "solute_drift_rel": (m1 - m0) / m0,
             "box": {"T": [round(box.T_lo, 3), round(box.T_hi, 3)], "c": [box.c_lo, box.c_hi]},
             "train_s": round(t_train, 2), "train_scaled_mse": hist[-1],
             "audit": {"max_err_mu_J_mol": audit[0], "max_err_dG_J_mol": audit[1], "fallback_cells": audit[2],
                       "audited_cells": audit[3]}}
+    wide = [v["tip_speed_error"] for k, v in accuracy.items() if k.startswith("wide")]
     return {"value": round(value, 3), "ms_per_step": round(ms, 5), "vs_fp32_exact": round(value / fp32_value, 3),
-            "vs_fp64_exact": round(value / fp64_value, 3), "box_of_speed": "fitted", "accuracy": accuracy,
+            "vs_fp64_exact": round(value / fp64_value, 3), "box_of_speed": "wide", "accuracy": accuracy,
+            "wide_tip_speed_error_spread": [min(wide), max(wide)],
             "note": "3->32->32->2 SiLU, FP16 mma.sync hidden layers; the network evaluates every cell that is "
                     "not bulk melt (the melt keeps its exact series form); exact fallback out of box and "
-                    "1/1024 audit"}
+                    "1/1024 audit; 20000 steps, tip every 1000"}
 
 
 def peritectic_3d_leg(peak, nsteps_run=5000, ntimed=10):
@@ -527,7 +626,7 @@ def ensemble_leg(flush, nruns=64, nsteps=100):
     ens.steps(3)  # step 0 pulls every run back (eager), then graph replays
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    flush.fill_(1.0)
+    flush(1)
     e0.record()
     ens.steps(nsteps)
     e1.record()
@@ -590,18 +689,20 @@ def _cpu_model():
 def run_reference(args):
     """The reference path has no CPU implementation of its own (its step is
     CUDA); its CPU form is the FP64 restatement in oracle/ (OpenMP, all host
-    threads), timed on a bounded sample: each step is one full-grid step."""
+    threads), timed on the same workload as the headline arm with the same
+    warm-up and step count (each step one full-grid step, capped so that the
+    run stays within minutes)."""
     rank, world, _ = rank_info()
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from rapidsolid import configs
-    p = configs.scale_fp32()
+    p = configs.scale()
     d = pyoracle.derive(p)
     s = pyoracle.initial_planar(p, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
-    steps = max(1, min(args.steps, 20))
-    warm = max(0, min(args.warmup, 1))
+    steps = max(1, min(args.steps, REF_MAX_STEPS))
+    warm = max(0, min(args.warmup, REF_MAX_STEPS))
     if warm:
         s = pyoracle.run(p, d, s, warm)
     t0 = time.time()
@@ -610,12 +711,11 @@ def run_reference(args):
     cells = (p.nx_all - 2) * (p.ny_all - 2)
     value = cells * steps / dt / 1e9
     cores = pyoracle.lib().ro_num_threads()
-    sample = f"{steps} FP64 steps of the {p.nx_all}x{p.ny_all} grid after {warm} warm-up"
+    sample = f"{steps} FP64 steps of the {p.nx_all}x{p.ny_all} grid after {warm} warm-up steps"
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
             "steps": steps, "warmup": warm, "ms_per_step": round(dt * 1e3 / steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-            "config": {"workload": "Ti-10Nb directional solidification 2048x2048, exact CALPHAD, frozen T",
-                       "grid": [p.nx_all, p.ny_all]},
+            "config": workload_config(p, d),
             "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample, "cpu": _cpu_model()},
             "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -623,6 +723,9 @@ def run_reference(args):
     if gpu:
         line["reference_kernels_b200"] = gpu
     print(json.dumps(line))
+
+
+REF_MAX_STEPS = 400  # about 30 s of the 2048^2 FP64 step on 16 host threads
 
 
 def _reference_kernels_gpu(pyoracle):
@@ -640,6 +743,7 @@ def _reference_kernels_gpu(pyoracle):
         return None
     out = {}
     for key, args in (("fp64_2d_2048", ["ref_harness_2048", "bench", "100", "0.144"]),
+                      ("fp64_2d_256_c1", ["ref_harness_256", "bench", "500", "0.144"]),
                       ("fp64_3d_512x512x128", ["ref3_harness_512", "bench", "10"])):
         binary = pyoracle.ref_binary(args[0])
         if not os.path.exists(binary):

@@ -181,8 +181,13 @@ int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
 
 /* Options: RS_OPT_TMA (default 1) stages the step's field tiles into shared
  * memory with TMA copies; 0 selects the register-prefetch kernel (always used
- * for pull-back steps, the coarse temperature and unaligned fields). */
+ * for pull-back steps, the coarse temperature and unaligned fields).
+ * RS_OPT_WAIT_LIMIT (default 0: the kernels' own limit of 2^20 tries) bounds
+ * the tile kernels' wait for their TMA loads; a tile whose wait gives up is
+ * not computed or stored, and rs_device_status reports RS_E_STATE.  Tests set
+ * it to 1 to run that path. */
 #define RS_OPT_TMA 1
+#define RS_OPT_WAIT_LIMIT 2
 int rs_set_option(rs_ctx *ctx, int32_t option, int64_t value);
 
 /* Device-side waits are bounded: if one gave up since the last call, returns
@@ -222,8 +227,11 @@ int rs_precise_tip(rs_ctx *ctx, const rs_fields *f, rs_tip *d_tip, rs_stream_t s
  * per-row scratch is a static device array of RS_NOALLOC_TIP_MAX_ROWS rows
  * (320 KiB, held by every GPU that loads the library); larger ny_all is
  * rejected with RS_E_INVALID.  The first call on a device looks up the
- * array's device address and should come before any stream capture.  All
- * calls share the scratch: calls whose kernels overlap on the GPU race. */
+ * array's device address and should come before any stream capture; the
+ * address is kept for the life of the process, so a cudaDeviceReset of that
+ * device leaves it stale (do not call this entry point on a device after
+ * resetting it).  All calls share the scratch: calls whose kernels overlap
+ * on the GPU race. */
 #define RS_NOALLOC_TIP_MAX_ROWS 16384
 int rs_precise_tip_noalloc(const rs_params *p, const rs_fields *f, rs_tip *d_tip, rs_stream_t stream);
 

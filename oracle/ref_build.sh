@@ -16,46 +16,70 @@
 # shipped (old-fun.cu:2002 uses `step`/`h_para` out of scope in save_parameters;
 # old-fun.cu:2205 assigns to a constexpr in AutoBlockSize):
 #   drop the "current pulling velocity" fprintf; constexpr int best_metric -> int
+# A second copy keeps ifTFC 1 (the reference's production coarse-grid
+# temperature) with the other edits, for the TFC harnesses.
 # Everything else comes in through -D exactly as run.sh passes it.
+#
+# Usage: ref_build.sh <reference root>   (or REF_ROOT=<reference root>)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${REF_ROOT:-/root/reference}"
+REF="${1:-${REF_ROOT:-}}"
 OUT="$HERE/_ref"
+if [ -z "$REF" ]; then
+  echo "ref_build: give the reference root as the argument or in REF_ROOT" >&2
+  exit 2
+fi
 if [ ! -f "$REF/old-fun.cu" ]; then
   echo "ref_build: $REF/old-fun.cu not present; keeping prebuilt $OUT" >&2
   exit 0
 fi
 mkdir -p "$OUT/src"
+patch_ref() { # out tfc(0|1)
+  local out=$1 tfc=$2
+  local tfc_edit='s/^#define[[:space:]]*ifTFC[[:space:]]*1/#define ifTFC 0/'
+  [ "$tfc" = 1 ] && tfc_edit='s/^#define[[:space:]]*ifTFC[[:space:]]*1/#define ifTFC 1/'
+  sed -e "$tfc_edit" \
+      -e 's/^\([[:space:]]*\)#define dx 0\.[0-9]*/\1#define dx REF_DX/' \
+      -e 's/^#define[[:space:]]*i_tip_target[[:space:]]*(Nx-268)/#define i_tip_target REF_ITIP/' \
+      -e 's/^#define[[:space:]]*cinf[[:space:]]*(0\.632514105)/#define cinf REF_CINF/' \
+      -e '/current pulling velocity.*Vp_ramp(step/d' \
+      -e 's/constexpr int best_metric/int best_metric/' \
+      "$REF/old-fun.cu" > "$out"
+  grep -q "^#define ifTFC $tfc" "$out"
+  grep -q '#define dx REF_DX' "$out"
+  grep -q '^#define i_tip_target REF_ITIP' "$out"
+  grep -q '^#define cinf REF_CINF' "$out"
+}
 PATCHED="$OUT/src/old-fun.fta.cu"
-sed -e 's/^#define[[:space:]]*ifTFC[[:space:]]*1/#define ifTFC 0/' \
-    -e 's/^\([[:space:]]*\)#define dx 0\.[0-9]*/\1#define dx REF_DX/' \
-    -e 's/^#define[[:space:]]*i_tip_target[[:space:]]*(Nx-268)/#define i_tip_target REF_ITIP/' \
-    -e 's/^#define[[:space:]]*cinf[[:space:]]*(0\.632514105)/#define cinf REF_CINF/' \
-    -e '/current pulling velocity.*Vp_ramp(step/d' \
-    -e 's/constexpr int best_metric/int best_metric/' \
-    "$REF/old-fun.cu" > "$PATCHED"
-grep -q '^#define ifTFC 0' "$PATCHED"
-grep -q '#define dx REF_DX' "$PATCHED"
-grep -q '^#define i_tip_target REF_ITIP' "$PATCHED"
-grep -q '^#define cinf REF_CINF' "$PATCHED"
+PATCHED_TFC="$OUT/src/old-fun.tfc.cu"
+patch_ref "$PATCHED" 0
+patch_ref "$PATCHED_TFC" 1
 
 NVCC="${NVCC:-nvcc}"
 COMMON=(-std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -ccbin g++
         -Xcompiler -ffp-contract=off -w
-        -DREF_PATCHED="\"$PATCHED\"" -DREF_DX=0.8 -DREF_CINF=0.90
+        -DREF_DX=0.8 -DREF_CINF=0.90
         -Dtotal_time=1000 -Dif_load=0 '-Dpath_input="./"' -Drun_time=1 -Drandom_seed=0
         -DVp=0.05 -DGG=0.001 -Deps1=0.06 -Deps2=0 -Depk1=0.15 -Dmain=ref_main)
 
-build() { # name nx ny itip extra...
+build() { # name nx ny itip extra...   (SRC_COPY: the patched copy, default the FTA one)
   local name=$1 nx=$2 ny=$3 itip=$4; shift 4
-  "$NVCC" "${COMMON[@]}" -DNx_all="$nx" -DNy_all="$ny" -DREF_ITIP="$itip" "$@" \
-      "$HERE/ref_harness.cu" -o "$OUT/$name"
+  "$NVCC" "${COMMON[@]}" -DREF_PATCHED="\"${SRC_COPY:-$PATCHED}\"" -DNx_all="$nx" -DNy_all="$ny" \
+      -DREF_ITIP="$itip" "$@" "$HERE/ref_harness.cu" -o "$OUT/$name"
 }
 build ref_harness_64 64 64 24
 build ref_harness_64_nofma 64 64 24 -fmad=false
 build ref_harness_256 256 256 16
 build ref_harness_256_nofma 256 256 16 -fmad=false
 build ref_harness_2048 2048 2048 16 -UGG -DGG=0.005 -UVp -DVp=0.5
+# coarse-grid temperature (TFC): G = 1e7 K/m, V = 0.5 m/s, the reference's own
+# TCOLD and 50 um coarse domain; Ny_all - 2 is a multiple of ratio_dxT_dx = 10
+# and Ny_all of BLOCK_SIZE_Y = 4, as the reference's TFC grids must be
+for tfc_grid in "64 72" "256 252"; do
+  set -- $tfc_grid
+  SRC_COPY="$PATCHED_TFC" build "ref_harness_tfc_$1x$2" "$1" "$2" 20 -UGG -DGG=0.01 -UVp -DVp=0.5
+  SRC_COPY="$PATCHED_TFC" build "ref_harness_tfc_$1x$2_nofma" "$1" "$2" 20 -UGG -DGG=0.01 -UVp -DVp=0.5 -fmad=false
+done
 # fun.cu as shipped (its own -D list, run.sh:75-90) for the parameter-file
 # layout: save_parameters / load_parameters only, host code.
 "$NVCC" -std=c++17 -O2 -gencode arch=compute_100a,code=sm_100a -ccbin g++ -w \

@@ -15,6 +15,9 @@
 //                                            GPU: pull_back, compute_phi,
 //                                            compute_psi, compute_c_CALPHAD
 //   ref_harness bench <nsteps> <dt>          GPU: times the three step kernels
+// Built from the coarse-temperature copy (ifTFC 1), the step modes give way to
+//   ref_harness_tfc tfc <in_dir> <out_dir> <nsteps> <dt> <delta_initial> <step_pull_back>
+//                                            GPU: the main() loop with TFC
 #include REF_PATCHED
 #undef main
 
@@ -93,6 +96,142 @@ int main(int argc, char **argv) {
     return 0;
   }
 
+#if (ifTFC)
+  // The coarse-temperature loop of the reference's main() (old-fun.cu:386-440
+  // with ifTFC 1): pull_back every step_pull_back steps with set_pull_back's
+  // i_offset / i_left_end bookkeeping (old-fun.cu:606-616), compute_phi,
+  // compute_psi, compute_c_CALPHAD on the interpolated T_fine, then
+  // integrate_phi, ratio_dt_dtT x compute_temperature and
+  // interpolate_temperature.  T starts from initial_temperature and
+  // interpolate_temperature as set_initial does (old-fun.cu:491-492).
+  //   ref_harness_tfc tfc <in_dir> <out_dir> <nsteps> <dt> <delta_initial> <step_pull_back>
+  // in_dir holds c/phi/psi.bin; out_dir receives c/phi/psi/T/T_fine.bin and
+  // the i_offset of every pull-back on stdout.
+  if (mode == "tfc") {
+    const std::string in_dir = argv[2], out_dir = argv[3];
+    const long nsteps = atol(argv[4]);
+    const double dt = atof(argv[5]);
+    const double delta_initial = atof(argv[6]);
+    const int step_pull_back = atoi(argv[7]);
+    std::vector<double> h_c = read_doubles(in_dir + "/c.bin", N);
+    std::vector<double> h_phi = read_doubles(in_dir + "/phi.bin", N);
+    std::vector<double> h_psi = read_doubles(in_dir + "/psi.bin", N);
+    constants h_para;
+    memset(&h_para, 0, sizeof(h_para));
+    set_parameters(&h_para);  // the reference's TFC geometry (NxT, NyT, Tcold, Thot, i_left_end_initial)
+    // the harness time step replaces set_parameters' 0.6 factor; the coarse
+    // sub-step count follows it by set_parameters' own rule
+    h_para.dt = dt;
+    {
+      constexpr real DDT = DT * tau0 / pow2(SS * W0 * ratio_dxT_dx);
+      constexpr real dtT = 0.9 * dx * dx / (4.0 * DDT);
+      h_para.ratio_dt_dtT = 1;
+      if (dtT < h_para.dt) h_para.ratio_dt_dtT = ceil(h_para.dt / dtT);
+      h_para.dtT = h_para.dt / h_para.ratio_dt_dtT;
+    }
+    h_para.delta_initial = delta_initial;
+    h_para.delta = delta_initial;
+    h_para.step_pull_back = step_pull_back;
+    printf("tfc NxT %d NyT %d NxT_all %d NyT_all %d ratio_dt_dtT %d i_left_end_initial %d\n", h_para.NxT,
+           h_para.NyT, h_para.NxT_all, h_para.NyT_all, h_para.ratio_dt_dtT, h_para.i_left_end_initial);
+    real h_orientation[num_axes * num_orientation];
+    set_orientation(h_orientation, alpha0, beta0, gamma0);
+    const size_t bytes = N * sizeof(real), bytesT = (size_t)h_para.NxT_all * h_para.NyT_all * sizeof(real);
+    real *d_c, *d_phi, *d_psi, *d_c_next, *d_phi_next, *d_psi_next, *d_orientation, *d_temp;
+    real *d_T, *d_T_next, *d_T_fine, *d_dphidt;
+    constants *d_para;
+    CK(cudaMalloc(&d_c, bytes));
+    CK(cudaMalloc(&d_phi, bytes));
+    CK(cudaMalloc(&d_psi, bytes));
+    CK(cudaMalloc(&d_c_next, bytes));
+    CK(cudaMalloc(&d_phi_next, bytes));
+    CK(cudaMalloc(&d_psi_next, bytes));
+    // compute_temperature reads its five-point stencil before testing the
+    // interior (old-fun.cu:1379-1398), so threads on the array's border read
+    // one row (NxT_all doubles) and one element outside it; each coarse
+    // array gets a zeroed guard of NxT_all + 1 doubles on both sides, which
+    // keeps those reads inside the allocation.  Their values only reach
+    // threads that write nothing from them.
+    const size_t guard = (size_t)h_para.NxT_all + 1;
+    real *g_T, *g_T_next, *g_dphidt;
+    CK(cudaMalloc(&g_T, bytesT + 2 * guard * sizeof(real)));
+    CK(cudaMalloc(&g_T_next, bytesT + 2 * guard * sizeof(real)));
+    CK(cudaMalloc(&g_dphidt, bytesT + 2 * guard * sizeof(real)));
+    CK(cudaMemset(g_T, 0, bytesT + 2 * guard * sizeof(real)));
+    CK(cudaMemset(g_T_next, 0, bytesT + 2 * guard * sizeof(real)));
+    CK(cudaMemset(g_dphidt, 0, bytesT + 2 * guard * sizeof(real)));
+    d_T = g_T + guard;
+    d_T_next = g_T_next + guard;
+    d_dphidt = g_dphidt + guard;
+    CK(cudaMalloc(&d_T_fine, bytes));
+    CK(cudaMalloc(&d_orientation, sizeof(h_orientation)));
+    CK(cudaMalloc(&d_para, sizeof(constants)));
+    CK(cudaMemset(d_c_next, 0, bytes));
+    CK(cudaMemset(d_phi_next, 0, bytes));
+    CK(cudaMemset(d_psi_next, 0, bytes));
+    CK(cudaMemcpy(d_para, &h_para, sizeof(constants), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_orientation, h_orientation, sizeof(h_orientation), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_c, h_c.data(), bytes, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_phi, h_phi.data(), bytes, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_psi, h_psi.data(), bytes, cudaMemcpyHostToDevice));
+    dim3 threadsPerBlock(BLOCK_SIZE_X, BLOCK_SIZE_Y);
+    dim3 numBlocks(Nx_all / threadsPerBlock.x, Ny_all / threadsPerBlock.y);
+    dim3 threadsPerBlockT(BLOCK_SIZE_T_X, BLOCK_SIZE_T_Y);
+    dim3 numBlocksT(h_para.NxT_all / threadsPerBlockT.x, h_para.NyT_all / threadsPerBlockT.y);
+    initial_temperature<<<numBlocksT, threadsPerBlockT>>>(d_T, d_para);
+    interpolate_temperature<<<numBlocks, threadsPerBlock>>>(d_T, d_T_fine, d_para, h_para.i_left_end, 0);
+    CK(cudaGetLastError());
+    for (long step = 0; step < nsteps; ++step) {
+      if (step % h_para.step_pull_back == 0) {
+        CK(cudaMemcpy(h_psi.data(), d_psi, bytes, cudaMemcpyDeviceToHost));
+        h_para.i_offset = get_itip_all_grain(h_psi.data()) - i_tip_target;
+        h_para.i_offset_history += h_para.i_offset;
+        h_para.i_left_end = h_para.i_left_end_initial + h_para.i_offset_history - int(h_para.l_offset_Vp / dx);
+        CK(cudaMemcpy(d_para, &h_para, sizeof(constants), cudaMemcpyHostToDevice));
+        printf("pull_back step %ld i_offset %d i_left_end %d\n", step, h_para.i_offset, h_para.i_left_end);
+        pull_back<<<numBlocks, threadsPerBlock>>>(d_c, d_phi, d_psi, d_c_next, d_phi_next, d_psi_next,
+                                                  h_para.i_offset, step);
+        d_temp = d_c; d_c = d_c_next; d_c_next = d_temp;
+        d_temp = d_phi; d_phi = d_phi_next; d_phi_next = d_temp;
+        d_temp = d_psi; d_psi = d_psi_next; d_psi_next = d_temp;
+      }
+      compute_phi<<<numBlocks, threadsPerBlock>>>(d_c, d_phi, d_psi, d_T_fine, d_c_next, d_phi_next, d_psi_next,
+                                                  d_orientation, NULL, d_para, step, h_para.i_offset_history,
+                                                  h_para.l_offset_Vp);
+      compute_psi<<<numBlocks, threadsPerBlock>>>(d_c, d_phi, d_psi, d_c_next, d_phi_next, d_psi_next,
+                                                  d_orientation, NULL, d_para, step);
+      compute_c_CALPHAD<<<numBlocks, threadsPerBlock>>>(d_c, d_phi, d_psi, d_T_fine, d_c_next, d_phi_next,
+                                                        d_psi_next, d_orientation, NULL, d_para, step,
+                                                        h_para.i_offset_history, h_para.l_offset_Vp);
+      integrate_phi<<<numBlocksT, threadsPerBlockT>>>(d_dphidt, d_psi, d_psi_next, d_para, h_para.i_left_end, step);
+      for (int sub_step = 0; sub_step < h_para.ratio_dt_dtT; sub_step++) {
+        compute_temperature<<<numBlocksT, threadsPerBlockT>>>(d_T, d_T_next, d_dphidt, d_para, step, sub_step);
+        d_temp = d_T; d_T = d_T_next; d_T_next = d_temp;
+      }
+      interpolate_temperature<<<numBlocks, threadsPerBlock>>>(d_T, d_T_fine, d_para, h_para.i_left_end, step);
+      d_temp = d_c; d_c = d_c_next; d_c_next = d_temp;
+      d_temp = d_phi; d_phi = d_phi_next; d_phi_next = d_temp;
+      d_temp = d_psi; d_psi = d_psi_next; d_psi_next = d_temp;
+      h_para.l_offset_Vp += Vp_ramp(step * tau0 * h_para.dt) * h_para.dt * tau0 / (SS * W0);
+      CK(cudaGetLastError());
+    }
+    CK(cudaDeviceSynchronize());
+    std::vector<double> h_T((size_t)h_para.NxT_all * h_para.NyT_all), h_Tf(N);
+    CK(cudaMemcpy(h_c.data(), d_c, bytes, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(h_phi.data(), d_phi, bytes, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(h_psi.data(), d_psi, bytes, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(h_T.data(), d_T, bytesT, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(h_Tf.data(), d_T_fine, bytes, cudaMemcpyDeviceToHost));
+    write_doubles(out_dir + "/c.bin", h_c.data(), N);
+    write_doubles(out_dir + "/phi.bin", h_phi.data(), N);
+    write_doubles(out_dir + "/psi.bin", h_psi.data(), N);
+    write_doubles(out_dir + "/T.bin", h_T.data(), h_T.size());
+    write_doubles(out_dir + "/T_fine.bin", h_Tf.data(), N);
+    printf("tfc done: %ld steps, i_offset_history %d, i_left_end %d, l_offset_Vp %.17g\n", nsteps,
+           h_para.i_offset_history, h_para.i_left_end, h_para.l_offset_Vp);
+    return 0;
+  }
+#else
   if (mode == "step" || mode == "bench") {
     const bool bench = mode == "bench";
     std::string in_dir, out_dir;
@@ -203,6 +342,7 @@ int main(int argc, char **argv) {
     }
     return 0;
   }
+#endif
   fprintf(stderr, "unknown mode %s\n", mode.c_str());
   return 1;
 }

@@ -15,6 +15,13 @@ parameter set), are run on seeded inputs and their raw FP64 outputs kept:
       OUT/step64.npz    64x64: pull_back(3) then 1 and 40 steps, plus the
                         nofma build (fun.cu kernels with -fmad=false)
       OUT/c1_500.npz    256x256 Ti-10Nb: pull_back(auto) then 500 steps
+  python tests/golden/make_golden.py gpu_tfc OUT  # reference TFC loop, needs a GPU
+      OUT/tfc_64x72.npz, OUT/tfc_256x252.npz   the reference's main() loop with
+                        its production coarse-grid temperature (ifTFC 1,
+                        fun.cu:431-514): pull-backs at a fixed cadence, the
+                        three step kernels on the interpolated T_fine,
+                        integrate_phi, ratio_dt_dtT x compute_temperature,
+                        interpolate_temperature (fun.cu:1494-1608)
 
 The inputs are built with the oracle's initial-condition routines (seeded), so
 the fixtures record inputs by seed, not by value.
@@ -30,7 +37,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "2d-rapid-solidification_b200"))
+sys.path.insert(0, os.path.dirname(HERE))
 import pyoracle  # noqa: E402
+from helpers import TFC_CASES, TFC_SEED, TFC_T_MARGIN, tfc_input, tfc_params  # noqa: E402
 from rapidsolid import configs  # noqa: E402
 
 
@@ -167,10 +176,54 @@ def make_gpu(out_dir):
     print("wrote", out_dir)
 
 
+def tfc_window(d, ile, nx):
+    """Coarse columns kept in a fixture: the phase-field window (integrate_phi's
+    iT1 .. iTn, fun.cu:1502-1503) with a margin, and both boundary strips."""
+    iT1, iTn = ile // 10, (ile + nx - 3) // 10
+    lo, hi = max(iT1 - TFC_T_MARGIN, 0), min(iTn + TFC_T_MARGIN + 1, d.NxT)
+    return list(range(0, 4)) + list(range(lo, hi)) + list(range(d.NxT - 4, d.NxT))
+
+
+def make_gpu_tfc(out_dir):
+    import re
+    os.makedirs(out_dir, exist_ok=True)
+    for name, (nx, ny, nsteps, spb) in TFC_CASES.items():
+        p = tfc_params(nx, ny, spb)
+        d = pyoracle.derive(p)
+        s = tfc_input(p)
+        res = {}
+        for tag, suffix in (("fma", ""), ("nofma", "_nofma")):
+            with tempfile.TemporaryDirectory() as td:
+                din, dout = os.path.join(td, "in"), os.path.join(td, "out")
+                write_state(din, s)
+                os.makedirs(dout, exist_ok=True)
+                r = subprocess.run([pyoracle.ref_binary(f"ref_harness_{name}{suffix}"), "tfc", din, dout,
+                                    str(nsteps), repr(d.dt), repr(p.delta_initial), str(spb)], check=True,
+                                   capture_output=True, text=True)
+                log = r.stdout
+                out = read_state(dout, s.c.shape)
+                T = np.fromfile(os.path.join(dout, "T.bin"), dtype=np.float64).reshape(d.NyT_all, d.NxT_all)
+                Tf = np.fromfile(os.path.join(dout, "T_fine.bin"), dtype=np.float64).reshape(s.c.shape)
+            geo = re.search(r"NxT (\d+) NyT (\d+) NxT_all (\d+) NyT_all (\d+) ratio_dt_dtT (\d+) "
+                            r"i_left_end_initial (-?\d+)", log).groups()
+            offsets = [int(v) for v in re.findall(r"i_offset (-?\d+) i_left_end", log)]
+            ile = int(re.findall(r"i_left_end (-?\d+)", log)[-1])
+            cols = tfc_window(d, ile, nx)
+            res.update({f"{tag}_c": out["c"], f"{tag}_psi": out["psi"], f"{tag}_T": T[:, cols],
+                        f"{tag}_T_fine": Tf, f"{tag}_offsets": np.array(offsets), f"{tag}_i_left_end": ile,
+                        f"{tag}_T_cols": np.array(cols), f"{tag}_geometry": np.array([int(v) for v in geo])})
+            print(name, tag, "offsets", offsets, "i_left_end", ile)
+        np.savez_compressed(os.path.join(out_dir, name + ".npz"), nsteps=nsteps, step_pull_back=spb,
+                            seed=TFC_SEED, dt=d.dt, **res)
+    print("wrote", out_dir)
+
+
 if __name__ == "__main__":
     if sys.argv[1] == "cpu":
         make_cpu()
     elif sys.argv[1] == "gpu":
         make_gpu(sys.argv[2])
+    elif sys.argv[1] == "gpu_tfc":
+        make_gpu_tfc(sys.argv[2])
     else:
-        raise SystemExit("usage: make_golden.py cpu | gpu OUT_DIR")
+        raise SystemExit("usage: make_golden.py cpu | gpu OUT_DIR | gpu_tfc OUT_DIR")

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import pyoracle
-from helpers import golden, maxabs, perturbed_state
+from helpers import TFC_CASES, golden, maxabs, perturbed_state, tfc_input, tfc_params, tfc_T_mask
 from rapidsolid import _abi, configs, lib
 from test_gpu_step import download, upload
 
@@ -294,3 +294,23 @@ def test_tfc_loop_fp32_against_fp64():
     assert maxabs(s32.psi, s64.psi) <= 2e-4 and maxabs(s32.c, s64.c) <= 2e-6
     assert abs(m32 - m64) <= 1e-8 * abs(m64), (m32, m64)
     assert maxabs(T32, T64) <= 1e-4
+
+
+@pytest.mark.parametrize("name", sorted(TFC_CASES))
+def test_tfc_loop_matches_reference_kernels(name):
+    """The FP64 coarse-temperature loop through the C-ABI against the
+    reference's own TFC kernels (fixture of its main() loop body with
+    ifTFC 1, pull-backs inside the run): psi and c within 1e-10, the coarse T
+    within 1e-10 K."""
+    z = golden(name + ".npz")
+    nx, ny, nsteps, spb = TFC_CASES[name]
+    p = tfc_params(nx, ny, spb)
+    d = pyoracle.derive(p)
+    g, T, _ = _gpu_tfc_loop(p, d, tfc_input(p), torch.float64, nsteps)
+    T = T.reshape(d.NyT_all, d.NxT_all)
+    for tag in ("fma", "nofma"):
+        assert maxabs(g.psi, z[f"{tag}_psi"]) <= 1e-10
+        assert maxabs(g.c, z[f"{tag}_c"]) <= 1e-10
+        cols = list(z[f"{tag}_T_cols"])
+        m = tfc_T_mask(d, cols)
+        assert maxabs(T[:d.NyT, cols][m], z[f"{tag}_T"][:d.NyT][m]) <= 1e-10

@@ -248,6 +248,29 @@ def test_f32_step_with_deep_solid_close_to_oracle(tma):
     assert np.array_equal(g.c[deep], s32.c[deep]) and np.array_equal(g.psi[deep], s32.psi[deep])
 
 
+@pytest.mark.parametrize("tma", [1, 0])
+def test_f64_step_with_deep_solid_matches_oracle(tma):
+    """The FP64 tile kernel's deep-solid rows (S = mu'' = 0, every face
+    weight there 0) and the interface rows around a liquid pocket: one step
+    against the oracle within 1e-13, the deep solid left exactly unchanged."""
+    p = configs.small(640, 70, i_tip_target=400, G=5e6, V=0.5)
+    d = pyoracle.derive(p)
+    s = solid_with_pocket(p, 5)
+    ctx = lib.Context(p)
+    ctx.set_option(_abi.RS_OPT_TMA, tma)
+    cur, nxt = upload(p, s), lib.FieldSet(p, torch.float64)
+    ctx.step(cur, nxt, 0)
+    o = pyoracle.step(p, d, s, 0)
+    g = download(p, nxt)
+    assert maxabs(g.psi, o.psi) <= 1e-13 and maxabs(g.c, o.c) <= 1e-13
+    deep = np.ones_like(s.psi, dtype=bool)
+    for dj in (-1, 0, 1):
+        for di in (-1, 0, 1):
+            deep &= np.roll(np.roll(s.psi == 1.0, dj, 0), di, 1)
+    deep[[0, -1], :] = deep[:, [0, -1]] = False
+    assert np.array_equal(g.c[deep], s.c[deep]) and np.array_equal(g.psi[deep], s.psi[deep])
+
+
 def test_tma_and_register_paths_agree():
     """Both kernels run the same per-cell arithmetic; they differ only where
     the compiler contracts a multiply-add differently."""

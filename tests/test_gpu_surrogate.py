@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import pymlp
-from rapidsolid import _abi, configs, lib, surrogate
+from rapidsolid import _abi, configs, lib, run, surrogate
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -65,6 +65,36 @@ def test_training_reduces_the_error():
     emax, erms = surrogate.errors(box, w, x, y)
     # six short epochs: well below the spread of the targets, not converged
     assert erms[0] < 0.5 * box.y_scale[0] and erms[1] < 0.5 * box.y_scale[1]
+
+
+def test_training_is_reproducible():
+    """Every random source of the training is seeded (Philox samples, Glorot
+    initial weights, the shuffle) and the gradient of a batch is summed in a
+    fixed order (one cluster, partial sums added in rank order), so two
+    trainings with one seed give the same weights bit for bit."""
+    p = configs.scale()
+    runs = [surrogate.train(p, n_samples=1 << 15, epochs=3, batch=2048, seed=11) for _ in range(2)]
+    assert torch.equal(runs[0][0], runs[1][0])
+    assert runs[0][2] == runs[1][2]
+    other = surrogate.train(p, n_samples=1 << 15, epochs=3, batch=2048, seed=12)
+    assert not torch.equal(runs[0][0], other[0])
+
+
+def test_surrogate_tip_speed_on_the_workload_box():
+    """The learned surrogate on the scale workload (2048^2 FP32, G = 5e6 K/m,
+    V = 0.5 m/s, noise 0.01, 20000 steps, moving frame), trained on the wide
+    box of the workload definition (T in [T_solidus - 200, T_liquidus + 50] K,
+    x_Nb <= 0.40): against the exact FP32 run, tip velocity over the second
+    half within 0.5 % and tip position within 0.25 dx at every sample (every
+    1000 steps); no cell falls outside the box."""
+    p = configs.scale()
+    w, box, _ = surrogate.train(p, box=surrogate.default_box(), epochs=40, seed=1)
+    n = configs.STEPS["scale_fp32"]
+    x0, v0, _, _, _ = run.tip_run(p, torch.float32, n)
+    x1, v1, audit, m0, m1 = run.tip_run(p, torch.float32, n, surrogate=(w, box))
+    assert abs(v1 - v0) <= 0.005 * abs(v0), (v0, v1)
+    assert max(abs(a - b) for a, b in zip(x0, x1)) <= 0.25 * p.dx, (x0, x1)
+    assert audit[2] == 0 and audit[3] > 0
 
 
 def test_surrogate_step_runs_with_audit():
