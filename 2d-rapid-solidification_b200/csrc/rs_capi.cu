@@ -75,6 +75,7 @@ struct rs_ctx {
   unsigned int *red_counter;  // fused final reduction of the FP32 tile kernel (device, 0 between launches)
   int use_tma;         // RS_OPT_TMA
   uint32_t wait_limit; // RS_OPT_WAIT_LIMIT (0: the kernels' default)
+  int pipeline;        // RS_OPT_PIPELINE
   TmaEntry tma[8];     // tensor-map cache keyed by field pointer
   int tma_n, tma_next;
 };
@@ -441,6 +442,7 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
     tm.col_tab64 = c->col_tab64;
     tm.col_tab64_len = c->col_tab64_len;
     tm.surr = c->surr.w && cur->precision == RS_F32 ? &c->surr : nullptr;
+    tm.pipeline = c->pipeline;
     tm.red = {};
     if (red) {  // both tile kernels reduce their partials themselves
       tm.red.counter = c->red_counter;
@@ -476,6 +478,9 @@ int rs_set_option(rs_ctx *c, int32_t option, int64_t value) {
   switch (option) {
     case RS_OPT_TMA:
       c->use_tma = value ? 1 : 0;
+      return RS_OK;
+    case RS_OPT_PIPELINE:
+      c->pipeline = value ? 1 : 0;
       return RS_OK;
     case RS_OPT_WAIT_LIMIT:
       if (value < 0 || value > (int64_t)1 << 30) return fail(RS_E_INVALID, "rs_set_option: wait limit %lld", (long long)value);
@@ -750,6 +755,7 @@ struct rs_ens {
   int32_t *d_tblk = nullptr, *d_order[3] = {nullptr, nullptr, nullptr};
   int ntblk = 0, ntiles = 0, choice = 0;
   bool ready = false;
+  bool surr = false;  // every run steps through its learned surrogate
   cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
   cudaStream_t cap = nullptr;
   int32_t *d_itip = nullptr, *h_itip = nullptr;
@@ -761,6 +767,16 @@ int ens_prepare(rs_ens *e) {
   if (e->ready) return RS_OK;
   for (int r = 0; r < e->n; ++r)
     if (!e->bound[r]) return fail(RS_E_STATE, "rs_ensemble: run %d has no field sets bound", r);
+  // the surrogate path: every run has its network set (rs_set_surrogate on
+  // its context), or none has
+  int nsurr = 0;
+  for (int r = 0; r < e->n; ++r) {
+    e->h_runs[r].surr = e->ctx[r]->surr;
+    nsurr += e->ctx[r]->surr.w != nullptr;
+  }
+  if (nsurr != 0 && nsurr != e->n)
+    return fail(RS_E_UNSUPPORTED, "rs_ensemble: %d of %d runs have a surrogate: all or none", nsurr, e->n);
+  e->surr = nsurr == e->n;
   std::vector<int32_t> tblk, ord[3];
   for (int r = 0; r < e->n; ++r) {
     const rs::EnsRun &R = e->h_runs[r];
@@ -801,8 +817,8 @@ int ens_graph(rs_ens *e, cudaGraphExec_t *out) {
   cudaGraph_t g = nullptr;
   cudaError_t c = cudaStreamBeginCapture(e->cap, cudaStreamCaptureModeThreadLocal);
   if (c == cudaSuccess) {
-    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles, true, e->ctx[0]->d_err,
-                        e->cap);
+    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles, true, e->surr,
+                        e->ctx[0]->d_err, e->cap);
     c = cudaStreamEndCapture(e->cap, &g);
   }
   if (c == cudaSuccess) c = cudaGraphInstantiate(&e->exec[e->choice], g, 0);
@@ -971,7 +987,7 @@ int rs_ensemble_steps(rs_ens *e, int64_t nsteps, rs_stream_t stream) {
     }
     if (cudaMemcpyAsync(e->d_runs, e->h_runs, sizeof(rs::EnsRun) * e->n, cudaMemcpyHostToDevice, st) != cudaSuccess)
       return fail(RS_E_CUDA, "rs_ensemble_steps: state upload failed");
-    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles, true,
+    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles, true, e->surr,
                         e->ctx[0]->d_err, st);
     if ((rc = cuda_check("rs_ensemble_steps"))) return rc;
     // the upload above reads h_runs: finish it before the mirror changes
@@ -1020,11 +1036,12 @@ int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choic
   int pick = 0;
   for (int k = 0; k < 3; ++k) {
     // without the advance kernel a launch recomputes the same step: the runs do not move
-    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->ctx[0]->d_err, st);
+    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->surr,
+                        e->ctx[0]->d_err, st);
     cudaEventRecord(t0, st);
     for (int q = 0; q < reps; ++q)
-      rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->ctx[0]->d_err,
-                          st);
+      rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->surr,
+                          e->ctx[0]->d_err, st);
     cudaEventRecord(t1, st);
     float ms = 0.f;
     if (cudaEventSynchronize(t1) != cudaSuccess || cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) {

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "rs_step_common.cuh"
+#include "rs_surrogate.cuh"
 
 namespace rs {
 
@@ -24,11 +25,13 @@ struct alignas(64) EnsRun {
   double l, inc_l;      // l_offset_Vp and its per-step increment
   // frozen temperature line (get_delta, fun.cu:1610-1619), evaluated as rs_step does
   double delta_initial, d1, GG, S, W0, deltaT0, l_init;
+  SurrArgs surr;  // the run's learned CALPHAD surrogate (surr.w == nullptr: exact)
 };
 
 // launches of rs_step_f32.cu for the ensemble: table blocks listed by
 // (run, block of that run), tiles in `order` as run << 16 | tile of that run
+// surr: every run evaluates its cells through its surrogate (all runs have one)
 int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
-                    bool advance, int *err, cudaStream_t st);
+                    bool advance, bool surr, int *err, cudaStream_t st);
 
 }  // namespace rs

@@ -858,9 +858,9 @@ __global__ void __launch_bounds__(kTabBlock) ens_table_kernel(const EnsRun *__re
   table_block(R.K, ens_d0(R), R.d1, R.tab_len, R.tab, e & 0xFFFF);
 }
 
-__global__ void __launch_bounds__(kThreads, 5) ens_tile_kernel(const EnsRun *__restrict__ runs,
-                                                              const int32_t *__restrict__ order, int *err,
-                                                              const int wave) {
+template <bool SURR>
+__global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
+    ens_tile_kernel(const EnsRun *__restrict__ runs, const int32_t *__restrict__ order, int *err, const int wave) {
   const int32_t e = order[blockIdx.x];
   const EnsRun &R = runs[e >> 16];
   if (!R.active) return;
@@ -883,8 +883,8 @@ __global__ void __launch_bounds__(kThreads, 5) ens_tile_kernel(const EnsRun *__r
     tma_prefetch_2d(&R2.map_psi[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
     tma_prefetch_2d(&R2.map_c[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
   };
-  tile_body<false>(R.K, R.F, PS, &R.map_psi[par], &R.map_c[par], R.tab, R.tab_len, R.psi[par ^ 1], R.c[par ^ 1],
-                   nullptr, nullptr, err, none, t % R.nrt, t / R.nrt, nullptr, prefetch);
+  tile_body<SURR>(R.K, R.F, PS, &R.map_psi[par], &R.map_c[par], R.tab, R.tab_len, R.psi[par ^ 1], R.c[par ^ 1],
+                  nullptr, nullptr, err, SURR ? R.surr : none, t % R.nrt, t / R.nrt, nullptr, prefetch);
 }
 
 __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
@@ -897,15 +897,16 @@ __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
 }  // namespace
 
 int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
-                    bool advance, int *err, cudaStream_t st) {
+                    bool advance, bool surr, int *err, cudaStream_t st) {
   const size_t smem = sizeof(TileSmem);
-  static std::atomic<unsigned long long> attr_done{0};
-  if (!smem_limit_once((const void *)ens_tile_kernel, (int)smem, attr_done)) return -3;
-  static std::atomic<int> wave_of[64];
-  const int wave = resident_ctas((const void *)ens_tile_kernel, kThreads, smem, wave_of);
+  auto kfn = surr ? ens_tile_kernel<true> : ens_tile_kernel<false>;
+  static std::atomic<unsigned long long> attr_done[2];
+  if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr])) return -3;
+  static std::atomic<int> wave_of[2][64];
+  const int wave = resident_ctas((const void *)kfn, kThreads, smem, wave_of[surr]);
   if (wave < 0) return -3;
   ens_table_kernel<<<ntblk, kTabBlock, 0, st>>>(runs, tblk);
-  ens_tile_kernel<<<ntiles, kThreads, smem, st>>>(runs, order, err, wave);
+  kfn<<<ntiles, kThreads, smem, st>>>(runs, order, err, wave);
   if (advance) ens_advance_kernel<<<(nruns + 63) / 64, 64, 0, st>>>(const_cast<EnsRun *>(runs), nruns);
   return 0;
 }

@@ -50,6 +50,18 @@
 // Launch order: the tile columns from the one holding the front
 // (front_first_block).  After phase 1 each CTA prefetches into L2 the input
 // tile of the block launched one resident wave later.
+//
+// Two kernels run these phases (same functions, same results bit for bit):
+//   * tile_kernel_f64: one tile per CTA of 128 threads, the phases in series
+//     separated by CTA barriers, five CTAs per SM;
+//   * pipe_kernel_f64: persistent CTAs of three warp roles that work on
+//     three tiles at once -- one producer warp issuing the TMA loads of tile
+//     k+2 into a three-slot input ring, four warps computing phase 1 of tile
+//     k+1 into a two-slot staging ring, four warps doing phases 2-4 of tile k
+//     and its bulk stores.  Hand-offs are mbarriers (full / empty per slot),
+//     each role synchronises its own warps by a named barrier, every wait is
+//     bounded (a wait that gives up sets the error flag and the CTA stops
+//     after draining its loads and stores).
 #include "rs_step_common.cuh"
 
 namespace rs {
@@ -59,13 +71,14 @@ constexpr int kW = kTileOutW64;   // output columns of a tile
 constexpr int kWin = kTmaBoxW64;  // input columns of a tile (kW + 8)
 constexpr int kTR = kTileRows;    // output rows of a tile
 constexpr int kTRin = kTmaBoxH;   // input rows of a tile
-constexpr int kThreads = 128;
+constexpr int kThreads = 128;     // threads of a phase group
 constexpr int kWarps = kThreads / 32;
 constexpr int kRowsPerWarp = kTR / kWarps;
 constexpr int kHaloL = 3, kHaloR = kW + 4;  // box columns of x0-1 and x0+kW
 constexpr uint32_t kWaitLimit = 1u << 20;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr unsigned long long kMinus1 = 0xBFF0000000000000ull, kPlus1 = 0x3FF0000000000000ull;
+constexpr uint32_t kTileBytes = 2u * kTRin * kWin * sizeof(double);
 static_assert(kW == 32 * 2, "two columns per lane");
 static_assert(kTR % kWarps == 0 && kRowsPerWarp == 4, "four output rows per warp");
 static_assert(kTRin <= 32, "row flags are 32-bit masks");
@@ -75,25 +88,43 @@ static_assert(64 + 2 * kTRin <= kThreads && 4 * kTR <= kThreads, "one thread per
 // describes column k - 4
 enum { kTabRT = 0, kTabC0 = 1, kTabDK = 2, kTabAnb = 3, kTabAti = 4 };
 
-struct alignas(128) TileSmem64 {
-  // TMA destinations (128-byte aligned); rows 1..16 receive the new psi / c
-  alignas(128) double psi[kTRin][kWin];
-  alignas(128) double c[kTRin][kWin];
-  alignas(16) double S[kTRin][kWin];  // after phase 2: new psi of the listed cells
-  alignas(16) double mu[kTRin][kWin];
-  uint16_t list[kTR * kW];   // interface cells: row << 8 | output column
+// the input tile: TMA destinations (128-byte aligned); after phase 3 rows
+// 1..16 receive the new psi / c for the bulk stores
+struct alignas(128) InSlot {
+  double psi[kTRin][kWin];
+  double c[kTRin][kWin];
+};
+// phase 1 -> phases 2-4: per-cell terms and row flags
+struct alignas(16) StSlot {
+  double S[kTRin][kWin];  // after phase 2: new psi of the listed cells
+  double mu[kTRin][kWin];
   uint8_t pmask[kTRin][32];  // per lane: bits 0-1 psi <= -1, bits 4-5 psi >= 1 of its two cells
   uint8_t hmask[kTRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
   uint32_t liq, sol;         // bit r: every cell of input row r has psi == -1 / +1
+};
+// phases 2-4: the interface list and the partial sums
+struct P2Smem {
+  uint16_t list[kTR * kW];  // interface cells: row << 8 | output column
   int nlist;
+  int last;  // this CTA finished last (fused final reduction)
   double part_mass[kWarps];
   int part_itip[kWarps];
-  uint64_t full;
-  int last;  // this CTA finished last (fused final reduction)
 };
-
-static_assert(offsetof(TileSmem64, psi) % 128 == 0 && offsetof(TileSmem64, c) % 128 == 0,
-              "TMA destinations start on 128-byte boundaries");
+struct alignas(128) TileSmem64 {
+  InSlot in;
+  StSlot st;
+  P2Smem p2;
+  uint64_t full;
+};
+constexpr int kRing = 3, kStage = 2;
+struct alignas(128) PipeSmem64 {
+  InSlot in[kRing];
+  StSlot st[kStage];
+  P2Smem p2;
+  uint64_t in_full[kRing], in_empty[kRing], st_full[kStage], st_empty[kStage];
+  int abort;  // a wait gave up: every role stops
+};
+static_assert(sizeof(InSlot) % 128 == 0, "ring slots stay 128-byte aligned");
 static_assert((kWin * sizeof(double)) % 16 == 0, "rows stay 16-byte aligned for double2 and bulk copies");
 
 __device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
@@ -102,6 +133,11 @@ __device__ __forceinline__ void st2(double *p, double a, double b) {
 }
 __device__ __forceinline__ double clamp1(double v) { return fmin(fmax(v, -1.0), 1.0); }
 __device__ __forceinline__ unsigned long long bits(double v) { return (unsigned long long)__double_as_longlong(v); }
+// barrier of one phase group of 128 threads (id 0 with 128-thread CTAs: the CTA)
+__device__ __forceinline__ void gsync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 
 // 2 atanh(s) by its odd series to s^15 (|s| < 1/9: truncation below
 // 3.3e-17 relative)
@@ -163,124 +199,67 @@ __global__ void __launch_bounds__(kTabBlock) column_table_kernel_f64(const StepC
   tab[kTabAti * len + k] = ct.A_ti;
 }
 
-__global__ void __launch_bounds__(kThreads, 5)
-    tile_kernel_f64(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<double> F,
-                    const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
-                    const __grid_constant__ CUtensorMap tm_c, const double *__restrict__ tab, const int tab_len,
-                    double *__restrict__ psi_n, double *__restrict__ c_n, double *__restrict__ phi_n,
-                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int wave) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  TileSmem64 &sm = *reinterpret_cast<TileSmem64 *>(smem_raw);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // blockIdx.x walks the tile rows of one tile column (they share halo rows
-  // in L2), blockIdx.y the tile columns, from the one holding column PS.i_front
-  const int f = max(PS.i_front, 0) / kW;
-  const int tr = blockIdx.x;
-  const int tc = front_first_block((int)blockIdx.y, f, (int)gridDim.y);
-  const int x0 = kW * tc;       // first output column of the tile
-  const int y0 = 1 + kTR * tr;  // first output row; input rows y0-1 .. y0+kTR
-  BlockPartial *part = partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr;
-  const FinalRed *FRp = partials && FR.counter ? &FR : nullptr;
-  constexpr uint32_t kTileBytes = 2u * kTRin * kWin * sizeof(double);
+// the column table, indexed by column
+struct Tab {
+  const double *RT, *C0, *DK, *Anb, *Ati;
+  __device__ Tab(const double *tab, int len)
+      : RT(tab + kTabRT * len + 4), C0(tab + kTabC0 * len + 4), DK(tab + kTabDK * len + 4),
+        Anb(tab + kTabAnb * len + 4), Ati(tab + kTabAti * len + 4) {}
+};
 
-  if (smem_u32(smem_raw) & 127u) {  // TMA destinations must be 128-byte aligned
-    if (threadIdx.x == 0) atomicExch(err, 2);
-    return;
-  }
-  if (threadIdx.x == 0) {
-    mbar_init(&sm.full, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    mbar_expect_tx(&sm.full, kTileBytes);
-    tma_load_2d(&sm.psi[0][0], &tm_psi, &sm.full, x0 - 4, y0 - 1);
-    tma_load_2d(&sm.c[0][0], &tm_c, &sm.full, x0 - 4, y0 - 1);
-    sm.liq = 0u;
-    sm.sol = 0u;
-    sm.nlist = 0;
-  }
-
-  const int col = 2 * lane;  // tile column of this lane's first cell
-  const int gi = x0 + col;   // its global column
-  const int bc = col + 4;    // its box column
-  uint32_t outm = 0;         // per cell: an interior (output) cell
+// Everything one phase group needs about a tile and its own lane.
+struct TileView {
+  const StepCoef &K;
+  const Coef<double> &F;
+  const StepScalars &PS;
+  Tab T;
+  int x0, y0;  // first output column, first output row (input rows y0-1 .. y0+kTR)
+  int gw, lane, gtid;  // warp and lane within the group, thread of the group
+  int col, gi, bc;     // the lane's first cell: tile column, global column, box column
+  uint32_t outm;       // per cell of the lane: an interior (output) cell
+  __device__ TileView(const StepCoef &K_, const Coef<double> &F_, const StepScalars &PS_, const double *tab,
+                      int tab_len, int x0_, int y0_, int gtid_)
+      : K(K_), F(F_), PS(PS_), T(tab, tab_len), x0(x0_), y0(y0_), gw(gtid_ >> 5), lane(gtid_ & 31), gtid(gtid_) {
+    col = 2 * lane;
+    gi = x0 + col;
+    bc = col + 4;
+    outm = 0;
 #pragma unroll
-  for (int q = 0; q < 2; ++q)
-    if (gi + q >= 1 && gi + q <= K.nx - 2) outm |= 1u << q;
+    for (int q = 0; q < 2; ++q)
+      if (gi + q >= 1 && gi + q <= K.nx - 2) outm |= 1u << q;
+  }
+};
+
+// columns beyond the array (right-most tiles; zero-filled by TMA) become
+// bulk melt, so they never force the general path; no output reads them.
+// Returns whether it wrote (the group then synchronises).
+__device__ __forceinline__ bool fix_beyond(const TileView &V, InSlot &in) {
+  if (V.x0 + kW + 4 <= V.K.nx) return false;
+  for (int k = V.gtid; k < kTRin * kWin; k += kThreads) {
+    const int rr = k / kWin, x = k % kWin;
+    if (V.x0 - 4 + x >= V.K.nx) {
+      in.psi[rr][x] = -1.0;
+      in.c[rr][x] = V.F.cinf;
+    }
+  }
+  return true;
+}
+
+// ---- phase 1: per-cell terms of the input rows of group warp gw (rows gw,
+// gw+4, ...) and of the halo columns (group threads 64..99); st.liq and
+// st.sol must be 0 on entry
+__device__ __forceinline__ void phase1(const TileView &V, const InSlot &in, StSlot &st) {
+  const Coef<double> &F = V.F;
+  const int lane = V.lane, bc = V.bc;
   const double cinf = F.cinf;
-  const double cflux4 = 0.25 * F.cflux;
   constexpr double KL = -2.0 * kL0Liq;
   // delta range of the bulk-melt form: s = delta / (A + B delta) with
   // A = 2 cinf (1 - cinf), B = 1 - 2 cinf, so |s| < 1/9 for
   // -A/(9+B) < delta < A/(9-B) (taken 0.1 % inside)
   const double sA = 2.0 * cinf * (1.0 - cinf), sB = 1.0 - 2.0 * cinf;
   const double d_hi = 0.999 * sA / (9.0 - sB), d_lo = -0.999 * sA / (9.0 + sB);
-
-  // the partial sums of this tile and the fused final reduction (the last
-  // CTA to finish sums every partial, in reduce_partials_kernel's order)
-  auto finish = [&](double mass, int itip) {
-    if (!part) return;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mass += __shfl_down_sync(FULL, mass, o);
-    itip = __reduce_max_sync(FULL, itip);
-    if (lane == 0) {
-      sm.part_mass[warp] = mass;
-      sm.part_itip[warp] = itip;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      BlockPartial b;
-      b.mass = 0.0;
-      b.itip = 0;
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) {
-        b.mass += sm.part_mass[w];
-        b.itip = max(b.itip, sm.part_itip[w]);
-      }
-      b.pad = 0;
-      *part = b;
-    }
-    if (!FRp) return;
-    if (threadIdx.x == 0) {
-      __threadfence();
-      sm.last = atomicAdd(FRp->counter, 1u) == (unsigned)(FRp->nparts - 1);
-    }
-    __syncthreads();
-    if (!sm.last) return;
-    __threadfence();
-    double *sm_m = &sm.S[0][0];  // S and mu are free now
-    int *sm_i = reinterpret_cast<int *>(&sm.mu[0][0]);
-    for (int v = threadIdx.x; v < 256; v += kThreads) {
-      double m = 0.0;
-      int it = 0;
-      for (int k = v; k < FRp->nparts; k += 256) {
-        m += __ldcg(&FRp->partials[k].mass);
-        it = max(it, __ldcg(&FRp->partials[k].itip));
-      }
-      sm_m[v] = m;
-      sm_i[v] = it;
-    }
-    __syncthreads();
-    for (int sz = 128; sz > 0; sz >>= 1) {
-      for (int v = threadIdx.x; v < sz; v += kThreads) {
-        sm_m[v] += sm_m[v + sz];
-        sm_i[v] = max(sm_i[v], sm_i[v + sz]);
-      }
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      if (FRp->mass_out) *FRp->mass_out = sm_m[0] + FRp->mass_offset;
-      if (FRp->itip_out) *FRp->itip_out = max(1, sm_i[0]);  // get_itip_all_grain starts at 1
-      *FRp->counter = 0u;
-    }
-  };
-
-  // the column table of this step (programmatic dependency on its kernel)
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  const double *tRT = tab + kTabRT * tab_len + 4, *tC0 = tab + kTabC0 * tab_len + 4;
-  const double *tDK = tab + kTabDK * tab_len + 4;
-  const double *tAnb = tab + kTabAnb * tab_len + 4, *tAti = tab + kTabAti * tab_len + 4;
-  const double2 RTv = ld2(tRT + gi), C0v = ld2(tC0 + gi);
+  const double2 RTv = ld2(V.T.RT + V.gi), C0v = ld2(V.T.C0 + V.gi);
   const double RTa[2] = {RTv.x, RTv.y}, C0a[2] = {C0v.x, C0v.y};
-
   // per lane, bit q: psi is exactly +1 over the 3x3 neighbourhood of cell
   // bc+q (rows of the box only; column -1 of the left-most tile enters no
   // face, column 0 being a ghost).  S = q(1) c (1 - c) = 0 there, so every
@@ -290,17 +269,464 @@ __global__ void __launch_bounds__(kThreads, 5)
     uint32_t v = 0x3u;
     bool hs = true;  // the halo column beside lanes 0 and 31
     for (int r2 = max(rr - 1, 0); r2 <= min(rr + 1, kTRin - 1); ++r2) {
-      const double2 q2 = ld2(&sm.psi[r2][bc]);
+      const double2 q2 = ld2(&in.psi[r2][bc]);
       v &= (bits(q2.x) == kPlus1 ? 1u : 0u) | (bits(q2.y) == kPlus1 ? 2u : 0u);
-      hs = hs && bits(sm.psi[r2][xh]) == kPlus1;
+      hs = hs && bits(in.psi[r2][xh]) == kPlus1;
     }
     uint32_t lf = __shfl_up_sync(FULL, v >> 1, 1) & 1u, rt = __shfl_down_sync(FULL, v, 1) & 1u;
-    if (lane == 0) lf = (hs || x0 == 0) ? 1u : 0u;
+    if (lane == 0) lf = (hs || V.x0 == 0) ? 1u : 0u;
     if (lane == 31) rt = hs ? 1u : 0u;
     const uint32_t e = lf | (v << 1) | (rt << 3);  // bit k: box column bc-1+k
     return e & (e >> 1) & (e >> 2) & 0x3u;
   };
+#pragma unroll 1
+  for (int rr = V.gw; rr < kTRin; rr += kWarps) {
+    if (V.y0 - 1 + rr > V.K.ny - 1) {  // beyond the array (last tile): never read by an output
+      st2(&st.S[rr][bc], 0.0, 0.0);
+      st2(&st.mu[rr][bc], 0.0, 0.0);
+      st.pmask[rr][lane] = 0x33u;
+      if (lane == 0) {
+        atomicOr(&st.liq, 1u << rr);
+        atomicOr(&st.sol, 1u << rr);
+      }
+      continue;
+    }
+    const double2 pv2 = ld2(&in.psi[rr][bc]), cv2 = ld2(&in.c[rr][bc]);
+    const double pv[2] = {pv2.x, pv2.y}, cv[2] = {cv2.x, cv2.y};
+    const double dv[2] = {cv[0] - cinf, cv[1] - cinf};
+    double Sv[2], mv[2];
+    const unsigned long long b0 = bits(pv[0]), b1 = bits(pv[1]);
+    const bool liq2 = b0 == kMinus1 && b1 == kMinus1;
+    const bool sol2 = b0 == kPlus1 && b1 == kPlus1;
+    uint32_t code;
+    if (__all_sync(FULL, liq2 && fmax(dv[0], dv[1]) < d_hi && fmin(dv[0], dv[1]) > d_lo)) {
+      // bulk melt: g = -1, q = 1
+      code = 1u;
+      st.pmask[rr][lane] = 0x03u;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const double c = cv[q], om = 1.0 - c;
+        const double sv = dv[q] / fma(2.0 * cinf, om, dv[q]);
+        Sv[q] = c * om;
+        mv[q] = fma(RTa[q], lam_series(sv), dv[q] * KL);
+      }
+    } else {
+      code = (__all_sync(FULL, liq2) ? 1u : 0u) | (__all_sync(FULL, sol2) ? 2u : 0u);
+      // deep solid row: no cell's mu'' enters a flux, so S = mu'' = 0 gives
+      // the same fluxes
+      const uint32_t s3 = (code & 2u) ? solid3(rr) : 0u;
+      if ((code & 2u) && __all_sync(FULL, s3 == 0x3u)) {
+        st.pmask[rr][lane] = 0x30u;
+        Sv[0] = Sv[1] = mv[0] = mv[1] = 0.0;
+      } else {
+        double sv[2];
+        bool small = true;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          sv[q] = dv[q] / fma(2.0 * cinf, 1.0 - cv[q], dv[q]);
+          small = small && fabs(sv[q]) < 1.0 / 9.0;
+        }
+        const bool series = __all_sync(FULL, small);
+        uint32_t L = 0u, Sm = 0u;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          if (pv[q] <= -1.0) L |= 1u << q;
+          if (pv[q] >= 1.0) Sm |= 1u << q;
+          cell_terms(F, pv[q], cv[q], sv[q], series, RTa[q], C0a[q], Sv[q], mv[q]);
+        }
+        st.pmask[rr][lane] = (uint8_t)(L | (Sm << 4));
+      }
+    }
+    st2(&st.S[rr][bc], Sv[0], Sv[1]);
+    st2(&st.mu[rr][bc], mv[0], mv[1]);
+    if (lane == 0) {
+      if (code & 1u) atomicOr(&st.liq, 1u << rr);
+      if (code & 2u) atomicOr(&st.sol, 1u << rr);
+    }
+  }
+  // halo columns x0-1 and x0+kW, one thread per cell, on group warps 2 and
+  // 3, which have one input row fewer than warps 0 and 1
+  if (V.gtid >= 64 && V.gtid < 64 + 2 * kTRin) {
+    const int i = V.gtid - 64;
+    const int rr = i >> 1, side = i & 1;
+    const int x = side ? kHaloR : kHaloL, g = V.x0 - 4 + x;
+    double Sh = 0.0, mh = 0.0;
+    uint8_t hm = 3u;
+    if (V.y0 - 1 + rr <= V.K.ny - 1) {
+      const double pv = in.psi[rr][x], cv = in.c[rr][x];
+      const double dv = cv - cinf;
+      const double sv = dv / fma(2.0 * cinf, 1.0 - cv, dv);
+      cell_terms(F, pv, cv, sv, fabs(sv) < 1.0 / 9.0, V.T.RT[g], V.T.C0[g], Sh, mh);
+      hm = (pv <= -1.0 ? 1u : 0u) | (pv >= 1.0 ? 2u : 0u);
+    }
+    st.S[rr][x] = Sh;
+    st.mu[rr][x] = mh;
+    st.hmask[rr][side] = hm;
+  }
+}
 
+// ---- phase 2: group warp gw computes output rows 1 + 4gw .. 4 + 4gw:
+// fluxes, the c update into dn, the interface cells into the list (nlist
+// must be 0 on entry).  Returns the listed cells, 2 bits per output row.
+__device__ __forceinline__ uint32_t phase2(const TileView &V, const InSlot &in, const StSlot &st, P2Smem &p2,
+                                           double dn[kRowsPerWarp][2], double &mass, bool red) {
+  const Coef<double> &F = V.F;
+  const int lane = V.lane, bc = V.bc;
+  const double cflux4 = 0.25 * F.cflux;
+  const uint32_t liq = st.liq, sol = st.sol;
+  const double dKa[3] = {V.T.DK[V.gi - 1], V.T.DK[V.gi], V.T.DK[V.gi + 1]};  // faces x-1|x for x = col .. col+2
+  struct Row {
+    double s[2], m[2], sl, sr, ml, mr;
+  };
+  // S pair sums of the faces left of cell f (f = 0..2) of a row
+  struct Pairs {
+    double q[3];
+  };
+  auto load_row = [&](int rr, Row &R) {
+    const double2 s = ld2(&st.S[rr][bc]), m = ld2(&st.mu[rr][bc]);
+    R.s[0] = s.x;
+    R.s[1] = s.y;
+    R.m[0] = m.x;
+    R.m[1] = m.y;
+    R.sl = st.S[rr][bc - 1];  // lane 0: the halo column x0-1
+    R.ml = st.mu[rr][bc - 1];
+    R.sr = st.S[rr][bc + 2];  // lane 31: the halo column x0+kW
+    R.mr = st.mu[rr][bc + 2];
+  };
+  auto pairs = [](const Row &R) {
+    Pairs P;
+    P.q[0] = R.sl + R.s[0];
+    P.q[1] = R.s[0] + R.s[1];
+    P.q[2] = R.s[1] + R.sr;
+    return P;
+  };
+  // fluxes through the faces between rows A and B = A+1 (compute_c_CALPHAD
+  // F01/F0m), rounded products so that a face rounds the same wherever the
+  // tiling puts it
+  auto vface = [&](const Row &A, const Row &B, double jv[2]) {
+    const double pp[4] = {A.sl + B.sl, A.s[0] + B.s[0], A.s[1] + B.s[1], A.sr + B.sr};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) jv[q] = __dmul_rn(fma(6.0, pp[q + 1], pp[q] + pp[q + 2]), B.m[q] - A.m[q]);
+  };
+
+  const int rbase = 1 + kRowsPerWarp * V.gw;
+  Row rb, rc;
+  Pairs pa, pb, pc;
+  double jv_lo[2], jv_hi[2];
+  uint32_t needs_all = 0u;
+  {
+    Row ra;
+    load_row(rbase - 1, ra);
+    load_row(rbase, rb);
+    vface(ra, rb, jv_lo);
+    pa = pairs(ra);
+    pb = pairs(rb);
+  }
+#pragma unroll
+  for (int j = 0; j < kRowsPerWarp; ++j) {
+    const int rr = rbase + j;  // tile input row of the output row
+    load_row(rr + 1, rc);
+    pc = pairs(rc);
+    vface(rb, rc, jv_hi);
+    // fluxes through the faces (x-1/2, r) for x = col .. col+2
+    const double mm[4] = {rb.ml, rb.m[0], rb.m[1], rb.mr};
+    double jh[3];
+#pragma unroll
+    for (int fc = 0; fc < 3; ++fc)
+      jh[fc] = __dmul_rn(fma(6.0, pb.q[fc], pa.q[fc] + pc.q[fc]), mm[fc + 1] - mm[fc] + dKa[fc]);
+    const double2 cv2 = ld2(&in.c[rr][bc]);
+    const double cv[2] = {cv2.x, cv2.y};
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+      dn[j][q] = fmax(fma(cflux4, (jh[q + 1] - jh[q]) + (jv_hi[q] - jv_lo[q]), cv[q]), F.c_floor);
+    const bool live = V.y0 - 1 + rr <= V.K.ny - 2;
+    if (red && live) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        if ((V.outm >> q) & 1u) mass += dn[j][q];
+    }
+    // phi: cells whose 3x3 neighbourhood is not uniformly +-1 are listed
+    const uint32_t w3 = 7u << (rr - 1);
+    if (live && (liq & w3) != w3 && (sol & w3) != w3) {
+      // per input row k: bits 0-1 psi <= -1, bits 4-5 psi >= 1 of the lane's cells
+      const uint32_t pk = (uint32_t)st.pmask[rr - 1][lane] | ((uint32_t)st.pmask[rr][lane] << 8) |
+                          ((uint32_t)st.pmask[rr + 1][lane] << 16);
+      const uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
+      // left neighbour's second cell: its bits 1 and 5; right neighbour's first: bits 0 and 4
+      uint32_t lL = 0u, lS = 0u, rL = 0u, rS = 0u;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lL |= ((lf >> (8 * k + 1)) & 1u) << k;
+        lS |= ((lf >> (8 * k + 5)) & 1u) << k;
+        rL |= ((rt >> (8 * k)) & 1u) << k;
+        rS |= ((rt >> (8 * k + 4)) & 1u) << k;
+      }
+      if (lane == 0) {
+        lL = lS = 0u;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t h = st.hmask[rr - 1 + k][0];
+          lL |= (h & 1u) << k;
+          lS |= ((h >> 1) & 1u) << k;
+        }
+      }
+      if (lane == 31) {
+        rL = rS = 0u;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t h = st.hmask[rr - 1 + k][1];
+          rL |= (h & 1u) << k;
+          rS |= ((h >> 1) & 1u) << k;
+        }
+      }
+      // over the three rows, bit b: box column bc-1+b is liquid / solid
+      uint32_t Lv = 0xFu, Sv = 0xFu;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t L = (pk >> (8 * k)) & 0x3u, S = (pk >> (8 * k + 4)) & 0x3u;
+        Lv &= ((lL >> k) & 1u) | (L << 1) | (((rL >> k) & 1u) << 3);
+        Sv &= ((lS >> k) & 1u) | (S << 1) | (((rS >> k) & 1u) << 3);
+      }
+      const uint32_t needs = ~((Lv & (Lv >> 1) & (Lv >> 2)) | (Sv & (Sv >> 1) & (Sv >> 2))) & V.outm;
+      const uint32_t cnt = __popc(needs);
+      uint32_t incl = cnt;  // inclusive warp scan of the counts
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t total = __shfl_sync(FULL, incl, 31);
+      int base = 0;
+      if (lane == 31 && total) base = atomicAdd(&p2.nlist, (int)total);
+      base = __shfl_sync(FULL, base, 31);
+      uint32_t off = (uint32_t)base + incl - cnt;
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        if ((needs >> q) & 1u) p2.list[off++] = (uint16_t)((rr << 8) | (V.col + q));
+      needs_all |= needs << (2 * j);
+    }
+    rb = rc;
+    pa = pb;
+    pb = pc;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) jv_lo[q] = jv_hi[q];
+  }
+  return needs_all;
+}
+
+// ---- phase 3: the listed interface cells, one per group thread
+// (compute_phi, fun.cu:1143-1218); new psi into np[rr][x]
+__device__ __forceinline__ void phase3(const TileView &V, const InSlot &in, const P2Smem &p2,
+                                       double (*np)[kWin], bool red, int &itip) {
+  const int nlist = p2.nlist;
+  for (int idx = V.gtid; idx < nlist; idx += kThreads) {
+    const uint32_t e = p2.list[idx];
+    const int rr = (int)(e >> 8), x = (int)(e & 0xFFu) + 4;  // box column
+    const int r = V.y0 - 1 + rr, g = V.x0 + x - 4;
+    const double c00 = in.c[rr][x];
+    const double dG = (1.0 - c00) * V.T.Anb[g] + c00 * V.T.Ati[g] + c00 * (1.0 - c00) * (kL0Liq - kL0Bcc);
+    const double res = phi_cell_dG<double>(
+        &V.F, clamp1(in.psi[rr][x]), clamp1(in.psi[rr][x + 1]), clamp1(in.psi[rr][x - 1]),
+        clamp1(in.psi[rr + 1][x]), clamp1(in.psi[rr - 1][x]), clamp1(in.psi[rr + 1][x + 1]),
+        clamp1(in.psi[rr + 1][x - 1]), clamp1(in.psi[rr - 1][x + 1]), clamp1(in.psi[rr - 1][x - 1]), dG,
+        V.PS.step, (int64_t)(r + V.K.j_offset) * V.K.nx + g, V.K.seed_lo, V.K.seed_hi);
+    np[rr][x] = res;
+    if (red && res > 0.0) itip = max(itip, g == V.K.nx - 2 ? V.K.nx - 1 : g);
+  }
+}
+
+// ---- phase 4: new psi and c of group warp gw's rows into the input tile
+// (after every group thread has finished phase 3)
+__device__ __forceinline__ void phase4_rows(const TileView &V, InSlot &in, const double (*np)[kWin],
+                                            uint32_t needs_all, const double dn[kRowsPerWarp][2], bool red,
+                                            int &itip) {
+  const int rbase = 1 + kRowsPerWarp * V.gw, bc = V.bc;
+#pragma unroll
+  for (int j = 0; j < kRowsPerWarp; ++j) {
+    const int rr = rbase + j;
+    const double2 pv2 = ld2(&in.psi[rr][bc]);
+    const double pv[2] = {pv2.x, pv2.y};
+    const bool live = V.y0 - 1 + rr <= V.K.ny - 2;
+    double po[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const bool listed = (needs_all >> (2 * j + q)) & 1u;
+      po[q] = listed ? np[rr][bc + q] : clamp1(pv[q]);  // phi_next = phi where uniformly +-1
+      if (red && live && !listed && ((V.outm >> q) & 1u) && po[q] > 0.0)
+        itip = max(itip, V.gi + q == V.K.nx - 2 ? V.K.nx - 1 : V.gi + q);
+    }
+    st2(&in.psi[rr][bc], po[0], po[1]);
+    st2(&in.c[rr][bc], dn[j][0], dn[j][1]);
+  }
+}
+
+// ghost columns, then the tile's rows out by bulk copies (group threads
+// < 64: row j, field, kind) and phi by plain stores; returns whether this
+// thread committed a bulk group (it then waits for its reads before the
+// tile's shared memory is reused)
+__device__ __forceinline__ bool store_tile(const TileView &V, InSlot &in, double *__restrict__ psi_n,
+                                           double *__restrict__ c_n, double *__restrict__ phi_n, int bar) {
+  const StepCoef &K = V.K;
+  const int x0 = V.x0, y0 = V.y0;
+  const int nrow = min(kTR, K.ny - 1 - y0);  // output rows of this tile inside the interior
+  const int ncol = min(kW, K.nx - x0);       // columns of this tile inside the array (even)
+  if (x0 == 0 || x0 + kW >= K.nx) {
+    // ghost columns 0 and nx-1 (compute_boundary_individual, fun.cu:1220-1230)
+    gsync(bar);
+    if (V.gtid < nrow) {
+      const int rr = 1 + V.gtid;
+      if (x0 == 0) {
+        in.psi[rr][4] = in.psi[rr][5];
+        in.c[rr][4] = in.c[rr][5];
+      }
+      if (x0 + kW >= K.nx) {
+        const int x = K.nx - 1 - x0 + 4;
+        in.psi[rr][x] = in.psi[rr][x - 1];
+        in.c[rr][x] = in.c[rr][x - 1];
+      }
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // tile writes -> bulk copies
+  gsync(bar);
+  bool any = false;
+  if (V.gtid < 4 * kTR) {
+    const int j = V.gtid >> 2, field = V.gtid & 1, kind = (V.gtid >> 1) & 1;
+    const int r = y0 + j;
+    if (j < nrow) {
+      double *fo = field ? c_n : psi_n;
+      const double *src = field ? &in.c[1 + j][4] : &in.psi[1 + j][4];
+      const uint32_t bytes = (uint32_t)ncol * 8u;
+      if (kind == 0) {
+        bulk_store(fo + (int64_t)r * K.pitch + x0, src, bytes);
+        any = true;
+      } else {
+        if (r == K.jmin) {
+          bulk_store(fo + x0, src, bytes);
+          any = true;
+        }
+        if (r == K.jmax) {
+          bulk_store(fo + (int64_t)(K.ny - 1) * K.pitch + x0, src, bytes);
+          any = true;
+        }
+      }
+      if (any) asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+  }
+  if (phi_n) {  // phi = clamp(psi) of the same rows, plain stores
+    for (int k = V.gtid; k < nrow * ncol; k += kThreads) {
+      const int j = k / ncol, x = k % ncol, r = y0 + j;
+      const double v = clamp1(in.psi[1 + j][4 + x]);
+      phi_n[(int64_t)r * K.pitch + x0 + x] = v;
+      if (r == K.jmin) phi_n[x0 + x] = v;
+      if (r == K.jmax) phi_n[(int64_t)(K.ny - 1) * K.pitch + x0 + x] = v;
+    }
+  }
+  return any;
+}
+
+// the tile's partial sums, and the fused final reduction (the last tile to
+// finish sums every partial, in reduce_partials_kernel's order); scratch of
+// at least 256 doubles and 256 ints
+__device__ __forceinline__ void finish_tile(const TileView &V, P2Smem &p2, double mass, int itip,
+                                            BlockPartial *part, const FinalRed *FR, double *sm_m, int *sm_i,
+                                            int bar) {
+  if (!part) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mass += __shfl_down_sync(FULL, mass, o);
+  itip = __reduce_max_sync(FULL, itip);
+  if (V.lane == 0) {
+    p2.part_mass[V.gw] = mass;
+    p2.part_itip[V.gw] = itip;
+  }
+  gsync(bar);
+  if (V.gtid == 0) {
+    BlockPartial b;
+    b.mass = 0.0;
+    b.itip = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      b.mass += p2.part_mass[w];
+      b.itip = max(b.itip, p2.part_itip[w]);
+    }
+    b.pad = 0;
+    *part = b;
+  }
+  if (!FR) return;
+  if (V.gtid == 0) {
+    __threadfence();
+    p2.last = atomicAdd(FR->counter, 1u) == (unsigned)(FR->nparts - 1);
+  }
+  gsync(bar);
+  if (!p2.last) return;
+  __threadfence();
+  for (int v = V.gtid; v < 256; v += kThreads) {
+    double m = 0.0;
+    int it = 0;
+    for (int k = v; k < FR->nparts; k += 256) {
+      m += __ldcg(&FR->partials[k].mass);
+      it = max(it, __ldcg(&FR->partials[k].itip));
+    }
+    sm_m[v] = m;
+    sm_i[v] = it;
+  }
+  gsync(bar);
+  for (int sz = 128; sz > 0; sz >>= 1) {
+    for (int v = V.gtid; v < sz; v += kThreads) {
+      sm_m[v] += sm_m[v + sz];
+      sm_i[v] = max(sm_i[v], sm_i[v + sz]);
+    }
+    gsync(bar);
+  }
+  if (V.gtid == 0) {
+    if (FR->mass_out) *FR->mass_out = sm_m[0] + FR->mass_offset;
+    if (FR->itip_out) *FR->itip_out = max(1, sm_i[0]);  // get_itip_all_grain starts at 1
+    *FR->counter = 0u;
+  }
+}
+
+// tile (row tr, column tc) of the launch order: tile columns from the one
+// holding the front, tile rows of a column consecutive (they share halo rows
+// in L2)
+__device__ __forceinline__ void tile_of(int t, int nrt, int ncb, int f, int &tr, int &tc) {
+  tr = t % nrt;
+  tc = front_first_block(t / nrt, f, ncb);
+}
+
+// ---------------------------------------------------------------- one tile per CTA
+__global__ void __launch_bounds__(kThreads, 5)
+    tile_kernel_f64(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<double> F,
+                    const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
+                    const __grid_constant__ CUtensorMap tm_c, const double *__restrict__ tab, const int tab_len,
+                    double *__restrict__ psi_n, double *__restrict__ c_n, double *__restrict__ phi_n,
+                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int wave) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  TileSmem64 &sm = *reinterpret_cast<TileSmem64 *>(smem_raw);
+  // blockIdx.x walks the tile rows of one tile column, blockIdx.y the tile
+  // columns, from the one holding column PS.i_front
+  const int f = max(PS.i_front, 0) / kW;
+  int tr, tc;
+  tile_of((int)(blockIdx.y * gridDim.x + blockIdx.x), (int)gridDim.x, (int)gridDim.y, f, tr, tc);
+  const int x0 = kW * tc, y0 = 1 + kTR * tr;
+  BlockPartial *part = partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr;
+  const FinalRed *FRp = partials && FR.counter ? &FR : nullptr;
+
+  if (smem_u32(smem_raw) & 127u) {  // TMA destinations must be 128-byte aligned
+    if (threadIdx.x == 0) atomicExch(err, 2);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.full, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_expect_tx(&sm.full, kTileBytes);
+    tma_load_2d(&sm.in.psi[0][0], &tm_psi, &sm.full, x0 - 4, y0 - 1);
+    tma_load_2d(&sm.in.c[0][0], &tm_c, &sm.full, x0 - 4, y0 - 1);
+    sm.st.liq = 0u;
+    sm.st.sol = 0u;
+    sm.p2.nlist = 0;
+  }
+  // the column table of this step (programmatic dependency on its kernel)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  const TileView V(K, F, PS, tab, tab_len, x0, y0, (int)threadIdx.x);
   __syncthreads();  // barrier initialised, flags cleared
   {
     // bounded wait for the tile; if any thread gives up, the whole CTA skips
@@ -324,360 +750,187 @@ __global__ void __launch_bounds__(kThreads, 5)
         }
       }
       __syncthreads();
-      finish(0.0, 0);
+      finish_tile(V, sm.p2, 0.0, 0, part, FRp, &sm.st.S[0][0], reinterpret_cast<int *>(&sm.st.mu[0][0]), 0);
       return;
     }
   }
-  // columns beyond the array (right-most tiles; zero-filled by TMA) become
-  // bulk melt, so they never force the general path; no output reads them
-  if (x0 + kW + 4 > K.nx) {
-    for (int k = threadIdx.x; k < kTRin * kWin; k += kThreads) {
-      const int rr = k / kWin, x = k % kWin;
-      if (x0 - 4 + x >= K.nx) {
-        sm.psi[rr][x] = -1.0;
-        sm.c[rr][x] = cinf;
-      }
-    }
-    __syncthreads();
-  }
-
-  // ---- phase 1: per-cell terms; warp w takes input rows w, w+4, ...
-#pragma unroll 1
-  for (int rr = warp; rr < kTRin; rr += kWarps) {
-    if (y0 - 1 + rr > K.ny - 1) {  // beyond the array (last tile): never read by an output
-      st2(&sm.S[rr][bc], 0.0, 0.0);
-      st2(&sm.mu[rr][bc], 0.0, 0.0);
-      sm.pmask[rr][lane] = 0x33u;
-      if (lane == 0) {
-        atomicOr(&sm.liq, 1u << rr);
-        atomicOr(&sm.sol, 1u << rr);
-      }
-      continue;
-    }
-    const double2 pv2 = ld2(&sm.psi[rr][bc]), cv2 = ld2(&sm.c[rr][bc]);
-    const double pv[2] = {pv2.x, pv2.y}, cv[2] = {cv2.x, cv2.y};
-    const double dv[2] = {cv[0] - cinf, cv[1] - cinf};
-    double Sv[2], mv[2];
-    const unsigned long long b0 = bits(pv[0]), b1 = bits(pv[1]);
-    const bool liq2 = b0 == kMinus1 && b1 == kMinus1;
-    const bool sol2 = b0 == kPlus1 && b1 == kPlus1;
-    uint32_t code;
-    if (__all_sync(FULL, liq2 && fmax(dv[0], dv[1]) < d_hi && fmin(dv[0], dv[1]) > d_lo)) {
-      // bulk melt: g = -1, q = 1
-      code = 1u;
-      sm.pmask[rr][lane] = 0x03u;
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const double c = cv[q], om = 1.0 - c;
-        const double s = dv[q] / fma(2.0 * cinf, om, dv[q]);
-        Sv[q] = c * om;
-        mv[q] = fma(RTa[q], lam_series(s), dv[q] * KL);
-      }
-    } else {
-      code = (__all_sync(FULL, liq2) ? 1u : 0u) | (__all_sync(FULL, sol2) ? 2u : 0u);
-      // deep solid row: no cell's mu'' enters a flux, so S = mu'' = 0 gives
-      // the same fluxes
-      const uint32_t s3 = (code & 2u) ? solid3(rr) : 0u;
-      if ((code & 2u) && __all_sync(FULL, s3 == 0x3u)) {
-        sm.pmask[rr][lane] = 0x30u;
-        Sv[0] = Sv[1] = mv[0] = mv[1] = 0.0;
-      } else {
-        double s[2];
-        bool small = true;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          s[q] = dv[q] / fma(2.0 * cinf, 1.0 - cv[q], dv[q]);
-          small = small && fabs(s[q]) < 1.0 / 9.0;
-        }
-        const bool series = __all_sync(FULL, small);
-        uint32_t L = 0u, Sm = 0u;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          if (pv[q] <= -1.0) L |= 1u << q;
-          if (pv[q] >= 1.0) Sm |= 1u << q;
-          cell_terms(F, pv[q], cv[q], s[q], series, RTa[q], C0a[q], Sv[q], mv[q]);
-        }
-        sm.pmask[rr][lane] = (uint8_t)(L | (Sm << 4));
-      }
-    }
-    st2(&sm.S[rr][bc], Sv[0], Sv[1]);
-    st2(&sm.mu[rr][bc], mv[0], mv[1]);
-    if (lane == 0) {
-      if (code & 1u) atomicOr(&sm.liq, 1u << rr);
-      if (code & 2u) atomicOr(&sm.sol, 1u << rr);
-    }
-  }
-  // halo columns x0-1 and x0+kW, one thread per cell, on warps 2 and 3, which
-  // have one input row fewer than warps 0 and 1
-  if (threadIdx.x >= 64 && threadIdx.x < 64 + 2 * kTRin) {
-    const int i = (int)threadIdx.x - 64;
-    const int rr = i >> 1, side = i & 1;
-    const int x = side ? kHaloR : kHaloL, g = x0 - 4 + x;
-    double Sh = 0.0, mh = 0.0;
-    uint8_t hm = 3u;
-    if (y0 - 1 + rr <= K.ny - 1) {
-      const double pv = sm.psi[rr][x], cv = sm.c[rr][x];
-      const double dv = cv - cinf;
-      const double s = dv / fma(2.0 * cinf, 1.0 - cv, dv);
-      cell_terms(F, pv, cv, s, fabs(s) < 1.0 / 9.0, tRT[g], tC0[g], Sh, mh);
-      hm = (pv <= -1.0 ? 1u : 0u) | (pv >= 1.0 ? 2u : 0u);
-    }
-    sm.S[rr][x] = Sh;
-    sm.mu[rr][x] = mh;
-    sm.hmask[rr][side] = hm;
-  }
-  const double dKa[3] = {tDK[gi - 1], tDK[gi], tDK[gi + 1]};  // faces x-1|x for x = col .. col+2
+  if (fix_beyond(V, sm.in)) __syncthreads();
+  phase1(V, sm.in, sm.st);
   __syncthreads();
   // phase 1 done: pull the tile of the CTA that will start about one resident
   // wave later into L2, so its loads overlap the rest of this wave's arithmetic
   if (threadIdx.x == 0 && wave > 0) {
     const unsigned nxt = blockIdx.y * gridDim.x + blockIdx.x + (unsigned)wave;
     if (nxt < gridDim.x * gridDim.y) {
-      const int pf_tr = (int)(nxt % gridDim.x);
-      const int pf_tc = front_first_block((int)(nxt / gridDim.x), f, (int)gridDim.y);
-      tma_prefetch_2d(&tm_psi, kW * pf_tc - 4, kTR * pf_tr);
-      tma_prefetch_2d(&tm_c, kW * pf_tc - 4, kTR * pf_tr);
+      int pr, pc;
+      tile_of((int)nxt, (int)gridDim.x, (int)gridDim.y, f, pr, pc);
+      tma_prefetch_2d(&tm_psi, kW * pc - 4, kTR * pr);
+      tma_prefetch_2d(&tm_c, kW * pc - 4, kTR * pr);
     }
   }
-
-  // ---- phase 2: warp w computes output rows 1 + 4w .. 4 + 4w of the tile
-  const uint32_t liq = sm.liq, sol = sm.sol;
   const bool red = part != nullptr;
   double mass = 0.0;
   int itip = 0;
-  struct Row {
-    double s[2], m[2], sl, sr, ml, mr;
-  };
-  // S pair sums of the faces left of cell f (f = 0..2) of a row
-  struct Pairs {
-    double q[3];
-  };
-  auto load_row = [&](int rr, Row &R) {
-    const double2 s = ld2(&sm.S[rr][bc]), m = ld2(&sm.mu[rr][bc]);
-    R.s[0] = s.x;
-    R.s[1] = s.y;
-    R.m[0] = m.x;
-    R.m[1] = m.y;
-    R.sl = sm.S[rr][bc - 1];  // lane 0: the halo column x0-1
-    R.ml = sm.mu[rr][bc - 1];
-    R.sr = sm.S[rr][bc + 2];  // lane 31: the halo column x0+kW
-    R.mr = sm.mu[rr][bc + 2];
-  };
-  auto pairs = [](const Row &R) {
-    Pairs P;
-    P.q[0] = R.sl + R.s[0];
-    P.q[1] = R.s[0] + R.s[1];
-    P.q[2] = R.s[1] + R.sr;
-    return P;
-  };
-  // fluxes through the faces between rows A and B = A+1 (compute_c_CALPHAD
-  // F01/F0m), rounded products so that a face rounds the same wherever the
-  // tiling puts it
-  auto vface = [&](const Row &A, const Row &B, double jv[2]) {
-    const double pp[4] = {A.sl + B.sl, A.s[0] + B.s[0], A.s[1] + B.s[1], A.sr + B.sr};
-#pragma unroll
-    for (int q = 0; q < 2; ++q) jv[q] = __dmul_rn(fma(6.0, pp[q + 1], pp[q] + pp[q + 2]), B.m[q] - A.m[q]);
-  };
-
-  const int rbase = 1 + kRowsPerWarp * warp;
-  Row rb, rc;
-  Pairs pa, pb, pc;
-  double jv_lo[2], jv_hi[2];
   double dn[kRowsPerWarp][2];
-  uint32_t needs_all = 0u;  // 2 bits per output row
-  {
-    Row ra;
-    load_row(rbase - 1, ra);
-    load_row(rbase, rb);
-    vface(ra, rb, jv_lo);
-    pa = pairs(ra);
-    pb = pairs(rb);
-  }
-#pragma unroll
-  for (int j = 0; j < kRowsPerWarp; ++j) {
-    const int rr = rbase + j;  // tile input row of the output row
-    load_row(rr + 1, rc);
-    pc = pairs(rc);
-    vface(rb, rc, jv_hi);
-    // fluxes through the faces (x-1/2, r) for x = col .. col+2
-    const double mm[4] = {rb.ml, rb.m[0], rb.m[1], rb.mr};
-    double jh[3];
-#pragma unroll
-    for (int fc = 0; fc < 3; ++fc)
-      jh[fc] = __dmul_rn(fma(6.0, pb.q[fc], pa.q[fc] + pc.q[fc]), mm[fc + 1] - mm[fc] + dKa[fc]);
-    const double2 cv2 = ld2(&sm.c[rr][bc]);
-    const double cv[2] = {cv2.x, cv2.y};
-#pragma unroll
-    for (int q = 0; q < 2; ++q)
-      dn[j][q] = fmax(fma(cflux4, (jh[q + 1] - jh[q]) + (jv_hi[q] - jv_lo[q]), cv[q]), F.c_floor);
-    const bool live = y0 - 1 + rr <= K.ny - 2;
-    if (red && live) {
-#pragma unroll
-      for (int q = 0; q < 2; ++q)
-        if ((outm >> q) & 1u) mass += dn[j][q];
-    }
-    // phi: cells whose 3x3 neighbourhood is not uniformly +-1 are listed
-    const uint32_t w3 = 7u << (rr - 1);
-    if (live && (liq & w3) != w3 && (sol & w3) != w3) {
-      // per input row k: bits 0-1 psi <= -1, bits 4-5 psi >= 1 of the lane's cells
-      const uint32_t pk = (uint32_t)sm.pmask[rr - 1][lane] | ((uint32_t)sm.pmask[rr][lane] << 8) |
-                          ((uint32_t)sm.pmask[rr + 1][lane] << 16);
-      uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
-      // left neighbour's second cell: its bits 1 and 5; right neighbour's first: bits 0 and 4
-      uint32_t lL = 0u, lS = 0u, rL = 0u, rS = 0u;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        lL |= ((lf >> (8 * k + 1)) & 1u) << k;
-        lS |= ((lf >> (8 * k + 5)) & 1u) << k;
-        rL |= ((rt >> (8 * k)) & 1u) << k;
-        rS |= ((rt >> (8 * k + 4)) & 1u) << k;
-      }
-      if (lane == 0) {
-        lL = lS = 0u;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const uint32_t h = sm.hmask[rr - 1 + k][0];
-          lL |= (h & 1u) << k;
-          lS |= ((h >> 1) & 1u) << k;
-        }
-      }
-      if (lane == 31) {
-        rL = rS = 0u;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const uint32_t h = sm.hmask[rr - 1 + k][1];
-          rL |= (h & 1u) << k;
-          rS |= ((h >> 1) & 1u) << k;
-        }
-      }
-      // over the three rows, bit b: box column bc-1+b is liquid / solid
-      uint32_t Lv = 0xFu, Sv = 0xFu;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const uint32_t L = (pk >> (8 * k)) & 0x3u, S = (pk >> (8 * k + 4)) & 0x3u;
-        Lv &= ((lL >> k) & 1u) | (L << 1) | (((rL >> k) & 1u) << 3);
-        Sv &= ((lS >> k) & 1u) | (S << 1) | (((rS >> k) & 1u) << 3);
-      }
-      const uint32_t needs = ~((Lv & (Lv >> 1) & (Lv >> 2)) | (Sv & (Sv >> 1) & (Sv >> 2))) & outm;
-      const uint32_t cnt = __popc(needs);
-      uint32_t incl = cnt;  // inclusive warp scan of the counts
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(FULL, incl, o);
-        if (lane >= o) incl += v;
-      }
-      const uint32_t total = __shfl_sync(FULL, incl, 31);
-      int base = 0;
-      if (lane == 31 && total) base = atomicAdd(&sm.nlist, (int)total);
-      base = __shfl_sync(FULL, base, 31);
-      uint32_t off = (uint32_t)base + incl - cnt;
-#pragma unroll
-      for (int q = 0; q < 2; ++q)
-        if ((needs >> q) & 1u) sm.list[off++] = (uint16_t)((rr << 8) | (col + q));
-      needs_all |= needs << (2 * j);
-    }
-    rb = rc;
-    pa = pb;
-    pb = pc;
-#pragma unroll
-    for (int q = 0; q < 2; ++q) jv_lo[q] = jv_hi[q];
-  }
+  const uint32_t needs_all = phase2(V, sm.in, sm.st, sm.p2, dn, mass, red);
   __syncthreads();
-
-  // ---- phase 3: interface cells, one per thread (compute_phi, fun.cu:1143-1218)
-  const int nlist = sm.nlist;
-  for (int idx = threadIdx.x; idx < nlist; idx += kThreads) {
-    const uint32_t e = sm.list[idx];
-    const int rr = (int)(e >> 8), x = (int)(e & 0xFFu) + 4;  // box column
-    const int r = y0 - 1 + rr, g = x0 + x - 4;
-    const double c00 = sm.c[rr][x];
-    const double dG = (1.0 - c00) * tAnb[g] + c00 * tAti[g] + c00 * (1.0 - c00) * (kL0Liq - kL0Bcc);
-    const double res = phi_cell_dG<double>(
-        &F, clamp1(sm.psi[rr][x]), clamp1(sm.psi[rr][x + 1]), clamp1(sm.psi[rr][x - 1]), clamp1(sm.psi[rr + 1][x]),
-        clamp1(sm.psi[rr - 1][x]), clamp1(sm.psi[rr + 1][x + 1]), clamp1(sm.psi[rr + 1][x - 1]),
-        clamp1(sm.psi[rr - 1][x + 1]), clamp1(sm.psi[rr - 1][x - 1]), dG, PS.step,
-        (int64_t)(r + K.j_offset) * K.nx + g, K.seed_lo, K.seed_hi);
-    sm.S[rr][x] = res;
-    if (red && res > 0.0) itip = max(itip, g == K.nx - 2 ? K.nx - 1 : g);
-  }
+  phase3(V, sm.in, sm.p2, sm.st.S, red, itip);  // S is free after phase 2
   __syncthreads();
-
-  // ---- phase 4: new psi and c into the tile rows
-#pragma unroll
-  for (int j = 0; j < kRowsPerWarp; ++j) {
-    const int rr = rbase + j;
-    const double2 pv2 = ld2(&sm.psi[rr][bc]);
-    const double pv[2] = {pv2.x, pv2.y};
-    const bool live = y0 - 1 + rr <= K.ny - 2;
-    double po[2];
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const bool listed = (needs_all >> (2 * j + q)) & 1u;
-      po[q] = listed ? sm.S[rr][bc + q] : clamp1(pv[q]);  // phi_next = phi where uniformly +-1
-      if (red && live && !listed && ((outm >> q) & 1u) && po[q] > 0.0)
-        itip = max(itip, gi + q == K.nx - 2 ? K.nx - 1 : gi + q);
-    }
-    st2(&sm.psi[rr][bc], po[0], po[1]);
-    st2(&sm.c[rr][bc], dn[j][0], dn[j][1]);
-  }
-  const int nrow = min(kTR, K.ny - 1 - y0);  // output rows of this tile inside the interior
-  const int ncol = min(kW, K.nx - x0);       // columns of this tile inside the array (even)
-  if (x0 == 0 || x0 + kW >= K.nx) {
-    // ghost columns 0 and nx-1 (compute_boundary_individual, fun.cu:1220-1230)
-    __syncthreads();
-    if (threadIdx.x < nrow) {
-      const int rr = 1 + threadIdx.x;
-      if (x0 == 0) {
-        sm.psi[rr][4] = sm.psi[rr][5];
-        sm.c[rr][4] = sm.c[rr][5];
-      }
-      if (x0 + kW >= K.nx) {
-        const int x = K.nx - 1 - x0 + 4;
-        sm.psi[rr][x] = sm.psi[rr][x - 1];
-        sm.c[rr][x] = sm.c[rr][x - 1];
-      }
-    }
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // tile writes -> bulk copies
-  __syncthreads();
-
-  // ---- bulk copies: thread (row j, field, kind): kind 0 the row itself,
-  // kind 1 its ghost copies (row jmin -> 0, row jmax -> ny-1)
-  if (threadIdx.x < 4 * kTR) {
-    const int j = threadIdx.x >> 2, field = threadIdx.x & 1, kind = (threadIdx.x >> 1) & 1;
-    const int r = y0 + j;
-    if (j < nrow) {
-      double *fo = field ? c_n : psi_n;
-      const double *src = field ? &sm.c[1 + j][4] : &sm.psi[1 + j][4];
-      const uint32_t bytes = (uint32_t)ncol * 8u;
-      bool any = false;
-      if (kind == 0) {
-        bulk_store(fo + (int64_t)r * K.pitch + x0, src, bytes);
-        any = true;
-      } else {
-        if (r == K.jmin) {
-          bulk_store(fo + x0, src, bytes);
-          any = true;
-        }
-        if (r == K.jmax) {
-          bulk_store(fo + (int64_t)(K.ny - 1) * K.pitch + x0, src, bytes);
-          any = true;
-        }
-      }
-      if (any) asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-    }
-  }
-  if (phi_n) {  // phi = clamp(psi) of the same rows, plain stores
-    for (int k = threadIdx.x; k < nrow * ncol; k += kThreads) {
-      const int j = k / ncol, x = k % ncol, r = y0 + j;
-      const double v = clamp1(sm.psi[1 + j][4 + x]);
-      phi_n[(int64_t)r * K.pitch + x0 + x] = v;
-      if (r == K.jmin) phi_n[x0 + x] = v;
-      if (r == K.jmax) phi_n[(int64_t)(K.ny - 1) * K.pitch + x0 + x] = v;
-    }
-  }
-  finish(mass, itip);
+  phase4_rows(V, sm.in, sm.st.S, needs_all, dn, red, itip);
+  store_tile(V, sm.in, psi_n, c_n, phi_n, 0);
+  finish_tile(V, sm.p2, mass, itip, part, FRp, &sm.st.mu[0][0], reinterpret_cast<int *>(&sm.st.mu[8][0]), 0);
   // shared memory stays allocated until the copies have read it
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// ---------------------------------------------------------------- persistent, warp roles
+constexpr int kPipeThreads = 32 + 2 * kThreads;  // producer warp, phase-1 group, phases 2-4 group
+enum { kBarP1 = 1, kBarP2 = 2 };                 // named barriers of the two groups
+
+// AND of a predicate over the 128 threads of a phase group (named barrier)
+__device__ __forceinline__ bool group_and(bool v, int id) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n barrier.red.and.pred q, %2, 128, p;\n"
+      " selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id)
+      : "memory");
+  return r != 0;
+}
+
+// bounded wait on an mbarrier phase; gives up (error flag, abort flag) after
+// the limit or when another role has given up
+__device__ __forceinline__ bool pipe_wait(uint64_t *bar, uint32_t parity, volatile int *abort, uint32_t limit,
+                                          int *err) {
+  uint32_t tries = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if (*abort) return false;
+    if (++tries >= limit) {
+      atomicExch(err, 1);
+      *abort = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kPipeThreads, 2)
+    pipe_kernel_f64(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<double> F,
+                    const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
+                    const __grid_constant__ CUtensorMap tm_c, const double *__restrict__ tab, const int tab_len,
+                    double *__restrict__ psi_n, double *__restrict__ c_n, double *__restrict__ phi_n,
+                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int nrt,
+                    const int ncb) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  PipeSmem64 &sm = *reinterpret_cast<PipeSmem64 *>(smem_raw);
+  const int warp = threadIdx.x >> 5;
+  const int ntiles = nrt * ncb;
+  const int f = max(PS.i_front, 0) / kW;
+  const FinalRed *FRp = partials && FR.counter ? &FR : nullptr;
+  const uint32_t limit = PS.wait_limit ? PS.wait_limit : kWaitLimit;
+  volatile int *abort = &sm.abort;
+  if (smem_u32(smem_raw) & 127u) {  // TMA destinations must be 128-byte aligned
+    if (threadIdx.x == 0) atomicExch(err, 2);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kRing; ++s) {
+      mbar_init(&sm.in_full[s], 1);
+      mbar_init(&sm.in_empty[s], 1);
+    }
+    for (int s = 0; s < kStage; ++s) {
+      mbar_init(&sm.st_full[s], 1);
+      mbar_init(&sm.st_empty[s], 1);
+    }
+    sm.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // the column table of this step (programmatic dependency on its kernel)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  __syncthreads();
+
+  if (warp == 0) {
+    // ---- producer: the input boxes of this CTA's tiles, kRing - 1 ahead of
+    // phases 2-4 (a slot is refilled once its tile's bulk stores have read it)
+    if ((threadIdx.x & 31) == 0) {
+      int k = 0;
+      for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+        const int s = k % kRing;
+        if (k >= kRing && !pipe_wait(&sm.in_empty[s], ((k / kRing) - 1) & 1, abort, limit, err)) break;
+        int tr, tc;
+        tile_of(t, nrt, ncb, f, tr, tc);
+        mbar_expect_tx(&sm.in_full[s], kTileBytes);
+        tma_load_2d(&sm.in[s].psi[0][0], &tm_psi, &sm.in_full[s], kW * tc - 4, kTR * tr);
+        tma_load_2d(&sm.in[s].c[0][0], &tm_c, &sm.in_full[s], kW * tc - 4, kTR * tr);
+      }
+      // loads still in flight into this CTA's shared memory complete before
+      // it exits (bounded)
+      // (a load's slot is only refilled after its tile is done, so only the
+      // last kRing loads can still be in flight)
+      for (int q = max(k - kRing, 0); q < k; ++q)
+        for (uint32_t tt = 0; tt < kWaitLimit && !mbar_try_wait(&sm.in_full[q % kRing], (q / kRing) & 1); ++tt) {
+        }
+    }
+    return;
+  }
+  if (warp <= kWarps) {
+    // ---- phase 1 of tile k into staging slot k % kStage
+    const int gtid = (int)threadIdx.x - 32;
+    int k = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+      const int s = k % kRing, q = k % kStage;
+      // every thread waits (bounded); the group goes on only if all of them saw the phases
+      bool ok = pipe_wait(&sm.in_full[s], (k / kRing) & 1, abort, limit, err);
+      if (ok && k >= kStage) ok = pipe_wait(&sm.st_empty[q], ((k / kStage) - 1) & 1, abort, limit, err);
+      if (!group_and(ok, kBarP1)) break;
+      int tr, tc;
+      tile_of(t, nrt, ncb, f, tr, tc);
+      const TileView V(K, F, PS, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
+      if (gtid == 0) {
+        sm.st[q].liq = 0u;
+        sm.st[q].sol = 0u;
+      }
+      fix_beyond(V, sm.in[s]);
+      gsync(kBarP1);
+      phase1(V, sm.in[s], sm.st[q]);
+      gsync(kBarP1);
+      if (gtid == 0) mbar_arrive(&sm.st_full[q]);
+    }
+    return;
+  }
+  // ---- phases 2-4 of tile k: fluxes, interface cells, stores
+  const int gtid = (int)threadIdx.x - 32 - kThreads;
+  int k = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+    const int s = k % kRing, q = k % kStage;
+    if (!group_and(pipe_wait(&sm.st_full[q], (k / kStage) & 1, abort, limit, err), kBarP2)) break;
+    int tr, tc;
+    tile_of(t, nrt, ncb, f, tr, tc);
+    const TileView V(K, F, PS, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
+    BlockPartial *part = partials ? partials + ((int64_t)tc * nrt + tr) : nullptr;
+    const bool red = part != nullptr;
+    if (gtid == 0) sm.p2.nlist = 0;
+    gsync(kBarP2);
+    double mass = 0.0;
+    int itip = 0;
+    double dn[kRowsPerWarp][2];
+    const uint32_t needs_all = phase2(V, sm.in[s], sm.st[q], sm.p2, dn, mass, red);
+    gsync(kBarP2);
+    phase3(V, sm.in[s], sm.p2, sm.st[q].S, red, itip);  // S of the slot is free after phase 2
+    gsync(kBarP2);
+    phase4_rows(V, sm.in[s], sm.st[q].S, needs_all, dn, red, itip);
+    const bool issued = store_tile(V, sm.in[s], psi_n, c_n, phi_n, kBarP2);
+    finish_tile(V, sm.p2, mass, itip, part, FRp, &sm.st[q].mu[0][0], reinterpret_cast<int *>(&sm.st[q].mu[8][0]),
+                kBarP2);
+    // the slots are free once the bulk copies have read the input tile
+    if (issued) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    gsync(kBarP2);
+    if (gtid == 0) {
+      mbar_arrive(&sm.st_empty[q]);
+      mbar_arrive(&sm.in_empty[s]);
+    }
+  }
   asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
@@ -688,23 +941,22 @@ int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScal
                         int *nparts_out, int *err, cudaStream_t st) {
   const int nj = K.ny - 2;
   if (K.nx % 2 || K.pitch != K.nx) return -1;  // rows are copied in 16-byte units
-  // column-major: consecutive CTAs share a column strip and its halo rows in L2
-  const dim3 grid((nj + kTR - 1) / kTR, (K.nx + kW - 1) / kW), block(kThreads);
-  if (grid.y > 65535 || (int64_t)grid.x * grid.y > (1 << 30)) return -1;
-  const int nparts = grid.x * grid.y;
+  const int nrt = (nj + kTR - 1) / kTR, ncb = (K.nx + kW - 1) / kW;
+  if (ncb > 65535 || (int64_t)nrt * ncb > (1 << 30)) return -1;
+  const int nparts = nrt * ncb;
   if (partials && nparts > max_partials) return -1;
-  if (!tm.col_tab64 || tm.col_tab64_len < (int)grid.y * kW + kWin) return -1;
-  const size_t smem = sizeof(TileSmem64);
-  static std::atomic<unsigned long long> attr_done{0};
-  if (!smem_limit_once((const void *)tile_kernel_f64, (int)smem, attr_done)) return -3;
-  static std::atomic<int> wave_of[64];
-  const int wave = resident_ctas((const void *)tile_kernel_f64, kThreads, smem, wave_of);
-  if (wave < 0) return -3;
+  if (!tm.col_tab64 || tm.col_tab64_len < ncb * kW + kWin) return -1;
+  const bool pipe = tm.pipeline != 0;
+  const size_t smem = pipe ? sizeof(PipeSmem64) : sizeof(TileSmem64);
+  const void *kfn = pipe ? (const void *)pipe_kernel_f64 : (const void *)tile_kernel_f64;
+  static std::atomic<unsigned long long> attr_done[2];
+  if (!smem_limit_once(kfn, (int)smem, attr_done[pipe])) return -3;
+  static std::atomic<int> resident_of[2][64];
+  const int resident = resident_ctas(kfn, pipe ? kPipeThreads : kThreads, smem, resident_of[pipe]);
+  if (resident <= 0) return -3;
   column_table_kernel_f64<<<(tm.col_tab64_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(
       K, P.d0, P.d1, tm.col_tab64_len, tm.col_tab64);
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
@@ -717,9 +969,21 @@ int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScal
   fr.partials = partials;
   fr.nparts = nparts;
   if (!partials || !(fr.mass_out || fr.itip_out)) fr.counter = nullptr;
-  if (cudaLaunchKernelEx(&cfg, tile_kernel_f64, K, F, P, tm.psi, tm.c, tab, tm.col_tab64_len, psi_n, c_n, phi_n,
-                         partials, err, fr, wave) != cudaSuccess)
-    return -3;
+  cudaError_t e;
+  if (pipe) {
+    // persistent: every CTA resident at once, each walking tiles b, b + G, ...
+    cfg.gridDim = dim3((unsigned)std::min(resident, nparts));
+    cfg.blockDim = dim3(kPipeThreads);
+    e = cudaLaunchKernelEx(&cfg, pipe_kernel_f64, K, F, P, tm.psi, tm.c, tab, tm.col_tab64_len, psi_n, c_n, phi_n,
+                           partials, err, fr, nrt, ncb);
+  } else {
+    // column-major: consecutive CTAs share a column strip and its halo rows in L2
+    cfg.gridDim = dim3(nrt, ncb);
+    cfg.blockDim = dim3(kThreads);
+    e = cudaLaunchKernelEx(&cfg, tile_kernel_f64, K, F, P, tm.psi, tm.c, tab, tm.col_tab64_len, psi_n, c_n, phi_n,
+                           partials, err, fr, resident);
+  }
+  if (e != cudaSuccess) return -3;
   if (nparts_out) *nparts_out = nparts;
   return 0;
 }

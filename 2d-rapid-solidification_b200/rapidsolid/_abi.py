@@ -9,6 +9,7 @@ RS_ABI_VERSION = 9
 RS_MLP_NPARAMS = 1250
 RS_OPT_TMA = 1
 RS_OPT_WAIT_LIMIT = 2
+RS_OPT_PIPELINE = 3
 RS_OK = 0
 RS_E_INVALID = -1
 RS_E_CUDA = -2

@@ -23,6 +23,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--grid", type=int, default=0, help="override Nx_all = Ny_all")
     ap.add_argument("--no-tma", action="store_true", help="use the register-prefetch kernel")
+    ap.add_argument("--pipeline", action="store_true", help="FP64: the persistent warp-role tile kernel")
     ap.add_argument("--nz", type=int, default=0, help="3D: override the number of z planes")
     a = ap.parse_args(argv)
     if a.config == "peritectic_3d":
@@ -33,6 +34,8 @@ def main(argv=None):
     ctx = lib.Context(p)
     if a.no_tma:
         ctx.set_option(_abi.RS_OPT_TMA, 0)
+    if a.pipeline:
+        ctx.set_option(_abi.RS_OPT_PIPELINE, 1)
     d = ctx.d
     dt = torch.float64 if a.precision == "f64" else torch.float32
     cur, nxt = lib.FieldSet(p, dt), lib.FieldSet(p, dt)
@@ -57,11 +60,12 @@ def main(argv=None):
     return 0
 
 
-def tip_run(p, dtype, nsteps, every=1000, surrogate=None, ic_seed=None):
+def tip_run(p, dtype, nsteps, every=1000, surrogate=None, ic_seed=None, initial=None):
     """The reference loop (main.cu:156-240) on the workload p from its seeded
     planar front: pull-back every step_pull_back steps, the precise tip every
     `every` steps as set_tip_output does (fun.cu:3024-3050).  surrogate:
     (weights, box) of a trained network, or None for the exact evaluation.
+    initial: (c_liquid, c_solid) of the planar front (default Ti-10Nb).
     Returns (tip positions x = (i_offset_history + tip.x) dx in units of W,
     tip velocity in m/s over the second half of the run, the surrogate's
     audit (or None), solute mass at the start and at the end)."""
@@ -73,8 +77,8 @@ def tip_run(p, dtype, nsteps, every=1000, surrogate=None, ic_seed=None):
     if surrogate is not None:
         ctx.set_surrogate(*surrogate)
     a, b = lib.FieldSet(p, dtype), lib.FieldSet(p, dtype)
-    ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ,
-                       configs.IC_SEED if ic_seed is None else ic_seed)
+    cl, cs = initial if initial is not None else (configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ)
+    ctx.initial_planar(a, cl, cs, configs.IC_SEED if ic_seed is None else ic_seed)
     itip = torch.zeros(1, dtype=torch.int32, device="cuda")
     tipbuf = torch.zeros(C.sizeof(_abi.Tip), dtype=torch.uint8, device="cuda")
     mass = torch.zeros(2, dtype=torch.float64, device="cuda")

@@ -37,6 +37,16 @@ def fitted_box(T_sol=configs.T_SOLIDUS_TI10NB, T_liq=configs.T_LIQUIDUS_TI10NB):
     return b
 
 
+def ensemble_box(params):
+    """A box over every run of an ensemble: T from 200 K below the lowest
+    front temperature (each run starts at its solidus) to 80 K above the
+    highest, c = x_Ti in [0.60, 0.999] (x_Nb <= 0.40, as the wide box)."""
+    Ts = [p.Tmelt + p.delta_initial * (p.Tmelt - p.T_ref) for p in params]
+    b = default_box()
+    b.T_lo, b.T_hi = min(Ts) - 200.0, max(Ts) + 80.0
+    return b
+
+
 def init_weights(seed=0):
     """Glorot-uniform weights, zero biases, as a float32 numpy vector."""
     rng = np.random.default_rng(seed)

@@ -49,6 +49,9 @@ WORKLOAD = ("Ti-10Nb directional solidification 2048x2048, exact CALPHAD, frozen
 # mass reduction is fused into that kernel)
 STEP_PATH = {"f32": ("rs::tile_kernel<false>", 2, True),
              "f64": ("rs::tile_kernel_f64", 2, True)}
+# the FP64 step's kernel of the headline: 0 one tile per CTA, 1 the
+# persistent warp-role pipeline (the other one is timed as a side leg)
+PIPELINE = 0
 
 
 def rank_info():
@@ -164,13 +167,15 @@ class Loop:
     tip reduced on the device, 4-byte read), then the fused step; counts the
     library's kernel launches."""
 
-    def __init__(self, p, dtype, ic_seed=None):
+    def __init__(self, p, dtype, ic_seed=None, options=None):
         import torch
         from rapidsolid import configs, lib
         self.torch = torch
         self.p, self.dtype = p, dtype
         self.prec = "f64" if dtype == torch.float64 else "f32"
         self.ctx = lib.Context(p)
+        for k, v in (options or {}).items():
+            self.ctx.set_option(k, v)
         self.d = self.ctx.d
         self.a, self.b = lib.FieldSet(p, dtype), lib.FieldSet(p, dtype)
         self.ctx.initial_planar(self.a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ,
@@ -262,6 +267,13 @@ def e2e_interval(loop, nsteps, dist, world, st):
                     "psi and c; no L2 flush"}
 
 
+def kernel_name(prec, options):
+    from rapidsolid import _abi
+    if prec == "f64" and (options or {}).get(_abi.RS_OPT_PIPELINE, 0):
+        return "rs::pipe_kernel_f64"
+    return STEP_PATH[prec][0]
+
+
 def roofline(prec, cells, kern_ms, peak, peak_kind, kernel):
     alg = BYTES_PER_CELL[prec] * cells
     achieved = alg / (kern_ms * 1e-3) / 1e9
@@ -271,9 +283,9 @@ def roofline(prec, cells, kern_ms, peak, peak_kind, kernel):
             "traffic": profiled_traffic(f"step_{prec}_2048")}
 
 
-def run_arm(p, dtype, args, flush, st, dist, world, clocks=None):
+def run_arm(p, dtype, args, flush, st, dist, world, clocks=None, options=None, e2e=True):
     """Warm-up, timed steps (L2 flushed), roofline and e2e of one precision."""
-    loop = Loop(p, dtype)
+    loop = Loop(p, dtype, options=options)
     for _ in range(args.warmup):
         loop.step()
     loop.torch.cuda.synchronize()
@@ -307,9 +319,10 @@ def run_arm(p, dtype, args, flush, st, dist, world, clocks=None):
     peak, peak_kind = measured_peak()
     out = {"value": round(job_throughput(world, cells, args.steps, total_ms), 4),
            "ms_per_step": round(total_ms / args.steps, 5),
-           "roofline": roofline(loop.prec, cells, kern_ms, peak, peak_kind, STEP_PATH[loop.prec][0]),
+           "roofline": roofline(loop.prec, cells, kern_ms, peak, peak_kind, kernel_name(loop.prec, options)),
            "gpu_launches": launches, "wall_s_timed": round(t_wall, 3), "clocks": clk}
-    out["e2e"] = e2e_interval(loop, loop.d.step_fields, dist, world, st)
+    if e2e:
+        out["e2e"] = e2e_interval(loop, loop.d.step_fields, dist, world, st)
     loop.close()
     return out
 
@@ -331,7 +344,9 @@ def run_ours(args):
     d = lib.derive(p)
     st = torch.cuda.current_stream()
     flush = Flush()
-    head = run_arm(p, torch.float64, args, flush, st, dist, world, clocks=ClockSampler(local))
+    from rapidsolid import _abi
+    head = run_arm(p, torch.float64, args, flush, st, dist, world, clocks=ClockSampler(local),
+                   options={_abi.RS_OPT_PIPELINE: PIPELINE})
 
     line = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -346,6 +361,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, seconds=args.cpu_seconds)
     if rank == 0 and world == 1 and not args.no_side_legs:
+        alt = run_arm(p, torch.float64, args, flush, st, None, 1, options={_abi.RS_OPT_PIPELINE: 1 - PIPELINE},
+                      e2e=False)
+        alt.pop("clocks")
+        line["fp64_other_kernel"] = {"pipeline": 1 - PIPELINE, "value": alt["value"],
+                                     "ms_per_step": alt["ms_per_step"], "roofline": alt["roofline"]}
         fp32 = run_arm(p, torch.float32, args, flush, st, None, 1)
         fp32.pop("clocks")
         line["fp32_exact"] = fp32
@@ -427,14 +447,14 @@ def beyond_l2_leg(n=8192, steps=10):
     FP64: 1 GiB), far beyond the 126 MB L2: no flush is needed and the
     sustained HBM fraction is read directly from back-to-back steps."""
     import torch
-    from rapidsolid import configs
+    from rapidsolid import _abi, configs
     p = configs.scale()
     p.nx_all = p.ny_all = n
     cells = (n - 2) * (n - 2)
     peak, peak_kind = measured_peak()
     out = {}
     for prec, dtype in (("f32", torch.float32), ("f64", torch.float64)):
-        loop = Loop(p, dtype)
+        loop = Loop(p, dtype, options={_abi.RS_OPT_PIPELINE: PIPELINE})
         for _ in range(3):
             loop.step()
         torch.cuda.synchronize()
@@ -446,7 +466,7 @@ def beyond_l2_leg(n=8192, steps=10):
         torch.cuda.synchronize()
         ts = sorted(s.elapsed_time(e) for s, e in ev)
         ms = ts[len(ts) // 2]
-        rl = roofline(prec, cells, ms, peak, peak_kind, STEP_PATH[prec][0])
+        rl = roofline(prec, cells, ms, peak, peak_kind, kernel_name(prec, {_abi.RS_OPT_PIPELINE: PIPELINE}))
         rl.pop("traffic")
         out[prec] = {"value": round(cells / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms, 5), "roofline": rl}
         loop.close()
@@ -607,22 +627,36 @@ def peritectic_3d_leg(peak, nsteps_run=5000, ntimed=10):
     return out
 
 
-def ensemble_leg(flush, nruns=64, nsteps=100):
-    """The batched ensemble of uneven runs (64 Ti-Nb runs, sizes 256^2 ..
-    1024x2048, V 0.01-2 m/s, G 1e5-1e7 K/m, x_Nb 0.05-0.20, seeded): aggregate
-    Gcell-steps/s of the one-launch, graph-replayed step, against the same runs
-    stepped one rs_step at a time."""
+def _ensemble(runs, sur=None):
     import torch
-    from rapidsolid import configs, lib
-    runs = configs.ensemble(nruns)
-    ps = [p for p, _, _ in runs]
-    cells = sum((p.nx_all - 2) * (p.ny_all - 2) for p in ps)
-    ens = lib.Ensemble(ps)
+    from rapidsolid import lib
+    ens = lib.Ensemble([p for p, _, _ in runs])
     for r, (p, cl, cs) in enumerate(runs):
         a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
         ens.ctx[r].initial_planar(a, cl, cs, 7 + r)
+        if sur is not None:
+            ens.ctx[r].set_surrogate(*sur)
         ens.bind(r, a, b)
-    choice, tune_ms = ens.autotune(reps=5)
+    return ens
+
+
+def _ensemble_tips(ens, runs):
+    """x of every run's precise tip, (i_offset_history + tip.x) dx in W."""
+    import ctypes as C
+    import torch
+    from rapidsolid import _abi, lib
+    buf = torch.zeros(C.sizeof(_abi.Tip), dtype=torch.uint8, device="cuda")
+    xs = []
+    for r, (p, _, _) in enumerate(runs):
+        _, hist, _, cur = ens.state(r)
+        ens.ctx[r].precise_tip(cur, buf)
+        t = lib.tip_from_bytes(buf.cpu().numpy().tobytes())
+        xs.append((hist + t.x) * p.dx)
+    return xs
+
+
+def _timed_ensemble(ens, flush, nsteps):
+    import torch
     ens.steps(3)  # step 0 pulls every run back (eager), then graph replays
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -631,7 +665,30 @@ def ensemble_leg(flush, nruns=64, nsteps=100):
     ens.steps(nsteps)
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    return e0.elapsed_time(e1)
+
+
+def ensemble_leg(flush, nruns=64, nsteps=100, vel_steps=4000):
+    """The batched ensemble of uneven runs (64 Ti-Nb runs, sizes 256^2 ..
+    1024x2048, V 0.01-2 m/s, G 1e5-1e7 K/m, x_Nb 0.05-0.20, seeded): aggregate
+    Gcell-steps/s of the one-launch, graph-replayed step, exact FP32 and
+    through the learned surrogate (one network trained on a box that spans
+    every run's compositions and temperatures), against the same runs stepped
+    one rs_step at a time; per-run tip velocity of the surrogate ensemble
+    against each run stepped alone on the exact path."""
+    import torch
+    from rapidsolid import configs, run, surrogate
+    runs = configs.ensemble(nruns)
+    ps = [p for p, _, _ in runs]
+    cells = sum((p.nx_all - 2) * (p.ny_all - 2) for p in ps)
+    out = {"runs": nruns, "cells": cells, "steps": nsteps}
+    # exact path
+    ens = _ensemble(runs)
+    choice, tune_ms = ens.autotune(reps=5)
+    ms = _timed_ensemble(ens, flush, nsteps)
+    out["exact"] = {"value": round(cells * nsteps / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms / nsteps, 5),
+                    "autotune": {"choice": ["run by run", "largest first", "interleaved"][choice],
+                                 "ms_per_launch": [round(x, 5) for x in tune_ms]}}
     # the same runs one by one (two launches per run and step)
     ctxs = [ens.ctx[r] for r in range(nruns)]
     cur = [ens.state(r)[3] for r in range(nruns)]
@@ -645,14 +702,51 @@ def ensemble_leg(flush, nruns=64, nsteps=100):
     s1.record()
     torch.cuda.synchronize()
     ms_single = s0.elapsed_time(s1) / 10
+    out["one_by_one"] = {"value": round(cells / (ms_single * 1e-3) / 1e9, 3), "ms_per_step": round(ms_single, 5)}
     ens.close()
-    return {"value": round(cells * nsteps / (ms * 1e-3) / 1e9, 3), "runs": nruns, "cells": cells,
-            "ms_per_step": round(ms / nsteps, 5), "steps": nsteps,
-            "one_by_one": {"value": round(cells / (ms_single * 1e-3) / 1e9, 3), "ms_per_step": round(ms_single, 5)},
-            "autotune": {"choice": ["run by run", "largest first", "interleaved"][choice],
-                         "ms_per_launch": [round(x, 5) for x in tune_ms]},
-            "note": "FP32 exact path (the surrogate is slower, see its leg); CUDA graph "
-                    "replays between pull-backs; every run equals its single run bit for bit (tests)"}
+    # surrogate path: one network on a box over all runs
+    box = surrogate.ensemble_box(ps)
+    w, box, hist = surrogate.train(ps[0], box=box, epochs=40, seed=1)
+    ens = _ensemble(runs, (w, box))
+    choice, tune_ms = ens.autotune(reps=5)
+    ms = _timed_ensemble(ens, flush, nsteps)
+    out["surrogate"] = {"value": round(cells * nsteps / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms / nsteps, 5),
+                        "autotune": {"choice": ["run by run", "largest first", "interleaved"][choice],
+                                     "ms_per_launch": [round(x, 5) for x in tune_ms]},
+                        "box": {"T": [round(box.T_lo, 2), round(box.T_hi, 2)], "c": [box.c_lo, box.c_hi]}}
+    ens.close()
+    # per-run tip velocity over the second half of vel_steps: the surrogate
+    # ensemble against each run stepped alone on the exact path
+    ens = _ensemble(runs, (w, box))
+    x0 = _ensemble_tips(ens, runs)
+    ens.steps(vel_steps // 2)
+    xh = _ensemble_tips(ens, runs)
+    ens.steps(vel_steps - vel_steps // 2)
+    x1 = _ensemble_tips(ens, runs)
+    audit = [ens.ctx[r].surrogate_audit() for r in range(nruns)]
+    ens.close()
+    errs = []
+    for r, (p, cl, cs) in enumerate(runs):
+        xs, v_exact, _, _, _ = run.tip_run(p, torch.float32, vel_steps, every=vel_steps // 2, ic_seed=7 + r,
+                                           initial=(cl, cs))
+        d = lib_derive(p)
+        v_ens = (x1[r] - xh[r]) * p.S * p.W0 / ((vel_steps - vel_steps // 2) * d.tau0 * d.dt)
+        errs.append({"run": r, "grid": [p.nx_all, p.ny_all], "V_pull": round(p.Vp, 4),
+                     "tip_speed_m_s": [round(v_exact, 5), round(v_ens, 5)],
+                     "rel_error": round(abs(v_ens - v_exact) / max(abs(v_exact), 1e-12), 5)})
+    rel = sorted(e["rel_error"] for e in errs)
+    out["surrogate"]["tip_velocity_vs_single_exact_runs"] = {
+        "steps": vel_steps, "median_rel_error": rel[len(rel) // 2], "max_rel_error": rel[-1],
+        "fallback_cells": int(sum(a[2] for a in audit)), "per_run": errs}
+    out["value"] = out["exact"]["value"]
+    out["note"] = ("CUDA graph replays between pull-backs; every run equals its single run bit for bit on both "
+                   "paths (tests)")
+    return out
+
+
+def lib_derive(p):
+    from rapidsolid import lib
+    return lib.derive(p)
 
 
 def cpu_baseline(p, seconds=12.0, steps=None):

@@ -185,9 +185,14 @@ int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
  * RS_OPT_WAIT_LIMIT (default 0: the kernels' own limit of 2^20 tries) bounds
  * the tile kernels' wait for their TMA loads; a tile whose wait gives up is
  * not computed or stored, and rs_device_status reports RS_E_STATE.  Tests set
- * it to 1 to run that path. */
+ * it to 1 to run that path.
+ * RS_OPT_PIPELINE (default 0) runs the FP64 tile step as a persistent kernel
+ * of warp roles (a TMA producer warp, a phase-1 group and a flux/update/store
+ * group working on three tiles at once) instead of one tile per CTA; both
+ * give the same fields bit for bit. */
 #define RS_OPT_TMA 1
 #define RS_OPT_WAIT_LIMIT 2
+#define RS_OPT_PIPELINE 3
 int rs_set_option(rs_ctx *ctx, int32_t option, int64_t value);
 
 /* Device-side waits are bounded: if one gave up since the last call, returns
@@ -348,7 +353,11 @@ int rs_surrogate_audit(rs_ctx *ctx, double *max_err_mu, double *max_err_dG, int6
  * run pulls back are replayed from a CUDA graph; a run's pull-back step
  * (every step_pull_back of its own) is taken by rs_itip + rs_step on its
  * context, as main.cu does.  Runs must use the frozen temperature without
- * the Vp ramp. */
+ * the Vp ramp.  Surrogate path: when every run's context has a network set
+ * (rs_set_surrogate) before the first rs_ensemble_steps or
+ * rs_ensemble_autotune, the batched launch evaluates the cells through each
+ * run's network (fallback and audit as in rs_step); a mix of runs with and
+ * without one is rejected with RS_E_UNSUPPORTED. */
 typedef struct rs_ens rs_ens;
 int rs_ensemble_create(const rs_params *params, int32_t nruns, rs_ens **out);
 int rs_ensemble_destroy(rs_ens *e);

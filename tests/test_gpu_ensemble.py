@@ -4,7 +4,7 @@ same runs stepped one by one through rs_step, bit for bit."""
 import numpy as np
 import pytest
 
-from rapidsolid import configs, lib
+from rapidsolid import configs, lib, surrogate
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -23,8 +23,10 @@ def params():
     return out
 
 
-def single(p):
+def single(p, sur=None):
     ctx = lib.Context(p)
+    if sur is not None:
+        ctx.set_surrogate(*sur)
     d = ctx.d
     a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
     ctx.initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, 7)
@@ -63,4 +65,28 @@ def test_ensemble_equals_single_runs():
         assert hist == hist1 and l == l1
         assert np.array_equal(cur.psi.cpu().numpy(), psi), r
         assert np.array_equal(cur.c.cpu().numpy(), c), r
+    ens.close()
+
+
+def test_ensemble_surrogate_path_equals_single_runs():
+    """With a network set on every run's context, the batched launch takes
+    the surrogate path of the tile kernel: each run equals the same run
+    stepped alone through rs_step with the same network, bit for bit."""
+    ps = params()
+    w, box, _ = surrogate.train(ps[0], n_samples=1 << 15, epochs=3, batch=2048, seed=3)
+    ens = lib.Ensemble(ps)
+    for r, p in enumerate(ps):
+        a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
+        ens.ctx[r].initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, 7)
+        ens.ctx[r].set_surrogate(w, box)
+        ens.bind(r, a, b)
+    ens.steps(STEPS)
+    torch.cuda.synchronize()
+    for r, p in enumerate(ps):
+        step, hist, l, cur = ens.state(r)
+        psi, c, hist1, l1 = single(p, (w, box))
+        assert hist == hist1 and l == l1
+        assert np.array_equal(cur.psi.cpu().numpy(), psi), r
+        assert np.array_equal(cur.c.cpu().numpy(), c), r
+        assert ens.ctx[r].surrogate_audit()[3] > 0  # the run's cells went through its network
     ens.close()

@@ -271,6 +271,36 @@ def test_f64_step_with_deep_solid_matches_oracle(tma):
     assert np.array_equal(g.c[deep], s.c[deep]) and np.array_equal(g.psi[deep], s.psi[deep])
 
 
+@pytest.mark.parametrize("shape", [(64, 48), (300, 130), (1030, 1038)])
+def test_f64_pipeline_kernel_equals_tile_kernel(shape):
+    """The persistent warp-role FP64 kernel (RS_OPT_PIPELINE) runs the same
+    phase functions as the one-tile-per-CTA kernel: fields and the fused
+    solute mass and coarse tip bit for bit, over 30 steps with noise, on grids
+    whose tiles do not divide them (1030 x 1038: several tiles per CTA)."""
+    p = configs.small(*shape, i_tip_target=22, G=5e6, V=0.5, noise_amplitude=0.05, seed=7)
+    d = pyoracle.derive(p)
+    s = perturbed_state(p, 3, amp=0.3)
+    out = []
+    for pipe in (0, 1):
+        ctx = lib.Context(p)
+        ctx.set_option(_abi.RS_OPT_PIPELINE, pipe)
+        a, b = upload(p, s, with_phi=True), lib.FieldSet(p, torch.float64, with_phi=True)
+        m = torch.zeros(30, dtype=torch.float64, device="cuda")
+        it = torch.zeros(30, dtype=torch.int32, device="cuda")
+        l = 0.0
+        for n in range(30):
+            ctx.step(a, b, n, l_offset_Vp=l, mass_out=m[n:n + 1], itip_out=it[n:n + 1])
+            l += pyoracle.l_offset_increment(p, d, n)
+            a, b = b, a
+        torch.cuda.synchronize()
+        ctx.device_status()
+        g = download(p, a)
+        out.append((g.psi, g.c, a.phi.cpu().numpy(), m.cpu().numpy(), it.cpu().numpy()))
+        ctx.close()
+    for x, y in zip(out[0], out[1]):
+        assert np.array_equal(x, y)
+
+
 def test_tma_and_register_paths_agree():
     """Both kernels run the same per-cell arithmetic; they differ only where
     the compiler contracts a multiply-add differently."""
