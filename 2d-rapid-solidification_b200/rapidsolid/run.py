@@ -24,6 +24,8 @@ def main(argv=None):
     ap.add_argument("--grid", type=int, default=0, help="override Nx_all = Ny_all")
     ap.add_argument("--no-tma", action="store_true", help="use the register-prefetch kernel")
     ap.add_argument("--pipeline", action="store_true", help="FP64: the persistent warp-role tile kernel")
+    ap.add_argument("--surrogate", action="store_true",
+                    help="FP32: train the CALPHAD surrogate on the wide box (10 epochs) and step through it")
     ap.add_argument("--nz", type=int, default=0, help="3D: override the number of z planes")
     a = ap.parse_args(argv)
     if a.config == "peritectic_3d":
@@ -36,6 +38,10 @@ def main(argv=None):
         ctx.set_option(_abi.RS_OPT_TMA, 0)
     if a.pipeline:
         ctx.set_option(_abi.RS_OPT_PIPELINE, 1)
+    if a.surrogate:
+        from . import surrogate
+        w, box, _ = surrogate.train(p, box=surrogate.default_box(), epochs=10, seed=1)
+        ctx.set_surrogate(w, box)
     d = ctx.d
     dt = torch.float64 if a.precision == "f64" else torch.float32
     cur, nxt = lib.FieldSet(p, dt), lib.FieldSet(p, dt)
