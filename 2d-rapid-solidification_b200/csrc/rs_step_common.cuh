@@ -275,6 +275,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// non-blocking: whether the phase has completed now (try_wait may suspend the
+// thread for a while first; a wait bounded by a count of test_wait polls
+// gives up after that many polls, which the tests use to reach the give-up
+// path)
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// one try of a bounded wait: the suspending try_wait, or (test limit set) a
+// non-blocking poll
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity, bool poll) {
+  return poll ? mbar_test_wait(bar, parity) : mbar_try_wait(bar, parity);
+}
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(

@@ -363,7 +363,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const uint32_t limit = PS.wait_limit ? PS.wait_limit : kWaitLimit;
     uint32_t tries = 0;
     bool gave_up = false;
-    while (!mbar_try_wait(&sm.full, 0)) {
+    while (!mbar_try(&sm.full, 0, PS.wait_limit != 0)) {
       if (++tries >= limit) {
         gave_up = true;
         break;

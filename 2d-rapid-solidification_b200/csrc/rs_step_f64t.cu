@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(kThreads, 5)
     const uint32_t limit = PS.wait_limit ? PS.wait_limit : kWaitLimit;
     uint32_t tries = 0;
     bool gave_up = false;
-    while (!mbar_try_wait(&sm.full, 0)) {
+    while (!mbar_try(&sm.full, 0, PS.wait_limit != 0)) {
       if (++tries >= limit) {
         gave_up = true;
         break;
@@ -802,9 +802,9 @@ __device__ __forceinline__ bool group_and(bool v, int id) {
 // bounded wait on an mbarrier phase; gives up (error flag, abort flag) after
 // the limit or when another role has given up
 __device__ __forceinline__ bool pipe_wait(uint64_t *bar, uint32_t parity, volatile int *abort, uint32_t limit,
-                                          int *err) {
+                                          int *err, bool poll) {
   uint32_t tries = 0;
-  while (!mbar_try_wait(bar, parity)) {
+  while (!mbar_try(bar, parity, poll)) {
     if (*abort) return false;
     if (++tries >= limit) {
       atomicExch(err, 1);
@@ -829,6 +829,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
   const int f = max(PS.i_front, 0) / kW;
   const FinalRed *FRp = partials && FR.counter ? &FR : nullptr;
   const uint32_t limit = PS.wait_limit ? PS.wait_limit : kWaitLimit;
+  const bool poll = PS.wait_limit != 0;
   volatile int *abort = &sm.abort;
   if (smem_u32(smem_raw) & 127u) {  // TMA destinations must be 128-byte aligned
     if (threadIdx.x == 0) atomicExch(err, 2);
@@ -857,7 +858,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
       int k = 0;
       for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
         const int s = k % kRing;
-        if (k >= kRing && !pipe_wait(&sm.in_empty[s], ((k / kRing) - 1) & 1, abort, limit, err)) break;
+        if (k >= kRing && !pipe_wait(&sm.in_empty[s], ((k / kRing) - 1) & 1, abort, limit, err, poll)) break;
         int tr, tc;
         tile_of(t, nrt, ncb, f, tr, tc);
         mbar_expect_tx(&sm.in_full[s], kTileBytes);
@@ -881,8 +882,8 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
       const int s = k % kRing, q = k % kStage;
       // every thread waits (bounded); the group goes on only if all of them saw the phases
-      bool ok = pipe_wait(&sm.in_full[s], (k / kRing) & 1, abort, limit, err);
-      if (ok && k >= kStage) ok = pipe_wait(&sm.st_empty[q], ((k / kStage) - 1) & 1, abort, limit, err);
+      bool ok = pipe_wait(&sm.in_full[s], (k / kRing) & 1, abort, limit, err, poll);
+      if (ok && k >= kStage) ok = pipe_wait(&sm.st_empty[q], ((k / kStage) - 1) & 1, abort, limit, err, poll);
       if (!group_and(ok, kBarP1)) break;
       int tr, tc;
       tile_of(t, nrt, ncb, f, tr, tc);
@@ -904,7 +905,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
   int k = 0;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
     const int s = k % kRing, q = k % kStage;
-    if (!group_and(pipe_wait(&sm.st_full[q], (k / kStage) & 1, abort, limit, err), kBarP2)) break;
+    if (!group_and(pipe_wait(&sm.st_full[q], (k / kStage) & 1, abort, limit, err, poll), kBarP2)) break;
     int tr, tc;
     tile_of(t, nrt, ncb, f, tr, tc);
     const TileView V(K, F, PS, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);

