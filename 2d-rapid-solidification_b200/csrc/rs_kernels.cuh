@@ -67,7 +67,7 @@ struct TmaMaps {
   int col_tab64_len;
   const SurrArgs *surr;  // learned CALPHAD surrogate, or nullptr (exact)
   FinalRed red;          // counter, offset and outputs (partials, nparts set by the launcher)
-  int pipeline;          // FP64: the persistent warp-role kernel instead of one tile per CTA
+  int pipeline;          // the persistent warp-role kernel instead of one tile per CTA
 };
 constexpr int kTileOutW = 128;                  // output columns of an FP32 tile
 constexpr int kTmaBoxW32 = kTileOutW + 8;        // input columns (4 each side keep x 16-byte aligned)

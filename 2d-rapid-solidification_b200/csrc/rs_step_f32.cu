@@ -894,6 +894,622 @@ __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
   runs[r].l += runs[r].inc_l;
 }
 
+
+// ---------------------------------------------------------------- persistent pipeline (exact FP32)
+// The exact path of tile_body split into phase functions run by warp roles of
+// persistent CTAs, as the FP64 pipeline of rs_step_f64t.cu: a producer warp
+// issuing the TMA loads of tile k+2 into a three-slot input ring, four warps
+// computing phase 1 of tile k+1 into a two-slot staging ring, four warps
+// doing phases 2-4 of tile k and its bulk stores; mbarrier hand-offs, named
+// barriers per group, every wait bounded.  Same arithmetic, expression for
+// expression, as tile_body.
+struct alignas(128) InSlot32 {
+  float psi[kTRin][kWin];
+  float d[kTRin][kWin];
+};
+struct alignas(16) StSlot32 {
+  float S[kTRin][kWin];  // after phase 2: new psi of the listed cells
+  float mu[kTRin][kWin];
+  uint8_t pmask[kTRin][32];  // per lane: bits 0-3 psi <= -1, bits 4-7 psi >= 1 of its four cells
+  uint8_t hmask[kTRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
+  uint32_t liq, sol;         // bit r: every cell of input row r has psi == -1 / +1
+};
+struct P2Smem32 {
+  uint16_t list[kTR * kW];  // interface cells: row << 8 | output column
+  int nlist;
+  int last;
+  double part_mass[kWarps];
+  int part_itip[kWarps];
+};
+constexpr int kRing = 3, kStage = 2;
+struct alignas(128) PipeSmem32 {
+  InSlot32 in[kRing];
+  StSlot32 st[kStage];
+  P2Smem32 p2;
+  uint64_t in_full[kRing], in_empty[kRing], st_full[kStage], st_empty[kStage];
+  int abort;
+};
+static_assert(sizeof(InSlot32) % 128 == 0, "ring slots stay 128-byte aligned");
+constexpr uint32_t kTileBytes32 = 2u * kTRin * kWin * sizeof(float);
+constexpr uint32_t kMinus1f = 0xBF800000u, kPlus1f = 0x3F800000u;
+constexpr int kPipeThreads = 32 + 2 * kThreads;
+enum { kBarP1 = 1, kBarP2 = 2 };
+
+__device__ __forceinline__ void gsync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ bool group_and(bool v, int id) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n barrier.red.and.pred q, %2, 128, p;\n"
+      " selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// bounded wait on an mbarrier phase; gives up (error flag, abort flag) after
+// the limit or when another role has given up
+__device__ __forceinline__ bool pipe_wait(uint64_t *bar, uint32_t parity, volatile int *abort, uint32_t limit,
+                                          int *err, bool poll) {
+  uint32_t tries = 0;
+  while (!mbar_try(bar, parity, poll)) {
+    if (*abort) return false;
+    if (++tries >= limit) {
+      atomicExch(err, 1);
+      *abort = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+// one phase group's view of a tile and of its own lane
+struct View32 {
+  const StepCoef &K;
+  const Coef<float> &F;
+  const StepScalars &PS;
+  const float *tRT, *tC0, *tDK, *tAnb, *tAti;  // column tables, indexed by column
+  int x0, y0, gw, lane, gtid, col, gi, bc;
+  uint32_t outm;
+  __device__ View32(const StepCoef &K_, const Coef<float> &F_, const StepScalars &PS_, const float *tab, int len,
+                    int x0_, int y0_, int gtid_)
+      : K(K_), F(F_), PS(PS_), tRT(tab + kTabRT * len + 4), tC0(tab + kTabC0 * len + 4),
+        tDK(tab + kTabDK * len + 4), tAnb(tab + kTabAnb * len + 4), tAti(tab + kTabAti * len + 4), x0(x0_),
+        y0(y0_), gw(gtid_ >> 5), lane(gtid_ & 31), gtid(gtid_) {
+    col = 4 * lane;
+    gi = x0 + col;
+    bc = col + 4;
+    outm = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (gi + q >= 1 && gi + q <= K.nx - 2) outm |= 1u << q;
+  }
+};
+
+__device__ __forceinline__ void fix_beyond32(const View32 &V, InSlot32 &in) {
+  if (V.x0 + kW + 4 <= V.K.nx) return;
+  for (int k = V.gtid; k < kTRin * kWin; k += kThreads) {
+    const int rr = k / kWin, x = k % kWin;
+    if (V.x0 - 4 + x >= V.K.nx) {
+      in.psi[rr][x] = -1.f;
+      in.d[rr][x] = 0.f;
+    }
+  }
+}
+
+// phase 1 of the group warp's input rows and of the halo columns (st.liq and
+// st.sol 0 on entry)
+__device__ __forceinline__ void phase1_32(const View32 &V, const InSlot32 &in, StSlot32 &st) {
+  const Coef<float> &F = V.F;
+  const int lane = V.lane, bc = V.bc;
+  const float two_cinf = F.cinf + F.cinf;
+  constexpr float KL = (float)(-2.0 * kL0Liq);
+  const float sA = 2.f * F.cinf * (1.f - F.cinf), sB = 1.f - 2.f * F.cinf;
+  const float d_hi = 0.999f * sA / (9.f - sB), d_lo = -0.999f * sA / (9.f + sB);
+  const float4 RTv = ld4(V.tRT + V.gi), C0v = ld4(V.tC0 + V.gi);
+  const float RTa[4] = {RTv.x, RTv.y, RTv.z, RTv.w}, C0a[4] = {C0v.x, C0v.y, C0v.z, C0v.w};
+  auto solid3 = [&](int rr) -> uint32_t {
+    const int xh = lane == 0 ? kHaloL : kHaloR;
+    uint32_t v = 0xFu;
+    bool hs = true;
+    for (int r2 = max(rr - 1, 0); r2 <= min(rr + 1, kTRin - 1); ++r2) {
+      const float4 q4 = ld4(&in.psi[r2][bc]);
+      v &= (__float_as_uint(q4.x) == kPlus1f ? 1u : 0u) | (__float_as_uint(q4.y) == kPlus1f ? 2u : 0u) |
+           (__float_as_uint(q4.z) == kPlus1f ? 4u : 0u) | (__float_as_uint(q4.w) == kPlus1f ? 8u : 0u);
+      hs = hs && __float_as_uint(in.psi[r2][xh]) == kPlus1f;
+    }
+    uint32_t lf = __shfl_up_sync(FULL, v >> 3, 1) & 1u, rt = __shfl_down_sync(FULL, v, 1) & 1u;
+    if (lane == 0) lf = (hs || V.x0 == 0) ? 1u : 0u;
+    if (lane == 31) rt = hs ? 1u : 0u;
+    const uint32_t e = lf | (v << 1) | (rt << 5);
+    return e & (e >> 1) & (e >> 2) & 0xFu;
+  };
+#pragma unroll 1
+  for (int rr = V.gw; rr < kTRin; rr += kWarps) {
+    if (V.y0 - 1 + rr > V.K.ny - 1) {
+      st4(&st.S[rr][bc], 0.f, 0.f, 0.f, 0.f);
+      st4(&st.mu[rr][bc], 0.f, 0.f, 0.f, 0.f);
+      st.pmask[rr][lane] = 0xFFu;
+      if (lane == 0) {
+        atomicOr(&st.liq, 1u << rr);
+        atomicOr(&st.sol, 1u << rr);
+      }
+      continue;
+    }
+    const float4 pv4 = ld4(&in.psi[rr][bc]), dv4 = ld4(&in.d[rr][bc]);
+    const float pv[4] = {pv4.x, pv4.y, pv4.z, pv4.w}, dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
+    float Sv[4], mv[4];
+    const uint32_t b0 = __float_as_uint(pv[0]), b1 = __float_as_uint(pv[1]), b2 = __float_as_uint(pv[2]),
+                   b3 = __float_as_uint(pv[3]);
+    const uint32_t band = b0 & b1 & b2 & b3, bor = b0 | b1 | b2 | b3;
+    const float dmx = fmaxf(fmaxf(dv[0], dv[1]), fmaxf(dv[2], dv[3]));
+    const float dmn = fminf(fminf(dv[0], dv[1]), fminf(dv[2], dv[3]));
+    const bool liq4 = band == kMinus1f && bor == kMinus1f;
+    uint32_t code;
+    if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
+      code = 1u;
+      st.pmask[rr][lane] = 0x0Fu;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float c = F.cinf + dv[q], om = 1.f - c;
+        const float sv = __fdividef(dv[q], fmaf(two_cinf, om, dv[q]));
+        const float s2 = sv * sv;
+        float p = fmaf(s2, 1.f / 7.f, 1.f / 5.f);
+        p = fmaf(s2, p, 1.f / 3.f);
+        const float ath = fmaf(sv * s2, p, sv);
+        Sv[q] = c * om;
+        mv[q] = fmaf(RTa[q] + RTa[q], ath, dv[q] * KL);
+      }
+    } else {
+      const bool sol4 = band == kPlus1f && bor == kPlus1f;
+      code = (__all_sync(FULL, liq4) ? 1u : 0u) | (__all_sync(FULL, sol4) ? 2u : 0u);
+      const uint32_t s3 = (code & 2u) ? solid3(rr) : 0u;
+      if ((code & 2u) && __all_sync(FULL, s3 == 0xFu)) {
+        st.pmask[rr][lane] = 0xF0u;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) Sv[q] = mv[q] = 0.f;
+      } else {
+        uint32_t L = 0u, Sm = 0u;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (pv[q] <= -1.f) L |= 1u << q;
+          if (pv[q] >= 1.f) Sm |= 1u << q;
+          cell_terms(F, pv[q], dv[q], RTa[q], C0a[q], Sv[q], mv[q]);
+        }
+        st.pmask[rr][lane] = (uint8_t)(L | (Sm << 4));
+      }
+    }
+    st4(&st.S[rr][bc], Sv[0], Sv[1], Sv[2], Sv[3]);
+    st4(&st.mu[rr][bc], mv[0], mv[1], mv[2], mv[3]);
+    if (lane == 0) {
+      if (code & 1u) atomicOr(&st.liq, 1u << rr);
+      if (code & 2u) atomicOr(&st.sol, 1u << rr);
+    }
+  }
+  if (V.gtid >= 64 && V.gtid < 64 + 2 * kTRin) {
+    const int i = V.gtid - 64;
+    const int rr = i >> 1, side = i & 1;
+    const int x = side ? kHaloR : kHaloL, g = V.x0 - 4 + x;
+    float Sh = 0.f, mh = 0.f;
+    uint8_t hm = 3u;
+    if (V.y0 - 1 + rr <= V.K.ny - 1) {
+      const float pv = in.psi[rr][x];
+      cell_terms(F, pv, in.d[rr][x], V.tRT[g], V.tC0[g], Sh, mh);
+      hm = (pv <= -1.f ? 1u : 0u) | (pv >= 1.f ? 2u : 0u);
+    }
+    st.S[rr][x] = Sh;
+    st.mu[rr][x] = mh;
+    st.hmask[rr][side] = hm;
+  }
+}
+
+// phase 2 of the group warp's output rows (nlist 0 on entry); returns the
+// listed cells, 4 bits per output row
+__device__ __forceinline__ uint32_t phase2_32(const View32 &V, const InSlot32 &in, const StSlot32 &st, P2Smem32 &p2,
+                                              float dn[kRowsPerWarp][4], double &mass, bool red) {
+  const Coef<float> &F = V.F;
+  const int lane = V.lane, bc = V.bc;
+  const float cflux4 = 0.25f * F.cflux;
+  const float floor_d = F.c_floor - F.cinf;
+  const float4 dKv = ld4(V.tDK + V.gi);
+  const float dKl = V.tDK[V.gi - 1];
+  const float dKa[5] = {dKl, dKv.x, dKv.y, dKv.z, dKv.w};
+  const uint32_t liq = st.liq, sol = st.sol;
+  struct Row {
+    float s[4], m[4], sl, sr, ml, mr, q[5];
+  };
+  auto load_row = [&](int rr, Row &R) {
+    const float4 s = ld4(&st.S[rr][bc]), m = ld4(&st.mu[rr][bc]);
+    R.s[0] = s.x; R.s[1] = s.y; R.s[2] = s.z; R.s[3] = s.w;
+    R.m[0] = m.x; R.m[1] = m.y; R.m[2] = m.z; R.m[3] = m.w;
+    R.sl = __shfl_up_sync(FULL, s.w, 1);
+    R.ml = __shfl_up_sync(FULL, m.w, 1);
+    R.sr = __shfl_down_sync(FULL, s.x, 1);
+    R.mr = __shfl_down_sync(FULL, m.x, 1);
+    if (lane == 0) {
+      R.sl = st.S[rr][kHaloL];
+      R.ml = st.mu[rr][kHaloL];
+    }
+    if (lane == 31) {
+      R.sr = st.S[rr][kHaloR];
+      R.mr = st.mu[rr][kHaloR];
+    }
+    R.q[0] = R.sl + R.s[0];
+    R.q[1] = R.s[0] + R.s[1];
+    R.q[2] = R.s[1] + R.s[2];
+    R.q[3] = R.s[2] + R.s[3];
+    R.q[4] = R.s[3] + R.sr;
+  };
+  auto vface = [&](const Row &A, const Row &B, float jv[4]) {
+    float pp[6];
+    pp[0] = A.sl + B.sl;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) pp[q + 1] = A.s[q] + B.s[q];
+    pp[5] = A.sr + B.sr;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) jv[q] = __fmul_rn(fmaf(6.f, pp[q + 1], pp[q] + pp[q + 2]), B.m[q] - A.m[q]);
+  };
+  const int rbase = 1 + kRowsPerWarp * V.gw;
+  Row ra, rb, rc;
+  float jv_lo[4], jv_hi[4];
+  uint32_t needs_all = 0u;
+  load_row(rbase - 1, ra);
+  load_row(rbase, rb);
+  vface(ra, rb, jv_lo);
+#pragma unroll
+  for (int j = 0; j < kRowsPerWarp; ++j) {
+    const int rr = rbase + j;
+    load_row(rr + 1, rc);
+    vface(rb, rc, jv_hi);
+    const float mm[6] = {rb.ml, rb.m[0], rb.m[1], rb.m[2], rb.m[3], rb.mr};
+    float jh[5];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) jh[f] = __fmul_rn(fmaf(6.f, rb.q[f], ra.q[f] + rc.q[f]), mm[f + 1] - mm[f] + dKa[f]);
+    const float4 dv4 = ld4(&in.d[rr][bc]);
+    const float dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      dn[j][q] = fmaxf(fmaf(cflux4, (jh[q + 1] - jh[q]) + (jv_hi[q] - jv_lo[q]), dv[q]), floor_d);
+    const bool live = V.y0 - 1 + rr <= V.K.ny - 2;
+    if (red && live) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if ((V.outm >> q) & 1u) mass += (double)dn[j][q];
+    }
+    const uint32_t w3 = 7u << (rr - 1);
+    if (live && (liq & w3) != w3 && (sol & w3) != w3) {
+      const uint32_t pk = (uint32_t)st.pmask[rr - 1][lane] | ((uint32_t)st.pmask[rr][lane] << 8) |
+                          ((uint32_t)st.pmask[rr + 1][lane] << 16);
+      uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
+      if (lane == 0) {
+        lf = 0u;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t h = st.hmask[rr - 1 + k][0];
+          lf |= ((h & 1u) << (8 * k + 3)) | (((h >> 1) & 1u) << (8 * k + 7));
+        }
+      }
+      if (lane == 31) {
+        rt = 0u;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t h = st.hmask[rr - 1 + k][1];
+          rt |= ((h & 1u) << (8 * k)) | (((h >> 1) & 1u) << (8 * k + 4));
+        }
+      }
+      uint32_t Lv = 0x3Fu, Sv = 0x3Fu;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t L = (pk >> (8 * k)) & 0xFu, S = (pk >> (8 * k + 4)) & 0xFu;
+        Lv &= (L << 1) | ((lf >> (8 * k + 3)) & 1u) | (((rt >> (8 * k)) & 1u) << 5);
+        Sv &= (S << 1) | ((lf >> (8 * k + 7)) & 1u) | (((rt >> (8 * k + 4)) & 1u) << 5);
+      }
+      const uint32_t needs = ~((Lv & (Lv >> 1) & (Lv >> 2)) | (Sv & (Sv >> 1) & (Sv >> 2))) & V.outm;
+      const uint32_t cnt = __popc(needs);
+      uint32_t incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const uint32_t total = __shfl_sync(FULL, incl, 31);
+      int base = 0;
+      if (lane == 31 && total) base = atomicAdd(&p2.nlist, (int)total);
+      base = __shfl_sync(FULL, base, 31);
+      uint32_t off = (uint32_t)base + incl - cnt;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if ((needs >> q) & 1u) p2.list[off++] = (uint16_t)((rr << 8) | (V.col + q));
+      needs_all |= needs << (4 * j);
+    }
+    ra = rb;
+    rb = rc;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) jv_lo[q] = jv_hi[q];
+  }
+  return needs_all;
+}
+
+// phase 3: listed interface cells, one per group thread; new psi into np
+__device__ __forceinline__ void phase3_32(const View32 &V, const InSlot32 &in, const P2Smem32 &p2,
+                                          float (*np)[kWin], bool red, int &itip) {
+  const int nlist = p2.nlist;
+  for (int idx = V.gtid; idx < nlist; idx += kThreads) {
+    const uint32_t e = p2.list[idx];
+    const int rr = (int)(e >> 8), x = (int)(e & 0xFFu) + 4;
+    const int r = V.y0 - 1 + rr, g = V.x0 + x - 4;
+    const float c00 = V.F.cinf + in.d[rr][x];
+    const float dG = (1.f - c00) * V.tAnb[g] + c00 * V.tAti[g] + c00 * (1.f - c00) * (float)(kL0Liq - kL0Bcc);
+    const float res = phi_cell_dG<float>(
+        &V.F, clamp1(in.psi[rr][x]), clamp1(in.psi[rr][x + 1]), clamp1(in.psi[rr][x - 1]),
+        clamp1(in.psi[rr + 1][x]), clamp1(in.psi[rr - 1][x]), clamp1(in.psi[rr + 1][x + 1]),
+        clamp1(in.psi[rr + 1][x - 1]), clamp1(in.psi[rr - 1][x + 1]), clamp1(in.psi[rr - 1][x - 1]), dG,
+        V.PS.step, (int64_t)(r + V.K.j_offset) * V.K.nx + g, V.K.seed_lo, V.K.seed_hi);
+    np[rr][x] = res;
+    if (red && res > 0.f) itip = max(itip, g == V.K.nx - 2 ? V.K.nx - 1 : g);
+  }
+}
+
+// phase 4: new psi and c of the group warp's rows into the input tile
+__device__ __forceinline__ void phase4_32(const View32 &V, InSlot32 &in, const float (*np)[kWin], uint32_t needs_all,
+                                          const float dn[kRowsPerWarp][4], bool red, int &itip) {
+  const int rbase = 1 + kRowsPerWarp * V.gw, bc = V.bc;
+#pragma unroll
+  for (int j = 0; j < kRowsPerWarp; ++j) {
+    const int rr = rbase + j;
+    const float4 pv4 = ld4(&in.psi[rr][bc]);
+    const float pv[4] = {pv4.x, pv4.y, pv4.z, pv4.w};
+    const bool live = V.y0 - 1 + rr <= V.K.ny - 2;
+    float po[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const bool listed = (needs_all >> (4 * j + q)) & 1u;
+      po[q] = listed ? np[rr][bc + q] : clamp1(pv[q]);
+      if (red && live && !listed && ((V.outm >> q) & 1u) && po[q] > 0.f)
+        itip = max(itip, V.gi + q == V.K.nx - 2 ? V.K.nx - 1 : V.gi + q);
+    }
+    st4(&in.psi[rr][bc], po[0], po[1], po[2], po[3]);
+    st4(&in.d[rr][bc], dn[j][0], dn[j][1], dn[j][2], dn[j][3]);
+  }
+}
+
+// ghost columns, bulk copies of the rows (group threads < 64) and phi;
+// returns whether this thread committed a bulk group
+__device__ __forceinline__ bool store_tile32(const View32 &V, InSlot32 &in, float *__restrict__ psi_n,
+                                             float *__restrict__ c_n, float *__restrict__ phi_n, int bar) {
+  const StepCoef &K = V.K;
+  const int x0 = V.x0, y0 = V.y0;
+  const int nrow = min(kTR, K.ny - 1 - y0);
+  const int ncol = min(kW, K.nx - x0);
+  if (x0 == 0 || x0 + kW >= K.nx) {
+    gsync(bar);
+    if (V.gtid < nrow) {
+      const int rr = 1 + V.gtid;
+      if (x0 == 0) {
+        in.psi[rr][4] = in.psi[rr][5];
+        in.d[rr][4] = in.d[rr][5];
+      }
+      if (x0 + kW >= K.nx) {
+        const int x = K.nx - 1 - x0 + 4;
+        in.psi[rr][x] = in.psi[rr][x - 1];
+        in.d[rr][x] = in.d[rr][x - 1];
+      }
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  gsync(bar);
+  bool any = false;
+  if (V.gtid < 4 * kTR) {
+    const int j = V.gtid >> 2, field = V.gtid & 1, kind = (V.gtid >> 1) & 1;
+    const int r = y0 + j;
+    if (j < nrow) {
+      float *fo = field ? c_n : psi_n;
+      const float *src = field ? &in.d[1 + j][4] : &in.psi[1 + j][4];
+      const uint32_t bytes = (uint32_t)ncol * 4u;
+      if (kind == 0) {
+        bulk_store(fo + (int64_t)r * K.pitch + x0, src, bytes);
+        any = true;
+      } else {
+        if (r == K.jmin) {
+          bulk_store(fo + x0, src, bytes);
+          any = true;
+        }
+        if (r == K.jmax) {
+          bulk_store(fo + (int64_t)(K.ny - 1) * K.pitch + x0, src, bytes);
+          any = true;
+        }
+      }
+      if (any) asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+  }
+  if (phi_n) {
+    for (int k = V.gtid; k < nrow * ncol; k += kThreads) {
+      const int j = k / ncol, x = k % ncol, r = y0 + j;
+      const float v = clamp1(in.psi[1 + j][4 + x]);
+      phi_n[(int64_t)r * K.pitch + x0 + x] = v;
+      if (r == K.jmin) phi_n[x0 + x] = v;
+      if (r == K.jmax) phi_n[(int64_t)(K.ny - 1) * K.pitch + x0 + x] = v;
+    }
+  }
+  return any;
+}
+
+// the tile's partial sums and the fused final reduction (scratch of at least
+// 256 doubles and 256 ints)
+__device__ __forceinline__ void finish32(const View32 &V, P2Smem32 &p2, double mass, int itip, BlockPartial *part,
+                                         const FinalRed *FR, double *sm_m, int *sm_i, int bar) {
+  if (!part) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mass += __shfl_down_sync(FULL, mass, o);
+  itip = __reduce_max_sync(FULL, itip);
+  if (V.lane == 0) {
+    p2.part_mass[V.gw] = mass;
+    p2.part_itip[V.gw] = itip;
+  }
+  gsync(bar);
+  if (V.gtid == 0) {
+    BlockPartial b;
+    b.mass = 0.0;
+    b.itip = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      b.mass += p2.part_mass[w];
+      b.itip = max(b.itip, p2.part_itip[w]);
+    }
+    b.pad = 0;
+    *part = b;
+  }
+  if (!FR) return;
+  if (V.gtid == 0) {
+    __threadfence();
+    p2.last = atomicAdd(FR->counter, 1u) == (unsigned)(FR->nparts - 1);
+  }
+  gsync(bar);
+  if (!p2.last) return;
+  __threadfence();
+  for (int v = V.gtid; v < 256; v += kThreads) {
+    double m = 0.0;
+    int it = 0;
+    for (int k = v; k < FR->nparts; k += 256) {
+      m += __ldcg(&FR->partials[k].mass);
+      it = max(it, __ldcg(&FR->partials[k].itip));
+    }
+    sm_m[v] = m;
+    sm_i[v] = it;
+  }
+  gsync(bar);
+  for (int sz = 128; sz > 0; sz >>= 1) {
+    for (int v = V.gtid; v < sz; v += kThreads) {
+      sm_m[v] += sm_m[v + sz];
+      sm_i[v] = max(sm_i[v], sm_i[v + sz]);
+    }
+    gsync(bar);
+  }
+  if (V.gtid == 0) {
+    if (FR->mass_out) *FR->mass_out = sm_m[0] + FR->mass_offset;
+    if (FR->itip_out) *FR->itip_out = max(1, sm_i[0]);
+    *FR->counter = 0u;
+  }
+}
+
+__device__ __forceinline__ void tile_of32(int t, int nrt, int ncb, int f, int &tr, int &tc) {
+  tr = t % nrt;
+  tc = front_first_block(t / nrt, f, ncb);
+}
+
+__global__ void __launch_bounds__(kPipeThreads, 2)
+    pipe_kernel_f32(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<float> F,
+                    const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
+                    const __grid_constant__ CUtensorMap tm_c, const float *__restrict__ tab, const int tab_len,
+                    float *__restrict__ psi_n, float *__restrict__ c_n, float *__restrict__ phi_n,
+                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int nrt,
+                    const int ncb) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  PipeSmem32 &sm = *reinterpret_cast<PipeSmem32 *>(smem_raw);
+  const int warp = threadIdx.x >> 5;
+  const int ntiles = nrt * ncb;
+  const int f = max(PS.i_front, 0) / kW;
+  const FinalRed *FRp = partials && FR.counter ? &FR : nullptr;
+  const uint32_t limit = PS.wait_limit ? PS.wait_limit : kWaitLimit;
+  const bool poll = PS.wait_limit != 0;
+  volatile int *abort = &sm.abort;
+  if (smem_u32(smem_raw) & 127u) {
+    if (threadIdx.x == 0) atomicExch(err, 2);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kRing; ++s) {
+      mbar_init(&sm.in_full[s], 1);
+      mbar_init(&sm.in_empty[s], 1);
+    }
+    for (int s = 0; s < kStage; ++s) {
+      mbar_init(&sm.st_full[s], 1);
+      mbar_init(&sm.st_empty[s], 1);
+    }
+    sm.abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  __syncthreads();
+
+  if (warp == 0) {  // producer
+    if ((threadIdx.x & 31) == 0) {
+      int k = 0;
+      for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+        const int s = k % kRing;
+        if (k >= kRing && !pipe_wait(&sm.in_empty[s], ((k / kRing) - 1) & 1, abort, limit, err, poll)) break;
+        int tr, tc;
+        tile_of32(t, nrt, ncb, f, tr, tc);
+        mbar_expect_tx(&sm.in_full[s], kTileBytes32);
+        tma_load_2d(&sm.in[s].psi[0][0], &tm_psi, &sm.in_full[s], kW * tc - 4, kTR * tr);
+        tma_load_2d(&sm.in[s].d[0][0], &tm_c, &sm.in_full[s], kW * tc - 4, kTR * tr);
+      }
+      // only the last kRing loads can still be in flight: they land before the CTA exits
+      for (int q = max(k - kRing, 0); q < k; ++q)
+        for (uint32_t tt = 0; tt < kWaitLimit && !mbar_try_wait(&sm.in_full[q % kRing], (q / kRing) & 1); ++tt) {
+        }
+    }
+    return;
+  }
+  if (warp <= kWarps) {  // phase 1
+    const int gtid = (int)threadIdx.x - 32;
+    int k = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+      const int s = k % kRing, q = k % kStage;
+      bool ok = pipe_wait(&sm.in_full[s], (k / kRing) & 1, abort, limit, err, poll);
+      if (ok && k >= kStage) ok = pipe_wait(&sm.st_empty[q], ((k / kStage) - 1) & 1, abort, limit, err, poll);
+      if (!group_and(ok, kBarP1)) break;
+      int tr, tc;
+      tile_of32(t, nrt, ncb, f, tr, tc);
+      const View32 V(K, F, PS, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
+      if (gtid == 0) {
+        sm.st[q].liq = 0u;
+        sm.st[q].sol = 0u;
+      }
+      fix_beyond32(V, sm.in[s]);
+      gsync(kBarP1);
+      phase1_32(V, sm.in[s], sm.st[q]);
+      gsync(kBarP1);
+      if (gtid == 0) mbar_arrive(&sm.st_full[q]);
+    }
+    return;
+  }
+  // phases 2-4
+  const int gtid = (int)threadIdx.x - 32 - kThreads;
+  int k = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+    const int s = k % kRing, q = k % kStage;
+    if (!group_and(pipe_wait(&sm.st_full[q], (k / kStage) & 1, abort, limit, err, poll), kBarP2)) break;
+    int tr, tc;
+    tile_of32(t, nrt, ncb, f, tr, tc);
+    const View32 V(K, F, PS, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
+    BlockPartial *part = partials ? partials + ((int64_t)tc * nrt + tr) : nullptr;
+    const bool red = part != nullptr;
+    if (gtid == 0) sm.p2.nlist = 0;
+    gsync(kBarP2);
+    double mass = 0.0;
+    int itip = 0;
+    float dn[kRowsPerWarp][4];
+    const uint32_t needs_all = phase2_32(V, sm.in[s], sm.st[q], sm.p2, dn, mass, red);
+    gsync(kBarP2);
+    phase3_32(V, sm.in[s], sm.p2, sm.st[q].S, red, itip);
+    gsync(kBarP2);
+    phase4_32(V, sm.in[s], sm.st[q].S, needs_all, dn, red, itip);
+    const bool issued = store_tile32(V, sm.in[s], psi_n, c_n, phi_n, kBarP2);
+    finish32(V, sm.p2, mass, itip, part, FRp, reinterpret_cast<double *>(&sm.st[q].mu[0][0]),
+             reinterpret_cast<int *>(&sm.st[q].mu[8][0]), kBarP2);
+    if (issued) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    gsync(kBarP2);
+    if (gtid == 0) {
+      mbar_arrive(&sm.st_empty[q]);
+      mbar_arrive(&sm.in_empty[s]);
+    }
+  }
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
 }  // namespace
 
 int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
@@ -922,8 +1538,39 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   const int nparts = grid.x * grid.y;
   if (partials && nparts > max_partials) return -1;
   if (tm.col_tab_len < (int)grid.y * kW + kWin) return -1;
-  const size_t smem = sizeof(TileSmem);
   const bool surr = tm.surr != nullptr;
+  if (tm.pipeline && !surr) {  // the persistent warp-role kernel (exact path)
+    const int nrt = (int)grid.x, ncb = (int)grid.y;
+    const size_t psmem = sizeof(PipeSmem32);
+    static std::atomic<unsigned long long> pattr{0};
+    if (!smem_limit_once((const void *)pipe_kernel_f32, (int)psmem, pattr)) return -3;
+    static std::atomic<int> president[64];
+    const int res = resident_ctas((const void *)pipe_kernel_f32, kPipeThreads, psmem, president);
+    if (res <= 0) return -3;
+    column_table_kernel<<<(tm.col_tab_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(
+        K, P.d0, P.d1, tm.col_tab_len, tm.col_tab);
+    cudaLaunchConfig_t pc = {};
+    pc.gridDim = dim3((unsigned)std::min(res, nparts));
+    pc.blockDim = dim3(kPipeThreads);
+    pc.dynamicSmemBytes = psmem;
+    pc.stream = st;
+    cudaLaunchAttribute pa[1];
+    pa[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    pa[0].val.programmaticStreamSerializationAllowed = 1;
+    pc.attrs = pa;
+    pc.numAttrs = 1;
+    FinalRed pfr = tm.red;
+    pfr.partials = partials;
+    pfr.nparts = nparts;
+    if (!partials || !(pfr.mass_out || pfr.itip_out)) pfr.counter = nullptr;
+    const float *ptab = tm.col_tab;
+    if (cudaLaunchKernelEx(&pc, pipe_kernel_f32, K, F, P, tm.psi, tm.c, ptab, tm.col_tab_len, psi_n, c_n, phi_n,
+                           partials, err, pfr, nrt, ncb) != cudaSuccess)
+      return -3;
+    if (nparts_out) *nparts_out = nparts;
+    return 0;
+  }
+  const size_t smem = sizeof(TileSmem);
   auto kfn = surr ? tile_kernel<true> : tile_kernel<false>;
   static std::atomic<unsigned long long> attr_done[2];
   if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr])) return -3;

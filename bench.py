@@ -49,8 +49,8 @@ WORKLOAD = ("Ti-10Nb directional solidification 2048x2048, exact CALPHAD, frozen
 # mass reduction is fused into that kernel)
 STEP_PATH = {"f32": ("rs::tile_kernel<false>", 2, True),
              "f64": ("rs::tile_kernel_f64", 2, True)}
-# the FP64 step's kernel of the headline: 0 one tile per CTA, 1 the
-# persistent warp-role pipeline (the other one is timed as a side leg)
+# the tile steps' kernel (RS_OPT_PIPELINE): 0 one tile per CTA, 1 the
+# persistent warp-role pipeline (the other one is timed beside it)
 PIPELINE = 0
 
 
@@ -269,8 +269,8 @@ def e2e_interval(loop, nsteps, dist, world, st):
 
 def kernel_name(prec, options):
     from rapidsolid import _abi
-    if prec == "f64" and (options or {}).get(_abi.RS_OPT_PIPELINE, 0):
-        return "rs::pipe_kernel_f64"
+    if (options or {}).get(_abi.RS_OPT_PIPELINE, 0):
+        return f"rs::pipe_kernel_{prec}"
     return STEP_PATH[prec][0]
 
 
@@ -366,7 +366,11 @@ def run_ours(args):
         alt.pop("clocks")
         line["fp64_other_kernel"] = {"pipeline": 1 - PIPELINE, "value": alt["value"],
                                      "ms_per_step": alt["ms_per_step"], "roofline": alt["roofline"]}
-        fp32 = run_arm(p, torch.float32, args, flush, st, None, 1)
+        fp32 = run_arm(p, torch.float32, args, flush, st, None, 1, options={_abi.RS_OPT_PIPELINE: PIPELINE})
+        alt32 = run_arm(p, torch.float32, args, flush, st, None, 1, options={_abi.RS_OPT_PIPELINE: 1 - PIPELINE},
+                        e2e=False)
+        fp32["other_kernel"] = {"pipeline": 1 - PIPELINE, "value": alt32["value"],
+                                "ms_per_step": alt32["ms_per_step"], "roofline": alt32["roofline"]}
         fp32.pop("clocks")
         line["fp32_exact"] = fp32
         line["fp32_exact_vs_fp64_exact"] = round(fp32["value"] / head["value"], 3)

@@ -187,10 +187,11 @@ int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
  * polls without suspending and gives up after that many polls.  A tile whose
  * wait gives up is not computed or stored, and rs_device_status reports
  * RS_E_STATE.  Tests set it to 1 to run that path.
- * RS_OPT_PIPELINE (default 0) runs the FP64 tile step as a persistent kernel
- * of warp roles (a TMA producer warp, a phase-1 group and a flux/update/store
- * group working on three tiles at once) instead of one tile per CTA; both
- * give the same fields bit for bit. */
+ * RS_OPT_PIPELINE (default 0) runs the tile step (FP64, and FP32 without a
+ * surrogate) as a persistent kernel of warp roles (a TMA producer warp, a
+ * phase-1 group and a flux/update/store group working on three tiles at
+ * once) instead of one tile per CTA; both give the same fields bit for
+ * bit. */
 #define RS_OPT_TMA 1
 #define RS_OPT_WAIT_LIMIT 2
 #define RS_OPT_PIPELINE 3

@@ -271,12 +271,14 @@ def test_f64_step_with_deep_solid_matches_oracle(tma):
     assert np.array_equal(g.c[deep], s.c[deep]) and np.array_equal(g.psi[deep], s.psi[deep])
 
 
-@pytest.mark.parametrize("shape", [(64, 48), (300, 130), (1030, 1038)])
-def test_f64_pipeline_kernel_equals_tile_kernel(shape):
-    """The persistent warp-role FP64 kernel (RS_OPT_PIPELINE) runs the same
-    phase functions as the one-tile-per-CTA kernel: fields and the fused
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("shape", [(64, 48), (300, 130), (1032, 1038)])
+def test_pipeline_kernel_equals_tile_kernel(shape, dtype):
+    """The persistent warp-role kernels (RS_OPT_PIPELINE) run the same
+    per-cell arithmetic as the one-tile-per-CTA kernels: fields and the fused
     solute mass and coarse tip bit for bit, over 30 steps with noise, on grids
-    whose tiles do not divide them (1030 x 1038: several tiles per CTA)."""
+    whose tiles do not divide them (1032 x 1038: several tiles per CTA)."""
+    dt = torch.float64 if dtype == "f64" else torch.float32
     p = configs.small(*shape, i_tip_target=22, G=5e6, V=0.5, noise_amplitude=0.05, seed=7)
     d = pyoracle.derive(p)
     s = perturbed_state(p, 3, amp=0.3)
@@ -284,7 +286,7 @@ def test_f64_pipeline_kernel_equals_tile_kernel(shape):
     for pipe in (0, 1):
         ctx = lib.Context(p)
         ctx.set_option(_abi.RS_OPT_PIPELINE, pipe)
-        a, b = upload(p, s, with_phi=True), lib.FieldSet(p, torch.float64, with_phi=True)
+        a, b = upload(p, s, dt, with_phi=True), lib.FieldSet(p, dt, with_phi=True)
         m = torch.zeros(30, dtype=torch.float64, device="cuda")
         it = torch.zeros(30, dtype=torch.int32, device="cuda")
         l = 0.0

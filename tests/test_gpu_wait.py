@@ -17,14 +17,14 @@ pytestmark = pytest.mark.gpu
 SENTINEL = 7.0
 
 
-@pytest.mark.parametrize("dtype", ["f32", "f64", "f64_pipeline"])
+@pytest.mark.parametrize("dtype", ["f32", "f64", "f32_pipeline", "f64_pipeline"])
 def test_wait_that_gives_up_skips_the_tile(dtype):
-    dt = torch.float32 if dtype == "f32" else torch.float64
+    dt = torch.float32 if dtype.startswith("f32") else torch.float64
     p = configs.small(256, 130, i_tip_target=40, G=5e6, V=0.5)
     d = pyoracle.derive(p)
     s = perturbed_state(p, 5, amp=0.2)
     ctx = lib.Context(p)
-    ctx.set_option(_abi.RS_OPT_PIPELINE, 1 if dtype == "f64_pipeline" else 0)
+    ctx.set_option(_abi.RS_OPT_PIPELINE, 1 if dtype.endswith("pipeline") else 0)
     cur = upload(p, s, dt)
     nxt = lib.FieldSet(p, dt)
     nxt.psi.fill_(SENTINEL)
