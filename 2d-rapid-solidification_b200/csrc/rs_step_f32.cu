@@ -903,9 +903,9 @@ __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
 // doing phases 2-4 of tile k and its bulk stores; mbarrier hand-offs, named
 // barriers per group, every wait bounded.  Same arithmetic, expression for
 // expression, as tile_body.
-struct alignas(128) InSlot32 {
-  float psi[kTRin][kWin];
-  float d[kTRin][kWin];
+struct alignas(128) InSlot32 {  // both arrays are TMA destinations: 128-byte aligned
+  alignas(128) float psi[kTRin][kWin];
+  alignas(128) float d[kTRin][kWin];
 };
 struct alignas(16) StSlot32 {
   float S[kTRin][kWin];  // after phase 2: new psi of the listed cells
@@ -929,7 +929,9 @@ struct alignas(128) PipeSmem32 {
   uint64_t in_full[kRing], in_empty[kRing], st_full[kStage], st_empty[kStage];
   int abort;
 };
-static_assert(sizeof(InSlot32) % 128 == 0, "ring slots stay 128-byte aligned");
+static_assert(sizeof(InSlot32) % 128 == 0 && offsetof(InSlot32, psi) % 128 == 0 && offsetof(InSlot32, d) % 128 == 0,
+              "ring slots and their TMA destinations stay 128-byte aligned");
+static_assert(offsetof(PipeSmem32, in) % 128 == 0, "the ring starts on a 128-byte boundary");
 constexpr uint32_t kTileBytes32 = 2u * kTRin * kWin * sizeof(float);
 constexpr uint32_t kMinus1f = 0xBF800000u, kPlus1f = 0x3F800000u;
 constexpr int kPipeThreads = 32 + 2 * kThreads;

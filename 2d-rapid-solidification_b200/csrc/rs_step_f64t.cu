@@ -90,9 +90,9 @@ enum { kTabRT = 0, kTabC0 = 1, kTabDK = 2, kTabAnb = 3, kTabAti = 4 };
 
 // the input tile: TMA destinations (128-byte aligned); after phase 3 rows
 // 1..16 receive the new psi / c for the bulk stores
-struct alignas(128) InSlot {
-  double psi[kTRin][kWin];
-  double c[kTRin][kWin];
+struct alignas(128) InSlot {  // both arrays are TMA destinations: 128-byte aligned
+  alignas(128) double psi[kTRin][kWin];
+  alignas(128) double c[kTRin][kWin];
 };
 // phase 1 -> phases 2-4: per-cell terms and row flags
 struct alignas(16) StSlot {
@@ -124,7 +124,10 @@ struct alignas(128) PipeSmem64 {
   uint64_t in_full[kRing], in_empty[kRing], st_full[kStage], st_empty[kStage];
   int abort;  // a wait gave up: every role stops
 };
-static_assert(sizeof(InSlot) % 128 == 0, "ring slots stay 128-byte aligned");
+static_assert(sizeof(InSlot) % 128 == 0 && offsetof(InSlot, psi) % 128 == 0 && offsetof(InSlot, c) % 128 == 0,
+              "ring slots and their TMA destinations stay 128-byte aligned");
+static_assert(offsetof(PipeSmem64, in) % 128 == 0 && offsetof(TileSmem64, in) % 128 == 0,
+              "the input slots start on 128-byte boundaries");
 static_assert((kWin * sizeof(double)) % 16 == 0, "rows stay 16-byte aligned for double2 and bulk copies");
 
 __device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
