@@ -6,7 +6,8 @@ import numpy as np
 import pytest
 
 import pyoracle
-from helpers import TFC_CASES, golden, maxabs, perturbed_state, tfc_input, tfc_params, tfc_T_mask
+from helpers import TFC_CASES, golden, maxabs, perturbed_state, tfc_input, tfc_T_mask
+from helpers import tfc_params as ref_tfc_params
 from rapidsolid import _abi, configs, lib
 from test_gpu_step import download, upload
 
@@ -306,7 +307,7 @@ def test_tfc_loop_matches_reference_kernels(name):
     5e-9, c within 1e-10, the coarse T within 1e-8 K."""
     z = golden(name + ".npz")
     nx, ny, nsteps, spb = TFC_CASES[name]
-    p = tfc_params(nx, ny, spb)
+    p = ref_tfc_params(nx, ny, spb)
     d = pyoracle.derive(p)
     g, T, _ = _gpu_tfc_loop(p, d, tfc_input(p), torch.float64, nsteps)
     T = T.reshape(d.NyT_all, d.NxT_all)
