@@ -274,14 +274,18 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     in[2] = clamp1(sm.psi[rr][b]);
   };
   // store the surrogate mu'' of one cell, or keep the exact value already in
-  // place (out-of-box and audited cells); audited cells record the errors
+  // place (out-of-box and audited cells); audited cells record the errors.
+  // The network gives mu'' less its ideal-mixing part RT lam(c), which is
+  // added here exactly (the same lam as the exact form)
   auto net_store = [&](int rr, int b, const float in[3], const float o[2]) {
     const int gx = x0 + b - 4;
-    const float T = SA.T_mid + in[0] / SA.T_ihalf, c = F.cinf + sm.d[rr][b];
+    const float dv = sm.d[rr][b];
+    const float T = SA.T_mid + in[0] / SA.T_ihalf, c = F.cinf + dv;
     const bool inbox = T >= SA.T_lo && T <= SA.T_hi && c >= SA.c_lo && c <= SA.c_hi;
     const bool real = gx >= 0 && gx <= K.nx - 1;
     const bool audit = real && surr_audit_cell(PS.step, (int64_t)(y0 - 1 + rr + K.j_offset) * K.nx + gx);
-    const float mu_net = fmaf(o[0], SA.y_scale[0], SA.y_mean[0]);
+    const float mu_net =
+        fmaf(o[0], SA.y_scale[0], SA.y_mean[0]) + tRT[gx] * Tr<float>::lam(c, 1.f - c, dv, F.cinf, F.Lref);
     if (inbox && !audit) {
       sm.mu[rr][b] = mu_net;
     } else if (real) {

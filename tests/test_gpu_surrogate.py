@@ -11,8 +11,10 @@ pytestmark = pytest.mark.gpu
 
 
 def exact_targets(p, box, x):
-    """mu'' = mu(T, c, phi) - Glc(T, cinf) and dG = Gl - Gs from the host build
-    of the reference evaluator (fun.cu:1671-1720)."""
+    """mu'' = mu(T, c, phi) - Glc(T, cinf) less its ideal-mixing part
+    RT [log(c/(1-c)) - log(cinf/(1-cinf))] (which the step adds exactly), and
+    dG = Gl - Gs, from the host build of the reference evaluator
+    (fun.cu:1671-1720)."""
     x = x.astype(np.float64)
     T = box.T_lo + (box.T_hi - box.T_lo) * (x[:, 0] + 1.0) / 2.0
     c = box.c_lo + (box.c_hi - box.c_lo) * (x[:, 1] + 1.0) / 2.0
@@ -21,7 +23,8 @@ def exact_targets(p, box, x):
     Glc, Gsc = lib.calphad_eval(2, T, c), lib.calphad_eval(3, T, c)
     mu = 0.5 * (1 + g) * Gsc + 0.5 * (1 - g) * Glc
     ref = lib.calphad_eval(2, T, np.full_like(T, p.cinf))
-    return np.stack([mu - ref, lib.calphad_eval(0, T, c) - lib.calphad_eval(1, T, c)], axis=1)
+    lam = np.log(c / (1 - c)) - np.log(p.cinf / (1 - p.cinf))
+    return np.stack([mu - ref - p.RR * T * lam, lib.calphad_eval(0, T, c) - lib.calphad_eval(1, T, c)], axis=1)
 
 
 def test_samples_are_exact_targets():
