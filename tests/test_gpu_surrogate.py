@@ -11,20 +11,20 @@ pytestmark = pytest.mark.gpu
 
 
 def exact_targets(p, box, x):
-    """mu'' = mu(T, c, phi) - Glc(T, cinf) less its ideal-mixing part
-    RT [log(c/(1-c)) - log(cinf/(1-cinf))] (which the step adds exactly), and
+    """Q = C0(T) + (L0_BCC - L0_Liq)(c - cinf), the CALPHAD part of mu'' (the
+    step applies g(phi) and the ideal-mixing term exactly), and
     dG = Gl - Gs, from the host build of the reference evaluator
-    (fun.cu:1671-1720)."""
+    (fun.cu:1671-1720): at c = 1/2 the log and L0 terms of Gsc, Glc vanish, so
+    they give dGs = G_Ti_BCC - G_Nb_BCC and dGl = G_Ti_Liq - G_Nb_Liq."""
     x = x.astype(np.float64)
     T = box.T_lo + (box.T_hi - box.T_lo) * (x[:, 0] + 1.0) / 2.0
     c = box.c_lo + (box.c_hi - box.c_lo) * (x[:, 1] + 1.0) / 2.0
-    phi = x[:, 2]
-    g = phi * (1.875 + phi * phi * (-1.25 + 0.375 * phi * phi))
-    Glc, Gsc = lib.calphad_eval(2, T, c), lib.calphad_eval(3, T, c)
-    mu = 0.5 * (1 + g) * Gsc + 0.5 * (1 - g) * Glc
-    ref = lib.calphad_eval(2, T, np.full_like(T, p.cinf))
-    lam = np.log(c / (1 - c)) - np.log(p.cinf / (1 - p.cinf))
-    return np.stack([mu - ref - p.RR * T * lam, lib.calphad_eval(0, T, c) - lib.calphad_eval(1, T, c)], axis=1)
+    half = np.full_like(T, 0.5)
+    dGs, dGl = lib.calphad_eval(3, T, half), lib.calphad_eval(2, T, half)
+    L0b, L0l = 12315.25, 5144.29
+    C0 = -0.5 * (dGs - dGl) - 0.5 * (L0b - L0l) * (1 - 2 * p.cinf)
+    Q = C0 + (L0b - L0l) * (c - p.cinf)
+    return np.stack([Q, lib.calphad_eval(0, T, c) - lib.calphad_eval(1, T, c)], axis=1)
 
 
 def test_samples_are_exact_targets():
