@@ -1,15 +1,12 @@
 // rs_mlp.cu — the learned stand-in for the per-cell CALPHAD evaluation:
 // training data from the exact evaluator, forward/backward and Adam kernels.
 //
-// Network: (T, c, phi) -> (Q, dG), 3 -> 32 -> 32 -> 2, SiLU, inputs scaled
-// to [-1, 1] over the training box, outputs scaled by the box's mean/scale.
-// mu'' is the chemical potential relative to the melt's column value used by
-// the FP32 tile kernel (rs_step_f32.cu),
-//   mu'' = -(g+1) C0(T) - delta (L0_BCC + L0_Liq + g (L0_BCC - L0_Liq)) + RT lam(c)
-//        = RT lam(c) - 2 L0_Liq delta - (1 + g) Q,  Q = C0(T) + (L0_BCC - L0_Liq) delta,
-// of which the network gives Q (the temperature-dependent CALPHAD part) and
-// the step the rest exactly;
-// dG = Gl - Gs = (1-c) A_Nb + c A_Ti + c (1-c) (L0_Liq - L0_BCC)
+// Network: (T, c, phi) -> (mu'', dG), 3 -> 32 -> 32 -> 2, SiLU, inputs scaled
+// to [-1, 1] over the training box, outputs scaled by the box's
+// mean/scale.  mu'' is the chemical potential relative to the melt's column
+// value used by the FP32 tile kernel (rs_step_f32.cu),
+//   mu'' = -(g+1) C0(T) - delta (L0_BCC + L0_Liq + g (L0_BCC - L0_Liq)) + RT lam(c),
+// and dG = Gl - Gs = (1-c) A_Nb + c A_Ti + c (1-c) (L0_Liq - L0_BCC)
 // (fun.cu:1671-1720 regrouped, rs_common.cuh).  Targets are evaluated in FP64
 // with the same device functions as the exact kernels.
 //
@@ -27,18 +24,13 @@ namespace {
 constexpr int kGradThreads = 128;
 constexpr int kGradCtas = 8;  // CTAs of the one gradient cluster (portable size)
 
-// The network's first output: Q = C0(T) + (L0_BCC - L0_Liq) (c - cinf), the
-// CALPHAD part of
-//   mu'' = RT lam(c) - 2 L0_Liq (c - cinf) - (1 + g(phi)) Q,
-// lam = log(c/(1-c)) - log(cinf/(1-cinf)); the step applies the rest
-// exactly.  The (1 + g) factor makes mu'' exact at phi = -1, where network
-// cells border the bulk-melt cells of the exact series form: a network
-// error there would put a spurious solute flux on that seam.
-__device__ __forceinline__ double mu2_network_part(double T, double c, double cinf, double RR) {
+__device__ __forceinline__ double mu2_exact(double T, double c, double phi, double cinf, double RR) {
   const TTerms tt = t_terms(T, RR);
   const double D = 0.5 * (tt.dGs - tt.dGl);
   const double C0 = -D - 0.5 * (kL0Bcc - kL0Liq) * (1.0 - 2.0 * cinf);
-  return C0 + (kL0Bcc - kL0Liq) * (c - cinf);
+  const double g = phi * (1.875 + phi * phi * (-1.25 + 0.375 * phi * phi));
+  const double lam = log(c / (1.0 - c)) - log(cinf / (1.0 - cinf));
+  return -(g + 1.0) * C0 - (c - cinf) * ((kL0Bcc + kL0Liq) + g * (kL0Bcc - kL0Liq)) + tt.RT * lam;
 }
 
 __device__ __forceinline__ double dG_exact(double T, double c, double RR) {
@@ -63,7 +55,7 @@ __global__ void sample_kernel(const double cinf, const double RR, const MlpBox b
   x[3 * k + 0] = (float)(2.0 * u0 - 1.0);
   x[3 * k + 1] = (float)(2.0 * u1 - 1.0);
   x[3 * k + 2] = (float)phi;
-  y[2 * k + 0] = (float)mu2_network_part(T, c, cinf, RR);
+  y[2 * k + 0] = (float)mu2_exact(T, c, phi, cinf, RR);
   y[2 * k + 1] = (float)dG_exact(T, c, RR);
 }
 

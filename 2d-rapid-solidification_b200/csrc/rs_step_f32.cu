@@ -274,23 +274,14 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     in[2] = clamp1(sm.psi[rr][b]);
   };
   // store the surrogate mu'' of one cell, or keep the exact value already in
-  // place (out-of-box and audited cells); audited cells record the errors.
-  // The network gives Q = C0(T) + (L0_BCC - L0_Liq) delta; the rest of
-  //   mu'' = RT lam(c) - 2 L0_Liq delta - (1 + g) Q
-  // is exact here (the same lam and g as the exact form), so mu'' is exact
-  // at psi = -1, where network cells border the exact bulk melt
+  // place (out-of-box and audited cells); audited cells record the errors
   auto net_store = [&](int rr, int b, const float in[3], const float o[2]) {
     const int gx = x0 + b - 4;
-    const float dv = sm.d[rr][b], pv = sm.psi[rr][b];
-    const float T = SA.T_mid + in[0] / SA.T_ihalf, c = F.cinf + dv;
+    const float T = SA.T_mid + in[0] / SA.T_ihalf, c = F.cinf + sm.d[rr][b];
     const bool inbox = T >= SA.T_lo && T <= SA.T_hi && c >= SA.c_lo && c <= SA.c_hi;
     const bool real = gx >= 0 && gx <= K.nx - 1;
     const bool audit = real && surr_audit_cell(PS.step, (int64_t)(y0 - 1 + rr + K.j_offset) * K.nx + gx);
-    const float p2 = pv * pv;
-    const float g = pv * (1.875f + p2 * (-1.25f + 0.375f * p2));
-    const float Q = fmaf(o[0], SA.y_scale[0], SA.y_mean[0]);
-    const float mu_net = fmaf(tRT[gx], Tr<float>::lam(c, 1.f - c, dv, F.cinf, F.Lref),
-                              fmaf(-(g + 1.f), Q, dv * (float)(-2.0 * kL0Liq)));
+    const float mu_net = fmaf(o[0], SA.y_scale[0], SA.y_mean[0]);
     if (inbox && !audit) {
       sm.mu[rr][b] = mu_net;
     } else if (real) {

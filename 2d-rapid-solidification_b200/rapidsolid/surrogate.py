@@ -1,11 +1,8 @@
 """Training of the learned CALPHAD surrogate on the GPU (rs_mlp_* entry points).
 
 The network (3 -> 32 -> 32 -> 2, SiLU) maps (T, c, phi) scaled over a box to
-Q = C0(T) + (L0_BCC - L0_Liq)(c - cinf), the CALPHAD part of the chemical
-potential relative to the melt's column value,
-mu'' = RT lam(c) - 2 L0_Liq (c - cinf) - (1 + g(phi)) Q (the step applies the
-rest exactly), and to the driving force Gl - Gs; the training data are
-evaluated by the exact FP64
+the chemical potential relative to the melt's column value (mu'') and the
+driving force Gl - Gs; the training data are evaluated by the exact FP64
 evaluator on the GPU (rs_mlp_sample), the gradients by the library's own
 backward kernel (rs_mlp_grad) and the update by its Adam kernel
 (rs_mlp_adam).  PyTorch only holds the buffers and shuffles the indices.
@@ -128,7 +125,7 @@ def train(p, box=None, n_samples=1 << 20, epochs=20, batch=4096, lr=3e-3, seed=1
 
 
 def errors(box, w, x, y):
-    """Max and RMS absolute error of the raw outputs (Q, dG) in J/mol."""
+    """Max and RMS absolute error of the raw outputs (mu'', dG) in J/mol."""
     out = forward(box, w, x)
     e = (out.double() - y.double()).abs()
     return e.max(0).values.tolist(), e.pow(2).mean(0).sqrt().tolist()

@@ -310,15 +310,9 @@ int rs_write_field_text(const char *path, const double *h_field, int32_t nx_all,
  * A 3 -> 32 -> 32 -> 2 SiLU network mapping (T, c, phi), scaled to [-1, 1]
  * over a training box, to the two per-cell CALPHAD terms of the FP32 step:
  * the chemical potential relative to the melt's column value (mu'') and the
- * driving force Gl - Gs (fun.cu:1671-1720).  Since
- *   mu'' = RT lam(c) - 2 L0_Liq (c - cinf) - (1 + g(phi)) Q,
- *   Q = C0(T) + (L0_BCC - L0_Liq)(c - cinf),  lam = log(c/(1-c)) - log(cinf/(1-cinf)),
- * the first output is Q, the temperature-dependent CALPHAD part, and the
- * step applies the rest exactly: mu'' is then exact at phi = -1, where the
- * network's cells border the exact bulk melt, and the unbounded log term
- * (c -> 0 or 1) stays out of the fit.  Parameters are one FP32 vector of RS_MLP_NPARAMS:
- * W1[32][3], b1[32], W2[32][32], b2[32], W3[2][32], b3[2].  Outputs are
- * scaled: raw = y_mean + y_scale * network output. */
+ * driving force Gl - Gs (fun.cu:1671-1720).  Parameters are one FP32 vector
+ * of RS_MLP_NPARAMS: W1[32][3], b1[32], W2[32][32], b2[32], W3[2][32], b3[2].
+ * Outputs are scaled: raw = y_mean + y_scale * network output. */
 #define RS_MLP_NPARAMS 1250
 typedef struct rs_mlp_box {
   double T_lo, T_hi;       /* K */
@@ -326,8 +320,7 @@ typedef struct rs_mlp_box {
   double y_mean[2], y_scale[2];
 } rs_mlp_box;
 /* n training samples, uniform over the box (Philox keyed by seed and index):
- * d_x[n][3] scaled inputs, d_y[n][2] exact targets (FP64 evaluator, rounded):
- * Q and Gl - Gs. */
+ * d_x[n][3] scaled inputs, d_y[n][2] exact targets (FP64 evaluator, rounded). */
 int rs_mlp_sample(const rs_params *p, const rs_mlp_box *box, int64_t n, uint64_t seed, float *d_x, float *d_y,
                   rs_stream_t stream);
 /* Adds the gradient of sum over samples of |out - (y - y_mean)/y_scale|^2 to
