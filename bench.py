@@ -208,16 +208,22 @@ class Loop:
         self.ctx.close()
 
 
-def timed_steps(loop, steps, flush, st):
-    """CUDA-event time (ms) of each of `steps` steps, L2 flushed before each."""
+def timed_steps(loop, steps, flush, st, nvtx=None):
+    """CUDA-event time (ms) of each of `steps` steps, L2 flushed before each.
+    `nvtx` names an NVTX range around them (a profiler can capture just the
+    timed launches with it; without a profiler the range costs nothing)."""
     torch = loop.torch
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     loop.launches = 0
+    if nvtx:
+        torch.cuda.nvtx.range_push(nvtx)
     for k in range(steps):
         flush(k)
         ev[k][0].record(st)
         loop.step()
         ev[k][1].record(st)
+    if nvtx:
+        torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     return [s.elapsed_time(e) for s, e in ev], loop.launches
 
@@ -301,9 +307,25 @@ def run_arm(p, dtype, args, flush, st, dist, world, clocks=None, options=None, e
             for _ in range(20):
                 loop.step()
             loop.torch.cuda.synchronize()
+    # the timed window starts on the step after a pull-back step, so that its
+    # K consecutive steps hold the loop's cadence (one pull-back step in
+    # step_pull_back) whatever the pre-roll took; the pull-back step itself is
+    # timed on its own afterwards
+    spb = loop.d.step_pull_back
+    while loop.n % spb != 1:
+        loop.step()
+    loop.torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    n0 = loop.n
     t_wall = time.time()
-    ms_steps, launches = timed_steps(loop, args.steps, flush, st)
+    ms_steps, launches = timed_steps(loop, args.steps, flush, st, nvtx=f"timed_{loop.prec}")
     t_wall = time.time() - t_wall
+    if dist:
+        dist.barrier()
+    while loop.n % spb != 0:
+        loop.step()
+    pb_ms, _ = timed_steps(loop, 1, flush, st)
     clk = None
     if clocks is not None:
         t_post = time.time()
@@ -320,8 +342,12 @@ def run_arm(p, dtype, args, flush, st, dist, world, clocks=None, options=None, e
     out = {"value": round(job_throughput(world, cells, args.steps, total_ms), 4),
            "ms_per_step": round(total_ms / args.steps, 5),
            "roofline": roofline(loop.prec, cells, kern_ms, peak, peak_kind, kernel_name(loop.prec, options)),
-           "gpu_launches": launches, "wall_s_timed": round(t_wall, 3), "clocks": clk}
+           "gpu_launches": launches, "wall_s_timed": round(t_wall, 3), "clocks": clk,
+           "first_timed_step": n0, "pull_back_step_ms": round(pb_ms[0], 5), "step_pull_back": spb}
     if e2e:
+        # an output interval that starts after a pull-back step, like the window above
+        while loop.n % spb != 1:
+            loop.step()
         out["e2e"] = e2e_interval(loop, loop.d.step_fields, dist, world, st)
     loop.close()
     return out
@@ -357,6 +383,8 @@ def run_ours(args):
         "l2": "flushed between timed steps (256 MiB written, then 256 MiB read)",
         "roofline": head["roofline"], "e2e": head["e2e"], "gpu_launches": head["gpu_launches"],
         "clocks": head["clocks"], "wall_s_timed": head["wall_s_timed"],
+        "first_timed_step": head["first_timed_step"], "pull_back_step_ms": head["pull_back_step_ms"],
+        "step_pull_back": head["step_pull_back"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, seconds=args.cpu_seconds)
