@@ -651,6 +651,15 @@ int rs_mlp_sample(const rs_params *p, const rs_mlp_box *box, int64_t n, uint64_t
   return cuda_check("rs_mlp_sample");
 }
 
+int rs_mlp_sample_g(const rs_params *p, const rs_mlp_box *box, int64_t n, uint64_t seed, float *d_x, float *d_y,
+                    rs_stream_t stream) {
+  if (!p || !d_x || !d_y || n < 0) return fail(RS_E_INVALID, "rs_mlp_sample_g: bad argument");
+  if (!box || !(box->T_hi > box->T_lo) || !(box->c_hi > box->c_lo) || box->c_lo <= 0.0 || box->c_hi >= 1.0)
+    return fail(RS_E_INVALID, "rs_mlp_sample_g: box must have T_lo < T_hi and 0 < c_lo < c_hi < 1");
+  rs::launch_mlp_sample(p->cinf, p->RR, to_box(box), n, seed, d_x, d_y, (cudaStream_t)stream, true);
+  return cuda_check("rs_mlp_sample_g");
+}
+
 int rs_mlp_grad(const rs_mlp_box *box, const float *d_w, int64_t n, const float *d_x, const float *d_y,
                 float *d_grad, double *d_loss, rs_stream_t stream) {
   if (!box_ok(box) || !d_w || !d_x || !d_y || !d_grad || !d_loss || n < 0)
@@ -678,59 +687,60 @@ static uint16_t to_f16(float f) {  // round to nearest even
   return __half_as_ushort(__float2half_rn(f));
 }
 
-int rs_set_surrogate(rs_ctx *c, const float *d_w, const rs_mlp_box *box) {
-  if (!c) return fail(RS_E_INVALID, "rs_set_surrogate: null context");
-  if (!d_w) {
-    c->surr.w = nullptr;
-    return RS_OK;
-  }
-  if (!box_ok(box)) return fail(RS_E_INVALID, "rs_set_surrogate: bad box");
+}  // extern "C"
+
+namespace rs {
+
+// Device copies of a trained network for a step kernel: FP32 parameters, FP16
+// copies of the two tensor-core layers (W2[i][j], W3 padded to 8 rows) and a
+// cleared audit record, allocated on first use; fills the kernel arguments.
+cudaError_t surrogate_setup(const float *d_w, const rs_mlp_box *box, float **w, uint16_t **b16,
+                            unsigned long long **audit, SurrArgs *s) {
   cudaError_t e = cudaSuccess;
-  if (!c->mlp_w) e = cudaMalloc(&c->mlp_w, sizeof(float) * rs::kMlpNParams);
-  if (e == cudaSuccess && !c->mlp_b16) e = cudaMalloc(&c->mlp_b16, sizeof(uint16_t) * rs::kSurrB16);
-  if (e == cudaSuccess && !c->mlp_audit) {
-    e = cudaMalloc(&c->mlp_audit, sizeof(unsigned long long) * 4);
-    if (e == cudaSuccess) e = cudaMemset(c->mlp_audit, 0, sizeof(unsigned long long) * 4);
+  if (!*w) e = cudaMalloc(w, sizeof(float) * kMlpNParams);
+  if (e == cudaSuccess && !*b16) e = cudaMalloc(b16, sizeof(uint16_t) * kSurrB16);
+  if (e == cudaSuccess && !*audit) {
+    e = cudaMalloc(audit, sizeof(unsigned long long) * 4);
+    if (e == cudaSuccess) e = cudaMemset(*audit, 0, sizeof(unsigned long long) * 4);
   }
-  float hw[rs::kMlpNParams];
+  float hw[kMlpNParams];
   if (e == cudaSuccess) e = cudaMemcpy(hw, d_w, sizeof(hw), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return fail(RS_E_CUDA, "rs_set_surrogate: %s", cudaGetErrorString(e));
-  // FP16 copies of the tensor-core layers: W2[i][j] and W3 padded to 8 rows
-  uint16_t hb[rs::kSurrB16];
+  if (e != cudaSuccess) return e;
+  uint16_t hb[kSurrB16];
   memset(hb, 0, sizeof(hb));
-  for (int k = 0; k < rs::kMlpH * rs::kMlpH; ++k) hb[k] = to_f16(hw[rs::kOffW2 + k]);
-  for (int k = 0; k < 2 * rs::kMlpH; ++k) hb[rs::kMlpH * rs::kMlpH + k] = to_f16(hw[rs::kOffW3 + k]);
-  e = cudaMemcpy(c->mlp_w, hw, sizeof(hw), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(c->mlp_b16, hb, sizeof(hb), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) return fail(RS_E_CUDA, "rs_set_surrogate: %s", cudaGetErrorString(e));
-  rs::SurrArgs &s = c->surr;
-  s.w = c->mlp_w;
-  s.b16 = c->mlp_b16;
-  s.audit = c->mlp_audit;
-  s.T_mid = (float)(0.5 * (box->T_lo + box->T_hi));
-  s.T_ihalf = (float)(2.0 / (box->T_hi - box->T_lo));
-  s.c_mid = (float)(0.5 * (box->c_lo + box->c_hi));
-  s.c_ihalf = (float)(2.0 / (box->c_hi - box->c_lo));
-  s.T_lo = (float)box->T_lo;
-  s.T_hi = (float)box->T_hi;
-  s.c_lo = (float)box->c_lo;
-  s.c_hi = (float)box->c_hi;
+  for (int k = 0; k < kMlpH * kMlpH; ++k) hb[k] = to_f16(hw[kOffW2 + k]);
+  for (int k = 0; k < 2 * kMlpH; ++k) hb[kMlpH * kMlpH + k] = to_f16(hw[kOffW3 + k]);
+  e = cudaMemcpy(*w, hw, sizeof(hw), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(*b16, hb, sizeof(hb), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return e;
+  s->w = *w;
+  s->b16 = *b16;
+  s->audit = *audit;
+  s->T_mid = (float)(0.5 * (box->T_lo + box->T_hi));
+  s->T_ihalf = (float)(2.0 / (box->T_hi - box->T_lo));
+  s->c_mid = (float)(0.5 * (box->c_lo + box->c_hi));
+  s->c_ihalf = (float)(2.0 / (box->c_hi - box->c_lo));
+  s->T_lo = (float)box->T_lo;
+  s->T_hi = (float)box->T_hi;
+  s->c_lo = (float)box->c_lo;
+  s->c_hi = (float)box->c_hi;
   for (int q = 0; q < 2; ++q) {
-    s.y_mean[q] = (float)box->y_mean[q];
-    s.y_scale[q] = (float)box->y_scale[q];
+    s->y_mean[q] = (float)box->y_mean[q];
+    s->y_scale[q] = (float)box->y_scale[q];
   }
-  return RS_OK;
+  return cudaSuccess;
 }
 
-int rs_surrogate_audit(rs_ctx *c, double *max_err_mu, double *max_err_dG, int64_t *n_fallback, int64_t *n_audit,
-                       rs_stream_t stream) {
-  if (!c) return fail(RS_E_INVALID, "rs_surrogate_audit: null context");
+// Reads and clears an audit record (max error bits of mu'' and dG, fallback
+// and audit counts); synchronizes the stream.
+cudaError_t surrogate_audit_read(unsigned long long *audit, cudaStream_t st, double *max_err_mu, double *max_err_dG,
+                                 int64_t *n_fallback, int64_t *n_audit) {
   unsigned long long h[4] = {0, 0, 0, 0};
-  cudaStream_t st = (cudaStream_t)stream;
-  if (c->mlp_audit) {
-    if (cudaMemcpyAsync(h, c->mlp_audit, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemsetAsync(c->mlp_audit, 0, sizeof(h), st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
-      return fail(RS_E_CUDA, "rs_surrogate_audit: copy failed");
+  if (audit) {
+    cudaError_t e = cudaMemcpyAsync(h, audit, sizeof(h), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(audit, 0, sizeof(h), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
   }
   float f[2];
   for (int q = 0; q < 2; ++q) {
@@ -741,6 +751,33 @@ int rs_surrogate_audit(rs_ctx *c, double *max_err_mu, double *max_err_dG, int64_
   if (max_err_dG) *max_err_dG = f[1];
   if (n_fallback) *n_fallback = (int64_t)h[2];
   if (n_audit) *n_audit = (int64_t)h[3];
+  return cudaSuccess;
+}
+
+bool surrogate_box_ok(const rs_mlp_box *b) { return box_ok(b); }
+
+}  // namespace rs
+
+extern "C" {
+
+int rs_set_surrogate(rs_ctx *c, const float *d_w, const rs_mlp_box *box) {
+  if (!c) return fail(RS_E_INVALID, "rs_set_surrogate: null context");
+  if (!d_w) {
+    c->surr.w = nullptr;
+    return RS_OK;
+  }
+  if (!box_ok(box)) return fail(RS_E_INVALID, "rs_set_surrogate: bad box");
+  const cudaError_t e = rs::surrogate_setup(d_w, box, &c->mlp_w, &c->mlp_b16, &c->mlp_audit, &c->surr);
+  if (e != cudaSuccess) return fail(RS_E_CUDA, "rs_set_surrogate: %s", cudaGetErrorString(e));
+  return RS_OK;
+}
+
+int rs_surrogate_audit(rs_ctx *c, double *max_err_mu, double *max_err_dG, int64_t *n_fallback, int64_t *n_audit,
+                       rs_stream_t stream) {
+  if (!c) return fail(RS_E_INVALID, "rs_surrogate_audit: null context");
+  if (rs::surrogate_audit_read(c->mlp_audit, (cudaStream_t)stream, max_err_mu, max_err_dG, n_fallback, n_audit) !=
+      cudaSuccess)
+    return fail(RS_E_CUDA, "rs_surrogate_audit: copy failed");
   return RS_OK;
 }
 

@@ -10,6 +10,7 @@
 #include <mutex>
 
 #include "rs_peri3d.cuh"
+#include "rs_surrogate.cuh"
 
 namespace rs {
 int set_error(int code, const char *msg);
@@ -26,6 +27,11 @@ struct rs3_ctx {
     rs::P3Maps maps;
   } cache[4];
   int ncache, next;
+  double *tab;                    // energy 1: per-plane CALPHAD table of the step (device)
+  rs::SurrArgs surr;              // energy 1, FP32: learned surrogate (surr.w == nullptr: exact)
+  float *mlp_w;
+  uint16_t *mlp_b16;
+  unsigned long long *mlp_audit;
 };
 
 namespace {
@@ -46,8 +52,11 @@ PFN_cuTensorMapEncodeTiled_v12000 encode3() {
 int bad(int code, const char *msg) { return rs::set_error(code, msg); }
 
 bool params_ok(const rs3_params *p) {
-  return p && p->nx >= 4 && p->ny >= 4 && p->nz >= 4 && p->nx % 4 == 0 && p->dt > 0.0 && p->z_chunk >= 0 &&
-         (int64_t)p->nx * p->ny * p->nz < ((int64_t)1 << 40);
+  if (!(p && p->nx >= 4 && p->ny >= 4 && p->nz >= 4 && p->nx % 4 == 0 && p->dt > 0.0 && p->z_chunk >= 0 &&
+        (int64_t)p->nx * p->ny * p->nz < ((int64_t)1 << 40)))
+    return false;
+  if (p->energy == 0) return true;
+  return p->energy == 1 && p->c_ref > 0.0 && p->c_ref < 1.0 && p->RR > 0.0 && p->T_ref > 0.0 && p->AA >= 1.0;
 }
 
 bool fields_ok(const rs3_fields *f) {
@@ -61,7 +70,9 @@ bool encode_field(const rs3_params &p, const void *ptr, int precision, CUtensorM
   const size_t es = precision == RS_F64 ? 8 : 4;
   cuuint64_t dims[3] = {(cuuint64_t)p.nx, (cuuint64_t)p.ny, (cuuint64_t)p.nz};
   cuuint64_t strides[2] = {(cuuint64_t)p.nx * es, (cuuint64_t)p.nx * p.ny * es};
-  cuuint32_t box[3] = {(cuuint32_t)rs::peri3d_box_width(precision), (cuuint32_t)rs::peri3d_box_height(precision), 1};
+  const bool tinb = p.energy == 1;
+  cuuint32_t box[3] = {(cuuint32_t)(tinb ? rs::tinb_box_width(precision) : rs::peri3d_box_width(precision)),
+                       (cuuint32_t)(tinb ? rs::tinb_box_height() : rs::peri3d_box_height(precision)), 1};
   cuuint32_t estr[3] = {1, 1, 1};
   return enc(out, precision == RS_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
              const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -132,6 +143,10 @@ int rs3_default_params(rs3_params *p) {
   p->B12 = -0.466867;
   p->B22 = -0.0662661;
   p->T_ref = 60.0 * 0.000321787;  // T (TiAg.cu:52)
+  p->energy = 0;
+  p->AA = 1.0;  // energy 1 fields: q(phi1) = phi1 unless set
+  p->RR = 8.3145;
+  p->c_ref = 0.0;
   return RS_OK;
 }
 
@@ -143,8 +158,10 @@ int rs3_create(const rs3_params *p, rs3_ctx **out) {
   cudaError_t e = cudaMalloc(&c->err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->err, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&c->partials, sizeof(double) * c->nparts);
+  if (e == cudaSuccess && p->energy == 1) e = cudaMalloc(&c->tab, sizeof(double) * rs::tinb_table_len(*p));
   if (e != cudaSuccess) {
     cudaFree(c->err);
+    cudaFree(c->partials);
     delete c;
     return bad(RS_E_CUDA, "rs3_create: device allocation failed");
   }
@@ -156,6 +173,10 @@ int rs3_destroy(rs3_ctx *c) {
   if (!c) return RS_OK;
   cudaFree(c->err);
   cudaFree(c->partials);
+  cudaFree(c->tab);
+  cudaFree(c->mlp_w);
+  cudaFree(c->mlp_b16);
+  cudaFree(c->mlp_audit);
   delete c;
   return RS_OK;
 }
@@ -167,15 +188,22 @@ int rs3_step(rs3_ctx *c, const rs3_fields *cur, const rs3_fields *next, int64_t 
     return bad(RS_E_INVALID, "rs3_step: next must not alias cur");
   rs::P3Maps m;
   if (!maps_of(c, cur, &m)) return bad(RS_E_UNSUPPORTED, "rs3_step: tensor maps unavailable");
-  const int rc = rs::launch_peri3d_step(c->p, m, cur->precision, next->phi1, next->phi2, next->c, step, c->err,
-                                        (cudaStream_t)stream);
+  const int rc =
+      c->p.energy == 1
+          ? rs::launch_tinb_step(c->p, m, cur->precision, next->phi1, next->phi2, next->c, step, c->err, c->tab,
+                                 c->surr.w && cur->precision == RS_F32 ? &c->surr : nullptr, (cudaStream_t)stream)
+          : rs::launch_peri3d_step(c->p, m, cur->precision, next->phi1, next->phi2, next->c, step, c->err,
+                                   (cudaStream_t)stream);
   if (rc) return bad(RS_E_CUDA, "rs3_step: shared memory configuration failed");
   return launched("rs3_step");
 }
 
 int rs3_mu(rs3_ctx *c, const rs3_fields *f, void *d_mu, rs_stream_t stream) {
   if (!c || !fields_ok(f) || !d_mu) return bad(RS_E_INVALID, "rs3_mu: bad argument");
-  rs::launch_peri3d_mu(c->p, f->precision, f->phi1, f->phi2, f->c, d_mu, (cudaStream_t)stream);
+  if (c->p.energy == 1)
+    rs::launch_tinb_mu(c->p, f->precision, f->phi1, f->phi2, f->c, d_mu, c->tab, (cudaStream_t)stream);
+  else
+    rs::launch_peri3d_mu(c->p, f->precision, f->phi1, f->phi2, f->c, d_mu, (cudaStream_t)stream);
   return launched("rs3_mu");
 }
 
@@ -212,6 +240,37 @@ int rs3_initial(rs3_ctx *c, const rs3_fields *f, double z_front, double amp, int
   }
   rs::launch_peri3d_init(p, f->precision, ini, f->phi1, f->phi2, f->c, (cudaStream_t)stream);
   return launched("rs3_initial");
+}
+
+int rs3_initial_grains(rs3_ctx *c, const rs3_fields *f, double z_front, double amp, double c_liquid,
+                       double c_solid, uint64_t seed, rs_stream_t stream) {
+  if (!c || !fields_ok(f) || !(c_liquid > 0.0 && c_liquid < 1.0) || !(c_solid > 0.0 && c_solid < 1.0) || amp < 0.0)
+    return bad(RS_E_INVALID, "rs3_initial_grains: bad argument");
+  rs::launch_grains_init(c->p, f->precision, seed, z_front, amp, c_liquid, c_solid, f->phi1, f->phi2, f->c,
+                         (cudaStream_t)stream);
+  return launched("rs3_initial_grains");
+}
+
+int rs3_set_surrogate(rs3_ctx *c, const float *d_w, const rs_mlp_box *box) {
+  if (!c) return bad(RS_E_INVALID, "rs3_set_surrogate: null context");
+  if (c->p.energy != 1) return bad(RS_E_UNSUPPORTED, "rs3_set_surrogate: the surrogate serves energy 1");
+  if (!d_w) {
+    c->surr.w = nullptr;
+    return RS_OK;
+  }
+  if (!rs::surrogate_box_ok(box)) return bad(RS_E_INVALID, "rs3_set_surrogate: bad box");
+  if (rs::surrogate_setup(d_w, box, &c->mlp_w, &c->mlp_b16, &c->mlp_audit, &c->surr) != cudaSuccess)
+    return bad(RS_E_CUDA, "rs3_set_surrogate: device copy failed");
+  return RS_OK;
+}
+
+int rs3_surrogate_audit(rs3_ctx *c, double *max_err_mu, double *max_err_dG, int64_t *n_fallback, int64_t *n_audit,
+                        rs_stream_t stream) {
+  if (!c) return bad(RS_E_INVALID, "rs3_surrogate_audit: null context");
+  if (rs::surrogate_audit_read(c->mlp_audit, (cudaStream_t)stream, max_err_mu, max_err_dG, n_fallback, n_audit) !=
+      cudaSuccess)
+    return bad(RS_E_CUDA, "rs3_surrogate_audit: copy failed");
+  return RS_OK;
 }
 
 int rs3_c_offset(const rs3_params *p, double *out) {

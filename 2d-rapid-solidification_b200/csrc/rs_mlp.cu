@@ -24,11 +24,11 @@ namespace {
 constexpr int kGradThreads = 128;
 constexpr int kGradCtas = 8;  // CTAs of the one gradient cluster (portable size)
 
-__device__ __forceinline__ double mu2_exact(double T, double c, double phi, double cinf, double RR) {
+// g: the interpolation weight, gg(phi) for the 2D model, 2 gS - 1 for the 3D one
+__device__ __forceinline__ double mu2_exact(double T, double c, double g, double cinf, double RR) {
   const TTerms tt = t_terms(T, RR);
   const double D = 0.5 * (tt.dGs - tt.dGl);
   const double C0 = -D - 0.5 * (kL0Bcc - kL0Liq) * (1.0 - 2.0 * cinf);
-  const double g = phi * (1.875 + phi * phi * (-1.25 + 0.375 * phi * phi));
   const double lam = log(c / (1.0 - c)) - log(cinf / (1.0 - cinf));
   return -(g + 1.0) * C0 - (c - cinf) * ((kL0Bcc + kL0Liq) + g * (kL0Bcc - kL0Liq)) + tt.RT * lam;
 }
@@ -38,6 +38,8 @@ __device__ __forceinline__ double dG_exact(double T, double c, double RR) {
   return (1.0 - c) * tt.A_nb + c * tt.A_ti + c * (1.0 - c) * (kL0Liq - kL0Bcc);
 }
 
+// G_INPUT: the third input is g itself (3D model) instead of phi (2D model)
+template <bool G_INPUT>
 __global__ void sample_kernel(const double cinf, const double RR, const MlpBox box, const int64_t n,
                               const uint32_t seed_lo, const uint32_t seed_hi, float *__restrict__ x,
                               float *__restrict__ y) {
@@ -55,7 +57,8 @@ __global__ void sample_kernel(const double cinf, const double RR, const MlpBox b
   x[3 * k + 0] = (float)(2.0 * u0 - 1.0);
   x[3 * k + 1] = (float)(2.0 * u1 - 1.0);
   x[3 * k + 2] = (float)phi;
-  y[2 * k + 0] = (float)mu2_exact(T, c, phi, cinf, RR);
+  const double g = G_INPUT ? phi : phi * (1.875 + phi * phi * (-1.25 + 0.375 * phi * phi));
+  y[2 * k + 0] = (float)mu2_exact(T, c, g, cinf, RR);
   y[2 * k + 1] = (float)dG_exact(T, c, RR);
 }
 
@@ -217,10 +220,10 @@ __global__ void forward_kernel(const MlpBox box, const float *__restrict__ w, co
 }  // namespace
 
 int launch_mlp_sample(double cinf, double RR, const MlpBox &box, int64_t n, uint64_t seed, float *x, float *y,
-                      cudaStream_t st) {
+                      cudaStream_t st, bool g_input) {
   if (n <= 0) return 0;
-  sample_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(cinf, RR, box, n, (uint32_t)seed,
-                                                             (uint32_t)(seed >> 32), x, y);
+  auto kfn = g_input ? sample_kernel<true> : sample_kernel<false>;
+  kfn<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(cinf, RR, box, n, (uint32_t)seed, (uint32_t)(seed >> 32), x, y);
   return 0;
 }
 

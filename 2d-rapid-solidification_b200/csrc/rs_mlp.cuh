@@ -71,7 +71,7 @@ __device__ __forceinline__ void mlp_forward(const MlpView &W, const float x[3], 
 }
 
 int launch_mlp_sample(double cinf, double RR, const MlpBox &box, int64_t n, uint64_t seed, float *x, float *y,
-                      cudaStream_t st);
+                      cudaStream_t st, bool g_input = false);
 int launch_mlp_grad(const MlpBox &box, const float *w, int64_t n, const float *x, const float *y, float *grad,
                     double *loss, cudaStream_t st);
 int launch_mlp_adam(float *w, const float *grad, float *m, float *v, int64_t t, float lr, float scale,

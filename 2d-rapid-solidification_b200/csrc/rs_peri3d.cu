@@ -22,28 +22,10 @@
 // Algorithmic bytes per cell-step: 3 fields read + 3 written.
 #include <cuda.h>
 
-#include "rs_peri3d.cuh"
-#include "rs_step_common.cuh"
+#include "rs_peri3d_common.cuh"
 
 namespace rs {
 namespace {
-
-constexpr int kP3Threads = 256;
-constexpr int kP3BY = 16;            // output rows of a CTA
-constexpr int kP3Slots = 4;          // input plane ring
-constexpr int kP3MuSlots = 4;        // mu plane ring
-constexpr uint32_t kP3WaitLimit = 1u << 22;
-
-template <typename R>
-struct P3Cfg {
-  static constexpr int BX = 256 / (int)sizeof(R);    // output columns: 64 (FP32), 32 (FP64)
-  static constexpr int BXin = BX + 16 / (int)sizeof(R);  // + halo rounded to 16 bytes
-  static constexpr int BYin = kP3BY + 2;
-  static constexpr int kPlane = BXin * BYin;          // elements of one field plane
-  // a TMA destination starts on a 128-byte boundary: field planes padded
-  static constexpr int kPlaneAl = ((kPlane * (int)sizeof(R) + 127) / 128) * 128 / (int)sizeof(R);
-  static constexpr int kCellsPerThread = BX * kP3BY / kP3Threads;
-};
 
 template <typename R>
 struct P3Smem {
@@ -52,85 +34,11 @@ struct P3Smem {
   uint64_t full[kP3Slots];
 };
 
-// Folch-Plapp interpolation and derivatives (TiAg.cu:72-74 g, gp1, gp2)
-template <typename R>
-__device__ __forceinline__ R g3(R pi, R pj, R pk) {
-  return pi * pi * R(0.25) * (R(15) * (R(1) - pi) * (R(1) + pi - (pk - pj) * (pk - pj)) + pi * (R(9) * (pi * pi) - R(5)));
-}
-template <typename R>
-__device__ __forceinline__ R gp1(R pi, R pj, R pk) {
-  return R(3.75) * pi *
-         (R(-4) * (pi * pi) + R(3) * (pi * pi * pi) + R(2) - pi + (R(3) * pi - R(2)) * ((pj - pk) * (pj - pk)));
-}
-template <typename R>
-__device__ __forceinline__ R gp2(R pi, R pj, R pk) {
-  return R(7.5) * (pi - R(1)) * (pi * pi) * (pj - pk);
-}
-
-template <typename R>
-struct K3 {  // kernel constants in the working precision
-  int nx, ny, nz, z_chunk;
-  R dt, dxi, dyi, dzi, dxi2, dyi2, dzi2;
-  R a1, a2, a3, b, lam, Da2, Db2, cfx, cfy, cfz;
-  R r1, r2, r3;
-  double B11, B12, B21, B22, T_ref, G_T, V_T, z_T;
-};
-
-template <typename R>
-K3<R> make_k3(const rs3_params &p) {
-  K3<R> k;
-  k.nx = p.nx;
-  k.ny = p.ny;
-  k.nz = p.nz;
-  k.z_chunk = p.z_chunk > 0 ? p.z_chunk : 32;
-  k.dt = (R)p.dt;
-  k.dxi = (R)p.dx_inv;
-  k.dyi = (R)p.dy_inv;
-  k.dzi = (R)p.dz_inv;
-  k.dxi2 = (R)(p.dx_inv * p.dx_inv);
-  k.dyi2 = (R)(p.dy_inv * p.dy_inv);
-  k.dzi2 = (R)(p.dz_inv * p.dz_inv);
-  k.a1 = (R)p.a1;
-  k.a2 = (R)p.a2;
-  k.a3 = (R)p.a3;
-  k.b = (R)p.b;
-  k.lam = (R)p.lambda;
-  // c' = c + dt alpha sum_d din^2 (H+ - H-) / 2 with H = M dmu, M = phi1 + phi1'
-  // (+ Da (phi2 + phi2') + Db (phi3 + phi3')), TiAg.cu:543-552
-  k.Da2 = (R)p.Da;
-  k.Db2 = (R)p.Db;
-  k.cfx = (R)(0.5 * p.dt * p.alpha * p.dx_inv * p.dx_inv);
-  k.cfy = (R)(0.5 * p.dt * p.alpha * p.dy_inv * p.dy_inv);
-  k.cfz = (R)(0.5 * p.dt * p.alpha * p.dz_inv * p.dz_inv);
-  k.r1 = (R)p.A1;
-  k.r2 = (R)(-p.A1 - p.A2);
-  k.r3 = (R)(-p.A1 + p.A2);
-  k.B11 = p.B11;
-  k.B12 = p.B12;
-  k.B21 = p.B21;
-  k.B22 = p.B22;
-  k.T_ref = p.T_ref;
-  k.G_T = p.G_T;
-  k.V_T = p.V_T;
-  k.z_T = p.z_T;
-  return k;
-}
-
+// mu = c - sum_i r_i g_i (computeMu, TiAg.cu:461-470)
 template <typename R>
 __device__ __forceinline__ R mu_of(const K3<R> &k, R p1, R p2, R c) {
   const R p3 = R(1) - p1 - p2;
   return c - k.r1 * g3(p1, p2, p3) - k.r2 * g3(p2, p3, p1) - k.r3 * g3(p3, p1, p2);
-}
-
-template <typename R>
-__device__ __forceinline__ bool p3_wait(uint64_t *bar, uint32_t parity, int *err) {
-  uint32_t tries = 0;
-  while (!mbar_try_wait(bar, parity))
-    if (++tries >= kP3WaitLimit) {
-      atomicExch(err, 1);
-      return false;
-    }
-  return true;
 }
 
 // SD: solid diffusivities Da or Db non-zero (the reference sets both to 0)
@@ -451,7 +359,8 @@ int launch_step(const rs3_params &p, const P3Maps &m, R *o1, R *o2, R *oc, int64
 
 }  // namespace
 
-double peri3d_c_offset(const rs3_params &p) {  // clb at T_ref (TiAg.cu:67)
+double peri3d_c_offset(const rs3_params &p) {  // clb at T_ref (TiAg.cu:67); c_ref for energy 1
+  if (p.energy == 1) return p.c_ref;
   const double B1 = p.B11 + p.B12 * p.T_ref, B2 = p.B21 + p.B22 * p.T_ref;
   return (B1 - 0.5 * B2) / (p.A1 - 0.5 * p.A2) + p.A1;
 }
@@ -499,6 +408,10 @@ int launch_peri3d_init(const rs3_params &p, int precision, const P3Init &ini, vo
   else
     peri3d_init_kernel<float><<<g, 128, 0, st>>>(make_k3<float>(p), ini, (float *)f1, (float *)f2, (float *)fc,
                                                  peri3d_c_offset(p));
+  return launch_peri3d_ghosts(p, precision, f1, f2, fc, st);
+}
+
+int launch_peri3d_ghosts(const rs3_params &p, int precision, void *f1, void *f2, void *fc, cudaStream_t st) {
   const int ext[3][2] = {{p.ny, p.nz}, {p.nx, p.nz}, {p.nx, p.ny}};
   for (int axis = 0; axis < 3; ++axis) {
     const dim3 gg((ext[axis][0] + 127) / 128, ext[axis][1]);

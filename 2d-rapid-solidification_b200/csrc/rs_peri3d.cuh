@@ -39,5 +39,22 @@ int launch_peri3d_mass(const rs3_params &p, int precision, const void *fc, doubl
                        cudaStream_t st);
 int launch_peri3d_init(const rs3_params &p, int precision, const P3Init &ini, void *f1, void *f2, void *fc,
                        cudaStream_t st);
+// ghost layers of a set as images (x, then y, then z)
+int launch_peri3d_ghosts(const rs3_params &p, int precision, void *f1, void *f2, void *fc, cudaStream_t st);
+
+// energy 1 (Ti-Nb CALPHAD, rs_peri3d_tinb.cu): TMA box of a field set, the
+// per-plane table (doubles), the step (table kernel + step kernel; surr:
+// the FP32 surrogate or null), mu of every cell at step 0's temperature,
+// and the two-grain initial state
+struct SurrArgs;
+int tinb_box_width(int precision);
+int tinb_box_height();
+int tinb_table_len(const rs3_params &p);
+int launch_tinb_step(const rs3_params &p, const P3Maps &m, int precision, void *o1, void *o2, void *oc, int64_t step,
+                     int *err, double *tab, const SurrArgs *surr, cudaStream_t st);
+int launch_tinb_mu(const rs3_params &p, int precision, const void *f1, const void *f2, const void *fc, void *mu,
+                   double *tab, cudaStream_t st);
+int launch_grains_init(const rs3_params &p, int precision, uint64_t seed, double z_front, double amp,
+                       double c_liquid, double c_solid, void *f1, void *f2, void *fc, cudaStream_t st);
 
 }  // namespace rs

@@ -149,6 +149,15 @@ __device__ __forceinline__ void surr_tile16(const SurrConst &C, const float in0[
   out1[1] = o[3];
 }
 
+// host side (rs_capi.cu): device copies of a trained network for a step
+// kernel (allocated on first use) and its kernel arguments; reading and
+// clearing an audit record (synchronizes the stream); the box check
+cudaError_t surrogate_setup(const float *d_w, const rs_mlp_box *box, float **w, uint16_t **b16,
+                            unsigned long long **audit, SurrArgs *s);
+cudaError_t surrogate_audit_read(unsigned long long *audit, cudaStream_t st, double *max_err_mu, double *max_err_dG,
+                                 int64_t *n_fallback, int64_t *n_audit);
+bool surrogate_box_ok(const rs_mlp_box *b);
+
 __device__ __forceinline__ bool surr_audit_cell(int64_t step, int64_t cell) {
   const uint64_t h = ((uint64_t)cell * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)step * 0xC2B2AE3D27D4EB4Full);
   return ((h >> 40) & 1023u) == 0u;

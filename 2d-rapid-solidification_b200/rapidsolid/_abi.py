@@ -109,6 +109,9 @@ class Params3(C.Structure):
         ("A1", C.c_double), ("A2", C.c_double), ("B11", C.c_double), ("B12", C.c_double),
         ("B21", C.c_double), ("B22", C.c_double),
         ("T_ref", C.c_double), ("G_T", C.c_double), ("V_T", C.c_double), ("z_T", C.c_double),
+        # energy 0: TiAg.cu's grand potentials; 1: Ti-Nb CALPHAD (AA, RR, c_ref apply)
+        ("energy", C.c_int32), ("reserved", C.c_int32),
+        ("AA", C.c_double), ("RR", C.c_double), ("c_ref", C.c_double),
     ]
 
 

@@ -218,3 +218,56 @@ def peritectic_3d(G_K_per_m=2.0e6, V_m_per_s=0.2, nx=512, ny=512, nz=1024, lib=N
     p.V_T = V_m_per_s * p.dt * TIME_UNIT_S / dx_m
     p.z_T = IC3["z_front"]
     return p
+
+
+# ---------------------------------------------------------------- 3D Ti-Nb CALPHAD variant (energy 1)
+# The three-phase structure with the Ti-Nb CALPHAD energy of the 2D model; its
+# units are the 2D model's: lengths in W = S W0, time in tau0 = W^2 / (Gamma
+# muk0), dx = 0.8 W, the coupling lambda = 1 / (2 hh v0) and the solute
+# coefficient alpha = Dl / (Gamma muk0 h0 v0) per J/mol, so that in the
+# two-phase limit the 3D phase and solute equations are those of the 2D step
+# (isotropic).  The two solids are two BCC grains.
+IC3_TINB = dict(z_front=24.0, amp=0.5, seed=11)
+STEPS["tinb_3d"] = 5000
+
+
+def tinb_3d(G_K_per_m=2.0e6, V_m_per_s=0.2, x_nb=0.10, nx=512, ny=512, nz=1024, z_front=24.0, lib=None):
+    """3D Ti-Nb directional solidification on one GPU (energy 1): nx x ny x nz
+    (ghost layers included), melt x_Nb = x_nb, a frozen gradient G moving at V,
+    T = the alloy's solidus at the front plane z_front at step 0 (as the 2D
+    scale workload).  The three-phase well terms are TiAg.cu's (a2 = 4.43,
+    a3 = 6.09, b = 12); they stiffen the phase equations, so dt is 0.45 of the
+    explicit diffusive limit dx^2/6 (0.9 of it oscillates where a grain meets
+    the melt).  Returns the rs3 parameters; the melt and solid compositions
+    are tinb_compositions(x_nb)."""
+    if lib is None:
+        from . import lib as _lib
+        lib = _lib
+    p2 = scale()
+    d2 = lib.derive(p2)
+    p = lib.default_params3()
+    p.nx, p.ny, p.nz = nx, ny, nz
+    p.energy = 1
+    dx = 0.8
+    p.dx_inv = p.dy_inv = p.dz_inv = 1.0 / dx
+    p.dt = 0.45 * dx * dx / 6.0
+    p.lam = 1.0 / (2.0 * d2.hh * p2.v0)
+    p.alpha = p2.Dl / (p2.Gamma * p2.muk0) / (d2.h0 * p2.v0)
+    p.AA, p.RR = p2.AA, p2.RR
+    c0 = 1.0 - x_nb
+    p.c_ref = c0
+    T_sol = T_SOLIDUS_TI10NB if abs(c0 - C_LIQUID_TI10NB) < 1e-12 else phase_boundaries(c0)[2]
+    W_nm = p2.S * p2.W0
+    p.T_ref = T_sol
+    p.z_T = z_front
+    p.G_T = G_K_per_m * dx * W_nm * 1e-9
+    p.V_T = V_m_per_s * p.dt * d2.tau0 / (dx * W_nm)
+    return p
+
+
+def tinb_compositions(x_nb=0.10):
+    """(c_liquid, c_solid): the melt and the solid of the tangent at its liquidus."""
+    c0 = 1.0 - x_nb
+    if abs(c0 - C_LIQUID_TI10NB) < 1e-12:
+        return C_LIQUID_TI10NB, C_SOLID_AT_TLIQ
+    return c0, phase_boundaries(c0)[1]

@@ -91,6 +91,10 @@ def load():
         "rs3_initial": ([vp, vp, C.c_double, C.c_double, i32, C.c_double, C.c_uint64, vp], C.c_int),
         "rs3_device_status": ([vp, vp], C.c_int),
         "rs3_c_offset": ([vp, vp], C.c_int),
+        "rs3_initial_grains": ([vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, vp], C.c_int),
+        "rs3_set_surrogate": ([vp, vp, vp], C.c_int),
+        "rs3_surrogate_audit": ([vp, vp, vp, vp, vp, vp], C.c_int),
+        "rs_mlp_sample_g": ([vp, vp, i64, C.c_uint64, vp, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -433,3 +437,22 @@ class Context3:
 
     def device_status(self, stream=None):
         check(self.lib.rs3_device_status(self._h, _stream(stream)))
+
+    def initial_grains(self, fs, z_front, amp, c_liquid, c_solid, seed, stream=None):
+        f = fs.fields()
+        check(self.lib.rs3_initial_grains(self._h, C.byref(f), z_front, amp, c_liquid, c_solid, seed,
+                                          _stream(stream)))
+
+    def set_surrogate(self, w=None, box=None):
+        """Energy 1, FP32: the learned CALPHAD surrogate (w: RS_MLP_NPARAMS float32
+        device tensor trained on rs_mlp_sample_g samples, box: _abi.MlpBox); None: exact."""
+        check(self.lib.rs3_set_surrogate(self._h, None if w is None else _ptr(w),
+                                         None if box is None else C.byref(box)))
+
+    def surrogate_audit(self, stream=None):
+        """(max |mu'' error|, max |dG error|, fallback cells, audited cells) since the last call."""
+        em, eg = C.c_double(), C.c_double()
+        nf, na = C.c_int64(), C.c_int64()
+        check(self.lib.rs3_surrogate_audit(self._h, C.byref(em), C.byref(eg), C.byref(nf), C.byref(na),
+                                           _stream(stream)))
+        return em.value, eg.value, nf.value, na.value

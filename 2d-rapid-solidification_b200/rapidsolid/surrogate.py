@@ -63,11 +63,14 @@ def init_weights(seed=0):
     return w
 
 
-def sample(p, box, n, seed, stream=None):
+def sample(p, box, n, seed, stream=None, g_input=False):
+    """n samples over the box: (T, c, phi) inputs of the 2D model, or with
+    g_input (T, c, g) of the 3D model's energy 1 (rs_mlp_sample_g)."""
     import torch
     x = torch.empty((n, 3), dtype=torch.float32, device="cuda")
     y = torch.empty((n, 2), dtype=torch.float32, device="cuda")
-    check(load().rs_mlp_sample(C.byref(p), C.byref(box), n, seed, _ptr(x), _ptr(y), _stream(stream)))
+    fn = load().rs_mlp_sample_g if g_input else load().rs_mlp_sample
+    check(fn(C.byref(p), C.byref(box), n, seed, _ptr(x), _ptr(y), _stream(stream)))
     return x, y
 
 
@@ -88,12 +91,14 @@ def forward(box, w, x, stream=None):
     return out
 
 
-def train(p, box=None, n_samples=1 << 20, epochs=20, batch=4096, lr=3e-3, seed=1, verbose=False):
-    """Returns (weights float32 cuda tensor, box with output scaling, history)."""
+def train(p, box=None, n_samples=1 << 20, epochs=20, batch=4096, lr=3e-3, seed=1, verbose=False, g_input=False):
+    """Returns (weights float32 cuda tensor, box with output scaling, history).
+    g_input: the 3D model's inputs (T, c, g), p a 2D parameter set whose cinf
+    is the 3D context's c_ref."""
     import torch
     L = load()
     box = default_box() if box is None else box
-    x, y = sample(p, box, n_samples, seed)
+    x, y = sample(p, box, n_samples, seed, g_input=g_input)
     ym, ys = y.double().mean(0), y.double().std(0)
     for q in range(2):
         box.y_mean[q], box.y_scale[q] = float(ym[q]), float(ys[q])

@@ -410,6 +410,8 @@ def run_ours(args):
         line["beyond_l2"] = beyond_l2_leg()
         torch.cuda.empty_cache()
         line["peritectic_3d"] = peritectic_3d_leg(measured_peak()[0])
+        torch.cuda.empty_cache()
+        line["tinb_3d"] = tinb_3d_leg(measured_peak()[0])
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -570,6 +572,134 @@ def surrogate_leg(p, flush, fp32_value, fp64_value, nsteps=30, seeds=(1, 2, 3)):
             "note": "3->32->32->2 SiLU, FP16 mma.sync hidden layers; the network evaluates every cell that is "
                     "not bulk melt (the melt keeps its exact series form); exact fallback out of box and "
                     "1/1024 audit; 20000 steps, tip every 1000"}
+
+
+def _time3(ctx, a, b, k0, ntimed):
+    """median CUDA-event time (ms) of ntimed 3D steps from step k0; returns (ms, a, b)"""
+    import torch
+    ts = []
+    for k in range(k0, k0 + ntimed):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.step(a, b, k)
+        e1.record()
+        a, b = b, a
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return sorted(ts)[len(ts) // 2], a, b
+
+
+def tinb_3d_leg(peak, nsteps_run=5000, ntimed=10):
+    """The 3D three-phase structure with the Ti-Nb CALPHAD energy (energy 1):
+    512 x 512 x 1024 FP32, two BCC grains under a seeded planar front at
+    z = 24 +- 0.5 dx, melt x_Nb = 0.10, G = 2e6 K/m, V = 0.2 m/s, on the exact
+    CALPHAD path and with the learned surrogate (trained here on the box of
+    the run's states, inputs T, c and the interpolation weight).  Step times
+    by CUDA events (1 GiB per field: far beyond L2, no flush), roofline
+    against 24 algorithmic bytes per cell-step, and the whole 5000-step run
+    on both paths: front advance (mean solid thickness per column, the sum
+    over z of 1 - phi1), front speed over the second half, solute drift, and
+    the surrogate's front-speed and front-position differences from the exact
+    run.  The FP64 kernel at 512 x 512 x 256."""
+    import torch
+    from rapidsolid import configs, lib, surrogate
+    out = {}
+    p = configs.tinb_3d()
+    cl, cs = configs.tinb_compositions()
+    ic = configs.IC3_TINB
+    cells = (p.nx - 2) * (p.ny - 2) * (p.nz - 2)
+    p2 = configs.scale()
+    d2 = lib.derive(p2)
+    m_per_cell = 0.8 * p2.S * p2.W0 * 1e-9
+    s_per_step = p.dt * d2.tau0 * 1e-9
+    p2.cinf = p.c_ref
+    t0 = time.time()
+    w, box, hist = surrogate.train(p2, box=surrogate.fitted_box(), epochs=40, seed=1, g_input=True)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+
+    def front(fs):  # mean solid thickness per (x, y) column, in cells: sum over z of 1 - phi1
+        return float((1.0 - fs.phi1[1:-1, 1:-1, 1:-1].double()).sum(0).mean())
+
+    for name, use in (("fp32_exact", False), ("fp32_surrogate", True)):
+        ctx = lib.Context3(p)
+        if use:
+            ctx.set_surrogate(w, box)
+        a, b = lib.FieldSet3(p, torch.float32), lib.FieldSet3(p, torch.float32)
+        ctx.initial_grains(a, ic["z_front"], ic["amp"], cl, cs, ic["seed"])
+        for k in range(3):
+            ctx.step(a, b, k)
+            a, b = b, a
+        ms, a, b = _time3(ctx, a, b, 3, ntimed)
+        # the whole run from the initial state
+        m = torch.zeros(2, dtype=torch.float64, device="cuda")
+        ctx.initial_grains(a, ic["z_front"], ic["amp"], cl, cs, ic["seed"])
+        ctx.mass(a, m[0:1])
+        if use:
+            ctx.surrogate_audit()
+        fr = [front(a)]
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record()
+        for k in range(nsteps_run):
+            ctx.step(a, b, k)
+            a, b = b, a
+            if k + 1 == nsteps_run // 2:
+                fr.append(front(a))
+        r1.record()
+        ctx.mass(a, m[1:2])
+        torch.cuda.synchronize()
+        ctx.device_status()
+        fr.append(front(a))
+        run_ms = r0.elapsed_time(r1)
+        m0, m1 = m.tolist()
+        alg = 24 * cells
+        achieved = alg / (ms * 1e-3) / 1e9
+        speed = (fr[2] - fr[1]) * m_per_cell / ((nsteps_run - nsteps_run // 2) * s_per_step)
+        out[name] = {"value": round(cells / (ms * 1e-3) / 1e9, 3), "unit": "Gcell-steps/s",
+                     "ms_per_step": round(ms, 4), "grid": [p.nx, p.ny, p.nz], "interior_cells": cells,
+                     "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                                  "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": alg,
+                                  "kernel": "rs::tinb_kernel<float>"},
+                     "run": {"steps": nsteps_run, "ms": round(run_ms, 1), "front_cells": [round(x, 4) for x in fr],
+                             "front_speed_m_s": round(speed, 6), "solute_drift_rel": (m1 - m0) / m0}}
+        if use:
+            em, eg, nfb, naud = ctx.surrogate_audit()
+            out[name]["audit"] = {"max_err_mu_J_mol": em, "max_err_dG_J_mol": eg, "fallback_cells": nfb,
+                                  "audited_cells": naud}
+            out[name]["box"] = {"T": [round(box.T_lo, 3), round(box.T_hi, 3)], "c": [box.c_lo, box.c_hi]}
+            out[name]["train_s"] = round(t_train, 2)
+        ctx.close()
+        del a, b
+        torch.cuda.empty_cache()
+    ve, vs = out["fp32_exact"]["run"]["front_speed_m_s"], out["fp32_surrogate"]["run"]["front_speed_m_s"]
+    out["fp32_surrogate"]["vs_exact"] = round(out["fp32_surrogate"]["value"] / out["fp32_exact"]["value"], 3)
+    out["fp32_surrogate"]["front_speed_error"] = round(abs(vs - ve) / abs(ve), 6) if ve else None
+    out["fp32_surrogate"]["front_position_diff_cells"] = round(
+        out["fp32_surrogate"]["run"]["front_cells"][-1] - out["fp32_exact"]["run"]["front_cells"][-1], 6)
+    # FP64 at 512 x 512 x 256
+    q = configs.tinb_3d(nz=256)
+    cells = (q.nx - 2) * (q.ny - 2) * (q.nz - 2)
+    ctx = lib.Context3(q)
+    a, b = lib.FieldSet3(q, torch.float64), lib.FieldSet3(q, torch.float64)
+    ctx.initial_grains(a, ic["z_front"], ic["amp"], cl, cs, ic["seed"])
+    for k in range(3):
+        ctx.step(a, b, k)
+        a, b = b, a
+    ms, a, b = _time3(ctx, a, b, 3, ntimed)
+    ctx.device_status()
+    achieved = 48 * cells / (ms * 1e-3) / 1e9
+    out["fp64"] = {"value": round(cells / (ms * 1e-3) / 1e9, 3), "unit": "Gcell-steps/s", "ms_per_step": round(ms, 4),
+                   "grid": [q.nx, q.ny, q.nz],
+                   "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                                "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": 48 * cells,
+                                "kernel": "rs::tinb_kernel<double>"}}
+    ctx.close()
+    del a, b
+    torch.cuda.empty_cache()
+    out["note"] = ("TiAg.cu's three-phase structure with the Ti-Nb CALPHAD energy of the 2D model (mu = g1 Glc + "
+                   "(1 - g1) Gsc, driving force Gl - Gs), two BCC grains; one table launch (per-plane CALPHAD "
+                   "groups) and one fused z-march launch per step")
+    return out
 
 
 def peritectic_3d_leg(peak, nsteps_run=5000, ntimed=10):

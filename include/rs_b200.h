@@ -323,6 +323,12 @@ typedef struct rs_mlp_box {
  * d_x[n][3] scaled inputs, d_y[n][2] exact targets (FP64 evaluator, rounded). */
 int rs_mlp_sample(const rs_params *p, const rs_mlp_box *box, int64_t n, uint64_t seed, float *d_x, float *d_y,
                   rs_stream_t stream);
+/* The same with the third input the interpolation weight itself, g = 2 gS - 1
+ * in [-1, 1] (gS the solid weight), for the 3D model's energy 1, where g comes
+ * from the Folch-Plapp weights rather than from one phi: x[2] = g and the mu''
+ * target uses g where rs_mlp_sample uses gg(phi). */
+int rs_mlp_sample_g(const rs_params *p, const rs_mlp_box *box, int64_t n, uint64_t seed, float *d_x, float *d_y,
+                    rs_stream_t stream);
 /* Adds the gradient of sum over samples of |out - (y - y_mean)/y_scale|^2 to
  * d_grad (not cleared) and the loss to *d_loss (double, not cleared). */
 int rs_mlp_grad(const rs_mlp_box *box, const float *d_w, int64_t n, const float *d_x, const float *d_y,
@@ -391,7 +397,24 @@ int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choic
  * Extension beyond the reference: a frozen temperature
  *   T(z, step) = T_ref + G_T (z - z_T - V_T step)
  * enters through B1(T) = B11 + B12 T, B2(T) = B21 + B22 T (TiAg.cu:61-62);
- * G_T = 0 is the reference's isothermal model. */
+ * G_T = 0 is the reference's isothermal model.
+ *
+ * energy = 1: the Ti-Nb CALPHAD free energy of the 2D model (fun.cu:1628-1720)
+ * on the same three-phase structure (no counterpart in the reference, whose
+ * 3D program has no CALPHAD).  The database has one solid phase, BCC, so
+ * phases 2 and 3 are two BCC grains.  c is the Ti mole fraction, T (K) the
+ * frozen line above with T_ref in K and G_T in K per cell, and per cell
+ *   mu  = g1 Glc(T, c) + (1 - g1) Gsc(T, c)         (fun.cu:1443-1452, 1700-1720)
+ *   dG  = Gl(T, c) - Gs(T, c)                       (fun.cu:1192-1193, 1671-1698)
+ * with g1 the liquid's Folch-Plapp weight.  dG is the grand-potential
+ * difference of the liquid against both grains: lambda dG takes the place of
+ * TiAg's lambda (s_1 - r_1 mu) - lambda (s_j - r_j mu), so lambda is the
+ * coupling per J/mol (1 / (2 hh v0) of the 2D model gives its phase equation
+ * in the two-phase limit).  The solute update is
+ *   c' = c + dt alpha sum_faces (S + S')/2 (mu' - mu) / dx^2,
+ *   S  = [q(phi1) + Da phi2 + Db phi3] c (1 - c),  q(p) = p (AA - (AA - 1) p)
+ * (fun.cu:1424-1464 with the liquid fraction phi1 for (1 - psi)/2), alpha the
+ * solute coefficient per J/mol (Dl / (Gamma muk0 h0 v0) of the 2D model). */
 typedef struct rs3_params {
   int32_t nx, ny, nz;               /* extents incl. ghost layers (TiAg Nx, Ny, devNz) */
   int32_t z_chunk;                  /* planes per CTA of the z march (0: 32) */
@@ -404,6 +427,11 @@ typedef struct rs3_params {
   double G_T;                       /* dT per cell along z */
   double V_T;                       /* isotherm speed, cells per step */
   double z_T;                       /* plane where T = T_ref at step 0 */
+  int32_t energy;                   /* 0 TiAg.cu's grand potentials; 1 Ti-Nb CALPHAD (above) */
+  int32_t reserved;
+  double AA;                        /* energy 1: interface mobility enhancement of q */
+  double RR;                        /* energy 1: gas constant, J/mol/K */
+  double c_ref;                     /* energy 1: Ti fraction of the melt; FP32 sets hold c - c_ref */
 } rs3_params;
 
 /* A 3D field set on the device (nx * ny * nz elements each, 16-byte aligned).
@@ -429,7 +457,8 @@ int rs3_destroy(rs3_ctx *ctx);
  * fused into one launch: next = step(cur), ghost layers included. */
 int rs3_step(rs3_ctx *ctx, const rs3_fields *cur, const rs3_fields *next, int64_t step, rs_stream_t stream);
 /* mu of every cell, ghost layers as images (computeMu + boundaryMu);
- * d_mu has the set's precision */
+ * d_mu has the set's precision; energy 1: the CALPHAD mu (J/mol) at the
+ * temperature of step 0 */
 int rs3_mu(rs3_ctx *ctx, const rs3_fields *f, void *d_mu, rs_stream_t stream);
 /* FP64 sum of c over the interior (the avg_c numerator, TiAg.cu:237-249) */
 int rs3_mass(rs3_ctx *ctx, const rs3_fields *f, double *d_mass, rs_stream_t stream);
@@ -441,10 +470,25 @@ int rs3_mass(rs3_ctx *ctx, const rs3_fields *f, double *d_mass, rs_stream_t stre
  * cb, clb): beta cb, alpha ca, liquid clb.  Ghost layers are images. */
 int rs3_initial(rs3_ctx *ctx, const rs3_fields *f, double z_front, double amp, int32_t n_alpha,
                 double cap_radius, uint64_t seed, rs_stream_t stream);
-/* the offset of c in RS_F32 sets: clb at T_ref (TiAg.cu:67) */
+/* Initial state of two grains: below the plane z_front + U(-amp, amp) (one
+ * seeded draw per (x, y) column) solid of composition c_solid, phase 2 for
+ * x <= (nx - 2) / 2 and phase 3 beyond; melt of composition c_liquid above.
+ * Ghost layers are images. */
+int rs3_initial_grains(rs3_ctx *ctx, const rs3_fields *f, double z_front, double amp, double c_liquid,
+                       double c_solid, uint64_t seed, rs_stream_t stream);
+/* the offset of c in RS_F32 sets: clb at T_ref (TiAg.cu:67); c_ref for energy 1 */
 int rs3_c_offset(const rs3_params *p, double *out);
 /* RS_E_STATE if a step kernel's bounded wait for a plane load gave up */
 int rs3_device_status(rs3_ctx *ctx, rs_stream_t stream);
+/* Energy 1, FP32 sets: the learned CALPHAD surrogate (trained on samples of
+ * rs_mlp_sample_g with cinf = c_ref) in place of the per-cell evaluation of
+ * mu'' and dG of every cell that is not bulk melt (phi1 = 1 exactly, which
+ * keeps its exact series form); out-of-box cells and one in 1024 per step of
+ * the others (audit) are evaluated exactly.  d_w = NULL: the exact path. */
+int rs3_set_surrogate(rs3_ctx *ctx, const float *d_w, const rs_mlp_box *box);
+/* as rs_surrogate_audit */
+int rs3_surrogate_audit(rs3_ctx *ctx, double *max_err_mu, double *max_err_dG, int64_t *n_fallback,
+                        int64_t *n_audit, rs_stream_t stream);
 
 /* ---- host-side helpers (no device work) ---- */
 /* CALPHAD Ti-Nb evaluator (fun.cu:1628-1720), host build of the same code

@@ -70,6 +70,8 @@ def lib():
         L.ro3_mass.argtypes = [vp, vp]
         L.ro3_cap_centres.argtypes = [vp, C.c_int, C.c_uint64, vp, vp]
         L.ro3_initial.argtypes = [vp, C.c_double, C.c_double, C.c_int, C.c_double, C.c_uint64, vp, vp, vp]
+        L.ro3_initial_grains.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, vp, vp,
+                                         vp]
         _lib = L
     return _lib
 
@@ -202,6 +204,13 @@ def zeros3(p):
 def initial3(p, z_front, amp, n_alpha, cap_radius, seed):
     f = [zeros3(p) for _ in range(3)]
     lib().ro3_initial(C.byref(p), z_front, amp, n_alpha, cap_radius, seed, *[_p(a) for a in f])
+    return f
+
+
+def initial_grains3(p, z_front, amp, c_liquid, c_solid, seed):
+    """Two grains under a seeded front, melt above (rs3_initial_grains)."""
+    f = [zeros3(p) for _ in range(3)]
+    lib().ro3_initial_grains(C.byref(p), z_front, amp, c_liquid, c_solid, seed, *[_p(a) for a in f])
     return f
 
 

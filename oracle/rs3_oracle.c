@@ -52,6 +52,10 @@ void ro3_default_params(rs3_params *p) {
   p->B12 = -0.466867;
   p->B22 = -0.0662661;
   p->T_ref = 60.0 * 0.000321787; /* TiAg.cu:52 */
+  p->energy = 0;
+  p->AA = 1.0;
+  p->RR = 8.3145;
+  p->c_ref = 0.0;
 }
 
 /* T of plane z at a step; B1, B2 (TiAg.cu:61-62) */
@@ -90,16 +94,47 @@ void ro3_boundary(const rs3_params *p, double *f) {
     }
 }
 
-/* computeMu on every cell, then boundaryMu* (TiAg.cu:461-500) */
-void ro3_mu(const rs3_params *p, const double *phi1, const double *phi2, const double *c, double *mu) {
+/* energy 1 (Ti-Nb CALPHAD): T of plane z at a step, in K */
+static double plane_T(const rs3_params *p, int z, int64_t step) {
+  return p->T_ref + p->G_T * ((double)z - p->z_T - p->V_T * (double)step);
+}
+/* the 2D parameter set whose CALPHAD functions serve energy 1 (only RR is read) */
+static rs_params calphad_params(const rs3_params *p) {
+  rs_params q;
+  ro_default_params(&q);
+  q.RR = p->RR;
+  return q;
+}
+
+/* computeMu on every cell, then boundaryMu* (TiAg.cu:461-500).  Energy 1:
+ * mu = g1 Glc + (1 - g1) Gsc at the plane's T (fun.cu:1443-1452 with
+ * 0.5 (1 + g) = 1 - g1), the ghost planes then images as in boundaryMu. */
+static void mu_at(const rs3_params *p, int64_t step, const double *phi1, const double *phi2, const double *c,
+                  double *mu) {
   const double r1 = p->A1, r2 = -p->A1 - p->A2, r3 = -p->A1 + p->A2;
   const int64_t n = (int64_t)p->nx * p->ny * p->nz;
+  if (p->energy == 1) {
+    const rs_params q = calphad_params(p);
+    const int64_t plane = (int64_t)p->nx * p->ny;
 #pragma omp parallel for schedule(static)
-  for (int64_t ps = 0; ps < n; ++ps) {
-    const double p1 = phi1[ps], p2 = phi2[ps], p3 = 1.0 - p1 - p2;
-    mu[ps] = c[ps] - r1 * g3(p1, p2, p3) - r2 * g3(p2, p3, p1) - r3 * g3(p3, p1, p2);
+    for (int64_t ps = 0; ps < n; ++ps) {
+      const double T = plane_T(p, (int)(ps / plane), step);
+      const double p1 = phi1[ps], p2 = phi2[ps], p3 = 1.0 - p1 - p2;
+      const double g1 = g3(p1, p2, p3), gS = 1.0 - g1;
+      mu[ps] = gS * ro_Gsc(&q, T, c[ps]) + g1 * ro_Glc(&q, T, c[ps]);
+    }
+  } else {
+#pragma omp parallel for schedule(static)
+    for (int64_t ps = 0; ps < n; ++ps) {
+      const double p1 = phi1[ps], p2 = phi2[ps], p3 = 1.0 - p1 - p2;
+      mu[ps] = c[ps] - r1 * g3(p1, p2, p3) - r2 * g3(p2, p3, p1) - r3 * g3(p3, p1, p2);
+    }
   }
   ro3_boundary(p, mu);
+}
+
+void ro3_mu(const rs3_params *p, const double *phi1, const double *phi2, const double *c, double *mu) {
+  mu_at(p, 0, phi1, phi2, c, mu);
 }
 
 /* diffuse on the interior (TiAg.cu:503-561) with the given mu */
@@ -110,11 +145,14 @@ static void diffuse(const rs3_params *p, int64_t step, const double *phi1, const
   const double r1 = p->A1, r2 = -p->A1 - p->A2, r3 = -p->A1 + p->A2;
   const double a1 = p->a1, a2 = p->a2, a3 = p->a3, b = p->b, lam = p->lambda;
   const double Da = p->Da, Db = p->Db;
+  const int tinb = p->energy == 1;
+  const rs_params q = calphad_params(p);
 #pragma omp parallel for schedule(static)
   for (int z = 1; z < nz - 1; ++z) {
     double B1, B2;
     plane_B(p, z, step, &B1, &B2);
     const double s1 = B1, s2 = -B1 - B2, s3 = -B1 + B2;
+    const double Tz = tinb ? plane_T(p, z, step) : 0.0;
     for (int y = 1; y < ny - 1; ++y)
       for (int x = 1; x < nx - 1; ++x) {
         const int64_t ps = P3(p, x, y, z);
@@ -122,15 +160,22 @@ static void diffuse(const rs3_params *p, int64_t step, const double *phi1, const
         const int64_t yp = P3(p, x, y + 1, z), ym = P3(p, x, y - 1, z);
         const int64_t zp = P3(p, x, y, z + 1), zm = P3(p, x, y, z - 1);
         const double p1 = phi1[ps], p2 = phi2[ps], p3 = 1.0 - p1 - p2, muu = mu[ps];
-        const double fcphi1 =
-            lam * (gp1(p1, p2, p3) * (s1 - r1 * muu) + gp2(p2, p1, p3) * (s2 - r2 * muu) +
-                   gp2(p3, p1, p2) * (s3 - r3 * muu));
-        const double fcphi2 =
-            lam * (gp2(p1, p2, p3) * (s1 - r1 * muu) + gp1(p2, p3, p1) * (s2 - r2 * muu) +
-                   gp2(p3, p2, p1) * (s3 - r3 * muu));
-        const double fcphi3 =
-            lam * (gp2(p1, p3, p2) * (s1 - r1 * muu) + gp2(p2, p3, p1) * (s2 - r2 * muu) +
-                   gp1(p3, p1, p2) * (s3 - r3 * muu));
+        double fcphi1, fcphi2, fcphi3;
+        if (tinb) {
+          /* the liquid's grand potential against both grains: Gl - Gs at the
+           * cell (fun.cu:1192-1193), for (s1 - r1 mu) - (s_j - r_j mu) */
+          const double dG = ro_Gl(&q, Tz, c[ps]) - ro_Gs(&q, Tz, c[ps]);
+          fcphi1 = lam * (gp1(p1, p2, p3) * dG);
+          fcphi2 = lam * (gp2(p1, p2, p3) * dG);
+          fcphi3 = lam * (gp2(p1, p3, p2) * dG);
+        } else {
+          fcphi1 = lam * (gp1(p1, p2, p3) * (s1 - r1 * muu) + gp2(p2, p1, p3) * (s2 - r2 * muu) +
+                          gp2(p3, p1, p2) * (s3 - r3 * muu));
+          fcphi2 = lam * (gp2(p1, p2, p3) * (s1 - r1 * muu) + gp1(p2, p3, p1) * (s2 - r2 * muu) +
+                          gp2(p3, p2, p1) * (s3 - r3 * muu));
+          fcphi3 = lam * (gp2(p1, p3, p2) * (s1 - r1 * muu) + gp2(p2, p3, p1) * (s2 - r2 * muu) +
+                          gp1(p3, p1, p2) * (s3 - r3 * muu));
+        }
         const double lap1 = (phi1[xp] + phi1[xm] - 2.0 * p1) * DXin * DXin +
                             (phi1[yp] + phi1[ym] - 2.0 * p1) * DYin * DYin +
                             (phi1[zp] + phi1[zm] - 2.0 * p1) * DZin * DZin;
@@ -155,14 +200,20 @@ static void diffuse(const rs3_params *p, int64_t step, const double *phi1, const
         const double phi2t = -(2.0 * muphi2 - muphi1 - muphi3) * 0.333333333333333333333333333;
         phi1_n[ps] = p1 + p->dt * phi1t;
         phi2_n[ps] = p2 + p->dt * phi2t;
-        /* solute: face mobilities 0.5 (phi1 + phi1') (+ Da, Db terms) */
-#define HFACE(n, dmu, din)                                                                              \
-  ((0.5 * (p1 + phi1[n]) + Da * 0.5 * (p2 + phi2[n]) + Db * 0.5 * (p3 + 1.0 - phi1[n] - phi2[n])) * (dmu) * \
-   (din))
+        /* solute: face mobilities 0.5 (phi1 + phi1') (+ Da, Db terms); energy 1:
+         * 0.5 (S + S'), S = [q(phi1) + Da phi2 + Db phi3] c (1 - c) with
+         * q(p) = p (AA - (AA - 1) p) (fun.cu:189, 1424-1464 in the liquid fraction) */
+#define SCELL(n) \
+  ((phi1[n] * (p->AA - (p->AA - 1.0) * phi1[n]) + Da * phi2[n] + Db * (1.0 - phi1[n] - phi2[n])) * c[n] * (1.0 - c[n]))
+#define HFACE(n, dmu, din)                                                                                    \
+  ((tinb ? 0.5 * (SCELL(ps) + SCELL(n))                                                                       \
+         : 0.5 * (p1 + phi1[n]) + Da * 0.5 * (p2 + phi2[n]) + Db * 0.5 * (p3 + 1.0 - phi1[n] - phi2[n])) * \
+   (dmu) * (din))
         const double Hxp = HFACE(xp, mu[xp] - muu, DXin), Hxn = HFACE(xm, muu - mu[xm], DXin);
         const double Hyp = HFACE(yp, mu[yp] - muu, DYin), Hyn = HFACE(ym, muu - mu[ym], DYin);
         const double Hzp = HFACE(zp, mu[zp] - muu, DZin), Hzn = HFACE(zm, muu - mu[zm], DZin);
 #undef HFACE
+#undef SCELL
         c_n[ps] = c[ps] + p->dt * p->alpha * ((Hxp - Hxn) * DXin + (Hyp - Hyn) * DYin + (Hzp - Hzn) * DZin);
       }
   }
@@ -174,7 +225,7 @@ void ro3_step(const rs3_params *p, int64_t step, const double *phi1, const doubl
               double *phi1_n, double *phi2_n, double *c_n, double *mu_out) {
   const int64_t n = (int64_t)p->nx * p->ny * p->nz;
   double *mu = mu_out ? mu_out : (double *)malloc(sizeof(double) * n);
-  ro3_mu(p, phi1, phi2, c, mu);
+  mu_at(p, step, phi1, phi2, c, mu);
   diffuse(p, step, phi1, phi2, c, mu, phi1_n, phi2_n, c_n);
   ro3_boundary(p, phi1_n);
   ro3_boundary(p, phi2_n);
@@ -244,6 +295,36 @@ void ro3_initial(const rs3_params *p, double z_front, double amp, int n_alpha, d
           phi1[ps] = 1.0;
           phi2[ps] = 0.0;
           c[ps] = clb;
+        }
+      }
+    }
+  ro3_boundary(p, phi1);
+  ro3_boundary(p, phi2);
+  ro3_boundary(p, c);
+}
+
+/* the initial state of rs3_initial_grains: solid c_solid below the seeded
+ * front (phase 2 for x <= (nx - 2) / 2, phase 3 beyond), melt c_liquid above */
+void ro3_initial_grains(const rs3_params *p, double z_front, double amp, double c_liquid, double c_solid,
+                        uint64_t seed, double *phi1, double *phi2, double *c) {
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  for (int y = 1; y < p->ny - 1; ++y)
+    for (int x = 1; x < p->nx - 1; ++x) {
+      const uint32_t ctr[4] = {(uint32_t)x, (uint32_t)y, 0u, 0x5A465254u};
+      uint32_t o[4];
+      ro_philox4x32(ctr, key, o);
+      const double zc = z_front + amp * (2.0 * u53(o[0], o[1]) - 1.0);
+      const int first = x <= (p->nx - 2) / 2;
+      for (int z = 1; z < p->nz - 1; ++z) {
+        const int64_t ps = P3(p, x, y, z);
+        if (z < zc) {
+          phi1[ps] = 0.0;
+          phi2[ps] = first ? 1.0 : 0.0;
+          c[ps] = c_solid;
+        } else {
+          phi1[ps] = 1.0;
+          phi2[ps] = 0.0;
+          c[ps] = c_liquid;
         }
       }
     }

@@ -100,6 +100,8 @@ double ro3_mass(const rs3_params *p, const double *c);
 void ro3_cap_centres(const rs3_params *p, int n_alpha, uint64_t seed, double *cx, double *cy);
 void ro3_initial(const rs3_params *p, double z_front, double amp, int n_alpha, double cap_radius, uint64_t seed,
                  double *phi1, double *phi2, double *c);
+void ro3_initial_grains(const rs3_params *p, double z_front, double amp, double c_liquid, double c_solid,
+                        uint64_t seed, double *phi1, double *phi2, double *c);
 
 #ifdef __cplusplus
 }
