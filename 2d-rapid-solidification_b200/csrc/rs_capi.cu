@@ -796,7 +796,32 @@ struct rs_ens {
   cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
   cudaStream_t cap = nullptr;
   int32_t *d_itip = nullptr, *h_itip = nullptr;
+  bool walk = false;            // stretches without pull-back as one persistent launch (else graph replays)
+  unsigned *d_bar = nullptr;    // grid-barrier counter and tile ticket counter of the persistent walk
+  double *h_lv = nullptr, *d_lv = nullptr;  // l_offset_Vp of every run at each step of a walk launch
 };
+
+namespace {
+constexpr int64_t kMaxWalk = 1024;  // steps per persistent launch
+
+// l_offset_Vp of every run at steps 0 .. k of a walk from the mirror's state,
+// by the additions ens_advance_kernel makes, on the device; the stream is
+// synchronized first, so the pinned buffer is free
+int ens_walk_l(rs_ens *e, int64_t k, cudaStream_t st) {
+  if (cudaStreamSynchronize(st) != cudaSuccess) return -1;
+  for (int r = 0; r < e->n; ++r) {
+    double l = e->h_runs[r].l;
+    for (int64_t s = 0; s <= k; ++s) {
+      e->h_lv[s * e->n + r] = l;
+      l += e->h_runs[r].inc_l;
+    }
+  }
+  return cudaMemcpyAsync(e->d_lv, e->h_lv, sizeof(double) * (k + 1) * e->n, cudaMemcpyHostToDevice, st) ==
+                 cudaSuccess
+             ? 0
+             : -1;
+}
+}  // namespace
 
 namespace {
 
@@ -841,6 +866,9 @@ int ens_prepare(rs_ens *e) {
     c = cudaMemcpy(e->d_order[k], ord[k].data(), sizeof(int32_t) * e->ntiles, cudaMemcpyHostToDevice);
   if (c == cudaSuccess) c = cudaMemcpy(e->d_runs, e->h_runs, sizeof(rs::EnsRun) * e->n, cudaMemcpyHostToDevice);
   if (c == cudaSuccess) c = cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking);
+  if (c == cudaSuccess) c = cudaMalloc(&e->d_bar, 2 * sizeof(unsigned));
+  if (c == cudaSuccess) c = cudaMalloc(&e->d_lv, sizeof(double) * (kMaxWalk + 1) * e->n);
+  if (c == cudaSuccess) c = cudaMallocHost(&e->h_lv, sizeof(double) * (kMaxWalk + 1) * e->n);
   if (c != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble: %s", cudaGetErrorString(c));
   e->ready = true;
   return RS_OK;
@@ -907,6 +935,9 @@ int rs_ensemble_destroy(rs_ens *e) {
   cudaFree(e->d_tblk);
   for (int k = 0; k < 3; ++k) cudaFree(e->d_order[k]);
   cudaFree(e->d_itip);
+  cudaFree(e->d_bar);
+  cudaFree(e->d_lv);
+  cudaFreeHost(e->h_lv);
   cudaFreeHost(e->h_itip);
   cudaFreeHost(e->h_runs);
   for (rs_ctx *c : e->ctx) rs_destroy(c);
@@ -983,16 +1014,32 @@ int rs_ensemble_steps(rs_ens *e, int64_t nsteps, rs_stream_t stream) {
           return fail(RS_E_CUDA, "rs_ensemble_steps: state upload failed");
         dirty = false;
       }
-      cudaGraphExec_t ex;
-      if ((rc = ens_graph(e, &ex))) return rc;
       const int64_t k = std::min(m, nsteps);
-      for (int64_t q = 0; q < k; ++q)
-        if (cudaGraphLaunch(ex, st) != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble_steps: graph launch");
-      for (int r = 0; r < e->n; ++r)
-        for (int64_t q = 0; q < k; ++q) {
-          e->h_runs[r].step += 1;
-          e->h_runs[r].l += e->h_runs[r].inc_l;
+      if (e->walk) {  // the stretch as persistent launches of up to kMaxWalk steps
+        for (int64_t q = 0; q < k; q += kMaxWalk) {
+          const int64_t kq = std::min(kMaxWalk, k - q);
+          if (ens_walk_l(e, kq, st) ||
+              rs::launch_ensemble_walk(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles,
+                                       (int)kq, e->d_lv, true, e->surr, e->d_bar, e->ctx[0]->d_err, st))
+            return fail(RS_E_CUDA, "rs_ensemble_steps: persistent launch failed");
+          for (int r = 0; r < e->n; ++r)  // the mirror follows (the next chunk starts from it)
+            for (int64_t s2 = 0; s2 < kq; ++s2) {
+              e->h_runs[r].step += 1;
+              e->h_runs[r].l += e->h_runs[r].inc_l;
+            }
         }
+      } else {
+        cudaGraphExec_t ex;
+        if ((rc = ens_graph(e, &ex))) return rc;
+        for (int64_t q = 0; q < k; ++q)
+          if (cudaGraphLaunch(ex, st) != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble_steps: graph launch");
+      }
+      if (!e->walk)
+        for (int r = 0; r < e->n; ++r)
+          for (int64_t q = 0; q < k; ++q) {
+            e->h_runs[r].step += 1;
+            e->h_runs[r].l += e->h_runs[r].inc_l;
+          }
       nsteps -= k;
       continue;
     }
@@ -1071,17 +1118,24 @@ int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choic
   cudaEventCreate(&t1);
   double best = 1e300;
   int pick = 0;
-  for (int k = 0; k < 3; ++k) {
-    // without the advance kernel a launch recomputes the same step: the runs do not move
-    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->surr,
-                        e->ctx[0]->d_err, st);
+  // without advancing, a launch recomputes the same step: the runs do not move
+  // (k < 3: the per-step launches with tile order k; k >= 3: one-step
+  // persistent walks with tile order k - 3)
+  auto launch = [&](int k) {
+    if (k < 3)
+      return rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->surr,
+                                 e->ctx[0]->d_err, st);
+    return rs::launch_ensemble_walk(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k - 3], e->ntiles, 1, e->d_lv,
+                                    false, e->surr, e->d_bar, e->ctx[0]->d_err, st);
+  };
+  if (ens_walk_l(e, 1, st)) return fail(RS_E_CUDA, "rs_ensemble_autotune: state upload failed");
+  for (int k = 0; k < 6; ++k) {
+    bool bad = launch(k) != 0;
     cudaEventRecord(t0, st);
-    for (int q = 0; q < reps; ++q)
-      rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->surr,
-                          e->ctx[0]->d_err, st);
+    for (int q = 0; q < reps && !bad; ++q) bad = launch(k) != 0;
     cudaEventRecord(t1, st);
     float ms = 0.f;
-    if (cudaEventSynchronize(t1) != cudaSuccess || cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) {
+    if (bad || cudaEventSynchronize(t1) != cudaSuccess || cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) {
       cudaEventDestroy(t0);
       cudaEventDestroy(t1);
       return fail(RS_E_CUDA, "rs_ensemble_autotune: timing failed");
@@ -1095,9 +1149,17 @@ int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choic
   }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
-  e->choice = pick;
+  e->choice = pick % 3;
+  e->walk = pick >= 3;
   if (choice) *choice = pick;
   return cuda_check("rs_ensemble_autotune");
+}
+
+int rs_ensemble_set_path(rs_ens *e, int32_t path) {
+  if (!e || path < 0 || path > 5) return fail(RS_E_INVALID, "rs_ensemble_set_path: path 0..5");
+  e->choice = path % 3;
+  e->walk = path >= 3;
+  return RS_OK;
 }
 
 // Host build of the Ti-Nb evaluator (fun.cu:1671-1720) from the same

@@ -33,5 +33,12 @@ struct alignas(64) EnsRun {
 // surr: every run evaluates its cells through its surrogate (all runs have one)
 int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
                     bool advance, bool surr, int *err, cudaStream_t st);
+// the persistent walk: nsteps steps of every run in one cooperative launch;
+// lv[s * nruns + r]: l_offset_Vp of run r at step s of the launch (s = 0 ..
+// nsteps); bar: two device counters (grid barrier, tile tickets), cleared here
+// before the launch; 0 on success
+int launch_ensemble_walk(EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
+                         int nsteps, const double *lv, bool advance, bool surr, unsigned *bar, int *err,
+                         cudaStream_t st);
 
 }  // namespace rs

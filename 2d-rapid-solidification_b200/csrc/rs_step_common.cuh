@@ -301,6 +301,40 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+__device__ __forceinline__ void mbar_inval(uint64_t *bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Grid-wide barrier of a cooperative launch (every CTA resident): each CTA
+// adds 1 to *bar (cleared before the launch) and waits until it reaches
+// target, the barrier's ordinal times gridDim.x.  Thread 0 releases the CTA's
+// prior writes (including completed bulk async stores) before it arrives and,
+// once through, orders them before the CTA's later TMA loads (proxy fence).
+// The wait is bounded: after `limit` polls it sets *err = 3 and the CTA's
+// threads all get false.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned target, int *err, uint32_t limit) {
+  __syncthreads();
+  int ok = 1;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(bar, 1u);
+    uint32_t tries = 0;
+    while (true) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+      if (v >= target) break;
+      if (++tries >= limit) {
+        atomicExch(err, 3);
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
 // L2 prefetch of the box a tma_load_2d at (x, y) would copy (no shared memory,
 // no barrier; the same 16-byte alignment of x as the load)
 __device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap *map, int x, int y) {

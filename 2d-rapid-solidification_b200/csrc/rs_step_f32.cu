@@ -136,9 +136,9 @@ __device__ __forceinline__ void bulk_store(void *gdst, const void *ssrc, uint32_
 // groups are rounded to FP32); K + C0 of the next column comes from the
 // neighbouring thread, so blocks overlap by one column and write 127 entries.
 constexpr int kTabBlock = 128;
+// kc: kTabBlock doubles of shared scratch
 __device__ __forceinline__ void table_block(const StepCoef &K, const double d0, const double d1, const int len,
-                                            float *__restrict__ tab, const int blk) {
-  __shared__ double kc[kTabBlock];
+                                            float *__restrict__ tab, const int blk, double *kc) {
   const int k = blk * (kTabBlock - 1) + threadIdx.x;  // table entry; column k - 4
   const int gi = min(max(k - 4, 0), K.nx - 1);
   const double T = (d0 + d1 * gi) * K.deltaT0 + K.Tmelt;  // get_delta, fun.cu:1610-1619
@@ -159,7 +159,8 @@ __global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef 
                                                                  const int len, float *__restrict__ tab) {
   // the tile kernel may start now; it waits for this grid before reading tab
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  table_block(K, d0, d1, len, tab, blockIdx.x);
+  __shared__ double kc[kTabBlock];
+  table_block(K, d0, d1, len, tab, blockIdx.x, kc);
 }
 
 // SURR: mu'' and the driving force of in-box cells that are not bulk melt
@@ -841,8 +842,8 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
 // d0 of the frozen temperature line, evaluated in the order rs_step uses on
 // the host (no contraction), so an ensemble run matches the same run stepped
 // alone bit for bit
-__device__ __forceinline__ double ens_d0(const EnsRun &R) {
-  double t = __dmul_rn(R.GG, __dsub_rn(R.l, R.l_init));
+__device__ __forceinline__ double ens_d0(const EnsRun &R, const double l) {
+  double t = __dmul_rn(R.GG, __dsub_rn(l, R.l_init));
   t = __dmul_rn(t, R.S);
   t = __dmul_rn(t, R.W0);
   t = __ddiv_rn(t, R.deltaT0);
@@ -855,7 +856,8 @@ __global__ void __launch_bounds__(kTabBlock) ens_table_kernel(const EnsRun *__re
   const int32_t e = tblk[blockIdx.x];
   const EnsRun &R = runs[e >> 16];
   if (!R.active) return;
-  table_block(R.K, ens_d0(R), R.d1, R.tab_len, R.tab, e & 0xFFFF);
+  __shared__ double kc[kTabBlock];
+  table_block(R.K, ens_d0(R, R.l), R.d1, R.tab_len, R.tab, e & 0xFFFF, kc);
 }
 
 template <bool SURR>
@@ -868,7 +870,7 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
   StepScalars PS;
   memset(&PS, 0, sizeof(PS));
   PS.step = R.step;
-  PS.d0 = ens_d0(R);
+  PS.d0 = ens_d0(R, R.l);
   PS.d1 = R.d1;
   const SurrArgs none = {};
   // the tile of the block launched `wave` (CTAs resident at once) positions
@@ -892,6 +894,100 @@ __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
   if (r >= nruns || !runs[r].active) return;
   runs[r].step += 1;
   runs[r].l += runs[r].inc_l;
+}
+
+// The persistent walk: one cooperative launch for nsteps steps of every run.
+// Per step the CTAs compute the runs' column tables (table blocks b, b + G,
+// ...), meet at a grid barrier, step the tiles b, b + G, ... of the order
+// with tile_body, wait for their bulk stores to complete, and meet again.  A
+// run's state at step s of the launch is step + s and l = lv[s * nruns + r],
+// which the host fills by the additions of inc_l that ens_advance_kernel
+// makes, so every tile computes what the per-step launches compute, bit for
+// bit.  The barriers are bounded: one that gives up sets *err; a CTA that
+// sees *err set stops working but keeps arriving at the barriers, so the
+// others do not wait out their limits.  advance: at the end (block 0, after
+// the last barrier) the runs move on to step + nsteps and l = lv[nsteps *
+// nruns + r].
+constexpr uint32_t kWalkBarrierLimit = 1u << 22;
+
+template <bool SURR>
+__global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
+    ens_walk_kernel(EnsRun *__restrict__ runs, const int nruns, const int32_t *__restrict__ tblk, const int ntblk,
+                    const int32_t *__restrict__ order, const int ntiles, const int nsteps,
+                    const double *__restrict__ lv, const int advance, unsigned *bar, int *err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
+  const unsigned G = gridDim.x;
+  unsigned target = 0;
+  bool dead = false;
+  const SurrArgs none = {};
+  auto l_at = [&](int r, int s) { return lv[(int64_t)s * nruns + r]; };
+  for (int s = 0; s < nsteps; ++s) {
+    if (!dead)
+      for (int i = blockIdx.x; i < ntblk; i += G) {
+        const int32_t e = tblk[i];
+        const EnsRun &R = runs[e >> 16];
+        if (R.active) table_block(R.K, ens_d0(R, l_at(e >> 16, s)), R.d1, R.tab_len, R.tab, e & 0xFFFF,
+                                  reinterpret_cast<double *>(smem_raw));
+        __syncthreads();  // the scratch is reused by the next block
+      }
+    target += G;
+    if (!grid_barrier(bar, target, err, kWalkBarrierLimit)) dead = true;
+    // tiles are handed out by a ticket counter (bar[1]): a CTA takes the next
+    // tile of the order when it finishes one, so the step ends when the
+    // work does, whatever the tiles cost; each CTA takes one ticket past the
+    // last tile per step, so step s's tickets start at s (ntiles + G)
+    const unsigned t0 = (unsigned)s * ((unsigned)ntiles + G);
+    while (!dead) {
+      __shared__ int tk;
+      if (threadIdx.x == 0) tk = (int)(atomicAdd(bar + 1, 1u) - t0);
+      __syncthreads();
+      const int i = tk;
+      __syncthreads();  // every thread has read the ticket
+      if (i < 0 || i >= ntiles) break;  // (i < 0 only after an error left tickets untaken)
+      {
+        const int32_t e = order[i];
+        const EnsRun &R = runs[e >> 16];
+        if (!R.active) continue;  // (every thread: the run is the same)
+        const int t = e & 0xFFFF;
+        const int64_t step = R.step + s;
+        const int par = (int)(step & 1);
+        StepScalars PS;
+        memset(&PS, 0, sizeof(PS));
+        PS.step = step;
+        PS.d0 = ens_d0(R, l_at(e >> 16, s));
+        PS.d1 = R.d1;
+        // L2 prefetch of this CTA's next tile of the step (as the per-step
+        // launch prefetches the tile one resident wave later)
+        auto prefetch = [&]() {
+          const int i2 = i + (int)G;
+          if (i2 >= ntiles) return;
+          const int32_t e2 = order[i2];
+          const EnsRun &R2 = runs[e2 >> 16];
+          if (!R2.active) return;
+          const int t2 = e2 & 0xFFFF, p2 = (int)((R2.step + s) & 1);
+          tma_prefetch_2d(&R2.map_psi[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
+          tma_prefetch_2d(&R2.map_c[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
+        };
+        tile_body<SURR>(R.K, R.F, PS, &R.map_psi[par], &R.map_c[par], R.tab, R.tab_len, R.psi[par ^ 1],
+                        R.c[par ^ 1], nullptr, nullptr, err, SURR ? R.surr : none, t % R.nrt, t / R.nrt, nullptr,
+                        prefetch);
+        __syncthreads();  // every thread is done with the tile's barrier and shared memory
+        if (threadIdx.x == 0) mbar_inval(&sm.full);
+        if (__syncthreads_or(*(volatile int *)err != 0)) dead = true;
+      }
+    }
+    // the bulk stores of this step complete before the barrier releases them
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    target += G;
+    if (!grid_barrier(bar, target, err, kWalkBarrierLimit)) dead = true;
+  }
+  if (advance && blockIdx.x == 0 && !dead)
+    for (int r = threadIdx.x; r < nruns; r += blockDim.x)
+      if (runs[r].active) {
+        runs[r].l = l_at(r, nsteps);
+        runs[r].step += nsteps;
+      }
 }
 
 
@@ -1526,6 +1622,37 @@ int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntbl
   ens_table_kernel<<<ntblk, kTabBlock, 0, st>>>(runs, tblk);
   kfn<<<ntiles, kThreads, smem, st>>>(runs, order, err, wave);
   if (advance) ens_advance_kernel<<<(nruns + 63) / 64, 64, 0, st>>>(const_cast<EnsRun *>(runs), nruns);
+  return 0;
+}
+
+int launch_ensemble_walk(EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
+                         int nsteps, const double *lv, bool advance, bool surr, unsigned *bar, int *err,
+                         cudaStream_t st) {
+  if (nsteps <= 0) return 0;
+  const size_t smem = sizeof(TileSmem);
+  static_assert(sizeof(TileSmem) >= kTabBlock * sizeof(double), "table scratch fits the tile's shared memory");
+  auto kfn = surr ? ens_walk_kernel<true> : ens_walk_kernel<false>;
+  static std::atomic<unsigned long long> attr_done[2];
+  if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr])) return -3;
+  static std::atomic<int> res_of[2][64];
+  const int res = resident_ctas((const void *)kfn, kThreads, smem, res_of[surr]);
+  if (res <= 0) return -3;
+  const int grid = std::max(1, std::min(res, std::max(ntiles, ntblk)));
+  if (cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return -2;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  const int adv = advance ? 1 : 0;
+  if (cudaLaunchKernelEx(&cfg, kfn, runs, nruns, tblk, ntblk, order, ntiles, nsteps, lv, adv, bar, err) !=
+      cudaSuccess)
+    return -2;
   return 0;
 }
 

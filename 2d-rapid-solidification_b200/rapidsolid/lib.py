@@ -80,6 +80,7 @@ def load():
         "rs_ensemble_steps": ([vp, i64, vp], C.c_int),
         "rs_ensemble_state": ([vp, i32, vp, vp, vp, vp], C.c_int),
         "rs_ensemble_autotune": ([vp, i32, vp, vp, vp], C.c_int),
+        "rs_ensemble_set_path": ([vp, i32], C.c_int),
         "rs_surrogate_audit": ([vp, vp, vp, vp, vp, vp], C.c_int),
         "rs3_default_params": ([vp], C.c_int),
         "rs3_sizeof_params": ([], sz),
@@ -343,11 +344,17 @@ class Ensemble:
         return st.value, h.value, l.value, self.sets[run][cur.value]
 
     def autotune(self, reps=5, stream=None):
-        """(choice, [mean ms of the three tile orders])."""
-        ms = (C.c_double * 3)()
+        """(path, [mean ms of one step on the six paths]): paths 0-2 per-step
+        launches (graph replays) with tile orders run by run, largest first,
+        interleaved; 3-5 the persistent walk with the same orders."""
+        ms = (C.c_double * 6)()
         ch = C.c_int32()
         check(self.lib.rs_ensemble_autotune(self._h, reps, ms, C.byref(ch), _stream(stream)))
         return ch.value, list(ms)
+
+    def set_path(self, path):
+        """select a stepping path (0..5, as autotune numbers them)"""
+        check(self.lib.rs_ensemble_set_path(self._h, path))
 
     def close(self):
         for c in self.ctx:

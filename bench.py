@@ -817,6 +817,12 @@ def _ensemble_tips(ens, runs):
     return xs
 
 
+# the ensemble's stepping paths (rs_ensemble_autotune): per-step launches replayed
+# from a CUDA graph, or the persistent walk, each with three tile orders
+ENS_PATHS = ["graph, run by run", "graph, largest first", "graph, interleaved", "walk, run by run",
+             "walk, largest first", "walk, interleaved"]
+
+
 def _timed_ensemble(ens, flush, nsteps):
     import torch
     ens.steps(3)  # step 0 pulls every run back (eager), then graph replays
@@ -833,7 +839,9 @@ def _timed_ensemble(ens, flush, nsteps):
 def ensemble_leg(flush, nruns=64, nsteps=100, vel_steps=4000):
     """The batched ensemble of uneven runs (64 Ti-Nb runs, sizes 256^2 ..
     1024x2048, V 0.01-2 m/s, G 1e5-1e7 K/m, x_Nb 0.05-0.20, seeded): aggregate
-    Gcell-steps/s of the one-launch, graph-replayed step, exact FP32 and
+    Gcell-steps/s of the batched step (per-step launches replayed from a
+    CUDA graph, or the persistent walk, as the autotuner picks; both timed
+    with its tile order), exact FP32 and
     through the learned surrogate (one network trained on a box that spans
     every run's compositions and temperatures), against the same runs stepped
     one rs_step at a time; per-run tip velocity of the surrogate ensemble
@@ -849,8 +857,14 @@ def ensemble_leg(flush, nruns=64, nsteps=100, vel_steps=4000):
     choice, tune_ms = ens.autotune(reps=5)
     ms = _timed_ensemble(ens, flush, nsteps)
     out["exact"] = {"value": round(cells * nsteps / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms / nsteps, 5),
-                    "autotune": {"choice": ["run by run", "largest first", "interleaved"][choice],
-                                 "ms_per_launch": [round(x, 5) for x in tune_ms]}}
+                    "autotune": {"choice": ENS_PATHS[choice], "ms_per_step_of_path": [round(x, 5) for x in tune_ms]}}
+    # the two stepping paths with the autotuned tile order
+    for name, path in (("graph", choice % 3), ("walk", 3 + choice % 3)):
+        ens.set_path(path)
+        msp = _timed_ensemble(ens, flush, nsteps)
+        out["exact"]["path_" + name] = {"value": round(cells * nsteps / (msp * 1e-3) / 1e9, 3),
+                                        "ms_per_step": round(msp / nsteps, 5)}
+    ens.set_path(choice)
     # the same runs one by one (two launches per run and step)
     ctxs = [ens.ctx[r] for r in range(nruns)]
     cur = [ens.state(r)[3] for r in range(nruns)]
@@ -873,8 +887,8 @@ def ensemble_leg(flush, nruns=64, nsteps=100, vel_steps=4000):
     choice, tune_ms = ens.autotune(reps=5)
     ms = _timed_ensemble(ens, flush, nsteps)
     out["surrogate"] = {"value": round(cells * nsteps / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms / nsteps, 5),
-                        "autotune": {"choice": ["run by run", "largest first", "interleaved"][choice],
-                                     "ms_per_launch": [round(x, 5) for x in tune_ms]},
+                        "autotune": {"choice": ENS_PATHS[choice],
+                                     "ms_per_step_of_path": [round(x, 5) for x in tune_ms]},
                         "box": {"T": [round(box.T_lo, 2), round(box.T_hi, 2)], "c": [box.c_lo, box.c_hi]}}
     ens.close()
     # per-run tip velocity over the second half of vel_steps: the surrogate

@@ -379,10 +379,18 @@ int rs_ensemble_steps(rs_ens *e, int64_t nsteps, rs_stream_t stream);
 /* a run's step, i_offset_history, l_offset_Vp and current set (0 = A, 1 = B) */
 int rs_ensemble_state(rs_ens *e, int32_t run, int64_t *step, int32_t *i_offset_history, double *l_offset_Vp,
                       int32_t *current);
-/* Times the tile orders (0 run by run, 1 largest runs first, 2 runs
- * interleaved) over reps launches without advancing the runs, keeps the
- * fastest; ms_out[3] receives the mean launch times. */
+/* Times the stepping paths over reps launches of one step without advancing
+ * the runs and keeps the fastest: paths 0-2 launch the column tables and the
+ * tiles per step (replayed from a CUDA graph) with the tile order 0 run by
+ * run, 1 largest runs first, 2 runs interleaved; paths 3-5 are the same
+ * orders as the persistent walk, one cooperative launch per stretch of steps
+ * without a pull-back (device-side grid barriers between the tables and the
+ * tiles of a step and between steps, bounded: one that gives up sets the
+ * status rs_device_status reports on run 0's context).  ms_out[6] receives
+ * the mean times, *choice the path. */
 int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choice, rs_stream_t stream);
+/* selects a stepping path (0..5, as rs_ensemble_autotune numbers them) */
+int rs_ensemble_set_path(rs_ens *e, int32_t path);
 
 /* ---- 3D three-phase variant (one GPU) ----
  * The reference's 3D peritectic model, multi/peritectic_multiGPU/TiAg.cu:

@@ -1,6 +1,8 @@
 """Batched ensemble (rs_ensemble_*): runs of uneven size stepped by one
-launch, pull-back-free stretches replayed from a CUDA graph, must equal the
-same runs stepped one by one through rs_step, bit for bit."""
+launch, pull-back-free stretches replayed from a CUDA graph or taken by one
+persistent launch (device-side grid barriers between tables and tiles and
+between steps), must equal the same runs stepped one by one through rs_step,
+bit for bit."""
 import numpy as np
 import pytest
 
@@ -45,7 +47,8 @@ def single(p, sur=None):
     return a.psi.cpu().numpy(), a.c.cpu().numpy(), hist, l
 
 
-def test_ensemble_equals_single_runs():
+@pytest.mark.parametrize("path", ["autotuned", 0, 4])
+def test_ensemble_equals_single_runs(path):
     ps = params()
     ens = lib.Ensemble(ps)
     for r, p in enumerate(ps):
@@ -53,7 +56,9 @@ def test_ensemble_equals_single_runs():
         ens.ctx[r].initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, 7)
         ens.bind(r, a, b)
     choice, ms = ens.autotune(reps=3)
-    assert choice in (0, 1, 2) and all(m > 0 for m in ms)
+    assert choice in range(6) and len(ms) == 6 and all(m > 0 for m in ms)
+    if path != "autotuned":
+        ens.set_path(path)
     ens.steps(250)
     ens.steps(STEPS - 250)
     torch.cuda.synchronize()
@@ -65,10 +70,12 @@ def test_ensemble_equals_single_runs():
         assert hist == hist1 and l == l1
         assert np.array_equal(cur.psi.cpu().numpy(), psi), r
         assert np.array_equal(cur.c.cpu().numpy(), c), r
+    ens.ctx[0].device_status()
     ens.close()
 
 
-def test_ensemble_surrogate_path_equals_single_runs():
+@pytest.mark.parametrize("path", [1, 5])
+def test_ensemble_surrogate_path_equals_single_runs(path):
     """With a network set on every run's context, the batched launch takes
     the surrogate path of the tile kernel: each run equals the same run
     stepped alone through rs_step with the same network, bit for bit."""
@@ -80,6 +87,7 @@ def test_ensemble_surrogate_path_equals_single_runs():
         ens.ctx[r].initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, 7)
         ens.ctx[r].set_surrogate(w, box)
         ens.bind(r, a, b)
+    ens.set_path(path)
     ens.steps(STEPS)
     torch.cuda.synchronize()
     for r, p in enumerate(ps):
