@@ -1020,7 +1020,8 @@ int rs_ensemble_steps(rs_ens *e, int64_t nsteps, rs_stream_t stream) {
           const int64_t kq = std::min(kMaxWalk, k - q);
           if (ens_walk_l(e, kq, st) ||
               rs::launch_ensemble_walk(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles,
-                                       (int)kq, e->d_lv, true, e->surr, e->d_bar, e->ctx[0]->d_err, st))
+                                       (int)kq, e->d_lv, true, e->surr, e->d_bar, e->ctx[0]->d_err,
+                                       e->ctx[0]->wait_limit, st))
             return fail(RS_E_CUDA, "rs_ensemble_steps: persistent launch failed");
           for (int r = 0; r < e->n; ++r)  // the mirror follows (the next chunk starts from it)
             for (int64_t s2 = 0; s2 < kq; ++s2) {
@@ -1126,7 +1127,7 @@ int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choic
       return rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->surr,
                                  e->ctx[0]->d_err, st);
     return rs::launch_ensemble_walk(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k - 3], e->ntiles, 1, e->d_lv,
-                                    false, e->surr, e->d_bar, e->ctx[0]->d_err, st);
+                                    false, e->surr, e->d_bar, e->ctx[0]->d_err, 0, st);
   };
   if (ens_walk_l(e, 1, st)) return fail(RS_E_CUDA, "rs_ensemble_autotune: state upload failed");
   for (int k = 0; k < 6; ++k) {

@@ -37,8 +37,9 @@ int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntbl
 // lv[s * nruns + r]: l_offset_Vp of run r at step s of the launch (s = 0 ..
 // nsteps); bar: two device counters (grid barrier, tile tickets), cleared here
 // before the launch; 0 on success
+// barrier_limit: polls of a grid-barrier wait before it gives up (0: the default)
 int launch_ensemble_walk(EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
                          int nsteps, const double *lv, bool advance, bool surr, unsigned *bar, int *err,
-                         cudaStream_t st);
+                         uint32_t barrier_limit, cudaStream_t st);
 
 }  // namespace rs

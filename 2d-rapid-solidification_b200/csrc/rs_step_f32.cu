@@ -914,7 +914,8 @@ template <bool SURR>
 __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
     ens_walk_kernel(EnsRun *__restrict__ runs, const int nruns, const int32_t *__restrict__ tblk, const int ntblk,
                     const int32_t *__restrict__ order, const int ntiles, const int nsteps,
-                    const double *__restrict__ lv, const int advance, unsigned *bar, int *err) {
+                    const double *__restrict__ lv, const int advance, unsigned *bar, int *err,
+                    const uint32_t barrier_limit) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
   const unsigned G = gridDim.x;
@@ -932,7 +933,7 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
         __syncthreads();  // the scratch is reused by the next block
       }
     target += G;
-    if (!grid_barrier(bar, target, err, kWalkBarrierLimit)) dead = true;
+    if (!grid_barrier(bar, target, err, barrier_limit)) dead = true;
     // tiles are handed out by a ticket counter (bar[1]): a CTA takes the next
     // tile of the order when it finishes one, so the step ends when the
     // work does, whatever the tiles cost; each CTA takes one ticket past the
@@ -980,7 +981,7 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
     // the bulk stores of this step complete before the barrier releases them
     asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     target += G;
-    if (!grid_barrier(bar, target, err, kWalkBarrierLimit)) dead = true;
+    if (!grid_barrier(bar, target, err, barrier_limit)) dead = true;
   }
   if (advance && blockIdx.x == 0 && !dead)
     for (int r = threadIdx.x; r < nruns; r += blockDim.x)
@@ -1627,7 +1628,7 @@ int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntbl
 
 int launch_ensemble_walk(EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
                          int nsteps, const double *lv, bool advance, bool surr, unsigned *bar, int *err,
-                         cudaStream_t st) {
+                         uint32_t barrier_limit, cudaStream_t st) {
   if (nsteps <= 0) return 0;
   const size_t smem = sizeof(TileSmem);
   static_assert(sizeof(TileSmem) >= kTabBlock * sizeof(double), "table scratch fits the tile's shared memory");
@@ -1650,7 +1651,8 @@ int launch_ensemble_walk(EnsRun *runs, int nruns, const int32_t *tblk, int ntblk
   cfg.attrs = at;
   cfg.numAttrs = 1;
   const int adv = advance ? 1 : 0;
-  if (cudaLaunchKernelEx(&cfg, kfn, runs, nruns, tblk, ntblk, order, ntiles, nsteps, lv, adv, bar, err) !=
+  const uint32_t lim = barrier_limit ? barrier_limit : kWalkBarrierLimit;
+  if (cudaLaunchKernelEx(&cfg, kfn, runs, nruns, tblk, ntblk, order, ntiles, nsteps, lv, adv, bar, err, lim) !=
       cudaSuccess)
     return -2;
   return 0;

@@ -186,7 +186,9 @@ int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
  * tries) bounds the tile kernels' waits for their TMA loads; when set, a wait
  * polls without suspending and gives up after that many polls.  A tile whose
  * wait gives up is not computed or stored, and rs_device_status reports
- * RS_E_STATE.  Tests set it to 1 to run that path.
+ * RS_E_STATE.  Tests set it to 1 to run that path.  Set on run 0's context
+ * of an ensemble, it also bounds the persistent walk's grid-barrier waits
+ * (polls; default 2^22).
  * RS_OPT_PIPELINE (default 0) runs the tile step (FP64, and FP32 without a
  * surrogate) as a persistent kernel of warp roles (a TMA producer warp, a
  * phase-1 group and a flux/update/store group working on three tiles at

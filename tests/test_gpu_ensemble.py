@@ -98,3 +98,34 @@ def test_ensemble_surrogate_path_equals_single_runs(path):
         assert np.array_equal(cur.c.cpu().numpy(), c), r
         assert ens.ctx[r].surrogate_audit()[3] > 0  # the run's cells went through its network
     ens.close()
+
+
+def test_walk_barrier_that_gives_up_reports_and_ends():
+    """The persistent walk's grid barriers are bounded: with run 0's wait
+    limit at one poll, early arrivals give up at once (the others have not
+    arrived yet), the CTAs that gave up stop working but keep arriving, the
+    launch ends, rs_device_status reports RS_E_STATE, and the context stays
+    usable (a walk with the default limit then runs clean).  No fault and no
+    hang: every wait is a bounded poll."""
+    from rapidsolid import _abi
+    ps = params()[:3]
+    ens = lib.Ensemble(ps)
+    for r, p in enumerate(ps):
+        a, b = lib.FieldSet(p, torch.float32), lib.FieldSet(p, torch.float32)
+        ens.ctx[r].initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, 7)
+        ens.bind(r, a, b)
+    ens.set_path(3)
+    ens.steps(2)  # step 0 pulls every run back (eager), step 1 is a walk
+    torch.cuda.synchronize()
+    ens.ctx[0].device_status()
+    ens.ctx[0].set_option(_abi.RS_OPT_WAIT_LIMIT, 1)
+    ens.steps(5)
+    torch.cuda.synchronize()
+    with pytest.raises(lib.RsError) as e:
+        ens.ctx[0].device_status()
+    assert e.value.code == _abi.RS_E_STATE
+    ens.ctx[0].set_option(_abi.RS_OPT_WAIT_LIMIT, 0)
+    ens.steps(5)
+    torch.cuda.synchronize()
+    ens.ctx[0].device_status()
+    ens.close()
