@@ -41,7 +41,9 @@
 //     cell of the warp's row has |s| < 1/9 (truncation below 3.3e-17
 //     relative), else by the logarithm;
 //   * bulk melt rows (psi = -1 exactly, delta in the series range): g = -1,
-//     q = 1, so mu'' = -2 L0_Liq delta + RT lam and S = c (1 - c);
+//     q = 1, so mu'' = -2 L0_Liq delta + RT lam and S = c (1 - c); far-melt
+//     rows (|delta| <= 1e-3 min(cinf, 1-cinf) as well) take lam as its
+//     Taylor polynomial in delta (MeltPoly), without the division of s;
 //   * deep solid rows (psi = +1 over the 3x3 neighbourhoods) store
 //     S = mu'' = 0: every face weight touching them is 0;
 //   * face weights by pair sums (6 P_i + P_{i-1} + P_{i+1}, four times the
@@ -87,6 +89,31 @@ static_assert(64 + 2 * kTRin <= kThreads && 4 * kTR <= kThreads, "one thread per
 // column table arrays (kColTabFields of them, len doubles each); entry k
 // describes column k - 4
 enum { kTabRT = 0, kTabC0 = 1, kTabDK = 2, kTabAnb = 3, kTabAti = 4 };
+
+// The solute log term lam = log(c/(1-c)) - log(cinf/(1-cinf)) of a far-melt
+// cell as its Taylor polynomial in delta = c - cinf:
+//   lam = sum_k a_k delta^k,  a_k = ((-1)^(k-1) / cinf^k + 1 / (1-cinf)^k) / k.
+// With m = min(cinf, 1-cinf), |a_k| <= 2 / (k m^k), so for |delta| <= 1e-3 m
+// the terms beyond k = 6 sum to below 3e-19 of lam: the polynomial is the
+// function to FP64 rounding, with no division.  Far from the front the melt
+// sits within that bound of cinf (the solute boundary layer decays
+// exponentially ahead of the front), so most melt rows take this form.
+constexpr int kMeltTerms = 6;
+struct MeltPoly {
+  double a[kMeltTerms];  // a_1 .. a_6
+  double tiny;           // |delta| bound of the polynomial form
+};
+MeltPoly make_melt_poly(double cinf) {
+  MeltPoly M;
+  double pc = 1.0, pm = 1.0;
+  for (int k = 1; k <= kMeltTerms; ++k) {
+    pc /= cinf;
+    pm /= 1.0 - cinf;
+    M.a[k - 1] = ((k % 2 ? pc : -pc) + pm) / k;
+  }
+  M.tiny = 1e-3 * std::min(cinf, 1.0 - cinf);
+  return M;
+}
 
 // the input tile: TMA destinations (128-byte aligned); after phase 3 rows
 // 1..16 receive the new psi / c for the bulk stores
@@ -215,14 +242,16 @@ struct TileView {
   const StepCoef &K;
   const Coef<double> &F;
   const StepScalars &PS;
+  const MeltPoly &M;
   Tab T;
   int x0, y0;  // first output column, first output row (input rows y0-1 .. y0+kTR)
   int gw, lane, gtid;  // warp and lane within the group, thread of the group
   int col, gi, bc;     // the lane's first cell: tile column, global column, box column
   uint32_t outm;       // per cell of the lane: an interior (output) cell
-  __device__ TileView(const StepCoef &K_, const Coef<double> &F_, const StepScalars &PS_, const double *tab,
-                      int tab_len, int x0_, int y0_, int gtid_)
-      : K(K_), F(F_), PS(PS_), T(tab, tab_len), x0(x0_), y0(y0_), gw(gtid_ >> 5), lane(gtid_ & 31), gtid(gtid_) {
+  __device__ TileView(const StepCoef &K_, const Coef<double> &F_, const StepScalars &PS_, const MeltPoly &M_,
+                      const double *tab, int tab_len, int x0_, int y0_, int gtid_)
+      : K(K_), F(F_), PS(PS_), M(M_), T(tab, tab_len), x0(x0_), y0(y0_), gw(gtid_ >> 5), lane(gtid_ & 31),
+        gtid(gtid_) {
     col = 2 * lane;
     gi = x0 + col;
     bc = col + 4;
@@ -302,7 +331,20 @@ __device__ __forceinline__ void phase1(const TileView &V, const InSlot &in, StSl
     const bool liq2 = b0 == kMinus1 && b1 == kMinus1;
     const bool sol2 = b0 == kPlus1 && b1 == kPlus1;
     uint32_t code;
-    if (__all_sync(FULL, liq2 && fmax(dv[0], dv[1]) < d_hi && fmin(dv[0], dv[1]) > d_lo)) {
+    if (__all_sync(FULL, liq2 && fmax(fabs(dv[0]), fabs(dv[1])) <= V.M.tiny)) {
+      // far melt: g = -1, q = 1, lam by its Taylor polynomial in delta;
+      // mu'' = RT lam - 2 L0_Liq delta = delta (RT p + KL), lam = delta p
+      code = 1u;
+      st.pmask[rr][lane] = 0x03u;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        double p = V.M.a[kMeltTerms - 1];
+#pragma unroll
+        for (int k = kMeltTerms - 2; k >= 0; --k) p = fma(p, dv[q], V.M.a[k]);
+        Sv[q] = cv[q] * (1.0 - cv[q]);
+        mv[q] = dv[q] * fma(RTa[q], p, KL);
+      }
+    } else if (__all_sync(FULL, liq2 && fmax(dv[0], dv[1]) < d_hi && fmin(dv[0], dv[1]) > d_lo)) {
       // bulk melt: g = -1, q = 1
       code = 1u;
       st.pmask[rr][lane] = 0x03u;
@@ -701,7 +743,8 @@ __global__ void __launch_bounds__(kThreads, 5)
                     const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
                     const __grid_constant__ CUtensorMap tm_c, const double *__restrict__ tab, const int tab_len,
                     double *__restrict__ psi_n, double *__restrict__ c_n, double *__restrict__ phi_n,
-                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int wave) {
+                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR,
+                    const __grid_constant__ MeltPoly MP, const int wave) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TileSmem64 &sm = *reinterpret_cast<TileSmem64 *>(smem_raw);
   // blockIdx.x walks the tile rows of one tile column, blockIdx.y the tile
@@ -729,7 +772,7 @@ __global__ void __launch_bounds__(kThreads, 5)
   }
   // the column table of this step (programmatic dependency on its kernel)
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  const TileView V(K, F, PS, tab, tab_len, x0, y0, (int)threadIdx.x);
+  const TileView V(K, F, PS, MP, tab, tab_len, x0, y0, (int)threadIdx.x);
   __syncthreads();  // barrier initialised, flags cleared
   {
     // bounded wait for the tile; if any thread gives up, the whole CTA skips
@@ -823,8 +866,8 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
                     const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
                     const __grid_constant__ CUtensorMap tm_c, const double *__restrict__ tab, const int tab_len,
                     double *__restrict__ psi_n, double *__restrict__ c_n, double *__restrict__ phi_n,
-                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int nrt,
-                    const int ncb) {
+                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR,
+                    const __grid_constant__ MeltPoly MP, const int nrt, const int ncb) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   PipeSmem64 &sm = *reinterpret_cast<PipeSmem64 *>(smem_raw);
   const int warp = threadIdx.x >> 5;
@@ -890,7 +933,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
       if (!group_and(ok, kBarP1)) break;
       int tr, tc;
       tile_of(t, nrt, ncb, f, tr, tc);
-      const TileView V(K, F, PS, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
+      const TileView V(K, F, PS, MP, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
       if (gtid == 0) {
         sm.st[q].liq = 0u;
         sm.st[q].sol = 0u;
@@ -911,7 +954,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
     if (!group_and(pipe_wait(&sm.st_full[q], (k / kStage) & 1, abort, limit, err, poll), kBarP2)) break;
     int tr, tc;
     tile_of(t, nrt, ncb, f, tr, tc);
-    const TileView V(K, F, PS, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
+    const TileView V(K, F, PS, MP, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
     BlockPartial *part = partials ? partials + ((int64_t)tc * nrt + tr) : nullptr;
     const bool red = part != nullptr;
     if (gtid == 0) sm.p2.nlist = 0;
@@ -969,6 +1012,7 @@ int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScal
   cfg.attrs = at;
   cfg.numAttrs = 1;
   const double *tab = tm.col_tab64;
+  const MeltPoly mp = make_melt_poly(F.cinf);
   FinalRed fr = tm.red;
   fr.partials = partials;
   fr.nparts = nparts;
@@ -979,13 +1023,13 @@ int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScal
     cfg.gridDim = dim3((unsigned)std::min(resident, nparts));
     cfg.blockDim = dim3(kPipeThreads);
     e = cudaLaunchKernelEx(&cfg, pipe_kernel_f64, K, F, P, tm.psi, tm.c, tab, tm.col_tab64_len, psi_n, c_n, phi_n,
-                           partials, err, fr, nrt, ncb);
+                           partials, err, fr, mp, nrt, ncb);
   } else {
     // column-major: consecutive CTAs share a column strip and its halo rows in L2
     cfg.gridDim = dim3(nrt, ncb);
     cfg.blockDim = dim3(kThreads);
     e = cudaLaunchKernelEx(&cfg, tile_kernel_f64, K, F, P, tm.psi, tm.c, tab, tm.col_tab64_len, psi_n, c_n, phi_n,
-                           partials, err, fr, resident);
+                           partials, err, fr, mp, resident);
   }
   if (e != cudaSuccess) return -3;
   if (nparts_out) *nparts_out = nparts;

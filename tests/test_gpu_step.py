@@ -92,6 +92,42 @@ def test_f64_series_rows_match_oracle_log_form():
     assert maxabs(g.psi, o.psi) <= 1e-13 and maxabs(g.c, o.c) <= 1e-13
 
 
+def test_f64_far_melt_rows_match_oracle_log_form():
+    """Far-melt rows (psi = -1 and |c - cinf| <= 1e-3 min(cinf, 1 - cinf) on
+    every cell of the warp's row) take the solute log term as its Taylor
+    polynomial in c - cinf.  A melt whose solute noise grows along the
+    growth axis from 1e-12 to 1e-3 (so warp rows fall on the polynomial, on
+    the atanh series and on the logarithm), with exact zeros in part of it,
+    gives one step and twenty steps within the tolerances of the oracle's
+    logarithm."""
+    p = make("default", 256, 64)
+    d = pyoracle.derive(p)
+    s = perturbed_state(p, 31, amp=0.2)
+    rng = np.random.default_rng(31)
+    liquid = s.psi < -0.999
+    i = np.arange(p.nx_all)[None, :]
+    amp = 10.0 ** (-12.0 + 9.0 * i / p.nx_all)
+    noise = amp * rng.standard_normal(s.c.shape)
+    noise[:, 200:230] = 0.0
+    s.c[:] = np.where(liquid, p.cinf + noise, s.c)
+    fix_ghosts(p, s)
+    tiny = 1e-3 * min(p.cinf, 1 - p.cinf)
+    far = liquid & (np.abs(s.c - p.cinf) <= tiny)
+    assert far.mean() > 0.3 and (liquid & ~far).any()
+    ctx = lib.Context(p)
+    cur, nxt = upload(p, s), lib.FieldSet(p, torch.float64)
+    ctx.step(cur, nxt, 0)
+    o = pyoracle.step(p, d, s, 0)
+    g = download(p, nxt)
+    assert maxabs(g.psi, o.psi) <= 1e-13 and maxabs(g.c, o.c) <= 1e-13
+    for n in range(1, 20):
+        ctx.step(nxt, cur, n)
+        cur, nxt = nxt, cur
+        o = pyoracle.step(p, d, o, n)
+    g = download(p, nxt)
+    assert maxabs(g.psi, o.psi) <= 1e-12 and maxabs(g.c, o.c) <= 1e-12
+
+
 def test_rotated_orientation_f64():
     p = make("default")
     a, b, gm = np.radians([20.0, 10.0, 35.0])
