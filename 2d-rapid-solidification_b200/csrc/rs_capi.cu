@@ -98,26 +98,31 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // 2D tiled descriptor of one field (row pitch = nx_all elements), box of
 // kTmaBoxW32/64 x kTmaBoxH elements, zero fill outside the array.  Returns false
 // when TMA cannot be used (alignment, driver entry point).
+// box_rows: the box height (input rows of a tile)
+bool encode_map(const rs_params &p, const void *ptr, int precision, int box_rows, CUtensorMap *out) {
+  auto enc = encode_fn();
+  const size_t es = precision == RS_F64 ? 8 : 4;
+  const uint64_t row_bytes = (uint64_t)p.nx_all * es;
+  if (!enc || ((uintptr_t)ptr % 16) || (row_bytes % 16)) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)p.nx_all, (cuuint64_t)p.ny_all};
+  cuuint64_t strides[1] = {row_bytes};
+  cuuint32_t box[2] = {(cuuint32_t)(precision == RS_F64 ? rs::kTmaBoxW64 : rs::kTmaBoxW32), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(out, precision == RS_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         2, const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 bool field_map(rs_ctx *c, const void *ptr, int precision, CUtensorMap *out) {
   for (int k = 0; k < c->tma_n; ++k)
     if (c->tma[k].ptr == ptr && c->tma[k].precision == precision) {
       *out = c->tma[k].map;
       return true;
     }
-  auto enc = encode_fn();
-  const size_t es = precision == RS_F64 ? 8 : 4;
-  const uint64_t row_bytes = (uint64_t)c->p.nx_all * es;
-  if (!enc || ((uintptr_t)ptr % 16) || (row_bytes % 16)) return false;
-  cuuint64_t dims[2] = {(cuuint64_t)c->p.nx_all, (cuuint64_t)c->p.ny_all};
-  cuuint64_t strides[1] = {row_bytes};
-  cuuint32_t box[2] = {(cuuint32_t)(precision == RS_F64 ? rs::kTmaBoxW64 : rs::kTmaBoxW32), (cuuint32_t)rs::kTmaBoxH};
-  cuuint32_t estr[2] = {1, 1};
   CUtensorMap m;
-  const CUresult r = enc(&m, precision == RS_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
-                         const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return false;
+  if (!encode_map(c->p, ptr, precision, rs::kTmaBoxH, &m)) return false;
   TmaEntry &e = c->tma[c->tma_next];
   e.ptr = ptr;
   e.precision = precision;
@@ -491,6 +496,35 @@ int rs_set_option(rs_ctx *c, int32_t option, int64_t value) {
   }
 }
 
+int rs_host_alloc(size_t bytes, void **host, void **device) {
+  if (!host || !device || !bytes) return fail(RS_E_INVALID, "rs_host_alloc: bad argument");
+  *host = *device = nullptr;
+  void *h = nullptr, *d = nullptr;
+  cudaError_t e = cudaHostAlloc(&h, bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+  if (e == cudaSuccess) {
+    e = cudaHostGetDevicePointer(&d, h, 0);
+    if (e != cudaSuccess) cudaFreeHost(h);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(RS_E_CUDA, "rs_host_alloc: %s", cudaGetErrorString(e));
+  }
+  memset(h, 0, bytes);
+  *host = h;
+  *device = d;
+  return RS_OK;
+}
+
+int rs_host_free(void *host) {
+  if (!host) return RS_OK;
+  const cudaError_t e = cudaFreeHost(host);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(RS_E_CUDA, "rs_host_free: %s", cudaGetErrorString(e));
+  }
+  return RS_OK;
+}
+
 int rs_device_status(rs_ctx *c, rs_stream_t stream) {
   if (!c) return fail(RS_E_INVALID, "rs_device_status: null ctx");
   int h = 0;
@@ -789,11 +823,12 @@ struct rs_ens {
   std::vector<int> bound;
   rs::EnsRun *h_runs = nullptr;  // pinned host mirror of the descriptors
   rs::EnsRun *d_runs = nullptr;
-  int32_t *d_tblk = nullptr, *d_order[3] = {nullptr, nullptr, nullptr};
-  int ntblk = 0, ntiles = 0, choice = 0;
+  // per tile shape: the three tile orders and the number of tiles
+  int32_t *d_tblk = nullptr, *d_order[rs::kTileShapes][3] = {};
+  int ntblk = 0, ntiles[rs::kTileShapes] = {}, choice = 0, shape = 0;
   bool ready = false;
   bool surr = false;  // every run steps through its learned surrogate
-  cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+  cudaGraphExec_t exec[rs::kTileShapes][3] = {};
   cudaStream_t cap = nullptr;
   int32_t *d_itip = nullptr, *h_itip = nullptr;
   bool walk = false;            // stretches without pull-back as one persistent launch (else graph replays)
@@ -839,31 +874,38 @@ int ens_prepare(rs_ens *e) {
   if (nsurr != 0 && nsurr != e->n)
     return fail(RS_E_UNSUPPORTED, "rs_ensemble: %d of %d runs have a surrogate: all or none", nsurr, e->n);
   e->surr = nsurr == e->n;
-  std::vector<int32_t> tblk, ord[3];
+  std::vector<int32_t> tblk;
   for (int r = 0; r < e->n; ++r) {
-    const rs::EnsRun &R = e->h_runs[r];
-    const int nb = (R.tab_len + 126) / 127;
+    const int nb = (e->h_runs[r].tab_len + 126) / 127;
     for (int b = 0; b < nb; ++b) tblk.push_back((r << 16) | b);
-    for (int t = 0; t < R.ntiles; ++t) ord[0].push_back((r << 16) | t);
   }
-  std::vector<int> by(e->n);
-  for (int r = 0; r < e->n; ++r) by[r] = r;
-  std::stable_sort(by.begin(), by.end(), [&](int a, int b) { return e->h_runs[a].ntiles > e->h_runs[b].ntiles; });
-  for (int r : by)
-    for (int t = 0; t < e->h_runs[r].ntiles; ++t) ord[1].push_back((r << 16) | t);
-  int tmax = 0;
-  for (int r = 0; r < e->n; ++r) tmax = std::max(tmax, e->h_runs[r].ntiles);
-  for (int t = 0; t < tmax; ++t)
-    for (int r = 0; r < e->n; ++r)
-      if (t < e->h_runs[r].ntiles) ord[2].push_back((r << 16) | t);
   e->ntblk = (int)tblk.size();
-  e->ntiles = (int)ord[0].size();
   cudaError_t c = cudaMalloc(&e->d_runs, sizeof(rs::EnsRun) * e->n);
   if (c == cudaSuccess) c = cudaMalloc(&e->d_tblk, sizeof(int32_t) * tblk.size());
-  for (int k = 0; k < 3 && c == cudaSuccess; ++k) c = cudaMalloc(&e->d_order[k], sizeof(int32_t) * e->ntiles);
   if (c == cudaSuccess) c = cudaMemcpy(e->d_tblk, tblk.data(), sizeof(int32_t) * tblk.size(), cudaMemcpyHostToDevice);
-  for (int k = 0; k < 3 && c == cudaSuccess; ++k)
-    c = cudaMemcpy(e->d_order[k], ord[k].data(), sizeof(int32_t) * e->ntiles, cudaMemcpyHostToDevice);
+  // per tile shape, the tile orders: run by run, largest runs first, interleaved
+  for (int sh = 0; sh < rs::kTileShapes && c == cudaSuccess; ++sh) {
+    auto nt = [&](int r) { return e->h_runs[r].ntiles[sh]; };
+    std::vector<int32_t> ord[3];
+    for (int r = 0; r < e->n; ++r)
+      for (int t = 0; t < nt(r); ++t) ord[0].push_back((r << 16) | t);
+    std::vector<int> by(e->n);
+    for (int r = 0; r < e->n; ++r) by[r] = r;
+    std::stable_sort(by.begin(), by.end(), [&](int a, int b) { return nt(a) > nt(b); });
+    for (int r : by)
+      for (int t = 0; t < nt(r); ++t) ord[1].push_back((r << 16) | t);
+    int tmax = 0;
+    for (int r = 0; r < e->n; ++r) tmax = std::max(tmax, nt(r));
+    for (int t = 0; t < tmax; ++t)
+      for (int r = 0; r < e->n; ++r)
+        if (t < nt(r)) ord[2].push_back((r << 16) | t);
+    e->ntiles[sh] = (int)ord[0].size();
+    for (int k = 0; k < 3 && c == cudaSuccess; ++k) {
+      c = cudaMalloc(&e->d_order[sh][k], sizeof(int32_t) * e->ntiles[sh]);
+      if (c == cudaSuccess)
+        c = cudaMemcpy(e->d_order[sh][k], ord[k].data(), sizeof(int32_t) * e->ntiles[sh], cudaMemcpyHostToDevice);
+    }
+  }
   if (c == cudaSuccess) c = cudaMemcpy(e->d_runs, e->h_runs, sizeof(rs::EnsRun) * e->n, cudaMemcpyHostToDevice);
   if (c == cudaSuccess) c = cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking);
   if (c == cudaSuccess) c = cudaMalloc(&e->d_bar, 2 * sizeof(unsigned));
@@ -875,21 +917,22 @@ int ens_prepare(rs_ens *e) {
 }
 
 int ens_graph(rs_ens *e, cudaGraphExec_t *out) {
-  if (e->exec[e->choice]) {
-    *out = e->exec[e->choice];
+  cudaGraphExec_t &ex = e->exec[e->shape][e->choice];
+  if (ex) {
+    *out = ex;
     return RS_OK;
   }
   cudaGraph_t g = nullptr;
   cudaError_t c = cudaStreamBeginCapture(e->cap, cudaStreamCaptureModeThreadLocal);
   if (c == cudaSuccess) {
-    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles, true, e->surr,
-                        e->ctx[0]->d_err, e->cap);
+    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->shape][e->choice], e->ntiles[e->shape],
+                        e->shape, true, e->surr, e->ctx[0]->d_err, e->cap);
     c = cudaStreamEndCapture(e->cap, &g);
   }
-  if (c == cudaSuccess) c = cudaGraphInstantiate(&e->exec[e->choice], g, 0);
+  if (c == cudaSuccess) c = cudaGraphInstantiate(&ex, g, 0);
   if (g) cudaGraphDestroy(g);
   if (c != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble: graph capture: %s", cudaGetErrorString(c));
-  *out = e->exec[e->choice];
+  *out = ex;
   return RS_OK;
 }
 
@@ -928,12 +971,14 @@ int rs_ensemble_create(const rs_params *params, int32_t nruns, rs_ens **out) {
 
 int rs_ensemble_destroy(rs_ens *e) {
   if (!e) return RS_OK;
-  for (int k = 0; k < 3; ++k)
-    if (e->exec[k]) cudaGraphExecDestroy(e->exec[k]);
+  for (int sh = 0; sh < rs::kTileShapes; ++sh)
+    for (int k = 0; k < 3; ++k) {
+      if (e->exec[sh][k]) cudaGraphExecDestroy(e->exec[sh][k]);
+      cudaFree(e->d_order[sh][k]);
+    }
   if (e->cap) cudaStreamDestroy(e->cap);
   cudaFree(e->d_runs);
   cudaFree(e->d_tblk);
-  for (int k = 0; k < 3; ++k) cudaFree(e->d_order[k]);
   cudaFree(e->d_itip);
   cudaFree(e->d_bar);
   cudaFree(e->d_lv);
@@ -963,8 +1008,10 @@ int rs_ensemble_bind(rs_ens *e, int32_t run, const rs_fields *a, const rs_fields
         ((uintptr_t)f->c % 16) || ((uintptr_t)f->psi % 16) || (c->p.nx_all % 4))
       return fail(RS_E_INVALID, "rs_ensemble_bind: run %d: FP32 field sets, 16-byte aligned, pitch nx_all, "
                                 "nx_all a multiple of 4", run);
-    if (!field_map(c, f->psi, RS_F32, &R.map_psi[k]) || !field_map(c, f->c, RS_F32, &R.map_c[k]))
-      return fail(RS_E_CUDA, "rs_ensemble_bind: run %d: no tensor map", run);
+    for (int sh = 0; sh < rs::kTileShapes; ++sh)
+      if (!encode_map(c->p, f->psi, RS_F32, rs::shape_rows(sh) + 2, &R.map_psi[sh][k]) ||
+          !encode_map(c->p, f->c, RS_F32, rs::shape_rows(sh) + 2, &R.map_c[sh][k]))
+        return fail(RS_E_CUDA, "rs_ensemble_bind: run %d: no tensor map", run);
     R.psi[k] = (float *)f->psi;
     R.c[k] = (float *)f->c;
   }
@@ -973,9 +1020,14 @@ int rs_ensemble_bind(rs_ens *e, int32_t run, const rs_fields *a, const rs_fields
   R.F = rs::make_coef<float>(c->K);
   R.tab = c->col_tab;
   R.tab_len = c->col_tab_len;
-  R.nrt = (p.ny_all - 2 + rs::kTileRows - 1) / rs::kTileRows;
-  R.ntiles = R.nrt * ((p.nx_all + rs::kTileOutW - 1) / rs::kTileOutW);
-  if (R.ntiles > 65535 || (R.tab_len + 126) / 127 > 65535)
+  for (int sh = 0; sh < rs::kTileShapes; ++sh) {
+    const int tr = rs::shape_rows(sh);
+    R.nrt[sh] = (p.ny_all - 2 + tr - 1) / tr;
+    R.ntiles[sh] = R.nrt[sh] * ((p.nx_all + rs::kTileOutW - 1) / rs::kTileOutW);
+    if (R.ntiles[sh] > 65535)
+      return fail(RS_E_INVALID, "rs_ensemble_bind: run %d is too large for the ensemble", run);
+  }
+  if ((R.tab_len + 126) / 127 > 65535)
     return fail(RS_E_INVALID, "rs_ensemble_bind: run %d is too large for the ensemble", run);
   R.active = 1;
   R.hist = R.hist_init = p.i_offset_history_initial;
@@ -1019,9 +1071,9 @@ int rs_ensemble_steps(rs_ens *e, int64_t nsteps, rs_stream_t stream) {
         for (int64_t q = 0; q < k; q += kMaxWalk) {
           const int64_t kq = std::min(kMaxWalk, k - q);
           if (ens_walk_l(e, kq, st) ||
-              rs::launch_ensemble_walk(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles,
-                                       (int)kq, e->d_lv, true, e->surr, e->d_bar, e->ctx[0]->d_err,
-                                       e->ctx[0]->wait_limit, st))
+              rs::launch_ensemble_walk(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->shape][e->choice],
+                                       e->ntiles[e->shape], e->shape, (int)kq, e->d_lv, true, e->surr, e->d_bar,
+                                       e->ctx[0]->d_err, e->ctx[0]->wait_limit, st))
             return fail(RS_E_CUDA, "rs_ensemble_steps: persistent launch failed");
           for (int r = 0; r < e->n; ++r)  // the mirror follows (the next chunk starts from it)
             for (int64_t s2 = 0; s2 < kq; ++s2) {
@@ -1072,8 +1124,8 @@ int rs_ensemble_steps(rs_ens *e, int64_t nsteps, rs_stream_t stream) {
     }
     if (cudaMemcpyAsync(e->d_runs, e->h_runs, sizeof(rs::EnsRun) * e->n, cudaMemcpyHostToDevice, st) != cudaSuccess)
       return fail(RS_E_CUDA, "rs_ensemble_steps: state upload failed");
-    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->choice], e->ntiles, true, e->surr,
-                        e->ctx[0]->d_err, st);
+    rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[e->shape][e->choice], e->ntiles[e->shape],
+                        e->shape, true, e->surr, e->ctx[0]->d_err, st);
     if ((rc = cuda_check("rs_ensemble_steps"))) return rc;
     // the upload above reads h_runs: finish it before the mirror changes
     if (cudaStreamSynchronize(st) != cudaSuccess) return fail(RS_E_CUDA, "rs_ensemble_steps: sync failed");
@@ -1120,17 +1172,19 @@ int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choic
   double best = 1e300;
   int pick = 0;
   // without advancing, a launch recomputes the same step: the runs do not move
-  // (k < 3: the per-step launches with tile order k; k >= 3: one-step
-  // persistent walks with tile order k - 3)
+  // (path k: tile shape k / 6; k % 6 < 3: the per-step launches with tile
+  // order k % 6; k % 6 >= 3: one-step persistent walks with tile order
+  // k % 6 - 3)
   auto launch = [&](int k) {
-    if (k < 3)
-      return rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k], e->ntiles, false, e->surr,
-                                 e->ctx[0]->d_err, st);
-    return rs::launch_ensemble_walk(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[k - 3], e->ntiles, 1, e->d_lv,
-                                    false, e->surr, e->d_bar, e->ctx[0]->d_err, 0, st);
+    const int sh = k / 6, o = k % 6;
+    if (o < 3)
+      return rs::launch_ensemble(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[sh][o], e->ntiles[sh], sh, false,
+                                 e->surr, e->ctx[0]->d_err, st);
+    return rs::launch_ensemble_walk(e->d_runs, e->n, e->d_tblk, e->ntblk, e->d_order[sh][o - 3], e->ntiles[sh], sh,
+                                    1, e->d_lv, false, e->surr, e->d_bar, e->ctx[0]->d_err, 0, st);
   };
   if (ens_walk_l(e, 1, st)) return fail(RS_E_CUDA, "rs_ensemble_autotune: state upload failed");
-  for (int k = 0; k < 6; ++k) {
+  for (int k = 0; k < RS_ENS_PATHS; ++k) {
     bool bad = launch(k) != 0;
     cudaEventRecord(t0, st);
     for (int q = 0; q < reps && !bad; ++q) bad = launch(k) != 0;
@@ -1150,16 +1204,19 @@ int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choic
   }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
+  e->shape = pick / 6;
   e->choice = pick % 3;
-  e->walk = pick >= 3;
+  e->walk = pick % 6 >= 3;
   if (choice) *choice = pick;
   return cuda_check("rs_ensemble_autotune");
 }
 
 int rs_ensemble_set_path(rs_ens *e, int32_t path) {
-  if (!e || path < 0 || path > 5) return fail(RS_E_INVALID, "rs_ensemble_set_path: path 0..5");
+  if (!e || path < 0 || path >= RS_ENS_PATHS)
+    return fail(RS_E_INVALID, "rs_ensemble_set_path: path 0..%d", RS_ENS_PATHS - 1);
+  e->shape = path / 6;
   e->choice = path % 3;
-  e->walk = path >= 3;
+  e->walk = path % 6 >= 3;
   return RS_OK;
 }
 

@@ -119,6 +119,26 @@ void launch_reduce_partials(const BlockPartial *partials, int n, double mass_off
   reduce_partials_kernel<<<1, 256, 0, st>>>(partials, n, mass_offset, mass_out, itip_out);
 }
 
+__global__ void __launch_bounds__(128) reduce_partials_dep_kernel(const FinalRed FR) {
+  __shared__ double s_m[256];
+  __shared__ int s_i[256];
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // the step grid has completed, its writes visible
+  final_reduce(FR, s_m, s_i, (int)threadIdx.x, [] { __syncthreads(); });
+}
+
+int launch_reduce_partials_dep(const FinalRed &FR, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(1);
+  cfg.blockDim = dim3(128);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, reduce_partials_dep_kernel, FR) == cudaSuccess ? 0 : -3;
+}
+
 // ---------------------------------------------------------------- precise tip
 // per row j: last column i in [0, nx-2] with psi > 0 (or -1), and the two
 // values get_tip_int can produce for the row: f_j at i0 = last, g_j at i0 = 0.

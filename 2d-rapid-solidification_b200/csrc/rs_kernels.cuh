@@ -58,6 +58,67 @@ struct FinalRed {
   double *mass_out;
   int32_t *itip_out;
 };
+// The fused final reduction, run by the 128 threads of the CTA that finished
+// last: the partials are summed in reduce_partials_kernel's order (slot v =
+// 0..255 adds partials v, v + 256, ... in turn, then a tree over the slots).
+// Each thread takes slots tid and tid + 128 and issues eight 16-byte loads
+// per slot before adding any of them, so the pass costs a few L2 round trips
+// rather than one per partial.  sm_m / sm_i: 256 doubles / ints of shared
+// scratch; sync(): the barrier of the 128 threads.
+template <typename Sync>
+__device__ __forceinline__ void final_reduce(const FinalRed &FR, double *sm_m, int *sm_i, int tid, Sync sync) {
+  constexpr int kB = 8;
+  static_assert(sizeof(BlockPartial) == 16, "a partial is one 16-byte load");
+  const int n = FR.nparts;
+  const double2 *P = reinterpret_cast<const double2 *>(FR.partials);
+  auto itip_of = [](double2 x) { return (int)(uint32_t)(unsigned long long)__double_as_longlong(x.y); };
+  double m[2] = {0.0, 0.0};
+  int it[2] = {0, 0};
+  int j = 0;
+  for (; (j + kB) * 256 <= n; j += kB) {
+    double2 x[2][kB];
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+      for (int u = 0; u < kB; ++u) x[s][u] = __ldcg(P + tid + 128 * s + (j + u) * 256);
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+      for (int u = 0; u < kB; ++u) {
+        m[s] += x[s][u].x;
+        it[s] = max(it[s], itip_of(x[s][u]));
+      }
+  }
+  for (; j * 256 < n; ++j)
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int k = tid + 128 * s + j * 256;
+      if (k < n) {
+        const double2 x = __ldcg(P + k);
+        m[s] += x.x;
+        it[s] = max(it[s], itip_of(x));
+      }
+    }
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    sm_m[tid + 128 * s] = m[s];
+    sm_i[tid + 128 * s] = it[s];
+  }
+  sync();
+  for (int sz = 128; sz > 0; sz >>= 1) {
+    if (tid < sz) {
+      sm_m[tid] += sm_m[tid + sz];
+      sm_i[tid] = max(sm_i[tid], sm_i[tid + sz]);
+    }
+    sync();
+  }
+  if (tid == 0) {
+    if (FR.mass_out) *FR.mass_out = sm_m[0] + FR.mass_offset;
+    if (FR.itip_out) *FR.itip_out = max(1, sm_i[0]);  // get_itip_all_grain starts at 1
+    if (FR.counter) *FR.counter = 0u;
+  }
+}
+
 struct TmaMaps {
   CUtensorMap psi;
   CUtensorMap c;
@@ -102,6 +163,13 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
 int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScalars &P, const TmaMaps &tm,
                         double *psi_n, double *c_n, double *phi_n, BlockPartial *partials, int max_partials,
                         int *nparts_out, int *err, cudaStream_t st);
+// The final reduction of FR (counter unused) as a programmatic dependent of
+// the kernel just launched on st, which wrote the partials: it is scheduled
+// while that kernel runs and waits for its completion on the device
+// (griddepcontrol.wait), so no host-side launch gap follows the step.  The
+// step kernel must execute griddepcontrol.launch_dependents.  Same order of
+// summation as launch_reduce_partials.
+int launch_reduce_partials_dep(const FinalRed &FR, cudaStream_t st);
 void launch_reduce_partials(const BlockPartial *partials, int n, double mass_offset,
                             double *mass_out, int32_t *itip_out, cudaStream_t st);
 

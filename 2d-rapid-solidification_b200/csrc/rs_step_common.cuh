@@ -74,6 +74,22 @@ struct Coef {
   R ox1, ox2, oy1, oy2, oz1, oz2;        // two-eps fallback
   R as0, ak0;                            // a_s, a_k at |grad phi| = 0
   R drive, cflux, AA, cinf, Lref, noise_amp, c_floor;
+  // far-melt form of the solute log term lam = log(c/(1-c)) -
+  // log(cinf/(1-cinf)): its Taylor polynomial in delta = c - cinf,
+  //   lam = sum_k a_k delta^k,  a_k = ((-1)^(k-1) / cinf^k + 1 / (1-cinf)^k) / k,
+  // melt_a[k-1] = a_k, used where |delta| <= melt_tiny.  With m = min(cinf,
+  // 1-cinf), |a_k| <= 2 / (k m^k): FP64 takes 6 terms for |delta| <= 1e-3 m
+  // (the rest below 3e-19 of lam), FP32 4 terms for |delta| <= 1e-2 m (below
+  // 4e-9); the polynomial is the function to the working precision's
+  // rounding, with no division.  Far from the front the melt sits within
+  // these bounds of cinf: the solute boundary layer ahead of the front decays
+  // exponentially.
+  R melt_a[6];
+  R melt_tiny;
+  // delta range of the bulk-melt series form: s = delta / (A + B delta), A =
+  // 2 cinf (1 - cinf), B = 1 - 2 cinf, so |s| < 1/9 for -A/(9+B) < delta <
+  // A/(9-B) (taken 0.1 % inside), evaluated in the working precision
+  R ser_lo, ser_hi;
   int one_eps;
 };
 
@@ -126,6 +142,20 @@ Coef<R> make_coef(const StepCoef &K) {
   F.Lref = (R)K.Lref;
   F.noise_amp = (R)K.noise_amp;
   F.c_floor = (R)1.0e-6;
+  {
+    const bool dbl = sizeof(R) == sizeof(double);
+    const int nt = dbl ? 6 : 4;
+    double pc = 1.0, pm = 1.0;
+    for (int k = 1; k <= 6; ++k) {
+      pc /= K.cinf;
+      pm /= 1.0 - K.cinf;
+      F.melt_a[k - 1] = k <= nt ? (R)(((k % 2 ? pc : -pc) + pm) / k) : (R)0;
+    }
+    F.melt_tiny = (R)((dbl ? 1e-3 : 1e-2) * (K.cinf < 0.5 ? K.cinf : 1.0 - K.cinf));
+    const R ci = (R)K.cinf, sA = (R)2 * ci * ((R)1 - ci), sB = (R)1 - (R)2 * ci;
+    F.ser_hi = (R)0.999 * sA / ((R)9 - sB);
+    F.ser_lo = -(R)0.999 * sA / ((R)9 + sB);
+  }
   F.one_eps = K.one_eps;
   return F;
 }

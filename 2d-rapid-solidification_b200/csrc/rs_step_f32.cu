@@ -84,25 +84,35 @@ static_assert(64 + 2 * kTRin <= kThreads && 4 * kTR <= kThreads, "one thread per
 // entry k describes column k - 4
 enum { kTabRT = 0, kTabC0 = 1, kTabDK = 2, kTabAnb = 3, kTabAti = 4 };
 
-struct alignas(128) TileSmem {
-  // TMA destinations (128-byte aligned); rows 1..16 receive the new psi / c - cinf
-  alignas(128) float psi[kTRin][kWin];
-  alignas(128) float d[kTRin][kWin];
-  alignas(16) float S[kTRin][kWin];  // after phase 2: new psi of the listed cells
-  alignas(16) float mu[kTRin][kWin];
-  uint16_t list[kTR * kW];   // interface cells: row << 8 | output column
-  uint8_t pmask[kTRin][32];  // per lane: bits 0-3 psi <= -1, bits 4-7 psi >= 1 of its four cells
-  uint8_t hmask[kTRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
-  uint32_t liq, sol;         // bit r: every cell of input row r has psi == -1 / +1
+// Shared memory of one tile of TR output rows x kW output columns (input
+// TR + 2 rows); the ensemble kernels take TR = 8, 16 or 32 (kTileShapes), the
+// single-run kernel TR = kTR.
+template <int TR>
+struct alignas(128) TileSmemT {
+  static constexpr int kRin = TR + 2;  // input rows
+  using Mask = std::conditional_t<(kRin <= 32), uint32_t, unsigned long long>;  // one bit per input row
+  // TMA destinations (128-byte aligned); rows 1..TR receive the new psi / c - cinf
+  alignas(128) float psi[kRin][kWin];
+  alignas(128) float d[kRin][kWin];
+  alignas(16) float S[kRin][kWin];  // after phase 2: new psi of the listed cells
+  alignas(16) float mu[kRin][kWin];
+  uint16_t list[TR * kW];   // interface cells: row << 8 | output column
+  uint8_t pmask[kRin][32];  // per lane: bits 0-3 psi <= -1, bits 4-7 psi >= 1 of its four cells
+  uint8_t hmask[kRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
+  Mask liq, sol;            // bit r: every cell of input row r has psi == -1 / +1
   int nlist;
   double part_mass[kWarps];
   int part_itip[kWarps];
   uint64_t full;
   int last;  // this CTA finished last (fused final reduction)
 };
+using TileSmem = TileSmemT<kTR>;
 
-static_assert(offsetof(TileSmem, psi) % 128 == 0 && offsetof(TileSmem, d) % 128 == 0,
+static_assert(offsetof(TileSmem, psi) % 128 == 0 && offsetof(TileSmem, d) % 128 == 0 &&
+                  offsetof(TileSmemT<8>, d) % 128 == 0 && offsetof(TileSmemT<32>, d) % 128 == 0,
               "TMA destinations start on 128-byte boundaries");
+static_assert(sizeof(TileSmemT<8>::S) >= 256 * sizeof(double) && sizeof(TileSmemT<8>::mu) >= 256 * sizeof(int),
+              "the final reduction's scratch fits S and mu");
 static_assert((kWin * sizeof(float)) % 16 == 0, "rows stay 16-byte aligned for float4 and bulk copies");
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
@@ -169,15 +179,25 @@ __global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef 
 // keep the exact series form: it is exact and cheaper than the network.
 // The work of one CTA on tile (row tile tr, column tile tc) of a field set;
 // part: this tile's partial (mass, coarse tip), or nullptr.
-template <bool SURR, typename Prefetch>
+// TR: output rows of the tile (8, 16 or 32; the tensor maps' box is TR + 2
+// rows high).
+template <bool SURR, int TR, typename Prefetch>
 __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &F, const StepScalars &PS,
                                           const CUtensorMap *tm_psi, const CUtensorMap *tm_c,
                                           const float *__restrict__ tab, const int tab_len, float *__restrict__ psi_n,
                                           float *__restrict__ c_n, float *__restrict__ phi_n, BlockPartial *part,
                                           int *err, const SurrArgs &SA, const int tr, const int tc,
                                           const FinalRed *FR, const Prefetch &prefetch) {
+  // the tile's shape (these hide the single-run constants of the same names)
+  constexpr int kTR = TR, kTRin = TR + 2, kRowsPerWarp = TR / kWarps;
+  static_assert(TR % kWarps == 0 && kRowsPerWarp * 4 <= 32, "output rows split evenly over the warps");
+  // halo-column threads: the last warps, which have one input row fewer
+  constexpr int kHalo0 = (64 + 2 * kTRin <= kThreads) ? 64 : kThreads - 2 * kTRin;
+  static_assert(kHalo0 >= 0 && 4 * kTR <= kThreads, "one thread per halo cell and per row copy");
+  using Smem = TileSmemT<TR>;
+  using Mask = typename Smem::Mask;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
+  Smem &sm = *reinterpret_cast<Smem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int x0 = kW * tc;       // first output column of the tile
   const int y0 = 1 + kTR * tr;  // first output row; input rows y0-1 .. y0+kTR
@@ -193,8 +213,8 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     mbar_expect_tx(&sm.full, kTileBytes);
     tma_load_2d(&sm.psi[0][0], tm_psi, &sm.full, x0 - 4, y0 - 1);
     tma_load_2d(&sm.d[0][0], tm_c, &sm.full, x0 - 4, y0 - 1);
-    sm.liq = 0u;
-    sm.sol = 0u;
+    sm.liq = 0;
+    sm.sol = 0;
     sm.nlist = 0;
   }
 
@@ -205,19 +225,22 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
 #pragma unroll
   for (int q = 0; q < 4; ++q)
     if (gi + q >= 1 && gi + q <= K.nx - 2) outm |= 1u << q;
+  // launch constants of the row loops in registers (one read of the
+  // arguments, which may live in global memory for the ensemble)
+  const int ny = K.ny, nx = K.nx;
+  const float cinf = F.cinf, tiny = F.melt_tiny;
+  const float ma0 = F.melt_a[0], ma1 = F.melt_a[1], ma2 = F.melt_a[2], ma3 = F.melt_a[3];
   const float two_cinf = F.cinf + F.cinf;
   const float cflux4 = 0.25f * F.cflux;
   const float floor_d = F.c_floor - F.cinf;
   constexpr float KL = (float)(-2.0 * kL0Liq);
-  // delta range of the series form: s = delta / (A + B delta) with
-  // A = 2 cinf (1 - cinf), B = 1 - 2 cinf, so |s| < 1/9 for
-  // -A/(9+B) < delta < A/(9-B) (taken 0.1 % inside)
-  const float sA = 2.f * F.cinf * (1.f - F.cinf), sB = 1.f - 2.f * F.cinf;
-  const float d_hi = 0.999f * sA / (9.f - sB), d_lo = -0.999f * sA / (9.f + sB);
+  const float d_hi = F.ser_hi, d_lo = F.ser_lo;  // series range of delta (Coef)
   constexpr uint32_t kMinus1 = 0xBF800000u, kPlus1 = 0x3F800000u;
 
   // the column table of this step (programmatic dependency on its kernel)
   asm volatile("griddepcontrol.wait;" ::: "memory");
+  // the step's final reduction (a programmatic dependent) may be scheduled now
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const float *tRT = tab + kTabRT * tab_len + 4, *tC0 = tab + kTabC0 * tab_len + 4;
   const float *tDK = tab + kTabDK * tab_len + 4;
   const float4 RTv = ld4(tRT + gi), C0v = ld4(tC0 + gi);
@@ -330,29 +353,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     __threadfence();
     double *sm_m = reinterpret_cast<double *>(&sm.S[0][0]);  // S and mu are free now
     int *sm_i = reinterpret_cast<int *>(&sm.mu[0][0]);
-    for (int v = threadIdx.x; v < 256; v += kThreads) {
-      double m = 0.0;
-      int it = 0;
-      for (int k = v; k < FR->nparts; k += 256) {
-        m += __ldcg(&FR->partials[k].mass);
-        it = max(it, __ldcg(&FR->partials[k].itip));
-      }
-      sm_m[v] = m;
-      sm_i[v] = it;
-    }
-    __syncthreads();
-    for (int sz = 128; sz > 0; sz >>= 1) {
-      for (int v = threadIdx.x; v < sz; v += kThreads) {
-        sm_m[v] += sm_m[v + sz];
-        sm_i[v] = max(sm_i[v], sm_i[v + sz]);
-      }
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      if (FR->mass_out) *FR->mass_out = sm_m[0] + FR->mass_offset;
-      if (FR->itip_out) *FR->itip_out = max(1, sm_i[0]);  // get_itip_all_grain starts at 1
-      *FR->counter = 0u;
-    }
+    final_reduce(*FR, sm_m, sm_i, (int)threadIdx.x, [] { __syncthreads(); });
   };
   __syncthreads();  // barrier initialised, flags cleared
   {
@@ -395,16 +396,16 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   }
 
   // ---- phase 1: per-cell terms; warp w takes input rows w, w+4, ...
+  // The warp's row flags (warp-uniform) are OR-ed into sm.liq / sm.sol once;
+  // rows flagged there store no phi masks (phase 2 takes 0x0F / 0xF0)
+  Mask liq_rows = 0, sol_rows = 0;
 #pragma unroll 1
   for (int rr = warp; rr < kTRin; rr += kWarps) {
-    if (y0 - 1 + rr > K.ny - 1) {  // beyond the array (last tile): never read by an output
+    if (y0 - 1 + rr > ny - 1) {  // beyond the array (last tile): never read by an output
       st4(&sm.S[rr][bc], 0.f, 0.f, 0.f, 0.f);
       st4(&sm.mu[rr][bc], 0.f, 0.f, 0.f, 0.f);
-      sm.pmask[rr][lane] = 0xFFu;
-      if (lane == 0) {
-        atomicOr(&sm.liq, 1u << rr);
-        atomicOr(&sm.sol, 1u << rr);
-      }
+      liq_rows |= Mask(1) << rr;
+      sol_rows |= Mask(1) << rr;
       continue;
     }
     const float4 pv4 = ld4(&sm.psi[rr][bc]), dv4 = ld4(&sm.d[rr][bc]);
@@ -419,12 +420,24 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const float dmn = fminf(fminf(dv[0], dv[1]), fminf(dv[2], dv[3]));
     const bool liq4 = band == kMinus1 && bor == kMinus1;
     uint32_t code, s3 = 0u;
-    if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
-      code = 1u | 4u;  // 4: every cell in the series form
-      sm.pmask[rr][lane] = 0x0Fu;
+    if (__all_sync(FULL, liq4 && fmaxf(dmx, -dmn) <= tiny)) {
+      // far melt: lam by its Taylor polynomial in delta (Coef::melt_a);
+      // mu'' = RT lam - 2 L0_Liq delta = delta (RT p + KL), lam = delta p
+      code = 1u | 4u;  // 4: every cell in the exact melt form
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const float c = F.cinf + dv[q], om = 1.f - c;
+        const float c = cinf + dv[q], om = 1.f - c;
+        float p = fmaf(ma3, dv[q], ma2);
+        p = fmaf(p, dv[q], ma1);
+        p = fmaf(p, dv[q], ma0);
+        Sv[q] = c * om;
+        mv[q] = dv[q] * fmaf(RTa[q], p, KL);
+      }
+    } else if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
+      code = 1u | 4u;  // 4: every cell in the series form
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float c = cinf + dv[q], om = 1.f - c;
         const float sv = __fdividef(dv[q], fmaf(two_cinf, om, dv[q]));
         const float s2 = sv * sv;
         // atanh(s) to s^7: relative truncation below 2.6e-9 for |s| < 1/9
@@ -450,7 +463,6 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       const bool deep = (code & 2u) && __all_sync(FULL, s3 == 0xFu);
       if (deep) {
         code |= 8u;  // 8: mu'' not needed (no network pass either)
-        sm.pmask[rr][lane] = 0xF0u;
 #pragma unroll
         for (int q = 0; q < 4; ++q) Sv[q] = mv[q] = 0.f;
       } else {
@@ -466,10 +478,8 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     }
     st4(&sm.S[rr][bc], Sv[0], Sv[1], Sv[2], Sv[3]);
     st4(&sm.mu[rr][bc], mv[0], mv[1], mv[2], mv[3]);
-    if (lane == 0) {
-      if (code & 1u) atomicOr(&sm.liq, 1u << rr);
-      if (code & 2u) atomicOr(&sm.sol, 1u << rr);
-    }
+    liq_rows |= Mask(code & 1u) << rr;
+    sol_rows |= Mask((code >> 1) & 1u) << rr;
     if constexpr (SURR) {  // the row's non-melt cells through the network, 16 at a time
       if (!(code & (4u | 8u))) {
         __syncwarp();
@@ -498,11 +508,15 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       }
     }
   }
+  if (lane == 0) {
+    if (liq_rows) atomicOr(&sm.liq, liq_rows);
+    if (sol_rows) atomicOr(&sm.sol, sol_rows);
+  }
   // halo columns x0-1 and x0+kW, one thread per cell, on warps 2 and 3, which
   // have one input row fewer than warps 0 and 1 (surrogate: warp 3 alone,
   // then the same network pass as the rows)
-  if (SURR ? warp == 3 : (threadIdx.x >= 64 && threadIdx.x < 64 + 2 * kTRin)) {
-   for (int i = SURR ? lane : (int)threadIdx.x - 64; i < 2 * kTRin; i += 32) {
+  if (SURR ? warp == 3 : (threadIdx.x >= kHalo0 && threadIdx.x < kHalo0 + 2 * kTRin)) {
+   for (int i = SURR ? lane : (int)threadIdx.x - kHalo0; i < 2 * kTRin; i += 32) {
     const int rr = i >> 1, side = i & 1;
     const int x = side ? kHaloR : kHaloL, g = x0 - 4 + x;
     float Sh = 0.f, mh = 0.f;
@@ -550,7 +564,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   if (threadIdx.x == 0) prefetch();
 
   // ---- phase 2: warp w computes output rows 1 + 4w .. 4 + 4w of the tile
-  const uint32_t liq = sm.liq, sol = sm.sol;
+  const Mask liq = sm.liq, sol = sm.sol;
   const bool red = part != nullptr;
   double mass = 0.0;
   int itip = 0;
@@ -617,17 +631,19 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
 #pragma unroll
     for (int q = 0; q < 4; ++q)
       dn[j][q] = fmaxf(fmaf(cflux4, (jh[q + 1] - jh[q]) + (jv_hi[q] - jv_lo[q]), dv[q]), floor_d);
-    const bool live = y0 - 1 + rr <= K.ny - 2;
+    const bool live = y0 - 1 + rr <= ny - 2;
     if (red && live) {
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         if ((outm >> q) & 1u) mass += (double)dn[j][q];
     }
     // phi: cells whose 3x3 neighbourhood is not uniformly +-1 are listed
-    const uint32_t w3 = 7u << (rr - 1);
+    const Mask w3 = Mask(7) << (rr - 1);
     if (live && (liq & w3) != w3 && (sol & w3) != w3) {
-      const uint32_t pk = (uint32_t)sm.pmask[rr - 1][lane] | ((uint32_t)sm.pmask[rr][lane] << 8) |
-                          ((uint32_t)sm.pmask[rr + 1][lane] << 16);
+      auto pm = [&](int k) -> uint32_t {  // rows flagged all -1 / all +1 store no masks
+        return ((liq >> k) & 1u) ? 0x0Fu : ((sol >> k) & 1u) ? 0xF0u : (uint32_t)sm.pmask[k][lane];
+      };
+      const uint32_t pk = pm(rr - 1) | (pm(rr) << 8) | (pm(rr + 1) << 16);
       uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
       if (lane == 0) {
         lf = 0u;
@@ -733,14 +749,18 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const int rr = rbase + j;
     const float4 pv4 = ld4(&sm.psi[rr][bc]);
     const float pv[4] = {pv4.x, pv4.y, pv4.z, pv4.w};
-    const bool live = y0 - 1 + rr <= K.ny - 2;
+    const bool live = y0 - 1 + rr <= ny - 2;
     float po[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const bool listed = (needs_all >> (4 * j + q)) & 1u;
-      po[q] = listed ? sm.S[rr][bc + q] : clamp1(pv[q]);  // phi_next = phi where uniformly +-1
+      // phi_next = phi where uniformly +-1: an output cell is not listed only
+      // where psi <= -1 or >= 1 over its 3x3 neighbourhood, so clamp(psi) is
+      // its sign (cells outside the interior are not stored or are
+      // overwritten by the ghost copies)
+      po[q] = listed ? sm.S[rr][bc + q] : (pv[q] > 0.f ? 1.f : -1.f);
       if (red && live && !listed && ((outm >> q) & 1u) && po[q] > 0.f)
-        itip = max(itip, gi + q == K.nx - 2 ? K.nx - 1 : gi + q);
+        itip = max(itip, gi + q == nx - 2 ? nx - 1 : gi + q);
     }
     st4(&sm.psi[rr][bc], po[0], po[1], po[2], po[3]);
     st4(&sm.d[rr][bc], dn[j][0], dn[j][1], dn[j][2], dn[j][3]);
@@ -833,7 +853,7 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
       tma_prefetch_2d(&tm_c, kW * pf_tc - 4, kTR * pf_tr);
     }
   };
-  tile_body<SURR>(K, F, PS, &tm_psi, &tm_c, tab, tab_len, psi_n, c_n, phi_n,
+  tile_body<SURR, kTR>(K, F, PS, &tm_psi, &tm_c, tab, tab_len, psi_n, c_n, phi_n,
                   partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr, err, SA, tr, tc,
                   partials && FR.counter ? &FR : nullptr, prefetch);
 }
@@ -860,9 +880,14 @@ __global__ void __launch_bounds__(kTabBlock) ens_table_kernel(const EnsRun *__re
   table_block(R.K, ens_d0(R, R.l), R.d1, R.tab_len, R.tab, e & 0xFFFF, kc);
 }
 
-template <bool SURR>
-__global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
+// CTAs per SM the tile kernels are built for, by tile height (32-row tiles
+// take 83 KB of shared memory: two per SM)
+constexpr int min_ctas(bool surr, int TR) { return TR > 16 ? 2 : surr ? 4 : 5; }
+
+template <bool SURR, int SHAPE>
+__global__ void __launch_bounds__(kThreads, min_ctas(SURR, shape_rows(SHAPE)))
     ens_tile_kernel(const EnsRun *__restrict__ runs, const int32_t *__restrict__ order, int *err, const int wave) {
+  constexpr int TR = shape_rows(SHAPE);
   const int32_t e = order[blockIdx.x];
   const EnsRun &R = runs[e >> 16];
   if (!R.active) return;
@@ -881,12 +906,14 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
     const int32_t e2 = order[nb];
     const EnsRun &R2 = runs[e2 >> 16];
     if (!R2.active) return;
-    const int t2 = e2 & 0xFFFF, p2 = (int)(R2.step & 1);
-    tma_prefetch_2d(&R2.map_psi[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
-    tma_prefetch_2d(&R2.map_c[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
+    const int t2 = e2 & 0xFFFF, p2 = (int)(R2.step & 1), n2 = R2.nrt[SHAPE];
+    tma_prefetch_2d(&R2.map_psi[SHAPE][p2], kW * (t2 / n2) - 4, TR * (t2 % n2));
+    tma_prefetch_2d(&R2.map_c[SHAPE][p2], kW * (t2 / n2) - 4, TR * (t2 % n2));
   };
-  tile_body<SURR>(R.K, R.F, PS, &R.map_psi[par], &R.map_c[par], R.tab, R.tab_len, R.psi[par ^ 1], R.c[par ^ 1],
-                  nullptr, nullptr, err, SURR ? R.surr : none, t % R.nrt, t / R.nrt, nullptr, prefetch);
+  const int nrt = R.nrt[SHAPE];
+  tile_body<SURR, TR>(R.K, R.F, PS, &R.map_psi[SHAPE][par], &R.map_c[SHAPE][par], R.tab, R.tab_len, R.psi[par ^ 1],
+                      R.c[par ^ 1], nullptr, nullptr, err, SURR ? R.surr : none, t % nrt, t / nrt, nullptr,
+                      prefetch);
 }
 
 __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
@@ -910,14 +937,15 @@ __global__ void ens_advance_kernel(EnsRun *runs, const int nruns) {
 // nruns + r].
 constexpr uint32_t kWalkBarrierLimit = 1u << 22;
 
-template <bool SURR>
-__global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
+template <bool SURR, int SHAPE>
+__global__ void __launch_bounds__(kThreads, min_ctas(SURR, shape_rows(SHAPE)))
     ens_walk_kernel(EnsRun *__restrict__ runs, const int nruns, const int32_t *__restrict__ tblk, const int ntblk,
                     const int32_t *__restrict__ order, const int ntiles, const int nsteps,
                     const double *__restrict__ lv, const int advance, unsigned *bar, int *err,
                     const uint32_t barrier_limit) {
+  constexpr int TR = shape_rows(SHAPE);
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  TileSmem &sm = *reinterpret_cast<TileSmem *>(smem_raw);
+  TileSmemT<TR> &sm = *reinterpret_cast<TileSmemT<TR> *>(smem_raw);
   const unsigned G = gridDim.x;
   unsigned target = 0;
   bool dead = false;
@@ -966,13 +994,14 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
           const int32_t e2 = order[i2];
           const EnsRun &R2 = runs[e2 >> 16];
           if (!R2.active) return;
-          const int t2 = e2 & 0xFFFF, p2 = (int)((R2.step + s) & 1);
-          tma_prefetch_2d(&R2.map_psi[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
-          tma_prefetch_2d(&R2.map_c[p2], kW * (t2 / R2.nrt) - 4, kTR * (t2 % R2.nrt));
+          const int t2 = e2 & 0xFFFF, p2 = (int)((R2.step + s) & 1), n2 = R2.nrt[SHAPE];
+          tma_prefetch_2d(&R2.map_psi[SHAPE][p2], kW * (t2 / n2) - 4, TR * (t2 % n2));
+          tma_prefetch_2d(&R2.map_c[SHAPE][p2], kW * (t2 / n2) - 4, TR * (t2 % n2));
         };
-        tile_body<SURR>(R.K, R.F, PS, &R.map_psi[par], &R.map_c[par], R.tab, R.tab_len, R.psi[par ^ 1],
-                        R.c[par ^ 1], nullptr, nullptr, err, SURR ? R.surr : none, t % R.nrt, t / R.nrt, nullptr,
-                        prefetch);
+        const int nrt = R.nrt[SHAPE];
+        tile_body<SURR, TR>(R.K, R.F, PS, &R.map_psi[SHAPE][par], &R.map_c[SHAPE][par], R.tab, R.tab_len,
+                            R.psi[par ^ 1], R.c[par ^ 1], nullptr, nullptr, err, SURR ? R.surr : none, t % nrt,
+                            t / nrt, nullptr, prefetch);
         __syncthreads();  // every thread is done with the tile's barrier and shared memory
         if (threadIdx.x == 0) mbar_inval(&sm.full);
         if (__syncthreads_or(*(volatile int *)err != 0)) dead = true;
@@ -1105,8 +1134,7 @@ __device__ __forceinline__ void phase1_32(const View32 &V, const InSlot32 &in, S
   const int lane = V.lane, bc = V.bc;
   const float two_cinf = F.cinf + F.cinf;
   constexpr float KL = (float)(-2.0 * kL0Liq);
-  const float sA = 2.f * F.cinf * (1.f - F.cinf), sB = 1.f - 2.f * F.cinf;
-  const float d_hi = 0.999f * sA / (9.f - sB), d_lo = -0.999f * sA / (9.f + sB);
+  const float d_hi = F.ser_hi, d_lo = F.ser_lo;  // series range of delta (Coef)
   const float4 RTv = ld4(V.tRT + V.gi), C0v = ld4(V.tC0 + V.gi);
   const float RTa[4] = {RTv.x, RTv.y, RTv.z, RTv.w}, C0a[4] = {C0v.x, C0v.y, C0v.z, C0v.w};
   auto solid3 = [&](int rr) -> uint32_t {
@@ -1147,7 +1175,20 @@ __device__ __forceinline__ void phase1_32(const View32 &V, const InSlot32 &in, S
     const float dmn = fminf(fminf(dv[0], dv[1]), fminf(dv[2], dv[3]));
     const bool liq4 = band == kMinus1f && bor == kMinus1f;
     uint32_t code;
-    if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
+    if (__all_sync(FULL, liq4 && fmaxf(dmx, -dmn) <= F.melt_tiny)) {
+      // far melt (as tile_body)
+      code = 1u;
+      st.pmask[rr][lane] = 0x0Fu;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float c = F.cinf + dv[q], om = 1.f - c;
+        float p = fmaf(F.melt_a[3], dv[q], F.melt_a[2]);
+        p = fmaf(p, dv[q], F.melt_a[1]);
+        p = fmaf(p, dv[q], F.melt_a[0]);
+        Sv[q] = c * om;
+        mv[q] = dv[q] * fmaf(RTa[q], p, KL);
+      }
+    } else if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
       code = 1u;
       st.pmask[rr][lane] = 0x0Fu;
 #pragma unroll
@@ -1468,29 +1509,7 @@ __device__ __forceinline__ void finish32(const View32 &V, P2Smem32 &p2, double m
   gsync(bar);
   if (!p2.last) return;
   __threadfence();
-  for (int v = V.gtid; v < 256; v += kThreads) {
-    double m = 0.0;
-    int it = 0;
-    for (int k = v; k < FR->nparts; k += 256) {
-      m += __ldcg(&FR->partials[k].mass);
-      it = max(it, __ldcg(&FR->partials[k].itip));
-    }
-    sm_m[v] = m;
-    sm_i[v] = it;
-  }
-  gsync(bar);
-  for (int sz = 128; sz > 0; sz >>= 1) {
-    for (int v = V.gtid; v < sz; v += kThreads) {
-      sm_m[v] += sm_m[v + sz];
-      sm_i[v] = max(sm_i[v], sm_i[v + sz]);
-    }
-    gsync(bar);
-  }
-  if (V.gtid == 0) {
-    if (FR->mass_out) *FR->mass_out = sm_m[0] + FR->mass_offset;
-    if (FR->itip_out) *FR->itip_out = max(1, sm_i[0]);
-    *FR->counter = 0u;
-  }
+  final_reduce(*FR, sm_m, sm_i, V.gtid, [&] { gsync(bar); });
 }
 
 __device__ __forceinline__ void tile_of32(int t, int nrt, int ncb, int f, int &tr, int &tc) {
@@ -1531,6 +1550,8 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("griddepcontrol.wait;" ::: "memory");
+  // the step's final reduction (a programmatic dependent) may be scheduled now
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   __syncthreads();
 
   if (warp == 0) {  // producer
@@ -1611,14 +1632,38 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
 
 }  // namespace
 
+namespace {
+// the ensemble kernels of one tile shape, and their shared memory
+using EnsTileFn = void (*)(const EnsRun *, const int32_t *, int *, int);
+using EnsWalkFn = void (*)(EnsRun *, int, const int32_t *, int, const int32_t *, int, int, const double *, int,
+                           unsigned *, int *, uint32_t);
+template <int SHAPE>
+void ens_kernels(bool surr, EnsTileFn &tile, EnsWalkFn &walk, size_t &smem) {
+  tile = surr ? ens_tile_kernel<true, SHAPE> : ens_tile_kernel<false, SHAPE>;
+  walk = surr ? ens_walk_kernel<true, SHAPE> : ens_walk_kernel<false, SHAPE>;
+  smem = sizeof(TileSmemT<shape_rows(SHAPE)>);
+}
+bool ens_kernels(int shape, bool surr, EnsTileFn &tile, EnsWalkFn &walk, size_t &smem) {
+  switch (shape) {
+    case 0: ens_kernels<0>(surr, tile, walk, smem); return true;
+    case 1: ens_kernels<1>(surr, tile, walk, smem); return true;
+    case 2: ens_kernels<2>(surr, tile, walk, smem); return true;
+    default: return false;
+  }
+}
+static_assert(kTileShapes == 3, "ens_kernels covers every tile shape");
+}  // namespace
+
 int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
-                    bool advance, bool surr, int *err, cudaStream_t st) {
-  const size_t smem = sizeof(TileSmem);
-  auto kfn = surr ? ens_tile_kernel<true> : ens_tile_kernel<false>;
-  static std::atomic<unsigned long long> attr_done[2];
-  if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr])) return -3;
-  static std::atomic<int> wave_of[2][64];
-  const int wave = resident_ctas((const void *)kfn, kThreads, smem, wave_of[surr]);
+                    int shape, bool advance, bool surr, int *err, cudaStream_t st) {
+  EnsTileFn kfn;
+  EnsWalkFn wfn;
+  size_t smem;
+  if (!ens_kernels(shape, surr, kfn, wfn, smem)) return -1;
+  static std::atomic<unsigned long long> attr_done[2][kTileShapes];
+  if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr][shape])) return -3;
+  static std::atomic<int> wave_of[2][kTileShapes][64];
+  const int wave = resident_ctas((const void *)kfn, kThreads, smem, wave_of[surr][shape]);
   if (wave < 0) return -3;
   ens_table_kernel<<<ntblk, kTabBlock, 0, st>>>(runs, tblk);
   kfn<<<ntiles, kThreads, smem, st>>>(runs, order, err, wave);
@@ -1627,16 +1672,18 @@ int launch_ensemble(const EnsRun *runs, int nruns, const int32_t *tblk, int ntbl
 }
 
 int launch_ensemble_walk(EnsRun *runs, int nruns, const int32_t *tblk, int ntblk, const int32_t *order, int ntiles,
-                         int nsteps, const double *lv, bool advance, bool surr, unsigned *bar, int *err,
+                         int shape, int nsteps, const double *lv, bool advance, bool surr, unsigned *bar, int *err,
                          uint32_t barrier_limit, cudaStream_t st) {
   if (nsteps <= 0) return 0;
-  const size_t smem = sizeof(TileSmem);
-  static_assert(sizeof(TileSmem) >= kTabBlock * sizeof(double), "table scratch fits the tile's shared memory");
-  auto kfn = surr ? ens_walk_kernel<true> : ens_walk_kernel<false>;
-  static std::atomic<unsigned long long> attr_done[2];
-  if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr])) return -3;
-  static std::atomic<int> res_of[2][64];
-  const int res = resident_ctas((const void *)kfn, kThreads, smem, res_of[surr]);
+  EnsTileFn tfn;
+  EnsWalkFn kfn;
+  size_t smem;
+  if (!ens_kernels(shape, surr, tfn, kfn, smem)) return -1;
+  static_assert(sizeof(TileSmemT<8>) >= kTabBlock * sizeof(double), "table scratch fits the tile's shared memory");
+  static std::atomic<unsigned long long> attr_done[2][kTileShapes];
+  if (!smem_limit_once((const void *)kfn, (int)smem, attr_done[surr][shape])) return -3;
+  static std::atomic<int> res_of[2][kTileShapes][64];
+  const int res = resident_ctas((const void *)kfn, kThreads, smem, res_of[surr][shape]);
   if (res <= 0) return -3;
   const int grid = std::max(1, std::min(res, std::max(ntiles, ntblk)));
   if (cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st) != cudaSuccess) return -2;
@@ -1690,14 +1737,17 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
     pa[0].val.programmaticStreamSerializationAllowed = 1;
     pc.attrs = pa;
     pc.numAttrs = 1;
+    // the final reduction is a programmatic dependent launch after the step
     FinalRed pfr = tm.red;
     pfr.partials = partials;
     pfr.nparts = nparts;
-    if (!partials || !(pfr.mass_out || pfr.itip_out)) pfr.counter = nullptr;
+    FinalRed none = pfr;
+    none.counter = nullptr;
     const float *ptab = tm.col_tab;
     if (cudaLaunchKernelEx(&pc, pipe_kernel_f32, K, F, P, tm.psi, tm.c, ptab, tm.col_tab_len, psi_n, c_n, phi_n,
-                           partials, err, pfr, nrt, ncb) != cudaSuccess)
+                           partials, err, none, nrt, ncb) != cudaSuccess)
       return -3;
+    if (partials && (pfr.mass_out || pfr.itip_out) && launch_reduce_partials_dep(pfr, st)) return -3;
     if (nparts_out) *nparts_out = nparts;
     return 0;
   }
@@ -1722,13 +1772,16 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   cfg.attrs = at;
   cfg.numAttrs = 1;
   const float *tab = tm.col_tab;
+  // the final reduction is a programmatic dependent launch after the step
   FinalRed fr = tm.red;
   fr.partials = partials;
   fr.nparts = nparts;
-  if (!partials || !(fr.mass_out || fr.itip_out)) fr.counter = nullptr;
+  FinalRed none = fr;
+  none.counter = nullptr;
   if (cudaLaunchKernelEx(&cfg, kfn, K, F, P, tm.psi, tm.c, tab, tm.col_tab_len, psi_n, c_n, phi_n, partials, err,
-                         sa, fr, wave) != cudaSuccess)
+                         sa, none, wave) != cudaSuccess)
     return -3;
+  if (partials && (fr.mass_out || fr.itip_out) && launch_reduce_partials_dep(fr, st)) return -3;
   if (nparts_out) *nparts_out = nparts;
   return 0;
 }

@@ -43,7 +43,7 @@
 //   * bulk melt rows (psi = -1 exactly, delta in the series range): g = -1,
 //     q = 1, so mu'' = -2 L0_Liq delta + RT lam and S = c (1 - c); far-melt
 //     rows (|delta| <= 1e-3 min(cinf, 1-cinf) as well) take lam as its
-//     Taylor polynomial in delta (MeltPoly), without the division of s;
+//     Taylor polynomial in delta (Coef::melt_a), without the division of s;
 //   * deep solid rows (psi = +1 over the 3x3 neighbourhoods) store
 //     S = mu'' = 0: every face weight touching them is 0;
 //   * face weights by pair sums (6 P_i + P_{i-1} + P_{i+1}, four times the
@@ -90,31 +90,6 @@ static_assert(64 + 2 * kTRin <= kThreads && 4 * kTR <= kThreads, "one thread per
 // describes column k - 4
 enum { kTabRT = 0, kTabC0 = 1, kTabDK = 2, kTabAnb = 3, kTabAti = 4 };
 
-// The solute log term lam = log(c/(1-c)) - log(cinf/(1-cinf)) of a far-melt
-// cell as its Taylor polynomial in delta = c - cinf:
-//   lam = sum_k a_k delta^k,  a_k = ((-1)^(k-1) / cinf^k + 1 / (1-cinf)^k) / k.
-// With m = min(cinf, 1-cinf), |a_k| <= 2 / (k m^k), so for |delta| <= 1e-3 m
-// the terms beyond k = 6 sum to below 3e-19 of lam: the polynomial is the
-// function to FP64 rounding, with no division.  Far from the front the melt
-// sits within that bound of cinf (the solute boundary layer decays
-// exponentially ahead of the front), so most melt rows take this form.
-constexpr int kMeltTerms = 6;
-struct MeltPoly {
-  double a[kMeltTerms];  // a_1 .. a_6
-  double tiny;           // |delta| bound of the polynomial form
-};
-MeltPoly make_melt_poly(double cinf) {
-  MeltPoly M;
-  double pc = 1.0, pm = 1.0;
-  for (int k = 1; k <= kMeltTerms; ++k) {
-    pc /= cinf;
-    pm /= 1.0 - cinf;
-    M.a[k - 1] = ((k % 2 ? pc : -pc) + pm) / k;
-  }
-  M.tiny = 1e-3 * std::min(cinf, 1.0 - cinf);
-  return M;
-}
-
 // the input tile: TMA destinations (128-byte aligned); after phase 3 rows
 // 1..16 receive the new psi / c for the bulk stores
 struct alignas(128) InSlot {  // both arrays are TMA destinations: 128-byte aligned
@@ -126,6 +101,7 @@ struct alignas(16) StSlot {
   double S[kTRin][kWin];  // after phase 2: new psi of the listed cells
   double mu[kTRin][kWin];
   uint8_t pmask[kTRin][32];  // per lane: bits 0-1 psi <= -1, bits 4-5 psi >= 1 of its two cells
+                             // (rows flagged in liq / sol store none)
   uint8_t hmask[kTRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
   uint32_t liq, sol;         // bit r: every cell of input row r has psi == -1 / +1
 };
@@ -242,16 +218,14 @@ struct TileView {
   const StepCoef &K;
   const Coef<double> &F;
   const StepScalars &PS;
-  const MeltPoly &M;
   Tab T;
   int x0, y0;  // first output column, first output row (input rows y0-1 .. y0+kTR)
   int gw, lane, gtid;  // warp and lane within the group, thread of the group
   int col, gi, bc;     // the lane's first cell: tile column, global column, box column
   uint32_t outm;       // per cell of the lane: an interior (output) cell
-  __device__ TileView(const StepCoef &K_, const Coef<double> &F_, const StepScalars &PS_, const MeltPoly &M_,
-                      const double *tab, int tab_len, int x0_, int y0_, int gtid_)
-      : K(K_), F(F_), PS(PS_), M(M_), T(tab, tab_len), x0(x0_), y0(y0_), gw(gtid_ >> 5), lane(gtid_ & 31),
-        gtid(gtid_) {
+  __device__ TileView(const StepCoef &K_, const Coef<double> &F_, const StepScalars &PS_, const double *tab,
+                      int tab_len, int x0_, int y0_, int gtid_)
+      : K(K_), F(F_), PS(PS_), T(tab, tab_len), x0(x0_), y0(y0_), gw(gtid_ >> 5), lane(gtid_ & 31), gtid(gtid_) {
     col = 2 * lane;
     gi = x0 + col;
     bc = col + 4;
@@ -261,6 +235,25 @@ struct TileView {
       if (gi + q >= 1 && gi + q <= K.nx - 2) outm |= 1u << q;
   }
 };
+
+// The column table entries a lane uses: RT and C0 of its two columns, dK of
+// the faces left of its columns and of the next one.  The tile kernel loads
+// them before it waits for its tile, so their latency hides under the load.
+struct LaneCols {
+  double RT[2], C0[2], dK[3];
+};
+__device__ __forceinline__ LaneCols lane_cols(const TileView &V) {
+  LaneCols L;
+  const double2 RTv = ld2(V.T.RT + V.gi), C0v = ld2(V.T.C0 + V.gi);
+  L.RT[0] = RTv.x;
+  L.RT[1] = RTv.y;
+  L.C0[0] = C0v.x;
+  L.C0[1] = C0v.y;
+  L.dK[0] = V.T.DK[V.gi - 1];  // faces x-1|x for x = col .. col+2
+  L.dK[1] = V.T.DK[V.gi];
+  L.dK[2] = V.T.DK[V.gi + 1];
+  return L;
+}
 
 // columns beyond the array (right-most tiles; zero-filled by TMA) become
 // bulk melt, so they never force the general path; no output reads them.
@@ -280,18 +273,13 @@ __device__ __forceinline__ bool fix_beyond(const TileView &V, InSlot &in) {
 // ---- phase 1: per-cell terms of the input rows of group warp gw (rows gw,
 // gw+4, ...) and of the halo columns (group threads 64..99); st.liq and
 // st.sol must be 0 on entry
-__device__ __forceinline__ void phase1(const TileView &V, const InSlot &in, StSlot &st) {
+__device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, const InSlot &in, StSlot &st) {
   const Coef<double> &F = V.F;
   const int lane = V.lane, bc = V.bc;
   const double cinf = F.cinf;
   constexpr double KL = -2.0 * kL0Liq;
-  // delta range of the bulk-melt form: s = delta / (A + B delta) with
-  // A = 2 cinf (1 - cinf), B = 1 - 2 cinf, so |s| < 1/9 for
-  // -A/(9+B) < delta < A/(9-B) (taken 0.1 % inside)
-  const double sA = 2.0 * cinf * (1.0 - cinf), sB = 1.0 - 2.0 * cinf;
-  const double d_hi = 0.999 * sA / (9.0 - sB), d_lo = -0.999 * sA / (9.0 + sB);
-  const double2 RTv = ld2(V.T.RT + V.gi), C0v = ld2(V.T.C0 + V.gi);
-  const double RTa[2] = {RTv.x, RTv.y}, C0a[2] = {C0v.x, C0v.y};
+  const double d_hi = F.ser_hi, d_lo = F.ser_lo;  // series range of delta (Coef)
+  const double RTa[2] = {LC.RT[0], LC.RT[1]}, C0a[2] = {LC.C0[0], LC.C0[1]};
   // per lane, bit q: psi is exactly +1 over the 3x3 neighbourhood of cell
   // bc+q (rows of the box only; column -1 of the left-most tile enters no
   // face, column 0 being a ghost).  S = q(1) c (1 - c) = 0 there, so every
@@ -311,16 +299,22 @@ __device__ __forceinline__ void phase1(const TileView &V, const InSlot &in, StSl
     const uint32_t e = lf | (v << 1) | (rt << 3);  // bit k: box column bc-1+k
     return e & (e >> 1) & (e >> 2) & 0x3u;
   };
+  // constants of the row loop in registers (one read of the launch
+  // arguments, not one per row)
+  double ma[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) ma[k] = F.melt_a[k];
+  const double tiny = F.melt_tiny;
+  const int rows_in = V.K.ny - V.y0;  // input rows inside the array: rr <= ny - y0
+  // this warp's row flags (warp-uniform), OR-ed into st.liq / st.sol once
+  uint32_t liq_rows = 0u, sol_rows = 0u;
 #pragma unroll 1
   for (int rr = V.gw; rr < kTRin; rr += kWarps) {
-    if (V.y0 - 1 + rr > V.K.ny - 1) {  // beyond the array (last tile): never read by an output
+    if (rr > rows_in) {  // beyond the array (last tile): never read by an output
       st2(&st.S[rr][bc], 0.0, 0.0);
       st2(&st.mu[rr][bc], 0.0, 0.0);
-      st.pmask[rr][lane] = 0x33u;
-      if (lane == 0) {
-        atomicOr(&st.liq, 1u << rr);
-        atomicOr(&st.sol, 1u << rr);
-      }
+      liq_rows |= 1u << rr;
+      sol_rows |= 1u << rr;
       continue;
     }
     const double2 pv2 = ld2(&in.psi[rr][bc]), cv2 = ld2(&in.c[rr][bc]);
@@ -331,23 +325,22 @@ __device__ __forceinline__ void phase1(const TileView &V, const InSlot &in, StSl
     const bool liq2 = b0 == kMinus1 && b1 == kMinus1;
     const bool sol2 = b0 == kPlus1 && b1 == kPlus1;
     uint32_t code;
-    if (__all_sync(FULL, liq2 && fmax(fabs(dv[0]), fabs(dv[1])) <= V.M.tiny)) {
-      // far melt: g = -1, q = 1, lam by its Taylor polynomial in delta;
-      // mu'' = RT lam - 2 L0_Liq delta = delta (RT p + KL), lam = delta p
+    if (__all_sync(FULL, liq2 && fmax(fabs(dv[0]), fabs(dv[1])) <= tiny)) {
+      // far melt: g = -1, q = 1, lam by its Taylor polynomial in delta
+      // (Coef::melt_a, six terms); mu'' = RT lam - 2 L0_Liq delta
+      // = delta (RT p + KL), lam = delta p
       code = 1u;
-      st.pmask[rr][lane] = 0x03u;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
-        double p = V.M.a[kMeltTerms - 1];
+        double p = ma[5];
 #pragma unroll
-        for (int k = kMeltTerms - 2; k >= 0; --k) p = fma(p, dv[q], V.M.a[k]);
+        for (int k = 4; k >= 0; --k) p = fma(p, dv[q], ma[k]);
         Sv[q] = cv[q] * (1.0 - cv[q]);
         mv[q] = dv[q] * fma(RTa[q], p, KL);
       }
     } else if (__all_sync(FULL, liq2 && fmax(dv[0], dv[1]) < d_hi && fmin(dv[0], dv[1]) > d_lo)) {
       // bulk melt: g = -1, q = 1
       code = 1u;
-      st.pmask[rr][lane] = 0x03u;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const double c = cv[q], om = 1.0 - c;
@@ -361,7 +354,6 @@ __device__ __forceinline__ void phase1(const TileView &V, const InSlot &in, StSl
       // the same fluxes
       const uint32_t s3 = (code & 2u) ? solid3(rr) : 0u;
       if ((code & 2u) && __all_sync(FULL, s3 == 0x3u)) {
-        st.pmask[rr][lane] = 0x30u;
         Sv[0] = Sv[1] = mv[0] = mv[1] = 0.0;
       } else {
         double sv[2];
@@ -384,10 +376,12 @@ __device__ __forceinline__ void phase1(const TileView &V, const InSlot &in, StSl
     }
     st2(&st.S[rr][bc], Sv[0], Sv[1]);
     st2(&st.mu[rr][bc], mv[0], mv[1]);
-    if (lane == 0) {
-      if (code & 1u) atomicOr(&st.liq, 1u << rr);
-      if (code & 2u) atomicOr(&st.sol, 1u << rr);
-    }
+    liq_rows |= (code & 1u) << rr;
+    sol_rows |= ((code >> 1) & 1u) << rr;
+  }
+  if (lane == 0) {
+    if (liq_rows) atomicOr(&st.liq, liq_rows);
+    if (sol_rows) atomicOr(&st.sol, sol_rows);
   }
   // halo columns x0-1 and x0+kW, one thread per cell, on group warps 2 and
   // 3, which have one input row fewer than warps 0 and 1
@@ -413,13 +407,15 @@ __device__ __forceinline__ void phase1(const TileView &V, const InSlot &in, StSl
 // ---- phase 2: group warp gw computes output rows 1 + 4gw .. 4 + 4gw:
 // fluxes, the c update into dn, the interface cells into the list (nlist
 // must be 0 on entry).  Returns the listed cells, 2 bits per output row.
-__device__ __forceinline__ uint32_t phase2(const TileView &V, const InSlot &in, const StSlot &st, P2Smem &p2,
+__device__ __forceinline__ uint32_t phase2(const TileView &V, const LaneCols &LC, const InSlot &in,
+                                           const StSlot &st, P2Smem &p2,
                                            double dn[kRowsPerWarp][2], double &mass, bool red) {
   const Coef<double> &F = V.F;
   const int lane = V.lane, bc = V.bc;
-  const double cflux4 = 0.25 * F.cflux;
+  const double cflux4 = 0.25 * F.cflux, c_floor = F.c_floor;
+  const int rows_live = V.K.ny - 1 - V.y0;  // output rows inside the interior: rr <= ny - 1 - y0
   const uint32_t liq = st.liq, sol = st.sol;
-  const double dKa[3] = {V.T.DK[V.gi - 1], V.T.DK[V.gi], V.T.DK[V.gi + 1]};  // faces x-1|x for x = col .. col+2
+  const double dKa[3] = {LC.dK[0], LC.dK[1], LC.dK[2]};  // faces x-1|x for x = col .. col+2
   struct Row {
     double s[2], m[2], sl, sr, ml, mr;
   };
@@ -483,8 +479,8 @@ __device__ __forceinline__ uint32_t phase2(const TileView &V, const InSlot &in, 
     const double cv[2] = {cv2.x, cv2.y};
 #pragma unroll
     for (int q = 0; q < 2; ++q)
-      dn[j][q] = fmax(fma(cflux4, (jh[q + 1] - jh[q]) + (jv_hi[q] - jv_lo[q]), cv[q]), F.c_floor);
-    const bool live = V.y0 - 1 + rr <= V.K.ny - 2;
+      dn[j][q] = fmax(fma(cflux4, (jh[q + 1] - jh[q]) + (jv_hi[q] - jv_lo[q]), cv[q]), c_floor);
+    const bool live = rr <= rows_live;
     if (red && live) {
 #pragma unroll
       for (int q = 0; q < 2; ++q)
@@ -494,8 +490,11 @@ __device__ __forceinline__ uint32_t phase2(const TileView &V, const InSlot &in, 
     const uint32_t w3 = 7u << (rr - 1);
     if (live && (liq & w3) != w3 && (sol & w3) != w3) {
       // per input row k: bits 0-1 psi <= -1, bits 4-5 psi >= 1 of the lane's cells
-      const uint32_t pk = (uint32_t)st.pmask[rr - 1][lane] | ((uint32_t)st.pmask[rr][lane] << 8) |
-                          ((uint32_t)st.pmask[rr + 1][lane] << 16);
+      // (rows flagged all -1 / all +1 store no masks: 0x03 / 0x30)
+      auto pm = [&](int k) -> uint32_t {
+        return ((liq >> k) & 1u) ? 0x03u : ((sol >> k) & 1u) ? 0x30u : (uint32_t)st.pmask[k][lane];
+      };
+      const uint32_t pk = pm(rr - 1) | (pm(rr) << 8) | (pm(rr + 1) << 16);
       const uint32_t lf = __shfl_up_sync(FULL, pk, 1), rt = __shfl_down_sync(FULL, pk, 1);
       // left neighbour's second cell: its bits 1 and 5; right neighbour's first: bits 0 and 4
       uint32_t lL = 0u, lS = 0u, rL = 0u, rS = 0u;
@@ -590,18 +589,32 @@ __device__ __forceinline__ void phase4_rows(const TileView &V, InSlot &in, const
   for (int j = 0; j < kRowsPerWarp; ++j) {
     const int rr = rbase + j;
     const double2 pv2 = ld2(&in.psi[rr][bc]);
-    const double pv[2] = {pv2.x, pv2.y};
-    const bool live = V.y0 - 1 + rr <= V.K.ny - 2;
-    double po[2];
+    // phi_next = phi where uniformly +-1: an output cell is not listed only
+    // where psi <= -1 or >= 1 over its 3x3 neighbourhood, so clamp(psi) is
+    // its sign (cells outside the interior are not stored or are overwritten
+    // by the ghost copies); listed cells take phase 3's result
+    double po[2] = {pv2.x > 0.0 ? 1.0 : -1.0, pv2.y > 0.0 ? 1.0 : -1.0};
+    const uint32_t lb = (needs_all >> (2 * j)) & 3u;
+    if (lb) {
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const bool listed = (needs_all >> (2 * j + q)) & 1u;
-      po[q] = listed ? np[rr][bc + q] : clamp1(pv[q]);  // phi_next = phi where uniformly +-1
-      if (red && live && !listed && ((V.outm >> q) & 1u) && po[q] > 0.0)
-        itip = max(itip, V.gi + q == V.K.nx - 2 ? V.K.nx - 1 : V.gi + q);
+      for (int q = 0; q < 2; ++q)
+        if ((lb >> q) & 1u) po[q] = np[rr][bc + q];
     }
     st2(&in.psi[rr][bc], po[0], po[1]);
     st2(&in.c[rr][bc], dn[j][0], dn[j][1]);
+  }
+  if (red) {  // coarse tip: the last column with phi > 0 (listed cells counted again, harmlessly)
+    const int rows_live = V.K.ny - 1 - V.y0, nx = V.K.nx;
+#pragma unroll
+    for (int j = 0; j < kRowsPerWarp; ++j) {
+      const int rr = rbase + j;
+      const double2 po2 = ld2(&in.psi[rr][bc]);
+      const double po[2] = {po2.x, po2.y};
+      if (rr > rows_live) continue;
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+        if (((V.outm >> q) & 1u) && po[q] > 0.0) itip = max(itip, V.gi + q == nx - 2 ? nx - 1 : V.gi + q);
+    }
   }
 }
 
@@ -704,29 +717,7 @@ __device__ __forceinline__ void finish_tile(const TileView &V, P2Smem &p2, doubl
   gsync(bar);
   if (!p2.last) return;
   __threadfence();
-  for (int v = V.gtid; v < 256; v += kThreads) {
-    double m = 0.0;
-    int it = 0;
-    for (int k = v; k < FR->nparts; k += 256) {
-      m += __ldcg(&FR->partials[k].mass);
-      it = max(it, __ldcg(&FR->partials[k].itip));
-    }
-    sm_m[v] = m;
-    sm_i[v] = it;
-  }
-  gsync(bar);
-  for (int sz = 128; sz > 0; sz >>= 1) {
-    for (int v = V.gtid; v < sz; v += kThreads) {
-      sm_m[v] += sm_m[v + sz];
-      sm_i[v] = max(sm_i[v], sm_i[v + sz]);
-    }
-    gsync(bar);
-  }
-  if (V.gtid == 0) {
-    if (FR->mass_out) *FR->mass_out = sm_m[0] + FR->mass_offset;
-    if (FR->itip_out) *FR->itip_out = max(1, sm_i[0]);  // get_itip_all_grain starts at 1
-    *FR->counter = 0u;
-  }
+  final_reduce(*FR, sm_m, sm_i, V.gtid, [&] { gsync(bar); });
 }
 
 // tile (row tr, column tc) of the launch order: tile columns from the one
@@ -743,15 +734,14 @@ __global__ void __launch_bounds__(kThreads, 5)
                     const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
                     const __grid_constant__ CUtensorMap tm_c, const double *__restrict__ tab, const int tab_len,
                     double *__restrict__ psi_n, double *__restrict__ c_n, double *__restrict__ phi_n,
-                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR,
-                    const __grid_constant__ MeltPoly MP, const int wave) {
+                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int wave) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TileSmem64 &sm = *reinterpret_cast<TileSmem64 *>(smem_raw);
   // blockIdx.x walks the tile rows of one tile column, blockIdx.y the tile
   // columns, from the one holding column PS.i_front
   const int f = max(PS.i_front, 0) / kW;
-  int tr, tc;
-  tile_of((int)(blockIdx.y * gridDim.x + blockIdx.x), (int)gridDim.x, (int)gridDim.y, f, tr, tc);
+  // tile t = blockIdx.y * gridDim.x + blockIdx.x of tile_of's order
+  const int tr = (int)blockIdx.x, tc = front_first_block((int)blockIdx.y, f, (int)gridDim.y);
   const int x0 = kW * tc, y0 = 1 + kTR * tr;
   BlockPartial *part = partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr;
   const FinalRed *FRp = partials && FR.counter ? &FR : nullptr;
@@ -772,7 +762,10 @@ __global__ void __launch_bounds__(kThreads, 5)
   }
   // the column table of this step (programmatic dependency on its kernel)
   asm volatile("griddepcontrol.wait;" ::: "memory");
-  const TileView V(K, F, PS, MP, tab, tab_len, x0, y0, (int)threadIdx.x);
+  // the step's final reduction (a programmatic dependent) may be scheduled now
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const TileView V(K, F, PS, tab, tab_len, x0, y0, (int)threadIdx.x);
+  const LaneCols LC = lane_cols(V);
   __syncthreads();  // barrier initialised, flags cleared
   {
     // bounded wait for the tile; if any thread gives up, the whole CTA skips
@@ -801,7 +794,7 @@ __global__ void __launch_bounds__(kThreads, 5)
     }
   }
   if (fix_beyond(V, sm.in)) __syncthreads();
-  phase1(V, sm.in, sm.st);
+  phase1(V, LC, sm.in, sm.st);
   __syncthreads();
   // phase 1 done: pull the tile of the CTA that will start about one resident
   // wave later into L2, so its loads overlap the rest of this wave's arithmetic
@@ -818,7 +811,7 @@ __global__ void __launch_bounds__(kThreads, 5)
   double mass = 0.0;
   int itip = 0;
   double dn[kRowsPerWarp][2];
-  const uint32_t needs_all = phase2(V, sm.in, sm.st, sm.p2, dn, mass, red);
+  const uint32_t needs_all = phase2(V, LC, sm.in, sm.st, sm.p2, dn, mass, red);
   __syncthreads();
   phase3(V, sm.in, sm.p2, sm.st.S, red, itip);  // S is free after phase 2
   __syncthreads();
@@ -866,8 +859,8 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
                     const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
                     const __grid_constant__ CUtensorMap tm_c, const double *__restrict__ tab, const int tab_len,
                     double *__restrict__ psi_n, double *__restrict__ c_n, double *__restrict__ phi_n,
-                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR,
-                    const __grid_constant__ MeltPoly MP, const int nrt, const int ncb) {
+                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int nrt,
+                    const int ncb) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   PipeSmem64 &sm = *reinterpret_cast<PipeSmem64 *>(smem_raw);
   const int warp = threadIdx.x >> 5;
@@ -895,6 +888,8 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
   }
   // the column table of this step (programmatic dependency on its kernel)
   asm volatile("griddepcontrol.wait;" ::: "memory");
+  // the step's final reduction (a programmatic dependent) may be scheduled now
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   __syncthreads();
 
   if (warp == 0) {
@@ -933,14 +928,14 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
       if (!group_and(ok, kBarP1)) break;
       int tr, tc;
       tile_of(t, nrt, ncb, f, tr, tc);
-      const TileView V(K, F, PS, MP, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
+      const TileView V(K, F, PS, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
       if (gtid == 0) {
         sm.st[q].liq = 0u;
         sm.st[q].sol = 0u;
       }
       fix_beyond(V, sm.in[s]);
       gsync(kBarP1);
-      phase1(V, sm.in[s], sm.st[q]);
+      phase1(V, lane_cols(V), sm.in[s], sm.st[q]);
       gsync(kBarP1);
       if (gtid == 0) mbar_arrive(&sm.st_full[q]);
     }
@@ -954,7 +949,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
     if (!group_and(pipe_wait(&sm.st_full[q], (k / kStage) & 1, abort, limit, err, poll), kBarP2)) break;
     int tr, tc;
     tile_of(t, nrt, ncb, f, tr, tc);
-    const TileView V(K, F, PS, MP, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
+    const TileView V(K, F, PS, tab, tab_len, kW * tc, 1 + kTR * tr, gtid);
     BlockPartial *part = partials ? partials + ((int64_t)tc * nrt + tr) : nullptr;
     const bool red = part != nullptr;
     if (gtid == 0) sm.p2.nlist = 0;
@@ -962,7 +957,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
     double mass = 0.0;
     int itip = 0;
     double dn[kRowsPerWarp][2];
-    const uint32_t needs_all = phase2(V, sm.in[s], sm.st[q], sm.p2, dn, mass, red);
+    const uint32_t needs_all = phase2(V, lane_cols(V), sm.in[s], sm.st[q], sm.p2, dn, mass, red);
     gsync(kBarP2);
     phase3(V, sm.in[s], sm.p2, sm.st[q].S, red, itip);  // S of the slot is free after phase 2
     gsync(kBarP2);
@@ -1012,26 +1007,28 @@ int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScal
   cfg.attrs = at;
   cfg.numAttrs = 1;
   const double *tab = tm.col_tab64;
-  const MeltPoly mp = make_melt_poly(F.cinf);
+  // the final reduction is a programmatic dependent launch after the step
   FinalRed fr = tm.red;
   fr.partials = partials;
   fr.nparts = nparts;
-  if (!partials || !(fr.mass_out || fr.itip_out)) fr.counter = nullptr;
+  FinalRed none = fr;
+  none.counter = nullptr;
   cudaError_t e;
   if (pipe) {
     // persistent: every CTA resident at once, each walking tiles b, b + G, ...
     cfg.gridDim = dim3((unsigned)std::min(resident, nparts));
     cfg.blockDim = dim3(kPipeThreads);
     e = cudaLaunchKernelEx(&cfg, pipe_kernel_f64, K, F, P, tm.psi, tm.c, tab, tm.col_tab64_len, psi_n, c_n, phi_n,
-                           partials, err, fr, mp, nrt, ncb);
+                           partials, err, none, nrt, ncb);
   } else {
     // column-major: consecutive CTAs share a column strip and its halo rows in L2
     cfg.gridDim = dim3(nrt, ncb);
     cfg.blockDim = dim3(kThreads);
     e = cudaLaunchKernelEx(&cfg, tile_kernel_f64, K, F, P, tm.psi, tm.c, tab, tm.col_tab64_len, psi_n, c_n, phi_n,
-                           partials, err, fr, mp, resident);
+                           partials, err, none, resident);
   }
   if (e != cudaSuccess) return -3;
+  if (partials && (fr.mass_out || fr.itip_out) && launch_reduce_partials_dep(fr, st)) return -3;
   if (nparts_out) *nparts_out = nparts;
   return 0;
 }

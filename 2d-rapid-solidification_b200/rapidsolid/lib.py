@@ -7,6 +7,8 @@ raises at load time.
 import ctypes as C
 import os
 
+import numpy as np
+
 from . import _abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -79,6 +81,8 @@ def load():
         "rs_ensemble_bind": ([vp, i32, vp, vp], C.c_int),
         "rs_ensemble_steps": ([vp, i64, vp], C.c_int),
         "rs_ensemble_state": ([vp, i32, vp, vp, vp, vp], C.c_int),
+        "rs_host_alloc": ([sz, C.POINTER(vp), C.POINTER(vp)], C.c_int),
+        "rs_host_free": ([vp], C.c_int),
         "rs_ensemble_autotune": ([vp, i32, vp, vp, vp], C.c_int),
         "rs_ensemble_set_path": ([vp, i32], C.c_int),
         "rs_surrogate_audit": ([vp, vp, vp, vp, vp, vp], C.c_int),
@@ -166,6 +170,41 @@ def _ptr(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 
 
+def _addr(x):
+    """A device-writable address: a tensor's data, or an int (e.g. a
+    HostBuffer's device address), or None."""
+    if x is None:
+        return None
+    return x if isinstance(x, int) else x.data_ptr()
+
+
+class HostBuffer:
+    """Mapped page-locked host memory (rs_host_alloc): `host` is a numpy view
+    of it, `device` its device address (an int).  A step given
+    device + 8 k as mass_out writes its mass into host[k]."""
+
+    def __init__(self, n, dtype=np.float64):
+        self.lib = load()
+        self.n, self.dtype = n, np.dtype(dtype)
+        h, d = C.c_void_p(), C.c_void_p()
+        check(self.lib.rs_host_alloc(n * self.dtype.itemsize, C.byref(h), C.byref(d)))
+        self._h = h
+        self.device = d.value
+        self.host = np.ctypeslib.as_array((C.c_byte * (n * self.dtype.itemsize)).from_address(h.value)).view(self.dtype)
+
+    def close(self):
+        if self._h:
+            self.host = None
+            self.lib.rs_host_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _stream(stream):
     import torch
     if stream is None:
@@ -240,8 +279,8 @@ class Context:
         a.i_left_end_T = i_left_end_T
         a.l_offset_Vp = l_offset_Vp
         a.T_coarse = None if T_coarse is None else T_coarse.data_ptr()
-        a.mass_out = None if mass_out is None else mass_out.data_ptr()
-        a.itip_out = None if itip_out is None else itip_out.data_ptr()
+        a.mass_out = _addr(mass_out)
+        a.itip_out = _addr(itip_out)
         fc, fn = cur.fields(), nxt.fields()
         check(self.lib.rs_step(self._h, C.byref(fc), C.byref(fn), C.byref(a), _stream(stream)))
 
@@ -312,6 +351,12 @@ def tip_from_bytes(buf):
     return t
 
 
+# the ensemble's stepping paths (include/rs_b200.h RS_ENS_PATHS): three tile
+# shapes (output rows of a 128-column tile) x two launch forms x three orders
+ENS_SHAPE_ROWS = (16, 8, 32)
+ENS_PATHS = 6 * len(ENS_SHAPE_ROWS)
+
+
 class Ensemble:
     """Batched ensemble of FP32 runs (rs_ensemble_*): one launch steps all runs,
     pull-back-free stretches replay a CUDA graph.  runs: list of _abi.Params."""
@@ -344,16 +389,18 @@ class Ensemble:
         return st.value, h.value, l.value, self.sets[run][cur.value]
 
     def autotune(self, reps=5, stream=None):
-        """(path, [mean ms of one step on the six paths]): paths 0-2 per-step
-        launches (graph replays) with tile orders run by run, largest first,
-        interleaved; 3-5 the persistent walk with the same orders."""
-        ms = (C.c_double * 6)()
+        """(path, [mean ms of one step on the ENS_PATHS paths]): path k uses
+        the tile shape k // 6 (ENS_SHAPE_ROWS rows by 128 columns); k % 6 =
+        0-2 per-step launches (graph replays) with tile orders run by run,
+        largest first, interleaved; 3-5 the persistent walk with the same
+        orders."""
+        ms = (C.c_double * ENS_PATHS)()
         ch = C.c_int32()
         check(self.lib.rs_ensemble_autotune(self._h, reps, ms, C.byref(ch), _stream(stream)))
         return ch.value, list(ms)
 
     def set_path(self, path):
-        """select a stepping path (0..5, as autotune numbers them)"""
+        """select a stepping path (0 .. ENS_PATHS - 1, as autotune numbers them)"""
         check(self.lib.rs_ensemble_set_path(self._h, path))
 
     def close(self):

@@ -19,8 +19,8 @@ steps (outside the events): a 256 MiB buffer is written, then another
 not pay the write-back of the flush's dirty lines.
 e2e: one output interval of the reference loop (step_fields = 200 steps,
 fun.cu:437-446) through the C-ABI from pinned host buffers: H2D of the
-fields (a restart), every step's fused FP64 solute-mass reduction read back
-to the host, D2H of the fields (the snapshot), all in one event-timed region.
+fields (a restart), every step's FP64 solute-mass reduction read back to the
+host, D2H of the fields (the snapshot), all in one event-timed region.
 
 python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 Under torchrun each rank runs an independent replica (the path has no
@@ -42,13 +42,14 @@ UNIT = "Gcell-steps/s"
 BYTES_PER_CELL = {"f32": 16, "f64": 32}  # psi, c read once + written once
 WORKLOAD = ("Ti-10Nb directional solidification 2048x2048, exact CALPHAD, frozen T G=5e6 K/m V=0.5 m/s, "
             "moving frame, interface noise 0.01")
-# kernels a step launches: the FP32 tile path (column table + tile, mass
-# reduction fused), the FP64 tile path (the same), and the register-prefetch
-# kernel that pull-back steps take (plus one reduction launch for the mass)
+# kernels a step launches: the FP32 tile path (column table + tile, plus the
+# mass reduction as a programmatic dependent launch when the mass is read),
+# the FP64 tile path (the same), and the register-prefetch kernel that
+# pull-back steps take (plus one reduction launch for the mass)
 # (kernel of the roofline, launches of a step without pull-back, whether the
 # mass reduction is fused into that kernel)
-STEP_PATH = {"f32": ("rs::tile_kernel<false>", 2, True),
-             "f64": ("rs::tile_kernel_f64", 2, True)}
+STEP_PATH = {"f32": ("rs::tile_kernel<false>", 2, False),
+             "f64": ("rs::tile_kernel_f64", 2, False)}
 # the tile steps' kernel (RS_OPT_PIPELINE): 0 one tile per CTA, 1 the
 # persistent warp-role pipeline (the other one is timed beside it)
 PIPELINE = 0
@@ -231,18 +232,18 @@ def timed_steps(loop, steps, flush, st, nvtx=None):
 def e2e_interval(loop, nsteps, dist, world, st):
     """One output interval of the reference loop through the C-ABI, from
     pinned host fields: H2D of psi and c (a restart), nsteps steps each with
-    its FP64 solute mass read back on a copy stream, D2H of psi and c (the
-    field snapshot of set_fields_output, fun.cu:621-666)."""
+    its FP64 solute mass written by the device into mapped host memory, D2H
+    of psi and c (the field snapshot of set_fields_output, fun.cu:621-666)."""
     torch = loop.torch
     p = loop.p
     h_psi = torch.empty((p.ny_all, p.nx_all), dtype=loop.dtype, pin_memory=True)
     h_c = torch.empty_like(h_psi).pin_memory()
     h_psi.copy_(loop.a.psi)
     h_c.copy_(loop.a.c)
-    h_mass = torch.zeros(nsteps, dtype=torch.float64, pin_memory=True)
-    d_mass = torch.zeros(nsteps, dtype=torch.float64, device="cuda")
-    cs = torch.cuda.Stream()
-    done = [torch.cuda.Event() for _ in range(nsteps)]
+    # every step's mass goes straight into mapped page-locked host memory
+    # (rs_host_alloc): the step's reduction writes it there, no copy call
+    from rapidsolid import lib
+    h_mass = lib.HostBuffer(nsteps)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -251,16 +252,16 @@ def e2e_interval(loop, nsteps, dist, world, st):
     loop.a.psi.copy_(h_psi, non_blocking=True)
     loop.a.c.copy_(h_c, non_blocking=True)
     for k in range(nsteps):
-        loop.step(mass_out=d_mass[k:k + 1])
-        done[k].record(st)
-        cs.wait_event(done[k])
-        with torch.cuda.stream(cs):
-            h_mass[k:k + 1].copy_(d_mass[k:k + 1], non_blocking=True)
+        loop.step(mass_out=h_mass.device + 8 * k)
     h_psi.copy_(loop.a.psi, non_blocking=True)
     h_c.copy_(loop.a.c, non_blocking=True)
-    st.wait_stream(cs)
     e1.record(st)
     torch.cuda.synchronize()
+    import numpy as np
+    masses = h_mass.host.copy()
+    h_mass.close()
+    if not (np.isfinite(masses).all() and masses.min() > 0):
+        raise RuntimeError("e2e: a step's mass did not arrive in host memory")
     ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     cells = (p.nx_all - 2) * (p.ny_all - 2)
     field_bytes = 2 * h_psi.numel() * h_psi.element_size()
@@ -269,8 +270,8 @@ def e2e_interval(loop, nsteps, dist, world, st):
             "d2h_bytes_per_step": round(8 + field_bytes / nsteps, 1), "ms_per_step": round(ms / nsteps, 5),
             "interval_steps": nsteps,
             "note": "C-ABI rs_step over one output interval of the reference loop (step_fields steps): H2D of "
-                    "psi and c from pinned memory, every step's FP64 mass read back on a copy stream, D2H of "
-                    "psi and c; no L2 flush"}
+                    "psi and c from pinned memory, every step's FP64 mass written by the device into mapped "
+                    "page-locked host memory (rs_host_alloc), D2H of psi and c; no L2 flush"}
 
 
 def kernel_name(prec, options):
@@ -817,10 +818,11 @@ def _ensemble_tips(ens, runs):
     return xs
 
 
-# the ensemble's stepping paths (rs_ensemble_autotune): per-step launches replayed
-# from a CUDA graph, or the persistent walk, each with three tile orders
-ENS_PATHS = ["graph, run by run", "graph, largest first", "graph, interleaved", "walk, run by run",
-             "walk, largest first", "walk, interleaved"]
+# the ensemble's stepping paths (rs_ensemble_autotune): per tile shape (rows x
+# 128 columns), per-step launches replayed from a CUDA graph or the persistent
+# walk, each with three tile orders
+ENS_PATHS = [f"{rows}x128 tiles, {form}, {order}" for rows in (16, 8, 32) for form in ("graph", "walk")
+             for order in ("run by run", "largest first", "interleaved")]
 
 
 def _timed_ensemble(ens, flush, nsteps):
@@ -858,8 +860,8 @@ def ensemble_leg(flush, nruns=64, nsteps=100, vel_steps=4000):
     ms = _timed_ensemble(ens, flush, nsteps)
     out["exact"] = {"value": round(cells * nsteps / (ms * 1e-3) / 1e9, 3), "ms_per_step": round(ms / nsteps, 5),
                     "autotune": {"choice": ENS_PATHS[choice], "ms_per_step_of_path": [round(x, 5) for x in tune_ms]}}
-    # the two stepping paths with the autotuned tile order
-    for name, path in (("graph", choice % 3), ("walk", 3 + choice % 3)):
+    # the two stepping paths with the autotuned tile shape and order
+    for name, path in (("graph", 6 * (choice // 6) + choice % 3), ("walk", 6 * (choice // 6) + 3 + choice % 3)):
         ens.set_path(path)
         msp = _timed_ensemble(ens, flush, nsteps)
         out["exact"]["path_" + name] = {"value": round(cells * nsteps / (msp * 1e-3) / 1e9, 3),

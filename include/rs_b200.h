@@ -147,8 +147,10 @@ typedef struct rs_step_args {
   int32_t reserved;
   double l_offset_Vp;       /* pulled distance in W */
   const void *T_coarse;     /* TFC: coarse T (double, NxT_all x NyT_all) */
-  double *mass_out;         /* device: if set, receives sum of interior c_next */
-  int32_t *itip_out;        /* device: if set, receives max i with psi_next>0 */
+  double *mass_out;         /* device-writable (device memory, or the device
+                               address of an rs_host_alloc buffer): if set,
+                               receives sum of interior c_next */
+  int32_t *itip_out;        /* device-writable: if set, receives max i with psi_next>0 */
 } rs_step_args;
 
 /* Precise tip (fun.cu:2612-2622 TIP). */
@@ -247,6 +249,16 @@ int rs_precise_tip_noalloc(const rs_params *p, const rs_fields *f, rs_tip *d_tip
 /* Sum of c over the interior cells in double precision into *d_mass: the
  * numerator of get_average (fun.cu:1756-1766), reduced on the device. */
 int rs_mass(rs_ctx *ctx, const rs_fields *f, double *d_mass, rs_stream_t stream);
+
+/* Page-locked host memory mapped into the device's address space (no
+ * counterpart in the reference, which copies get_average's inputs to the
+ * host): *host and *device address the same zeroed bytes.  Passing
+ * device-side addresses of it as rs_step_args.mass_out / itip_out lets the
+ * step's reduction write its result straight into host memory, so a host loop
+ * reads every step's mass after that step completes (an event or stream
+ * synchronisation) without a copy call.  Free with rs_host_free. */
+int rs_host_alloc(size_t bytes, void **host, void **device);
+int rs_host_free(void *host);
 
 /* ---- initial conditions ---- */
 /* Reference initial condition (kernel initial, fun.cu:983-1021): tanh front
@@ -382,16 +394,20 @@ int rs_ensemble_steps(rs_ens *e, int64_t nsteps, rs_stream_t stream);
 int rs_ensemble_state(rs_ens *e, int32_t run, int64_t *step, int32_t *i_offset_history, double *l_offset_Vp,
                       int32_t *current);
 /* Times the stepping paths over reps launches of one step without advancing
- * the runs and keeps the fastest: paths 0-2 launch the column tables and the
- * tiles per step (replayed from a CUDA graph) with the tile order 0 run by
- * run, 1 largest runs first, 2 runs interleaved; paths 3-5 are the same
+ * the runs and keeps the fastest.  Path k uses the tile shape k / 6: 128
+ * columns by 16 (shape 0, the single-run kernel's), 8 (shape 1) or 32
+ * (shape 2) rows.  Within a shape, k % 6 = 0-2 launch the column tables and
+ * the tiles per step (replayed from a CUDA graph) with the tile order 0 run
+ * by run, 1 largest runs first, 2 runs interleaved; k % 6 = 3-5 are the same
  * orders as the persistent walk, one cooperative launch per stretch of steps
  * without a pull-back (device-side grid barriers between the tables and the
  * tiles of a step and between steps, bounded: one that gives up sets the
- * status rs_device_status reports on run 0's context).  ms_out[6] receives
- * the mean times, *choice the path. */
+ * status rs_device_status reports on run 0's context).  ms_out[RS_ENS_PATHS]
+ * receives the mean times, *choice the path. */
+#define RS_ENS_PATHS 18
 int rs_ensemble_autotune(rs_ens *e, int32_t reps, double *ms_out, int32_t *choice, rs_stream_t stream);
-/* selects a stepping path (0..5, as rs_ensemble_autotune numbers them) */
+/* selects a stepping path (0 .. RS_ENS_PATHS - 1, as rs_ensemble_autotune
+ * numbers them) */
 int rs_ensemble_set_path(rs_ens *e, int32_t path);
 
 /* ---- 3D three-phase variant (one GPU) ----

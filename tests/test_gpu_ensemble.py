@@ -47,7 +47,9 @@ def single(p, sur=None):
     return a.psi.cpu().numpy(), a.c.cpu().numpy(), hist, l
 
 
-@pytest.mark.parametrize("path", ["autotuned", 0, 4])
+# paths: tile shape path // 6 (16, 8 or 32 rows by 128 columns), per-step
+# launches (path % 6 < 3) or the persistent walk, tile order path % 3
+@pytest.mark.parametrize("path", ["autotuned", 0, 4, 6, 11, 13, 15])
 def test_ensemble_equals_single_runs(path):
     ps = params()
     ens = lib.Ensemble(ps)
@@ -56,7 +58,7 @@ def test_ensemble_equals_single_runs(path):
         ens.ctx[r].initial_planar(a, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, 7)
         ens.bind(r, a, b)
     choice, ms = ens.autotune(reps=3)
-    assert choice in range(6) and len(ms) == 6 and all(m > 0 for m in ms)
+    assert choice in range(lib.ENS_PATHS) and len(ms) == lib.ENS_PATHS and all(m > 0 for m in ms)
     if path != "autotuned":
         ens.set_path(path)
     ens.steps(250)
@@ -74,7 +76,7 @@ def test_ensemble_equals_single_runs(path):
     ens.close()
 
 
-@pytest.mark.parametrize("path", [1, 5])
+@pytest.mark.parametrize("path", [1, 5, 8, 16])
 def test_ensemble_surrogate_path_equals_single_runs(path):
     """With a network set on every run's context, the batched launch takes
     the surrogate path of the tile kernel: each run equals the same run

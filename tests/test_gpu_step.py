@@ -368,6 +368,30 @@ def test_f32_tracks_f64_over_steps():
     assert abs(m32 - m64) / m64 <= 1e-9
 
 
+def test_mass_into_mapped_host_memory():
+    """rs_host_alloc: a step given the device address of mapped page-locked
+    host memory as mass_out / itip_out writes its reductions there; after the
+    stream synchronises the host reads the same values the step writes into
+    device memory, on both tile paths and on a pull-back step."""
+    p = make("default")
+    s = perturbed_state(p, 8, amp=0.3)
+    ctx = lib.Context(p)
+    hb = lib.HostBuffer(4)
+    hi = lib.HostBuffer(4, np.int32)
+    for dtype in (torch.float64, torch.float32):
+        for pb in (None, 2):
+            cur, nxt = upload(p, s, dtype), lib.FieldSet(p, dtype)
+            ctx.step(cur, nxt, 0, pull_back=pb, mass_out=hb.device, itip_out=hi.device)
+            m = torch.zeros(1, dtype=torch.float64, device="cuda")
+            it = torch.zeros(1, dtype=torch.int32, device="cuda")
+            ctx.step(cur, nxt, 0, pull_back=pb, mass_out=m, itip_out=it)
+            torch.cuda.synchronize()
+            assert hb.host[0] == m.item() and hi.host[0] == it.item(), (dtype, pb)
+            assert hb.host[1] == 0.0
+    hb.close()
+    hi.close()
+
+
 def test_fused_reductions_match_standalone():
     p = make("default")
     s = perturbed_state(p, 6, amp=0.3)
