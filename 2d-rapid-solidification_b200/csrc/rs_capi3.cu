@@ -24,6 +24,7 @@ struct rs3_ctx {
   struct Entry {
     const void *f1, *f2, *fc;
     int precision;
+    bool surr;  // maps for the surrogate's scalar kernel (energy 1, FP32)
     rs::P3Maps maps;
   } cache[4];
   int ncache, next;
@@ -64,15 +65,17 @@ bool fields_ok(const rs3_fields *f) {
          ((uintptr_t)f->phi1 % 16 == 0) && ((uintptr_t)f->phi2 % 16 == 0) && ((uintptr_t)f->c % 16 == 0);
 }
 
-bool encode_field(const rs3_params &p, const void *ptr, int precision, CUtensorMap *out) {
+// surr: the step runs the energy-1 FP32 surrogate kernel (its own box)
+bool encode_field(const rs3_params &p, const void *ptr, int precision, bool surr, CUtensorMap *out) {
   auto enc = encode3();
   if (!enc) return false;
   const size_t es = precision == RS_F64 ? 8 : 4;
   cuuint64_t dims[3] = {(cuuint64_t)p.nx, (cuuint64_t)p.ny, (cuuint64_t)p.nz};
   cuuint64_t strides[2] = {(cuuint64_t)p.nx * es, (cuuint64_t)p.nx * p.ny * es};
   const bool tinb = p.energy == 1;
-  cuuint32_t box[3] = {(cuuint32_t)(tinb ? rs::tinb_box_width(precision) : rs::peri3d_box_width(precision)),
-                       (cuuint32_t)(tinb ? rs::tinb_box_height() : rs::peri3d_box_height(precision)), 1};
+  cuuint32_t box[3] = {(cuuint32_t)(tinb ? rs::tinb_box_width(precision, surr) : rs::peri3d_box_width(precision)),
+                       (cuuint32_t)(tinb ? rs::tinb_box_height(precision, surr) : rs::peri3d_box_height(precision)),
+                       1};
   cuuint32_t estr[3] = {1, 1, 1};
   return enc(out, precision == RS_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
              const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -81,22 +84,24 @@ bool encode_field(const rs3_params &p, const void *ptr, int precision, CUtensorM
 }
 
 bool maps_of(rs3_ctx *c, const rs3_fields *f, rs::P3Maps *m) {
+  const bool surr = c->p.energy == 1 && f->precision == RS_F32 && c->surr.w != nullptr;
   for (int k = 0; k < c->ncache; ++k) {
     const rs3_ctx::Entry &e = c->cache[k];
-    if (e.f1 == f->phi1 && e.f2 == f->phi2 && e.fc == f->c && e.precision == f->precision) {
+    if (e.f1 == f->phi1 && e.f2 == f->phi2 && e.fc == f->c && e.precision == f->precision && e.surr == surr) {
       *m = e.maps;
       return true;
     }
   }
   rs::P3Maps n;
-  if (!encode_field(c->p, f->phi1, f->precision, &n.phi1) || !encode_field(c->p, f->phi2, f->precision, &n.phi2) ||
-      !encode_field(c->p, f->c, f->precision, &n.c))
+  if (!encode_field(c->p, f->phi1, f->precision, surr, &n.phi1) ||
+      !encode_field(c->p, f->phi2, f->precision, surr, &n.phi2) || !encode_field(c->p, f->c, f->precision, surr, &n.c))
     return false;
   rs3_ctx::Entry &e = c->cache[c->next];
   e.f1 = f->phi1;
   e.f2 = f->phi2;
   e.fc = f->c;
   e.precision = f->precision;
+  e.surr = surr;
   e.maps = n;
   c->next = (c->next + 1) % 4;
   if (c->ncache < 4) ++c->ncache;

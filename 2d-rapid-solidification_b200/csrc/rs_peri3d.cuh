@@ -47,8 +47,10 @@ int launch_peri3d_ghosts(const rs3_params &p, int precision, void *f1, void *f2,
 // the FP32 surrogate or null), mu of every cell at step 0's temperature,
 // and the two-grain initial state
 struct SurrArgs;
-int tinb_box_width(int precision);
-int tinb_box_height();
+// (surr: the FP32 step runs the surrogate's scalar kernel; otherwise FP32 runs
+// on packed pairs with the TiAg pair kernel's box)
+int tinb_box_width(int precision, bool surr);
+int tinb_box_height(int precision, bool surr);
 int tinb_table_len(const rs3_params &p);
 int launch_tinb_step(const rs3_params &p, const P3Maps &m, int precision, void *o1, void *o2, void *oc, int64_t step,
                      int *err, double *tab, const SurrArgs *surr, cudaStream_t st);

@@ -55,6 +55,12 @@ struct K3 {  // kernel constants in the working precision
   R AA, AA1;
   double RR, c_ref, c_off;
   const double *tab;
+  // energy 1, FP32 pair kernel: far-melt form of the solute log term,
+  // lam = log(c/(1-c)) - log(c_ref/(1-c_ref)) = sum_k melt_a[k-1] d^k for
+  // |d| <= melt_tiny, d = c - c_ref (four terms, |d| <= 1e-2 min(c_ref,
+  // 1-c_ref): the remainder is below 4e-9 of lam; see Coef::melt_a)
+  R melt_a[4];
+  R melt_tiny;
 };
 
 template <typename R>
@@ -100,6 +106,17 @@ K3<R> make_k3(const rs3_params &p) {
   k.c_ref = p.c_ref;
   k.c_off = 0.0;
   k.tab = nullptr;
+  for (int j = 0; j < 4; ++j) k.melt_a[j] = (R)0;
+  k.melt_tiny = (R)-1;  // never (energy 0 has no log term)
+  if (p.energy == 1 && p.c_ref > 0.0 && p.c_ref < 1.0) {
+    double pc = 1.0, pm = 1.0;
+    for (int j = 1; j <= 4; ++j) {
+      pc /= p.c_ref;
+      pm /= 1.0 - p.c_ref;
+      k.melt_a[j - 1] = (R)(((j % 2 ? pc : -pc) + pm) / j);
+    }
+    k.melt_tiny = (R)(1e-2 * (p.c_ref < 0.5 ? p.c_ref : 1.0 - p.c_ref));
+  }
   return k;
 }
 

@@ -28,6 +28,7 @@
 // Algorithmic bytes per cell-step: 3 fields read + 3 written.
 #include <cuda.h>
 
+#include "rs_f32x2.cuh"
 #include "rs_peri3d_common.cuh"
 #include "rs_surrogate.cuh"
 
@@ -434,6 +435,307 @@ __global__ void grains_init_kernel(const K3<R> k, const uint64_t seed, const dou
   }
 }
 
+// ---------------------------------------------------------------- FP32 exact step on packed pairs
+// The exact FP32 step of tinb_kernel<float> with every thread computing two
+// x-adjacent cells per instruction (add/sub/mul/fma.rn.f32x2, rs_f32x2.cuh;
+// each lane rounds as the scalar FP32 operation), in the tiling of the TiAg
+// pair kernel (rs_peri3d_x2.cu): output cells x0 .. x0+63 (x0 a multiple of
+// 64, pairs start on even x), rows y0+1 .. y0+14; input box x0-4 .. x0+67 x
+// y0 .. y0+15 per field and plane by 3D TMA into a four-slot ring; 224
+// threads, warp w owns rows 2w, 2w+1, lane j the pair x0+2j, x0+2j+1.  mu''
+// and S of each plane (tile and halo) are computed once into four-slot rings,
+// so one barrier per plane suffices, as in tinb_kernel.  The surrogate path
+// keeps the scalar kernel.
+constexpr int kT2Threads = 224, kT2BX = 64, kT2BXin = 72, kT2BY = 14, kT2BYin = 16;
+constexpr unsigned long long kOne2 = 0x3F8000003F800000ull, kAbs2 = 0x7FFFFFFF7FFFFFFFull;
+__device__ __forceinline__ unsigned long long f2bits(f2 v) { return (unsigned long long)v; }
+constexpr int kT2Plane = kT2BXin * kT2BYin;  // 1152 floats = 4608 bytes (36 x 128)
+constexpr int kT2Slots = 4, kT2MuSlots = 4;
+static_assert((kT2Plane * 4) % 128 == 0, "TMA destinations stay 128-byte aligned");
+static_assert(kT2Threads == 32 * (kT2BY / 2) && kT2BX == 64, "a warp per row pair, a lane per column pair");
+
+struct T2Smem {
+  alignas(128) float in[kT2Slots][3][kT2Plane];
+  alignas(16) float mu[kT2MuSlots][kT2Plane];  // mu'' (FP32 form, see mu_cell)
+  alignas(16) float S[kT2MuSlots][kT2Plane];   // face-mobility terms q(phi1) c (1 - c)
+  uint64_t full[kT2Slots];
+  // per plane (q mod 8): every cell of the box inside the array is pure melt,
+  // phi1 == 1 and phi2 == 0 exactly
+  int melt[8];
+};
+
+// A1: the a1 well terms are non-zero; SD: solid diffusivities Da or Db non-zero
+template <bool A1, bool SD>
+__global__ void __launch_bounds__(kT2Threads, 2)
+    tinb_x2_kernel(const __grid_constant__ K3<float> k, const __grid_constant__ CUtensorMap m1,
+                   const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap mc,
+                   float *__restrict__ o1, float *__restrict__ o2, float *__restrict__ oc, int *err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T2Smem &sm = *reinterpret_cast<T2Smem *>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int x0 = kT2BX * blockIdx.x;  // first output column of the tile
+  const int yb = kT2BY * blockIdx.y;  // box row 0 = array row yb; outputs yb+1 .. yb+14
+  const int zo0 = 1 + k.z_chunk * blockIdx.z;
+  const int zo1 = min(zo0 + k.z_chunk, k.nz - 1);
+  if (zo0 >= zo1) return;
+  const int zin0 = zo0 - 1, zin1 = zo1;
+  constexpr uint32_t kBytes = 3u * kT2Plane * sizeof(float);
+  if (smem_u32(smem_raw) & 127u) {
+    if (tid == 0) atomicExch(err, 2);
+    return;
+  }
+  auto issue = [&](int z) {
+    const int q = z - zin0, s = q % kT2Slots;
+    mbar_expect_tx(&sm.full[s], kBytes);
+    tma_load_3d(&sm.in[s][0][0], &m1, &sm.full[s], x0 - 4, yb, z);
+    tma_load_3d(&sm.in[s][1][0], &m2, &sm.full[s], x0 - 4, yb, z);
+    tma_load_3d(&sm.in[s][2][0], &mc, &sm.full[s], x0 - 4, yb, z);
+  };
+  if (tid == 0) {
+    for (int s = 0; s < kT2Slots; ++s) mbar_init(&sm.full[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int z = zin0; z <= min(zin1, zin0 + kT2Slots - 1); ++z) issue(z);
+    for (int s = 0; s < 8; ++s) sm.melt[s] = 1;
+  }
+  __syncthreads();
+  int issued = min(zin1, zin0 + kT2Slots - 1);
+  const float c_ref = (float)k.c_ref;
+  const float lref = (float)log(k.c_ref / (1.0 - k.c_ref));
+  const f2 one = bc(1.f);
+  constexpr float L0d = (float)(kL0Bcc - kL0Liq), L0s = (float)(kL0Bcc + kL0Liq), L0x = (float)(kL0Liq - kL0Bcc);
+
+  // mu'' and S of plane z (tile and halo) into their ring slots
+  auto mu_plane = [&](int z) {
+    const int q = z - zin0, s = q % kT2Slots;
+    const bool got = p3_wait<float>(&sm.full[s], (uint32_t)((q / kT2Slots) & 1), err);
+    // a ghost plane images its neighbour, T included
+    const PlaneT<float> t = plane_terms<float>(k.tab, z == 0 ? 1 : (z == k.nz - 1 ? k.nz - 2 : z));
+    if (!got) return false;
+    float *mu = sm.mu[q % kT2MuSlots], *Sv = sm.S[q % kT2MuSlots];
+    const float *f1 = sm.in[s][0], *f2p = sm.in[s][1], *fc = sm.in[s][2];
+    bool all_melt = true;  // this thread's pairs inside the array
+    for (int e = 2 * tid; e < kT2Plane; e += 2 * kT2Threads) {
+      const f2 p1 = ld2(f1 + e), p2 = ld2(f2p + e), d = ld2(fc + e);
+      // a pair lies wholly inside or outside the array (nx % 4 == 0, even x)
+      const int ax = x0 - 4 + e % kT2BXin, ay = yb + e / kT2BXin;
+      const bool inside = ax >= 0 && ax < k.nx && ay < k.ny;
+      const bool melt = f2bits(p1) == kOne2 && (f2bits(p2) & kAbs2) == 0ull;
+      all_melt = all_melt && (melt || !inside);
+      if (melt && fmaxf(fabsf(lo_of(d)), fabsf(hi_of(d))) <= k.melt_tiny) {
+        // far melt: g = -1, q(1) c (1 - c); lam by its Taylor polynomial
+        // (K3::melt_a), mu'' = d (RT p - 2 L0_Liq), lam = d p
+        f2 pp = fma2(bc(k.melt_a[3]), d, bc(k.melt_a[2]));
+        pp = fma2(pp, d, bc(k.melt_a[1]));
+        pp = fma2(pp, d, bc(k.melt_a[0]));
+        const f2 c = add2(bc(c_ref), d);
+        st2(mu + e, mul2(d, fma2(bc(t.RT), pp, bc((float)(-2.0 * kL0Liq)))));
+        st2(Sv + e, mul2(mul2(p1, fma2(bc(-k.AA1), p1, bc(k.AA))), mul2(c, sub2(one, c))));
+        continue;
+      }
+      const f2 p3 = sub2(sub2(one, p1), p2);
+      // g3(p1, p2, p3) = p1^2 / 4 (15 (1 - p1)(1 + p1 - (p3 - p2)^2) + p1 (9 p1^2 - 5)); g = 1 - 2 g3
+      const f2 dk = sub2(p3, p2);
+      const f2 a = mul2(mul2(sub2(one, p1), bc(15.f)), fma2(dk, mul2(dk, bc(-1.f)), add2(one, p1)));
+      const f2 gq = mul2(mul2(p1, p1), fma2(p1, fma2(mul2(p1, p1), bc(9.f), bc(-5.f)), a));
+      const f2 g = fma2(gq, bc(-0.5f), one);
+      const f2 c = add2(bc(c_ref), d), omc = sub2(one, c);
+      // lam per lane (the logarithm's guard as in mu_cell)
+      const float cl = lo_of(c), ch = hi_of(c), ol = lo_of(omc), oh = hi_of(omc);
+      const f2 lam = pk(cl > 1.e-8f && ol > 1.e-8f ? lam_fast(lo_of(d), ol, c_ref + c_ref) : -lref,
+                        ch > 1.e-8f && oh > 1.e-8f ? lam_fast(hi_of(d), oh, c_ref + c_ref) : -lref);
+      // mu'' = -(g + 1) C0 - d (L0_BCC + L0_Liq + g (L0_BCC - L0_Liq)) + RT lam
+      f2 m = mul2(add2(g, one), bc(-t.C0));
+      m = fma2(d, mul2(fma2(bc(L0d), g, bc(L0s)), bc(-1.f)), m);
+      m = fma2(bc(t.RT), lam, m);
+      f2 q1 = mul2(p1, fma2(bc(-k.AA1), p1, bc(k.AA)));
+      if constexpr (SD) q1 = fma2(bc(k.Db2), p3, fma2(bc(k.Da2), p2, q1));
+      st2(mu + e, m);
+      st2(Sv + e, mul2(q1, mul2(c, omc)));
+    }
+    if (!all_melt) sm.melt[q & 7] = 0;
+    return true;
+  };
+  auto drain = [&](int from) {
+    if (tid == 0)
+      for (int z = from; z <= issued; ++z) {
+        const int q = z - zin0;
+        uint32_t tries = 0;
+        while (!mbar_try_wait(&sm.full[q % kT2Slots], (uint32_t)((q / kT2Slots) & 1)) && ++tries < kP3WaitLimit) {
+        }
+      }
+  };
+  bool ok = mu_plane(zin0);
+  ok = mu_plane(zin0 + 1) && ok;
+  if (!__syncthreads_and(ok)) {
+    drain(zin0);
+    return;
+  }
+
+  const int gx = x0 + 2 * lane;                                        // array x of the pair's first cell
+  const bool v0 = gx >= 1 && gx <= k.nx - 2, v1 = gx + 1 <= k.nx - 2;  // outputs
+  const bool any = v0 || v1;
+  const int ry = 2 * warp;                           // first output row of the thread (tile row)
+  const int ec = (ry + 1) * kT2BXin + 2 * lane + 4;  // box element of its first cell (even)
+  const int64_t plane = (int64_t)k.nx * k.ny;
+  const bool xedge = !(v0 && v1) || gx == 1 || gx + 1 == k.nx - 2;  // a ghost column is involved
+  const f2 dt = bc(k.dt), dt3 = bc(k.dt * (1.f / 3.f));
+
+  for (int z = zo0; z < zo1; ++z) {
+    // one barrier per plane: afterwards the input slot of plane z-2 takes the
+    // load of plane z+2 (mu'' and S have four slots: plane z+1 overwrites z-3)
+    if (!__syncthreads_and(mu_plane(z + 1))) {
+      drain(z + 1);
+      return;
+    }
+    if (z + 2 <= zin1 && z + 2 > issued) {
+      if (tid == 0) issue(z + 2);
+      issued = z + 2;
+    }
+    const int q = z - zin0;
+    // planes z-1 .. z+1 pure melt wherever a stencil of an output cell reaches:
+    // phi1 and phi2 stay exactly 1 and 0 (every phase term and Laplacian is
+    // an exact zero there), only c is updated.  The flag of plane z+3 is
+    // re-armed here: its computation (mu_plane(z+3), before the barrier of
+    // iteration z+2) is separated from this write by the barrier of z+1.
+    const bool melt3 = sm.melt[(q - 1) & 7] && sm.melt[q & 7] && sm.melt[(q + 1) & 7];
+    if (tid == 0) sm.melt[(q + 3) & 7] = 1;
+    if (!any) continue;
+    const float *c1 = sm.in[q % kT2Slots][0], *c2 = sm.in[q % kT2Slots][1], *cc = sm.in[q % kT2Slots][2];
+    const float *d1 = sm.in[(q - 1) % kT2Slots][0], *d2 = sm.in[(q - 1) % kT2Slots][1];
+    const float *u1 = sm.in[(q + 1) % kT2Slots][0], *u2 = sm.in[(q + 1) % kT2Slots][1];
+    const float *mu = sm.mu[q % kT2MuSlots], *mud = sm.mu[(q - 1) % kT2MuSlots], *muu = sm.mu[(q + 1) % kT2MuSlots];
+    const float *Sc = sm.S[q % kT2MuSlots], *Sd = sm.S[(q - 1) % kT2MuSlots], *Su = sm.S[(q + 1) % kT2MuSlots];
+    const PlaneT<float> t = plane_terms<float>(k.tab, z);
+    // z faces of mu'' add the melt's mu difference between the planes; a face
+    // to a ghost plane has none (the ghost's mu'' is taken at this T)
+    const f2 dKu = bc(z + 1 < k.nz - 1 ? t.dK : 0.f);
+    const f2 dKd = bc(z - 1 > 0 ? (float)k.tab[(int64_t)kTW * (z - 1) + kTdK] : 0.f);
+    const int zg = z == 1 ? 0 : (z == k.nz - 2 ? k.nz - 1 : -1);
+    // column window rows ry-1 .. ry+2 of phi1, phi2, mu'', S (pairs)
+    f2 w1[4], w2[4], wm[4], ws[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int e = ec + (r - 1) * kT2BXin;
+      w1[r] = ld2(c1 + e);
+      w2[r] = ld2(c2 + e);
+      wm[r] = ld2(mu + e);
+      ws[r] = ld2(Sc + e);
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int gy = yb + 1 + ry + r;
+      if (gy > k.ny - 2) break;
+      const int e = ec + r * kT2BXin;
+      const f2 p1 = w1[r + 1], p2 = w2[r + 1], m0 = wm[r + 1], S0 = ws[r + 1];
+      const f2 cv = ld2(cc + e);
+      // x neighbours: (left, right) pairs from the pairs beside this one
+      const f2 Lm = ld2(mu + e - 2), Rm = ld2(mu + e + 2), Ls = ld2(Sc + e - 2), Rs = ld2(Sc + e + 2);
+      const f2 mxm = pk(hi_of(Lm), lo_of(m0)), mxp = pk(hi_of(m0), lo_of(Rm));
+      const f2 sxm = pk(hi_of(Ls), lo_of(S0)), sxp = pk(hi_of(S0), lo_of(Rs));
+
+      f2 n1 = bc(1.f), n2 = bc(0.f);
+      if (!melt3) {
+      const f2 L1 = ld2(c1 + e - 2), R1 = ld2(c1 + e + 2), L2 = ld2(c2 + e - 2), R2 = ld2(c2 + e + 2);
+      const f2 x1m = pk(hi_of(L1), lo_of(p1)), x1p = pk(hi_of(p1), lo_of(R1));
+      const f2 x2m = pk(hi_of(L2), lo_of(p2)), x2p = pk(hi_of(p2), lo_of(R2));
+      const f2 p3 = sub2(sub2(one, p1), p2);
+      // driving force of phase 1 against both grains (fun.cu:1192-1193)
+      const f2 c = add2(bc(c_ref), cv), omc = sub2(one, c);
+      const f2 dGv = fma2(mul2(c, omc), bc(L0x), fma2(c, bc(t.Ati), mul2(omc, bc(t.Anb))));
+      const f2 d23 = sub2(p2, p3);
+      // gp2 = Q_1 (pj - pk), Q_1 = 7.5 (p1 - 1) p1^2; gp1 = G_1
+      const f2 Q1 = mul2(fma2(p1, bc(7.5f), bc(-7.5f)), mul2(p1, p1));
+      f2 Ga = fma2(p1, bc(3.f), bc(-4.f));
+      Ga = fma2(Ga, p1, bc(-1.f));
+      Ga = fma2(Ga, p1, bc(2.f));
+      const f2 G1 = mul2(mul2(p1, bc(3.75f)), fma2(fma2(p1, bc(3.f), bc(-2.f)), mul2(d23, d23), Ga));
+      const f2 A = mul2(mul2(Q1, d23), dGv);
+      // multi-well terms (fphi, TiAg.cu:522-527) with their shared factors
+      const f2 s12 = mul2(p1, p2), s13 = mul2(p1, p3), s23 = mul2(p2, p3);
+      const f2 p1s = mul2(p1, p1), p2s = mul2(p2, p2), p3s = mul2(p3, p3);
+      const f2 U2 = fma2(s13, bc(3.f), mul2(p2, fma2(p2, bc(k.b), bc(3.f))));
+      const f2 U3 = fma2(s12, bc(3.f), mul2(p3, fma2(p3, bc(k.b), bc(3.f))));
+      const f2 k2 = mul2(U2, bc(2.f * k.a2)), k3 = mul2(U3, bc(2.f * k.a3));
+      auto dw = [&](f2 p) { return mul2(fma2(fma2(p, bc(4.f), bc(-6.f)), p, bc(2.f)), p); };  // 2p(1-p)(1-2p)
+      f2 F1 = fma2(mul2(p1, p3s), k2, dw(p1));
+      F1 = fma2(mul2(p1, p2s), k3, F1);
+      F1 = fma2(mul2(G1, dGv), bc(k.lam), F1);
+      f2 F2 = fma2(mul2(s13, s13), mul2(fma2(p2, bc(2.f * k.b), bc(3.f)), bc(k.a2)), dw(p2));
+      F2 = fma2(mul2(p2, p1s), k3, F2);
+      F2 = fma2(A, bc(k.lam), F2);
+      f2 F3 = fma2(mul2(p3, p1s), k2, dw(p3));
+      F3 = fma2(mul2(s12, s12), mul2(fma2(p3, bc(2.f * k.b), bc(3.f)), bc(k.a3)), F3);
+      F3 = fma2(A, bc(-k.lam), F3);
+      if constexpr (A1) {
+        const f2 U1 = fma2(s23, bc(3.f), mul2(p1, fma2(p1, bc(k.b), bc(3.f))));
+        const f2 k1 = mul2(U1, bc(2.f * k.a1));
+        F1 = fma2(mul2(s23, s23), mul2(fma2(p1, bc(2.f * k.b), bc(3.f)), bc(k.a1)), F1);
+        F2 = fma2(mul2(p2, p3s), k1, F2);
+        F3 = fma2(mul2(p3, p2s), k1, F3);
+      }
+      // Laplacians
+      auto lap = [&](f2 p, f2 xp, f2 xm, f2 yp, f2 ym, f2 zp, f2 zm) {
+        f2 l = mul2(fma2(p, bc(-2.f), add2(xp, xm)), bc(k.dxi2));
+        l = fma2(fma2(p, bc(-2.f), add2(yp, ym)), bc(k.dyi2), l);
+        return fma2(fma2(p, bc(-2.f), add2(zp, zm)), bc(k.dzi2), l);
+      };
+      const f2 lap1 = lap(p1, x1p, x1m, w1[r + 2], w1[r], ld2(u1 + e), ld2(d1 + e));
+      const f2 lap2 = lap(p2, x2p, x2m, w2[r + 2], w2[r], ld2(u2 + e), ld2(d2 + e));
+      // phi_i' = phi_i + dt lap_i - dt (2F_i - F_j - F_k) / 3
+      const f2 T3 = mul2(add2(add2(F1, F2), F3), dt3);
+      n1 = fma2(F1, bc(-k.dt), add2(T3, fma2(lap1, dt, p1)));
+      n2 = fma2(F2, bc(-k.dt), add2(T3, fma2(lap2, dt, p2)));
+      }
+      // solute: face mobility (S + S') / 2 (the 1/2 is in cf)
+      const f2 jx = fma2(add2(S0, sxp), sub2(mxp, m0), mul2(add2(S0, sxm), sub2(mxm, m0)));
+      const f2 jy = fma2(add2(S0, ws[r + 2]), sub2(wm[r + 2], m0), mul2(add2(S0, ws[r]), sub2(wm[r], m0)));
+      const f2 jz = fma2(add2(S0, ld2(Su + e)), add2(sub2(ld2(muu + e), m0), dKu),
+                         mul2(add2(S0, ld2(Sd + e)), sub2(sub2(ld2(mud + e), m0), dKd)));
+      const f2 nc = add2(cv, fma2(bc(k.cfz), jz, fma2(bc(k.cfy), jy, mul2(bc(k.cfx), jx))));
+      // stores: the pair, and every ghost cell that images one of its cells
+      const int yg = gy == k.ny - 2 ? 0 : (gy == 1 ? k.ny - 1 : -1);
+      const int64_t o = (int64_t)z * plane + (int64_t)gy * k.nx + gx;
+      if (!xedge && (yg & zg) < 0) {
+        st2(o1 + o, n1);
+        st2(o2 + o, n2);
+        st2(oc + o, nc);
+      } else {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int x = gx + h;
+          if (!(h ? v1 : v0)) continue;
+          const float a = h ? hi_of(n1) : lo_of(n1), bb = h ? hi_of(n2) : lo_of(n2), cvv = h ? hi_of(nc) : lo_of(nc);
+          const int xg = x == k.nx - 2 ? 0 : (x == 1 ? k.nx - 1 : -1);
+          const int xs[2] = {x, xg}, ys[2] = {gy, yg}, zs[2] = {z, zg};
+#pragma unroll
+          for (int ia = 0; ia < 2; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < 2; ++ib)
+#pragma unroll
+              for (int ic = 0; ic < 2; ++ic) {
+                if (xs[ia] < 0 || ys[ib] < 0 || zs[ic] < 0) continue;
+                const int64_t oo = (int64_t)zs[ic] * plane + (int64_t)ys[ib] * k.nx + xs[ia];
+                o1[oo] = a;
+                o2[oo] = bb;
+                oc[oo] = cvv;
+              }
+        }
+      }
+    }
+  }
+}
+
+template <bool A1, bool SD>
+int launch_tinb_x2(const K3<float> &k, const P3Maps &m, float *o1, float *o2, float *oc, int *err, cudaStream_t st) {
+  const size_t smem = sizeof(T2Smem) + 128;
+  auto kfn = tinb_x2_kernel<A1, SD>;
+  static std::atomic<unsigned long long> attr;
+  if (!smem_limit_once((const void *)kfn, (int)smem, attr)) return -3;
+  const dim3 grid((k.nx + kT2BX - 1) / kT2BX, (k.ny - 2 + kT2BY - 1) / kT2BY, (k.nz - 2 + k.z_chunk - 1) / k.z_chunk);
+  kfn<<<grid, kT2Threads, smem, st>>>(k, m.phi1, m.phi2, m.c, o1, o2, oc, err);
+  return 0;
+}
+
 template <typename R, bool SD, bool SURR>
 int launch_tinb(const K3<R> &k, const P3Maps &m, R *o1, R *o2, R *oc, int64_t step, int *err, const SurrArgs &sa,
                 cudaStream_t st) {
@@ -450,10 +752,10 @@ int launch_tinb(const K3<R> &k, const P3Maps &m, R *o1, R *o2, R *oc, int64_t st
 
 }  // namespace
 
-int tinb_box_width(int precision) {
-  return precision == RS_F64 ? P3Cfg<double>::BXin : P3Cfg<float>::BXin;
+int tinb_box_width(int precision, bool surr) {
+  return precision == RS_F64 ? P3Cfg<double>::BXin : surr ? P3Cfg<float>::BXin : kT2BXin;
 }
-int tinb_box_height() { return kP3BY + 2; }
+int tinb_box_height(int precision, bool surr) { return precision == RS_F32 && !surr ? kT2BYin : kP3BY + 2; }
 int tinb_table_len(const rs3_params &p) { return kTW * p.nz; }
 
 int launch_tinb_step(const rs3_params &p, const P3Maps &m, int precision, void *o1, void *o2, void *oc, int64_t step,
@@ -480,8 +782,12 @@ int launch_tinb_step(const rs3_params &p, const P3Maps &m, int precision, void *
   if (surr)
     return sd ? launch_tinb<float, true, true>(k, m, f1, f2, fc, step, err, *surr, st)
               : launch_tinb<float, false, true>(k, m, f1, f2, fc, step, err, *surr, st);
-  return sd ? launch_tinb<float, true, false>(k, m, f1, f2, fc, step, err, none, st)
-            : launch_tinb<float, false, false>(k, m, f1, f2, fc, step, err, none, st);
+  // the exact FP32 step on packed pairs
+  const bool a1 = p.a1 != 0.0;
+  return a1 ? (sd ? launch_tinb_x2<true, true>(k, m, f1, f2, fc, err, st)
+                  : launch_tinb_x2<true, false>(k, m, f1, f2, fc, err, st))
+            : (sd ? launch_tinb_x2<false, true>(k, m, f1, f2, fc, err, st)
+                  : launch_tinb_x2<false, false>(k, m, f1, f2, fc, err, st));
 }
 
 int launch_tinb_mu(const rs3_params &p, int precision, const void *f1, const void *f2, const void *fc, void *mu,

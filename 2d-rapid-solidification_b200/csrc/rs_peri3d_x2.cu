@@ -38,7 +38,11 @@ struct X2Smem {
   alignas(128) float in[kX2Slots][3][kX2Plane];
   alignas(128) float mu[kX2MuSlots][kX2Plane];
   uint64_t full[kX2Slots];
+  // per plane (q mod 8): every cell of the box inside the array is pure melt,
+  // phi1 == 1 and phi2 == 0 exactly
+  int melt[8];
 };
+constexpr unsigned long long kOne2 = 0x3F8000003F800000ull, kAbs2 = 0x7FFFFFFF7FFFFFFFull;
 
 // kernel constants, FP32
 struct X2K {
@@ -98,6 +102,7 @@ __global__ void __launch_bounds__(kX2Threads, 3)
     for (int s = 0; s < kX2Slots; ++s) mbar_init(&sm.full[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     for (int z = zin0; z <= min(zin1, zin0 + kX2Slots - 1); ++z) issue(z);
+    for (int s = 0; s < 8; ++s) sm.melt[s] = 1;
   }
   __syncthreads();
   int issued = min(zin1, zin0 + kX2Slots - 1);
@@ -116,8 +121,18 @@ __global__ void __launch_bounds__(kX2Threads, 3)
     const int q = z - zin0, s = q % kX2Slots;
     float *mu = sm.mu[q % kX2MuSlots];
     const float *f1 = sm.in[s][0], *f2p = sm.in[s][1], *fc = sm.in[s][2];
-    if (got)
-      for (int e = 2 * tid; e < kX2Plane; e += 2 * kX2Threads) st2(mu + e, mu2(k, ld2(f1 + e), ld2(f2p + e), ld2(fc + e)));
+    if (got) {
+      bool all_melt = true;  // this thread's pairs inside the array
+      for (int e = 2 * tid; e < kX2Plane; e += 2 * kX2Threads) {
+        const f2 p1 = ld2(f1 + e), p2 = ld2(f2p + e);
+        st2(mu + e, mu2(k, p1, p2, ld2(fc + e)));
+        // a pair lies wholly inside or outside the array (nx % 4 == 0, even x)
+        const int ax = x0 - 4 + e % kX2BXin, ay = yb + e / kX2BXin;
+        const bool inside = ax >= 0 && ax < k.nx && ay < k.ny;
+        all_melt = all_melt && (!inside || ((unsigned long long)p1 == kOne2 && ((unsigned long long)p2 & kAbs2) == 0ull));
+      }
+      if (!all_melt) sm.melt[q & 7] = 0;
+    }
     return got;
   };
   auto drain = [&](int from) {
@@ -157,6 +172,12 @@ __global__ void __launch_bounds__(kX2Threads, 3)
       issued = z + 2;
     }
     const int q = z - zin0;
+    // planes z-1 .. z+1 pure melt wherever a stencil of an output cell
+    // reaches (the flag of plane z+3 is re-armed here: its computation,
+    // mu_plane(z+3) before the barrier of iteration z+2, is separated from
+    // this write by the barrier of z+1)
+    const bool melt3 = sm.melt[(q - 1) & 7] && sm.melt[q & 7] && sm.melt[(q + 1) & 7];
+    if (tid == 0) sm.melt[(q + 3) & 7] = 1;
     const float *c1 = sm.in[q % kX2Slots][0], *c2 = sm.in[q % kX2Slots][1], *cc = sm.in[q % kX2Slots][2];
     const float *d1 = sm.in[(q - 1) % kX2Slots][0], *d2 = sm.in[(q - 1) % kX2Slots][1];
     const float *u1 = sm.in[(q + 1) % kX2Slots][0], *u2 = sm.in[(q + 1) % kX2Slots][1];
@@ -167,7 +188,57 @@ __global__ void __launch_bounds__(kX2Threads, 3)
     const f2 s1 = bc((float)(B1 - k.r1d * k.c_off)), s2 = bc((float)(-B1 - B2 - k.r2d * k.c_off)),
              s3 = bc((float)(-B1 + B2 - k.r3d * k.c_off));
     const int zg = z == 1 ? 0 : (z == k.nz - 2 ? k.nz - 1 : -1);
-    if (any) {
+    // stores: the pair, and every ghost cell that images one of its cells
+    auto store_pair = [&](int gy, f2 n1, f2 n2, f2 nc) {
+      const int yg = gy == k.ny - 2 ? 0 : (gy == 1 ? k.ny - 1 : -1);
+      const int64_t o = (int64_t)z * plane + (int64_t)gy * k.nx + gx;
+      if (!xedge && (yg & zg) < 0) {
+        st2(o1 + o, n1);
+        st2(o2 + o, n2);
+        st2(oc + o, nc);
+      } else {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int x = gx + h;
+          if (!(h ? v1 : v0)) continue;
+          const float a = h ? hi_of(n1) : lo_of(n1), bb = h ? hi_of(n2) : lo_of(n2), cv = h ? hi_of(nc) : lo_of(nc);
+          const int xg = x == k.nx - 2 ? 0 : (x == 1 ? k.nx - 1 : -1);
+          const int xs[2] = {x, xg}, ys[2] = {gy, yg}, zs[2] = {z, zg};
+#pragma unroll
+          for (int ia = 0; ia < 2; ++ia)
+#pragma unroll
+            for (int ib = 0; ib < 2; ++ib)
+#pragma unroll
+              for (int ic = 0; ic < 2; ++ic) {
+                if (xs[ia] < 0 || ys[ib] < 0 || zs[ic] < 0) continue;
+                const int64_t oo = (int64_t)zs[ic] * plane + (int64_t)ys[ib] * k.nx + xs[ia];
+                o1[oo] = a;
+                o2[oo] = bb;
+                oc[oo] = cv;
+              }
+        }
+      }
+    };
+    if (any && melt3) {
+      // pure-melt neighbourhood: phi1 and phi2 stay exactly 1 and 0 (every
+      // phase term and Laplacian is a zero there) and every face mobility is
+      // phi1 + phi1' = 2 exactly (the solid terms vanish), so the solute
+      // update is c + sum_d cf_d 2 ((mu+ - mu) + (mu- - mu)), the general
+      // form's value bit for bit
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int gy = yb + 1 + ry + r;
+        if (gy > k.ny - 2) break;
+        const int e = ec + r * kX2BXin;
+        const f2 m0 = ld2(mu + e);
+        const f2 Lm = ld2(mu + e - 2), Rm = ld2(mu + e + 2);
+        auto face_m = [&](f2 mp, f2 mm) { return mul2(bc(2.f), add2(sub2(mp, m0), sub2(mm, m0))); };
+        f2 nc = fma2(face_m(pk(hi_of(m0), lo_of(Rm)), pk(hi_of(Lm), lo_of(m0))), bc(k.cfx), ld2(cc + e));
+        nc = fma2(face_m(ld2(mu + e + kX2BXin), ld2(mu + e - kX2BXin)), bc(k.cfy), nc);
+        nc = fma2(face_m(ld2(muu + e), ld2(mud + e)), bc(k.cfz), nc);
+        store_pair(gy, bc(1.f), bc(0.f), nc);
+      }
+    } else if (any) {
       // column window rows ry-1 .. ry+2 of phi1, phi2, mu (pairs)
       f2 w1[4], w2[4], wm[4];
 #pragma unroll
@@ -261,35 +332,7 @@ __global__ void __launch_bounds__(kX2Threads, 3)
         f2 nc = fma2(face2(x1p, x2p, mxp, x1m, x2m, mxm), bc(k.cfx), ld2(cc + e));
         nc = fma2(face2(y1p, y2p, myp, y1m, y2m, mym), bc(k.cfy), nc);
         nc = fma2(face2(z1p, z2p, mzp, z1m, z2m, mzm), bc(k.cfz), nc);
-        // stores: the pair, and every ghost cell that images one of its cells
-        const int yg = gy == k.ny - 2 ? 0 : (gy == 1 ? k.ny - 1 : -1);
-        const int64_t o = (int64_t)z * plane + (int64_t)gy * k.nx + gx;
-        if (!xedge && (yg & zg) < 0) {
-          st2(o1 + o, n1);
-          st2(o2 + o, n2);
-          st2(oc + o, nc);
-        } else {
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int x = gx + h;
-            if (!(h ? v1 : v0)) continue;
-            const float a = h ? hi_of(n1) : lo_of(n1), bb = h ? hi_of(n2) : lo_of(n2), cv = h ? hi_of(nc) : lo_of(nc);
-            const int xg = x == k.nx - 2 ? 0 : (x == 1 ? k.nx - 1 : -1);
-            const int xs[2] = {x, xg}, ys[2] = {gy, yg}, zs[2] = {z, zg};
-#pragma unroll
-            for (int ia = 0; ia < 2; ++ia)
-#pragma unroll
-              for (int ib = 0; ib < 2; ++ib)
-#pragma unroll
-                for (int ic = 0; ic < 2; ++ic) {
-                  if (xs[ia] < 0 || ys[ib] < 0 || zs[ic] < 0) continue;
-                  const int64_t oo = (int64_t)zs[ic] * plane + (int64_t)ys[ib] * k.nx + xs[ia];
-                  o1[oo] = a;
-                  o2[oo] = bb;
-                  oc[oo] = cv;
-                }
-          }
-        }
+        store_pair(gy, n1, n2, nc);
       }
     }
   }

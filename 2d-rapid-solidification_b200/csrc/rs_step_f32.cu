@@ -748,22 +748,32 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   for (int j = 0; j < kRowsPerWarp; ++j) {
     const int rr = rbase + j;
     const float4 pv4 = ld4(&sm.psi[rr][bc]);
-    const float pv[4] = {pv4.x, pv4.y, pv4.z, pv4.w};
-    const bool live = y0 - 1 + rr <= ny - 2;
-    float po[4];
+    // phi_next = phi where uniformly +-1: an output cell is not listed only
+    // where psi <= -1 or >= 1 over its 3x3 neighbourhood, so clamp(psi) is
+    // its sign (cells outside the interior are not stored or are overwritten
+    // by the ghost copies); listed cells take phase 3's result
+    float po[4] = {pv4.x > 0.f ? 1.f : -1.f, pv4.y > 0.f ? 1.f : -1.f, pv4.z > 0.f ? 1.f : -1.f,
+                   pv4.w > 0.f ? 1.f : -1.f};
+    const uint32_t lb = (needs_all >> (4 * j)) & 0xFu;
+    if (lb) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const bool listed = (needs_all >> (4 * j + q)) & 1u;
-      // phi_next = phi where uniformly +-1: an output cell is not listed only
-      // where psi <= -1 or >= 1 over its 3x3 neighbourhood, so clamp(psi) is
-      // its sign (cells outside the interior are not stored or are
-      // overwritten by the ghost copies)
-      po[q] = listed ? sm.S[rr][bc + q] : (pv[q] > 0.f ? 1.f : -1.f);
-      if (red && live && !listed && ((outm >> q) & 1u) && po[q] > 0.f)
-        itip = max(itip, gi + q == nx - 2 ? nx - 1 : gi + q);
+      for (int q = 0; q < 4; ++q)
+        if ((lb >> q) & 1u) po[q] = sm.S[rr][bc + q];
     }
     st4(&sm.psi[rr][bc], po[0], po[1], po[2], po[3]);
     st4(&sm.d[rr][bc], dn[j][0], dn[j][1], dn[j][2], dn[j][3]);
+  }
+  if (red) {  // coarse tip: the last column with phi > 0 (listed cells counted again, harmlessly)
+#pragma unroll
+    for (int j = 0; j < kRowsPerWarp; ++j) {
+      const int rr = rbase + j;
+      const float4 po4 = ld4(&sm.psi[rr][bc]);
+      const float po[4] = {po4.x, po4.y, po4.z, po4.w};
+      if (y0 - 1 + rr > ny - 2) continue;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (((outm >> q) & 1u) && po[q] > 0.f) itip = max(itip, gi + q == nx - 2 ? nx - 1 : gi + q);
+    }
   }
   const int nrow = min(kTR, K.ny - 1 - y0);  // output rows of this tile inside the interior
   const int ncol = min(kW, K.nx - x0);       // columns of this tile inside the array (a multiple of 4)
