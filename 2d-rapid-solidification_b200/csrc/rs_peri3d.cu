@@ -32,6 +32,7 @@ struct P3Smem {
   alignas(128) R in[kP3Slots][3][P3Cfg<R>::kPlaneAl];  // [slot][field][row][col]
   alignas(16) R mu[kP3MuSlots][P3Cfg<R>::kPlane];
   uint64_t full[kP3Slots];
+  int melt[8];  // per plane (q mod 8): the box is pure melt inside the array (p3_melt)
 };
 
 // mu = c - sum_i r_i g_i (computeMu, TiAg.cu:461-470)
@@ -74,6 +75,7 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
     for (int s = 0; s < kP3Slots; ++s) mbar_init(&sm.full[s], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     for (int z = zin0; z <= min(zin1, zin0 + kP3Slots - 1); ++z) issue(z);
+    for (int s = 0; s < 8; ++s) sm.melt[s] = 1;
   }
   __syncthreads();
   int issued = min(zin1, zin0 + kP3Slots - 1);  // last plane whose load was issued
@@ -83,8 +85,14 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
     const bool got = p3_wait<R>(&sm.full[s], (uint32_t)((q / kP3Slots) & 1), err);
     R *mu = sm.mu[q % kP3MuSlots];
     const R *f1 = sm.in[s][0], *f2 = sm.in[s][1], *fc = sm.in[s][2];
-    if (got)
-      for (int e = tid; e < C::kPlane; e += kP3Threads) mu[e] = mu_of(k, f1[e], f2[e], fc[e]);
+    if (got) {
+      bool all_melt = true;
+      for (int e = tid; e < C::kPlane; e += kP3Threads) {
+        mu[e] = mu_of(k, f1[e], f2[e], fc[e]);
+        all_melt = all_melt && p3_melt_cell(k, f1[e], f2[e], xb + e % C::BXin, yb + e / C::BXin);
+      }
+      if (!all_melt) sm.melt[q & 7] = 0;
+    }
     return got;
   };
   // a load that did not arrive in time: wait (bounded) for every load still
@@ -128,6 +136,12 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
       issued = z + 2;
     }
     const int q = z - zin0;
+    // planes z-1 .. z+1 pure melt wherever a stencil of an output cell reaches
+    // (p3_melt_cell); the flag of plane z+3 is re-armed here (its computation,
+    // mu_plane(z+3) before the barrier of iteration z+2, is separated from
+    // this write by the barrier of z+1)
+    const bool melt3 = sm.melt[(q - 1) & 7] && sm.melt[q & 7] && sm.melt[(q + 1) & 7];
+    if (tid == 0) sm.melt[(q + 3) & 7] = 1;
     const R *c1 = sm.in[q % kP3Slots][0], *c2 = sm.in[q % kP3Slots][1], *cc = sm.in[q % kP3Slots][2];
     const R *d1 = sm.in[(q - 1) % kP3Slots][0], *d2 = sm.in[(q - 1) % kP3Slots][1];
     const R *u1 = sm.in[(q + 1) % kP3Slots][0], *u2 = sm.in[(q + 1) % kP3Slots][1];
@@ -137,7 +151,49 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
     const double B1 = k.B11 + k.B12 * Tz, B2 = k.B21 + k.B22 * Tz;
     const R s1 = (R)B1, s2 = (R)(-B1 - B2), s3 = (R)(-B1 + B2);
     const int zg = z == 1 ? 0 : (z == k.nz - 2 ? k.nz - 1 : -1);
-    if (xin) {
+    // the cell and every ghost cell that images it
+    auto store_cell = [&](int gy, R n1, R n2, R nc) {
+      const int yg = gy == k.ny - 2 ? 0 : (gy == 1 ? k.ny - 1 : -1);
+      if ((xg & yg & zg) < 0) {  // no ghost cell images this one
+        const int64_t o = (int64_t)z * plane + (int64_t)gy * k.nx + gx;
+        o1[o] = n1;
+        o2[o] = n2;
+        oc[o] = nc;
+      } else {
+        const int xs[2] = {gx, xg}, ys[2] = {gy, yg}, zs[2] = {z, zg};
+  #pragma unroll
+        for (int a = 0; a < 2; ++a)
+  #pragma unroll
+          for (int bq = 0; bq < 2; ++bq)
+  #pragma unroll
+            for (int cq = 0; cq < 2; ++cq) {
+              if (xs[a] < 0 || ys[bq] < 0 || zs[cq] < 0) continue;
+              const int64_t o = (int64_t)zs[cq] * plane + (int64_t)ys[bq] * k.nx + xs[a];
+              o1[o] = n1;
+              o2[o] = n2;
+              oc[o] = nc;
+            }
+      }
+    };
+    if (xin && melt3) {
+      // pure melt (p3_melt_cell): phi1, phi2 stay 1 and 0 and the face
+      // mobilities are 2, the values the general form gives bit for bit
+      const int e0 = (iy0 + 1) * C::BXin + ix + 1;
+      R wm[K + 2];
+  #pragma unroll
+      for (int r = 0; r < K + 2; ++r) wm[r] = mu[e0 + (r - 1) * C::BXin];
+  #pragma unroll
+      for (int r = 0; r < K; ++r) {
+        const int gy = yb + 1 + iy0 + r;
+        if (gy > k.ny - 2) break;
+        const int e = e0 + r * C::BXin;
+        const R m0 = wm[r + 1];
+        const R jx = R(2) * (mu[e + 1] - m0) - R(2) * (m0 - mu[e - 1]);
+        const R jy = R(2) * (wm[r + 2] - m0) - R(2) * (m0 - wm[r]);
+        const R jz = R(2) * (muu[e] - m0) - R(2) * (m0 - mud[e]);
+        store_cell(gy, R(1), R(0), cc[e] + (k.cfx * jx + k.cfy * jy + k.cfz * jz));
+      }
+    } else if (xin) {
       const int e0 = (iy0 + 1) * C::BXin + ix + 1;  // box element of the strip's first cell
       R w1[K + 2], w2[K + 2], wm[K + 2];            // the strip's column, rows iy0-1 .. iy0+K
   #pragma unroll
@@ -197,28 +253,7 @@ __global__ void __launch_bounds__(kP3Threads, sizeof(R) == 4 ? 3 : 2)
         const R jy = mob(w1[r + 2], w2[r + 2]) * (wm[r + 2] - m0) - mob(w1[r], w2[r]) * (m0 - wm[r]);
         const R jz = mob(z1p, z2p) * (muu[e] - m0) - mob(z1m, z2m) * (m0 - mud[e]);
         const R nc = cc[e] + (k.cfx * jx + k.cfy * jy + k.cfz * jz);
-        // the cell and every ghost cell that images it
-        const int yg = gy == k.ny - 2 ? 0 : (gy == 1 ? k.ny - 1 : -1);
-        if ((xg & yg & zg) < 0) {  // no ghost cell images this one
-          const int64_t o = (int64_t)z * plane + (int64_t)gy * k.nx + gx;
-          o1[o] = n1;
-          o2[o] = n2;
-          oc[o] = nc;
-        } else {
-          const int xs[2] = {gx, xg}, ys[2] = {gy, yg}, zs[2] = {z, zg};
-  #pragma unroll
-          for (int a = 0; a < 2; ++a)
-  #pragma unroll
-            for (int bq = 0; bq < 2; ++bq)
-  #pragma unroll
-              for (int cq = 0; cq < 2; ++cq) {
-                if (xs[a] < 0 || ys[bq] < 0 || zs[cq] < 0) continue;
-                const int64_t o = (int64_t)zs[cq] * plane + (int64_t)ys[bq] * k.nx + xs[a];
-                o1[o] = n1;
-                o2[o] = n2;
-                oc[o] = nc;
-              }
-        }
+        store_cell(gy, n1, n2, nc);
       }
     }
   }

@@ -120,6 +120,17 @@ K3<R> make_k3(const rs3_params &p) {
   return k;
 }
 
+// A box element counts as pure melt for a plane's flag when it lies outside
+// the array (no stencil of an output cell reaches it) or holds phi1 == 1 and
+// phi2 == 0 exactly.  Where planes z-1 .. z+1 are pure melt in this sense,
+// every phase term and Laplacian of an output cell of plane z is an exact
+// zero: phi1 and phi2 stay 1 and 0, and every face mobility phi1 + phi1' is
+// exactly 2 (the solid terms vanish).
+template <typename R>
+__device__ __forceinline__ bool p3_melt_cell(const K3<R> &k, R p1, R p2, int x, int y) {
+  return x >= k.nx || y >= k.ny || (p1 == R(1) && p2 == R(0));
+}
+
 template <typename R>
 __device__ __forceinline__ bool p3_wait(uint64_t *bar, uint32_t parity, int *err) {
   uint32_t tries = 0;

@@ -145,6 +145,7 @@ struct TSmem {
   // (before the plane barrier) while slower threads still read plane z-1
   alignas(16) float dG[3][SURR ? P3Cfg<R>::BX * kP3BY : 1];
   uint64_t full[kP3Slots];
+  int melt[8];  // per plane (q mod 8): the box is pure melt inside the array (p3_melt_cell)
 };
 
 // SD: solid diffusivities Da or Db non-zero
@@ -181,6 +182,7 @@ __global__ void __launch_bounds__(kP3Threads, 2)
   };
   if (tid == 0) {
     for (int s = 0; s < kP3Slots; ++s) mbar_init(&sm.full[s], 1);
+    for (int s = 0; s < 8; ++s) sm.melt[s] = 1;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     for (int z = zin0; z <= min(zin1, zin0 + kP3Slots - 1); ++z) issue(z);
   }
@@ -200,9 +202,11 @@ __global__ void __launch_bounds__(kP3Threads, 2)
     // the imaged cell's, as TiAg.cu's boundaryMu leaves it)
     const PlaneT<R> t = plane_terms<R>(k.tab, z == 0 ? 1 : (z == k.nz - 1 ? k.nz - 2 : z));
     if (!got) return false;
+    bool all_melt = true;  // this thread's box elements (p3_melt_cell)
     if constexpr (!SURR) {
       for (int e = tid; e < C::kPlane; e += kP3Threads) {
         const R p1 = f1[e], p2 = f2[e], cv = fc[e];
+        all_melt = all_melt && p3_melt_cell(k, p1, p2, xb + e % C::BXin, yb + e / C::BXin);
         R c, m;
         if constexpr (kF32) {
           c = c_ref + cv;
@@ -255,6 +259,7 @@ __global__ void __launch_bounds__(kP3Threads, 2)
           }
         }
         if (in && !melt && !inbox) atomicAdd(&SA.audit[2], 1ull);
+        if (in) all_melt = all_melt && p3_melt_cell(k, p1, p2, xb + e % C::BXin, yb + e / C::BXin);
         if (in) {
           const float q1 = p1 * (k.AA - k.AA1 * p1) + (SD ? k.Da2 * p2 + k.Db2 * (1.f - p1 - p2) : 0.f);
           mu[e] = m;
@@ -264,6 +269,7 @@ __global__ void __launch_bounds__(kP3Threads, 2)
         }
       }
     }
+    if (!all_melt) sm.melt[q & 7] = 0;
     return true;
   };
   // a load that did not arrive in time: wait (bounded) for every load still
@@ -303,6 +309,12 @@ __global__ void __launch_bounds__(kP3Threads, 2)
       issued = z + 2;
     }
     const int q = z - zin0;
+    // planes z-1 .. z+1 pure melt wherever a stencil of an output cell reaches
+    // (p3_melt_cell); the flag of plane z+3 is re-armed here (its computation,
+    // mu_plane(z+3) before the barrier of iteration z+2, is separated from
+    // this write by the barrier of z+1)
+    const bool melt3 = sm.melt[(q - 1) & 7] && sm.melt[q & 7] && sm.melt[(q + 1) & 7];
+    if (tid == 0) sm.melt[(q + 3) & 7] = 1;
     const R *c1 = sm.in[q % kP3Slots][0], *c2 = sm.in[q % kP3Slots][1], *cc = sm.in[q % kP3Slots][2];
     const R *d1 = sm.in[(q - 1) % kP3Slots][0], *d2 = sm.in[(q - 1) % kP3Slots][1];
     const R *u1 = sm.in[(q + 1) % kP3Slots][0], *u2 = sm.in[(q + 1) % kP3Slots][1];
@@ -314,7 +326,52 @@ __global__ void __launch_bounds__(kP3Threads, 2)
     const R dKu = kF32 && z + 1 < k.nz - 1 ? t.dK : R(0);
     const R dKd = kF32 && z - 1 > 0 ? (R)k.tab[(int64_t)kTW * (z - 1) + kTdK] : R(0);
     const int zg = z == 1 ? 0 : (z == k.nz - 2 ? k.nz - 1 : -1);
-    if (xin) {
+    // the cell and every ghost cell that images it
+    auto store_cell = [&](int gy, R n1, R n2, R nc) {
+      const int yg = gy == k.ny - 2 ? 0 : (gy == 1 ? k.ny - 1 : -1);
+      if ((xg & yg & zg) < 0) {
+        const int64_t o = (int64_t)z * plane + (int64_t)gy * k.nx + gx;
+        o1[o] = n1;
+        o2[o] = n2;
+        oc[o] = nc;
+      } else {
+        const int xs[2] = {gx, xg}, ys[2] = {gy, yg}, zs[2] = {z, zg};
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int bq = 0; bq < 2; ++bq)
+#pragma unroll
+            for (int cq = 0; cq < 2; ++cq) {
+              if (xs[a] < 0 || ys[bq] < 0 || zs[cq] < 0) continue;
+              const int64_t o = (int64_t)zs[cq] * plane + (int64_t)ys[bq] * k.nx + xs[a];
+              o1[o] = n1;
+              o2[o] = n2;
+              oc[o] = nc;
+            }
+      }
+    };
+    if (xin && melt3) {
+      // pure melt (p3_melt_cell): phi1, phi2 stay exactly 1 and 0 (every phase
+      // term and Laplacian is a zero); the solute update is the general one
+      const int e0 = (iy0 + 1) * C::BXin + ix + 1;
+      R wm[K + 2], ws[K + 2];
+#pragma unroll
+      for (int r = 0; r < K + 2; ++r) {
+        wm[r] = mu[e0 + (r - 1) * C::BXin];
+        ws[r] = Sc[e0 + (r - 1) * C::BXin];
+      }
+#pragma unroll
+      for (int r = 0; r < K; ++r) {
+        const int gy = yb + 1 + iy0 + r;
+        if (gy > k.ny - 2) break;
+        const int e = e0 + r * C::BXin;
+        const R m0 = wm[r + 1], S0 = ws[r + 1];
+        const R jx = (S0 + Sc[e + 1]) * (mu[e + 1] - m0) - (S0 + Sc[e - 1]) * (m0 - mu[e - 1]);
+        const R jy = (S0 + ws[r + 2]) * (wm[r + 2] - m0) - (S0 + ws[r]) * (m0 - wm[r]);
+        const R jz = (S0 + Su[e]) * ((muu[e] - m0) + dKu) - (S0 + Sd[e]) * ((m0 - mud[e]) + dKd);
+        store_cell(gy, R(1), R(0), cc[e] + (k.cfx * jx + k.cfy * jy + k.cfz * jz));
+      }
+    } else if (xin) {
       const int e0 = (iy0 + 1) * C::BXin + ix + 1;
       R w1[K + 2], w2[K + 2], wm[K + 2], ws[K + 2];
 #pragma unroll
@@ -367,27 +424,7 @@ __global__ void __launch_bounds__(kP3Threads, 2)
         const R jy = (S0 + ws[r + 2]) * (wm[r + 2] - m0) - (S0 + ws[r]) * (m0 - wm[r]);
         const R jz = (S0 + Su[e]) * ((muu[e] - m0) + dKu) - (S0 + Sd[e]) * ((m0 - mud[e]) + dKd);
         const R nc = cv + (k.cfx * jx + k.cfy * jy + k.cfz * jz);
-        const int yg = gy == k.ny - 2 ? 0 : (gy == 1 ? k.ny - 1 : -1);
-        if ((xg & yg & zg) < 0) {
-          const int64_t o = (int64_t)z * plane + (int64_t)gy * k.nx + gx;
-          o1[o] = n1;
-          o2[o] = n2;
-          oc[o] = nc;
-        } else {
-          const int xs[2] = {gx, xg}, ys[2] = {gy, yg}, zs[2] = {z, zg};
-#pragma unroll
-          for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int bq = 0; bq < 2; ++bq)
-#pragma unroll
-              for (int cq = 0; cq < 2; ++cq) {
-                if (xs[a] < 0 || ys[bq] < 0 || zs[cq] < 0) continue;
-                const int64_t o = (int64_t)zs[cq] * plane + (int64_t)ys[bq] * k.nx + xs[a];
-                o1[o] = n1;
-                o2[o] = n2;
-                oc[o] = nc;
-              }
-        }
+        store_cell(gy, n1, n2, nc);
       }
     }
   }
