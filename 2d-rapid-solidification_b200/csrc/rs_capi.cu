@@ -48,6 +48,7 @@ int set_error(int code, const char *msg) { return fail(code, "%s", msg); }
 struct TmaEntry {
   const void *ptr;
   int precision;
+  int rows;  // box height
   CUtensorMap map;
 };
 
@@ -115,17 +116,19 @@ bool encode_map(const rs_params &p, const void *ptr, int precision, int box_rows
   return r == CUDA_SUCCESS;
 }
 
-bool field_map(rs_ctx *c, const void *ptr, int precision, CUtensorMap *out) {
+// box_rows: kTmaBoxH, or kTfcTileRows32 + 2 for FP32 coarse-grid-temperature steps
+bool field_map(rs_ctx *c, const void *ptr, int precision, int box_rows, CUtensorMap *out) {
   for (int k = 0; k < c->tma_n; ++k)
-    if (c->tma[k].ptr == ptr && c->tma[k].precision == precision) {
+    if (c->tma[k].ptr == ptr && c->tma[k].precision == precision && c->tma[k].rows == box_rows) {
       *out = c->tma[k].map;
       return true;
     }
   CUtensorMap m;
-  if (!encode_map(c->p, ptr, precision, rs::kTmaBoxH, &m)) return false;
+  if (!encode_map(c->p, ptr, precision, box_rows, &m)) return false;
   TmaEntry &e = c->tma[c->tma_next];
   e.ptr = ptr;
   e.precision = precision;
+  e.rows = box_rows;
   e.map = m;
   c->tma_next = (c->tma_next + 1) % 8;
   if (c->tma_n < 8) ++c->tma_n;
@@ -440,8 +443,9 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
   const uintptr_t vec = 16;
   const bool out_aligned =
       ((uintptr_t)next->psi % vec) == 0 && ((uintptr_t)next->c % vec) == 0 && ((uintptr_t)next->phi % vec) == 0;
-  if (c->use_tma && out_aligned && !c->p.tfc && !a->pull_back && field_map(c, cur->psi, cur->precision, &tm.psi) &&
-      field_map(c, cur->c, cur->precision, &tm.c)) {
+  const int box_rows = c->p.tfc && cur->precision == RS_F32 ? rs::kTfcTileRows32 + 2 : rs::kTmaBoxH;
+  if (c->use_tma && out_aligned && !a->pull_back && field_map(c, cur->psi, cur->precision, box_rows, &tm.psi) &&
+      field_map(c, cur->c, cur->precision, box_rows, &tm.c)) {
     tm.col_tab = c->col_tab;
     tm.col_tab_len = c->col_tab_len;
     tm.col_tab64 = c->col_tab64;
@@ -801,6 +805,7 @@ int rs_set_surrogate(rs_ctx *c, const float *d_w, const rs_mlp_box *box) {
     return RS_OK;
   }
   if (!box_ok(box)) return fail(RS_E_INVALID, "rs_set_surrogate: bad box");
+  if (c->p.tfc) return fail(RS_E_UNSUPPORTED, "rs_set_surrogate: frozen temperature only");
   const cudaError_t e = rs::surrogate_setup(d_w, box, &c->mlp_w, &c->mlp_b16, &c->mlp_audit, &c->surr);
   if (e != cudaSuccess) return fail(RS_E_CUDA, "rs_set_surrogate: %s", cudaGetErrorString(e));
   return RS_OK;

@@ -136,6 +136,7 @@ constexpr int kTileOutW64 = 64;                  // output columns of an FP64 ti
 constexpr int kTmaBoxW64 = kTileOutW64 + 8;      // its input columns
 constexpr int kTileRows = 16;    // output rows of a tile
 constexpr int kTmaBoxH = kTileRows + 2;  // input rows of a tile
+constexpr int kTfcTileRows32 = 8;        // output rows of an FP32 coarse-grid-temperature tile
 constexpr int kColTabFields = 5;
 // length of the per-column table (entry k is column k - 4) for nx_all columns
 inline int col_tab_len(int nx_all) { return ((nx_all + kTileOutW - 1) / kTileOutW) * kTileOutW + kTmaBoxW32; }

@@ -323,7 +323,7 @@ static int launch(const StepCoef &K, const StepScalars &P, const typename Tr<R>:
   const Coef<R> F = make_coef<R>(K);
   const int ni = K.nx - 2, nj = K.ny - 2;
   const bool tfc = K.tfc != 0;
-  if (tm && !tfc && !P.pull_back) {
+  if (tm && !P.pull_back) {
     if constexpr (sizeof(R) == 4)
       return launch_step_f32_tma(K, make_coef<float>(K), P, *tm, (float *)psi_n, (float *)c_n, (float *)phi_n,
                                  partials, max_partials, nwarps_out, err, st);

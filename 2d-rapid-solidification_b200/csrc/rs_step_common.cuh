@@ -239,6 +239,78 @@ __device__ __forceinline__ double t_fine_at(const StepCoef &K, const double *__r
   return f00 + a10 * x + a01 * y + a11 * x * y;
 }
 
+// TFC (the coarse-grid temperature, fun.cu:1580-1608): every cell has its own
+// temperature, bilinear from the coarse grid, so the column table entries of
+// the tile kernels become per-cell CALPHAD groups, and K + C0 varies along
+// both axes: the FP64 tile kernel stores mu = mu'' + (K + C0) of the cell, the
+// FP32 one keeps K + C0 in FP64 beside mu'' and adds its face differences.
+struct CellGroups {
+  double RT, C0, KC;  // RT, C0 and K + C0 at the cell's temperature
+  double Anb, Ati;    // the driving-force groups
+};
+// the CALPHAD groups at temperature T (lT = log T).  K + C0 = G_Ti_Liq -
+// G_Nb_Liq + L0_Liq (1 - 2 cinf) + RT Lref needs the liquid functions only,
+// which is all the melt rows use; full adds C0 and the driving-force groups
+// (the solid functions).  Every caller takes K + C0 from this one expression,
+// so a cell's value does not depend on which row form or tile evaluates it.
+__device__ __forceinline__ CellGroups groups_at(const StepCoef &K, double T, double lT, bool full) {
+  const double tl = g_ti_liq(T, lT), nl = g_nb_liq(T, lT);
+  CellGroups g;
+  g.RT = K.RR * T;
+  g.KC = (tl - nl) + kL0Liq * (1.0 - 2.0 * K.cinf) + g.RT * K.Lref;
+  g.C0 = g.Anb = g.Ati = 0.0;
+  if (full) {
+    const double tb = g_ti_bcc(T, lT), nb = g_nb_bcc(T, lT);
+    g.C0 = -0.5 * ((tb - nb) - (tl - nl)) - 0.5 * (kL0Bcc - kL0Liq) * (1.0 - 2.0 * K.cinf);
+    g.Anb = nl - nb;
+    g.Ati = tl - tb;
+  }
+  return g;
+}
+// log T near a reference T0: log T0 + log1p(u), u = (T - T0)/T0, by
+// the Taylor series of log1p to u^8 where |u| <= 2^-6 (the remainder, below
+// |u|^9/9 < 7e-18, is under 1 % of an ulp of log T), else log itself.  The
+// tile kernels take T0 per lane: over its cells T changes by far less than
+// 1.5 %.
+struct LogRef {
+  double T0, lT0, iT0;  // T0, log T0, 1 / T0
+};
+__device__ __forceinline__ LogRef log_ref(double T0) { return LogRef{T0, log(T0), 1.0 / T0}; }
+__device__ __forceinline__ double log_near(const LogRef &L, double T) {
+  const double u = (T - L.T0) * L.iT0;
+  if (fabs(u) > 0.015625) return log(T);
+  double p = -1.0 / 8.0;
+  p = fma(p, u, 1.0 / 7.0);
+  p = fma(p, u, -1.0 / 6.0);
+  p = fma(p, u, 1.0 / 5.0);
+  p = fma(p, u, -1.0 / 4.0);
+  p = fma(p, u, 1.0 / 3.0);
+  p = fma(p, u, -1.0 / 2.0);
+  p = fma(p, u, 1.0);
+  return fma(p, u, L.lT0);
+}
+// interpolate_temperature's coordinates (fun.cu:1588-1594), split into the
+// column part (fixed per lane) and the row part (one per row): the same
+// expressions as t_fine_at, so the same temperature
+__device__ __forceinline__ void tfc_col(const StepCoef &K, int ile, int i, int &iT, double &x) {
+  i = min(max(i, 0), K.nx - 1);
+  iT = (i - 1 + ile) / K.ratio;
+  x = (i - 1.0 + ile) / K.ratio - iT;
+  iT = min(max(iT, 0), K.NxT_all - 2);
+}
+__device__ __forceinline__ void tfc_row(const StepCoef &K, int j, int &jT, double &y) {
+  j = min(j, K.ny - 1);
+  jT = (int)((j - 1 + K.dxT) / K.ratio);
+  y = (j - 1.0 + K.dxT) / K.ratio - jT;
+  jT = min(max(jT, 0), K.NyT_all - 2);
+}
+__device__ __forceinline__ double tfc_T(const StepCoef &K, const double *__restrict__ T, int iT, double x, int jT,
+                                        double y) {
+  const double *r0 = T + (int64_t)jT * K.NxT_all + iT, *r1 = r0 + K.NxT_all;
+  const double f00 = r0[0], f10 = r0[1], f01 = r1[0], f11 = r1[1];
+  const double a10 = f10 - f00, a01 = f01 - f00, a11 = f11 - f10 - f01 + f00;
+  return f00 + a10 * x + a01 * y + a11 * x * y;
+}
 // column (or, with TFC, cell) CALPHAD groups in the working precision
 template <typename R>
 struct ColT {

@@ -87,7 +87,7 @@ enum { kTabRT = 0, kTabC0 = 1, kTabDK = 2, kTabAnb = 3, kTabAti = 4 };
 // Shared memory of one tile of TR output rows x kW output columns (input
 // TR + 2 rows); the ensemble kernels take TR = 8, 16 or 32 (kTileShapes), the
 // single-run kernel TR = kTR.
-template <int TR>
+template <int TR, bool TFC = false>
 struct alignas(128) TileSmemT {
   static constexpr int kRin = TR + 2;  // input rows
   using Mask = std::conditional_t<(kRin <= 32), uint32_t, unsigned long long>;  // one bit per input row
@@ -96,6 +96,8 @@ struct alignas(128) TileSmemT {
   alignas(128) float d[kRin][kWin];
   alignas(16) float S[kRin][kWin];  // after phase 2: new psi of the listed cells
   alignas(16) float mu[kRin][kWin];
+  // TFC: K + C0 of every cell in FP64 (the face terms are its differences)
+  alignas(16) double kc[TFC ? kRin : 1][TFC ? kWin : 2];
   uint16_t list[TR * kW];   // interface cells: row << 8 | output column
   uint8_t pmask[kRin][32];  // per lane: bits 0-3 psi <= -1, bits 4-7 psi >= 1 of its four cells
   uint8_t hmask[kRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(kTabBlock) column_table_kernel(const StepCoef 
 // part: this tile's partial (mass, coarse tip), or nullptr.
 // TR: output rows of the tile (8, 16 or 32; the tensor maps' box is TR + 2
 // rows high).
-template <bool SURR, int TR, typename Prefetch>
+template <bool SURR, int TR, typename Prefetch, bool TFC = false>
 __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &F, const StepScalars &PS,
                                           const CUtensorMap *tm_psi, const CUtensorMap *tm_c,
                                           const float *__restrict__ tab, const int tab_len, float *__restrict__ psi_n,
@@ -194,7 +196,8 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   // halo-column threads: the last warps, which have one input row fewer
   constexpr int kHalo0 = (64 + 2 * kTRin <= kThreads) ? 64 : kThreads - 2 * kTRin;
   static_assert(kHalo0 >= 0 && 4 * kTR <= kThreads, "one thread per halo cell and per row copy");
-  using Smem = TileSmemT<TR>;
+  static_assert(!(SURR && TFC), "the surrogate takes the frozen temperature");
+  using Smem = TileSmemT<TR, TFC>;
   using Mask = typename Smem::Mask;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Smem &sm = *reinterpret_cast<Smem *>(smem_raw);
@@ -243,8 +246,42 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const float *tRT = tab + kTabRT * tab_len + 4, *tC0 = tab + kTabC0 * tab_len + 4;
   const float *tDK = tab + kTabDK * tab_len + 4;
-  const float4 RTv = ld4(tRT + gi), C0v = ld4(tC0 + gi);
-  const float RTa[4] = {RTv.x, RTv.y, RTv.z, RTv.w}, C0a[4] = {C0v.x, C0v.y, C0v.z, C0v.w};
+  float4 RTv = make_float4(0.f, 0.f, 0.f, 0.f), C0v = RTv, dKv = RTv;
+  float dKl = 0.f;
+  if constexpr (!TFC) {
+    RTv = ld4(tRT + gi);
+    C0v = ld4(tC0 + gi);
+  }
+  if constexpr (!TFC && !SURR) {
+    // dK of the lane's faces, loaded now so that the load hides under the
+    // tile's (the surrogate path, short of registers, loads them after phase 1)
+    dKv = ld4(tDK + gi);
+    dKl = tDK[gi - 1];
+  }
+  // TFC: RT and C0 per row, from each cell's own temperature
+  float RTa[4] = {RTv.x, RTv.y, RTv.z, RTv.w}, C0a[4] = {C0v.x, C0v.y, C0v.z, C0v.w};
+  // TFC: the column part of each cell's temperature (interpolate_temperature,
+  // fun.cu:1580-1608) and the lane's reference temperature for log_near
+  int tiT[4] = {0, 0, 0, 0};
+  double tx[4] = {0.0, 0.0, 0.0, 0.0};
+  LogRef lref{0.0, 0.0, 0.0};
+  if constexpr (TFC) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) tfc_col(K, PS.i_left_end_T, gi + q, tiT[q], tx[q]);
+    int jT;
+    double y;
+    tfc_row(K, y0, jT, y);
+    lref = log_ref(tfc_T(K, PS.T_coarse, tiT[0], tx[0], jT, y));
+  }
+  // TFC: all groups of one cell, the logarithm exact (halo and interface cells)
+  auto tfc_cell = [&](int gx, int row) {
+    int iT, jT;
+    double x, y;
+    tfc_col(K, PS.i_left_end_T, gx, iT, x);
+    tfc_row(K, row, jT, y);
+    const double T = tfc_T(K, PS.T_coarse, iT, x, jT, y);
+    return groups_at(K, T, log(T), true);
+  };
   // surrogate: per-lane fragments, and the scaled inputs as T(x) = TnA + TnB x
   // (tile column x; frozen T is linear in the column) and c = cnA + delta c_ihalf
   float TnA = 0.f, TnB = 0.f, cnA = 0.f;
@@ -404,6 +441,10 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     if (y0 - 1 + rr > ny - 1) {  // beyond the array (last tile): never read by an output
       st4(&sm.S[rr][bc], 0.f, 0.f, 0.f, 0.f);
       st4(&sm.mu[rr][bc], 0.f, 0.f, 0.f, 0.f);
+      if constexpr (TFC) {
+        *reinterpret_cast<double2 *>(&sm.kc[rr][bc]) = make_double2(0.0, 0.0);
+        *reinterpret_cast<double2 *>(&sm.kc[rr][bc + 2]) = make_double2(0.0, 0.0);
+      }
       liq_rows |= Mask(1) << rr;
       sol_rows |= Mask(1) << rr;
       continue;
@@ -419,8 +460,29 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const float dmx = fmaxf(fmaxf(dv[0], dv[1]), fmaxf(dv[2], dv[3]));
     const float dmn = fminf(fminf(dv[0], dv[1]), fminf(dv[2], dv[3]));
     const bool liq4 = band == kMinus1 && bor == kMinus1;
+    // the row's form (warp-uniform): far melt, bulk melt or general (voted
+    // here with TFC, where it decides which groups to evaluate)
+    bool far = false, bulk = false;
+    if constexpr (TFC) {  // the melt forms need RT and K + C0 only
+      far = __all_sync(FULL, liq4 && fmaxf(dmx, -dmn) <= tiny);
+      bulk = !far && __all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo);
+      int jT;
+      double y;
+      tfc_row(K, y0 - 1 + rr, jT, y);
+      double kq[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double T = tfc_T(K, PS.T_coarse, tiT[q], tx[q], jT, y);
+        const CellGroups cg = groups_at(K, T, log_near(lref, T), !(far || bulk));
+        RTa[q] = (float)cg.RT;
+        C0a[q] = (float)cg.C0;
+        kq[q] = cg.KC;
+      }
+      *reinterpret_cast<double2 *>(&sm.kc[rr][bc]) = make_double2(kq[0], kq[1]);
+      *reinterpret_cast<double2 *>(&sm.kc[rr][bc + 2]) = make_double2(kq[2], kq[3]);
+    }
     uint32_t code, s3 = 0u;
-    if (__all_sync(FULL, liq4 && fmaxf(dmx, -dmn) <= tiny)) {
+    if (TFC ? far : __all_sync(FULL, liq4 && fmaxf(dmx, -dmn) <= tiny)) {
       // far melt: lam by its Taylor polynomial in delta (Coef::melt_a);
       // mu'' = RT lam - 2 L0_Liq delta = delta (RT p + KL), lam = delta p
       code = 1u | 4u;  // 4: every cell in the exact melt form
@@ -433,7 +495,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
         Sv[q] = c * om;
         mv[q] = dv[q] * fmaf(RTa[q], p, KL);
       }
-    } else if (__all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
+    } else if (TFC ? bulk : __all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo)) {
       code = 1u | 4u;  // 4: every cell in the series form
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -520,14 +582,22 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const int rr = i >> 1, side = i & 1;
     const int x = side ? kHaloR : kHaloL, g = x0 - 4 + x;
     float Sh = 0.f, mh = 0.f;
+    double kh = 0.0;
     uint8_t hm = 3u;
     if (y0 - 1 + rr <= K.ny - 1) {
       const float pv = sm.psi[rr][x];
-      cell_terms(F, pv, sm.d[rr][x], tRT[g], tC0[g], Sh, mh);
+      if constexpr (TFC) {
+        const CellGroups cg = tfc_cell(g, y0 - 1 + rr);
+        cell_terms(F, pv, sm.d[rr][x], (float)cg.RT, (float)cg.C0, Sh, mh);
+        kh = cg.KC;
+      } else {
+        cell_terms(F, pv, sm.d[rr][x], tRT[g], tC0[g], Sh, mh);
+      }
       hm = (pv <= -1.f ? 1u : 0u) | (pv >= 1.f ? 2u : 0u);
     }
     sm.S[rr][x] = Sh;
     sm.mu[rr][x] = mh;
+    if constexpr (TFC) sm.kc[rr][x] = kh;
     sm.hmask[rr][side] = hm;
     if (!SURR) break;
    }
@@ -554,8 +624,10 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     }
    }
   }
-  const float4 dKv = ld4(tDK + gi);
-  const float dKl = tDK[gi - 1];
+  if constexpr (SURR) {
+    dKv = ld4(tDK + gi);
+    dKl = tDK[gi - 1];
+  }
   const float dKa[5] = {dKl, dKv.x, dKv.y, dKv.z, dKv.w};  // faces x-1|x for x = col .. col+4
   __syncthreads();
   // phase 1 done: pull the tile of the CTA that will start about one resident
@@ -570,6 +642,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   int itip = 0;
   struct Row {
     float s[4], m[4], sl, sr, ml, mr, q[5];  // q[f]: S pair sum of the face left of cell f (f = 0..4)
+    double k[4], kl, kr;                     // TFC: K + C0 of the cells and of their neighbours
   };
   auto load_row = [&](int rr, Row &R) {
     const float4 s = ld4(&sm.S[rr][bc]), m = ld4(&sm.mu[rr][bc]);
@@ -586,6 +659,15 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     if (lane == 31) {
       R.sr = sm.S[rr][kHaloR];
       R.mr = sm.mu[rr][kHaloR];
+    }
+    if constexpr (TFC) {
+      const double2 k01 = *reinterpret_cast<const double2 *>(&sm.kc[rr][bc]);
+      const double2 k23 = *reinterpret_cast<const double2 *>(&sm.kc[rr][bc + 2]);
+      R.k[0] = k01.x; R.k[1] = k01.y; R.k[2] = k23.x; R.k[3] = k23.y;
+      R.kl = __shfl_up_sync(FULL, R.k[3], 1);
+      R.kr = __shfl_down_sync(FULL, R.k[0], 1);
+      if (lane == 0) R.kl = sm.kc[rr][kHaloL];
+      if (lane == 31) R.kr = sm.kc[rr][kHaloR];
     }
     R.q[0] = R.sl + R.s[0];
     R.q[1] = R.s[0] + R.s[1];
@@ -605,7 +687,11 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     for (int q = 0; q < 4; ++q) pp[q + 1] = A.s[q] + B.s[q];
     pp[5] = A.sr + B.sr;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) jv[q] = __fmul_rn(fmaf(6.f, pp[q + 1], pp[q] + pp[q + 2]), B.m[q] - A.m[q]);
+    for (int q = 0; q < 4; ++q) {
+      float dm = B.m[q] - A.m[q];
+      if constexpr (TFC) dm = dm + (float)(B.k[q] - A.k[q]);  // K + C0 differs along y too
+      jv[q] = __fmul_rn(fmaf(6.f, pp[q + 1], pp[q] + pp[q + 2]), dm);
+    }
   };
 
   const int rbase = 1 + kRowsPerWarp * warp;
@@ -623,9 +709,17 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     vface(rb, rc, jv_hi);
     // fluxes through the faces (x-1/2, r) for x = col .. col+4
     const float mm[6] = {rb.ml, rb.m[0], rb.m[1], rb.m[2], rb.m[3], rb.mr};
-    float jh[5];
+    float jh[5], dKf[5];
+    if constexpr (TFC) {  // the cells' own K + C0 differences, rounded from FP64
+      const double kk[6] = {rb.kl, rb.k[0], rb.k[1], rb.k[2], rb.k[3], rb.kr};
 #pragma unroll
-    for (int f = 0; f < 5; ++f) jh[f] = __fmul_rn(fmaf(6.f, rb.q[f], ra.q[f] + rc.q[f]), mm[f + 1] - mm[f] + dKa[f]);
+      for (int f = 0; f < 5; ++f) dKf[f] = (float)(kk[f + 1] - kk[f]);
+    } else {
+#pragma unroll
+      for (int f = 0; f < 5; ++f) dKf[f] = dKa[f];
+    }
+#pragma unroll
+    for (int f = 0; f < 5; ++f) jh[f] = __fmul_rn(fmaf(6.f, rb.q[f], ra.q[f] + rc.q[f]), mm[f + 1] - mm[f] + dKf[f]);
     const float4 dv4 = ld4(&sm.d[rr][bc]);
     const float dv[4] = {dv4.x, dv4.y, dv4.z, dv4.w};
 #pragma unroll
@@ -724,7 +818,16 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     const int rr = (int)(e >> 8), x = (int)(e & 0xFFu) + 4;  // box column
     const int r = y0 - 1 + rr, g = x0 + x - 4;
     const float c00 = F.cinf + sm.d[rr][x];
-    float dG = (1.f - c00) * tAnb[g] + c00 * tAti[g] + c00 * (1.f - c00) * (float)(kL0Liq - kL0Bcc);
+    float Anb, Ati;
+    if constexpr (TFC) {
+      const CellGroups cg = tfc_cell(g, r);
+      Anb = (float)cg.Anb;
+      Ati = (float)cg.Ati;
+    } else {
+      Anb = tAnb[g];
+      Ati = tAti[g];
+    }
+    float dG = (1.f - c00) * Anb + c00 * Ati + c00 * (1.f - c00) * (float)(kL0Liq - kL0Bcc);
     if constexpr (SURR) {  // driving force from the surrogate for in-box, unaudited cells
       float in[3];
       net_inputs(rr, x, in);
@@ -866,6 +969,38 @@ __global__ void __launch_bounds__(kThreads, SURR ? 4 : 5)
   tile_body<SURR, kTR>(K, F, PS, &tm_psi, &tm_c, tab, tab_len, psi_n, c_n, phi_n,
                   partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr, err, SA, tr, tc,
                   partials && FR.counter ? &FR : nullptr, prefetch);
+}
+
+// The coarse-grid temperature (TFC): tiles of kTfcTileRows32 output rows, whose
+// per-cell K + C0 (FP64) fits beside the tile with six CTAs per SM; per-cell
+// CALPHAD groups instead of the column table.
+constexpr int kTfcTR = kTfcTileRows32;
+__global__ void __launch_bounds__(kThreads, 5)
+    tile_kernel_tfc(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<float> F,
+                    const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
+                    const __grid_constant__ CUtensorMap tm_c, const float *__restrict__ tab, const int tab_len,
+                    float *__restrict__ psi_n, float *__restrict__ c_n, float *__restrict__ phi_n,
+                    BlockPartial *partials, int *err, const __grid_constant__ FinalRed FR, const int wave) {
+  const int f = max(PS.i_front, 0) / kW;
+  const int tr = blockIdx.x;
+  const int tc = front_first_block((int)blockIdx.y, f, (int)gridDim.y);
+  const unsigned nxt = blockIdx.y * gridDim.x + blockIdx.x + (unsigned)wave;
+  int pf_tr = -1, pf_tc = -1;
+  if (wave > 0 && nxt < gridDim.x * gridDim.y) {
+    pf_tr = (int)(nxt % gridDim.x);
+    pf_tc = front_first_block((int)(nxt / gridDim.x), f, (int)gridDim.y);
+  }
+  auto prefetch = [&]() {
+    if (pf_tc >= 0) {
+      tma_prefetch_2d(&tm_psi, kW * pf_tc - 4, kTfcTR * pf_tr);
+      tma_prefetch_2d(&tm_c, kW * pf_tc - 4, kTfcTR * pf_tr);
+    }
+  };
+  const SurrArgs none = {};
+  tile_body<false, kTfcTR, decltype(prefetch), true>(
+      K, F, PS, &tm_psi, &tm_c, tab, tab_len, psi_n, c_n, phi_n,
+      partials ? partials + ((int64_t)tc * gridDim.x + tr) : nullptr, err, none, tr, tc,
+      partials && FR.counter ? &FR : nullptr, prefetch);
 }
 
 // ---------------------------------------------------------------- ensemble
@@ -1727,6 +1862,39 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
   if (partials && nparts > max_partials) return -1;
   if (tm.col_tab_len < (int)grid.y * kW + kWin) return -1;
   const bool surr = tm.surr != nullptr;
+  if (K.tfc) {
+    // the coarse-grid temperature: no table kernel, so the tile kernel runs
+    // in plain stream order (it issues its TMA loads before
+    // griddepcontrol.wait, which is safe only after the table kernel); the
+    // maps' boxes are kTfcTR + 2 rows high
+    if (!P.T_coarse || surr) return -1;
+    const dim3 tg((nj + kTfcTR - 1) / kTfcTR, grid.y);
+    const int np = (int)(tg.x * tg.y);
+    if (partials && np > max_partials) return -1;
+    const size_t tsmem = sizeof(TileSmemT<kTfcTR, true>);
+    static std::atomic<unsigned long long> tattr{0};
+    if (!smem_limit_once((const void *)tile_kernel_tfc, (int)tsmem, tattr)) return -3;
+    static std::atomic<int> twave[64];
+    const int wave = resident_ctas((const void *)tile_kernel_tfc, kThreads, tsmem, twave);
+    if (wave < 0) return -3;
+    cudaLaunchConfig_t tc = {};
+    tc.gridDim = tg;
+    tc.blockDim = block;
+    tc.dynamicSmemBytes = tsmem;
+    tc.stream = st;
+    FinalRed fr = tm.red;
+    fr.partials = partials;
+    fr.nparts = np;
+    FinalRed none = fr;
+    none.counter = nullptr;
+    const float *tab = tm.col_tab;
+    if (cudaLaunchKernelEx(&tc, tile_kernel_tfc, K, F, P, tm.psi, tm.c, tab, tm.col_tab_len, psi_n, c_n, phi_n,
+                           partials, err, none, wave) != cudaSuccess)
+      return -3;
+    if (partials && (fr.mass_out || fr.itip_out) && launch_reduce_partials_dep(fr, st)) return -3;
+    if (nparts_out) *nparts_out = np;
+    return 0;
+  }
   if (tm.pipeline && !surr) {  // the persistent warp-role kernel (exact path)
     const int nrt = (int)grid.x, ncb = (int)grid.y;
     const size_t psmem = sizeof(PipeSmem32);

@@ -241,9 +241,33 @@ struct TileView {
 // them before it waits for its tile, so their latency hides under the load.
 struct LaneCols {
   double RT[2], C0[2], dK[3];
+  int tiT[2];       // TFC: the coarse column left of each of the lane's two columns
+  double tx[2];     // and the column's offset from it, in coarse cells
+  LogRef lr;        // TFC: the lane's reference temperature for log_near
 };
+__device__ __forceinline__ CellGroups cell_groups(const TileView &V, int gx, int row) {
+  int iT, jT;
+  double x, y;
+  tfc_col(V.K, V.PS.i_left_end_T, gx, iT, x);
+  tfc_row(V.K, row, jT, y);
+  const double T = tfc_T(V.K, V.PS.T_coarse, iT, x, jT, y);
+  return groups_at(V.K, T, log(T), true);
+}
+
+template <bool TFC>
 __device__ __forceinline__ LaneCols lane_cols(const TileView &V) {
   LaneCols L;
+  if constexpr (TFC) {  // per cell (cell_groups); no column differences
+    L.RT[0] = L.RT[1] = L.C0[0] = L.C0[1] = 0.0;
+    L.dK[0] = L.dK[1] = L.dK[2] = 0.0;
+    tfc_col(V.K, V.PS.i_left_end_T, V.gi, L.tiT[0], L.tx[0]);
+    tfc_col(V.K, V.PS.i_left_end_T, V.gi + 1, L.tiT[1], L.tx[1]);
+    int jT;
+    double y;
+    tfc_row(V.K, V.y0, jT, y);
+    L.lr = log_ref(tfc_T(V.K, V.PS.T_coarse, L.tiT[0], L.tx[0], jT, y));
+    return L;
+  }
   const double2 RTv = ld2(V.T.RT + V.gi), C0v = ld2(V.T.C0 + V.gi);
   L.RT[0] = RTv.x;
   L.RT[1] = RTv.y;
@@ -252,6 +276,9 @@ __device__ __forceinline__ LaneCols lane_cols(const TileView &V) {
   L.dK[0] = V.T.DK[V.gi - 1];  // faces x-1|x for x = col .. col+2
   L.dK[1] = V.T.DK[V.gi];
   L.dK[2] = V.T.DK[V.gi + 1];
+  L.tiT[0] = L.tiT[1] = 0;
+  L.tx[0] = L.tx[1] = 0.0;
+  L.lr = LogRef{0.0, 0.0, 0.0};
   return L;
 }
 
@@ -273,13 +300,14 @@ __device__ __forceinline__ bool fix_beyond(const TileView &V, InSlot &in) {
 // ---- phase 1: per-cell terms of the input rows of group warp gw (rows gw,
 // gw+4, ...) and of the halo columns (group threads 64..99); st.liq and
 // st.sol must be 0 on entry
+template <bool TFC>
 __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, const InSlot &in, StSlot &st) {
   const Coef<double> &F = V.F;
   const int lane = V.lane, bc = V.bc;
   const double cinf = F.cinf;
   constexpr double KL = -2.0 * kL0Liq;
   const double d_hi = F.ser_hi, d_lo = F.ser_lo;  // series range of delta (Coef)
-  const double RTa[2] = {LC.RT[0], LC.RT[1]}, C0a[2] = {LC.C0[0], LC.C0[1]};
+  double RTa[2] = {LC.RT[0], LC.RT[1]}, C0a[2] = {LC.C0[0], LC.C0[1]}, KCa[2] = {0.0, 0.0};
   // per lane, bit q: psi is exactly +1 over the 3x3 neighbourhood of cell
   // bc+q (rows of the box only; column -1 of the left-most tile enters no
   // face, column 0 being a ghost).  S = q(1) c (1 - c) = 0 there, so every
@@ -324,8 +352,25 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
     const unsigned long long b0 = bits(pv[0]), b1 = bits(pv[1]);
     const bool liq2 = b0 == kMinus1 && b1 == kMinus1;
     const bool sol2 = b0 == kPlus1 && b1 == kPlus1;
+    // the row's form (warp-uniform): far melt, bulk melt or general
+    const bool far = __all_sync(FULL, liq2 && fmax(fabs(dv[0]), fabs(dv[1])) <= tiny);
+    const bool bulk = !far && __all_sync(FULL, liq2 && fmax(dv[0], dv[1]) < d_hi && fmin(dv[0], dv[1]) > d_lo);
+    if constexpr (TFC) {  // the melt forms need RT and K + C0 only
+      int jT;
+      double y;
+      tfc_row(V.K, V.y0 - 1 + rr, jT, y);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const double T = tfc_T(V.K, V.PS.T_coarse, LC.tiT[q], LC.tx[q], jT, y);
+        const CellGroups cg = groups_at(V.K, T, log_near(LC.lr, T), !(far || bulk));
+        RTa[q] = cg.RT;
+        C0a[q] = cg.C0;
+        KCa[q] = cg.KC;
+      }
+    }
     uint32_t code;
-    if (__all_sync(FULL, liq2 && fmax(fabs(dv[0]), fabs(dv[1])) <= tiny)) {
+    bool deep = false;
+    if (far) {
       // far melt: g = -1, q = 1, lam by its Taylor polynomial in delta
       // (Coef::melt_a, six terms); mu'' = RT lam - 2 L0_Liq delta
       // = delta (RT p + KL), lam = delta p
@@ -338,7 +383,7 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
         Sv[q] = cv[q] * (1.0 - cv[q]);
         mv[q] = dv[q] * fma(RTa[q], p, KL);
       }
-    } else if (__all_sync(FULL, liq2 && fmax(dv[0], dv[1]) < d_hi && fmin(dv[0], dv[1]) > d_lo)) {
+    } else if (bulk) {
       // bulk melt: g = -1, q = 1
       code = 1u;
 #pragma unroll
@@ -355,6 +400,7 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
       const uint32_t s3 = (code & 2u) ? solid3(rr) : 0u;
       if ((code & 2u) && __all_sync(FULL, s3 == 0x3u)) {
         Sv[0] = Sv[1] = mv[0] = mv[1] = 0.0;
+        deep = true;
       } else {
         double sv[2];
         bool small = true;
@@ -373,6 +419,10 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
         }
         st.pmask[rr][lane] = (uint8_t)(L | (Sm << 4));
       }
+    }
+    if (TFC && !deep) {  // mu = mu'' + (K + C0) of the cell itself
+      mv[0] += KCa[0];
+      mv[1] += KCa[1];
     }
     st2(&st.S[rr][bc], Sv[0], Sv[1]);
     st2(&st.mu[rr][bc], mv[0], mv[1]);
@@ -395,7 +445,13 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
       const double pv = in.psi[rr][x], cv = in.c[rr][x];
       const double dv = cv - cinf;
       const double sv = dv / fma(2.0 * cinf, 1.0 - cv, dv);
-      cell_terms(F, pv, cv, sv, fabs(sv) < 1.0 / 9.0, V.T.RT[g], V.T.C0[g], Sh, mh);
+      if constexpr (TFC) {
+        const CellGroups cg = cell_groups(V, g, V.y0 - 1 + rr);
+        cell_terms(F, pv, cv, sv, fabs(sv) < 1.0 / 9.0, cg.RT, cg.C0, Sh, mh);
+        mh += cg.KC;
+      } else {
+        cell_terms(F, pv, cv, sv, fabs(sv) < 1.0 / 9.0, V.T.RT[g], V.T.C0[g], Sh, mh);
+      }
       hm = (pv <= -1.0 ? 1u : 0u) | (pv >= 1.0 ? 2u : 0u);
     }
     st.S[rr][x] = Sh;
@@ -560,6 +616,7 @@ __device__ __forceinline__ uint32_t phase2(const TileView &V, const LaneCols &LC
 
 // ---- phase 3: the listed interface cells, one per group thread
 // (compute_phi, fun.cu:1143-1218); new psi into np[rr][x]
+template <bool TFC>
 __device__ __forceinline__ void phase3(const TileView &V, const InSlot &in, const P2Smem &p2,
                                        double (*np)[kWin], bool red, int &itip) {
   const int nlist = p2.nlist;
@@ -568,7 +625,16 @@ __device__ __forceinline__ void phase3(const TileView &V, const InSlot &in, cons
     const int rr = (int)(e >> 8), x = (int)(e & 0xFFu) + 4;  // box column
     const int r = V.y0 - 1 + rr, g = V.x0 + x - 4;
     const double c00 = in.c[rr][x];
-    const double dG = (1.0 - c00) * V.T.Anb[g] + c00 * V.T.Ati[g] + c00 * (1.0 - c00) * (kL0Liq - kL0Bcc);
+    double Anb, Ati;
+    if constexpr (TFC) {
+      const CellGroups cg = cell_groups(V, g, r);
+      Anb = cg.Anb;
+      Ati = cg.Ati;
+    } else {
+      Anb = V.T.Anb[g];
+      Ati = V.T.Ati[g];
+    }
+    const double dG = (1.0 - c00) * Anb + c00 * Ati + c00 * (1.0 - c00) * (kL0Liq - kL0Bcc);
     const double res = phi_cell_dG<double>(
         &V.F, clamp1(in.psi[rr][x]), clamp1(in.psi[rr][x + 1]), clamp1(in.psi[rr][x - 1]),
         clamp1(in.psi[rr + 1][x]), clamp1(in.psi[rr - 1][x]), clamp1(in.psi[rr + 1][x + 1]),
@@ -729,6 +795,7 @@ __device__ __forceinline__ void tile_of(int t, int nrt, int ncb, int f, int &tr,
 }
 
 // ---------------------------------------------------------------- one tile per CTA
+template <bool TFC>
 __global__ void __launch_bounds__(kThreads, 5)
     tile_kernel_f64(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<double> F,
                     const __grid_constant__ StepScalars PS, const __grid_constant__ CUtensorMap tm_psi,
@@ -765,7 +832,7 @@ __global__ void __launch_bounds__(kThreads, 5)
   // the step's final reduction (a programmatic dependent) may be scheduled now
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const TileView V(K, F, PS, tab, tab_len, x0, y0, (int)threadIdx.x);
-  const LaneCols LC = lane_cols(V);
+  const LaneCols LC = lane_cols<TFC>(V);
   __syncthreads();  // barrier initialised, flags cleared
   {
     // bounded wait for the tile; if any thread gives up, the whole CTA skips
@@ -794,7 +861,7 @@ __global__ void __launch_bounds__(kThreads, 5)
     }
   }
   if (fix_beyond(V, sm.in)) __syncthreads();
-  phase1(V, LC, sm.in, sm.st);
+  phase1<TFC>(V, LC, sm.in, sm.st);
   __syncthreads();
   // phase 1 done: pull the tile of the CTA that will start about one resident
   // wave later into L2, so its loads overlap the rest of this wave's arithmetic
@@ -813,7 +880,7 @@ __global__ void __launch_bounds__(kThreads, 5)
   double dn[kRowsPerWarp][2];
   const uint32_t needs_all = phase2(V, LC, sm.in, sm.st, sm.p2, dn, mass, red);
   __syncthreads();
-  phase3(V, sm.in, sm.p2, sm.st.S, red, itip);  // S is free after phase 2
+  phase3<TFC>(V, sm.in, sm.p2, sm.st.S, red, itip);  // S is free after phase 2
   __syncthreads();
   phase4_rows(V, sm.in, sm.st.S, needs_all, dn, red, itip);
   store_tile(V, sm.in, psi_n, c_n, phi_n, 0);
@@ -935,7 +1002,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
       }
       fix_beyond(V, sm.in[s]);
       gsync(kBarP1);
-      phase1(V, lane_cols(V), sm.in[s], sm.st[q]);
+      phase1<false>(V, lane_cols<false>(V), sm.in[s], sm.st[q]);
       gsync(kBarP1);
       if (gtid == 0) mbar_arrive(&sm.st_full[q]);
     }
@@ -957,9 +1024,9 @@ __global__ void __launch_bounds__(kPipeThreads, 2)
     double mass = 0.0;
     int itip = 0;
     double dn[kRowsPerWarp][2];
-    const uint32_t needs_all = phase2(V, lane_cols(V), sm.in[s], sm.st[q], sm.p2, dn, mass, red);
+    const uint32_t needs_all = phase2(V, lane_cols<false>(V), sm.in[s], sm.st[q], sm.p2, dn, mass, red);
     gsync(kBarP2);
-    phase3(V, sm.in[s], sm.p2, sm.st[q].S, red, itip);  // S of the slot is free after phase 2
+    phase3<false>(V, sm.in[s], sm.p2, sm.st[q].S, red, itip);  // S of the slot is free after phase 2
     gsync(kBarP2);
     phase4_rows(V, sm.in[s], sm.st[q].S, needs_all, dn, red, itip);
     const bool issued = store_tile(V, sm.in[s], psi_n, c_n, phi_n, kBarP2);
@@ -988,16 +1055,23 @@ int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScal
   const int nparts = nrt * ncb;
   if (partials && nparts > max_partials) return -1;
   if (!tm.col_tab64 || tm.col_tab64_len < ncb * kW + kWin) return -1;
-  const bool pipe = tm.pipeline != 0;
+  // the coarse-grid temperature: per-cell groups, no column table (the
+  // persistent pipeline has no TFC form and is not taken then)
+  const bool tfc = K.tfc != 0;
+  if (tfc && !P.T_coarse) return -1;
+  const bool pipe = tm.pipeline != 0 && !tfc;
+  const int which = pipe ? 1 : tfc ? 2 : 0;
   const size_t smem = pipe ? sizeof(PipeSmem64) : sizeof(TileSmem64);
-  const void *kfn = pipe ? (const void *)pipe_kernel_f64 : (const void *)tile_kernel_f64;
-  static std::atomic<unsigned long long> attr_done[2];
-  if (!smem_limit_once(kfn, (int)smem, attr_done[pipe])) return -3;
-  static std::atomic<int> resident_of[2][64];
-  const int resident = resident_ctas(kfn, pipe ? kPipeThreads : kThreads, smem, resident_of[pipe]);
+  const void *kfn = pipe ? (const void *)pipe_kernel_f64
+                         : tfc ? (const void *)tile_kernel_f64<true> : (const void *)tile_kernel_f64<false>;
+  static std::atomic<unsigned long long> attr_done[3];
+  if (!smem_limit_once(kfn, (int)smem, attr_done[which])) return -3;
+  static std::atomic<int> resident_of[3][64];
+  const int resident = resident_ctas(kfn, pipe ? kPipeThreads : kThreads, smem, resident_of[which]);
   if (resident <= 0) return -3;
-  column_table_kernel_f64<<<(tm.col_tab64_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(
-      K, P.d0, P.d1, tm.col_tab64_len, tm.col_tab64);
+  if (!tfc)
+    column_table_kernel_f64<<<(tm.col_tab64_len + kTabBlock - 2) / (kTabBlock - 1), kTabBlock, 0, st>>>(
+        K, P.d0, P.d1, tm.col_tab64_len, tm.col_tab64);
   cudaLaunchConfig_t cfg = {};
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
@@ -1005,7 +1079,11 @@ int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScal
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  // a programmatic dependent of the table kernel only: the tile kernel issues
+  // its TMA loads before griddepcontrol.wait, which is safe after the table
+  // kernel (it writes no field) but not after the previous step's kernels,
+  // so a TFC step (no table kernel) launches in plain stream order
+  cfg.numAttrs = tfc ? 0 : 1;
   const double *tab = tm.col_tab64;
   // the final reduction is a programmatic dependent launch after the step
   FinalRed fr = tm.red;
@@ -1024,8 +1102,8 @@ int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScal
     // column-major: consecutive CTAs share a column strip and its halo rows in L2
     cfg.gridDim = dim3(nrt, ncb);
     cfg.blockDim = dim3(kThreads);
-    e = cudaLaunchKernelEx(&cfg, tile_kernel_f64, K, F, P, tm.psi, tm.c, tab, tm.col_tab64_len, psi_n, c_n, phi_n,
-                           partials, err, none, resident);
+    e = cudaLaunchKernelEx(&cfg, tfc ? tile_kernel_f64<true> : tile_kernel_f64<false>, K, F, P, tm.psi, tm.c, tab,
+                           tm.col_tab64_len, psi_n, c_n, phi_n, partials, err, none, resident);
   }
   if (e != cudaSuccess) return -3;
   if (partials && (fr.mass_out || fr.itip_out) && launch_reduce_partials_dep(fr, st)) return -3;

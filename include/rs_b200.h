@@ -182,8 +182,9 @@ int rs_destroy(rs_ctx *ctx);
 int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
 
 /* Options: RS_OPT_TMA (default 1) stages the step's field tiles into shared
- * memory with TMA copies; 0 selects the register-prefetch kernel (always used
- * for pull-back steps, the coarse temperature and unaligned fields).
+ * memory with TMA copies (frozen and coarse-grid temperature); 0 selects the
+ * register-prefetch kernel (always used for pull-back steps and unaligned
+ * fields).
  * RS_OPT_WAIT_LIMIT (default 0: the kernels' own limit of 2^20 suspending
  * tries) bounds the tile kernels' waits for their TMA loads; when set, a wait
  * polls without suspending and gives up after that many polls.  A tile whose
@@ -191,8 +192,8 @@ int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
  * RS_E_STATE.  Tests set it to 1 to run that path.  Set on run 0's context
  * of an ensemble, it also bounds the persistent walk's grid-barrier waits
  * (polls; default 2^22).
- * RS_OPT_PIPELINE (default 0) runs the tile step (FP64, and FP32 without a
- * surrogate) as a persistent kernel of warp roles (a TMA producer warp, a
+ * RS_OPT_PIPELINE (default 0) runs the frozen-temperature tile step (FP64,
+ * and FP32 without a surrogate) as a persistent kernel of warp roles (a TMA producer warp, a
  * phase-1 group and a flux/update/store group working on three tiles at
  * once) instead of one tile per CTA; both give the same fields bit for
  * bit. */
@@ -358,7 +359,8 @@ int rs_mlp_forward(const rs_mlp_box *box, const float *d_w, int64_t n, const flo
  * two tensor-core layers, FP32 for the first) and of the box.  The network
  * stands in for the cells outside the exact bulk-melt form; cells whose T or
  * c lie outside the box, and one cell in 1024 per step of those (audit), are
- * evaluated exactly. */
+ * evaluated exactly.  Frozen temperature only: RS_E_UNSUPPORTED on a context
+ * with the coarse-grid temperature. */
 int rs_set_surrogate(rs_ctx *ctx, const float *d_w, const rs_mlp_box *box);
 /* Largest |surrogate - exact| of mu'' and dG over the audited cells and the
  * counts of fallback and audited cells since the last call; clears them.

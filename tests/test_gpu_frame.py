@@ -172,6 +172,39 @@ def test_tfc_step_f64():
     assert maxabs(g.psi, o.psi) <= 1e-13 and maxabs(g.c, o.c) <= 1e-13
 
 
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_tfc_back_to_back_tile_steps(dtype):
+    """Coarse-grid-temperature steps on the TMA tile kernels, launched back to
+    back with no other kernel between them (no reduction, fixed T), against
+    the same steps on the register-window kernel (RS_OPT_TMA = 0): each step
+    must read the previous step's finished fields.  The two kernels group the
+    arithmetic differently, so they agree to rounding, not bit for bit (FP32:
+    to its rounding over 40 steps)."""
+    dt = getattr(torch, dtype)
+    tol_psi, tol_c = (1e-11, 1e-11) if dt == torch.float64 else (2e-4, 2e-5)
+    p = configs.small(256, 250, i_tip_target=40, tfc=1, G=1e7, V=0.5)
+    p.length_sample_um = 2.0
+    p.Tcold = p.T_ref - p.GG * p.dx * p.S * p.W0 * (p.i_tip_target + 30)
+    d = pyoracle.derive(p)
+    s = perturbed_state(p, 31, amp=0.3)
+    out = []
+    for tma in (1, 0):
+        ctx = lib.Context(p)
+        ctx.set_option(_abi.RS_OPT_TMA, tma)
+        T = torch.zeros(d.NxT_all * d.NyT_all, dtype=torch.float64, device="cuda")
+        ctx.temperature_init(T)
+        ile = d.i_left_end_initial
+        a, b = upload(p, s, dt), lib.FieldSet(p, dt)
+        for n in range(40):
+            ctx.step(a, b, n, T_coarse=T, i_left_end=ile, i_left_end_T=ile)
+            a, b = b, a
+        torch.cuda.synchronize()
+        ctx.device_status()
+        out.append(download(p, a))
+        ctx.close()
+    assert maxabs(out[0].psi, out[1].psi) <= tol_psi and maxabs(out[0].c, out[1].c) <= tol_c
+
+
 def test_tfc_loop_with_pull_back_f64():
     """The coarse-temperature loop of fun.cu:431-514 over 120 steps, pull-back
     every 30 steps with non-zero shifts, on the GPU (pull-back fused into
