@@ -11,9 +11,10 @@
 //   * ghost cells (compute_boundary_individual, fun.cu:1220-1230) are written
 //     by the cell they copy, corners included.
 //
-// Three kernels: this file's register-prefetch kernel (pull-back steps, the
-// coarse-grid temperature, unaligned fields) and the TMA-staged tile kernels
-// of rs_step_f32.cu (FP32) and rs_step_f64t.cu (FP64).
+// Three kernels: this file's register-prefetch kernel (pull-back steps,
+// unaligned fields, RS_OPT_TMA = 0) and the TMA-staged tile kernels of
+// rs_step_f32.cu (FP32) and rs_step_f64t.cu (FP64), frozen and coarse-grid
+// temperature.
 //
 // Layout of the work here: a warp owns a strip of 30 output columns (32 input
 // columns with a one-column halo on each side) and marches down H rows (H

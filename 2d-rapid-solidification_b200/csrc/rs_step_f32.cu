@@ -57,6 +57,12 @@
 // launched one resident wave later, so the tiles of the next wave arrive
 // while this wave computes (the CTAs of a wave otherwise load, compute and
 // store in step).
+// The coarse-grid temperature (TFC, interpolate_temperature fun.cu:1580-1608)
+// takes tile_kernel_tfc alone: every cell evaluates its CALPHAD groups from its
+// own bilinear temperature (the melt rows only the liquid functions, log T by
+// the series of log_near), keeps K + C0 in FP64 in shared memory, and the
+// faces add its differences, rounded to FP32, along both axes; tiles of 8
+// output rows, so that the FP64 array fits with five CTAs per SM.
 // Fields store psi and delta = c - cinf (include/rs_b200.h).
 #include "rs_step_common.cuh"
 #include "rs_surrogate.cuh"

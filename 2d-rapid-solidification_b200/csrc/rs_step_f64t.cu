@@ -52,6 +52,12 @@
 // Launch order: the tile columns from the one holding the front
 // (front_first_block).  After phase 1 each CTA prefetches into L2 the input
 // tile of the block launched one resident wave later.
+// The coarse-grid temperature (TFC, interpolate_temperature
+// fun.cu:1580-1608): no table kernel; every cell evaluates its CALPHAD groups
+// from its own bilinear temperature (melt rows only the liquid functions, log
+// T by the series of log_near) and stores mu = mu'' + (K + C0), so the faces
+// take plain differences of mu.  The tile kernel then runs in plain stream
+// order: it issues its TMA loads before griddepcontrol.wait.
 //
 // Two kernels run these phases (same functions, same results bit for bit):
 //   * tile_kernel_f64: one tile per CTA of 128 threads, the phases in series
