@@ -27,12 +27,18 @@ def main(argv=None):
     ap.add_argument("--surrogate", action="store_true",
                     help="FP32: train the CALPHAD surrogate on the wide box (10 epochs) and step through it")
     ap.add_argument("--nz", type=int, default=0, help="3D: override the number of z planes")
+    ap.add_argument("--tfc", action="store_true",
+                    help="2D: the coarse-grid temperature, initialised and then held fixed (the step alone)")
     a = ap.parse_args(argv)
     if a.config == "peritectic_3d":
         return run3(a)
     p = getattr(configs, a.config)()
     if a.grid:
         p.nx_all = p.ny_all = a.grid
+    if a.tfc:  # coarse T: a 4 um sample, the front 30 cells above Tcold
+        p.tfc = 1
+        p.length_sample_um = 4.0
+        p.Tcold = p.T_ref - p.GG * p.dx * p.S * p.W0 * (p.i_tip_target + 30)
     ctx = lib.Context(p)
     if a.no_tma:
         ctx.set_option(_abi.RS_OPT_TMA, 0)
@@ -46,6 +52,11 @@ def main(argv=None):
     dt = torch.float64 if a.precision == "f64" else torch.float32
     cur, nxt = lib.FieldSet(p, dt), lib.FieldSet(p, dt)
     ctx.initial_planar(cur, configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ, configs.IC_SEED)
+    T, ile = None, 0
+    if a.tfc:
+        T = torch.zeros(d.NxT_all * d.NyT_all, dtype=torch.float64, device="cuda")
+        ctx.temperature_init(T)
+        ile = d.i_left_end_initial
     itip = torch.zeros(1, dtype=torch.int32, device="cuda")
     mass = torch.zeros(1, dtype=torch.float64, device="cuda")
     hist, l = 0, 0.0
@@ -55,7 +66,8 @@ def main(argv=None):
             ctx.itip(cur, itip)
             pb = int(itip.item()) - p.i_tip_target
             hist += pb
-        ctx.step(cur, nxt, n, i_offset_history=hist, l_offset_Vp=l, pull_back=pb)
+        ctx.step(cur, nxt, n, i_offset_history=hist, l_offset_Vp=l, pull_back=pb, T_coarse=T, i_left_end=ile,
+                 i_left_end_T=ile)
         l += p.Vp * d.dt * d.tau0 / (p.S * p.W0)
         cur, nxt = nxt, cur
     ctx.mass(cur, mass)
@@ -85,6 +97,11 @@ def tip_run(p, dtype, nsteps, every=1000, surrogate=None, ic_seed=None, initial=
     a, b = lib.FieldSet(p, dtype), lib.FieldSet(p, dtype)
     cl, cs = initial if initial is not None else (configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ)
     ctx.initial_planar(a, cl, cs, configs.IC_SEED if ic_seed is None else ic_seed)
+    T, ile = None, 0
+    if a.tfc:
+        T = torch.zeros(d.NxT_all * d.NyT_all, dtype=torch.float64, device="cuda")
+        ctx.temperature_init(T)
+        ile = d.i_left_end_initial
     itip = torch.zeros(1, dtype=torch.int32, device="cuda")
     tipbuf = torch.zeros(C.sizeof(_abi.Tip), dtype=torch.uint8, device="cuda")
     mass = torch.zeros(2, dtype=torch.float64, device="cuda")
