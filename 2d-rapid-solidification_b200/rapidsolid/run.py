@@ -97,11 +97,6 @@ def tip_run(p, dtype, nsteps, every=1000, surrogate=None, ic_seed=None, initial=
     a, b = lib.FieldSet(p, dtype), lib.FieldSet(p, dtype)
     cl, cs = initial if initial is not None else (configs.C_LIQUID_TI10NB, configs.C_SOLID_AT_TLIQ)
     ctx.initial_planar(a, cl, cs, configs.IC_SEED if ic_seed is None else ic_seed)
-    T, ile = None, 0
-    if a.tfc:
-        T = torch.zeros(d.NxT_all * d.NyT_all, dtype=torch.float64, device="cuda")
-        ctx.temperature_init(T)
-        ile = d.i_left_end_initial
     itip = torch.zeros(1, dtype=torch.int32, device="cuda")
     tipbuf = torch.zeros(C.sizeof(_abi.Tip), dtype=torch.uint8, device="cuda")
     mass = torch.zeros(2, dtype=torch.float64, device="cuda")
