@@ -660,7 +660,8 @@ def tinb_3d_leg(peak, nsteps_run=5000, ntimed=10):
                      "ms_per_step": round(ms, 4), "grid": [p.nx, p.ny, p.nz], "interior_cells": cells,
                      "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                                   "frac": round(achieved / peak, 4), "algorithmic_bytes_per_launch": alg,
-                                  "kernel": "rs::tinb_kernel<float>"},
+                                  "kernel": "rs::tinb_kernel<float> (surrogate)" if use
+                                  else "rs::tinb_x2_kernel (packed FP32 pairs)"},
                      "run": {"steps": nsteps_run, "ms": round(run_ms, 1), "front_cells": [round(x, 4) for x in fr],
                              "front_speed_m_s": round(speed, 6), "solute_drift_rel": (m1 - m0) / m0}}
         if use:
