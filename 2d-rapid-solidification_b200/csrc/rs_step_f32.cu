@@ -108,6 +108,8 @@ struct alignas(128) TileSmemT {
   uint8_t pmask[kRin][32];  // per lane: bits 0-3 psi <= -1, bits 4-7 psi >= 1 of its four cells
   uint8_t hmask[kRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
   Mask liq, sol;            // bit r: every cell of input row r has psi == -1 / +1
+  double ty[kRin];          // TFC: the row part of each input row's temperature
+  int tj[kRin];             // (tfc_row), once per tile
   int nlist;
   double part_mass[kWarps];
   int part_itip[kWarps];
@@ -278,6 +280,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     double y;
     tfc_row(K, y0, jT, y);
     lref = log_ref(tfc_T(K, PS.T_coarse, tiT[0], tx[0], jT, y));
+    if (threadIdx.x < kTRin) tfc_row(K, y0 - 1 + (int)threadIdx.x, sm.tj[threadIdx.x], sm.ty[threadIdx.x]);
   }
   // TFC: all groups of one cell, the logarithm exact (halo and interface cells)
   auto tfc_cell = [&](int gx, int row) {
@@ -472,9 +475,8 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     if constexpr (TFC) {  // the melt forms need RT and K + C0 only
       far = __all_sync(FULL, liq4 && fmaxf(dmx, -dmn) <= tiny);
       bulk = !far && __all_sync(FULL, liq4 && dmx < d_hi && dmn > d_lo);
-      int jT;
-      double y;
-      tfc_row(K, y0 - 1 + rr, jT, y);
+      const int jT = sm.tj[rr];
+      const double y = sm.ty[rr];
       double kq[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -593,7 +595,13 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     if (y0 - 1 + rr <= K.ny - 1) {
       const float pv = sm.psi[rr][x];
       if constexpr (TFC) {
-        const CellGroups cg = tfc_cell(g, y0 - 1 + rr);
+        // C0 enters mu'' as (g + 1) C0, 0 at psi = -1 exactly: the liquid
+        // groups suffice there
+        int iT;
+        double xc;
+        tfc_col(K, PS.i_left_end_T, g, iT, xc);
+        const double T = tfc_T(K, PS.T_coarse, iT, xc, sm.tj[rr], sm.ty[rr]);
+        const CellGroups cg = groups_at(K, T, log_near(lref, T), __float_as_uint(pv) != kMinus1);
         cell_terms(F, pv, sm.d[rr][x], (float)cg.RT, (float)cg.C0, Sh, mh);
         kh = cg.KC;
       } else {

@@ -110,6 +110,8 @@ struct alignas(16) StSlot {
                              // (rows flagged in liq / sol store none)
   uint8_t hmask[kTRin][2];   // halo cells: bit 0 psi <= -1, bit 1 psi >= 1
   uint32_t liq, sol;         // bit r: every cell of input row r has psi == -1 / +1
+  double ty[kTRin];          // TFC: the row part of each input row's temperature
+  int tj[kTRin];             // (tfc_row), once per tile
 };
 // phases 2-4: the interface list and the partial sums
 struct P2Smem {
@@ -362,9 +364,8 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
     const bool far = __all_sync(FULL, liq2 && fmax(fabs(dv[0]), fabs(dv[1])) <= tiny);
     const bool bulk = !far && __all_sync(FULL, liq2 && fmax(dv[0], dv[1]) < d_hi && fmin(dv[0], dv[1]) > d_lo);
     if constexpr (TFC) {  // the melt forms need RT and K + C0 only
-      int jT;
-      double y;
-      tfc_row(V.K, V.y0 - 1 + rr, jT, y);
+      const int jT = st.tj[rr];
+      const double y = st.ty[rr];
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const double T = tfc_T(V.K, V.PS.T_coarse, LC.tiT[q], LC.tx[q], jT, y);
@@ -452,7 +453,13 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
       const double dv = cv - cinf;
       const double sv = dv / fma(2.0 * cinf, 1.0 - cv, dv);
       if constexpr (TFC) {
-        const CellGroups cg = cell_groups(V, g, V.y0 - 1 + rr);
+        // C0 enters mu'' as (g + 1) C0, 0 at psi = -1 exactly: the liquid
+        // groups suffice there
+        int iT;
+        double xc;
+        tfc_col(V.K, V.PS.i_left_end_T, g, iT, xc);
+        const double T = tfc_T(V.K, V.PS.T_coarse, iT, xc, st.tj[rr], st.ty[rr]);
+        const CellGroups cg = groups_at(V.K, T, log_near(LC.lr, T), bits(pv) != kMinus1);
         cell_terms(F, pv, cv, sv, fabs(sv) < 1.0 / 9.0, cg.RT, cg.C0, Sh, mh);
         mh += cg.KC;
       } else {
@@ -839,7 +846,10 @@ __global__ void __launch_bounds__(kThreads, 5)
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const TileView V(K, F, PS, tab, tab_len, x0, y0, (int)threadIdx.x);
   const LaneCols LC = lane_cols<TFC>(V);
-  __syncthreads();  // barrier initialised, flags cleared
+  if constexpr (TFC) {  // the row part of the cells' temperatures, once per tile row
+    if (threadIdx.x < kTRin) tfc_row(K, y0 - 1 + (int)threadIdx.x, sm.st.tj[threadIdx.x], sm.st.ty[threadIdx.x]);
+  }
+  __syncthreads();  // barrier initialised, flags cleared (and the TFC row table written)
   {
     // bounded wait for the tile; if any thread gives up, the whole CTA skips
     // the tile: no phase runs on a partly filled tile and nothing is stored.
