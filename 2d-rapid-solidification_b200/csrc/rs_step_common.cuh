@@ -289,6 +289,60 @@ __device__ __forceinline__ double log_near(const LogRef &L, double T) {
   p = fma(p, u, 1.0);
   return fma(p, u, L.lT0);
 }
+// K + C0 near a tile's reference temperature T0 as its Taylor polynomial in
+// T - T0 (degree 6).  For T in [1941, 2750) K, G_Ti_Liq - G_Nb_Liq is one SGTE
+// expression a + bT + cT lnT + dT^2 + eT^3 + f/T + hT^7 (the coefficients of
+// g_ti_liq's upper and g_nb_liq's lower piece, fun.cu:1628-1669), whose
+// derivatives are closed forms; the remainder after degree 6 is below
+// |KC^(7)| |T - T0|^7 / 7! < 2e-16 J/mol for |T - T0| <= 4 K.  The constant
+// term is the cell form itself (groups_at) at T0.  Cells outside the range
+// or farther than 4 K from T0 take groups_at.
+struct KcPoly {
+  LogRef lr;     // T0, log T0, 1 / T0 (also log_near's reference)
+  double c[7];   // KC^(k)(T0) / k!
+  int ok;        // T0 in [1941, 2750)
+};
+__device__ __forceinline__ KcPoly kc_poly(const StepCoef &K, double T0) {
+  KcPoly P;
+  P.lr = log_ref(T0);
+  P.ok = T0 >= 1941.0 && T0 < 2750.0;
+  constexpr double c = -46.29 + 26.4711, d = -0.203475e-3, e = 0.35012e-6, f = -93399.0, h = 306.098e-25;
+  const double b = (298.7367 - 131.229057) + K.RR * K.Lref;
+  const double T = T0, lT = P.lr.lT0, i1 = P.lr.iT0;
+  const double i2 = i1 * i1, i3 = i2 * i1, i4 = i2 * i2, i5 = i4 * i1, i6 = i3 * i3, i7 = i6 * i1;
+  const double T2 = T * T, T3 = T2 * T, T4 = T2 * T2, T5 = T4 * T, T6 = T3 * T3;
+  P.c[0] = groups_at(K, T, lT, false).KC;
+  P.c[1] = b + c * (lT + 1.0) + 2.0 * d * T + 3.0 * e * T2 - f * i2 + 7.0 * h * T6;
+  P.c[2] = (c * i1 + 2.0 * d + 6.0 * e * T + 2.0 * f * i3 + 42.0 * h * T5) / 2.0;
+  P.c[3] = (-c * i2 + 6.0 * e - 6.0 * f * i4 + 210.0 * h * T4) / 6.0;
+  P.c[4] = (2.0 * c * i3 + 24.0 * f * i5 + 840.0 * h * T3) / 24.0;
+  P.c[5] = (-6.0 * c * i4 - 120.0 * f * i6 + 2520.0 * h * T2) / 120.0;
+  P.c[6] = (24.0 * c * i5 + 720.0 * f * i7 + 5040.0 * h * T) / 720.0;
+  return P;
+}
+// K + C0 at T from P, or false where the polynomial does not apply
+__device__ __forceinline__ bool kc_eval(const KcPoly &P, double T, double &kc) {
+  const double u = T - P.lr.T0;
+  if (!P.ok || !(T >= 1941.0 && T < 2750.0 && fabs(u) <= 4.0)) return false;
+  double r = P.c[6];
+#pragma unroll
+  for (int k = 5; k >= 0; --k) r = fma(r, u, P.c[k]);
+  kc = r;
+  return true;
+}
+// the groups a cell needs: RT and K + C0 always, C0 where full (the general
+// row form; the melt forms multiply C0 by g + 1 = 0)
+__device__ __forceinline__ void cell_tfc(const StepCoef &K, const KcPoly &P, double T, bool full, double &RT,
+                                         double &C0, double &KC) {
+  RT = K.RR * T;
+  C0 = 0.0;
+  const bool poly = kc_eval(P, T, KC);
+  if (!poly || full) {
+    const CellGroups g = groups_at(K, T, log_near(P.lr, T), full);
+    C0 = g.C0;
+    if (!poly) KC = g.KC;
+  }
+}
 // interpolate_temperature's coordinates (fun.cu:1588-1594), split into the
 // column part (fixed per lane) and the row part (one per row): the same
 // expressions as t_fine_at, so the same temperature

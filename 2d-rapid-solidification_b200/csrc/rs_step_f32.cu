@@ -110,6 +110,7 @@ struct alignas(128) TileSmemT {
   Mask liq, sol;            // bit r: every cell of input row r has psi == -1 / +1
   double ty[kRin];          // TFC: the row part of each input row's temperature
   int tj[kRin];             // (tfc_row), once per tile
+  std::conditional_t<TFC, KcPoly, char> kp;  // TFC: K + C0 near the tile's temperature
   int nlist;
   double part_mass[kWarps];
   int part_itip[kWarps];
@@ -269,18 +270,21 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   // TFC: RT and C0 per row, from each cell's own temperature
   float RTa[4] = {RTv.x, RTv.y, RTv.z, RTv.w}, C0a[4] = {C0v.x, C0v.y, C0v.z, C0v.w};
   // TFC: the column part of each cell's temperature (interpolate_temperature,
-  // fun.cu:1580-1608) and the lane's reference temperature for log_near
+  // fun.cu:1580-1608); the row part and K + C0 about the tile's centre once
+  // per tile, in shared memory
   int tiT[4] = {0, 0, 0, 0};
   double tx[4] = {0.0, 0.0, 0.0, 0.0};
-  LogRef lref{0.0, 0.0, 0.0};
   if constexpr (TFC) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) tfc_col(K, PS.i_left_end_T, gi + q, tiT[q], tx[q]);
-    int jT;
-    double y;
-    tfc_row(K, y0, jT, y);
-    lref = log_ref(tfc_T(K, PS.T_coarse, tiT[0], tx[0], jT, y));
     if (threadIdx.x < kTRin) tfc_row(K, y0 - 1 + (int)threadIdx.x, sm.tj[threadIdx.x], sm.ty[threadIdx.x]);
+    if (threadIdx.x == kTRin) {
+      int iT, jT;
+      double x, y;
+      tfc_col(K, PS.i_left_end_T, x0 + kW / 2, iT, x);
+      tfc_row(K, y0 + kTR / 2, jT, y);
+      sm.kp = kc_poly(K, tfc_T(K, PS.T_coarse, iT, x, jT, y));
+    }
   }
   // TFC: all groups of one cell, the logarithm exact (halo and interface cells)
   auto tfc_cell = [&](int gx, int row) {
@@ -480,11 +484,10 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       double kq[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const double T = tfc_T(K, PS.T_coarse, tiT[q], tx[q], jT, y);
-        const CellGroups cg = groups_at(K, T, log_near(lref, T), !(far || bulk));
-        RTa[q] = (float)cg.RT;
-        C0a[q] = (float)cg.C0;
-        kq[q] = cg.KC;
+        double RT, C0;
+        cell_tfc(K, sm.kp, tfc_T(K, PS.T_coarse, tiT[q], tx[q], jT, y), !(far || bulk), RT, C0, kq[q]);
+        RTa[q] = (float)RT;
+        C0a[q] = (float)C0;
       }
       *reinterpret_cast<double2 *>(&sm.kc[rr][bc]) = make_double2(kq[0], kq[1]);
       *reinterpret_cast<double2 *>(&sm.kc[rr][bc + 2]) = make_double2(kq[2], kq[3]);
@@ -600,10 +603,10 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
         int iT;
         double xc;
         tfc_col(K, PS.i_left_end_T, g, iT, xc);
-        const double T = tfc_T(K, PS.T_coarse, iT, xc, sm.tj[rr], sm.ty[rr]);
-        const CellGroups cg = groups_at(K, T, log_near(lref, T), __float_as_uint(pv) != kMinus1);
-        cell_terms(F, pv, sm.d[rr][x], (float)cg.RT, (float)cg.C0, Sh, mh);
-        kh = cg.KC;
+        double RT, C0;
+        cell_tfc(K, sm.kp, tfc_T(K, PS.T_coarse, iT, xc, sm.tj[rr], sm.ty[rr]), __float_as_uint(pv) != kMinus1, RT,
+                 C0, kh);
+        cell_terms(F, pv, sm.d[rr][x], (float)RT, (float)C0, Sh, mh);
       } else {
         cell_terms(F, pv, sm.d[rr][x], tRT[g], tC0[g], Sh, mh);
       }

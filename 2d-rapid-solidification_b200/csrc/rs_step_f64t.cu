@@ -112,6 +112,7 @@ struct alignas(16) StSlot {
   uint32_t liq, sol;         // bit r: every cell of input row r has psi == -1 / +1
   double ty[kTRin];          // TFC: the row part of each input row's temperature
   int tj[kTRin];             // (tfc_row), once per tile
+  KcPoly kp;                 // TFC: K + C0 near the tile's temperature
 };
 // phases 2-4: the interface list and the partial sums
 struct P2Smem {
@@ -251,7 +252,6 @@ struct LaneCols {
   double RT[2], C0[2], dK[3];
   int tiT[2];       // TFC: the coarse column left of each of the lane's two columns
   double tx[2];     // and the column's offset from it, in coarse cells
-  LogRef lr;        // TFC: the lane's reference temperature for log_near
 };
 __device__ __forceinline__ CellGroups cell_groups(const TileView &V, int gx, int row) {
   int iT, jT;
@@ -270,10 +270,6 @@ __device__ __forceinline__ LaneCols lane_cols(const TileView &V) {
     L.dK[0] = L.dK[1] = L.dK[2] = 0.0;
     tfc_col(V.K, V.PS.i_left_end_T, V.gi, L.tiT[0], L.tx[0]);
     tfc_col(V.K, V.PS.i_left_end_T, V.gi + 1, L.tiT[1], L.tx[1]);
-    int jT;
-    double y;
-    tfc_row(V.K, V.y0, jT, y);
-    L.lr = log_ref(tfc_T(V.K, V.PS.T_coarse, L.tiT[0], L.tx[0], jT, y));
     return L;
   }
   const double2 RTv = ld2(V.T.RT + V.gi), C0v = ld2(V.T.C0 + V.gi);
@@ -286,7 +282,6 @@ __device__ __forceinline__ LaneCols lane_cols(const TileView &V) {
   L.dK[2] = V.T.DK[V.gi + 1];
   L.tiT[0] = L.tiT[1] = 0;
   L.tx[0] = L.tx[1] = 0.0;
-  L.lr = LogRef{0.0, 0.0, 0.0};
   return L;
 }
 
@@ -367,13 +362,9 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
       const int jT = st.tj[rr];
       const double y = st.ty[rr];
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const double T = tfc_T(V.K, V.PS.T_coarse, LC.tiT[q], LC.tx[q], jT, y);
-        const CellGroups cg = groups_at(V.K, T, log_near(LC.lr, T), !(far || bulk));
-        RTa[q] = cg.RT;
-        C0a[q] = cg.C0;
-        KCa[q] = cg.KC;
-      }
+      for (int q = 0; q < 2; ++q)
+        cell_tfc(V.K, st.kp, tfc_T(V.K, V.PS.T_coarse, LC.tiT[q], LC.tx[q], jT, y), !(far || bulk), RTa[q], C0a[q],
+                 KCa[q]);
     }
     uint32_t code;
     bool deep = false;
@@ -458,10 +449,11 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
         int iT;
         double xc;
         tfc_col(V.K, V.PS.i_left_end_T, g, iT, xc);
-        const double T = tfc_T(V.K, V.PS.T_coarse, iT, xc, st.tj[rr], st.ty[rr]);
-        const CellGroups cg = groups_at(V.K, T, log_near(LC.lr, T), bits(pv) != kMinus1);
-        cell_terms(F, pv, cv, sv, fabs(sv) < 1.0 / 9.0, cg.RT, cg.C0, Sh, mh);
-        mh += cg.KC;
+        double RT, C0, KC;
+        cell_tfc(V.K, st.kp, tfc_T(V.K, V.PS.T_coarse, iT, xc, st.tj[rr], st.ty[rr]), bits(pv) != kMinus1, RT, C0,
+                 KC);
+        cell_terms(F, pv, cv, sv, fabs(sv) < 1.0 / 9.0, RT, C0, Sh, mh);
+        mh += KC;
       } else {
         cell_terms(F, pv, cv, sv, fabs(sv) < 1.0 / 9.0, V.T.RT[g], V.T.C0[g], Sh, mh);
       }
@@ -848,6 +840,13 @@ __global__ void __launch_bounds__(kThreads, 5)
   const LaneCols LC = lane_cols<TFC>(V);
   if constexpr (TFC) {  // the row part of the cells' temperatures, once per tile row
     if (threadIdx.x < kTRin) tfc_row(K, y0 - 1 + (int)threadIdx.x, sm.st.tj[threadIdx.x], sm.st.ty[threadIdx.x]);
+    if (threadIdx.x == kTRin) {  // K + C0 about the temperature of the tile's centre
+      int iT, jT;
+      double x, y;
+      tfc_col(K, PS.i_left_end_T, x0 + kW / 2, iT, x);
+      tfc_row(K, y0 + kTR / 2, jT, y);
+      sm.st.kp = kc_poly(K, tfc_T(K, PS.T_coarse, iT, x, jT, y));
+    }
   }
   __syncthreads();  // barrier initialised, flags cleared (and the TFC row table written)
   {

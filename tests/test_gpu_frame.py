@@ -104,8 +104,8 @@ def test_initial_conditions(dtype):
     assert maxabs(g.psi, o.psi) <= tol and maxabs(g.c, o.c) <= tol
 
 
-def tfc_params():
-    p = configs.small(64, 42, i_tip_target=20, tfc=1, G=1e7, V=0.5)
+def tfc_params(G=1e7):
+    p = configs.small(64, 42, i_tip_target=20, tfc=1, G=G, V=0.5)
     p.length_sample_um = 1.0
     # coarse domain starts 30 cells left of the window (i_left_end ~ 30)
     p.Tcold = p.T_ref - p.GG * p.dx * p.S * p.W0 * (p.i_tip_target + 30)
@@ -151,10 +151,14 @@ def test_temperature_kernels():
     assert maxabs(Tf.cpu().numpy(), Tfo) <= 1e-11
 
 
-def test_tfc_step_f64():
+@pytest.mark.parametrize("G", [1e7, 5e8])
+def test_tfc_step_f64(G):
     """The fused step evaluates the fine T by bilinear interpolation of the
-    coarse T on the fly; same result as interpolate_temperature + step."""
-    p = tfc_params()
+    coarse T on the fly; same result as interpolate_temperature + step.  At
+    G = 1e7 K/m every cell is within 4 K of its tile's reference temperature
+    (K + C0 by its Taylor polynomial); at 5e8 K/m (0.5 K per cell) most cells
+    are not, and take the cell form."""
+    p = tfc_params(G)
     d = pyoracle.derive(p)
     ctx = lib.Context(p)
     nT = d.NxT_all * d.NyT_all
