@@ -59,8 +59,8 @@
 // store in step).
 // The coarse-grid temperature (TFC, interpolate_temperature fun.cu:1580-1608)
 // takes tile_kernel_tfc alone: every cell evaluates its CALPHAD groups from its
-// own bilinear temperature (the melt rows only the liquid functions, log T by
-// the series of log_near), keeps K + C0 in FP64 in shared memory, and the
+// own bilinear temperature (K + C0 by its Taylor polynomial about the tile's
+// centre temperature, kc_poly), keeps K + C0 in FP64 in shared memory, and the
 // faces add its differences, rounded to FP32, along both axes; tiles of 8
 // output rows, so that the FP64 array fits with five CTAs per SM.
 // Fields store psi and delta = c - cinf (include/rs_b200.h).

@@ -54,9 +54,10 @@
 // tile of the block launched one resident wave later.
 // The coarse-grid temperature (TFC, interpolate_temperature
 // fun.cu:1580-1608): no table kernel; every cell evaluates its CALPHAD groups
-// from its own bilinear temperature (melt rows only the liquid functions, log
-// T by the series of log_near) and stores mu = mu'' + (K + C0), so the faces
-// take plain differences of mu.  The tile kernel then runs in plain stream
+// from its own bilinear temperature (K + C0 by its Taylor polynomial about
+// the tile's centre temperature, kc_poly; C0 in general rows and cells out of
+// the polynomial's range by the Gibbs functions) and stores
+// mu = mu'' + (K + C0), so the faces take plain differences of mu.  The tile kernel then runs in plain stream
 // order: it issues its TMA loads before griddepcontrol.wait.
 //
 // Two kernels run these phases (same functions, same results bit for bit):
