@@ -295,17 +295,18 @@ __device__ __forceinline__ double log_near(const LogRef &L, double T) {
 // g_ti_liq's upper and g_nb_liq's lower piece, fun.cu:1628-1669), whose
 // derivatives are closed forms; the remainder after degree 6 is below
 // |KC^(7)| |T - T0|^7 / 7! < 2e-16 J/mol for |T - T0| <= 4 K.  The constant
-// term is the cell form itself (groups_at) at T0.  Cells outside the range
-// or farther than 4 K from T0 take groups_at.
+// term is the cell form itself (groups_at) at T0.  Cells farther than 4 K from
+// T0, or all cells when T0 is not in [1945, 2746) K (so that the cells within
+// 4 K of it stay in [1941, 2750) K), take groups_at.
 struct KcPoly {
   LogRef lr;     // T0, log T0, 1 / T0 (also log_near's reference)
   double c[7];   // KC^(k)(T0) / k!
-  int ok;        // T0 in [1941, 2750)
+  int ok;        // T0 in [1945, 2746)
 };
 __device__ __forceinline__ KcPoly kc_poly(const StepCoef &K, double T0) {
   KcPoly P;
   P.lr = log_ref(T0);
-  P.ok = T0 >= 1941.0 && T0 < 2750.0;
+  P.ok = T0 >= 1945.0 && T0 < 2746.0;
   constexpr double c = -46.29 + 26.4711, d = -0.203475e-3, e = 0.35012e-6, f = -93399.0, h = 306.098e-25;
   const double b = (298.7367 - 131.229057) + K.RR * K.Lref;
   const double T = T0, lT = P.lr.lT0, i1 = P.lr.iT0;
@@ -323,12 +324,22 @@ __device__ __forceinline__ KcPoly kc_poly(const StepCoef &K, double T0) {
 // K + C0 at T from P, or false where the polynomial does not apply
 __device__ __forceinline__ bool kc_eval(const KcPoly &P, double T, double &kc) {
   const double u = T - P.lr.T0;
-  if (!P.ok || !(T >= 1941.0 && T < 2750.0 && fabs(u) <= 4.0)) return false;
+  if (!(P.ok && fabs(u) <= 4.0)) return false;
   double r = P.c[6];
 #pragma unroll
   for (int k = 5; k >= 0; --k) r = fma(r, u, P.c[k]);
   kc = r;
   return true;
+}
+// the cell form of the groups, out of line: the general rows and the cells
+// the polynomial does not cover are few, and one copy of the code keeps the
+// tile kernels' instruction footprint small
+static __device__ __noinline__ CellGroups groups_cell(const StepCoef &K, const LogRef &L, double T, bool full) {
+  return groups_at(K, T, log_near(L, T), full);
+}
+// every group of a cell, the logarithm exact (interface cells), out of line
+static __device__ __noinline__ CellGroups groups_exact(const StepCoef &K, double T) {
+  return groups_at(K, T, log(T), true);
 }
 // the groups a cell needs: RT and K + C0 always, C0 where full (the general
 // row form; the melt forms multiply C0 by g + 1 = 0)
@@ -338,7 +349,7 @@ __device__ __forceinline__ void cell_tfc(const StepCoef &K, const KcPoly &P, dou
   C0 = 0.0;
   const bool poly = kc_eval(P, T, KC);
   if (!poly || full) {
-    const CellGroups g = groups_at(K, T, log_near(P.lr, T), full);
+    const CellGroups g = groups_cell(K, P.lr, T, full);
     C0 = g.C0;
     if (!poly) KC = g.KC;
   }

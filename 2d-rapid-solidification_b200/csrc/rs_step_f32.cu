@@ -111,6 +111,8 @@ struct alignas(128) TileSmemT {
   double ty[kRin];          // TFC: the row part of each input row's temperature
   int tj[kRin];             // (tfc_row), once per tile
   std::conditional_t<TFC, KcPoly, char> kp;  // TFC: K + C0 near the tile's temperature
+  double hx[2];             // TFC: column part of the halo columns' temperatures
+  int hiT[2];
   int nlist;
   double part_mass[kWarps];
   int part_itip[kWarps];
@@ -278,6 +280,10 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
 #pragma unroll
     for (int q = 0; q < 4; ++q) tfc_col(K, PS.i_left_end_T, gi + q, tiT[q], tx[q]);
     if (threadIdx.x < kTRin) tfc_row(K, y0 - 1 + (int)threadIdx.x, sm.tj[threadIdx.x], sm.ty[threadIdx.x]);
+    if (threadIdx.x >= kTRin + 1 && threadIdx.x < kTRin + 3) {  // the halo columns x0-1, x0+kW
+      const int side = (int)threadIdx.x - (kTRin + 1);
+      tfc_col(K, PS.i_left_end_T, side ? x0 + kW : x0 - 1, sm.hiT[side], sm.hx[side]);
+    }
     if (threadIdx.x == kTRin) {
       int iT, jT;
       double x, y;
@@ -292,8 +298,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     double x, y;
     tfc_col(K, PS.i_left_end_T, gx, iT, x);
     tfc_row(K, row, jT, y);
-    const double T = tfc_T(K, PS.T_coarse, iT, x, jT, y);
-    return groups_at(K, T, log(T), true);
+    return groups_exact(K, tfc_T(K, PS.T_coarse, iT, x, jT, y));
   };
   // surrogate: per-lane fragments, and the scaled inputs as T(x) = TnA + TnB x
   // (tile column x; frozen T is linear in the column) and c = cnA + delta c_ihalf
@@ -600,12 +605,9 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
       if constexpr (TFC) {
         // C0 enters mu'' as (g + 1) C0, 0 at psi = -1 exactly: the liquid
         // groups suffice there
-        int iT;
-        double xc;
-        tfc_col(K, PS.i_left_end_T, g, iT, xc);
         double RT, C0;
-        cell_tfc(K, sm.kp, tfc_T(K, PS.T_coarse, iT, xc, sm.tj[rr], sm.ty[rr]), __float_as_uint(pv) != kMinus1, RT,
-                 C0, kh);
+        cell_tfc(K, sm.kp, tfc_T(K, PS.T_coarse, sm.hiT[side], sm.hx[side], sm.tj[rr], sm.ty[rr]),
+                 __float_as_uint(pv) != kMinus1, RT, C0, kh);
         cell_terms(F, pv, sm.d[rr][x], (float)RT, (float)C0, Sh, mh);
       } else {
         cell_terms(F, pv, sm.d[rr][x], tRT[g], tC0[g], Sh, mh);

@@ -114,6 +114,8 @@ struct alignas(16) StSlot {
   double ty[kTRin];          // TFC: the row part of each input row's temperature
   int tj[kTRin];             // (tfc_row), once per tile
   KcPoly kp;                 // TFC: K + C0 near the tile's temperature
+  double hx[2];              // TFC: column part of the halo columns' temperatures
+  int hiT[2];
 };
 // phases 2-4: the interface list and the partial sums
 struct P2Smem {
@@ -259,8 +261,7 @@ __device__ __forceinline__ CellGroups cell_groups(const TileView &V, int gx, int
   double x, y;
   tfc_col(V.K, V.PS.i_left_end_T, gx, iT, x);
   tfc_row(V.K, row, jT, y);
-  const double T = tfc_T(V.K, V.PS.T_coarse, iT, x, jT, y);
-  return groups_at(V.K, T, log(T), true);
+  return groups_exact(V.K, tfc_T(V.K, V.PS.T_coarse, iT, x, jT, y));
 }
 
 template <bool TFC>
@@ -447,12 +448,9 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
       if constexpr (TFC) {
         // C0 enters mu'' as (g + 1) C0, 0 at psi = -1 exactly: the liquid
         // groups suffice there
-        int iT;
-        double xc;
-        tfc_col(V.K, V.PS.i_left_end_T, g, iT, xc);
         double RT, C0, KC;
-        cell_tfc(V.K, st.kp, tfc_T(V.K, V.PS.T_coarse, iT, xc, st.tj[rr], st.ty[rr]), bits(pv) != kMinus1, RT, C0,
-                 KC);
+        cell_tfc(V.K, st.kp, tfc_T(V.K, V.PS.T_coarse, st.hiT[side], st.hx[side], st.tj[rr], st.ty[rr]),
+                 bits(pv) != kMinus1, RT, C0, KC);
         cell_terms(F, pv, cv, sv, fabs(sv) < 1.0 / 9.0, RT, C0, Sh, mh);
         mh += KC;
       } else {
@@ -841,6 +839,10 @@ __global__ void __launch_bounds__(kThreads, 5)
   const LaneCols LC = lane_cols<TFC>(V);
   if constexpr (TFC) {  // the row part of the cells' temperatures, once per tile row
     if (threadIdx.x < kTRin) tfc_row(K, y0 - 1 + (int)threadIdx.x, sm.st.tj[threadIdx.x], sm.st.ty[threadIdx.x]);
+    if (threadIdx.x >= kTRin + 1 && threadIdx.x < kTRin + 3) {  // the halo columns x0-1, x0+kW
+      const int side = (int)threadIdx.x - (kTRin + 1);
+      tfc_col(K, PS.i_left_end_T, side ? x0 + kW : x0 - 1, sm.st.hiT[side], sm.st.hx[side]);
+    }
     if (threadIdx.x == kTRin) {  // K + C0 about the temperature of the tile's centre
       int iT, jT;
       double x, y;
