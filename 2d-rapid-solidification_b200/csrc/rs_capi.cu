@@ -402,7 +402,7 @@ static int check_fields(const rs_ctx *c, const rs_fields *f, const char *what, b
   return RS_OK;
 }
 
-static rs::StepScalars step_scalars(const rs_ctx *c, const rs_step_args *a) {
+static rs::StepScalars step_scalars(const rs_ctx *c, const rs_step_args *a, const rs_fields *cur) {
   const rs_params &p = c->p;
   rs::StepScalars P;
   memset(&P, 0, sizeof(P));
@@ -418,6 +418,8 @@ static rs::StepScalars step_scalars(const rs_ctx *c, const rs_step_args *a) {
   P.i_front = p.i_tip_target;
   P.wait_limit = c->wait_limit;
   P.T_coarse = (const double *)a->T_coarse;
+  P.src_psi = cur->psi;
+  P.src_c = cur->c;
   return P;
 }
 
@@ -430,7 +432,7 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
   if (cur->psi == next->psi || cur->c == next->c || (next->phi && (next->phi == cur->psi || next->phi == cur->c)))
     return fail(RS_E_INVALID, "rs_step: cur and next alias");
   if (c->p.tfc && !a->T_coarse) return fail(RS_E_INVALID, "rs_step: TFC needs T_coarse");
-  const rs::StepScalars P = step_scalars(c, a);
+  const rs::StepScalars P = step_scalars(c, a, cur);
   cudaStream_t st = (cudaStream_t)stream;
   c->pb_cur = a->pull_back ? cur->psi : nullptr;
   c->pb_offset = a->pull_back ? a->i_offset : 0;
@@ -444,7 +446,7 @@ int rs_step(rs_ctx *c, const rs_fields *cur, const rs_fields *next, const rs_ste
   const bool out_aligned =
       ((uintptr_t)next->psi % vec) == 0 && ((uintptr_t)next->c % vec) == 0 && ((uintptr_t)next->phi % vec) == 0;
   const int box_rows = c->p.tfc && cur->precision == RS_F32 ? rs::kTfcTileRows32 + 2 : rs::kTmaBoxH;
-  if (c->use_tma && out_aligned && !a->pull_back && field_map(c, cur->psi, cur->precision, box_rows, &tm.psi) &&
+  if (c->use_tma && out_aligned && field_map(c, cur->psi, cur->precision, box_rows, &tm.psi) &&
       field_map(c, cur->c, cur->precision, box_rows, &tm.c)) {
     tm.col_tab = c->col_tab;
     tm.col_tab_len = c->col_tab_len;

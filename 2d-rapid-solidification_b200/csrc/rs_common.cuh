@@ -234,6 +234,9 @@ struct StepScalars {
   // default); a test option makes it tiny so that the give-up path runs
   uint32_t wait_limit;
   const double *T_coarse;
+  // the current fields (the tile kernels gather a pull-back step's shifted
+  // tile through them instead of a TMA box)
+  const void *src_psi, *src_c;
 };
 
 }  // namespace rs

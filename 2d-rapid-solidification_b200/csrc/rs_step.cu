@@ -11,10 +11,10 @@
 //   * ghost cells (compute_boundary_individual, fun.cu:1220-1230) are written
 //     by the cell they copy, corners included.
 //
-// Three kernels: this file's register-prefetch kernel (pull-back steps,
-// unaligned fields, RS_OPT_TMA = 0) and the TMA-staged tile kernels of
-// rs_step_f32.cu (FP32) and rs_step_f64t.cu (FP64), frozen and coarse-grid
-// temperature.
+// Three kernels: this file's register-prefetch kernel (unaligned fields,
+// RS_OPT_TMA = 0) and the TMA-staged tile kernels of rs_step_f32.cu (FP32) and
+// rs_step_f64t.cu (FP64): frozen and coarse-grid temperature, pull-back steps
+// included (those gather their shifted tile).
 //
 // Layout of the work here: a warp owns a strip of 30 output columns (32 input
 // columns with a one-column halo on each side) and marches down H rows (H
@@ -324,7 +324,7 @@ static int launch(const StepCoef &K, const StepScalars &P, const typename Tr<R>:
   const Coef<R> F = make_coef<R>(K);
   const int ni = K.nx - 2, nj = K.ny - 2;
   const bool tfc = K.tfc != 0;
-  if (tm && !P.pull_back) {
+  if (tm) {
     if constexpr (sizeof(R) == 4)
       return launch_step_f32_tma(K, make_coef<float>(K), P, *tm, (float *)psi_n, (float *)c_n, (float *)phi_n,
                                  partials, max_partials, nwarps_out, err, st);

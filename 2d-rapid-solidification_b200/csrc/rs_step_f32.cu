@@ -221,12 +221,19 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     if (threadIdx.x == 0) atomicExch(err, 2);
     return;
   }
+  // a pull-back step reads column clamp(i + i_offset, 1, nx - 2) for column i
+  // (pull_back, fun.cu:1469-1492): no TMA box has that shape, so the CTA
+  // gathers its tile instead (same box, zeros outside the array, delta = 0
+  // where the source is column nx - 2: the melt entering at the right edge)
+  const bool pb = PS.pull_back != 0;
   if (threadIdx.x == 0) {
     mbar_init(&sm.full, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    mbar_expect_tx(&sm.full, kTileBytes);
-    tma_load_2d(&sm.psi[0][0], tm_psi, &sm.full, x0 - 4, y0 - 1);
-    tma_load_2d(&sm.d[0][0], tm_c, &sm.full, x0 - 4, y0 - 1);
+    if (!pb) {
+      mbar_expect_tx(&sm.full, kTileBytes);
+      tma_load_2d(&sm.psi[0][0], tm_psi, &sm.full, x0 - 4, y0 - 1);
+      tma_load_2d(&sm.d[0][0], tm_c, &sm.full, x0 - 4, y0 - 1);
+    }
     sm.liq = 0;
     sm.sol = 0;
     sm.nlist = 0;
@@ -410,8 +417,25 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
     int *sm_i = reinterpret_cast<int *>(&sm.mu[0][0]);
     final_reduce(*FR, sm_m, sm_i, (int)threadIdx.x, [] { __syncthreads(); });
   };
-  __syncthreads();  // barrier initialised, flags cleared
-  {
+  if (pb) {
+    const float *__restrict__ gpsi = static_cast<const float *>(PS.src_psi);
+    const float *__restrict__ gd = static_cast<const float *>(PS.src_c);
+    for (int k = threadIdx.x; k < kTRin * kWin; k += kThreads) {
+      const int rr = k / kWin, x = k % kWin;
+      const int row = y0 - 1 + rr, g = x0 - 4 + x;
+      float pv = 0.f, dv = 0.f;
+      if (row <= ny - 1 && g >= 0 && g <= nx - 1) {
+        const int si = min(max(g + PS.i_offset, 1), nx - 2);
+        const int64_t o = (int64_t)row * K.pitch + si;
+        pv = gpsi[o];
+        dv = si >= nx - 2 ? 0.f : gd[o];
+      }
+      sm.psi[rr][x] = pv;
+      sm.d[rr][x] = dv;
+    }
+  }
+  __syncthreads();  // barrier initialised, flags cleared (a pull-back tile gathered)
+  if (!pb) {
     // bounded wait for the tile; if any thread gives up, the whole CTA skips
     // the tile: no phase runs on a partly filled tile and nothing is stored.
     // Thread 0 first waits (bounded again) for the load still in flight into
@@ -652,7 +676,7 @@ __device__ __forceinline__ void tile_body(const StepCoef &K, const Coef<float> &
   // phase 1 done: pull the tile of the CTA that will start about one resident
   // wave later into L2, so its loads overlap the rest of this wave's
   // arithmetic (issued after the own load and phase 1, it measured fastest)
-  if (threadIdx.x == 0) prefetch();
+  if (threadIdx.x == 0 && !pb) prefetch();
 
   // ---- phase 2: warp w computes output rows 1 + 4w .. 4 + 4w of the tile
   const Mask liq = sm.liq, sol = sm.sol;
@@ -1914,7 +1938,7 @@ int launch_step_f32_tma(const StepCoef &K, const Coef<float> &F, const StepScala
     if (nparts_out) *nparts_out = np;
     return 0;
   }
-  if (tm.pipeline && !surr) {  // the persistent warp-role kernel (exact path)
+  if (tm.pipeline && !surr && !P.pull_back) {  // the persistent warp-role kernel (exact path)
     const int nrt = (int)grid.x, ncb = (int)grid.y;
     const size_t psmem = sizeof(PipeSmem32);
     static std::atomic<unsigned long long> pattr{0};

@@ -799,6 +799,29 @@ __device__ __forceinline__ void tile_of(int t, int nrt, int ncb, int f, int &tr,
 }
 
 // ---------------------------------------------------------------- one tile per CTA
+// the input tile of a pull-back step: the same box as the TMA load (columns
+// x0-4 .. x0+kW+3, rows y0-1 .. y0+kTR, zeros outside the array), each
+// column i read from clamp(i + i_offset, 1, nx - 2), with c = cinf where that
+// is nx - 2 (the melt entering at the right edge)
+__device__ __forceinline__ void gather_pull_back(const StepCoef &K, const StepScalars &PS, int x0, int y0,
+                                                 InSlot &in) {
+  const double *__restrict__ psi = static_cast<const double *>(PS.src_psi);
+  const double *__restrict__ c = static_cast<const double *>(PS.src_c);
+  for (int k = threadIdx.x; k < kTRin * kWin; k += kThreads) {
+    const int rr = k / kWin, x = k % kWin;
+    const int row = y0 - 1 + rr, g = x0 - 4 + x;
+    double pv = 0.0, cv = 0.0;
+    if (row <= K.ny - 1 && g >= 0 && g <= K.nx - 1) {
+      const int si = min(max(g + PS.i_offset, 1), K.nx - 2);
+      const int64_t o = (int64_t)row * K.pitch + si;
+      pv = psi[o];
+      cv = si >= K.nx - 2 ? K.cinf : c[o];
+    }
+    in.psi[rr][x] = pv;
+    in.c[rr][x] = cv;
+  }
+}
+
 template <bool TFC>
 __global__ void __launch_bounds__(kThreads, 5)
     tile_kernel_f64(const __grid_constant__ StepCoef K, const __grid_constant__ Coef<double> F,
@@ -821,12 +844,18 @@ __global__ void __launch_bounds__(kThreads, 5)
     if (threadIdx.x == 0) atomicExch(err, 2);
     return;
   }
+  // a pull-back step reads column clamp(i + i_offset, 1, nx - 2) for column i
+  // (pull_back, fun.cu:1469-1492): no TMA box has that shape, so the CTA
+  // gathers its tile (gather_pull_back) instead
+  const bool pb = PS.pull_back != 0;
   if (threadIdx.x == 0) {
     mbar_init(&sm.full, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    mbar_expect_tx(&sm.full, kTileBytes);
-    tma_load_2d(&sm.in.psi[0][0], &tm_psi, &sm.full, x0 - 4, y0 - 1);
-    tma_load_2d(&sm.in.c[0][0], &tm_c, &sm.full, x0 - 4, y0 - 1);
+    if (!pb) {
+      mbar_expect_tx(&sm.full, kTileBytes);
+      tma_load_2d(&sm.in.psi[0][0], &tm_psi, &sm.full, x0 - 4, y0 - 1);
+      tma_load_2d(&sm.in.c[0][0], &tm_c, &sm.full, x0 - 4, y0 - 1);
+    }
     sm.st.liq = 0u;
     sm.st.sol = 0u;
     sm.p2.nlist = 0;
@@ -851,8 +880,9 @@ __global__ void __launch_bounds__(kThreads, 5)
       sm.st.kp = kc_poly(K, tfc_T(K, PS.T_coarse, iT, x, jT, y));
     }
   }
+  if (pb) gather_pull_back(K, PS, x0, y0, sm.in);
   __syncthreads();  // barrier initialised, flags cleared (and the TFC row table written)
-  {
+  if (!pb) {
     // bounded wait for the tile; if any thread gives up, the whole CTA skips
     // the tile: no phase runs on a partly filled tile and nothing is stored.
     // Thread 0 first waits (bounded again) for the load still in flight into
@@ -883,7 +913,7 @@ __global__ void __launch_bounds__(kThreads, 5)
   __syncthreads();
   // phase 1 done: pull the tile of the CTA that will start about one resident
   // wave later into L2, so its loads overlap the rest of this wave's arithmetic
-  if (threadIdx.x == 0 && wave > 0) {
+  if (threadIdx.x == 0 && wave > 0 && !pb) {
     const unsigned nxt = blockIdx.y * gridDim.x + blockIdx.x + (unsigned)wave;
     if (nxt < gridDim.x * gridDim.y) {
       int pr, pc;
@@ -1077,7 +1107,7 @@ int launch_step_f64_tma(const StepCoef &K, const Coef<double> &F, const StepScal
   // persistent pipeline has no TFC form and is not taken then)
   const bool tfc = K.tfc != 0;
   if (tfc && !P.T_coarse) return -1;
-  const bool pipe = tm.pipeline != 0 && !tfc;
+  const bool pipe = tm.pipeline != 0 && !tfc && !P.pull_back;
   const int which = pipe ? 1 : tfc ? 2 : 0;
   const size_t smem = pipe ? sizeof(PipeSmem64) : sizeof(TileSmem64);
   const void *kfn = pipe ? (const void *)pipe_kernel_f64

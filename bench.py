@@ -195,12 +195,12 @@ class Loop:
             self.hist += pb
         self.ctx.step(self.a, self.b, n, i_offset_history=self.hist, l_offset_Vp=self.l, pull_back=pb,
                       mass_out=mass_out)
-        # a pull-back step is one register-kernel launch (+1 reduction for the
-        # mass); the others launch the column table and the tile kernel, which
+        # every step, pull-back steps included (the tile kernel gathers the
+        # shifted tile), launches the column table and the tile kernel, which
         # reduces the mass itself
         red = 1 if mass_out is not None else 0
         _, nl, fused = STEP_PATH[self.prec]
-        self.launches += (1 + red) if pb is not None else nl + (0 if fused else red)
+        self.launches += nl + (0 if fused else red)
         self.l += p.Vp * d.dt * d.tau0 / (p.S * p.W0)
         self.a, self.b = self.b, self.a
         self.n = n + 1

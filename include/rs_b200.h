@@ -182,9 +182,9 @@ int rs_destroy(rs_ctx *ctx);
 int rs_get_derived(const rs_ctx *ctx, rs_derived *d);
 
 /* Options: RS_OPT_TMA (default 1) stages the step's field tiles into shared
- * memory with TMA copies (frozen and coarse-grid temperature); 0 selects the
- * register-prefetch kernel (always used for pull-back steps and unaligned
- * fields).
+ * memory (TMA copies; a pull-back step's shifted tile by a gather), frozen and
+ * coarse-grid temperature; 0 selects the register-prefetch kernel (always used
+ * for fields whose rows are not 16-byte aligned).
  * RS_OPT_WAIT_LIMIT (default 0: the kernels' own limit of 2^20 suspending
  * tries) bounds the tile kernels' waits for their TMA loads; when set, a wait
  * polls without suspending and gives up after that many polls.  A tile whose

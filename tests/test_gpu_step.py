@@ -148,17 +148,40 @@ def test_rotated_orientation_f64():
     assert maxabs(g.psi, o.psi) <= 1e-13 and maxabs(g.c, o.c) <= 1e-13
 
 
-@pytest.mark.parametrize("off", [-2, 0, 3])
-def test_fused_pull_back_step_f64(off):
+@pytest.mark.parametrize("tma", [1, 0])
+@pytest.mark.parametrize("off", [-2, 0, 3, 40])
+def test_fused_pull_back_step_f64(off, tma):
+    """A pull-back step fused into rs_step (the tile kernel gathers its
+    shifted tile; the register kernel remaps its loads) against the oracle's
+    pull_back then step; off = 40 fills most columns from the right edge."""
     p = make("default")
     d = pyoracle.derive(p)
     s = perturbed_state(p, 23, amp=0.2)
     ctx = lib.Context(p)
+    ctx.set_option(_abi.RS_OPT_TMA, tma)
     cur, nxt = upload(p, s), lib.FieldSet(p, torch.float64)
     ctx.step(cur, nxt, 0, i_offset_history=off, pull_back=off)
     o = pyoracle.step(p, d, pyoracle.pull_back(p, s, off), 0, off, 0.0)
     g = download(p, nxt)
     assert maxabs(g.psi, o.psi) <= 1e-13 and maxabs(g.c, o.c) <= 1e-13
+
+
+@pytest.mark.parametrize("tma", [1, 0])
+@pytest.mark.parametrize("off", [-2, 3, 40])
+def test_fused_pull_back_step_f32(off, tma):
+    p = make("steep", 64, 48)
+    d = pyoracle.derive(p)
+    s = perturbed_state(p, 8, amp=0.25)
+    ctx = lib.Context(p)
+    ctx.set_option(_abi.RS_OPT_TMA, tma)
+    cur, nxt = upload(p, s, torch.float32), lib.FieldSet(p, torch.float32)
+    ctx.step(cur, nxt, 0, i_offset_history=off, pull_back=off)
+    sp = pyoracle.pull_back(p, s, off)
+    o = pyoracle.step(p, d, sp, 0, off, 0.0)
+    g = download(p, nxt)
+    # increments over the shifted state, as for the unshifted FP32 step
+    assert maxabs(g.psi - sp.psi, o.psi - sp.psi) <= 5e-6
+    assert maxabs(g.c - sp.c, o.c - sp.c) <= 5e-8
 
 
 def run_gpu(ctx, p, d, s, nsteps, dtype=torch.float64):
