@@ -341,6 +341,11 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
   const int rows_in = V.K.ny - V.y0;  // input rows inside the array: rr <= ny - y0
   // this warp's row flags (warp-uniform), OR-ed into st.liq / st.sol once
   uint32_t liq_rows = 0u, sol_rows = 0u;
+  // TFC: along a column the bilinear temperature is P + Q y within one coarse
+  // row band jT; the lane keeps P and Q of its two columns for the band of
+  // its last row (rows of a warp are 4 apart, bands `ratio` rows high)
+  int band_jT = -1;
+  double Pb[2] = {0.0, 0.0}, Qb[2] = {0.0, 0.0};
 #pragma unroll 1
   for (int rr = V.gw; rr < kTRin; rr += kWarps) {
     if (rr > rows_in) {  // beyond the array (last tile): never read by an output
@@ -363,10 +368,19 @@ __device__ __forceinline__ void phase1(const TileView &V, const LaneCols &LC, co
     if constexpr (TFC) {  // the melt forms need RT and K + C0 only
       const int jT = st.tj[rr];
       const double y = st.ty[rr];
+      if (jT != band_jT) {  // warp-uniform: jT depends on the row only
+        band_jT = jT;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const double *r0 = V.PS.T_coarse + (int64_t)jT * V.K.NxT_all + LC.tiT[q], *r1 = r0 + V.K.NxT_all;
+          const double f00 = r0[0], f10 = r0[1], f01 = r1[0], f11 = r1[1];
+          Pb[q] = fma(f10 - f00, LC.tx[q], f00);
+          Qb[q] = fma(f11 - f10 - f01 + f00, LC.tx[q], f01 - f00);
+        }
+      }
 #pragma unroll
       for (int q = 0; q < 2; ++q)
-        cell_tfc(V.K, st.kp, tfc_T(V.K, V.PS.T_coarse, LC.tiT[q], LC.tx[q], jT, y), !(far || bulk), RTa[q], C0a[q],
-                 KCa[q]);
+        cell_tfc(V.K, st.kp, fma(Qb[q], y, Pb[q]), !(far || bulk), RTa[q], C0a[q], KCa[q]);
     }
     uint32_t code;
     bool deep = false;
